@@ -1,0 +1,221 @@
+"""ctypes mirror of include/cicy_b200.h and the loader of libcicy_b200.so.
+
+The shared library is the product; this module only declares its C types and
+signatures.  Loading fails loudly when the library is missing: there is no
+Python or CPU fallback for the device path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcicy_b200.so")
+
+CICY_OK = 0
+STATUS_NAMES = {
+    0: "CICY_OK",
+    1: "CICY_E_INPUT",
+    2: "CICY_E_CAPACITY",
+    3: "CICY_E_DEVICE",
+    4: "CICY_E_TIMEOUT",
+    5: "CICY_E_ZERO_DIAGONAL",
+    6: "CICY_E_STATE",
+    7: "CICY_E_INTERNAL",
+}
+
+i32p = C.POINTER(C.c_int32)
+i64p = C.POINTER(C.c_int64)
+f64p = C.POINTER(C.c_double)
+
+
+class Cuboid(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("min_x", "min_y", "min_z", "len_x", "len_y", "len_z", "max_x", "max_y", "max_z")]
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("gs_min", C.c_double * 3),
+        ("gs_overlap_cnt", C.c_double),
+        ("gs_overlap_gnp", C.c_double),
+        ("van_der_waals_dist", C.c_double),
+        ("tunneling_dist", C.c_double),
+        ("min_points", C.c_int32),
+        ("simulation_scope", C.c_int32),
+        ("resistances", C.c_int32 * 3),
+        ("junction_type", C.c_int32),
+        ("tolerance", C.c_double),
+        ("applied_voltage", C.c_double),
+        ("resistivity_cnt", C.c_double),
+        ("resistivity_matrix", C.c_double),
+        ("junction_resistance", C.c_double),
+        ("C1", C.c_double),
+        ("C2", C.c_double),
+    ]
+
+
+class Network(C.Structure):
+    _fields_ = [
+        ("n_points", C.c_int64),
+        ("x", f64p),
+        ("y", f64p),
+        ("z", f64p),
+        ("flag", i32p),
+        ("n_cnts", C.c_int32),
+        ("structure_ptr", i64p),
+        ("structure_idx", i64p),
+        ("radii", f64p),
+        ("n_inside", C.c_int32),
+        ("cnts_inside", i32p),
+        ("boundary_cnt_ptr", i64p),
+        ("boundary_cnt_idx", i32p),
+        ("boundary_pts_ptr", i64p),
+        ("boundary_pts_idx", i64p),
+        ("window", Cuboid),
+    ]
+
+
+class SolverOpts(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("preconditioner", C.c_int32), ("max_iter_factor", C.c_int32), ("reserved0", C.c_int32)]
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [
+        ("cluster", C.c_int32),
+        ("pass_", C.c_int32),
+        ("nodes", C.c_int64),
+        ("reserved", C.c_int64),
+        ("nnz_lower", C.c_int64),
+        ("iterations", C.c_int64),
+        ("rel_residual", C.c_double),
+        ("seconds", C.c_double),
+    ]
+
+
+class Result(C.Structure):
+    _fields_ = [
+        ("resistances", C.c_double * 3),
+        ("resistivities", C.c_double * 3),
+        ("n_slots", C.c_int64),
+        ("n_point_contacts", C.c_int64),
+        ("n_labels", C.c_int32),
+        ("n_junctions", C.c_int32),
+        ("n_percolated", C.c_int32),
+        ("n_solves", C.c_int32),
+        ("solves", SolveInfo * 32),
+        ("stage_seconds", C.c_double * 6),
+    ]
+
+
+class GenParams(C.Structure):
+    _fields_ = [
+        ("sample", Cuboid),
+        ("n_cnts", C.c_int32),
+        ("n_threads", C.c_int32),
+        ("seed", C.c_uint64),
+        ("step", C.c_double),
+        ("len_min", C.c_double),
+        ("len_max", C.c_double),
+        ("radius", C.c_double),
+        ("max_turn_rad", C.c_double),
+    ]
+
+
+class WindowParams(C.Structure):
+    _fields_ = [
+        ("sample", Cuboid),
+        ("win_max", C.c_double * 3),
+        ("win_min", C.c_double * 3),
+        ("win_delt", C.c_double * 3),
+        ("step_length", C.c_double),
+        ("min_points", C.c_int32),
+        ("reserved0", C.c_int32),
+    ]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libcicy_b200.so (built in-tree by cicy_geom_b200/build.py)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m cicy_geom_b200.build` (no CPU fallback exists)")
+    L = C.CDLL(LIB_PATH)
+    P = C.POINTER
+    sig = {
+        "cicy_ctx_create": (C.c_int, [P(C.c_void_p), C.c_int]),
+        "cicy_ctx_destroy": (C.c_int, [C.c_void_p]),
+        "cicy_ctx_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+        "cicy_ctx_stream": (C.c_void_p, [C.c_void_p]),
+        "cicy_ctx_set_solver": (C.c_int, [C.c_void_p, P(SolverOpts)]),
+        "cicy_last_error": (C.c_char_p, [C.c_void_p]),
+        "cicy_ctx_kernel_launches": (C.c_int64, [C.c_void_p]),
+        "cicy_upload_network": (C.c_int, [C.c_void_p, P(Network)]),
+        "cicy_contact_grid": (C.c_int, [C.c_void_p, P(Params)]),
+        "cicy_clusters": (C.c_int, [C.c_void_p, P(Params)]),
+        "cicy_electrical_analysis": (C.c_int, [C.c_void_p, P(Params), P(Result)]),
+        "cicy_network_to_conductance": (C.c_int, [C.c_void_p, P(Params), P(Result)]),
+        "cicy_get_sectioned_domain": (C.c_int, [C.c_void_p, i64p, i64p, i64p, i64p]),
+        "cicy_get_point_contacts": (C.c_int, [C.c_void_p, i64p, i64p, i32p, i64p, f64p]),
+        "cicy_get_labels": (C.c_int, [C.c_void_p, i32p, i32p, i32p]),
+        "cicy_get_junctions": (C.c_int, [C.c_void_p, i64p, i64p, i32p, i64p, i32p, f64p]),
+        "cicy_get_elements": (C.c_int, [C.c_void_p, C.c_int32, i64p, i64p, i64p, i64p]),
+        "cicy_get_clusters": (C.c_int, [C.c_void_p, C.c_int32, i32p, i64p, i64p, i32p, i32p, i64p, i64p, i32p]),
+        "cicy_get_system": (C.c_int, [C.c_void_p, C.c_int32, i64p, i64p, i64p, i64p, i64p, f64p, f64p, f64p, f64p, f64p]),
+        "cicy_generate_cnt_network": (C.c_int, [P(GenParams), P(C.c_void_p)]),
+        "cicy_extract_window": (C.c_int, [C.c_void_p, P(WindowParams), P(C.c_void_p)]),
+        "cicy_host_network_from_arrays": (C.c_int, [P(Network), P(C.c_void_p)]),
+        "cicy_host_network_view": (C.c_int, [C.c_void_p, P(Network)]),
+        "cicy_host_network_free": (None, [C.c_void_p]),
+        "cicy_host_last_error": (C.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        if not hasattr(L, name):  # completeness is asserted by tests/test_abi.py
+            continue
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def declared_symbols() -> list[str]:
+    """Function names declared in include/cicy_b200.h (parsed from the header)."""
+    import re
+
+    hdr = os.path.join(os.path.dirname(HERE), "include", "cicy_b200.h")
+    txt = open(hdr).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(cicy_[a-z0-9_]+)\s*\(", txt)))
+
+
+def ptr(a: np.ndarray, ctype):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+class CicyError(RuntimeError):
+    def __init__(self, status: int, where: str, msg: str = ""):
+        super().__init__(f"{where}: {STATUS_NAMES.get(status, status)} {msg}".strip())
+        self.status = status
+
+
+def check(status: int, where: str, ctx=None):
+    if status != CICY_OK:
+        msg = ""
+        try:
+            if ctx is not None:
+                m = lib().cicy_last_error(ctx)
+                msg = m.decode() if m else ""
+            else:
+                m = lib().cicy_host_last_error()
+                msg = m.decode() if m else ""
+        except Exception:  # pragma: no cover - message retrieval is best effort
+            pass
+        raise CicyError(status, where, msg)

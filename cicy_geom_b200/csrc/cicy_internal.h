@@ -1,0 +1,36 @@
+// Internal declarations shared by the host-side sources of libcicy_b200.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/cicy_b200.h"
+
+struct cicy_host_network;
+
+namespace cicy {
+
+// Host-owned CNT network in the layout of cicy_network.
+struct HostNetwork {
+    std::vector<double> x, y, z;
+    std::vector<int32_t> flag;
+    std::vector<double> radii;
+    std::vector<int64_t> structure_ptr, structure_idx;
+    std::vector<int32_t> cnts_inside;
+    std::vector<int64_t> boundary_cnt_ptr;
+    std::vector<int32_t> boundary_cnt_idx;
+    std::vector<int64_t> boundary_pts_ptr, boundary_pts_idx;
+    cicy_cuboid window;
+};
+
+HostNetwork* generate_cnt_network(const cicy_gen_params& g);
+cicy_status extract_window(const HostNetwork& in, const cicy_window_params& w, HostNetwork** out, std::string& err);
+HostNetwork* host_network_from_view(const cicy_network& n);
+void host_network_view(const HostNetwork& h, cicy_network& v);
+
+}  // namespace cicy
+
+struct cicy_host_network {
+    cicy::HostNetwork net;
+};

@@ -1,0 +1,436 @@
+// Host-side network sources upstream of the device hot path:
+//  * a seeded, counter-based synthetic CNT network generator, and
+//  * the single-window extraction (Shells + Cutoff_Wins, CNT_wires branch)
+//    that turns a read/generated network into the window-trimmed network the
+//    hot path consumes.
+// Both are plain CPU code by design: they run once per network, are O(N_p),
+// and sit before the drop-in boundary (App_Network_3D.cpp:85-136).
+#include "cicy_internal.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace cicy {
+
+// ---------------------------------------------------------------------------
+// Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): counter-based RNG.
+struct Philox {
+    uint32_t k0, k1;
+    static inline void mulhilo(uint32_t a, uint32_t b, uint32_t& hi, uint32_t& lo) {
+        uint64_t p = (uint64_t)a * (uint64_t)b;
+        hi = (uint32_t)(p >> 32);
+        lo = (uint32_t)p;
+    }
+    void block(const uint32_t ctr_in[4], uint32_t out[4]) const {
+        uint32_t c0 = ctr_in[0], c1 = ctr_in[1], c2 = ctr_in[2], c3 = ctr_in[3];
+        uint32_t key0 = k0, key1 = k1;
+        for (int r = 0; r < 10; r++) {
+            uint32_t hi0, lo0, hi1, lo1;
+            mulhilo(0xD2511F53u, c0, hi0, lo0);
+            mulhilo(0xCD9E8D57u, c2, hi1, lo1);
+            uint32_t n0 = hi1 ^ c1 ^ key0;
+            uint32_t n1 = lo1;
+            uint32_t n2 = hi0 ^ c3 ^ key1;
+            uint32_t n3 = lo0;
+            c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+            key0 += 0x9E3779B9u;
+            key1 += 0xBB67AE85u;
+        }
+        out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+    }
+    // Two uniform doubles in [0,1) from draw `d` of stream `s`.
+    void uniform2(uint32_t s, uint32_t d, double& u0, double& u1) const {
+        uint32_t c[4] = {s, d, 0x43494359u, 0x42323030u}, o[4];
+        block(c, o);
+        uint64_t a = ((uint64_t)o[0] << 32) | o[1];
+        uint64_t b = ((uint64_t)o[2] << 32) | o[3];
+        u0 = (double)(a >> 11) * (1.0 / 9007199254740992.0);
+        u1 = (double)(b >> 11) * (1.0 / 9007199254740992.0);
+    }
+};
+
+static int cnt_point_count(const Philox& rng, int32_t i, const cicy_gen_params& g) {
+    double u0, u1;
+    rng.uniform2((uint32_t)i, 0, u0, u1);
+    double L = g.len_min + u0 * (g.len_max - g.len_min);
+    return 1 + (int)std::floor(L / g.step);
+}
+
+static void cnt_fill(const Philox& rng, int32_t i, const cicy_gen_params& g, int np, double* x, double* y, double* z) {
+    const double two_pi = 6.283185307179586476925286766559;
+    double u0, u1, u2, u3;
+    rng.uniform2((uint32_t)i, 1, u0, u1);
+    rng.uniform2((uint32_t)i, 2, u2, u3);
+    double px = g.sample.min_x + u0 * g.sample.len_x;
+    double py = g.sample.min_y + u1 * g.sample.len_y;
+    double pz = g.sample.min_z + u2 * g.sample.len_z;
+    double v0, v1;
+    rng.uniform2((uint32_t)i, 3, v0, v1);
+    // isotropic initial direction: cos(theta) ~ U[-1,1], phi ~ U[0,2pi)
+    double ct = 2.0 * v0 - 1.0;
+    double st = std::sqrt(std::max(0.0, 1.0 - ct * ct));
+    double ph = two_pi * v1;
+    double dx = st * std::cos(ph), dy = st * std::sin(ph), dz = ct;
+    (void)u3;
+    x[0] = px; y[0] = py; z[0] = pz;
+    for (int k = 1; k < np; k++) {
+        double w0, w1;
+        rng.uniform2((uint32_t)i, 3u + (uint32_t)k, w0, w1);
+        double th = w0 * g.max_turn_rad;
+        double az = two_pi * w1;
+        // orthonormal frame (e1, e2) perpendicular to d
+        double ax, ay, az_;
+        if (std::fabs(dx) < 0.9) { ax = 1; ay = 0; az_ = 0; } else { ax = 0; ay = 1; az_ = 0; }
+        double e1x = ay * dz - az_ * dy, e1y = az_ * dx - ax * dz, e1z = ax * dy - ay * dx;
+        double n1 = std::sqrt(e1x * e1x + e1y * e1y + e1z * e1z);
+        e1x /= n1; e1y /= n1; e1z /= n1;
+        double e2x = dy * e1z - dz * e1y, e2y = dz * e1x - dx * e1z, e2z = dx * e1y - dy * e1x;
+        double c = std::cos(th), s = std::sin(th), ca = std::cos(az), sa = std::sin(az);
+        double nx = c * dx + s * (ca * e1x + sa * e2x);
+        double ny = c * dy + s * (ca * e1y + sa * e2y);
+        double nz = c * dz + s * (ca * e1z + sa * e2z);
+        double nn = std::sqrt(nx * nx + ny * ny + nz * nz);
+        dx = nx / nn; dy = ny / nn; dz = nz / nn;
+        px = px + g.step * dx;
+        py = py + g.step * dy;
+        pz = pz + g.step * dz;
+        x[k] = px; y[k] = py; z[k] = pz;
+    }
+}
+
+HostNetwork* generate_cnt_network(const cicy_gen_params& g) {
+    HostNetwork* h = new HostNetwork;
+    Philox rng{(uint32_t)(g.seed & 0xffffffffu), (uint32_t)(g.seed >> 32)};
+    int32_t nc = g.n_cnts;
+    h->radii.assign(nc, g.radius);
+    h->structure_ptr.assign(nc + 1, 0);
+    for (int32_t i = 0; i < nc; i++) h->structure_ptr[i + 1] = h->structure_ptr[i] + cnt_point_count(rng, i, g);
+    int64_t np = h->structure_ptr[nc];
+    h->x.resize(np); h->y.resize(np); h->z.resize(np); h->flag.resize(np);
+    h->structure_idx.resize(np);
+    unsigned nt = g.n_threads > 0 ? (unsigned)g.n_threads : std::max(1u, std::thread::hardware_concurrency());
+    nt = std::min<unsigned>(nt, 64);
+    auto work = [&](unsigned t) {
+        for (int32_t i = (int32_t)t; i < nc; i += (int32_t)nt) {
+            int64_t s = h->structure_ptr[i], e = h->structure_ptr[i + 1];
+            cnt_fill(rng, i, g, (int)(e - s), &h->x[s], &h->y[s], &h->z[s]);
+            for (int64_t p = s; p < e; p++) { h->flag[p] = i; h->structure_idx[p] = p; }
+        }
+    };
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nt; t++) th.emplace_back(work, t);
+    work(0);
+    for (auto& t : th) t.join();
+    h->boundary_cnt_ptr.assign(7, 0);
+    h->boundary_pts_ptr.assign(7, 0);
+    h->window = g.sample;
+    return h;
+}
+
+// ---------------------------------------------------------------------------
+// Window extraction (window 0, CNT_wires).  Restates, with the same operation
+// order, Shells::Generate_shells / Find_shell (Shells.cpp:21-149) and
+// Cutoff_Wins::Trim_boundary_cnts (Cutoff_Wins.cpp:82-276),
+// Add_cnt_segment_to_structure (:298-467), Substitute_boundary_point (:468-548),
+// Where_is (:554-566), Where_is_with_boundary (:683-743),
+// Add_cnt_point_to_boundary_vectors (:745-769), Fill_cnts_inside (:803-831).
+namespace {
+
+const double kZero = 1.0e-10;  // MathMatrix.h:18
+
+struct P3 {
+    double x, y, z;
+    int flag;
+};
+
+enum Loc { INSIDE = 0, OUTSIDE = 1, BOUNDARY = 2 };
+
+struct WinCtx {
+    cicy_cuboid win;
+    double mid[3], layer[3], core[3], half[3];
+    int n_shells;
+    std::vector<P3> pts;
+    std::vector<std::vector<int64_t> > structure;
+    std::vector<double> radii;
+    std::vector<std::vector<int> > shells;
+    std::vector<std::vector<int> > bcnt;
+    std::vector<std::vector<int64_t> > bpts;
+    double step_cutoff;
+    int min_points;
+
+    bool at_boundary(const P3& p) const {  // Point_3D::is_at_cuboid_boundary (Geometry_3D.cpp:238-246)
+        return std::fabs(p.x - win.min_x) < kZero || std::fabs(p.x - win.max_x) < kZero ||
+               std::fabs(p.y - win.min_y) < kZero || std::fabs(p.y - win.max_y) < kZero ||
+               std::fabs(p.z - win.min_z) < kZero || std::fabs(p.z - win.max_z) < kZero;
+    }
+    bool outside(const P3& p) const {  // Point_3D::is_outside_cuboid (Geometry_3D.cpp:227-235)
+        return (p.x - win.min_x < kZero) || (p.x - win.max_x > kZero) || (p.y - win.min_y < kZero) ||
+               (p.y - win.max_y > kZero) || (p.z - win.min_z < kZero) || (p.z - win.max_z > kZero);
+    }
+    Loc where_is(const P3& p) const {
+        if (at_boundary(p)) return BOUNDARY;
+        if (outside(p)) return OUTSIDE;
+        return INSIDE;
+    }
+    int find_shell(double x_in, int a) const {  // Shells::Find_shell
+        double x = (x_in > mid[a]) ? 2 * mid[a] - x_in : x_in;
+        if (x < layer[a] || std::fabs(x - layer[a]) < kZero) return 0;
+        if (x > core[a]) return n_shells - 1;
+        return (int)((x - layer[a] + kZero) / half[a]) + 1;
+    }
+    void add_to_shells(const P3& p) {  // Shells::Add_to_cnt_shells + Find_minimum_shell (CNT_wires)
+        int s = std::min(find_shell(p.x, 0), find_shell(p.y, 1));
+        s = std::min(s, find_shell(p.z, 2));
+        if (shells[s].empty() || shells[s].back() != p.flag) shells[s].push_back(p.flag);
+    }
+    void substitute(const P3& pin, P3& pout) const {
+        double Tx = pin.x - pout.x, Ty = pin.y - pout.y, Tz = pin.z - pout.z;
+        auto lam = [](double plane, double xo, double xt) { return (plane - xo) / xt; };
+        double lx = -1.0, ly = -1.0, lz = -1.0;
+        if ((pout.x - win.min_x) < kZero) lx = lam(win.min_x, pout.x, Tx);
+        else if ((win.max_x - pout.x) < kZero) lx = lam(win.max_x, pout.x, Tx);
+        if ((pout.y - win.min_y) < kZero) ly = lam(win.min_y, pout.y, Ty);
+        else if ((win.max_y - pout.y) < kZero) ly = lam(win.max_y, pout.y, Ty);
+        if ((pout.z - win.min_z) < kZero) lz = lam(win.min_z, pout.z, Tz);
+        else if ((win.max_z - pout.z) < kZero) lz = lam(win.max_z, pout.z, Tz);
+        double l = std::max(lx, std::max(ly, lz));
+        double tx = Tx * l, ty = Ty * l, tz = Tz * l;
+        pout.x = pout.x + tx;
+        pout.y = pout.y + ty;
+        pout.z = pout.z + tz;
+        pout.flag = pin.flag;
+    }
+    int boundary_of(const P3& p) const {  // Where_is_with_boundary; -1 when not at a boundary
+        auto bounded = [](double c, double lo, double hi) { return (lo - c <= kZero && c - hi <= kZero); };
+        if (!bounded(p.x, win.min_x, win.max_x)) return -1;
+        if (!bounded(p.y, win.min_y, win.max_y)) return -1;
+        if (!bounded(p.z, win.min_z, win.max_z)) return -1;
+        if (std::fabs(p.x - win.min_x) < kZero) return 4;
+        if (std::fabs(p.x - win.max_x) < kZero) return 2;
+        if (std::fabs(p.y - win.min_y) < kZero) return 5;
+        if (std::fabs(p.y - win.max_y) < kZero) return 3;
+        if (std::fabs(p.z - win.min_z) < kZero) return 1;
+        if (std::fabs(p.z - win.max_z) < kZero) return 0;
+        return -1;
+    }
+    bool add_boundary(int64_t P, int cnt_num) {
+        int b = boundary_of(pts[P]);
+        if (b < 0) return false;
+        if (bcnt[b].empty() || bcnt[b].back() != cnt_num) bcnt[b].push_back(cnt_num);
+        bpts[b].push_back(P);
+        return true;
+    }
+    bool add_segment(int start, int end, int CNT, Loc end_loc, int& segments, int& first_idx, int& last_idx) {
+        int new_start = start, new_end = end;
+        int64_t p_out_start = structure[CNT][new_start];
+        int64_t p_ins_start = structure[CNT][new_start + 1];
+        Loc sl = where_is(pts[p_out_start]);
+        if (sl != INSIDE) {
+            if (sl == OUTSIDE) substitute(pts[p_ins_start], pts[p_out_start]);
+            int cnt_num = segments ? (int)structure.size() : CNT;
+            if (dist(pts[p_out_start], pts[p_out_start + 1]) - step_cutoff < kZero) {
+                pts[p_out_start + 1] = pts[p_out_start];
+                new_start++;
+                p_out_start++;
+            }
+            if (!add_boundary(p_out_start, cnt_num)) return false;
+        }
+        int64_t p_out_end = structure[CNT][new_end];
+        int64_t p_ins_end = structure[CNT][new_end - 1];
+        if (end_loc != INSIDE) {
+            if (end_loc == OUTSIDE) substitute(pts[p_ins_end], pts[p_out_end]);
+            int cnt_num = segments ? (int)structure.size() : CNT;
+            if (dist(pts[p_out_end - 1], pts[p_out_end]) - step_cutoff < kZero) {
+                pts[p_out_end - 1] = pts[p_out_end];
+                new_end--;
+                p_out_end--;
+            }
+            if (!add_boundary(p_out_end, cnt_num)) return false;
+        }
+        if (segments == 0) {
+            first_idx = new_start;
+            last_idx = new_end;
+        } else {
+            int new_cnt = (int)structure.size();
+            std::vector<int64_t> tmp;
+            for (int j = new_start; j <= new_end; j++) {
+                int64_t P = structure[CNT][j];
+                pts[P].flag = new_cnt;
+                tmp.push_back(P);
+                add_to_shells(pts[P]);
+            }
+            radii.push_back(radii[CNT]);
+            structure.push_back(tmp);
+        }
+        segments++;
+        return true;
+    }
+    static double dist(const P3& a, const P3& b) {  // Point_3D::distance_to (Geometry_3D.cpp:64-70)
+        double dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+        return std::sqrt(dx * dx + dy * dy + dz * dz);
+    }
+    bool trim() {
+        bcnt.assign(6, std::vector<int>());
+        bpts.assign(6, std::vector<int64_t>());
+        Loc point_location = INSIDE;
+        for (size_t i = 0; i < shells[0].size(); i++) {
+            int CNT = shells[0][i];
+            int start = 0, end = 0, first_idx = 0, last_idx = 0, segments = 0, last_inside = 0;
+            int cnt_points = (int)structure[CNT].size();
+            if (!cnt_points) continue;
+            int64_t P1 = structure[CNT][0];
+            Loc first_loc = where_is(pts[P1]);
+            for (int j = 1; j < cnt_points; j++) {
+                P1 = structure[CNT][j];
+                point_location = where_is(pts[P1]);
+                if (point_location != OUTSIDE) {
+                    last_inside = j;
+                } else {
+                    end = j;
+                    int n_points = (start == 0 && first_loc != OUTSIDE) ? end - start : end - start - 1;
+                    if (n_points >= min_points)
+                        if (!add_segment(start, end, CNT, point_location, segments, first_idx, last_idx)) return false;
+                    start = j;
+                }
+            }
+            if (last_inside == cnt_points - 1 && (last_inside - start + 1) >= min_points) {
+                end = cnt_points - 1;
+                if (!add_segment(start, end, CNT, point_location, segments, first_idx, last_idx)) return false;
+            }
+            if (segments > 0) {
+                if (first_idx != 0) {
+                    for (int k = first_idx; k <= last_idx; k++) structure[CNT][k - first_idx] = structure[CNT][k];
+                    last_idx = last_idx - first_idx;
+                }
+                for (int k = last_idx + 1; k < cnt_points; k++) structure[CNT].pop_back();
+            } else {
+                structure[CNT].clear();
+            }
+        }
+        return true;
+    }
+};
+
+}  // namespace
+
+cicy_status extract_window(const HostNetwork& in, const cicy_window_params& w, HostNetwork** out, std::string& err) {
+    WinCtx c;
+    // Geom_sample::update_observation_window_geometry(0, ...) (Input_Reader.h:110-135)
+    c.win.len_x = w.win_max[0];
+    c.win.len_y = w.win_max[1];
+    c.win.len_z = w.win_max[2];
+    c.win.min_x = w.sample.min_x + (w.sample.len_x - c.win.len_x) / 2.0;
+    c.win.min_y = w.sample.min_y + (w.sample.len_y - c.win.len_y) / 2.0;
+    c.win.min_z = w.sample.min_z + (w.sample.len_z - c.win.len_z) / 2.0;
+    c.win.max_x = c.win.min_x + c.win.len_x;
+    c.win.max_y = c.win.min_y + c.win.len_y;
+    c.win.max_z = c.win.min_z + c.win.len_z;
+    const double* smin[3] = {&w.sample.min_x, &w.sample.min_y, &w.sample.min_z};
+    const double* slen[3] = {&w.sample.len_x, &w.sample.len_y, &w.sample.len_z};
+    for (int a = 0; a < 3; a++) {
+        c.mid[a] = *smin[a] + *slen[a] / 2.0;
+        c.layer[a] = *smin[a] + (*slen[a] - w.win_max[a]) / 2.0;
+        c.core[a] = *smin[a] + (*slen[a] - w.win_min[a]) / 2.0;
+        c.half[a] = w.win_delt[a] / 2.0;
+    }
+    int num = (int)((w.win_max[0] - w.win_min[0] + kZero) / w.win_delt[0]);
+    if (num != 0) {
+        err = "extract_window: only single-window runs (win_max == win_min, cut_num = 0) are supported";
+        return CICY_E_INPUT;
+    }
+    c.n_shells = num + 2;
+    c.step_cutoff = w.step_length * 0.5;
+    c.min_points = w.min_points;
+    int64_t np = (int64_t)in.x.size();
+    c.pts.resize(np);
+    for (int64_t i = 0; i < np; i++) c.pts[i] = P3{in.x[i], in.y[i], in.z[i], in.flag[i]};
+    int32_t nc = (int32_t)in.radii.size();
+    c.structure.resize(nc);
+    for (int32_t i = 0; i < nc; i++)
+        c.structure[i].assign(in.structure_idx.begin() + in.structure_ptr[i], in.structure_idx.begin() + in.structure_ptr[i + 1]);
+    c.radii = in.radii;
+    c.shells.assign(c.n_shells, std::vector<int>());
+    for (int64_t i = 0; i < np; i++) c.add_to_shells(c.pts[i]);
+    if (!c.trim()) {
+        err = "Error: point should be at boundary but it is not (Cutoff_Wins::Add_cnt_point_to_boundary_vectors)";
+        return CICY_E_INPUT;
+    }
+    HostNetwork* h = new HostNetwork;
+    h->x.resize(np); h->y.resize(np); h->z.resize(np); h->flag.resize(np);
+    for (int64_t i = 0; i < np; i++) { h->x[i] = c.pts[i].x; h->y[i] = c.pts[i].y; h->z[i] = c.pts[i].z; h->flag[i] = c.pts[i].flag; }
+    h->radii = c.radii;
+    h->structure_ptr.assign(1, 0);
+    for (auto& s : c.structure) {
+        for (auto p : s) h->structure_idx.push_back(p);
+        h->structure_ptr.push_back((int64_t)h->structure_idx.size());
+    }
+    // Cutoff_Wins::Fill_cnts_inside
+    for (size_t i = 0; i < c.structure.size(); i++) {
+        if (c.structure[i].size() > 2) h->cnts_inside.push_back((int32_t)i);
+        else if (c.structure[i].size() == 1) {
+            delete h;
+            err = "Error in Extract_observation_window. CNT " + std::to_string(i) + " has only one point.";
+            return CICY_E_INPUT;
+        }
+    }
+    h->boundary_cnt_ptr.assign(1, 0);
+    h->boundary_pts_ptr.assign(1, 0);
+    for (int b = 0; b < 6; b++) {
+        for (auto v : c.bcnt[b]) h->boundary_cnt_idx.push_back(v);
+        h->boundary_cnt_ptr.push_back((int64_t)h->boundary_cnt_idx.size());
+        for (auto v : c.bpts[b]) h->boundary_pts_idx.push_back(v);
+        h->boundary_pts_ptr.push_back((int64_t)h->boundary_pts_idx.size());
+    }
+    h->window = c.win;
+    *out = h;
+    return CICY_OK;
+}
+
+HostNetwork* host_network_from_view(const cicy_network& n) {
+    HostNetwork* h = new HostNetwork;
+    h->x.assign(n.x, n.x + n.n_points);
+    h->y.assign(n.y, n.y + n.n_points);
+    h->z.assign(n.z, n.z + n.n_points);
+    h->flag.assign(n.flag, n.flag + n.n_points);
+    h->radii.assign(n.radii, n.radii + n.n_cnts);
+    h->structure_ptr.assign(n.structure_ptr, n.structure_ptr + n.n_cnts + 1);
+    h->structure_idx.assign(n.structure_idx, n.structure_idx + n.structure_ptr[n.n_cnts]);
+    if (n.n_inside > 0) h->cnts_inside.assign(n.cnts_inside, n.cnts_inside + n.n_inside);
+    if (n.boundary_cnt_ptr) {
+        h->boundary_cnt_ptr.assign(n.boundary_cnt_ptr, n.boundary_cnt_ptr + 7);
+        h->boundary_cnt_idx.assign(n.boundary_cnt_idx, n.boundary_cnt_idx + n.boundary_cnt_ptr[6]);
+    } else {
+        h->boundary_cnt_ptr.assign(7, 0);
+    }
+    if (n.boundary_pts_ptr) {
+        h->boundary_pts_ptr.assign(n.boundary_pts_ptr, n.boundary_pts_ptr + 7);
+        h->boundary_pts_idx.assign(n.boundary_pts_idx, n.boundary_pts_idx + n.boundary_pts_ptr[6]);
+    } else {
+        h->boundary_pts_ptr.assign(7, 0);
+    }
+    h->window = n.window;
+    return h;
+}
+
+void host_network_view(const HostNetwork& h, cicy_network& v) {
+    std::memset(&v, 0, sizeof(v));
+    v.n_points = (int64_t)h.x.size();
+    v.x = h.x.data(); v.y = h.y.data(); v.z = h.z.data(); v.flag = h.flag.data();
+    v.n_cnts = (int32_t)h.radii.size();
+    v.structure_ptr = h.structure_ptr.data();
+    v.structure_idx = h.structure_idx.data();
+    v.radii = h.radii.data();
+    v.n_inside = (int32_t)h.cnts_inside.size();
+    v.cnts_inside = h.cnts_inside.data();
+    v.boundary_cnt_ptr = h.boundary_cnt_ptr.data();
+    v.boundary_cnt_idx = h.boundary_cnt_idx.data();
+    v.boundary_pts_ptr = h.boundary_pts_ptr.data();
+    v.boundary_pts_idx = h.boundary_pts_idx.data();
+    v.window = h.window;
+}
+
+}  // namespace cicy

@@ -1,0 +1,300 @@
+"""Host-side networks and parameters (the inputs of the hot path).
+
+`HostNetwork` owns a network in the layout of the upstream `points_cnt`,
+`structure_cnt`, `radii` and `Cutoff_Wins` outputs; `generate_cnt_network`
+and `HostNetwork.extract_window` call the library's CPU network sources;
+`write_read_network_files` writes the binary files `Read_Network` reads
+(Read_Network.cpp:154-201, :348-467), so the upstream program and this
+library can be run on the very same network.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+from ._abi import check, lib
+
+
+@dataclass
+class NetworkConfig:
+    """A seeded synthetic CNT network and the run settings of the hot path."""
+
+    side: float = 2.0            # cube side (um)
+    n_cnts: int = 400
+    seed: int = 1
+    step: float = 0.01           # polyline step (um)
+    len_min: float = 0.5
+    len_max: float = 1.5
+    radius: float = 0.005        # um
+    max_turn_deg: float = 10.0
+    gs_min: float = 0.05         # background grid cell (um)
+    vdw: float = 0.00034         # van der Waals distance (um)
+    tunnel: float = 0.0018       # tunnelling cutoff (um)
+    min_points: int = 5          # junction compression (Cutoff_dist::min_points)
+    cnt_min_points: int = 5      # shortest CNT segment kept by the window trimming (Nanotube_Geo::min_points)
+    tolerance: float = 1e-10
+    applied_voltage: float = 1.0
+    resistivity_cnt: float = 1e-3
+    resistivity_matrix: float = 1.03e20
+    junction: str = "exponential"
+    junction_resistance: float = 1e7
+    h_planck: float = 6.62606957
+    e_charge: float = 1.60217662
+    e_mass: float = 9.10938291
+    barrier: float = 0.5
+    resistances: tuple = (1, 0, 0)
+    simulation_scope: int = 0
+    gen_threads: int = 0
+
+    def sample(self) -> _abi.Cuboid:
+        s = self.side
+        return _abi.Cuboid(0.0, 0.0, 0.0, s, s, s, s, s, s)
+
+    def c1_c2(self):
+        """Electric_para::C1, C2 exactly as Input_Reader.cpp:1450-1456 forms them."""
+        sq = math.sqrt(2.0 * self.e_mass * self.barrier * self.e_charge)
+        c1 = 10.0 * self.h_planck * self.h_planck / (self.e_mass * self.e_mass * sq)
+        c2 = 4000.0 * 3.1415926535897932384626433832795 * sq / self.h_planck
+        return c1, c2
+
+    def params(self) -> _abi.Params:
+        p = _abi.Params()
+        for a in range(3):
+            p.gs_min[a] = self.gs_min
+        p.gs_overlap_cnt = 2 * self.radius + self.tunnel
+        p.gs_overlap_gnp = 0.0
+        p.van_der_waals_dist = self.vdw
+        p.tunneling_dist = self.tunnel
+        p.min_points = self.min_points
+        p.simulation_scope = self.simulation_scope
+        for a in range(3):
+            p.resistances[a] = int(self.resistances[a])
+        p.junction_type = 1 if self.junction == "exponential" else 0
+        p.tolerance = self.tolerance
+        p.applied_voltage = self.applied_voltage
+        p.resistivity_cnt = self.resistivity_cnt
+        p.resistivity_matrix = self.resistivity_matrix
+        p.junction_resistance = self.junction_resistance
+        p.C1, p.C2 = self.c1_c2()
+        return p
+
+    def window_params(self) -> _abi.WindowParams:
+        w = _abi.WindowParams()
+        w.sample = self.sample()
+        for a in range(3):
+            w.win_max[a] = self.side
+            w.win_min[a] = self.side
+            w.win_delt[a] = 0.25
+        w.step_length = self.step
+        w.min_points = self.cnt_min_points
+        return w
+
+
+class HostNetwork:
+    """A CNT network in host memory owned by libcicy_b200."""
+
+    def __init__(self, handle: int):
+        self._h = C.c_void_p(handle)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().cicy_host_network_free(h)
+            except Exception:
+                pass
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def view(self) -> _abi.Network:
+        v = _abi.Network()
+        check(lib().cicy_host_network_view(self._h, C.byref(v)), "cicy_host_network_view")
+        return v
+
+    def arrays(self) -> dict:
+        """Copies of the network arrays as numpy arrays."""
+        v = self.view()
+        n, c = v.n_points, v.n_cnts
+
+        def arr(p, count, dt):
+            if count == 0 or not p:
+                return np.zeros(0, dtype=dt)
+            return np.ctypeslib.as_array(p, shape=(count,)).astype(dt, copy=True)
+
+        sp = arr(v.structure_ptr, c + 1, np.int64)
+        bcp = arr(v.boundary_cnt_ptr, 7, np.int64)
+        bpp = arr(v.boundary_pts_ptr, 7, np.int64)
+        w = v.window
+        return {
+            "x": arr(v.x, n, np.float64),
+            "y": arr(v.y, n, np.float64),
+            "z": arr(v.z, n, np.float64),
+            "flag": arr(v.flag, n, np.int32),
+            "structure_ptr": sp,
+            "structure_idx": arr(v.structure_idx, int(sp[-1]) if c >= 0 else 0, np.int64),
+            "radii": arr(v.radii, c, np.float64),
+            "cnts_inside": arr(v.cnts_inside, v.n_inside, np.int32),
+            "boundary_cnt_ptr": bcp,
+            "boundary_cnt_idx": arr(v.boundary_cnt_idx, int(bcp[6]), np.int32),
+            "boundary_pts_ptr": bpp,
+            "boundary_pts_idx": arr(v.boundary_pts_idx, int(bpp[6]), np.int64),
+            "window": np.array([w.min_x, w.min_y, w.min_z, w.len_x, w.len_y, w.len_z, w.max_x, w.max_y, w.max_z]),
+        }
+
+    @property
+    def n_points(self) -> int:
+        return int(self.view().n_points)
+
+    @property
+    def n_cnts(self) -> int:
+        return int(self.view().n_cnts)
+
+    def extract_window(self, cfg: NetworkConfig) -> "HostNetwork":
+        """Shells + Cutoff_Wins for window 0 (cicy_extract_window)."""
+        out = C.c_void_p()
+        wp = cfg.window_params()
+        check(lib().cicy_extract_window(self._h, C.byref(wp), C.byref(out)), "cicy_extract_window")
+        return HostNetwork(out.value)
+
+    @staticmethod
+    def from_arrays(a: dict) -> "HostNetwork":
+        keep = {}
+
+        def p(name, ct, dt):
+            x = np.ascontiguousarray(a[name], dtype=dt)
+            keep[name] = x
+            return x.ctypes.data_as(C.POINTER(ct))
+
+        v = _abi.Network()
+        v.n_points = len(a["x"])
+        v.x, v.y, v.z = p("x", C.c_double, np.float64), p("y", C.c_double, np.float64), p("z", C.c_double, np.float64)
+        v.flag = p("flag", C.c_int32, np.int32)
+        v.n_cnts = len(a["radii"])
+        v.structure_ptr = p("structure_ptr", C.c_int64, np.int64)
+        v.structure_idx = p("structure_idx", C.c_int64, np.int64)
+        v.radii = p("radii", C.c_double, np.float64)
+        v.n_inside = len(a.get("cnts_inside", []))
+        if v.n_inside:
+            v.cnts_inside = p("cnts_inside", C.c_int32, np.int32)
+        if "boundary_cnt_ptr" in a:
+            v.boundary_cnt_ptr = p("boundary_cnt_ptr", C.c_int64, np.int64)
+            v.boundary_cnt_idx = p("boundary_cnt_idx", C.c_int32, np.int32)
+            v.boundary_pts_ptr = p("boundary_pts_ptr", C.c_int64, np.int64)
+            v.boundary_pts_idx = p("boundary_pts_idx", C.c_int64, np.int64)
+        w = np.asarray(a["window"], dtype=np.float64)
+        v.window = _abi.Cuboid(*[float(t) for t in w])
+        out = C.c_void_p()
+        check(lib().cicy_host_network_from_arrays(C.byref(v), C.byref(out)), "cicy_host_network_from_arrays")
+        return HostNetwork(out.value)
+
+
+def generate_cnt_network(cfg: NetworkConfig) -> HostNetwork:
+    """Seeded synthetic CNT network (cicy_generate_cnt_network)."""
+    g = _abi.GenParams()
+    g.sample = cfg.sample()
+    g.n_cnts = cfg.n_cnts
+    g.n_threads = cfg.gen_threads
+    g.seed = cfg.seed
+    g.step = cfg.step
+    g.len_min = cfg.len_min
+    g.len_max = cfg.len_max
+    g.radius = cfg.radius
+    g.max_turn_rad = math.radians(cfg.max_turn_deg)
+    out = C.c_void_p()
+    check(lib().cicy_generate_cnt_network(C.byref(g), C.byref(out)), "cicy_generate_cnt_network")
+    return HostNetwork(out.value)
+
+
+def write_read_network_files(directory: str, net: HostNetwork, cfg: NetworkConfig) -> None:
+    """Write input.dat, sample_geom.csv, cnt_struct.dat and cnt_coordinates.dat.
+
+    Binary layout as Read_Network::Read_cnt_data_from_dat reads it
+    (Read_Network.cpp:348-467): cnt_struct.dat = int n_cnts, then per CNT
+    {int n_points; double radius}; cnt_coordinates.dat = x, y, z doubles per
+    point in CNT order.
+    """
+    os.makedirs(directory, exist_ok=True)
+    a = net.arrays()
+    sp = a["structure_ptr"]
+    counts = np.diff(sp).astype(np.int32)
+    rec = np.zeros(len(counts), dtype=np.dtype([("np", "<i4"), ("r", "<f8")], align=False))
+    rec["np"] = counts
+    rec["r"] = a["radii"]
+    with open(os.path.join(directory, "cnt_struct.dat"), "wb") as f:
+        f.write(np.int32(len(counts)).tobytes())
+        f.write(rec.tobytes())
+    idx = a["structure_idx"]
+    xyz = np.stack([a["x"][idx], a["y"][idx], a["z"][idx]], axis=1).astype("<f8")
+    with open(os.path.join(directory, "cnt_coordinates.dat"), "wb") as f:
+        f.write(xyz.tobytes())
+    s = cfg.side
+    with open(os.path.join(directory, "sample_geom.csv"), "w") as f:
+        f.write(f"0,0,0\n{s!r},{s!r},{s!r}\n")
+    with open(os.path.join(directory, "input.dat"), "w") as f:
+        f.write(input_dat(cfg))
+
+
+def input_dat(cfg: NetworkConfig) -> str:
+    """An upstream input.dat for a single-window Read_Network run of `cfg`."""
+    s = repr(float(cfg.side))
+    r = cfg.resistances
+    if cfg.junction == "exponential":
+        junc = f"exponential {cfg.h_planck!r} {cfg.e_charge!r} {cfg.e_mass!r} {cfg.barrier!r}"
+    else:
+        junc = f"constant {cfg.junction_resistance!r}"
+    scope = f"{cfg.simulation_scope} {r[0]} {r[1]} {r[2]}" if cfg.simulation_scope == 0 else f"{cfg.simulation_scope}"
+    return f"""Application
+3D_Electrical_Network
+Simulation_Parameters
+Synthetic
+1
+CNT_wires
+Read_Network
+dat
+vol 0.01
+1
+{scope}
+{cfg.tolerance!r}
+5
+Sample_Geometry
+0 0 0 {s} {s} {s}
+{s} {s} {s}
+0.25 0.25 0.25
+{s} {s} {s}
+{cfg.gs_min!r} {cfg.gs_min!r} {cfg.gs_min!r}
+1.03
+Cutoff_Distances
+{cfg.vdw!r} {cfg.tunnel!r} {cfg.min_points}
+CNT_Geometry
+random
+-1.5707963267948966 1.5707963267948966
+{cfg.step!r}
+uniform {cfg.len_min!r} {cfg.len_max!r}
+points {cfg.cnt_min_points}
+uniform {cfg.radius!r} {cfg.radius!r}
+1.78
+Electrical_Parameters
+{cfg.applied_voltage!r}
+{cfg.resistivity_cnt!r}
+1.0 1e-4
+{cfg.resistivity_matrix!r}
+{junc}
+Visualization_Flags
+0
+0
+0
+0
+0
+Output_Data_Flags
+0
+0
+0
+"""

@@ -1,0 +1,243 @@
+/*
+ * cicy_b200.h — C ABI of the B200 (sm_100a) network-to-conductance hot path of
+ * CICY_geom: tunnelling-contact search, Hoshen-Kopelman cluster labelling,
+ * junction compression, percolation, DEA resistor-network assembly, Jacobi
+ * conjugate-gradient voltage solves, backbone extraction and the effective
+ * resistance, exactly as the upstream classes compute them.
+ *
+ * Plain C: pointers and sizes only, no C++ or CUDA types.  Every function
+ * returns a cicy_status (0 = success).  A failing call leaves a message
+ * readable through cicy_last_error(ctx); that mirrors the upstream convention
+ * of returning 0 and printing "Error in <function> ..." to hout.
+ *
+ * Upstream interfaces each entry point replaces are cited as file:line of the
+ * CICY_geom sources.
+ *
+ * Threading: a context owns one CUDA device, one CUDA stream and the device
+ * buffers of one network.  Calls on one context must not overlap; distinct
+ * contexts are independent.  All compute calls are synchronous from the
+ * host's point of view: they return once their results are complete.
+ *
+ * Index widths: point ids are int64 at the boundary (upstream `long int`),
+ * CNT ids int32 (upstream `int`).  Inside the device path point ids are
+ * 32-bit; networks with 2^31 or more points are rejected with CICY_E_CAPACITY.
+ */
+#ifndef CICY_B200_H
+#define CICY_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    CICY_OK = 0,
+    CICY_E_INPUT = 1,         /* malformed or inconsistent input */
+    CICY_E_CAPACITY = 2,      /* a documented size limit was exceeded */
+    CICY_E_DEVICE = 3,        /* a CUDA runtime error */
+    CICY_E_TIMEOUT = 4,       /* a bounded device-side wait gave up */
+    CICY_E_ZERO_DIAGONAL = 5, /* Direct_Electrifying.cpp:458-484 zero-diagonal check */
+    CICY_E_STATE = 6,         /* stages called out of order */
+    CICY_E_INTERNAL = 7
+} cicy_status;
+
+typedef struct cicy_ctx cicy_ctx;
+typedef struct cicy_host_network cicy_host_network;
+
+/* struct cuboid (Geometry_3D.h:133-152). */
+typedef struct {
+    double min_x, min_y, min_z;
+    double len_x, len_y, len_z;
+    double max_x, max_y, max_z;
+} cicy_cuboid;
+
+/* The fields of Geom_sample, Cutoff_dist, Simu_para and Electric_para
+ * (Input_Reader.h:33-297) that the hot path reads. */
+typedef struct {
+    double gs_min[3];           /* Geom_sample::gs_minx, gs_miny, gs_minz */
+    double gs_overlap_cnt;      /* Geom_sample::gs_overlap_cnt (= 2 r_max + d_tunnel, Input_Reader.cpp:1035) */
+    double gs_overlap_gnp;      /* Geom_sample::gs_overlap_gnp (only enters region sizing) */
+    double van_der_waals_dist;  /* Cutoff_dist::van_der_Waals_dist */
+    double tunneling_dist;      /* Cutoff_dist::tunneling_dist */
+    int32_t min_points;         /* Cutoff_dist::min_points (junction compression) */
+    int32_t simulation_scope;   /* Simu_para::simulation_scope: 0 resistances, 1 backbone only, 2 clusters only */
+    int32_t resistances[3];     /* Simu_para::resistances (x, y, z) */
+    int32_t junction_type;      /* Electric_para::junction_type: 0 "constant", 1 "exponential" */
+    double tolerance;           /* Simu_para::tolerance (CG stop: |r_k| <= tol |r_0|) */
+    double applied_voltage;     /* Electric_para::applied_voltage */
+    double resistivity_cnt;     /* Electric_para::resistivity_CNT */
+    double resistivity_matrix;  /* Electric_para::resistivity_matrix */
+    double junction_resistance; /* Electric_para::junction_resistance ("constant") */
+    double C1, C2;              /* Electric_para::C1, C2 ("exponential", Input_Reader.cpp:1450-1456) */
+} cicy_params;
+
+/* A window-trimmed CNT network: exactly the inputs that
+ * Contact_grid::Generate_contact_grid, Hoshen_Kopelman::Determine_clusters_and_percolation
+ * and Electrical_analysis::Perform_analysis_on_clusters read
+ * (points_cnt, structure_cnt, radii, Cutoff_Wins::cnts_inside, boundary_cnt, boundary_cnt_pts).
+ * Each structure list must be a run of consecutive point ids (upstream assumes
+ * this too: Direct_Electrifying.cpp:620-624 walks P1..P2 by id). */
+typedef struct {
+    int64_t n_points;
+    const double* x;               /* points_cnt[i].x */
+    const double* y;
+    const double* z;
+    const int32_t* flag;           /* points_cnt[i].flag: CNT id of the point */
+    int32_t n_cnts;
+    const int64_t* structure_ptr;  /* n_cnts + 1 offsets into structure_idx */
+    const int64_t* structure_idx;  /* point ids of each CNT, in order */
+    const double* radii;           /* n_cnts */
+    int32_t n_inside;
+    const int32_t* cnts_inside;    /* Cutoff_Wins::cnts_inside */
+    const int64_t* boundary_cnt_ptr;  /* 7 offsets: faces 0..5 (0 z_max, 1 z_min, 2 x_max, 3 y_max, 4 x_min, 5 y_min) */
+    const int32_t* boundary_cnt_idx;  /* Cutoff_Wins::boundary_cnt */
+    const int64_t* boundary_pts_ptr;  /* 7 offsets */
+    const int64_t* boundary_pts_idx;  /* Cutoff_Wins::boundary_cnt_pts */
+    cicy_cuboid window;            /* observation window (Geom_sample::update_observation_window_geometry) */
+} cicy_network;
+
+/* Solver choices for the DEA conjugate gradient (no upstream counterpart:
+ * upstream always runs FP64 Jacobi-PCG, Direct_Electrifying.cpp:1538-1659). */
+typedef enum {
+    CICY_PRECISION_FP64 = 0,  /* FP64 everywhere (upstream arithmetic) */
+    CICY_PRECISION_MIXED = 1  /* FP32 SpMV and preconditioner apply; FP64 dots, residual replacement, refinement */
+} cicy_precision;
+
+typedef enum {
+    CICY_PRECOND_JACOBI = 0,  /* M^-1 = 1/diag (Direct_Electrifying.cpp:1662-1668) */
+    CICY_PRECOND_LEARNED = 1  /* learned scalings, Jacobi fallback when they fail to reduce the residual */
+} cicy_preconditioner;
+
+typedef struct {
+    int32_t precision;        /* cicy_precision */
+    int32_t preconditioner;   /* cicy_preconditioner */
+    int32_t max_iter_factor;  /* max iterations = factor * nodes (upstream 300, Direct_Electrifying.cpp:1559) */
+    int32_t reserved0;
+} cicy_solver_opts;
+
+/* One DEA linear solve (unit-resistor or real-resistor pass) of one cluster. */
+typedef struct {
+    int32_t cluster;          /* percolated cluster index */
+    int32_t pass;             /* -1 unit-resistor pass, 0/1/2 real pass along x/y/z */
+    int64_t nodes;            /* global nodes incl. reserved */
+    int64_t reserved;         /* reserved (prescribed-voltage) nodes */
+    int64_t nnz_lower;        /* strict-lower non-zeros of the free block */
+    int64_t iterations;       /* CG iterations */
+    double rel_residual;      /* FP64 |b - A x| / |b| after the solve */
+    double seconds;           /* device time of the solve (CUDA events) */
+} cicy_solve_info;
+
+typedef struct {
+    double resistances[3];     /* resistances.txt row (Electrical_analysis.cpp:873-932) */
+    double resistivities[3];   /* resistivities.txt row */
+    int64_t n_slots;           /* entries of the sectioned domain */
+    int64_t n_point_contacts;  /* distinct (Pa, CNTb) contacts */
+    int32_t n_labels;          /* clusters before percolation */
+    int32_t n_junctions;       /* compressed CNT-CNT junctions */
+    int32_t n_percolated;      /* percolated clusters */
+    int32_t n_solves;          /* entries used in `solves` */
+    cicy_solve_info solves[32];
+    double stage_seconds[6];   /* grid, clusters, unit DEA, backbone, real DEA, total (device events) */
+} cicy_result;
+
+/* ---------------- context ---------------- */
+cicy_status cicy_ctx_create(cicy_ctx** out, int device);
+cicy_status cicy_ctx_destroy(cicy_ctx* ctx);
+/* Use an external cudaStream_t (passed as void*) instead of the context's own. */
+cicy_status cicy_ctx_set_stream(cicy_ctx* ctx, void* cuda_stream);
+void* cicy_ctx_stream(cicy_ctx* ctx);
+cicy_status cicy_ctx_set_solver(cicy_ctx* ctx, const cicy_solver_opts* opts);
+const char* cicy_last_error(const cicy_ctx* ctx);
+/* Number of kernels this context has launched so far. */
+int64_t cicy_ctx_kernel_launches(const cicy_ctx* ctx);
+
+/* ---------------- inputs ---------------- */
+/* Copy a window-trimmed network from host memory into the context's device buffers. */
+cicy_status cicy_upload_network(cicy_ctx* ctx, const cicy_network* net);
+
+/* ---------------- hot path stages ---------------- */
+/* Contact_grid::Generate_contact_grid (Contact_grid.cpp:18-80, CNT branch :104-295). */
+cicy_status cicy_contact_grid(cicy_ctx* ctx, const cicy_params* p);
+/* Hoshen_Kopelman::Determine_clusters_and_percolation, CNT-only path
+ * (Hoshen_Kopelman.cpp:17-201, :203-572, :2331-2738). */
+cicy_status cicy_clusters(cicy_ctx* ctx, const cicy_params* p);
+/* Electrical_analysis::Perform_analysis_on_clusters (Electrical_analysis.cpp:10-145) with
+ * Direct_Electrifying::Compute_voltage_field (Direct_Electrifying.cpp:11-113) and
+ * Backbone_Network::Determine_backbone_network (Backbone_Network.cpp:11-62). */
+cicy_status cicy_electrical_analysis(cicy_ctx* ctx, const cicy_params* p, cicy_result* out);
+/* All three stages (App_Network_3D.cpp:140-179 for one window). */
+cicy_status cicy_network_to_conductance(cicy_ctx* ctx, const cicy_params* p, cicy_result* out);
+
+/* ---------------- copy-out (size query: pass NULL buffers, read the counts) ----------------
+ * These fill the public members the upstream classes expose to later stages. */
+/* Contact_grid::sectioned_domain_cnts as CSR (n_regions + 1 offsets). */
+cicy_status cicy_get_sectioned_domain(cicy_ctx* ctx, int64_t* n_regions, int64_t* n_slots, int64_t* ptr, int64_t* idx);
+/* The point_contacts / point_contacts_dist maps of Hoshen_Kopelman::Label_cnts_in_window
+ * (Hoshen_Kopelman.cpp:249-372), sorted by (Pa, CNTb). */
+cicy_status cicy_get_point_contacts(cicy_ctx* ctx, int64_t* n, int64_t* pa, int32_t* cnt_b, int64_t* pb, double* dist);
+/* labels_cnt after Cleanup_labels (Hoshen_Kopelman.cpp:374-425); n = number of CNTs. */
+cicy_status cicy_get_labels(cicy_ctx* ctx, int32_t* n_cnts, int32_t* n_labels, int32_t* labels);
+/* Hoshen_Kopelman::junctions_cnt (Hoshen_Kopelman.cpp:443-554). */
+cicy_status cicy_get_junctions(cicy_ctx* ctx, int64_t* n, int64_t* p1, int32_t* n1, int64_t* p2, int32_t* n2, double* dist);
+/* Hoshen_Kopelman::elements_cnt as CSR over all CNTs; which = 0 after labelling,
+ * which = 1 the backbone-trimmed elements (Backbone_Network.cpp:412-556). */
+cicy_status cicy_get_elements(cicy_ctx* ctx, int32_t which, int64_t* n_cnts, int64_t* n_idx, int64_t* ptr, int64_t* idx);
+/* clusters_cnt (percolated clusters, CSR), family, cluster_cnt_junctions (CSR);
+ * which = 0 after percolation, 1 after backbone extraction. */
+cicy_status cicy_get_clusters(cicy_ctx* ctx, int32_t which, int32_t* n_clusters, int64_t* n_idx, int64_t* ptr, int32_t* idx,
+                              int32_t* family, int64_t* n_junc_idx, int64_t* junc_ptr, int32_t* junc_idx);
+/* One DEA system and its solution, as upstream builds it in SSS form
+ * (strict-lower CSR of the free block, diagonal, right-hand side after the BC
+ * elimination, initial guess, prescribed voltages, voltages of all nodes).
+ * solve = index into cicy_result::solves. */
+cicy_status cicy_get_system(cicy_ctx* ctx, int32_t solve, int64_t* nodes, int64_t* reserved, int64_t* nnz_lower,
+                            int64_t* row_ptr, int64_t* col_ind, double* values, double* diag, double* b, double* x0,
+                            double* voltages);
+
+/* ---------------- host-side network sources (CPU, upstream of the hot path) ---------------- */
+/* Seeded synthetic CNT network (no upstream counterpart; emits the same layout
+ * Read_Network::Read_cnt_data_from_dat builds, Read_Network.cpp:348-467):
+ * start U(sample), isotropic initial direction, polyline of `step` steps with
+ * polar turn U[0, max_turn] at uniform azimuth, length U[len_min, len_max],
+ * 1 + floor(L/step) points. Counter-based (Philox-4x32-10) so each CNT is
+ * reproducible by index. */
+typedef struct {
+    cicy_cuboid sample;
+    int32_t n_cnts;
+    int32_t n_threads;   /* host threads (0: all) */
+    uint64_t seed;
+    double step;
+    double len_min, len_max;
+    double radius;
+    double max_turn_rad;
+} cicy_gen_params;
+cicy_status cicy_generate_cnt_network(const cicy_gen_params* g, cicy_host_network** out);
+
+/* Window extraction for window 0 of a single-window run: Shells::Generate_shells
+ * (Shells.cpp:21-69) + Cutoff_Wins::Trim_boundary_cnts / Add_cnt_segment_to_structure /
+ * Substitute_boundary_point / Add_cnt_point_to_boundary_vectors / Fill_cnts_inside
+ * (Cutoff_Wins.cpp:82-831), CNT_wires branch. */
+typedef struct {
+    cicy_cuboid sample;     /* Geom_sample::sample */
+    double win_max[3];      /* Geom_sample::win_max_x/y/z */
+    double win_min[3];      /* Geom_sample::win_min_x/y/z */
+    double win_delt[3];     /* Geom_sample::win_delt_x/y/z */
+    double step_length;     /* Nanotube_Geo::step_length */
+    int32_t min_points;     /* Nanotube_Geo::min_points */
+    int32_t reserved0;
+} cicy_window_params;
+cicy_status cicy_extract_window(const cicy_host_network* in, const cicy_window_params* w, cicy_host_network** out);
+
+/* Wrap caller-owned arrays (copied) as a host network, e.g. a network read from files. */
+cicy_status cicy_host_network_from_arrays(const cicy_network* net, cicy_host_network** out);
+/* Borrowed view of a host network; valid until cicy_host_network_free. */
+cicy_status cicy_host_network_view(const cicy_host_network* h, cicy_network* view);
+void cicy_host_network_free(cicy_host_network* h);
+/* Message of the last failing host-side call on this thread. */
+const char* cicy_host_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CICY_B200_H */
