@@ -1,0 +1,343 @@
+// C ABI entry points of the device hot path (cicy_b200.h): context, stages, copy-out.
+#include <algorithm>
+#include <cstring>
+#include <new>
+
+#include "ctx.cuh"
+
+struct cicy_ctx {
+    cicy::Ctx c;
+};
+
+namespace {
+
+template <class F>
+cicy_status guarded(cicy_ctx* ctx, F&& f) {
+    if (!ctx) return CICY_E_INPUT;
+    try {
+        CICY_CUDA(cudaSetDevice(ctx->c.device));
+        f(ctx->c);
+        ctx->c.err.clear();
+        return CICY_OK;
+    } catch (const cicy::Fail& e) {
+        ctx->c.err = e.msg;
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        ctx->c.err = "host allocation failed";
+        return CICY_E_INTERNAL;
+    }
+}
+
+template <class T>
+void d2h(cicy::Ctx& c, T* h, const T* d, size_t n) {
+    if (n && h) CICY_CUDA(cudaMemcpyAsync(h, d, sizeof(T) * n, cudaMemcpyDeviceToHost, c.stream));
+}
+
+void sync(cicy::Ctx& c) { CICY_CUDA(cudaStreamSynchronize(c.stream)); }
+
+}  // namespace
+
+extern "C" {
+
+cicy_status cicy_ctx_create(cicy_ctx** out, int device) {
+    if (!out) return CICY_E_INPUT;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return CICY_E_DEVICE;
+    if (device < 0 || device >= ndev) return CICY_E_INPUT;
+    cicy_ctx* ctx = new (std::nothrow) cicy_ctx;
+    if (!ctx) return CICY_E_INTERNAL;
+    ctx->c.device = device;
+    cicy_status s = guarded(ctx, [](cicy::Ctx& c) {
+        CICY_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+        c.own_stream = true;
+        cudaDeviceProp prop;
+        CICY_CUDA(cudaGetDeviceProperties(&prop, c.device));
+        c.num_sms = prop.multiProcessorCount;
+        if (!prop.cooperativeLaunch) throw cicy::Fail{CICY_E_DEVICE, "device lacks cooperative launch"};
+        c.status.ensure(1);
+        CICY_CUDA(cudaMemsetAsync(c.status.get(), 0, sizeof(int), c.stream));
+        c.i32_scalar.ensure(8);
+        c.i64_scalar.ensure(8);
+    });
+    if (s != CICY_OK) {
+        delete ctx;
+        return s;
+    }
+    *out = ctx;
+    return CICY_OK;
+}
+
+cicy_status cicy_ctx_destroy(cicy_ctx* ctx) {
+    if (!ctx) return CICY_OK;
+    cudaSetDevice(ctx->c.device);
+    if (ctx->c.stream) cudaStreamSynchronize(ctx->c.stream);
+    if (ctx->c.own_stream && ctx->c.stream) cudaStreamDestroy(ctx->c.stream);
+    delete ctx;  // DBuf members hold raw device pointers; the process-wide context frees them at exit
+    return CICY_OK;
+}
+
+cicy_status cicy_ctx_set_stream(cicy_ctx* ctx, void* stream) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (c.stream) CICY_CUDA(cudaStreamSynchronize(c.stream));
+        if (c.own_stream && c.stream) CICY_CUDA(cudaStreamDestroy(c.stream));
+        c.stream = (cudaStream_t)stream;
+        c.own_stream = false;
+    });
+}
+
+void* cicy_ctx_stream(cicy_ctx* ctx) { return ctx ? (void*)ctx->c.stream : nullptr; }
+
+cicy_status cicy_ctx_set_solver(cicy_ctx* ctx, const cicy_solver_opts* o) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (!o || o->precision < 0 || o->precision > 1 || o->preconditioner < 0 || o->preconditioner > 1 || o->max_iter_factor <= 0)
+            throw cicy::Fail{CICY_E_INPUT, "cicy_ctx_set_solver: invalid options"};
+        c.solver = *o;
+    });
+}
+
+const char* cicy_last_error(const cicy_ctx* ctx) { return ctx ? ctx->c.err.c_str() : "null context"; }
+
+int64_t cicy_ctx_kernel_launches(const cicy_ctx* ctx) { return ctx ? ctx->c.launches : 0; }
+
+cicy_status cicy_upload_network(cicy_ctx* ctx, const cicy_network* net) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (!net) throw cicy::Fail{CICY_E_INPUT, "null network"};
+        cicy::upload_network(c, *net);
+    });
+}
+
+cicy_status cicy_contact_grid(cicy_ctx* ctx, const cicy_params* p) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (!p) throw cicy::Fail{CICY_E_INPUT, "null params"};
+        cicy::run_contact_grid(c, *p);
+    });
+}
+
+cicy_status cicy_clusters(cicy_ctx* ctx, const cicy_params* p) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (!p) throw cicy::Fail{CICY_E_INPUT, "null params"};
+        cicy::run_clusters(c, *p);
+    });
+}
+
+cicy_status cicy_electrical_analysis(cicy_ctx* ctx, const cicy_params* p, cicy_result* out) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (!p) throw cicy::Fail{CICY_E_INPUT, "null params"};
+        if (out) std::memset(out, 0, sizeof(*out));
+        cicy::run_electrical(c, *p, out);
+        if (out) {
+            out->n_slots = c.n_slots;
+            out->n_point_contacts = c.n_uc;
+            out->n_labels = c.n_labels;
+            out->n_junctions = c.n_junc;
+        }
+    });
+}
+
+cicy_status cicy_network_to_conductance(cicy_ctx* ctx, const cicy_params* p, cicy_result* out) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (!p) throw cicy::Fail{CICY_E_INPUT, "null params"};
+        cudaEvent_t ev[4];
+        for (auto& e : ev) CICY_CUDA(cudaEventCreate(&e));
+        CICY_CUDA(cudaEventRecord(ev[0], c.stream));
+        cicy::run_contact_grid(c, *p);
+        CICY_CUDA(cudaEventRecord(ev[1], c.stream));
+        cicy::run_clusters(c, *p);
+        CICY_CUDA(cudaEventRecord(ev[2], c.stream));
+        if (out) std::memset(out, 0, sizeof(*out));
+        cicy::run_electrical(c, *p, out);
+        CICY_CUDA(cudaEventRecord(ev[3], c.stream));
+        CICY_CUDA(cudaEventSynchronize(ev[3]));
+        float ms[3];
+        cudaEventElapsedTime(&ms[0], ev[0], ev[1]);
+        cudaEventElapsedTime(&ms[1], ev[1], ev[2]);
+        cudaEventElapsedTime(&ms[2], ev[0], ev[3]);
+        for (auto& e : ev) cudaEventDestroy(e);
+        if (out) {
+            out->n_slots = c.n_slots;
+            out->n_point_contacts = c.n_uc;
+            out->n_labels = c.n_labels;
+            out->n_junctions = c.n_junc;
+            out->stage_seconds[0] = ms[0] * 1e-3;
+            out->stage_seconds[1] = ms[1] * 1e-3;
+            out->stage_seconds[5] = ms[2] * 1e-3;
+        }
+    });
+}
+
+cicy_status cicy_get_sectioned_domain(cicy_ctx* ctx, int64_t* n_regions, int64_t* n_slots, int64_t* ptr, int64_t* idx) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (c.stage < 2) throw cicy::Fail{CICY_E_STATE, "no contact grid"};
+        const int R = (int)c.grid.total, S = c.n_slots;
+        if (n_regions) *n_regions = R;
+        if (n_slots) *n_slots = S;
+        if (ptr) {
+            std::vector<int32_t> h(R + 1);
+            d2h(c, h.data(), c.region_ptr.get(), R + 1);
+            sync(c);
+            for (int i = 0; i <= R; i++) ptr[i] = h[i];
+        }
+        if (idx && S > 0) {
+            std::vector<uint32_t> q(S);
+            std::vector<int32_t> tp(c.n_trav);
+            d2h(c, q.data(), c.slot_sorted.get(), S);
+            d2h(c, tp.data(), c.trav_pt.get(), c.n_trav);
+            sync(c);
+            for (int i = 0; i < S; i++) idx[i] = tp[q[i]];
+        }
+    });
+}
+
+cicy_status cicy_get_point_contacts(cicy_ctx* ctx, int64_t* n, int64_t* pa, int32_t* cnt_b, int64_t* pb, double* dist) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (c.stage < 3) throw cicy::Fail{CICY_E_STATE, "no clusters"};
+        const int N = c.n_uc;
+        if (n) *n = N;
+        if (!pa && !cnt_b && !pb && !dist) return;
+        std::vector<int32_t> a(N), b(N), qa(N), qb(N);
+        std::vector<double> d(N);
+        d2h(c, b.data(), c.uc_b.get(), N);
+        d2h(c, qa.data(), c.uc_pa.get(), N);
+        d2h(c, qb.data(), c.uc_pb.get(), N);
+        d2h(c, d.data(), c.uc_d.get(), N);
+        sync(c);
+        std::vector<int> order(N);
+        for (int i = 0; i < N; i++) order[i] = i;
+        std::sort(order.begin(), order.end(), [&](int u, int v) { return qa[u] != qa[v] ? qa[u] < qa[v] : b[u] < b[v]; });
+        for (int i = 0; i < N; i++) {
+            int o = order[i];
+            if (pa) pa[i] = qa[o];
+            if (cnt_b) cnt_b[i] = b[o];
+            if (pb) pb[i] = qb[o];
+            if (dist) dist[i] = d[o];
+        }
+    });
+}
+
+cicy_status cicy_get_labels(cicy_ctx* ctx, int32_t* n_cnts, int32_t* n_labels, int32_t* labels) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (c.stage < 3) throw cicy::Fail{CICY_E_STATE, "no clusters"};
+        if (n_cnts) *n_cnts = c.n_cnts;
+        if (n_labels) *n_labels = c.n_labels;
+        d2h(c, labels, c.labels.get(), c.n_cnts);
+        sync(c);
+    });
+}
+
+cicy_status cicy_get_junctions(cicy_ctx* ctx, int64_t* n, int64_t* p1, int32_t* n1, int64_t* p2, int32_t* n2, double* dist) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (c.stage < 3) throw cicy::Fail{CICY_E_STATE, "no clusters"};
+        const int N = c.n_junc;
+        if (n) *n = N;
+        std::vector<int32_t> a(N), b(N);
+        if (p1) { d2h(c, a.data(), c.j_p1.get(), N); sync(c); for (int i = 0; i < N; i++) p1[i] = a[i]; }
+        if (p2) { d2h(c, b.data(), c.j_p2.get(), N); sync(c); for (int i = 0; i < N; i++) p2[i] = b[i]; }
+        d2h(c, n1, c.j_n1.get(), N);
+        d2h(c, n2, c.j_n2.get(), N);
+        d2h(c, dist, c.j_d.get(), N);
+        sync(c);
+    });
+}
+
+cicy_status cicy_get_elements(cicy_ctx* ctx, int32_t which, int64_t* n_cnts, int64_t* n_idx, int64_t* ptr, int64_t* idx) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (c.stage < 3) throw cicy::Fail{CICY_E_STATE, "no clusters"};
+        if (which == 1 && !c.have_backbone) throw cicy::Fail{CICY_E_STATE, "no backbone yet"};
+        const int NC = c.n_cnts;
+        std::vector<int32_t> lo(NC), hi(NC);
+        int n_elem = 0;
+        std::vector<int32_t> mscan(c.n_points + 1);
+        d2h(c, mscan.data(), c.mark_scan.get(), c.n_points + 1);
+        sync(c);
+        n_elem = mscan[c.n_points];
+        if (which == 1) {
+            d2h(c, lo.data(), c.bb_lo.get(), NC);
+            d2h(c, hi.data(), c.bb_hi.get(), NC);
+            sync(c);
+        } else {
+            for (int i = 0; i < NC; i++) {
+                int b = c.h_clen[i] ? mscan[c.h_cstart[i]] : 0, e = c.h_clen[i] ? mscan[c.h_cstart[i] + c.h_clen[i]] : 0;
+                lo[i] = e > b ? b : -1;
+                hi[i] = e > b ? e - 1 : -2;
+            }
+        }
+        std::vector<int32_t> el(std::max(n_elem, 1));
+        d2h(c, el.data(), c.elem_idx.get(), n_elem);
+        sync(c);
+        int64_t total = 0;
+        if (ptr) ptr[0] = 0;
+        for (int i = 0; i < NC; i++) {
+            int64_t len = lo[i] >= 0 ? (hi[i] - lo[i] + 1) : 0;
+            if (idx)
+                for (int64_t k = 0; k < len; k++) idx[total + k] = el[lo[i] + k];
+            total += len;
+            if (ptr) ptr[i + 1] = total;
+        }
+        if (n_cnts) *n_cnts = NC;
+        if (n_idx) *n_idx = total;
+    });
+}
+
+cicy_status cicy_get_clusters(cicy_ctx* ctx, int32_t which, int32_t* n_clusters, int64_t* n_idx, int64_t* ptr, int32_t* idx,
+                              int32_t* family, int64_t* n_junc_idx, int64_t* junc_ptr, int32_t* junc_idx) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (c.stage < 3) throw cicy::Fail{CICY_E_STATE, "no clusters"};
+        if (which == 1 && !c.have_backbone) throw cicy::Fail{CICY_E_STATE, "no backbone yet"};
+        const int K = c.n_perc;
+        if (n_clusters) *n_clusters = K;
+        if (family)
+            for (int k = 0; k < K; k++) family[k] = c.h_family[k];
+        const std::vector<int32_t>& cp = c.h_clu_ptr;  // storage offsets are those of the percolation stage
+        const std::vector<int32_t>& jp = c.h_cj_ptr;
+        int64_t tot = 0, jtot = 0;
+        if (ptr) ptr[0] = 0;
+        if (junc_ptr) junc_ptr[0] = 0;
+        for (int k = 0; k < K; k++) {
+            int len = which == 1 ? c.bb_clu_len[k] : cp[k + 1] - cp[k];
+            int jlen = which == 1 ? c.bb_cj_len[k] : jp[k + 1] - jp[k];
+            const int32_t* src = which == 1 ? c.bbclu_idx.get() : c.clu_idx.get();
+            const int32_t* jsrc = which == 1 ? c.bbcj_idx.get() : c.cj_idx.get();
+            if (idx && len) d2h(c, idx + tot, src + cp[k], len);
+            if (junc_idx && jlen) d2h(c, junc_idx + jtot, jsrc + jp[k], jlen);
+            tot += len;
+            jtot += jlen;
+            if (ptr) ptr[k + 1] = tot;
+            if (junc_ptr) junc_ptr[k + 1] = jtot;
+        }
+        sync(c);
+        if (n_idx) *n_idx = tot;
+        if (n_junc_idx) *n_junc_idx = jtot;
+    });
+}
+
+cicy_status cicy_get_system(cicy_ctx* ctx, int32_t solve, int64_t* nodes, int64_t* reserved, int64_t* nnz_lower, int64_t* row_ptr,
+                            int64_t* col_ind, double* values, double* diag, double* b, double* x0, double* voltages) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (solve < 0 || solve >= (int)c.systems.size()) throw cicy::Fail{CICY_E_INPUT, "no such solve"};
+        cicy::DeaSystem& s = *c.systems[solve];
+        const int n = (int)(s.nodes - s.reserved), m = (int)s.nnz_lower;
+        if (nodes) *nodes = s.nodes;
+        if (reserved) *reserved = s.reserved;
+        if (nnz_lower) *nnz_lower = m;
+        std::vector<int32_t> rp(n + 1), ci(std::max(m, 1));
+        if (row_ptr) {
+            d2h(c, rp.data(), s.row_ptr.get(), n + 1);
+            sync(c);
+            for (int i = 0; i <= n; i++) row_ptr[i] = rp[i];
+        }
+        if (col_ind) {
+            d2h(c, ci.data(), s.col.get(), m);
+            sync(c);
+            for (int i = 0; i < m; i++) col_ind[i] = ci[i];
+        }
+        d2h(c, values, s.val.get(), m);
+        d2h(c, diag, s.diag.get(), n);
+        d2h(c, b, s.b.get(), n);
+        d2h(c, x0, s.x0.get(), n);
+        d2h(c, voltages, s.volt.get(), s.nodes);
+        sync(c);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,124 @@
+// The device context behind `cicy_ctx`: one network's device buffers, the
+// stream, and the host-side bookkeeping of the stage sequence.
+#pragma once
+
+#include <vector>
+
+#include "dev_common.cuh"
+
+namespace cicy {
+
+// Region grid of Contact_grid::Generate_contact_grid / Adjust_regions_if_needed.
+struct GridGeom {
+    int n[3];
+    double l[3];
+    double min[3];
+    double overlap;  // Geom_sample::gs_overlap_cnt
+    long long total;
+};
+
+// One assembled DEA system kept for copy-out and for the backbone/current steps.
+struct DeaSystem {
+    int cluster = -1, pass = -2;  // pass -1: unit resistors; 0,1,2: real, along x,y,z
+    int64_t nodes = 0, reserved = 0, nnz_lower = 0, iterations = 0;
+    double rel_residual = 0, seconds = 0;
+    // device: strict-lower CSR of the free block (SSS), diagonal, rhs, x0, voltages (all nodes)
+    DBuf<int32_t> row_ptr, col;
+    DBuf<double> val, diag, b, x0, volt;
+};
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string err;
+    int64_t launches = 0;
+    int stage = 0;  // 1 uploaded, 2 grid, 3 clusters, 4 electrical
+    cicy_solver_opts solver{CICY_PRECISION_FP64, CICY_PRECOND_JACOBI, 300, 0};
+    int num_sms = 148;
+
+    // ---- network (device) ----
+    int n_points = 0, n_cnts = 0, n_inside = 0, n_trav = 0;
+    cicy_cuboid window{};
+    DBuf<double> x, y, z, radii;
+    DBuf<int32_t> flag, cstart, clen, inside, trav_off, trav_pt;
+    std::vector<int32_t> h_bcnt_ptr, h_bcnt_idx, h_bpts_ptr;  // host copies of the face lists (sizes)
+    DBuf<int32_t> bcnt_idx, bpts_idx, bcnt_ptr, bpts_ptr;
+    std::vector<int32_t> h_cstart, h_clen;
+
+    // ---- grid ----
+    GridGeom grid{};
+    int n_slots = 0;
+    DBuf<int32_t> region_cnt, region_ptr, region_cur, slot_region, seg_large;
+    DBuf<uint32_t> slot_q, slot_sorted;
+    DBuf<int> status;      // device status word (DevErr)
+    DBuf<int32_t> i32_scalar;  // small device scalars for totals
+    DBuf<int64_t> i64_scalar;
+
+    // ---- contacts / labels ----
+    int n_raw = 0, n_uc = 0, n_labels = 0, n_junc = 0, n_perc = 0;
+    DBuf<int32_t> raw_a, raw_b, raw_pa, raw_pb;
+    DBuf<double> raw_d;
+    DBuf<uint64_t> raw_key;
+    DBuf<int32_t> raw_count;
+    DBuf<uint64_t> sort_k;
+    DBuf<uint32_t> sort_v;
+    DBuf<int32_t> flags, flags_scan;
+    DBuf<int32_t> uc_a, uc_b, uc_pa, uc_pb;
+    DBuf<double> uc_d;
+    DBuf<int32_t> parent, uf_root, labels, root_rank;
+    DBuf<unsigned long long> minkey;
+    DBuf<int32_t> grp_start, junc_cnt, junc_ofs;
+    DBuf<int32_t> j_p1, j_n1, j_p2, j_n2;
+    DBuf<double> j_d;
+    DBuf<int32_t> mark, mark_scan, elem_idx, has_junc;
+    DBuf<int32_t> face_bits, perc_bits, perc_index;
+    std::vector<int32_t> h_family;  // family of each percolated cluster
+    DBuf<int32_t> clu_ptr, clu_idx, cj_ptr, cj_idx;          // percolated clusters (after percolation)
+    std::vector<int32_t> h_clu_ptr, h_cj_ptr;
+    // backbone state: kept element range per CNT, alive flags, trimmed cluster lists
+    DBuf<int32_t> bb_lo, bb_hi;                              // element-list index range kept per CNT (-1 dead)
+    DBuf<int32_t> bbclu_ptr, bbclu_idx, bbcj_ptr, bbcj_idx;  // clusters/junctions after backbone
+    std::vector<int32_t> h_bbclu_ptr, h_bbcj_ptr;
+    bool have_backbone = false;
+
+    // ---- DEA ----
+    std::vector<DeaSystem*> systems;
+    DBuf<int32_t> lmm;         // node of each point in the current solve (-1 none)
+    DBuf<int32_t> cnt_nodes, cnt_node_base;
+    DBuf<int32_t> e_n1, e_n2, e_op;
+    DBuf<double> e_g;
+    DBuf<int32_t> work_i32a, work_i32b, work_i32c;
+    DBuf<double> work_f64a;
+    RadixScratch rs;
+    DBuf<int32_t> scan_tmp32;
+    DBuf<int64_t> scan_tmp64;
+    // CG scratch
+    DBuf<int32_t> cg_rp, cg_ci;
+    DBuf<double> cg_val, cg_minv, cg_x, cg_r, cg_p, cg_q, cg_z, cg_w, cg_s, cg_part;
+    DBuf<float> cg_val32, cg_minv32, cg_z32;
+    DBuf<unsigned int> barrier;
+    DBuf<double> cg_scal;
+    DBuf<long long> cg_iters;
+    // assembly / backbone scratch
+    DBuf<uint64_t> dkey, stage_keys;
+    DBuf<uint32_t> dval;
+    DBuf<double> runval, vef, cur_out;
+    DBuf<int32_t> eb, ee, alive, alive_scan, tmp_list;
+    DBuf<unsigned long long> imax;
+    std::vector<int32_t> bb_clu_len, bb_cj_len;
+
+    ~Ctx();
+};
+
+// Stage entry points (throw Fail on error).
+void upload_network(Ctx& c, const cicy_network& net);
+void run_contact_grid(Ctx& c, const cicy_params& p);
+void run_clusters(Ctx& c, const cicy_params& p);
+void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out);
+
+// Helpers shared across translation units.
+int32_t read_i32(Ctx& c, const int32_t* dptr);
+void check_status(Ctx& c, const char* where);
+
+}  // namespace cicy

@@ -1,0 +1,999 @@
+// Direct Electrifying Algorithm on the device: node numbering, resistor
+// assembly by sort-and-reduce, boundary-condition elimination, the Jacobi-PCG
+// voltage solve, backbone extraction and boundary currents
+// (Direct_Electrifying.cpp, Backbone_Network.cpp, Electrical_analysis.cpp).
+#include <algorithm>
+#include <cmath>
+#include <cooperative_groups.h>
+
+#include "ctx.cuh"
+
+namespace cicy {
+
+namespace {
+
+constexpr double kZero = 1.0e-10;                         // MathMatrix.h:18
+constexpr double kPI = 3.1415926535897932384626433832795;  // Input_Reader.h:23
+enum EdgeOp : int { OP_SKIP = 0, OP_OVERWRITE = 1, OP_ADD = 2 };
+
+int grid_for(long long n, int threads = 256) {
+    long long b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > 148LL * 32) b = 148LL * 32;
+    return (int)b;
+}
+
+// Get_vector_of_boundaries (Direct_Electrifying.cpp:249-305)
+int boundaries_of_family(int family, int out[6]) {
+    static const int tab[7][6] = {{2, 4}, {3, 5}, {0, 1}, {2, 4, 3, 5}, {2, 4, 0, 1}, {3, 5, 0, 1}, {2, 4, 3, 5, 0, 1}};
+    static const int len[7] = {2, 2, 2, 4, 4, 4, 6};
+    if (family < 0 || family > 6) return -1;
+    for (int i = 0; i < len[family]; i++) out[i] = tab[family][i];
+    return len[family];
+}
+
+// Per-CNT element ranges of the cluster being solved: [eb, ee) into elem_idx.
+__global__ void k_cluster_ranges(int n, const int32_t* __restrict__ members, const int32_t* __restrict__ cur_lo,
+                                 const int32_t* __restrict__ cur_hi, int32_t* __restrict__ eb, int32_t* __restrict__ ee,
+                                 int* status) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int c = members[i];
+        int lo = cur_lo[c], hi = cur_hi[c];
+        eb[i] = lo;
+        ee[i] = hi + 1;
+        // LM_matrix_for_cnts: "There is a CNT with not enough points to form an element"
+        if (lo < 0 || hi - lo + 1 <= 1) atomicCAS(status, 0, (int)DEV_INPUT);
+    }
+}
+
+__global__ void k_lmm_face(int b, int e, const int32_t* __restrict__ bpts, int node, int32_t* lmm) {
+    for (int i = b + blockIdx.x * blockDim.x + threadIdx.x; i < e; i += gridDim.x * blockDim.x) lmm[bpts[i]] = node;
+}
+
+// LM_matrix_for_cnts (Direct_Electrifying.cpp:139-215): new nodes per CNT.
+__global__ void k_node_counts(int n, const int32_t* __restrict__ eb, const int32_t* __restrict__ ee,
+                              const int32_t* __restrict__ elem, const int32_t* __restrict__ lmm, int32_t* __restrict__ cnt) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int b = eb[i], e = ee[i];
+        int m = e - b;
+        cnt[i] = (lmm[elem[b]] < 0 ? 1 : 0) + (m - 2) + (lmm[elem[e - 1]] < 0 ? 1 : 0);
+    }
+}
+
+__global__ void k_node_assign(int n, int reserved, const int32_t* __restrict__ eb, const int32_t* __restrict__ ee,
+                              const int32_t* __restrict__ elem, const int32_t* __restrict__ base, int32_t* lmm) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int b = eb[i], e = ee[i];
+        int node = reserved + base[i];
+        bool first_free = lmm[elem[b]] < 0, last_free = lmm[elem[e - 1]] < 0;
+        if (first_free) lmm[elem[b]] = node++;
+        for (int k = b + 1; k < e - 1; k++) lmm[elem[k]] = node++;
+        if (last_free) lmm[elem[e - 1]] = node++;
+    }
+}
+
+// Calculate_resistance_cnt (Direct_Electrifying.cpp:611-646): rho L / (pi r^2), L summed point by point.
+__device__ __forceinline__ double cnt_resistance(int P1, int P2, double radius, double rho, const double* __restrict__ x,
+                                                 const double* __restrict__ y, const double* __restrict__ z) {
+    double length = 0;
+    for (int i = P1; i < P2; i++) {
+        double dx = x[i] - x[i + 1], dy = y[i] - y[i + 1], dz = z[i] - z[i + 1];
+        length = length + sqrt(dx * dx + dy * dy + dz * dz);
+    }
+    return rho * length / (kPI * radius * radius);
+}
+
+__global__ void k_cnt_edge_counts(int n, const int32_t* __restrict__ eb, const int32_t* __restrict__ ee,
+                                  const int32_t* __restrict__ elem, const int32_t* __restrict__ lmm, int32_t* __restrict__ cnt) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int b = eb[i], m = ee[i] - b;
+        bool three = (m == 3) && lmm[elem[b]] == lmm[elem[b + 2]];
+        cnt[i] = three ? 1 : m - 1;
+    }
+}
+
+// Fill_2d_matrices_cnts + Three_points_in_element (Direct_Electrifying.cpp:489-608).
+__global__ void k_cnt_edges(int n, int r_flag, double rho, const int32_t* __restrict__ members, const int32_t* __restrict__ eb,
+                            const int32_t* __restrict__ ee, const int32_t* __restrict__ elem, const int32_t* __restrict__ lmm,
+                            const int32_t* __restrict__ ofs, const double* __restrict__ radii, const double* __restrict__ x,
+                            const double* __restrict__ y, const double* __restrict__ z, int32_t* __restrict__ n1,
+                            int32_t* __restrict__ n2, int32_t* __restrict__ op, double* __restrict__ g) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int b = eb[i], m = ee[i] - b, o = ofs[i];
+        double r = radii[members[i]];
+        if (m == 3 && lmm[elem[b]] == lmm[elem[b + 2]]) {
+            double g1 = 1.0, g2 = 1.0;
+            if (r_flag == 1) {
+                g1 = 1 / cnt_resistance(elem[b], elem[b + 1], r, rho, x, y, z);
+                g2 = 1 / cnt_resistance(elem[b + 1], elem[b + 2], r, rho, x, y, z);
+            }
+            n1[o] = lmm[elem[b]];
+            n2[o] = lmm[elem[b + 1]];
+            op[o] = OP_OVERWRITE;
+            g[o] = g1 + g2;
+            continue;
+        }
+        for (int k = 0; k < m - 1; k++) {
+            int P1 = elem[b + k], P2 = elem[b + k + 1];
+            double gi = r_flag ? 1 / cnt_resistance(P1, P2, r, rho, x, y, z) : 1.0;
+            n1[o + k] = lmm[P1];
+            n2[o + k] = lmm[P2];
+            op[o + k] = OP_OVERWRITE;
+            g[o + k] = gi;
+        }
+    }
+}
+
+// Fill_2d_matrices_cnt_junctions + Calculate_junction_resistance (Direct_Electrifying.cpp:737-901).
+__global__ void k_junction_edges(int nj, int base, int r_flag, int reserved, int jtype, double jres, double C1, double C2,
+                                 const int32_t* __restrict__ jlist, const int32_t* __restrict__ jp1, const int32_t* __restrict__ jn1,
+                                 const int32_t* __restrict__ jp2, const int32_t* __restrict__ jn2, const double* __restrict__ jd,
+                                 const double* __restrict__ radii, const int32_t* __restrict__ lmm, int32_t* __restrict__ n1,
+                                 int32_t* __restrict__ n2, int32_t* __restrict__ op, double* __restrict__ g) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nj; i += gridDim.x * blockDim.x) {
+        int idx = jlist[i];
+        int a = lmm[jp1[idx]], b = lmm[jp2[idx]];
+        int o = base + i;
+        n1[o] = a;
+        n2[o] = b;
+        g[o] = 0;
+        op[o] = OP_SKIP;
+        if (a == -1 || b == -1) continue;
+        double ginv = 1.0;
+        if (r_flag == 1) {
+            double Re;
+            if (jtype == 0) {
+                Re = jres;
+            } else {
+                double l1 = radii[jn1[idx]], l2 = radii[jn2[idx]];
+                double jl1 = l1 + l1, jl2 = l2 + l2;  // CNT diameters
+                double A = (jl1 - jl2 < kZero) ? jl1 * jl1 : jl2 * jl2;
+                double d = jd[idx];
+                Re = C1 * d * exp(C2 * d) / A;
+            }
+            ginv = 1 / Re;
+        }
+        if (a >= reserved && b >= reserved) {
+            op[o] = OP_OVERWRITE;
+            g[o] = ginv;
+        } else if (reserved > 2) {
+            op[o] = OP_ADD;
+            g[o] = ginv;
+        }
+    }
+}
+
+// Off-diagonal keys (row = max node, col = min node) and diagonal contributions.
+// Skipped edges get the key 1 << (2 bn) (off-diagonal) / 1 << bn (diagonal) and sort last.
+__global__ void k_edge_keys(int ne, int bn, const int32_t* __restrict__ n1, const int32_t* __restrict__ n2,
+                            const int32_t* __restrict__ op, uint64_t* __restrict__ okey, uint32_t* __restrict__ oval,
+                            uint64_t* __restrict__ dkey, uint32_t* __restrict__ dval) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ne; i += gridDim.x * blockDim.x) {
+        int a = n1[i], b = n2[i];
+        bool live = op[i] != OP_SKIP;
+        uint64_t hi = (uint64_t)max(a, b), lo = (uint64_t)min(a, b);
+        okey[i] = live ? ((hi << bn) | lo) : (1ull << (2 * bn));
+        oval[i] = (uint32_t)i;
+        dkey[2 * i] = live ? (uint64_t)a : (1ull << bn);
+        dval[2 * i] = (uint32_t)i;
+        dkey[2 * i + 1] = live ? (uint64_t)b : (1ull << bn);
+        dval[2 * i + 1] = (uint32_t)i;
+    }
+}
+
+// diagonal[node] += g in insertion order (Add_new_elements_to_2d_sparse_matrix et al.)
+__global__ void k_diag_reduce(int n2e, uint64_t skip, const uint64_t* __restrict__ dkey, const uint32_t* __restrict__ dval,
+                              const double* __restrict__ g, double* __restrict__ diag_all) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n2e; i += gridDim.x * blockDim.x) {
+        uint64_t k = dkey[i];
+        if (k == skip) continue;
+        if (i > 0 && dkey[i - 1] == k) continue;
+        double s = 0;
+        for (int j = i; j < n2e && dkey[j] == k; j++) s += g[dval[j]];
+        diag_all[k] = s;
+    }
+}
+
+// col_values[row][col]: overwrite / subtract in insertion order.
+__global__ void k_offdiag_reduce(int ne, uint64_t skip, const uint64_t* __restrict__ okey, const uint32_t* __restrict__ oval,
+                                 const int32_t* __restrict__ op, const double* __restrict__ g, int32_t* __restrict__ head,
+                                 double* __restrict__ runval) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ne; i += gridDim.x * blockDim.x) {
+        uint64_t k = okey[i];
+        bool h = (k != skip) && (i == 0 || okey[i - 1] != k);
+        head[i] = h ? 1 : 0;
+        if (!h) continue;
+        double v = 0;
+        for (int j = i; j < ne && okey[j] == k; j++) {
+            uint32_t e = oval[j];
+            if (op[e] == OP_OVERWRITE) v = -g[e];
+            else v = v - g[e];
+        }
+        runval[i] = v;
+    }
+}
+
+// From_2d_to_1d_vectors (Direct_Electrifying.cpp:1329-1394): split the unique
+// (row, col) entries of the free rows into the SSS lower block and the rhs.
+__global__ void k_sss_flags(int ne, int bn, int reserved, const uint64_t* __restrict__ okey, const int32_t* __restrict__ head,
+                            int32_t* __restrict__ lower_flag) {
+    const uint64_t mask = (1ull << bn) - 1;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ne; i += gridDim.x * blockDim.x) {
+        bool f = false;
+        if (head[i]) {
+            long long row = (long long)(okey[i] >> bn), col = (long long)(okey[i] & mask);
+            f = row >= reserved && col >= reserved;
+        }
+        lower_flag[i] = f ? 1 : 0;
+    }
+}
+
+__global__ void k_sss_fill(int ne, int bn, int reserved, const uint64_t* __restrict__ okey, const int32_t* __restrict__ lower_flag,
+                           const int32_t* __restrict__ lower_scan, const double* __restrict__ runval, int32_t* __restrict__ row_cnt,
+                           int32_t* __restrict__ col, double* __restrict__ val) {
+    const uint64_t mask = (1ull << bn) - 1;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ne; i += gridDim.x * blockDim.x) {
+        if (!lower_flag[i]) continue;
+        int row = (int)(okey[i] >> bn) - reserved, c = (int)(okey[i] & mask) - reserved;
+        int o = lower_scan[i];
+        col[o] = c;
+        val[o] = runval[i];
+        atomicAdd(&row_cnt[row], 1);
+    }
+}
+
+// rhs: R[i] = R[i] - K_ij * VEF[j] for reserved columns j, ascending j.
+__global__ void k_rhs(int ne, int bn, int reserved, const uint64_t* __restrict__ okey, const int32_t* __restrict__ head,
+                      const double* __restrict__ runval, const double* __restrict__ vef, double* __restrict__ b) {
+    const uint64_t mask = (1ull << bn) - 1;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ne; i += gridDim.x * blockDim.x) {
+        if (!head[i]) continue;
+        long long row = (long long)(okey[i] >> bn), col = (long long)(okey[i] & mask);
+        if (row < reserved || col >= reserved) continue;
+        // the first reserved-column entry of a row performs the row's ordered fold
+        bool first = true;
+        for (int j = i - 1; j >= 0; j--) {
+            if (!head[j]) continue;
+            long long r2 = (long long)(okey[j] >> bn);
+            if (r2 == row) first = false;
+            break;
+        }
+        if (!first) continue;
+        double R = 0;
+        for (int j = i; j < ne; j++) {
+            if (!head[j]) continue;
+            long long r2 = (long long)(okey[j] >> bn), c2 = (long long)(okey[j] & mask);
+            if (r2 != row || c2 >= reserved) break;
+            R = R - runval[j] * vef[c2];
+        }
+        b[row - reserved] = R;
+    }
+}
+
+__global__ void k_diag_free(int n, int reserved, const double* __restrict__ diag_all, double* __restrict__ diag, int* status) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double d = diag_all[i + reserved];
+        diag[i] = d;
+        if (fabs(d) < kZero) atomicCAS(status, 0, (int)DEV_ZERO_DIAG);
+    }
+}
+
+// Full symmetric CSR (diagonal + lower + upper) for the gather SpMV of the CG.
+__global__ void k_full_keys(int n, int m, int bn, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
+                            uint64_t* __restrict__ key, uint32_t* __restrict__ val) {
+    // entries: [0, n) diagonal, [n, n+m) lower (row, col), [n+m, n+2m) upper (col, row)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + 2 * m; i += gridDim.x * blockDim.x) {
+        uint64_t r, c;
+        if (i < n) {
+            r = c = (uint64_t)i;
+        } else {
+            int e = (i < n + m) ? i - n : i - n - m;
+            // row of lower entry e: binary search in rp
+            int lo = 0, hi = n;
+            while (hi - lo > 1) {
+                int mid = (lo + hi) >> 1;
+                if (rp[mid] <= e) lo = mid; else hi = mid;
+            }
+            uint64_t rr = (uint64_t)lo, cc = (uint64_t)col[e];
+            if (i < n + m) { r = rr; c = cc; } else { r = cc; c = rr; }
+        }
+        key[i] = (r << bn) | c;
+        val[i] = (uint32_t)i;
+    }
+}
+
+__global__ void k_full_fill(int n, int m, int bn, const uint64_t* __restrict__ key, const uint32_t* __restrict__ val,
+                            const double* __restrict__ diag, const double* __restrict__ lval, int32_t* __restrict__ rcnt,
+                            int32_t* __restrict__ fcol, double* __restrict__ fval, double* __restrict__ minv) {
+    const uint64_t mask = (1ull << bn) - 1;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + 2 * m; i += gridDim.x * blockDim.x) {
+        uint32_t src = val[i];
+        int r = (int)(key[i] >> bn);
+        fcol[i] = (int)(key[i] & mask);
+        double v;
+        if ((int)src < n) {
+            v = diag[src];
+            minv[src] = 1 / diag[src];  // Jacobi_preconditioner (Direct_Electrifying.cpp:1662-1668)
+        } else {
+            int e = ((int)src < n + m) ? (int)src - n : (int)src - n - m;
+            v = lval[e];
+        }
+        fval[i] = v;
+        atomicAdd(&rcnt[r], 1);
+    }
+}
+
+// Initial_guess_for_cnt_nodes (Direct_Electrifying.cpp:1434-1470).
+__global__ void k_initial_guess(int n, int reserved, int family, double v_p_coord, double max_coord, const int32_t* __restrict__ eb,
+                                const int32_t* __restrict__ ee, const int32_t* __restrict__ elem, const int32_t* __restrict__ lmm,
+                                const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
+                                double* __restrict__ x0) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        for (int k = eb[i]; k < ee[i]; k++) {
+            int P = elem[k];
+            int node = lmm[P];
+            if (node >= 2) {
+                double c = family == 0 ? x[P] : family == 1 ? y[P] : z[P];
+                x0[node - reserved] = v_p_coord * (max_coord - c);
+            }
+        }
+    }
+}
+
+__global__ void k_spmv_residual(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const double* __restrict__ v,
+                                const double* __restrict__ xin, const double* __restrict__ b, double* __restrict__ r) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double s = 0;
+        for (int k = rp[i]; k < rp[i + 1]; k++) s += v[k] * xin[ci[k]];
+        r[i] = b[i] - s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Persistent Jacobi-PCG (FP64).  Same recurrence as Solve_DEA_equations_CG_SSS
+// (Direct_Electrifying.cpp:1538-1659) with q = A p carried by recurrence
+// (q = A z + beta q) so each iteration needs two grid barriers:
+//   B: x += a p, r -= a q, z = M^-1 r, partials (r.r, r.z)   | barrier
+//   A: w = A z, q = w + b q, p = z + b p, partial (p.q)      | barrier
+// Stop when |r| <= tol |r0| (r0 after the initial guess), or after max_iter.
+struct CgArgs {
+    int n;
+    const int32_t* rp;
+    const int32_t* ci;
+    const double* val;
+    const double* minv;
+    double* x;
+    double* r;
+    double* z;
+    double* p;
+    double* q;
+    double* partA;  // 2 doubles per block
+    double* partB;  // 1 double per block
+    double* scal;   // [0] rr final, [1] iterations as double, [2] r0 norm
+    long long* iters;
+    GridBarrier bar;
+    int* err;
+    double tol;
+    long long max_iter;
+};
+
+__device__ __forceinline__ void block_reduce2(double a, double b, double* sm, double& ra, double& rb) {
+    a = warp_sum(a);
+    b = warp_sum(b);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) { sm[w] = a; sm[32 + w] = b; }
+    __syncthreads();
+    if (w == 0) {
+        const int nw = blockDim.x >> 5;
+        double x = lane < nw ? sm[lane] : 0.0, y = lane < nw ? sm[32 + lane] : 0.0;
+        x = warp_sum(x);
+        y = warp_sum(y);
+        if (lane == 0) { sm[64] = x; sm[65] = y; }
+    }
+    __syncthreads();
+    ra = sm[64];
+    rb = sm[65];
+    __syncthreads();
+}
+
+// Every block sums the per-block partials in the same fixed order.
+__device__ __forceinline__ void sum_partials(const double* part, int stride, int nb, double* sm, double& s0, double& s1) {
+    double a = 0, b = 0;
+    if (threadIdx.x < 32) {
+        for (int i = threadIdx.x; i < nb; i += 32) {
+            a += ((volatile double*)part)[i * stride];
+            if (stride > 1) b += ((volatile double*)part)[i * stride + 1];
+        }
+        a = warp_sum(a);
+        b = warp_sum(b);
+        if (threadIdx.x == 0) { sm[66] = a; sm[67] = b; }
+    }
+    __syncthreads();
+    s0 = sm[66];
+    s1 = sm[67];
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) k_cg_fp64(CgArgs a) {
+    __shared__ double sm[72];
+    const int nb = gridDim.x;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = nb * blockDim.x;
+    // z0 = M^-1 r0, p = z0, q = A p, partials: r.r, r.z
+    double rr_l = 0, rz_l = 0;
+    for (int i = tid; i < a.n; i += nth) {
+        double zi = a.minv[i] * a.r[i];
+        a.z[i] = zi;
+        a.p[i] = zi;
+        rr_l += a.r[i] * a.r[i];
+        rz_l += a.r[i] * zi;
+    }
+    double s0, s1;
+    block_reduce2(rr_l, rz_l, sm, s0, s1);
+    if (threadIdx.x == 0) { a.partA[2 * blockIdx.x] = s0; a.partA[2 * blockIdx.x + 1] = s1; }
+    if (!grid_sync(a.bar, nb, a.err)) return;
+    double rr, rz;
+    sum_partials(a.partA, 2, nb, sm, rr, rz);
+    const double R0 = a.tol * sqrt(rr);
+    double pq_l = 0;
+    for (int i = tid; i < a.n; i += nth) {
+        double w = 0;
+        for (int k = a.rp[i]; k < a.rp[i + 1]; k++) w += a.val[k] * a.p[a.ci[k]];
+        a.q[i] = w;
+        pq_l += a.p[i] * w;
+    }
+    block_reduce2(pq_l, 0.0, sm, s0, s1);
+    if (threadIdx.x == 0) a.partB[blockIdx.x] = s0;
+    if (!grid_sync(a.bar, nb, a.err)) return;
+    double pq, dummy;
+    sum_partials(a.partB, 1, nb, sm, pq, dummy);
+    long long k = 1;
+    double rr_new = rr;
+    for (; k <= a.max_iter; k++) {
+        const double alpha = rz / pq;
+        rr_l = 0;
+        rz_l = 0;
+        for (int i = tid; i < a.n; i += nth) {
+            a.x[i] += alpha * a.p[i];
+            double ri = a.r[i] - alpha * a.q[i];
+            a.r[i] = ri;
+            double zi = a.minv[i] * ri;
+            a.z[i] = zi;
+            rr_l += ri * ri;
+            rz_l += ri * zi;
+        }
+        block_reduce2(rr_l, rz_l, sm, s0, s1);
+        if (threadIdx.x == 0) { a.partA[2 * blockIdx.x] = s0; a.partA[2 * blockIdx.x + 1] = s1; }
+        if (!grid_sync(a.bar, nb, a.err)) return;
+        double rz_new;
+        sum_partials(a.partA, 2, nb, sm, rr_new, rz_new);
+        if (sqrt(rr_new) <= R0) break;
+        const double beta = rz_new / rz;
+        rz = rz_new;
+        pq_l = 0;
+        for (int i = tid; i < a.n; i += nth) {
+            double w = 0;
+            for (int kk = a.rp[i]; kk < a.rp[i + 1]; kk++) w += a.val[kk] * a.z[a.ci[kk]];
+            double qi = w + beta * a.q[i];
+            double pi = a.z[i] + beta * a.p[i];
+            a.q[i] = qi;
+            a.p[i] = pi;
+            pq_l += pi * qi;
+        }
+        block_reduce2(pq_l, 0.0, sm, s0, s1);
+        if (threadIdx.x == 0) a.partB[blockIdx.x] = s0;
+        if (!grid_sync(a.bar, nb, a.err)) return;
+        sum_partials(a.partB, 1, nb, sm, pq, dummy);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *a.iters = k > a.max_iter ? a.max_iter : k;
+        a.scal[0] = rr_new;
+        a.scal[2] = R0;
+    }
+}
+
+__global__ void k_true_residual(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const double* __restrict__ v,
+                                const double* __restrict__ xs, const double* __restrict__ b, double* out) {
+    __shared__ double sm[72];
+    double rr = 0, bb = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double s = 0;
+        for (int k = rp[i]; k < rp[i + 1]; k++) s += v[k] * xs[ci[k]];
+        double ri = b[i] - s;
+        rr += ri * ri;
+        bb += b[i] * b[i];
+    }
+    double s0, s1;
+    block_reduce2(rr, bb, sm, s0, s1);
+    if (threadIdx.x == 0) {
+        atomicAdd(&out[0], s0);
+        atomicAdd(&out[1], s1);
+    }
+}
+
+__global__ void k_voltages(int nodes, int reserved, const double* __restrict__ vef, const double* __restrict__ xs, double* __restrict__ v) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nodes; i += gridDim.x * blockDim.x)
+        v[i] = i < reserved ? vef[i] : xs[i - reserved];
+}
+
+// ---------------------------------------------------------------------------
+// Backbone (Backbone_Network.cpp:64-409): element currents on unit resistors,
+// zero current = 1e-9 I_max, one kept run per CNT.
+__device__ __forceinline__ void atomic_max_pos(unsigned long long* addr, double v) {
+    atomicMax(addr, (unsigned long long)__double_as_longlong(v));  // v >= 0: IEEE order == integer order
+}
+
+__global__ void k_current_max(int n, const int32_t* __restrict__ eb, const int32_t* __restrict__ ee, const int32_t* __restrict__ elem,
+                              const int32_t* __restrict__ lmm, const double* __restrict__ volt, int nj,
+                              const int32_t* __restrict__ jlist, const int32_t* __restrict__ jp1, const int32_t* __restrict__ jp2,
+                              unsigned long long* imax) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n + nj; i += gridDim.x * blockDim.x) {
+        double m = 0;
+        if (i < n) {
+            for (int k = eb[i]; k < ee[i] - 1; k++) m = fmax(m, fabs(volt[lmm[elem[k]]] - volt[lmm[elem[k + 1]]]));
+        } else {
+            int j = jlist[i - n];
+            m = fabs(volt[lmm[jp1[j]]] - volt[lmm[jp2[j]]]);
+        }
+        atomic_max_pos(imax, m);
+    }
+}
+
+__global__ void k_backbone_cnts(int n, const int32_t* __restrict__ members, const int32_t* __restrict__ eb, const int32_t* __restrict__ ee,
+                                const int32_t* __restrict__ elem, const int32_t* __restrict__ lmm, const double* __restrict__ volt,
+                                const unsigned long long* __restrict__ imax_bits, int trim, int32_t* __restrict__ cur_lo,
+                                int32_t* __restrict__ cur_hi, int32_t* __restrict__ alive) {
+    const double i_max = fmax(__longlong_as_double((long long)*imax_bits), kZero);
+    const double zero_current = i_max * 1e-9;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int b = eb[i], e = ee[i];
+        int idx1 = -1, idx2 = -1;
+        for (int k = 0; k < e - b - 1; k++) {
+            double I = fabs(volt[lmm[elem[b + k]]] - volt[lmm[elem[b + k + 1]]]);
+            if (I - zero_current > kZero) {
+                if (idx1 == -1) idx1 = k;
+            } else if (idx1 != -1 && idx2 == -1) {
+                idx2 = k;
+                break;
+            }
+        }
+        int c = members[i];
+        if (!trim) {
+            alive[i] = 1;
+            continue;
+        }
+        if (idx1 == -1) {
+            cur_lo[c] = -1;
+            cur_hi[c] = -2;
+            alive[i] = 0;
+        } else {
+            cur_lo[c] = b + idx1;
+            cur_hi[c] = (idx2 == -1) ? e - 1 : b + idx2;
+            alive[i] = 1;
+        }
+    }
+}
+
+// Remove_junctions_with_dead_particles_cnts (Backbone_Network.cpp:950-992).
+__global__ void k_junction_alive(int nj, const int32_t* __restrict__ jlist, const int32_t* __restrict__ jp1, const int32_t* __restrict__ jn1,
+                                 const int32_t* __restrict__ jp2, const int32_t* __restrict__ jn2, const int32_t* __restrict__ cur_lo,
+                                 const int32_t* __restrict__ cur_hi, const int32_t* __restrict__ elem_pos, int32_t* __restrict__ alive) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nj; i += gridDim.x * blockDim.x) {
+        int j = jlist[i];
+        int c1 = jn1[j], c2 = jn2[j];
+        bool ok = cur_lo[c1] >= 0 && cur_lo[c2] >= 0;
+        if (ok) {
+            int q1 = elem_pos[jp1[j]], q2 = elem_pos[jp2[j]];
+            ok = q1 >= cur_lo[c1] && q1 <= cur_hi[c1] && q2 >= cur_lo[c2] && q2 <= cur_hi[c2];
+        }
+        alive[i] = ok ? 1 : 0;
+    }
+}
+
+__global__ void k_compact_i32(int n, const int32_t* __restrict__ in, const int32_t* __restrict__ flag, const int32_t* __restrict__ scan,
+                              int32_t* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (flag[i]) out[scan[i]] = in[i];
+}
+
+// Currents_through_boundary_cnts / Current_of_element_in_boundary (Electrical_analysis.cpp:499-605),
+// summed sequentially in boundary order like upstream.
+__global__ void k_boundary_current(int b, int e, const int32_t* __restrict__ bcnt, const int32_t* __restrict__ cur_lo,
+                                   const int32_t* __restrict__ cur_hi, const int32_t* __restrict__ elem, const int32_t* __restrict__ lmm,
+                                   const double* __restrict__ volt, const double* __restrict__ radii, double rho,
+                                   const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
+                                   double* out) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    double I = 0;
+    for (int i = b; i < e; i++) {
+        int c = bcnt[i];
+        int lo = cur_lo[c], hi = cur_hi[c];
+        if (lo < 0 || hi < lo) continue;
+        for (int side = 0; side < 2; side++) {
+            int P1 = side == 0 ? elem[lo] : elem[hi];
+            int P2 = side == 0 ? elem[lo + 1] : elem[hi - 1];
+            int n1 = lmm[P1];
+            if (n1 < 0 || n1 > 1) continue;
+            int n2 = lmm[P2];
+            if (n2 < 0) continue;
+            double V = volt[n2] - volt[n1];
+            double Re = (P1 > P2) ? cnt_resistance(P2, P1, radii[c], rho, x, y, z) : cnt_resistance(P1, P2, radii[c], rho, x, y, z);
+            I = I + V / Re;
+        }
+    }
+    *out = I;
+}
+
+__global__ void k_init_ranges(int nc, const int32_t* __restrict__ cstart, const int32_t* __restrict__ clen, const int32_t* __restrict__ mscan,
+                              int32_t* __restrict__ lo, int32_t* __restrict__ hi) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+        int b = mscan[cstart[c]], e = mscan[cstart[c] + clen[c]];
+        if (clen[c] == 0) b = e = 0;
+        lo[c] = e > b ? b : -1;
+        hi[c] = e > b ? e - 1 : -2;
+    }
+}
+
+// ---------------------------------------------------------------------------
+struct SolveInput {
+    int cluster;
+    int pass;  // -1 unit, 0..2 direction
+    int family;
+    const int32_t* members;
+    int n_members;
+    const int32_t* jlist;
+    int n_jlist;
+};
+
+double seconds_between(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms * 1e-3;
+}
+
+// Direct_Electrifying::Compute_voltage_field (Direct_Electrifying.cpp:11-113), CNT branch.
+DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<int32_t>& eb, DBuf<int32_t>& ee) {
+    cudaStream_t s = c.stream;
+    const int r_flag = in.pass >= 0 ? 1 : 0;
+    int bnd[6];
+    const int nbnd = boundaries_of_family(in.family, bnd);
+    if (nbnd < 0) throw Fail{CICY_E_INPUT, "Compute_voltage_field: invalid family"};
+    const int reserved = nbnd;  // Get_global_nodes: 2/4/6
+    const int NM = in.n_members;
+    DeaSystem* sys = new DeaSystem;
+    sys->cluster = in.cluster;
+    sys->pass = in.pass;
+    sys->reserved = reserved;
+    try {
+        eb.ensure(NM + 1);
+        ee.ensure(NM + 1);
+        k_cluster_ranges<<<grid_for(NM), 256, 0, s>>>(NM, in.members, c.bb_lo.get(), c.bb_hi.get(), eb.get(), ee.get(), c.status.get());
+        c.launches++;
+        check_status(c, "LM_matrix_for_cnts");
+        // ---- LMM ----
+        c.lmm.ensure(std::max(c.n_points, 1));
+        CICY_CUDA(cudaMemsetAsync(c.lmm.get(), 0xff, sizeof(int32_t) * std::max(c.n_points, 1), s));
+        for (int k = 0; k < nbnd; k++) {
+            int f = bnd[k];
+            int b = c.h_bpts_ptr[f], e = c.h_bpts_ptr[f + 1];
+            if (e > b) {
+                k_lmm_face<<<grid_for(e - b), 256, 0, s>>>(b, e, c.bpts_idx.get(), k, c.lmm.get());
+                c.launches++;
+            }
+        }
+        c.cnt_nodes.ensure(NM + 1);
+        c.cnt_node_base.ensure(NM + 1);
+        k_node_counts<<<grid_for(NM), 256, 0, s>>>(NM, eb.get(), ee.get(), c.elem_idx.get(), c.lmm.get(), c.cnt_nodes.get());
+        exclusive_scan_i32(c.cnt_nodes.get(), c.cnt_node_base.get(), NM, c.i32_scalar.get(), c.scan_tmp32, s, c.launches);
+        k_node_assign<<<grid_for(NM), 256, 0, s>>>(NM, reserved, eb.get(), ee.get(), c.elem_idx.get(), c.cnt_node_base.get(), c.lmm.get());
+        c.launches += 2;
+        const int nodes = reserved + read_i32(c, c.i32_scalar.get());
+        const int n = nodes - reserved;
+        sys->nodes = nodes;
+        // ---- edges ----
+        k_cnt_edge_counts<<<grid_for(NM), 256, 0, s>>>(NM, eb.get(), ee.get(), c.elem_idx.get(), c.lmm.get(), c.cnt_nodes.get());
+        exclusive_scan_i32(c.cnt_nodes.get(), c.cnt_node_base.get(), NM, c.i32_scalar.get(), c.scan_tmp32, s, c.launches);
+        c.launches++;
+        const int n_cnt_edges = read_i32(c, c.i32_scalar.get());
+        const int NE = n_cnt_edges + in.n_jlist;
+        c.e_n1.ensure(NE + 1); c.e_n2.ensure(NE + 1); c.e_op.ensure(NE + 1); c.e_g.ensure(NE + 1);
+        k_cnt_edges<<<grid_for(NM), 256, 0, s>>>(NM, r_flag, p.resistivity_cnt, in.members, eb.get(), ee.get(), c.elem_idx.get(), c.lmm.get(),
+                                               c.cnt_node_base.get(), c.radii.get(), c.x.get(), c.y.get(), c.z.get(), c.e_n1.get(),
+                                               c.e_n2.get(), c.e_op.get(), c.e_g.get());
+        c.launches++;
+        if (in.n_jlist > 0) {
+            k_junction_edges<<<grid_for(in.n_jlist), 256, 0, s>>>(in.n_jlist, n_cnt_edges, r_flag, reserved, p.junction_type,
+                                                                p.junction_resistance, p.C1, p.C2, in.jlist, c.j_p1.get(), c.j_n1.get(),
+                                                                c.j_p2.get(), c.j_n2.get(), c.j_d.get(), c.radii.get(), c.lmm.get(),
+                                                                c.e_n1.get(), c.e_n2.get(), c.e_op.get(), c.e_g.get());
+            c.launches++;
+        }
+        // ---- sort-and-reduce assembly ----
+        const int bn = bits_for((uint64_t)std::max(nodes, 1));
+        const int ND = 2 * NE;
+        c.sort_k.ensure(std::max(ND, 2 * NE) + 2);
+        c.sort_v.ensure(std::max(ND, 2 * NE) + 2);
+        DBuf<uint64_t>& dkey = c.dkey;
+        DBuf<uint32_t>& dval = c.dval;
+        dkey.ensure(ND + 2);
+        dval.ensure(ND + 2);
+        k_edge_keys<<<grid_for(NE), 256, 0, s>>>(NE, bn, c.e_n1.get(), c.e_n2.get(), c.e_op.get(), c.sort_k.get(), c.sort_v.get(),
+                                               dkey.get(), dval.get());
+        c.launches++;
+        radix_sort_pairs(c.sort_k.get(), c.sort_v.get(), NE, 2 * bn + 1, c.rs, s, c.launches);
+        radix_sort_pairs(dkey.get(), dval.get(), ND, bn + 1, c.rs, s, c.launches);
+        c.work_f64a.ensure(std::max(nodes, NE) + 1);  // diag over all nodes
+        CICY_CUDA(cudaMemsetAsync(c.work_f64a.get(), 0, sizeof(double) * (nodes + 1), s));
+        k_diag_reduce<<<grid_for(ND), 256, 0, s>>>(ND, 1ull << bn, dkey.get(), dval.get(), c.e_g.get(), c.work_f64a.get());
+        c.work_i32a.ensure(NE + 1);
+        c.work_i32b.ensure(NE + 1);
+        c.work_i32c.ensure(NE + 1);
+        c.runval.ensure(NE + 1);
+        k_offdiag_reduce<<<grid_for(NE), 256, 0, s>>>(NE, 1ull << (2 * bn), c.sort_k.get(), c.sort_v.get(), c.e_op.get(), c.e_g.get(), c.work_i32a.get(),
+                                                    c.runval.get());
+        k_sss_flags<<<grid_for(NE), 256, 0, s>>>(NE, bn, reserved, c.sort_k.get(), c.work_i32a.get(), c.work_i32b.get());
+        exclusive_scan_i32(c.work_i32b.get(), c.work_i32c.get(), NE, c.i32_scalar.get(), c.scan_tmp32, s, c.launches);
+        c.launches += 3;
+        const int m = read_i32(c, c.i32_scalar.get());
+        sys->nnz_lower = m;
+        sys->row_ptr.ensure(n + 1); sys->col.ensure(std::max(m, 1)); sys->val.ensure(std::max(m, 1));
+        sys->diag.ensure(std::max(n, 1)); sys->b.ensure(std::max(n, 1)); sys->x0.ensure(std::max(n, 1));
+        sys->volt.ensure(std::max(nodes, 1));
+        c.cnt_nodes.ensure(n + 1);
+        CICY_CUDA(cudaMemsetAsync(c.cnt_nodes.get(), 0, sizeof(int32_t) * (n + 1), s));
+        k_sss_fill<<<grid_for(NE), 256, 0, s>>>(NE, bn, reserved, c.sort_k.get(), c.work_i32b.get(), c.work_i32c.get(), c.runval.get(),
+                                              c.cnt_nodes.get(), sys->col.get(), sys->val.get());
+        exclusive_scan_i32(c.cnt_nodes.get(), sys->row_ptr.get(), n + 1, nullptr, c.scan_tmp32, s, c.launches);
+        // Get_voltage_vector (Direct_Electrifying.cpp:1472-1500)
+        std::vector<double> vef(reserved, 0.0);
+        const double V = r_flag ? p.applied_voltage : (double)nodes;
+        for (int i = 1; i < reserved; i++) vef[i] = vef[i - 1] + V;
+        c.vef.ensure(8);
+        CICY_CUDA(cudaMemcpyAsync(c.vef.get(), vef.data(), sizeof(double) * reserved, cudaMemcpyHostToDevice, s));
+        CICY_CUDA(cudaMemsetAsync(sys->b.get(), 0, sizeof(double) * std::max(n, 1), s));
+        k_rhs<<<grid_for(NE), 256, 0, s>>>(NE, bn, reserved, c.sort_k.get(), c.work_i32a.get(), c.runval.get(), c.vef.get(), sys->b.get());
+        k_diag_free<<<grid_for(n), 256, 0, s>>>(n, reserved, c.work_f64a.get(), sys->diag.get(), c.status.get());
+        c.launches += 3;
+        check_status(c, "Fill_sparse_stiffness_matrix");
+        // ---- full CSR for the CG ----
+        const int NF = n + 2 * m;
+        const int bnf = bits_for((uint64_t)std::max(n, 1));
+        c.sort_k.ensure(NF + 1);
+        c.sort_v.ensure(NF + 1);
+        c.cg_rp.ensure(n + 1); c.cg_ci.ensure(NF + 1); c.cg_val.ensure(NF + 1); c.cg_minv.ensure(n + 1);
+        k_full_keys<<<grid_for(NF), 256, 0, s>>>(n, m, bnf, sys->row_ptr.get(), sys->col.get(), c.sort_k.get(), c.sort_v.get());
+        radix_sort_pairs(c.sort_k.get(), c.sort_v.get(), NF, 2 * bnf, c.rs, s, c.launches);
+        CICY_CUDA(cudaMemsetAsync(c.cnt_nodes.get(), 0, sizeof(int32_t) * (n + 1), s));
+        k_full_fill<<<grid_for(NF), 256, 0, s>>>(n, m, bnf, c.sort_k.get(), c.sort_v.get(), sys->diag.get(), sys->val.get(), c.cnt_nodes.get(),
+                                               c.cg_ci.get(), c.cg_val.get(), c.cg_minv.get());
+        exclusive_scan_i32(c.cnt_nodes.get(), c.cg_rp.get(), n + 1, nullptr, c.scan_tmp32, s, c.launches);
+        c.launches += 2;
+        // ---- initial guess and r0 ----
+        c.cg_x.ensure(n + 1); c.cg_r.ensure(n + 1); c.cg_z.ensure(n + 1); c.cg_p.ensure(n + 1); c.cg_q.ensure(n + 1);
+        CICY_CUDA(cudaMemsetAsync(sys->x0.get(), 0, sizeof(double) * std::max(n, 1), s));
+        if (r_flag && reserved == 2) {
+            const cicy_cuboid& w = c.window;
+            const double Lw = in.family == 0 ? w.len_x : in.family == 1 ? w.len_y : w.len_z;
+            const double maxc = in.family == 0 ? w.max_x : in.family == 1 ? w.max_y : w.max_z;
+            k_initial_guess<<<grid_for(NM), 256, 0, s>>>(NM, reserved, in.family, p.applied_voltage / Lw, maxc, eb.get(), ee.get(),
+                                                       c.elem_idx.get(), c.lmm.get(), c.x.get(), c.y.get(), c.z.get(), sys->x0.get());
+            c.launches++;
+        }
+        if (n > 0) {
+            k_spmv_residual<<<grid_for(n), 256, 0, s>>>(n, c.cg_rp.get(), c.cg_ci.get(), c.cg_val.get(), sys->x0.get(), sys->b.get(), c.cg_r.get());
+            CICY_CUDA(cudaMemcpyAsync(c.cg_x.get(), sys->x0.get(), sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+            c.launches++;
+        }
+        // ---- CG ----
+        cudaEvent_t e0, e1;
+        CICY_CUDA(cudaEventCreate(&e0));
+        CICY_CUDA(cudaEventCreate(&e1));
+        CICY_CUDA(cudaEventRecord(e0, s));
+        if (n > 0) {
+            int occ = 0;
+            CICY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cg_fp64, 256, 0));
+            int nb = std::min(std::max(1, occ) * c.num_sms, std::max(1, ceil_div(n, 256)));
+            c.cg_part.ensure(4 * nb + 8);
+            c.barrier.ensure(2);
+            c.cg_scal.ensure(4);
+            c.cg_iters.ensure(1);
+            CICY_CUDA(cudaMemsetAsync(c.barrier.get(), 0, sizeof(unsigned) * 2, s));
+            CgArgs a;
+            a.n = n; a.rp = c.cg_rp.get(); a.ci = c.cg_ci.get(); a.val = c.cg_val.get(); a.minv = c.cg_minv.get();
+            a.x = c.cg_x.get(); a.r = c.cg_r.get(); a.z = c.cg_z.get(); a.p = c.cg_p.get(); a.q = c.cg_q.get();
+            a.partA = c.cg_part.get(); a.partB = c.cg_part.get() + 2 * nb; a.scal = c.cg_scal.get(); a.iters = c.cg_iters.get();
+            a.bar = GridBarrier{c.barrier.get(), c.barrier.get() + 1};
+            a.err = c.status.get();
+            a.tol = p.tolerance;
+            a.max_iter = (long long)c.solver.max_iter_factor * nodes;
+            void* args[] = {&a};
+            CICY_CUDA(cudaLaunchCooperativeKernel((void*)k_cg_fp64, dim3(nb), dim3(256), args, 0, s));
+            c.launches++;
+        }
+        CICY_CUDA(cudaEventRecord(e1, s));
+        check_status(c, "Solve_DEA_equations_CG_SSS");
+        sys->seconds = seconds_between(e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        long long iters = 0;
+        if (n > 0) CICY_CUDA(cudaMemcpy(&iters, c.cg_iters.get(), sizeof(long long), cudaMemcpyDeviceToHost));
+        sys->iterations = iters;
+        // true FP64 residual |b - A x| / |b|
+        double rb[2] = {0, 0};
+        if (n > 0) {
+            CICY_CUDA(cudaMemsetAsync(c.cg_scal.get(), 0, sizeof(double) * 2, s));
+            k_true_residual<<<grid_for(n), 256, 0, s>>>(n, c.cg_rp.get(), c.cg_ci.get(), c.cg_val.get(), c.cg_x.get(), sys->b.get(), c.cg_scal.get());
+            c.launches++;
+            CICY_CUDA(cudaMemcpyAsync(rb, c.cg_scal.get(), sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+        }
+        k_voltages<<<grid_for(nodes), 256, 0, s>>>(nodes, reserved, c.vef.get(), c.cg_x.get(), sys->volt.get());
+        c.launches++;
+        CICY_CUDA(cudaStreamSynchronize(s));
+        sys->rel_residual = rb[1] > 0 ? std::sqrt(rb[0] / rb[1]) : 0.0;
+    } catch (...) {
+        delete sys;
+        throw;
+    }
+    return sys;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Electrical_analysis::Perform_analysis_on_clusters (Electrical_analysis.cpp:10-145).
+void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out) {
+    if (c.stage < 3) throw Fail{CICY_E_STATE, "cicy_electrical_analysis: run cicy_clusters first"};
+    cudaStream_t s = c.stream;
+    for (auto* sy : c.systems) delete sy;
+    c.systems.clear();
+    const int NC = std::max(c.n_cnts, 1);
+    // current elements_cnt state of every CNT: [lo, hi] into elem_idx
+    c.bb_lo.ensure(NC);
+    c.bb_hi.ensure(NC);
+    k_init_ranges<<<grid_for(NC), 256, 0, s>>>(c.n_cnts, c.cstart.get(), c.clen.get(), c.mark_scan.get(), c.bb_lo.get(), c.bb_hi.get());
+    c.launches++;
+    // working copies of the percolated clusters and their junction lists (backbone shrinks them)
+    const int n_clu_idx = c.h_clu_ptr.empty() ? 0 : c.h_clu_ptr.back();
+    const int n_cj_idx = c.h_cj_ptr.empty() ? 0 : c.h_cj_ptr.back();
+    c.bbclu_idx.ensure(std::max(n_clu_idx, 1));
+    c.bbcj_idx.ensure(std::max(n_cj_idx, 1));
+    if (n_clu_idx) CICY_CUDA(cudaMemcpyAsync(c.bbclu_idx.get(), c.clu_idx.get(), sizeof(int32_t) * n_clu_idx, cudaMemcpyDeviceToDevice, s));
+    if (n_cj_idx) CICY_CUDA(cudaMemcpyAsync(c.bbcj_idx.get(), c.cj_idx.get(), sizeof(int32_t) * n_cj_idx, cudaMemcpyDeviceToDevice, s));
+    c.h_bbclu_ptr = c.h_clu_ptr;
+    c.h_bbcj_ptr = c.h_cj_ptr;
+    std::vector<int32_t> clu_len(c.n_perc), cj_len(c.n_perc);
+    for (int k = 0; k < c.n_perc; k++) {
+        clu_len[k] = c.h_clu_ptr[k + 1] - c.h_clu_ptr[k];
+        cj_len[k] = c.h_cj_ptr[k + 1] - c.h_cj_ptr[k];
+    }
+    std::vector<std::vector<double> > parallel(3);
+    double t_unit = 0, t_bb = 0, t_real = 0;
+    DBuf<int32_t>& eb = c.eb;
+    DBuf<int32_t>& ee = c.ee;
+    c.imax.ensure(1);
+    c.alive.ensure(std::max(std::max(n_clu_idx, n_cj_idx), 1) + 1);
+    c.alive_scan.ensure(std::max(std::max(n_clu_idx, n_cj_idx), 1) + 1);
+    c.tmp_list.ensure(std::max(std::max(n_clu_idx, n_cj_idx), 1) + 1);
+    c.cur_out.ensure(4);
+    const int scope = p.simulation_scope;
+    for (int k = 0; k < c.n_perc && scope < 2; k++) {
+        int32_t* members = c.bbclu_idx.get() + c.h_clu_ptr[k];
+        int32_t* jl = c.bbcj_idx.get() + c.h_cj_ptr[k];
+        SolveInput u{k, -1, c.h_family[k], members, clu_len[k], jl, cj_len[k]};
+        DeaSystem* su = solve_dea(c, p, u, eb, ee);
+        c.systems.push_back(su);
+        t_unit += su->seconds;
+        // ---- backbone ----
+        cudaEvent_t e0, e1;
+        CICY_CUDA(cudaEventCreate(&e0));
+        CICY_CUDA(cudaEventCreate(&e1));
+        CICY_CUDA(cudaEventRecord(e0, s));
+        const int NM = clu_len[k], NJ = cj_len[k];
+        CICY_CUDA(cudaMemsetAsync(c.imax.get(), 0, sizeof(unsigned long long), s));
+        k_current_max<<<grid_for(NM + NJ), 256, 0, s>>>(NM, eb.get(), ee.get(), c.elem_idx.get(), c.lmm.get(), su->volt.get(), NJ, jl,
+                                                      c.j_p1.get(), c.j_p2.get(), c.imax.get());
+        k_backbone_cnts<<<grid_for(NM), 256, 0, s>>>(NM, members, eb.get(), ee.get(), c.elem_idx.get(), c.lmm.get(), su->volt.get(),
+                                                   c.imax.get(), scope == 0 ? 1 : 0, c.bb_lo.get(), c.bb_hi.get(), c.alive.get());
+        c.launches += 2;
+        if (scope == 0) {
+            exclusive_scan_i32(c.alive.get(), c.alive_scan.get(), NM, c.i32_scalar.get(), c.scan_tmp32, s, c.launches);
+            k_compact_i32<<<grid_for(NM), 256, 0, s>>>(NM, members, c.alive.get(), c.alive_scan.get(), c.tmp_list.get());
+            c.launches++;
+            int nm2 = read_i32(c, c.i32_scalar.get());
+            if (nm2) CICY_CUDA(cudaMemcpyAsync(members, c.tmp_list.get(), sizeof(int32_t) * nm2, cudaMemcpyDeviceToDevice, s));
+            clu_len[k] = nm2;
+            if (NJ > 0) {
+                k_junction_alive<<<grid_for(NJ), 256, 0, s>>>(NJ, jl, c.j_p1.get(), c.j_n1.get(), c.j_p2.get(), c.j_n2.get(), c.bb_lo.get(),
+                                                            c.bb_hi.get(), c.mark_scan.get(), c.alive.get());
+                exclusive_scan_i32(c.alive.get(), c.alive_scan.get(), NJ, c.i32_scalar.get(), c.scan_tmp32, s, c.launches);
+                k_compact_i32<<<grid_for(NJ), 256, 0, s>>>(NJ, jl, c.alive.get(), c.alive_scan.get(), c.tmp_list.get());
+                c.launches += 2;
+                int nj2 = read_i32(c, c.i32_scalar.get());
+                if (nj2) CICY_CUDA(cudaMemcpyAsync(jl, c.tmp_list.get(), sizeof(int32_t) * nj2, cudaMemcpyDeviceToDevice, s));
+                cj_len[k] = nj2;
+            }
+        }
+        CICY_CUDA(cudaEventRecord(e1, s));
+        CICY_CUDA(cudaEventSynchronize(e1));
+        t_bb += seconds_between(e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (scope != 0) continue;
+        // ---- real-resistor passes per percolated direction (Electrical_analysis.cpp:229-289) ----
+        std::vector<int> dirs;
+        const int fam = c.h_family[k];
+        const int dir_bits[7] = {1, 2, 4, 3, 5, 6, 7};
+        for (int d = 0; d < 3; d++)
+            if ((dir_bits[fam] >> d & 1) && p.resistances[d]) dirs.push_back(d);
+        for (int d : dirs) {
+            SolveInput r{k, d, d, members, clu_len[k], jl, cj_len[k]};
+            DeaSystem* sr = solve_dea(c, p, r, eb, ee);
+            c.systems.push_back(sr);
+            t_real += sr->seconds;
+            // Calculate_parallel_resistor (Electrical_analysis.cpp:355-473)
+            const int b1 = d == 0 ? 2 : d == 1 ? 3 : 0;
+            const int b2 = d == 0 ? 4 : d == 1 ? 5 : 1;
+            if (c.h_bcnt_ptr[b1 + 1] == c.h_bcnt_ptr[b1] || c.h_bcnt_ptr[b2 + 1] == c.h_bcnt_ptr[b2])
+                throw Fail{CICY_E_INPUT, "Calculate_parallel_resistor: one boundary vector along the direction is empty"};
+            k_boundary_current<<<1, 32, 0, s>>>(c.h_bcnt_ptr[b1], c.h_bcnt_ptr[b1 + 1], c.bcnt_idx.get(), c.bb_lo.get(), c.bb_hi.get(),
+                                                c.elem_idx.get(), c.lmm.get(), sr->volt.get(), c.radii.get(), p.resistivity_cnt, c.x.get(),
+                                                c.y.get(), c.z.get(), c.cur_out.get());
+            c.launches++;
+            double I = 0;
+            CICY_CUDA(cudaMemcpyAsync(&I, c.cur_out.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
+            CICY_CUDA(cudaStreamSynchronize(s));
+            parallel[d].push_back(p.applied_voltage / I);
+        }
+    }
+    c.h_bbclu_ptr.assign(c.n_perc + 1, 0);
+    c.h_bbcj_ptr.assign(c.n_perc + 1, 0);
+    for (int k = 0; k < c.n_perc; k++) {
+        c.h_bbclu_ptr[k + 1] = c.h_bbclu_ptr[k] + clu_len[k];
+        c.h_bbcj_ptr[k + 1] = c.h_bbcj_ptr[k] + cj_len[k];
+    }
+    c.bb_clu_len = clu_len;
+    c.bb_cj_len = cj_len;
+    c.have_backbone = true;
+    // Calculate_resistances_and_resistivities (Electrical_analysis.cpp:873-987)
+    if (out) {
+        const cicy_cuboid& w = c.window;
+        const double L[3] = {w.len_x, w.len_y, w.len_z};
+        const double A[3] = {w.len_y * w.len_z, w.len_x * w.len_z, w.len_x * w.len_y};
+        for (int d = 0; d < 3; d++) {
+            double R;
+            if (parallel[d].empty()) {
+                out->resistivities[d] = p.resistivity_matrix;
+                R = p.resistivity_matrix * L[d] / A[d];
+                out->resistances[d] = R;
+                continue;
+            } else if (parallel[d].size() == 1) {
+                R = parallel[d][0];
+            } else {
+                double sum = 0;
+                for (double r : parallel[d]) sum = sum + 1 / r;
+                R = 1 / sum;
+            }
+            out->resistances[d] = R;
+            out->resistivities[d] = R * A[d] / L[d];
+        }
+        out->n_percolated = c.n_perc;
+        out->n_solves = (int32_t)std::min<size_t>(c.systems.size(), 32);
+        for (int i = 0; i < out->n_solves; i++) {
+            DeaSystem* sy = c.systems[i];
+            cicy_solve_info& si = out->solves[i];
+            si.cluster = sy->cluster;
+            si.pass = sy->pass;
+            si.nodes = sy->nodes;
+            si.reserved = sy->reserved;
+            si.nnz_lower = sy->nnz_lower;
+            si.iterations = sy->iterations;
+            si.rel_residual = sy->rel_residual;
+            si.seconds = sy->seconds;
+        }
+        out->stage_seconds[2] = t_unit;
+        out->stage_seconds[3] = t_bb;
+        out->stage_seconds[4] = t_real;
+    }
+    c.stage = 4;
+}
+
+}  // namespace cicy

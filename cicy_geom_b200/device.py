@@ -1,0 +1,189 @@
+"""Device context: the hot path through the C ABI of libcicy_b200.
+
+`Context` mirrors the upstream call sequence of App_Network_3D for one window
+(App_Network_3D.cpp:140-179):
+
+    ctx = Context(0)
+    ctx.upload(window_network)           # window-trimmed network (host arrays)
+    ctx.contact_grid(params)             # Contact_grid::Generate_contact_grid
+    ctx.clusters(params)                 # Hoshen_Kopelman::Determine_clusters_and_percolation
+    res = ctx.electrical_analysis(params)  # Electrical_analysis::Perform_analysis_on_clusters
+
+and exposes the public members the upstream classes hand to later stages
+(sectioned domain, point contacts, labels, junctions, elements, clusters,
+families, each DEA system and its voltages) as numpy arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._abi import check, lib
+from .network import HostNetwork
+
+
+def _p(a, ct):
+    return None if a is None else a.ctypes.data_as(C.POINTER(ct))
+
+
+class Context:
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(lib().cicy_ctx_create(C.byref(h), device), "cicy_ctx_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().cicy_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _check(self, st, where):
+        check(st, where, self._h)
+
+    # ---- configuration ----
+    def set_stream(self, stream_ptr: int):
+        self._check(lib().cicy_ctx_set_stream(self._h, C.c_void_p(stream_ptr)), "cicy_ctx_set_stream")
+
+    def stream(self) -> int:
+        return lib().cicy_ctx_stream(self._h) or 0
+
+    def set_solver(self, precision: int = 0, preconditioner: int = 0, max_iter_factor: int = 300):
+        o = _abi.SolverOpts(precision, preconditioner, max_iter_factor, 0)
+        self._check(lib().cicy_ctx_set_solver(self._h, C.byref(o)), "cicy_ctx_set_solver")
+
+    def kernel_launches(self) -> int:
+        return int(lib().cicy_ctx_kernel_launches(self._h))
+
+    # ---- stages ----
+    def upload(self, net: HostNetwork):
+        v = net.view()
+        self._check(lib().cicy_upload_network(self._h, C.byref(v)), "cicy_upload_network")
+
+    def contact_grid(self, p: _abi.Params):
+        self._check(lib().cicy_contact_grid(self._h, C.byref(p)), "cicy_contact_grid")
+
+    def clusters(self, p: _abi.Params):
+        self._check(lib().cicy_clusters(self._h, C.byref(p)), "cicy_clusters")
+
+    def electrical_analysis(self, p: _abi.Params) -> _abi.Result:
+        r = _abi.Result()
+        self._check(lib().cicy_electrical_analysis(self._h, C.byref(p), C.byref(r)), "cicy_electrical_analysis")
+        return r
+
+    def network_to_conductance(self, p: _abi.Params) -> _abi.Result:
+        r = _abi.Result()
+        self._check(lib().cicy_network_to_conductance(self._h, C.byref(p), C.byref(r)), "cicy_network_to_conductance")
+        return r
+
+    # ---- copy-out ----
+    def sectioned_domain(self):
+        nr, ns = C.c_int64(), C.c_int64()
+        self._check(lib().cicy_get_sectioned_domain(self._h, C.byref(nr), C.byref(ns), None, None), "get_sectioned_domain")
+        ptr = np.zeros(nr.value + 1, np.int64)
+        idx = np.zeros(max(ns.value, 1), np.int64)
+        self._check(lib().cicy_get_sectioned_domain(self._h, C.byref(nr), C.byref(ns), _p(ptr, C.c_int64), _p(idx, C.c_int64)),
+                    "get_sectioned_domain")
+        return ptr, idx[: ns.value]
+
+    def point_contacts(self):
+        n = C.c_int64()
+        self._check(lib().cicy_get_point_contacts(self._h, C.byref(n), None, None, None, None), "get_point_contacts")
+        N = n.value
+        pa, pb = np.zeros(max(N, 1), np.int64), np.zeros(max(N, 1), np.int64)
+        cb, d = np.zeros(max(N, 1), np.int32), np.zeros(max(N, 1), np.float64)
+        self._check(lib().cicy_get_point_contacts(self._h, C.byref(n), _p(pa, C.c_int64), _p(cb, C.c_int32), _p(pb, C.c_int64),
+                                                  _p(d, C.c_double)), "get_point_contacts")
+        return pa[:N], cb[:N], pb[:N], d[:N]
+
+    def labels(self):
+        nc, nl = C.c_int32(), C.c_int32()
+        self._check(lib().cicy_get_labels(self._h, C.byref(nc), C.byref(nl), None), "get_labels")
+        lab = np.zeros(max(nc.value, 1), np.int32)
+        self._check(lib().cicy_get_labels(self._h, C.byref(nc), C.byref(nl), _p(lab, C.c_int32)), "get_labels")
+        return lab[: nc.value], nl.value
+
+    def junctions(self):
+        n = C.c_int64()
+        self._check(lib().cicy_get_junctions(self._h, C.byref(n), None, None, None, None, None), "get_junctions")
+        N = max(n.value, 1)
+        p1, p2 = np.zeros(N, np.int64), np.zeros(N, np.int64)
+        n1, n2 = np.zeros(N, np.int32), np.zeros(N, np.int32)
+        d = np.zeros(N, np.float64)
+        self._check(lib().cicy_get_junctions(self._h, C.byref(n), _p(p1, C.c_int64), _p(n1, C.c_int32), _p(p2, C.c_int64),
+                                             _p(n2, C.c_int32), _p(d, C.c_double)), "get_junctions")
+        k = n.value
+        return p1[:k], n1[:k], p2[:k], n2[:k], d[:k]
+
+    def elements(self, which: int = 0):
+        nc, ni = C.c_int64(), C.c_int64()
+        self._check(lib().cicy_get_elements(self._h, which, C.byref(nc), C.byref(ni), None, None), "get_elements")
+        ptr = np.zeros(nc.value + 1, np.int64)
+        idx = np.zeros(max(ni.value, 1), np.int64)
+        self._check(lib().cicy_get_elements(self._h, which, C.byref(nc), C.byref(ni), _p(ptr, C.c_int64), _p(idx, C.c_int64)),
+                    "get_elements")
+        return ptr, idx[: ni.value]
+
+    def percolated_clusters(self, which: int = 0):
+        k, ni, nj = C.c_int32(), C.c_int64(), C.c_int64()
+        self._check(lib().cicy_get_clusters(self._h, which, C.byref(k), C.byref(ni), None, None, None, C.byref(nj), None, None),
+                    "get_clusters")
+        K = k.value
+        ptr, jptr = np.zeros(K + 1, np.int64), np.zeros(K + 1, np.int64)
+        idx, jidx = np.zeros(max(ni.value, 1), np.int32), np.zeros(max(nj.value, 1), np.int32)
+        fam = np.zeros(max(K, 1), np.int32)
+        self._check(lib().cicy_get_clusters(self._h, which, C.byref(k), C.byref(ni), _p(ptr, C.c_int64), _p(idx, C.c_int32),
+                                            _p(fam, C.c_int32), C.byref(nj), _p(jptr, C.c_int64), _p(jidx, C.c_int32)),
+                    "get_clusters")
+        return {"ptr": ptr, "idx": idx[: ni.value], "family": fam[:K], "junc_ptr": jptr, "junc_idx": jidx[: nj.value]}
+
+    def system(self, solve: int) -> dict:
+        nodes, res, m = C.c_int64(), C.c_int64(), C.c_int64()
+        self._check(lib().cicy_get_system(self._h, solve, C.byref(nodes), C.byref(res), C.byref(m), None, None, None, None, None,
+                                          None, None), "get_system")
+        n = nodes.value - res.value
+        rp = np.zeros(n + 1, np.int64)
+        ci = np.zeros(max(m.value, 1), np.int64)
+        val = np.zeros(max(m.value, 1), np.float64)
+        diag, b, x0 = np.zeros(max(n, 1)), np.zeros(max(n, 1)), np.zeros(max(n, 1))
+        volt = np.zeros(max(nodes.value, 1))
+        self._check(lib().cicy_get_system(self._h, solve, C.byref(nodes), C.byref(res), C.byref(m), _p(rp, C.c_int64),
+                                          _p(ci, C.c_int64), _p(val, C.c_double), _p(diag, C.c_double), _p(b, C.c_double),
+                                          _p(x0, C.c_double), _p(volt, C.c_double)), "get_system")
+        return {"nodes": nodes.value, "reserved": res.value, "row_ptr": rp, "col_ind": ci[: m.value], "values": val[: m.value],
+                "diag": diag[:n], "b": b[:n], "x0": x0[:n], "voltages": volt[: nodes.value]}
+
+
+def result_dict(r: _abi.Result) -> dict:
+    return {
+        "resistances": list(r.resistances),
+        "resistivities": list(r.resistivities),
+        "n_slots": r.n_slots,
+        "n_point_contacts": r.n_point_contacts,
+        "n_labels": r.n_labels,
+        "n_junctions": r.n_junctions,
+        "n_percolated": r.n_percolated,
+        "solves": [
+            {"cluster": s.cluster, "pass": s.pass_, "nodes": s.nodes, "reserved": s.reserved, "nnz_lower": s.nnz_lower,
+             "iterations": s.iterations, "rel_residual": s.rel_residual, "seconds": s.seconds}
+            for s in r.solves[: r.n_solves]
+        ],
+        "stage_seconds": list(r.stage_seconds),
+    }
