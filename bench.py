@@ -34,7 +34,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-SIDE, N_CNTS, TOL = 6.0, 25000, 1e-8
+SIDE, N_CNTS, TOL, TOL_UNIT = 6.0, 25000, 1e-8, 1e-10
 METRIC = "networks solved/s at 1e-8 residual (25k-CNT 6um network, full hot path)"
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "ref_dump")
 
@@ -60,7 +60,7 @@ def dist_env():
 def workload(rank: int):
     from cicy_geom_b200.network import NetworkConfig, generate_cnt_network
 
-    cfg = NetworkConfig(side=SIDE, n_cnts=N_CNTS, seed=2_000_000 + rank, tolerance=TOL)
+    cfg = NetworkConfig(side=SIDE, n_cnts=N_CNTS, seed=2_000_000 + rank, tolerance=TOL, tolerance_unit=TOL_UNIT)
     raw = generate_cnt_network(cfg)
     return cfg, raw, raw.extract_window(cfg)
 

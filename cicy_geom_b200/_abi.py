@@ -53,6 +53,7 @@ class Params(C.Structure):
         ("junction_resistance", C.c_double),
         ("C1", C.c_double),
         ("C2", C.c_double),
+        ("tolerance_unit", C.c_double),
     ]
 
 

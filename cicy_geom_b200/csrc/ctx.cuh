@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "dev_common.cuh"
+#include "solver.cuh"
 
 namespace cicy {
 
@@ -21,6 +22,7 @@ struct GridGeom {
 struct DeaSystem {
     int cluster = -1, pass = -2;  // pass -1: unit resistors; 0,1,2: real, along x,y,z
     int64_t nodes = 0, reserved = 0, nnz_lower = 0, iterations = 0;
+    int restarts = 0;
     double rel_residual = 0, seconds = 0;
     // device: strict-lower CSR of the free block (SSS), diagonal, rhs, x0, voltages (all nodes)
     DBuf<int32_t> row_ptr, col;
@@ -107,6 +109,8 @@ struct Ctx {
     DBuf<int32_t> eb, ee, alive, alive_scan, tmp_list;
     DBuf<unsigned long long> imax;
     std::vector<int32_t> bb_clu_len, bb_cj_len;
+    DBuf<int32_t> chain_start, chain_len;
+    SolverWork sw;
 
     ~Ctx();
 };
@@ -116,6 +120,10 @@ void upload_network(Ctx& c, const cicy_network& net);
 void run_contact_grid(Ctx& c, const cicy_params& p);
 void run_clusters(Ctx& c, const cicy_params& p);
 void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out);
+
+// Learned preconditioner scalings for the system being solved (learned.cu).
+void learned_scalings(Ctx& c, const cicy_params& p, const SolverSystem& ss, int n_chains, int r_flag, const float** node_scale,
+                      const float** edge_scale);
 
 // Helpers shared across translation units.
 int32_t read_i32(Ctx& c, const int32_t* dptr);

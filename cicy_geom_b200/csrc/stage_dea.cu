@@ -7,6 +7,7 @@
 #include <cooperative_groups.h>
 
 #include "ctx.cuh"
+#include "solver.cuh"
 
 namespace cicy {
 
@@ -349,34 +350,7 @@ __global__ void k_spmv_residual(int n, const int32_t* __restrict__ rp, const int
     }
 }
 
-// ---------------------------------------------------------------------------
-// Persistent Jacobi-PCG (FP64).  Same recurrence as Solve_DEA_equations_CG_SSS
-// (Direct_Electrifying.cpp:1538-1659) with q = A p carried by recurrence
-// (q = A z + beta q) so each iteration needs two grid barriers:
-//   B: x += a p, r -= a q, z = M^-1 r, partials (r.r, r.z)   | barrier
-//   A: w = A z, q = w + b q, p = z + b p, partial (p.q)      | barrier
-// Stop when |r| <= tol |r0| (r0 after the initial guess), or after max_iter.
-struct CgArgs {
-    int n;
-    const int32_t* rp;
-    const int32_t* ci;
-    const double* val;
-    const double* minv;
-    double* x;
-    double* r;
-    double* z;
-    double* p;
-    double* q;
-    double* partA;  // 2 doubles per block
-    double* partB;  // 1 double per block
-    double* scal;   // [0] rr final, [1] iterations as double, [2] r0 norm
-    long long* iters;
-    GridBarrier bar;
-    int* err;
-    double tol;
-    long long max_iter;
-};
-
+// block_reduce2 for the residual report
 __device__ __forceinline__ void block_reduce2(double a, double b, double* sm, double& ra, double& rb) {
     a = warp_sum(a);
     b = warp_sum(b);
@@ -394,101 +368,6 @@ __device__ __forceinline__ void block_reduce2(double a, double b, double* sm, do
     ra = sm[64];
     rb = sm[65];
     __syncthreads();
-}
-
-// Every block sums the per-block partials in the same fixed order.
-__device__ __forceinline__ void sum_partials(const double* part, int stride, int nb, double* sm, double& s0, double& s1) {
-    double a = 0, b = 0;
-    if (threadIdx.x < 32) {
-        for (int i = threadIdx.x; i < nb; i += 32) {
-            a += ((volatile double*)part)[i * stride];
-            if (stride > 1) b += ((volatile double*)part)[i * stride + 1];
-        }
-        a = warp_sum(a);
-        b = warp_sum(b);
-        if (threadIdx.x == 0) { sm[66] = a; sm[67] = b; }
-    }
-    __syncthreads();
-    s0 = sm[66];
-    s1 = sm[67];
-    __syncthreads();
-}
-
-__global__ void __launch_bounds__(256) k_cg_fp64(CgArgs a) {
-    __shared__ double sm[72];
-    const int nb = gridDim.x;
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = nb * blockDim.x;
-    // z0 = M^-1 r0, p = z0, q = A p, partials: r.r, r.z
-    double rr_l = 0, rz_l = 0;
-    for (int i = tid; i < a.n; i += nth) {
-        double zi = a.minv[i] * a.r[i];
-        a.z[i] = zi;
-        a.p[i] = zi;
-        rr_l += a.r[i] * a.r[i];
-        rz_l += a.r[i] * zi;
-    }
-    double s0, s1;
-    block_reduce2(rr_l, rz_l, sm, s0, s1);
-    if (threadIdx.x == 0) { a.partA[2 * blockIdx.x] = s0; a.partA[2 * blockIdx.x + 1] = s1; }
-    if (!grid_sync(a.bar, nb, a.err)) return;
-    double rr, rz;
-    sum_partials(a.partA, 2, nb, sm, rr, rz);
-    const double R0 = a.tol * sqrt(rr);
-    double pq_l = 0;
-    for (int i = tid; i < a.n; i += nth) {
-        double w = 0;
-        for (int k = a.rp[i]; k < a.rp[i + 1]; k++) w += a.val[k] * a.p[a.ci[k]];
-        a.q[i] = w;
-        pq_l += a.p[i] * w;
-    }
-    block_reduce2(pq_l, 0.0, sm, s0, s1);
-    if (threadIdx.x == 0) a.partB[blockIdx.x] = s0;
-    if (!grid_sync(a.bar, nb, a.err)) return;
-    double pq, dummy;
-    sum_partials(a.partB, 1, nb, sm, pq, dummy);
-    long long k = 1;
-    double rr_new = rr;
-    for (; k <= a.max_iter; k++) {
-        const double alpha = rz / pq;
-        rr_l = 0;
-        rz_l = 0;
-        for (int i = tid; i < a.n; i += nth) {
-            a.x[i] += alpha * a.p[i];
-            double ri = a.r[i] - alpha * a.q[i];
-            a.r[i] = ri;
-            double zi = a.minv[i] * ri;
-            a.z[i] = zi;
-            rr_l += ri * ri;
-            rz_l += ri * zi;
-        }
-        block_reduce2(rr_l, rz_l, sm, s0, s1);
-        if (threadIdx.x == 0) { a.partA[2 * blockIdx.x] = s0; a.partA[2 * blockIdx.x + 1] = s1; }
-        if (!grid_sync(a.bar, nb, a.err)) return;
-        double rz_new;
-        sum_partials(a.partA, 2, nb, sm, rr_new, rz_new);
-        if (sqrt(rr_new) <= R0) break;
-        const double beta = rz_new / rz;
-        rz = rz_new;
-        pq_l = 0;
-        for (int i = tid; i < a.n; i += nth) {
-            double w = 0;
-            for (int kk = a.rp[i]; kk < a.rp[i + 1]; kk++) w += a.val[kk] * a.z[a.ci[kk]];
-            double qi = w + beta * a.q[i];
-            double pi = a.z[i] + beta * a.p[i];
-            a.q[i] = qi;
-            a.p[i] = pi;
-            pq_l += pi * qi;
-        }
-        block_reduce2(pq_l, 0.0, sm, s0, s1);
-        if (threadIdx.x == 0) a.partB[blockIdx.x] = s0;
-        if (!grid_sync(a.bar, nb, a.err)) return;
-        sum_partials(a.partB, 1, nb, sm, pq, dummy);
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        *a.iters = k > a.max_iter ? a.max_iter : k;
-        a.scal[0] = rr_new;
-        a.scal[2] = R0;
-    }
 }
 
 __global__ void k_true_residual(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const double* __restrict__ v,
@@ -687,6 +566,11 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
         k_node_assign<<<grid_for(NM), 256, 0, s>>>(NM, reserved, eb.get(), ee.get(), c.elem_idx.get(), c.cnt_node_base.get(), c.lmm.get());
         c.launches += 2;
         const int nodes = reserved + read_i32(c, c.i32_scalar.get());
+        // free nodes of each CNT are one consecutive range: the chains of the block preconditioner
+        c.chain_start.ensure(NM + 1);
+        c.chain_len.ensure(NM + 1);
+        CICY_CUDA(cudaMemcpyAsync(c.chain_start.get(), c.cnt_node_base.get(), sizeof(int32_t) * NM, cudaMemcpyDeviceToDevice, s));
+        CICY_CUDA(cudaMemcpyAsync(c.chain_len.get(), c.cnt_nodes.get(), sizeof(int32_t) * NM, cudaMemcpyDeviceToDevice, s));
         const int n = nodes - reserved;
         sys->nodes = nodes;
         // ---- edges ----
@@ -784,42 +668,36 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
             c.launches++;
         }
         // ---- CG ----
-        cudaEvent_t e0, e1;
-        CICY_CUDA(cudaEventCreate(&e0));
-        CICY_CUDA(cudaEventCreate(&e1));
-        CICY_CUDA(cudaEventRecord(e0, s));
-        if (n > 0) {
-            int occ = 0;
-            CICY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cg_fp64, 256, 0));
-            int nb = std::min(std::max(1, occ) * c.num_sms, std::max(1, ceil_div(n, 256)));
-            c.cg_part.ensure(4 * nb + 8);
-            c.barrier.ensure(2);
-            c.cg_scal.ensure(4);
-            c.cg_iters.ensure(1);
-            CICY_CUDA(cudaMemsetAsync(c.barrier.get(), 0, sizeof(unsigned) * 2, s));
-            CgArgs a;
-            a.n = n; a.rp = c.cg_rp.get(); a.ci = c.cg_ci.get(); a.val = c.cg_val.get(); a.minv = c.cg_minv.get();
-            a.x = c.cg_x.get(); a.r = c.cg_r.get(); a.z = c.cg_z.get(); a.p = c.cg_p.get(); a.q = c.cg_q.get();
-            a.partA = c.cg_part.get(); a.partB = c.cg_part.get() + 2 * nb; a.scal = c.cg_scal.get(); a.iters = c.cg_iters.get();
-            a.bar = GridBarrier{c.barrier.get(), c.barrier.get() + 1};
-            a.err = c.status.get();
-            a.tol = p.tolerance;
-            a.max_iter = (long long)c.solver.max_iter_factor * nodes;
-            void* args[] = {&a};
-            CICY_CUDA(cudaLaunchCooperativeKernel((void*)k_cg_fp64, dim3(nb), dim3(256), args, 0, s));
-            c.launches++;
+        SolverSystem ss;
+        ss.n = n;
+        ss.nnz = NF;
+        ss.rp = c.cg_rp.get();
+        ss.ci = c.cg_ci.get();
+        ss.val = c.cg_val.get();
+        ss.diag = sys->diag.get();
+        ss.b = sys->b.get();
+        ss.x = c.cg_x.get();
+        const bool mixed = c.solver.precision == CICY_PRECISION_MIXED;
+        int kind = PRECOND_KIND_JACOBI;
+        if (c.solver.preconditioner != CICY_PRECOND_JACOBI && n > 0) {
+            kind = PRECOND_KIND_BLOCK;
+            const float* ns = nullptr;
+            const float* es = nullptr;
+            if (c.solver.preconditioner == CICY_PRECOND_LEARNED) learned_scalings(c, p, ss, NM, r_flag, &ns, &es);
+            build_block_preconditioner(c.sw, ss, NM, c.chain_start.get(), c.chain_len.get(), ns, es, mixed, s, c.launches);
         }
-        CICY_CUDA(cudaEventRecord(e1, s));
+        PcgStats st;
+        const double tol = (r_flag == 0 && p.tolerance_unit > 0) ? p.tolerance_unit : p.tolerance;
+        pcg_solve(c.sw, ss, kind, mixed, tol, (long long)c.solver.max_iter_factor * nodes, c.num_sms, c.status.get(), s,
+                  c.launches, st);
         check_status(c, "Solve_DEA_equations_CG_SSS");
-        sys->seconds = seconds_between(e0, e1);
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        long long iters = 0;
-        if (n > 0) CICY_CUDA(cudaMemcpy(&iters, c.cg_iters.get(), sizeof(long long), cudaMemcpyDeviceToHost));
-        sys->iterations = iters;
+        sys->seconds = st.seconds;
+        sys->iterations = st.iterations;
+        sys->restarts = st.restarts;
         // true FP64 residual |b - A x| / |b|
         double rb[2] = {0, 0};
         if (n > 0) {
+            c.cg_scal.ensure(4);
             CICY_CUDA(cudaMemsetAsync(c.cg_scal.get(), 0, sizeof(double) * 2, s));
             k_true_residual<<<grid_for(n), 256, 0, s>>>(n, c.cg_rp.get(), c.cg_ci.get(), c.cg_val.get(), c.cg_x.get(), sys->b.get(), c.cg_scal.get());
             c.launches++;

@@ -38,6 +38,7 @@ class NetworkConfig:
     min_points: int = 5          # junction compression (Cutoff_dist::min_points)
     cnt_min_points: int = 5      # shortest CNT segment kept by the window trimming (Nanotube_Geo::min_points)
     tolerance: float = 1e-10
+    tolerance_unit: float = 0.0  # unit-resistor (backbone) pass; 0: same as `tolerance`
     applied_voltage: float = 1.0
     resistivity_cnt: float = 1e-3
     resistivity_matrix: float = 1.03e20
@@ -81,6 +82,7 @@ class NetworkConfig:
         p.resistivity_matrix = self.resistivity_matrix
         p.junction_resistance = self.junction_resistance
         p.C1, p.C2 = self.c1_c2()
+        p.tolerance_unit = self.tolerance_unit
         return p
 
     def window_params(self) -> _abi.WindowParams:

@@ -70,6 +70,10 @@ typedef struct {
     double resistivity_matrix;  /* Electric_para::resistivity_matrix */
     double junction_resistance; /* Electric_para::junction_resistance ("constant") */
     double C1, C2;              /* Electric_para::C1, C2 ("exponential", Input_Reader.cpp:1450-1456) */
+    double tolerance_unit;      /* CG tolerance of the unit-resistor (backbone) pass; 0: `tolerance`.
+                                   No upstream counterpart: upstream uses one tolerance for both passes,
+                                   but the backbone's 1e-9 I_max current threshold (Backbone_Network.cpp:227)
+                                   needs the unit pass solved tighter than a loose real-pass tolerance. */
 } cicy_params;
 
 /* A window-trimmed CNT network: exactly the inputs that
@@ -106,7 +110,8 @@ typedef enum {
 
 typedef enum {
     CICY_PRECOND_JACOBI = 0,  /* M^-1 = 1/diag (Direct_Electrifying.cpp:1662-1668) */
-    CICY_PRECOND_LEARNED = 1  /* learned scalings, Jacobi fallback when they fail to reduce the residual */
+    CICY_PRECOND_LEARNED = 1, /* learned scalings of the chain blocks, chain blocks when they fail to reduce the residual */
+    CICY_PRECOND_CHAIN = 2    /* block-Jacobi over CNT element chains (tridiagonal blocks, explicit inverses) */
 } cicy_preconditioner;
 
 typedef struct {
