@@ -79,7 +79,7 @@ class Network(C.Structure):
 
 
 class SolverOpts(C.Structure):
-    _fields_ = [("precision", C.c_int32), ("preconditioner", C.c_int32), ("max_iter_factor", C.c_int32), ("reserved0", C.c_int32)]
+    _fields_ = [("precision", C.c_int32), ("preconditioner", C.c_int32), ("max_iter_factor", C.c_int32), ("flags", C.c_int32)]
 
 
 class SolveInfo(C.Structure):

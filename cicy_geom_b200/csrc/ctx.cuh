@@ -23,6 +23,7 @@ struct DeaSystem {
     int cluster = -1, pass = -2;  // pass -1: unit resistors; 0,1,2: real, along x,y,z
     int64_t nodes = 0, reserved = 0, nnz_lower = 0, iterations = 0;
     int restarts = 0;
+    bool cluster_solver = false;
     double rel_residual = 0, seconds = 0;
     // device: strict-lower CSR of the free block (SSS), diagonal, rhs, x0, voltages (all nodes)
     DBuf<int32_t> row_ptr, col;

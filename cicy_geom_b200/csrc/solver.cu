@@ -503,3 +503,20 @@ __global__ void k_fill_ones(int n, int32_t* __restrict__ a) {
 }
 
 }  // namespace cicy
+
+namespace cicy {
+
+// Host wrappers shared with the cluster solver (solver_cluster.cu).
+void launch_block_marks(int nchains, const int32_t* chain_start, const int32_t* chain_len, int32_t* is_start, cudaStream_t s) {
+    if (nchains > 0) k_block_marks<<<grid_for(nchains), 256, 0, s>>>(nchains, chain_start, chain_len, is_start);
+}
+
+void launch_block_fill(int n, const int32_t* is_start, const int32_t* start_scan, int32_t* blk_row, cudaStream_t s) {
+    k_block_fill<<<grid_for(n), 256, 0, s>>>(n, is_start, start_scan, blk_row);
+}
+
+void launch_cta_rows(int nb_cta, int n, const int32_t* is_start, int32_t* cta_row, cudaStream_t s) {
+    k_cta_rows<<<1, 256, 0, s>>>(nb_cta, n, is_start, cta_row);
+}
+
+}  // namespace cicy

@@ -6,6 +6,8 @@
 namespace cicy {
 
 constexpr int kBlockMax = 32;  // largest block of the chain block-Jacobi preconditioner
+constexpr int kClusterCtas = 16;                // CTAs of the cluster-resident solver (non-portable cluster size)
+constexpr int kClusterSmemMax = 232448 - 1024;  // dynamic shared memory per CTA it may use
 enum PrecondKind : int { PRECOND_KIND_JACOBI = 0, PRECOND_KIND_BLOCK = 1 };
 
 // A free-node system in full symmetric CSR (diagonal included).
@@ -51,13 +53,14 @@ struct PcgStats {
     long long iterations = 0;
     int restarts = 0;
     int ctas = 0;
+    bool cluster = false;
     double seconds = 0;
 };
 
 struct SolverWork {
-    DBuf<double> r, z, p, q, minv, tinv, part, stats;
+    DBuf<double> r, z, p, q, minv, tinv, part, stats, lfac, ipiv;
     DBuf<float> z32, p32, q32, val32, minv32, tinv32;
-    DBuf<int32_t> is_start, start_scan, blk_row, blk_msq, blk_off, row_off, row_base, row_m, cta_row, total, scan_tmp;
+    DBuf<int32_t> is_start, start_scan, blk_row, blk_msq, blk_off, row_off, row_base, row_m, cta_row, total, scan_tmp, cta_stats;
     DBuf<unsigned int> barrier;
     int n_blocks = 0, block_entries = 0;
 };
@@ -71,6 +74,16 @@ __global__ void k_fill_ones(int n, int32_t* __restrict__ a);
 void build_block_preconditioner(SolverWork& w, const SolverSystem& sys, int nchains, const int32_t* chain_start,
                                 const int32_t* chain_len, const float* node_scale, const float* edge_scale, bool mixed,
                                 cudaStream_t s, int64_t& launches);
+
+void launch_block_marks(int nchains, const int32_t* chain_start, const int32_t* chain_len, int32_t* is_start, cudaStream_t s);
+void launch_block_fill(int n, const int32_t* is_start, const int32_t* start_scan, int32_t* blk_row, cudaStream_t s);
+void launch_cta_rows(int nb_cta, int n, const int32_t* is_start, int32_t* cta_row, cudaStream_t s);
+
+// Cluster-resident PCG (solver_cluster.cu).  Returns false, without touching x,
+// when the system does not fit one cluster's shared memory.
+bool pcg_solve_cluster(SolverWork& w, const SolverSystem& sys, bool block_precond, const float* node_scale,
+                       const float* edge_scale, int nchains, const int32_t* chain_start, const int32_t* chain_len, double tol,
+                       long long max_iter, cudaStream_t s, int64_t& launches, PcgStats& st);
 
 void pcg_solve(SolverWork& w, const SolverSystem& sys, int precond, bool mixed, double tol, long long max_iter, int num_sms,
                int* status, cudaStream_t s, int64_t& launches, PcgStats& st);

@@ -679,18 +679,28 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
         ss.x = c.cg_x.get();
         const bool mixed = c.solver.precision == CICY_PRECISION_MIXED;
         int kind = PRECOND_KIND_JACOBI;
+        const float* ns = nullptr;
+        const float* es = nullptr;
         if (c.solver.preconditioner != CICY_PRECOND_JACOBI && n > 0) {
             kind = PRECOND_KIND_BLOCK;
-            const float* ns = nullptr;
-            const float* es = nullptr;
             if (c.solver.preconditioner == CICY_PRECOND_LEARNED) learned_scalings(c, p, ss, NM, r_flag, &ns, &es);
-            build_block_preconditioner(c.sw, ss, NM, c.chain_start.get(), c.chain_len.get(), ns, es, mixed, s, c.launches);
         }
         PcgStats st;
         const double tol = (r_flag == 0 && p.tolerance_unit > 0) ? p.tolerance_unit : p.tolerance;
-        pcg_solve(c.sw, ss, kind, mixed, tol, (long long)c.solver.max_iter_factor * nodes, c.num_sms, c.status.get(), s,
-                  c.launches, st);
+        const long long max_iter = (long long)c.solver.max_iter_factor * nodes;
+        // small and medium systems: one cluster with everything in shared memory;
+        // otherwise (or when disabled) the grid-wide persistent kernel
+        bool solved = false;
+        if (!mixed && !(c.solver.flags & CICY_SOLVER_NO_CLUSTER))
+            solved = pcg_solve_cluster(c.sw, ss, kind == PRECOND_KIND_BLOCK, ns, es, NM, c.chain_start.get(), c.chain_len.get(), tol,
+                                       max_iter, s, c.launches, st);
+        if (!solved) {
+            if (kind == PRECOND_KIND_BLOCK)
+                build_block_preconditioner(c.sw, ss, NM, c.chain_start.get(), c.chain_len.get(), ns, es, mixed, s, c.launches);
+            pcg_solve(c.sw, ss, kind, mixed, tol, max_iter, c.num_sms, c.status.get(), s, c.launches, st);
+        }
         check_status(c, "Solve_DEA_equations_CG_SSS");
+        sys->cluster_solver = st.cluster;
         sys->seconds = st.seconds;
         sys->iterations = st.iterations;
         sys->restarts = st.restarts;

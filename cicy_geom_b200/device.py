@@ -65,8 +65,10 @@ class Context:
     def stream(self) -> int:
         return lib().cicy_ctx_stream(self._h) or 0
 
-    def set_solver(self, precision: int = 0, preconditioner: int = 0, max_iter_factor: int = 300):
-        o = _abi.SolverOpts(precision, preconditioner, max_iter_factor, 0)
+    def set_solver(self, precision: int = 0, preconditioner: int = 0, max_iter_factor: int = 300, cluster: bool = True):
+        """precision: 0 FP64, 1 mixed; preconditioner: 0 Jacobi (upstream), 1 learned, 2 chain blocks;
+        cluster: allow the cluster-resident solver for systems that fit in shared memory."""
+        o = _abi.SolverOpts(precision, preconditioner, max_iter_factor, 0 if cluster else 1)
         self._check(lib().cicy_ctx_set_solver(self._h, C.byref(o)), "cicy_ctx_set_solver")
 
     def kernel_launches(self) -> int:

@@ -118,8 +118,10 @@ typedef struct {
     int32_t precision;        /* cicy_precision */
     int32_t preconditioner;   /* cicy_preconditioner */
     int32_t max_iter_factor;  /* max iterations = factor * nodes (upstream 300, Direct_Electrifying.cpp:1559) */
-    int32_t reserved0;
+    int32_t flags;            /* bit 0: never use the cluster-resident solver (grid-wide persistent kernel only) */
 } cicy_solver_opts;
+
+#define CICY_SOLVER_NO_CLUSTER 1
 
 /* One DEA linear solve (unit-resistor or real-resistor pass) of one cluster. */
 typedef struct {
