@@ -174,6 +174,8 @@ def lib() -> C.CDLL:
         "cicy_host_network_view": (C.c_int, [C.c_void_p, P(Network)]),
         "cicy_host_network_free": (None, [C.c_void_p]),
         "cicy_host_last_error": (C.c_char_p, []),
+        "cicy_jacobi_pcg_static": (C.c_int, [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_double, C.c_int64, C.c_void_p, i64p, f64p]),
     }
     for name, (res, args) in sig.items():
         if not hasattr(L, name):  # completeness is asserted by tests/test_abi.py

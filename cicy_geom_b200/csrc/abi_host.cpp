@@ -7,6 +7,10 @@ namespace {
 thread_local std::string g_host_error;
 }
 
+namespace cicy {
+void set_host_error(const std::string& msg) { g_host_error = msg; }
+}  // namespace cicy
+
 extern "C" {
 
 cicy_status cicy_generate_cnt_network(const cicy_gen_params* g, cicy_host_network** out) {

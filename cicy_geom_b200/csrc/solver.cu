@@ -520,3 +520,16 @@ void launch_cta_rows(int nb_cta, int n, const int32_t* is_start, int32_t* cta_ro
 }
 
 }  // namespace cicy
+
+namespace cicy {
+
+// Exported launchers of the FP64 Jacobi kernels for the allocation-free entry point (noalloc.cu).
+void launch_jacobi_fp64(int n, const double* diag, double* minv, cudaStream_t s) {
+    k_jacobi<<<grid_for(n), 256, 0, s>>>(n, diag, minv, nullptr);
+}
+
+int max_coop_blocks_jacobi_fp64(int num_sms) { return max_coop_blocks<PRECOND_KIND_JACOBI, false>(num_sms); }
+
+void launch_pcg_jacobi_fp64(PcgArgs& a, int nb, cudaStream_t s) { launch_pcg<PRECOND_KIND_JACOBI, false>(a, nb, s); }
+
+}  // namespace cicy

@@ -78,6 +78,9 @@ void build_block_preconditioner(SolverWork& w, const SolverSystem& sys, int ncha
 void launch_block_marks(int nchains, const int32_t* chain_start, const int32_t* chain_len, int32_t* is_start, cudaStream_t s);
 void launch_block_fill(int n, const int32_t* is_start, const int32_t* start_scan, int32_t* blk_row, cudaStream_t s);
 void launch_cta_rows(int nb_cta, int n, const int32_t* is_start, int32_t* cta_row, cudaStream_t s);
+void launch_jacobi_fp64(int n, const double* diag, double* minv, cudaStream_t s);
+int max_coop_blocks_jacobi_fp64(int num_sms);
+void launch_pcg_jacobi_fp64(PcgArgs& a, int nb, cudaStream_t s);
 
 // Cluster-resident PCG (solver_cluster.cu).  Returns false, without touching x,
 // when the system does not fit one cluster's shared memory.

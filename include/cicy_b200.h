@@ -244,6 +244,28 @@ void cicy_host_network_free(cicy_host_network* h);
 /* Message of the last failing host-side call on this thread. */
 const char* cicy_host_last_error(void);
 
+/* ---------------- allocation-free solve ----------------
+ * No counterpart in the reference.  FP64 Jacobi-PCG (the algorithm of
+ * Solve_DEA_equations_CG_SSS) on a system the caller already holds in device
+ * memory as full symmetric CSR (row_ptr[n+1], col_ind/values[nnz], diagonal
+ * included), right-hand side b[n] and solution x[n] (in: initial guess, out:
+ * solution), that allocates no device memory: for callers that may not let
+ * cudaMalloc/cudaFree synchronize the device or take the allocator's lock
+ * mid-loop, or whose host owns all device memory.  All scratch lives in one
+ * fixed static device array of about 5.3 MB that every GPU loading the library
+ * holds until exit; systems above 131072 rows are rejected with
+ * CICY_E_CAPACITY.  Runs on the current device and `stream` (a cudaStream_t, or
+ * NULL); returns once the solve is complete.  The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress), so make that first call
+ * before any stream capture.  Every call shares the one array and the call
+ * resets the words that must start at zero, so calls that overlap on the GPU
+ * (other streams, other host threads) race: serialize them.  Stops when
+ * |r| <= tol |r0|; `rel_residual` gets |r| / |r0|.  Errors: message via
+ * cicy_host_last_error(). */
+cicy_status cicy_jacobi_pcg_static(int32_t n, int32_t nnz, const int32_t* row_ptr, const int32_t* col_ind, const double* values,
+                                   const double* b, double* x, double tol, int64_t max_iter, void* stream, int64_t* iterations,
+                                   double* rel_residual);
+
 #ifdef __cplusplus
 }
 #endif
