@@ -92,6 +92,8 @@ class SolveInfo(C.Structure):
         ("iterations", C.c_int64),
         ("rel_residual", C.c_double),
         ("seconds", C.c_double),
+        ("kernel", C.c_int32),
+        ("restarts", C.c_int32),
     ]
 
 

@@ -61,6 +61,9 @@ struct SolverWork {
     DBuf<double> r, z, p, q, minv, tinv, part, stats, lfac, ipiv;
     DBuf<float> z32, p32, q32, val32, minv32, tinv32;
     DBuf<int32_t> is_start, start_scan, blk_row, blk_msq, blk_off, row_off, row_base, row_m, cta_row, total, scan_tmp, cta_stats;
+    DBuf<int32_t> halo_mark, halo_scan, halo_ptr, send_cnt, send_ptr;
+    DBuf<unsigned long long> send;
+    DBuf<uint16_t> code;
     DBuf<unsigned int> barrier;
     int n_blocks = 0, block_entries = 0;
 };

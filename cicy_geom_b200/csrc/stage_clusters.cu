@@ -4,6 +4,7 @@
 #include <cmath>
 
 #include "ctx.cuh"
+#include "trace.cuh"
 
 namespace cicy {
 

@@ -8,6 +8,7 @@
 
 #include "ctx.cuh"
 #include "solver.cuh"
+#include "trace.cuh"
 
 namespace cicy {
 
@@ -548,6 +549,7 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
         k_cluster_ranges<<<grid_for(NM), 256, 0, s>>>(NM, in.members, c.bb_lo.get(), c.bb_hi.get(), eb.get(), ee.get(), c.status.get());
         c.launches++;
         check_status(c, "LM_matrix_for_cnts");
+        TraceSeq tr(s);
         // ---- LMM ----
         c.lmm.ensure(std::max(c.n_points, 1));
         CICY_CUDA(cudaMemsetAsync(c.lmm.get(), 0xff, sizeof(int32_t) * std::max(c.n_points, 1), s));
@@ -573,6 +575,7 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
         CICY_CUDA(cudaMemcpyAsync(c.chain_len.get(), c.cnt_nodes.get(), sizeof(int32_t) * NM, cudaMemcpyDeviceToDevice, s));
         const int n = nodes - reserved;
         sys->nodes = nodes;
+        tr.mark(r_flag ? "dea.real.lmm" : "dea.unit.lmm");
         // ---- edges ----
         k_cnt_edge_counts<<<grid_for(NM), 256, 0, s>>>(NM, eb.get(), ee.get(), c.elem_idx.get(), c.lmm.get(), c.cnt_nodes.get());
         exclusive_scan_i32(c.cnt_nodes.get(), c.cnt_node_base.get(), NM, c.i32_scalar.get(), c.scan_tmp32, s, c.launches);
@@ -591,6 +594,7 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
                                                                 c.e_n1.get(), c.e_n2.get(), c.e_op.get(), c.e_g.get());
             c.launches++;
         }
+        tr.mark(r_flag ? "dea.real.edges" : "dea.unit.edges");
         // ---- sort-and-reduce assembly ----
         const int bn = bits_for((uint64_t)std::max(nodes, 1));
         const int ND = 2 * NE;
@@ -638,6 +642,7 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
         k_diag_free<<<grid_for(n), 256, 0, s>>>(n, reserved, c.work_f64a.get(), sys->diag.get(), c.status.get());
         c.launches += 3;
         check_status(c, "Fill_sparse_stiffness_matrix");
+        tr.mark(r_flag ? "dea.real.assembly" : "dea.unit.assembly");
         // ---- full CSR for the CG ----
         const int NF = n + 2 * m;
         const int bnf = bits_for((uint64_t)std::max(n, 1));
@@ -651,6 +656,7 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
                                                c.cg_ci.get(), c.cg_val.get(), c.cg_minv.get());
         exclusive_scan_i32(c.cnt_nodes.get(), c.cg_rp.get(), n + 1, nullptr, c.scan_tmp32, s, c.launches);
         c.launches += 2;
+        tr.mark(r_flag ? "dea.real.full_csr" : "dea.unit.full_csr");
         // ---- initial guess and r0 ----
         c.cg_x.ensure(n + 1); c.cg_r.ensure(n + 1); c.cg_z.ensure(n + 1); c.cg_p.ensure(n + 1); c.cg_q.ensure(n + 1);
         CICY_CUDA(cudaMemsetAsync(sys->x0.get(), 0, sizeof(double) * std::max(n, 1), s));
@@ -667,6 +673,7 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
             CICY_CUDA(cudaMemcpyAsync(c.cg_x.get(), sys->x0.get(), sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
             c.launches++;
         }
+        tr.mark(r_flag ? "dea.real.guess" : "dea.unit.guess");
         // ---- CG ----
         SolverSystem ss;
         ss.n = n;
@@ -704,6 +711,7 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
         sys->seconds = st.seconds;
         sys->iterations = st.iterations;
         sys->restarts = st.restarts;
+        tr.mark(r_flag ? "dea.real.cg" : "dea.unit.cg");
         // true FP64 residual |b - A x| / |b|
         double rb[2] = {0, 0};
         if (n > 0) {
@@ -876,6 +884,8 @@ void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out) {
             si.iterations = sy->iterations;
             si.rel_residual = sy->rel_residual;
             si.seconds = sy->seconds;
+            si.kernel = sy->cluster_solver ? 1 : 0;
+            si.restarts = sy->restarts;
         }
         out->stage_seconds[2] = t_unit;
         out->stage_seconds[3] = t_bb;

@@ -184,7 +184,8 @@ def result_dict(r: _abi.Result) -> dict:
         "n_percolated": r.n_percolated,
         "solves": [
             {"cluster": s.cluster, "pass": s.pass_, "nodes": s.nodes, "reserved": s.reserved, "nnz_lower": s.nnz_lower,
-             "iterations": s.iterations, "rel_residual": s.rel_residual, "seconds": s.seconds}
+             "iterations": s.iterations, "rel_residual": s.rel_residual, "seconds": s.seconds, "kernel": s.kernel,
+             "restarts": s.restarts}
             for s in r.solves[: r.n_solves]
         ],
         "stage_seconds": list(r.stage_seconds),

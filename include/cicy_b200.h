@@ -133,6 +133,8 @@ typedef struct {
     int64_t iterations;       /* CG iterations */
     double rel_residual;      /* FP64 |b - A x| / |b| after the solve */
     double seconds;           /* device time of the solve (CUDA events) */
+    int32_t kernel;           /* 0: grid-wide persistent PCG, 1: cluster-resident PCG */
+    int32_t restarts;         /* FP64 true-residual restarts taken */
 } cicy_solve_info;
 
 typedef struct {
