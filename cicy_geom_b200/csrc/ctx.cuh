@@ -106,7 +106,8 @@ struct Ctx {
     // assembly / backbone scratch
     DBuf<uint64_t> dkey, stage_keys;
     DBuf<uint32_t> dval;
-    DBuf<double> runval, vef, cur_out;
+    DBuf<double> runval, vef, cur_out, bterm;
+    DBuf<int32_t> bvalid;
     DBuf<int32_t> eb, ee, alive, alive_scan, tmp_list;
     DBuf<unsigned long long> imax;
     std::vector<int32_t> bb_clu_len, bb_cj_len;

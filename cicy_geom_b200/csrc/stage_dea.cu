@@ -475,31 +475,47 @@ __global__ void k_compact_i32(int n, const int32_t* __restrict__ in, const int32
         if (flag[i]) out[scan[i]] = in[i];
 }
 
-// Currents_through_boundary_cnts / Current_of_element_in_boundary (Electrical_analysis.cpp:499-605),
-// summed sequentially in boundary order like upstream.
-__global__ void k_boundary_current(int b, int e, const int32_t* __restrict__ bcnt, const int32_t* __restrict__ cur_lo,
-                                   const int32_t* __restrict__ cur_hi, const int32_t* __restrict__ elem, const int32_t* __restrict__ lmm,
-                                   const double* __restrict__ volt, const double* __restrict__ radii, double rho,
-                                   const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
-                                   double* out) {
+// Currents_through_boundary_cnts / Current_of_element_in_boundary (Electrical_analysis.cpp:499-605).
+// The terms V/Re (two per boundary CNT) are independent: one thread each computes
+// them; k_boundary_sum then adds them in upstream boundary order, so the total is
+// the same sequence of FP64 additions as the upstream loop.
+__global__ void k_boundary_terms(int b, int e, const int32_t* __restrict__ bcnt, const int32_t* __restrict__ cur_lo,
+                                 const int32_t* __restrict__ cur_hi, const int32_t* __restrict__ elem, const int32_t* __restrict__ lmm,
+                                 const double* __restrict__ volt, const double* __restrict__ radii, double rho,
+                                 const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
+                                 double* __restrict__ term, int32_t* __restrict__ valid) {
+    const int m = 2 * (e - b);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
+        const int i = b + (t >> 1), side = t & 1;
+        int ok = 0;
+        double v = 0;
+        const int c = bcnt[i];
+        const int lo = cur_lo[c], hi = cur_hi[c];
+        if (lo >= 0 && hi >= lo) {
+            const int P1 = side == 0 ? elem[lo] : elem[hi];
+            const int P2 = side == 0 ? elem[lo + 1] : elem[hi - 1];
+            const int n1 = lmm[P1];
+            if (n1 >= 0 && n1 <= 1) {
+                const int n2 = lmm[P2];
+                if (n2 >= 0) {
+                    const double V = volt[n2] - volt[n1];
+                    const double Re = (P1 > P2) ? cnt_resistance(P2, P1, radii[c], rho, x, y, z)
+                                                : cnt_resistance(P1, P2, radii[c], rho, x, y, z);
+                    v = V / Re;
+                    ok = 1;
+                }
+            }
+        }
+        term[t] = v;
+        valid[t] = ok;
+    }
+}
+
+__global__ void k_boundary_sum(int m, const double* __restrict__ term, const int32_t* __restrict__ valid, double* out) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     double I = 0;
-    for (int i = b; i < e; i++) {
-        int c = bcnt[i];
-        int lo = cur_lo[c], hi = cur_hi[c];
-        if (lo < 0 || hi < lo) continue;
-        for (int side = 0; side < 2; side++) {
-            int P1 = side == 0 ? elem[lo] : elem[hi];
-            int P2 = side == 0 ? elem[lo + 1] : elem[hi - 1];
-            int n1 = lmm[P1];
-            if (n1 < 0 || n1 > 1) continue;
-            int n2 = lmm[P2];
-            if (n2 < 0) continue;
-            double V = volt[n2] - volt[n1];
-            double Re = (P1 > P2) ? cnt_resistance(P2, P1, radii[c], rho, x, y, z) : cnt_resistance(P1, P2, radii[c], rho, x, y, z);
-            I = I + V / Re;
-        }
-    }
+    for (int t = 0; t < m; t++)
+        if (valid[t]) I = I + term[t];
     *out = I;
 }
 
@@ -830,10 +846,15 @@ void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out) {
             const int b2 = d == 0 ? 4 : d == 1 ? 5 : 1;
             if (c.h_bcnt_ptr[b1 + 1] == c.h_bcnt_ptr[b1] || c.h_bcnt_ptr[b2 + 1] == c.h_bcnt_ptr[b2])
                 throw Fail{CICY_E_INPUT, "Calculate_parallel_resistor: one boundary vector along the direction is empty"};
-            k_boundary_current<<<1, 32, 0, s>>>(c.h_bcnt_ptr[b1], c.h_bcnt_ptr[b1 + 1], c.bcnt_idx.get(), c.bb_lo.get(), c.bb_hi.get(),
-                                                c.elem_idx.get(), c.lmm.get(), sr->volt.get(), c.radii.get(), p.resistivity_cnt, c.x.get(),
-                                                c.y.get(), c.z.get(), c.cur_out.get());
-            c.launches++;
+            const int nb = (int)(c.h_bcnt_ptr[b1 + 1] - c.h_bcnt_ptr[b1]);
+            c.bterm.ensure(2 * (size_t)nb);
+            c.bvalid.ensure(2 * (size_t)nb);
+            k_boundary_terms<<<grid_for(2 * nb), 128, 0, s>>>((int)c.h_bcnt_ptr[b1], (int)c.h_bcnt_ptr[b1 + 1], c.bcnt_idx.get(),
+                                                             c.bb_lo.get(), c.bb_hi.get(), c.elem_idx.get(), c.lmm.get(), sr->volt.get(),
+                                                             c.radii.get(), p.resistivity_cnt, c.x.get(), c.y.get(), c.z.get(),
+                                                             c.bterm.get(), c.bvalid.get());
+            k_boundary_sum<<<1, 32, 0, s>>>(2 * nb, c.bterm.get(), c.bvalid.get(), c.cur_out.get());
+            c.launches += 2;
             double I = 0;
             CICY_CUDA(cudaMemcpyAsync(&I, c.cur_out.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
             CICY_CUDA(cudaStreamSynchronize(s));
