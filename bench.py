@@ -37,8 +37,9 @@ sys.path.insert(0, ROOT)
 SIDE, N_CNTS, TOL, TOL_UNIT = 6.0, 25000, 1e-8, 1e-10
 METRIC = "networks solved/s at 1e-8 residual (25k-CNT 6um network, full hot path)"
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "ref_dump")
-PRECONDS = {"jacobi": 0, "learned": 1, "chain": 2}
-KERNELS = {0: "k_pcg (grid-wide persistent PCG)", 1: "k_pcg_cluster (16-CTA cluster-resident PCG)"}
+PRECONDS = {"jacobi": 0, "learned": 1, "chain": 2, "mg": 3}
+KERNELS = {0: "k_pcg (grid-wide persistent PCG)", 1: "k_pcg_cluster (16-CTA cluster-resident PCG)",
+           2: "k_mg_pcg (chain-aggregation multigrid PCG)"}
 
 
 def parse():
@@ -48,7 +49,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--precond", default="chain", choices=["jacobi", "chain", "learned"])
+    ap.add_argument("--precond", default="chain", choices=["jacobi", "chain", "learned", "mg"])
+    # a smaller network of the same generator, for profiler captures (the bench line names the size it ran)
+    ap.add_argument("--side", type=float, default=SIDE)
+    ap.add_argument("--cnts", type=int, default=N_CNTS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -60,10 +64,10 @@ def dist_env():
     return rank, world, local
 
 
-def workload(rank: int):
+def workload(rank: int, side: float = SIDE, cnts: int = N_CNTS):
     from cicy_geom_b200.network import NetworkConfig, generate_cnt_network
 
-    cfg = NetworkConfig(side=SIDE, n_cnts=N_CNTS, seed=2_000_000 + rank, tolerance=TOL, tolerance_unit=TOL_UNIT)
+    cfg = NetworkConfig(side=side, n_cnts=cnts, seed=2_000_000 + rank, tolerance=TOL, tolerance_unit=TOL_UNIT)
     raw = generate_cnt_network(cfg)
     return cfg, raw, raw.extract_window(cfg)
 
@@ -242,7 +246,7 @@ def run_ours(args):
 
         dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo", timeout=__import__("datetime").timedelta(seconds=600))
     torch.cuda.set_device(local)
-    cfg, raw, net = workload(rank)
+    cfg, raw, net = workload(rank, args.side, args.cnts)
     params = cfg.params()
     ctx = Context(local)
     ctx.set_solver(precision=1 if args.precision == "mixed" else 0, preconditioner=PRECONDS[args.precond])
@@ -328,7 +332,8 @@ def run_ours(args):
             "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f32/f64 mixed",
             "data": "synthetic (seeded CNT polylines with BASELINE statistics; one independent network per GPU)",
-            "config": {"workload": "single CNT network: 25,000 CNTs, 6 um cube, ~2.5M points, CG to 1e-8",
+            "config": {"workload": f"single CNT network: {args.cnts:,} CNTs, {args.side:g} um cube, {len(net.arrays()['x']):,} points "
+                                   f"in the window, CG to 1e-8",
                        "l2": "256 MB buffer written between steps (L2 flush)", "parallelism": f"replicas x{world}",
                        "precision": args.precision, "preconditioner": args.precond},
             "roofline": {"kernel": KERNELS[top], "bound": "hbm", "achieved": achieved, "peak": hbm,

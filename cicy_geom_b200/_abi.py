@@ -94,6 +94,8 @@ class SolveInfo(C.Structure):
         ("seconds", C.c_double),
         ("kernel", C.c_int32),
         ("restarts", C.c_int32),
+        ("levels", C.c_int32),
+        ("reserved0", C.c_int32),
     ]
 
 

@@ -90,7 +90,7 @@ void* cicy_ctx_stream(cicy_ctx* ctx) { return ctx ? (void*)ctx->c.stream : nullp
 
 cicy_status cicy_ctx_set_solver(cicy_ctx* ctx, const cicy_solver_opts* o) {
     return guarded(ctx, [&](cicy::Ctx& c) {
-        if (!o || o->precision < 0 || o->precision > 1 || o->preconditioner < 0 || o->preconditioner > 2 || o->max_iter_factor <= 0)
+        if (!o || o->precision < 0 || o->precision > 1 || o->preconditioner < 0 || o->preconditioner > 3 || o->max_iter_factor <= 0)
             throw cicy::Fail{CICY_E_INPUT, "cicy_ctx_set_solver: invalid options"};
         c.solver = *o;
     });

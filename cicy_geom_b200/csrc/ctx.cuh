@@ -24,6 +24,7 @@ struct DeaSystem {
     int64_t nodes = 0, reserved = 0, nnz_lower = 0, iterations = 0;
     int restarts = 0;
     bool cluster_solver = false;
+    int mg_levels = 0;
     double rel_residual = 0, seconds = 0;
     // device: strict-lower CSR of the free block (SSS), diagonal, rhs, x0, voltages (all nodes)
     DBuf<int32_t> row_ptr, col;

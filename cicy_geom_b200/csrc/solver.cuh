@@ -1,6 +1,8 @@
 // Preconditioned CG for DEA systems (see solver.cu).
 #pragma once
 
+#include <vector>
+
 #include "dev_common.cuh"
 
 namespace cicy {
@@ -53,8 +55,56 @@ struct PcgStats {
     long long iterations = 0;
     int restarts = 0;
     int ctas = 0;
+    int levels = 0;  // multigrid levels (0: one-level preconditioner)
     bool cluster = false;
     double seconds = 0;
+};
+
+// ---- chain-aggregation multigrid (solver_mg.cu) ----
+constexpr int kMgMaxLevels = 16;
+constexpr int kMgDenseMax = 128;  // coarsest levels up to this size get a dense inverse
+
+// One level as the solve kernel sees it.  Level 0 is the system's own CSR
+// (diagonal included); levels >= 1 hold off-diagonal CSR plus `diag`.
+struct MgLevel {
+    int n;
+    const int32_t* rp;
+    const int32_t* ci;
+    const double* val;
+    const double* diag;
+    const double* l1inv;
+    const int32_t* agg;   // row -> aggregate on level l+1 (coarsest: nullptr)
+    const int32_t* mptr;  // aggregate J of level l+1 -> its rows of level l: midx[mptr[J] .. mptr[J+1])
+    const int32_t* midx;
+    const int32_t* cagg;    // per nonzero: aggregate of its column (levels < coarsest)
+    const int32_t* ra_ptr;  // rows of P^T A_l, one per aggregate of level l+1 (levels 1 .. coarsest-1)
+    const int32_t* ra_col;
+    const double* ra_val;
+    double* r;
+    double* z;
+    double* zf;
+};
+
+struct MgWork {
+    struct Lvl {
+        int n = 0, nnz = 0;
+        const int32_t* rp_ptr = nullptr;
+        const int32_t* ci_ptr = nullptr;
+        const double* val_ptr = nullptr;
+        DBuf<int32_t> rp, ci, agg, mptr, midx, cagg, ra_ptr, ra_col;
+        DBuf<double> val, diag, l1inv, rs, r, z, zf, ra_val;
+    };
+    std::vector<Lvl> L;
+    std::vector<MgLevel> host_lv;
+    DBuf<MgLevel> dev_lv;
+    DBuf<double> cinv, z0, wtmp;
+    DBuf<unsigned long long> bar;
+    DBuf<uint64_t> keys;
+    DBuf<uint32_t> vals;
+    DBuf<int32_t> flag, pos, head, uidx, row, mate, best, rep, total, scan_tmp;
+    RadixScratch radix;
+    int levels = 0;
+    bool dense = false;
 };
 
 struct SolverWork {
@@ -66,6 +116,7 @@ struct SolverWork {
     DBuf<uint16_t> code;
     DBuf<unsigned int> barrier;
     int n_blocks = 0, block_entries = 0;
+    MgWork mg;
 };
 
 __global__ void k_residual(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const double* __restrict__ v,
@@ -90,6 +141,13 @@ void launch_pcg_jacobi_fp64(PcgArgs& a, int nb, cudaStream_t s);
 bool pcg_solve_cluster(SolverWork& w, const SolverSystem& sys, bool block_precond, const float* node_scale,
                        const float* edge_scale, int nchains, const int32_t* chain_start, const int32_t* chain_len, double tol,
                        long long max_iter, cudaStream_t s, int64_t& launches, PcgStats& st);
+
+// Multigrid hierarchy over the chain blocks of build_block_preconditioner (which
+// must have run on the same system), then the MG-preconditioned CG solve.
+void build_mg_hierarchy(SolverWork& w, const SolverSystem& sys, cudaStream_t s, int64_t& launches);
+// allow_cluster: one 16-CTA cluster with hardware barriers when it fits, else the grid-wide kernel.
+void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long max_iter, bool allow_cluster, int num_sms, int* status,
+                  cudaStream_t s, int64_t& launches, PcgStats& st);
 
 void pcg_solve(SolverWork& w, const SolverSystem& sys, int precond, bool mixed, double tol, long long max_iter, int num_sms,
                int* status, cudaStream_t s, int64_t& launches, PcgStats& st);

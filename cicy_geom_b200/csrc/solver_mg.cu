@@ -1,0 +1,916 @@
+// Chain-aggregation multigrid (CAMG) preconditioned conjugate gradient for the
+// DEA systems (device).
+//
+// Why: in a CNT resistor network the element resistors along one CNT conduct
+// 1e4-1e9 times better than the tunnelling junctions between CNTs, so after the
+// chain block-Jacobi has equilibrated every CNT the remaining error is "one
+// potential per CNT", a graph Laplacian over CNTs with junction conductances
+// spanning five orders of magnitude.  One-level preconditioners take thousands
+// of iterations on it; a coarse space with one unknown per chain block removes
+// it.  The hierarchy:
+//
+//   level 0   the free-node system; smoother: the chain blocks (explicit
+//             tridiagonal inverses), damped by kOmega0 so 2 M^-1 - A stays
+//             positive definite on floating islands (bipartite trees of CNTs
+//             that no prescribed node reaches, where the undamped block smoother
+//             would make the V-cycle singular)
+//   level 1   one unknown per chain block (aggregate = block)
+//   level l+1 pairwise aggregates of level l: three rounds of handshake
+//             matching on the strongest coupling |a_ij| (ties: smaller j), then
+//             every unmatched row joins the pair of its strongest neighbour
+//   coarsest  <= kMgDenseMax rows: dense inverse (Gauss-Jordan in shared
+//             memory, 1e-8 diagonal regularisation, variables with a vanishing
+//             pivot dropped); otherwise an l1-Jacobi step
+//
+// Coarse operators are Galerkin products P^T A P with piecewise-constant P, built
+// by sort-and-reduce of the cross-aggregate couplings (stable radix sort, runs
+// summed in input order: deterministic).  Their diagonals come from summed row
+// sums, diag_J = sum_{I in J} rowsum_I - sum_{J' != J} A_JJ', so the large
+// intra-aggregate conductances never cancel in floating point and an aggregate
+// with no outside coupling gets an exact zero row.  Levels >= 1 are smoothed by
+// l1-Jacobi (1 / (|d| + sum |a|)), which makes the symmetric V(1,1)-cycle an SPD
+// preconditioner.
+//
+// The solve is one persistent cooperative launch.  Level-0 rows are split over
+// CTAs at block boundaries (the block smoother only reads rows of its own CTA);
+// coarse levels are spread over all threads.  Per CG iteration the grid barriers
+// are: 1 after the pre-smoother and r.r, one per restriction, one after the
+// coarse solve, one per prolongation above level 1, one after the post-smoother
+// and r.z, one after p.q.  The stopping rule, FP64 true-residual replacement and
+// the first-iteration behaviour are those of the one-level kernel (solver.cu).
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "solver.cuh"
+
+namespace cicy {
+
+namespace {
+
+constexpr int kMgThreads = 256;
+constexpr int kMgClusterThreads = 1024;
+constexpr int kMgClusterCtas = 16;            // non-portable cluster size
+constexpr int kMgClusterMaxRows = 1 << 18;    // above this the grid-wide variant has more threads per row
+constexpr int kMgMaxRestarts = 24;
+constexpr double kOmega0 = 0.95;
+constexpr int kGjThreads = 1024;
+
+int grid_for(long long n, int threads = 256) {
+    long long b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > 148LL * 32) b = 148LL * 32;
+    return (int)b;
+}
+
+// ---------------------------------------------------------------------------
+// Setup kernels
+
+__global__ void k_block_of_row(int n, const int32_t* __restrict__ is_start, const int32_t* __restrict__ start_scan,
+                               int32_t* __restrict__ agg) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        agg[i] = start_scan[i] + is_start[i] - 1;
+}
+
+// Row sums of the level-0 matrix (diagonal included); a row sum at rounding level
+// of its diagonal is an unconnected (floating) row: exactly 0.
+__global__ void k_rowsum0(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const double* __restrict__ v,
+                          double* __restrict__ rs) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double s = 0, d = 0;
+        for (int k = rp[i]; k < rp[i + 1]; k++) {
+            s += v[k];
+            if (ci[k] == i) d = v[k];
+        }
+        rs[i] = (fabs(s) <= 1e-13 * fabs(d)) ? 0.0 : s;
+    }
+}
+
+// Per nonzero: 1 if it couples two different aggregates.
+__global__ void k_cross_flags(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const int32_t* __restrict__ agg,
+                              int32_t* __restrict__ flag) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int ai = agg[i];
+        for (int k = rp[i]; k < rp[i + 1]; k++) flag[k] = agg[ci[k]] != ai ? 1 : 0;
+    }
+}
+
+__global__ void k_cross_keys(int n, int b, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                             const int32_t* __restrict__ agg, const int32_t* __restrict__ flag, const int32_t* __restrict__ pos,
+                             uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint64_t ai = (uint64_t)agg[i] << b;
+        for (int k = rp[i]; k < rp[i + 1]; k++)
+            if (flag[k]) {
+                keys[pos[k]] = ai | (uint64_t)agg[ci[k]];
+                vals[pos[k]] = (uint32_t)k;
+            }
+    }
+}
+
+__global__ void k_run_heads64(int n, const uint64_t* __restrict__ keys, int32_t* __restrict__ head) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        head[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1 : 0;
+}
+
+// One thread per run of equal keys: sum its values in sorted (= input) order.
+__global__ void k_run_reduce(int n, int b, const uint64_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                             const int32_t* __restrict__ head, const int32_t* __restrict__ uidx, const double* __restrict__ src,
+                             int32_t* __restrict__ row, int32_t* __restrict__ col, double* __restrict__ out) {
+    const uint64_t mask = (b >= 64) ? ~0ull : ((1ull << b) - 1);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (!head[i]) continue;
+        const uint64_t key = keys[i];
+        double s = 0;
+        for (int j = i; j < n && keys[j] == key; j++) s += src[vals[j]];
+        const int u = uidx[i];
+        row[u] = (int32_t)(key >> b);
+        col[u] = (int32_t)(key & mask);
+        out[u] = s;
+    }
+}
+
+// CSR row pointers from the (sorted) row index of each entry.
+__global__ void k_row_ptr(int m, int nrows, const int32_t* __restrict__ row, int32_t* __restrict__ rp) {
+    for (int u = blockIdx.x * blockDim.x + threadIdx.x; u <= m; u += gridDim.x * blockDim.x) {
+        const int lo = (u == 0) ? 0 : row[u - 1] + 1;
+        const int hi = (u == m) ? nrows : row[u];
+        for (int r = lo; r <= hi && r <= nrows; r++) rp[r] = u;
+        if (u == m && m == 0)
+            for (int r = 0; r <= nrows; r++) rp[r] = 0;
+    }
+}
+
+__global__ void k_member_keys(int n, const int32_t* __restrict__ agg, uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        keys[i] = (uint64_t)agg[i];
+        vals[i] = (uint32_t)i;
+    }
+}
+
+__global__ void k_member_lists(int n, const uint64_t* __restrict__ keys, const uint32_t* __restrict__ vals, int32_t* __restrict__ row,
+                               int32_t* __restrict__ midx) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        row[i] = (int32_t)keys[i];
+        midx[i] = (int32_t)vals[i];
+    }
+}
+
+// Coarse row sums, diagonal and l1-Jacobi weights.
+__global__ void k_coarse_diag(int nc, const int32_t* __restrict__ mptr, const int32_t* __restrict__ midx, const double* __restrict__ rs_f,
+                              const int32_t* __restrict__ rp, const double* __restrict__ v, double* __restrict__ rs,
+                              double* __restrict__ diag, double* __restrict__ l1inv) {
+    for (int J = blockIdx.x * blockDim.x + threadIdx.x; J < nc; J += gridDim.x * blockDim.x) {
+        double s = 0;
+        for (int m = mptr[J]; m < mptr[J + 1]; m++) s += rs_f[midx[m]];
+        double off = 0, offabs = 0;
+        for (int k = rp[J]; k < rp[J + 1]; k++) {
+            off += v[k];
+            offabs += fabs(v[k]);
+        }
+        const double d = s - off;
+        rs[J] = s;
+        diag[J] = d;
+        const double l1 = fabs(d) + offabs;
+        l1inv[J] = l1 > 0 ? 1.0 / l1 : 0.0;
+    }
+}
+
+// Strongest neighbour of each row (|a_ij| largest, ties: smaller j); with
+// free_only, among unmatched rows and only for unmatched rows.
+__global__ void k_strongest(int n, int free_only, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                            const double* __restrict__ v, const int32_t* __restrict__ mate, int32_t* __restrict__ best) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int bj = -1;
+        if (!(free_only && mate[i] >= 0)) {
+            double bs = -1.0;
+            for (int k = rp[i]; k < rp[i + 1]; k++) {
+                const int j = ci[k];
+                if (free_only && mate[j] >= 0) continue;
+                const double s = fabs(v[k]);
+                if (s > bs || (s == bs && j < bj)) {
+                    bs = s;
+                    bj = j;
+                }
+            }
+        }
+        best[i] = bj;
+    }
+}
+
+__global__ void k_handshake(int n, const int32_t* __restrict__ best, int32_t* __restrict__ mate) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int j = best[i];
+        if (mate[i] < 0 && j >= 0 && best[j] == i) mate[i] = j;
+    }
+}
+
+__global__ void k_pair_rep(int n, const int32_t* __restrict__ mate, int32_t* __restrict__ rep) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        rep[i] = mate[i] >= 0 ? min(i, mate[i]) : i;
+}
+
+// Unmatched rows join the pair of their strongest neighbour (pairs' representatives
+// are never rewritten here, so reading rep[j] is race-free).
+__global__ void k_join(int n, const int32_t* __restrict__ mate, const int32_t* __restrict__ best, int32_t* __restrict__ rep) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int j = best[i];
+        if (mate[i] < 0 && j >= 0 && mate[j] >= 0) rep[i] = rep[j];
+    }
+}
+
+__global__ void k_is_rep(int n, const int32_t* __restrict__ rep, int32_t* __restrict__ flag) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) flag[i] = rep[i] == i ? 1 : 0;
+}
+
+__global__ void k_agg_ids(int n, const int32_t* __restrict__ rep, const int32_t* __restrict__ id, int32_t* __restrict__ agg) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) agg[i] = id[rep[i]];
+}
+
+__global__ void k_fill_neg(int n, int32_t* __restrict__ a) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = -1;
+}
+
+// Dense coarsest matrix, then its inverse in place by Gauss-Jordan without
+// pivoting (SPD up to floating islands) in shared memory.
+__global__ void k_dense_coarse(int nc, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const double* __restrict__ v,
+                               const double* __restrict__ diag, double* __restrict__ M) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nc; i += gridDim.x * blockDim.x) {
+        for (int j = 0; j < nc; j++) M[(size_t)i * nc + j] = 0.0;
+        for (int k = rp[i]; k < rp[i + 1]; k++) M[(size_t)i * nc + ci[k]] = v[k];
+        M[(size_t)i * nc + i] = diag[i];
+    }
+}
+
+__global__ void __launch_bounds__(kGjThreads) k_gauss_jordan(int n, double* __restrict__ M) {
+    extern __shared__ double S[];  // n * n + n
+    double* f = S + (size_t)n * n;
+    __shared__ double dmax_s;
+    __shared__ int drop_s;
+    const int t = threadIdx.x, T = blockDim.x;
+    for (int e = t; e < n * n; e += T) S[e] = M[e];
+    __syncthreads();
+    if (t == 0) {
+        double m = 0;
+        for (int i = 0; i < n; i++) m = fmax(m, fabs(S[i * n + i]));
+        dmax_s = m;
+    }
+    __syncthreads();
+    const double thr = 1e-12 * dmax_s;
+    for (int i = t; i < n; i += T) S[i * n + i] *= (1.0 + 1e-8);
+    __syncthreads();
+    for (int k = 0; k < n; k++) {
+        const double p = S[k * n + k];
+        if (t == 0) drop_s = !(p > thr);
+        __syncthreads();
+        if (drop_s) {
+            for (int j = t; j < n; j += T) {
+                S[k * n + j] = 0.0;
+                S[j * n + k] = 0.0;
+            }
+            __syncthreads();
+            continue;
+        }
+        for (int j = t; j < n; j += T) f[j] = (j == k) ? 0.0 : S[j * n + k];
+        __syncthreads();
+        for (int j = t; j < n; j += T) S[k * n + j] = ((j == k) ? 1.0 : S[k * n + j]) / p;
+        __syncthreads();
+        for (int e = t; e < n * n; e += T) {
+            const int i = e / n, j = e - i * n;
+            if (i == k) continue;
+            S[e] = ((j == k) ? 0.0 : S[e]) - f[i] * S[k * n + j];
+        }
+        __syncthreads();
+    }
+    for (int e = t; e < n * n; e += T) M[e] = S[e];
+}
+
+// Restriction operator rows P^T A_l of a level l >= 1: row J lists, for each
+// member I of aggregate J (ascending), (I, diag_I) and then row I's couplings.
+__global__ void k_ra_len(int nc, const int32_t* __restrict__ mptr, const int32_t* __restrict__ midx, const int32_t* __restrict__ rp,
+                         int32_t* __restrict__ len) {
+    for (int J = blockIdx.x * blockDim.x + threadIdx.x; J < nc; J += gridDim.x * blockDim.x) {
+        int s = 0;
+        for (int m = mptr[J]; m < mptr[J + 1]; m++) {
+            const int I = midx[m];
+            s += 1 + rp[I + 1] - rp[I];
+        }
+        len[J] = s;
+    }
+}
+
+__global__ void k_ra_fill(int nc, const int32_t* __restrict__ mptr, const int32_t* __restrict__ midx, const int32_t* __restrict__ rp,
+                          const int32_t* __restrict__ ci, const double* __restrict__ v, const double* __restrict__ diag,
+                          const int32_t* __restrict__ ra_ptr, int32_t* __restrict__ ra_col, double* __restrict__ ra_val) {
+    for (int J = blockIdx.x * blockDim.x + threadIdx.x; J < nc; J += gridDim.x * blockDim.x) {
+        int e = ra_ptr[J];
+        for (int m = mptr[J]; m < mptr[J + 1]; m++) {
+            const int I = midx[m];
+            ra_col[e] = I;
+            ra_val[e] = diag[I];
+            e++;
+            for (int k = rp[I]; k < rp[I + 1]; k++) {
+                ra_col[e] = ci[k];
+                ra_val[e] = v[k];
+                e++;
+            }
+        }
+    }
+}
+
+// Aggregate of each nonzero's column, so prolongated values load without a
+// dependent index load.
+__global__ void k_cagg(int nnz, const int32_t* __restrict__ ci, const int32_t* __restrict__ agg, int32_t* __restrict__ cagg) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += gridDim.x * blockDim.x) cagg[k] = agg[ci[k]];
+}
+
+// ---------------------------------------------------------------------------
+// Solve kernel
+
+constexpr int kGroup = 8;  // lanes cooperating on one coarse row
+
+struct MgArgs {
+    int n;
+    const int32_t* rp;
+    const int32_t* ci;
+    const double* val;
+    const double* b;
+    double* x;
+    double *r, *z0, *z, *w, *p, *q;
+    const double* tinv;
+    const int32_t *row_off, *row_base, *row_m;
+    const int32_t* cta_row;
+    int levels;            // number of levels including level 0
+    const MgLevel* lv;     // device descriptors
+    const double* cinv;    // dense inverse of the coarsest level, or nullptr
+    double omega0;
+    double* partA;
+    double* partB;
+    double* stats;
+    unsigned long long* bar;  // monotonic arrival counter (zeroed before the launch)
+    int* err;
+    double tol;
+    long long max_iter;
+    int max_restarts;
+};
+
+// Grid barrier on a monotonic counter: one release-add per CTA, then an acquire
+// spin until all CTAs of this round arrived.  Bounded: after kSpinLimit polls the
+// CTA records DEV_TIMEOUT and returns false.
+__device__ __forceinline__ bool mg_sync(unsigned long long* bar, unsigned long long& target, int* err, int* s_ok) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        target += gridDim.x;
+        __threadfence();
+        atomicAdd(bar, 1ull);
+        long long spins = 0;
+        int ok = 1;
+        while (true) {
+            unsigned long long v;
+            asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(bar) : "memory");
+            if (v >= target) break;
+            if ((++spins & 1023) == 0 && (spins > kSpinLimit || *((volatile int*)err) != 0)) {
+                atomicCAS(err, 0, (int)DEV_TIMEOUT);
+                ok = 0;
+                break;
+            }
+        }
+        *s_ok = ok;
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
+
+// Cluster variant: the hardware cluster barrier (release/acquire at cluster
+// scope orders the global-memory writes of all CTAs of the cluster).
+template <bool CL>
+__device__ __forceinline__ bool sync_all(unsigned long long* bar, unsigned long long& target, int* err, int* s_ok) {
+    if constexpr (CL) {
+        asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+        asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+        return true;
+    } else {
+        return mg_sync(bar, target, err, s_ok);
+    }
+}
+
+__device__ __forceinline__ void mg_reduce1(double a, double* sm, double& ra) {
+    a = warp_sum(a);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sm[w] = a;
+    __syncthreads();
+    if (w == 0) {
+        const int nw = blockDim.x >> 5;
+        double x = lane < nw ? sm[lane] : 0.0;
+        x = warp_sum(x);
+        if (lane == 0) sm[64] = x;
+    }
+    __syncthreads();
+    ra = sm[64];
+    __syncthreads();
+}
+
+__device__ __forceinline__ double mg_sum_partials(const double* part, int nb, double* sm) {
+    if (threadIdx.x < 32) {
+        double a = 0;
+        for (int i = threadIdx.x; i < nb; i += 32) a += __ldcg(&part[i]);
+        a = warp_sum(a);
+        if (threadIdx.x == 0) sm[66] = a;
+    }
+    __syncthreads();
+    const double s = sm[66];
+    __syncthreads();
+    return s;
+}
+
+__device__ __forceinline__ double group_sum(double v, unsigned mask) {
+    for (int o = kGroup / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, kGroup);
+    return v;
+}
+
+__device__ __forceinline__ double block_apply(const MgArgs& a, const double* __restrict__ v, int i) {
+    const int off = a.row_off[i], base = a.row_base[i], m = a.row_m[i];
+    double s = 0;
+    for (int j = 0; j < m; j++) s += a.tinv[off + j] * v[base + j];
+    return s;
+}
+
+template <bool CL>
+__global__ void __launch_bounds__(CL ? kMgClusterThreads : kMgThreads) k_mg_pcg(MgArgs a) {
+    __shared__ double sm[72];
+    __shared__ MgLevel lv[kMgMaxLevels];
+    __shared__ double rc[kMgDenseMax];
+    __shared__ int s_ok;
+    if (threadIdx.x < a.levels) lv[threadIdx.x] = a.lv[threadIdx.x];
+    __syncthreads();
+    const int C = a.levels - 1;
+    const int nb = gridDim.x;
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+    const int grp = gt / kGroup, glane = gt % kGroup, ngrp = gs / kGroup;
+    const unsigned gmask = ((1u << kGroup) - 1) << ((threadIdx.x & 31) & ~(kGroup - 1));
+    const int r_lo = a.cta_row[blockIdx.x], r_hi = a.cta_row[blockIdx.x + 1];
+    unsigned long long target = 0;
+    double R0 = 0, rr = 0, rz = 0, beta = 0;
+    long long k = 0;
+    int restarts = 0;
+    bool fresh = true;      // p = z, q = A z on the next direction update
+    bool recursive = false; // r is the recursively updated residual (not b - A x)
+    while (true) {
+        // ---- pre-smoother z0 = w M0^-1 r on own rows; r.r ----
+        __syncthreads();
+        double rr_l = 0;
+        for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
+            a.z0[i] = a.omega0 * block_apply(a, a.r, i);
+            const double ri = a.r[i];
+            rr_l += ri * ri;
+        }
+        double s0;
+        mg_reduce1(rr_l, sm, s0);
+        if (threadIdx.x == 0) a.partA[blockIdx.x] = s0;
+        if (!sync_all<CL>(a.bar, target, a.err, &s_ok)) return;
+        rr = mg_sum_partials(a.partA, nb, sm);
+        if (k == 0 && !recursive && restarts == 0) R0 = a.tol * sqrt(rr);
+        if (k > 0 && sqrt(rr) <= R0) {
+            if (!recursive || restarts >= a.max_restarts) break;
+            // the recursive residual met the test: replace it by the FP64 true residual
+            for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
+                double s = 0;
+                for (int kk = a.rp[i]; kk < a.rp[i + 1]; kk++) s += a.val[kk] * __ldcg(&a.x[a.ci[kk]]);
+                a.r[i] = a.b[i] - s;
+            }
+            restarts++;
+            recursive = false;
+            fresh = true;
+            continue;
+        }
+        if (k >= a.max_iter) break;
+        // ---- restriction 0 -> 1 inside the CTA (its blocks are its own rows) ----
+        {
+            const MgLevel& F = lv[0];
+            const MgLevel& G = lv[1];
+            for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
+                double res = a.r[i];
+                for (int kk = a.rp[i]; kk < a.rp[i + 1]; kk++) res -= a.val[kk] * __ldcg(&a.z0[a.ci[kk]]);
+                a.w[i] = res;
+            }
+            __syncthreads();
+            const bool smooth = (C > 1) || a.cinv == nullptr;
+            if (r_hi > r_lo) {
+                const int b0 = F.agg[r_lo], b1 = F.agg[r_hi - 1];
+                for (int J = b0 + threadIdx.x; J <= b1; J += blockDim.x) {
+                    double s = 0;
+                    for (int m = F.mptr[J]; m < F.mptr[J + 1]; m++) s += a.w[F.midx[m]];
+                    G.r[J] = s;
+                    if (smooth) G.z[J] = G.l1inv[J] * s;
+                }
+            }
+            if (!sync_all<CL>(a.bar, target, a.err, &s_ok)) return;
+        }
+        // ---- restrictions l -> l+1 (l >= 1): r_{l+1} = P^T r_l - (P^T A_l) z_l ----
+        for (int l = 1; l < C; l++) {
+            const MgLevel& F = lv[l];
+            const MgLevel& G = lv[l + 1];
+            const bool smooth = (l + 1 < C) || a.cinv == nullptr;
+            for (int J = grp; J < G.n; J += ngrp) {
+                double s = 0;
+                for (int m = F.mptr[J] + glane; m < F.mptr[J + 1]; m += kGroup) s += __ldcg(&F.r[F.midx[m]]);
+                for (int e = F.ra_ptr[J] + glane; e < F.ra_ptr[J + 1]; e += kGroup) s -= F.ra_val[e] * __ldcg(&F.z[F.ra_col[e]]);
+                s = group_sum(s, gmask);
+                if (glane == 0) {
+                    G.r[J] = s;
+                    if (smooth) G.z[J] = G.l1inv[J] * s;
+                }
+            }
+            if (!sync_all<CL>(a.bar, target, a.err, &s_ok)) return;
+        }
+        // ---- coarsest: dense inverse, one warp per row ----
+        if (a.cinv) {
+            const MgLevel& Cl = lv[C];
+            const int nC = Cl.n;
+            const int wpb = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+            if (blockIdx.x * wpb < nC) {
+                for (int j = threadIdx.x; j < nC; j += blockDim.x) rc[j] = __ldcg(&Cl.r[j]);
+                __syncthreads();
+                for (int i = blockIdx.x * wpb + warp; i < nC; i += gridDim.x * wpb) {
+                    const double* row = a.cinv + (size_t)i * nC;
+                    double s = 0;
+                    for (int j = lane; j < nC; j += 32) s += row[j] * rc[j];
+                    s = warp_sum(s);
+                    if (lane == 0) Cl.zf[i] = s;
+                }
+            }
+            if (!sync_all<CL>(a.bar, target, a.err, &s_ok)) return;
+        }
+        // ---- prolongation + l1-Jacobi post-smoother, levels C-1 .. 1 ----
+        for (int l = C - 1; l >= 1; l--) {
+            const MgLevel& F = lv[l];
+            const double* zc = lv[l + 1].zf;
+            for (int I = grp; I < F.n; I += ngrp) {
+                double w = 0;
+                for (int kk = F.rp[I] + glane; kk < F.rp[I + 1]; kk += kGroup)
+                    w -= F.val[kk] * (__ldcg(&F.z[F.ci[kk]]) + __ldcg(&zc[F.cagg[kk]]));
+                w = group_sum(w, gmask);
+                if (glane == 0) {
+                    const double zp = __ldcg(&F.z[I]) + __ldcg(&zc[F.agg[I]]);
+                    w += __ldcg(&F.r[I]) - F.diag[I] * zp;
+                    F.zf[I] = zp + F.l1inv[I] * w;
+                }
+            }
+            if (!sync_all<CL>(a.bar, target, a.err, &s_ok)) return;
+        }
+        // ---- level-0 post-smoother: z = z0 + P z1, z += w M0^-1 (r - A z); r.z ----
+        {
+            const double* zc = lv[1].zf;
+            const int32_t* agg = lv[0].agg;
+            const int32_t* cagg = lv[0].cagg;
+            for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
+                double w = a.r[i];
+                for (int kk = a.rp[i]; kk < a.rp[i + 1]; kk++)
+                    w -= a.val[kk] * (__ldcg(&a.z0[a.ci[kk]]) + __ldcg(&zc[cagg[kk]]));
+                a.w[i] = w;
+                a.z[i] = a.z0[i] + __ldcg(&zc[agg[i]]);
+            }
+            __syncthreads();
+            double rz_l = 0;
+            for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
+                const double zi = a.z[i] + a.omega0 * block_apply(a, a.w, i);
+                a.z[i] = zi;
+                rz_l += a.r[i] * zi;
+            }
+            mg_reduce1(rz_l, sm, s0);
+            if (threadIdx.x == 0) a.partB[blockIdx.x] = s0;
+            if (!sync_all<CL>(a.bar, target, a.err, &s_ok)) return;
+            const double rz_new = mg_sum_partials(a.partB, nb, sm);
+            beta = fresh ? 0.0 : rz_new / rz;
+            rz = rz_new;
+        }
+        // ---- q = A z + beta q, p = z + beta p; p.q ----
+        double pq_l = 0;
+        for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
+            double w = 0;
+            for (int kk = a.rp[i]; kk < a.rp[i + 1]; kk++) w += a.val[kk] * __ldcg(&a.z[a.ci[kk]]);
+            const double zi = a.z[i];
+            const double qi = fresh ? w : w + beta * a.q[i];
+            const double pi = fresh ? zi : zi + beta * a.p[i];
+            a.q[i] = qi;
+            a.p[i] = pi;
+            pq_l += pi * qi;
+        }
+        mg_reduce1(pq_l, sm, s0);
+        if (threadIdx.x == 0) a.partA[nb + blockIdx.x] = s0;
+        if (!sync_all<CL>(a.bar, target, a.err, &s_ok)) return;
+        const double pq = mg_sum_partials(a.partA + nb, nb, sm);
+        fresh = false;
+        k++;
+        // ---- x += alpha p, r -= alpha q ----
+        const double alpha = rz / pq;
+        for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
+            a.x[i] += alpha * a.p[i];
+            a.r[i] -= alpha * a.q[i];
+        }
+        recursive = true;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.stats[0] = (double)k;
+        a.stats[1] = rr;
+        a.stats[2] = R0;
+        a.stats[3] = (double)restarts;
+    }
+}
+
+// Galerkin coarse level l+1 from level l and its aggregates (g.L[l].agg, nc of them).
+void coarsen(MgWork& g, int l, int nc, cudaStream_t s, int64_t& launches) {
+    if ((int)g.L.size() < l + 2) g.L.resize(l + 2);
+    MgWork::Lvl& F = g.L[l];
+    MgWork::Lvl& G = g.L[l + 1];
+    const int nf = F.n, nnz = F.nnz;
+    const int b = bits_for((uint64_t)std::max(nc - 1, 1));
+    // cross-aggregate couplings -> sorted (row, col) keys
+    g.flag.ensure(nnz + 1);
+    g.pos.ensure(nnz + 1);
+    k_cross_flags<<<grid_for(nf), 256, 0, s>>>(nf, F.rp_ptr, F.ci_ptr, F.agg.get(), g.flag.get());
+    launches++;
+    exclusive_scan_i32(g.flag.get(), g.pos.get(), nnz, g.total.get(), g.scan_tmp, s, launches);
+    int m = 0;
+    CICY_CUDA(cudaMemcpyAsync(&m, g.total.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    CICY_CUDA(cudaStreamSynchronize(s));
+    const int cap = std::max(std::max(m, nf), 1) + 1;
+    g.keys.ensure(cap);
+    g.vals.ensure(cap);
+    g.head.ensure(cap);
+    g.uidx.ensure(cap);
+    g.row.ensure(cap);
+    G.n = nc;
+    int nu = 0;
+    if (m > 0) {
+        k_cross_keys<<<grid_for(nf), 256, 0, s>>>(nf, b, F.rp_ptr, F.ci_ptr, F.agg.get(), g.flag.get(), g.pos.get(), g.keys.get(),
+                                                  g.vals.get());
+        launches++;
+        radix_sort_pairs(g.keys.get(), g.vals.get(), m, 2 * b, g.radix, s, launches);
+        k_run_heads64<<<grid_for(m), 256, 0, s>>>(m, g.keys.get(), g.head.get());
+        launches++;
+        exclusive_scan_i32(g.head.get(), g.uidx.get(), m, g.total.get(), g.scan_tmp, s, launches);
+        CICY_CUDA(cudaMemcpyAsync(&nu, g.total.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        CICY_CUDA(cudaStreamSynchronize(s));
+    }
+    G.nnz = nu;
+    G.rp.ensure(nc + 1);
+    G.ci.ensure(std::max(nu, 1));
+    G.val.ensure(std::max(nu, 1));
+    if (m > 0) {
+        k_run_reduce<<<grid_for(m), 256, 0, s>>>(m, b, g.keys.get(), g.vals.get(), g.head.get(), g.uidx.get(), F.val_ptr, g.row.get(),
+                                                 G.ci.get(), G.val.get());
+        launches++;
+    }
+    k_row_ptr<<<grid_for(nu + 1), 256, 0, s>>>(nu, nc, g.row.get(), G.rp.get());
+    launches++;
+    G.rp_ptr = G.rp.get();
+    G.ci_ptr = G.ci.get();
+    G.val_ptr = G.val.get();
+    // members of each aggregate, ascending row order
+    F.mptr.ensure(nc + 1);
+    F.midx.ensure(std::max(nf, 1));
+    k_member_keys<<<grid_for(nf), 256, 0, s>>>(nf, F.agg.get(), g.keys.get(), g.vals.get());
+    launches++;
+    radix_sort_pairs(g.keys.get(), g.vals.get(), nf, b, g.radix, s, launches);
+    k_member_lists<<<grid_for(nf), 256, 0, s>>>(nf, g.keys.get(), g.vals.get(), g.row.get(), F.midx.get());
+    k_row_ptr<<<grid_for(nf + 1), 256, 0, s>>>(nf, nc, g.row.get(), F.mptr.get());
+    launches += 2;
+    // row sums, diagonal, l1 weights
+    G.rs.ensure(nc);
+    G.diag.ensure(nc);
+    G.l1inv.ensure(nc);
+    k_coarse_diag<<<grid_for(nc), 256, 0, s>>>(nc, F.mptr.get(), F.midx.get(), F.rs.get(), G.rp.get(), G.val.get(), G.rs.get(),
+                                               G.diag.get(), G.l1inv.get());
+    launches++;
+    CICY_LAUNCH_CHECK();
+}
+
+// Pairwise aggregates of level l; returns their number.
+int pairwise(MgWork& g, int l, cudaStream_t s, int64_t& launches) {
+    MgWork::Lvl& F = g.L[l];
+    const int n = F.n;
+    g.mate.ensure(n + 1);
+    g.best.ensure(n + 1);
+    g.rep.ensure(n + 1);
+    g.flag.ensure(n + 1);
+    g.pos.ensure(n + 1);
+    k_fill_neg<<<grid_for(n), 256, 0, s>>>(n, g.mate.get());
+    launches++;
+    for (int round = 0; round < 3; round++) {
+        k_strongest<<<grid_for(n), 256, 0, s>>>(n, 1, F.rp_ptr, F.ci_ptr, F.val_ptr, g.mate.get(), g.best.get());
+        k_handshake<<<grid_for(n), 256, 0, s>>>(n, g.best.get(), g.mate.get());
+        launches += 2;
+    }
+    k_pair_rep<<<grid_for(n), 256, 0, s>>>(n, g.mate.get(), g.rep.get());
+    k_strongest<<<grid_for(n), 256, 0, s>>>(n, 0, F.rp_ptr, F.ci_ptr, F.val_ptr, g.mate.get(), g.best.get());
+    k_join<<<grid_for(n), 256, 0, s>>>(n, g.mate.get(), g.best.get(), g.rep.get());
+    k_is_rep<<<grid_for(n), 256, 0, s>>>(n, g.rep.get(), g.flag.get());
+    launches += 4;
+    exclusive_scan_i32(g.flag.get(), g.pos.get(), n, g.total.get(), g.scan_tmp, s, launches);
+    F.agg.ensure(n + 1);
+    k_agg_ids<<<grid_for(n), 256, 0, s>>>(n, g.rep.get(), g.pos.get(), F.agg.get());
+    launches++;
+    int nc = 0;
+    CICY_CUDA(cudaMemcpyAsync(&nc, g.total.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    CICY_CUDA(cudaStreamSynchronize(s));
+    CICY_LAUNCH_CHECK();
+    return nc;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+void build_mg_hierarchy(SolverWork& w, const SolverSystem& sys, cudaStream_t s, int64_t& launches) {
+    MgWork& g = w.mg;
+    const int n = sys.n;
+    g.total.ensure(2);
+    if (g.L.empty()) g.L.resize(1);
+    MgWork::Lvl& L0 = g.L[0];
+    L0.n = n;
+    L0.nnz = sys.nnz;
+    L0.rp_ptr = sys.rp;
+    L0.ci_ptr = sys.ci;
+    L0.val_ptr = sys.val;
+    L0.agg.ensure(n + 1);
+    L0.rs.ensure(n + 1);
+    k_block_of_row<<<grid_for(n), 256, 0, s>>>(n, w.is_start.get(), w.start_scan.get(), L0.agg.get());
+    k_rowsum0<<<grid_for(n), 256, 0, s>>>(n, sys.rp, sys.ci, sys.val, L0.rs.get());
+    launches += 2;
+    int nc = w.n_blocks;
+    int C = 0;
+    for (int l = 0;; l++) {
+        coarsen(g, l, nc, s, launches);
+        C = l + 1;
+        if (g.L[C].n <= kMgDenseMax || C + 1 >= kMgMaxLevels) break;
+        const int nc2 = pairwise(g, C, s, launches);
+        if (nc2 > 0.9 * g.L[C].n) break;
+        nc = nc2;
+    }
+    g.dense = false;
+    MgWork::Lvl& Lc = g.L[C];
+    if (Lc.n <= kMgDenseMax) {
+        g.cinv.ensure((size_t)Lc.n * Lc.n);
+        k_dense_coarse<<<grid_for(Lc.n, 128), 128, 0, s>>>(Lc.n, Lc.rp.get(), Lc.ci.get(), Lc.val.get(), Lc.diag.get(), g.cinv.get());
+        const size_t smem = sizeof(double) * ((size_t)Lc.n * Lc.n + Lc.n);
+        if (smem > 48 * 1024)
+            CICY_CUDA(cudaFuncSetAttribute(k_gauss_jordan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_gauss_jordan<<<1, kGjThreads, smem, s>>>(Lc.n, g.cinv.get());
+        launches += 2;
+        g.dense = true;
+    }
+    // restriction rows P^T A_l (levels 1 .. C-1) and column aggregates (levels 0 .. C-1)
+    for (int l = 0; l < C; l++) {
+        MgWork::Lvl& L = g.L[l];
+        const int ncl = g.L[l + 1].n;
+        L.cagg.ensure(std::max(L.nnz, 1));
+        k_cagg<<<grid_for(L.nnz), 256, 0, s>>>(L.nnz, L.ci_ptr, L.agg.get(), L.cagg.get());
+        launches++;
+        if (l == 0) continue;
+        L.ra_ptr.ensure(ncl + 1);
+        k_ra_len<<<grid_for(ncl), 256, 0, s>>>(ncl, L.mptr.get(), L.midx.get(), L.rp_ptr, L.ra_ptr.get());
+        exclusive_scan_i32(L.ra_ptr.get(), L.ra_ptr.get(), ncl, g.total.get(), g.scan_tmp, s, launches);
+        int tot = 0;
+        CICY_CUDA(cudaMemcpyAsync(&tot, g.total.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        CICY_CUDA(cudaStreamSynchronize(s));
+        CICY_CUDA(cudaMemcpyAsync(L.ra_ptr.get() + ncl, &tot, sizeof(int), cudaMemcpyHostToDevice, s));
+        L.ra_col.ensure(std::max(tot, 1));
+        L.ra_val.ensure(std::max(tot, 1));
+        k_ra_fill<<<grid_for(ncl), 256, 0, s>>>(ncl, L.mptr.get(), L.midx.get(), L.rp_ptr, L.ci_ptr, L.val_ptr, L.diag.get(),
+                                                L.ra_ptr.get(), L.ra_col.get(), L.ra_val.get());
+        launches += 2;
+    }
+    // work vectors and device descriptors
+    g.host_lv.assign(C + 1, MgLevel{});
+    for (int l = 0; l <= C; l++) {
+        MgWork::Lvl& L = g.L[l];
+        MgLevel& d = g.host_lv[l];
+        d.n = L.n;
+        d.rp = L.rp_ptr;
+        d.ci = L.ci_ptr;
+        d.val = L.val_ptr;
+        d.agg = (l < C) ? L.agg.get() : nullptr;
+        d.mptr = (l < C) ? L.mptr.get() : nullptr;
+        d.midx = (l < C) ? L.midx.get() : nullptr;
+        d.cagg = (l < C) ? L.cagg.get() : nullptr;
+        d.ra_ptr = (l >= 1 && l < C) ? L.ra_ptr.get() : nullptr;
+        d.ra_col = (l >= 1 && l < C) ? L.ra_col.get() : nullptr;
+        d.ra_val = (l >= 1 && l < C) ? L.ra_val.get() : nullptr;
+        if (l >= 1) {
+            L.r.ensure(L.n + 1);
+            L.z.ensure(L.n + 1);
+            d.diag = L.diag.get();
+            d.l1inv = L.l1inv.get();
+            d.r = L.r.get();
+            d.z = L.z.get();
+            if (l == C && !g.dense) {
+                d.zf = L.z.get();
+            } else {
+                L.zf.ensure(L.n + 1);
+                d.zf = L.zf.get();
+            }
+        }
+    }
+    g.dev_lv.ensure(C + 1);
+    CICY_CUDA(cudaMemcpyAsync(g.dev_lv.get(), g.host_lv.data(), sizeof(MgLevel) * (C + 1), cudaMemcpyHostToDevice, s));
+    CICY_CUDA(cudaStreamSynchronize(s));
+    g.levels = C + 1;
+    CICY_LAUNCH_CHECK();
+}
+
+void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long max_iter, bool allow_cluster, int num_sms, int* status,
+                  cudaStream_t s, int64_t& launches, PcgStats& st) {
+    const int n = sys.n;
+    st = PcgStats{};
+    if (n <= 0) return;
+    MgWork& g = w.mg;
+    w.r.ensure(n); w.z.ensure(n); w.p.ensure(n); w.q.ensure(n);
+    g.z0.ensure(n);
+    g.wtmp.ensure(n);
+    k_residual<<<grid_for(n), 256, 0, s>>>(n, sys.rp, sys.ci, sys.val, sys.x, sys.b, w.r.get());
+    launches++;
+    // one 16-CTA cluster with hardware barriers when it can be launched, else the
+    // grid-wide cooperative launch
+    static int cl_state = 0;  // 0 unknown, 1 ok, -1 unsupported
+    if (cl_state == 0) {
+        cl_state = cudaFuncSetAttribute(k_mg_pcg<true>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess ? 1 : -1;
+        cudaGetLastError();
+    }
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    bool cluster = false;
+    if (allow_cluster && cl_state > 0 && n <= kMgClusterMaxRows) {
+        cfg.gridDim = dim3(kMgClusterCtas);
+        cfg.blockDim = dim3(kMgClusterThreads);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = s;
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = kMgClusterCtas;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int nclusters = 0;
+        cluster = cudaOccupancyMaxActiveClusters(&nclusters, (void*)k_mg_pcg<true>, &cfg) == cudaSuccess && nclusters >= 1;
+        cudaGetLastError();
+    }
+    int nb = kMgClusterCtas;
+    if (!cluster) {
+        int occ = 0;
+        CICY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mg_pcg<false>, kMgThreads, 0));
+        const int cap = std::max(1, occ) * num_sms;
+        nb = std::max(1, std::min({cap, num_sms, ceil_div(n, 2 * kMgThreads)}));
+    }
+    w.cta_row.ensure(nb + 1);
+    launch_cta_rows(nb, n, w.is_start.get(), w.cta_row.get(), s);
+    w.part.ensure(4 * nb + 8);
+    g.bar.ensure(1);
+    w.stats.ensure(4);
+    CICY_CUDA(cudaMemsetAsync(g.bar.get(), 0, sizeof(unsigned long long), s));
+    CICY_CUDA(cudaMemsetAsync(w.stats.get(), 0, sizeof(double) * 4, s));
+    MgArgs a{};
+    a.n = n;
+    a.rp = sys.rp; a.ci = sys.ci; a.val = sys.val; a.b = sys.b; a.x = sys.x;
+    a.r = w.r.get(); a.z0 = g.z0.get(); a.z = w.z.get(); a.w = g.wtmp.get(); a.p = w.p.get(); a.q = w.q.get();
+    a.tinv = w.tinv.get(); a.row_off = w.row_off.get(); a.row_base = w.row_base.get(); a.row_m = w.row_m.get();
+    a.cta_row = w.cta_row.get();
+    a.levels = g.levels;
+    a.lv = g.dev_lv.get();
+    a.cinv = g.dense ? g.cinv.get() : nullptr;
+    a.omega0 = kOmega0;
+    a.partA = w.part.get();
+    a.partB = w.part.get() + 2 * nb;
+    a.stats = w.stats.get();
+    a.bar = g.bar.get();
+    a.err = status;
+    a.tol = tol;
+    a.max_iter = max_iter;
+    a.max_restarts = kMgMaxRestarts;
+    cudaEvent_t e0, e1;
+    CICY_CUDA(cudaEventCreate(&e0));
+    CICY_CUDA(cudaEventCreate(&e1));
+    CICY_CUDA(cudaEventRecord(e0, s));
+    if (cluster) {
+        CICY_CUDA(cudaLaunchKernelEx(&cfg, k_mg_pcg<true>, a));
+    } else {
+        void* args[] = {&a};
+        CICY_CUDA(cudaLaunchCooperativeKernel((void*)k_mg_pcg<false>, dim3(nb), dim3(kMgThreads), args, 0, s));
+    }
+    CICY_CUDA(cudaEventRecord(e1, s));
+    launches++;
+    double hs[4];
+    CICY_CUDA(cudaMemcpyAsync(hs, w.stats.get(), sizeof(hs), cudaMemcpyDeviceToHost, s));
+    CICY_CUDA(cudaStreamSynchronize(s));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    st.iterations = (long long)hs[0];
+    st.restarts = (int)hs[3];
+    st.seconds = ms * 1e-3;
+    st.ctas = nb;
+    st.levels = g.levels;
+    st.cluster = cluster;
+}
+
+}  // namespace cicy

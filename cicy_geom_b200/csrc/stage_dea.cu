@@ -714,7 +714,14 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
         // small and medium systems: one cluster with everything in shared memory;
         // otherwise (or when disabled) the grid-wide persistent kernel
         bool solved = false;
-        if (!mixed && !(c.solver.flags & CICY_SOLVER_NO_CLUSTER))
+        if (c.solver.preconditioner == CICY_PRECOND_MG && n > 0) {
+            build_block_preconditioner(c.sw, ss, NM, c.chain_start.get(), c.chain_len.get(), nullptr, nullptr, false, s, c.launches);
+            build_mg_hierarchy(c.sw, ss, s, c.launches);
+            pcg_solve_mg(c.sw, ss, tol, max_iter, !(c.solver.flags & CICY_SOLVER_NO_CLUSTER), c.num_sms, c.status.get(), s, c.launches,
+                         st);
+            solved = true;
+        }
+        if (!solved && !mixed && !(c.solver.flags & CICY_SOLVER_NO_CLUSTER))
             solved = pcg_solve_cluster(c.sw, ss, kind == PRECOND_KIND_BLOCK, ns, es, NM, c.chain_start.get(), c.chain_len.get(), tol,
                                        max_iter, s, c.launches, st);
         if (!solved) {
@@ -724,6 +731,7 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
         }
         check_status(c, "Solve_DEA_equations_CG_SSS");
         sys->cluster_solver = st.cluster;
+        sys->mg_levels = st.levels;
         sys->seconds = st.seconds;
         sys->iterations = st.iterations;
         sys->restarts = st.restarts;
@@ -905,7 +913,8 @@ void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out) {
             si.iterations = sy->iterations;
             si.rel_residual = sy->rel_residual;
             si.seconds = sy->seconds;
-            si.kernel = sy->cluster_solver ? 1 : 0;
+            si.kernel = sy->mg_levels > 0 ? 2 : sy->cluster_solver ? 1 : 0;
+            si.levels = sy->mg_levels;
             si.restarts = sy->restarts;
         }
         out->stage_seconds[2] = t_unit;

@@ -66,7 +66,7 @@ class Context:
         return lib().cicy_ctx_stream(self._h) or 0
 
     def set_solver(self, precision: int = 0, preconditioner: int = 0, max_iter_factor: int = 300, cluster: bool = True):
-        """precision: 0 FP64, 1 mixed; preconditioner: 0 Jacobi (upstream), 1 learned, 2 chain blocks;
+        """precision: 0 FP64, 1 mixed; preconditioner: 0 Jacobi (upstream), 1 learned, 2 chain blocks, 3 multigrid;
         cluster: allow the cluster-resident solver for systems that fit in shared memory."""
         o = _abi.SolverOpts(precision, preconditioner, max_iter_factor, 0 if cluster else 1)
         self._check(lib().cicy_ctx_set_solver(self._h, C.byref(o)), "cicy_ctx_set_solver")
@@ -185,7 +185,7 @@ def result_dict(r: _abi.Result) -> dict:
         "solves": [
             {"cluster": s.cluster, "pass": s.pass_, "nodes": s.nodes, "reserved": s.reserved, "nnz_lower": s.nnz_lower,
              "iterations": s.iterations, "rel_residual": s.rel_residual, "seconds": s.seconds, "kernel": s.kernel,
-             "restarts": s.restarts}
+             "restarts": s.restarts, "levels": s.levels}
             for s in r.solves[: r.n_solves]
         ],
         "stage_seconds": list(r.stage_seconds),

@@ -111,7 +111,9 @@ typedef enum {
 typedef enum {
     CICY_PRECOND_JACOBI = 0,  /* M^-1 = 1/diag (Direct_Electrifying.cpp:1662-1668) */
     CICY_PRECOND_LEARNED = 1, /* learned scalings of the chain blocks, chain blocks when they fail to reduce the residual */
-    CICY_PRECOND_CHAIN = 2    /* block-Jacobi over CNT element chains (tridiagonal blocks, explicit inverses) */
+    CICY_PRECOND_CHAIN = 2,   /* block-Jacobi over CNT element chains (tridiagonal blocks, explicit inverses) */
+    CICY_PRECOND_MG = 3       /* chain-aggregation multigrid V-cycle: chain blocks as the fine smoother, one coarse
+                                 unknown per chain block, pairwise aggregation below, dense coarsest inverse */
 } cicy_preconditioner;
 
 typedef struct {
@@ -133,8 +135,10 @@ typedef struct {
     int64_t iterations;       /* CG iterations */
     double rel_residual;      /* FP64 |b - A x| / |b| after the solve */
     double seconds;           /* device time of the solve (CUDA events) */
-    int32_t kernel;           /* 0: grid-wide persistent PCG, 1: cluster-resident PCG */
+    int32_t kernel;           /* 0: grid-wide persistent PCG, 1: cluster-resident PCG, 2: multigrid PCG */
     int32_t restarts;         /* FP64 true-residual restarts taken */
+    int32_t levels;           /* multigrid levels (0 for one-level preconditioners) */
+    int32_t reserved0;
 } cicy_solve_info;
 
 typedef struct {

@@ -16,7 +16,7 @@ def test_struct_sizes_match_header_layout():
     # the ctypes mirrors must have the C layout: spot-check sizes against the field lists
     assert C.sizeof(_abi.Cuboid) == 9 * 8
     assert C.sizeof(_abi.Params) == 8 * 3 + 8 * 4 + 4 * 6 + 8 * 8
-    assert C.sizeof(_abi.SolveInfo) == 4 * 2 + 8 * 6 + 4 * 2
+    assert C.sizeof(_abi.SolveInfo) == 4 * 2 + 8 * 6 + 4 * 4
     assert C.sizeof(_abi.Result) == 8 * 6 + 8 * 2 + 4 * 4 + 32 * C.sizeof(_abi.SolveInfo) + 8 * 6
 
 

@@ -1,0 +1,85 @@
+"""Solver options of the DEA solve (chain block-Jacobi, chain-aggregation
+multigrid) against an FP64 direct solve and against the upstream Jacobi-PCG.
+
+The preconditioners change the iteration, not the system: solved tight, every
+option must give the voltages of the FP64 direct solve within 1e-9 relative
+(on the nodes a prescribed voltage reaches), and at the bench's tolerances the
+same effective resistance as upstream Jacobi-PCG within the CG tolerance.
+"""
+import numpy as np
+import pytest
+from conftest import golden_network
+
+from cicy_geom_b200.device import Context
+from oracle import cicy_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+PRECONDS = {"chain": 2, "mg": 3}
+
+
+def run(net, cfg, preconditioner, tol):
+    cfg.tolerance = tol
+    p = cfg.params()
+    ctx = Context(0)
+    ctx.set_solver(preconditioner=preconditioner)
+    ctx.upload(net)
+    r = ctx.network_to_conductance(p)
+    return ctx, r
+
+
+@pytest.mark.parametrize("pre", list(PRECONDS))
+@pytest.mark.parametrize("name", ["c1p_1200_s1", "c1p_800_s2", "c1p_800_s5", "kat_series", "kat_three_chain"])
+def test_voltages_match_fp64_direct_solve(cuda_ok, name, pre):
+    cfg, net, z = golden_network(name)
+    ctx, r = run(net, cfg, PRECONDS[pre], 1e-14)
+    for i in range(r.n_solves):
+        S = ctx.system(i)
+        if len(S["diag"]) == 0:
+            continue
+        vd = O.solve_direct({**S, "vef": S["voltages"][: S["reserved"]]})
+        m = np.concatenate([np.ones(S["reserved"], bool), O.grounded_mask(S)])
+        rel = np.max(np.abs(S["voltages"][m] - vd[m])) / np.max(np.abs(vd[m]))
+        assert rel < 1e-9, (i, rel)
+        if pre == "mg":
+            assert r.solves[i].kernel == 2 and r.solves[i].levels >= 2
+    ref = O.network_to_conductance(net.arrays(), O.params_from_config(cfg), solver="direct")
+    np.testing.assert_allclose(np.array(r.resistances), ref["resistances"], rtol=1e-9)
+
+
+@pytest.fixture(scope="module")
+def medium(cuda_ok):
+    from cicy_geom_b200.network import NetworkConfig, generate_cnt_network
+
+    cfg = NetworkConfig(side=3.2, n_cnts=8000, seed=1, tolerance=1e-8, tolerance_unit=1e-10)
+    return cfg, generate_cnt_network(cfg).extract_window(cfg)
+
+
+def test_multigrid_matches_jacobi_on_a_medium_network(medium):
+    cfg, net = medium
+    _, rj = run(net, cfg, 0, 1e-8)
+    _, rm = run(net, cfg, 3, 1e-8)
+    assert rm.n_solves == rj.n_solves
+    for sj, sm in zip(rj.solves[: rj.n_solves], rm.solves[: rm.n_solves]):
+        assert sm.nodes == sj.nodes and sm.nnz_lower == sj.nnz_lower
+        assert sm.rel_residual <= 1e-8 * 1.01
+        assert sm.iterations * 4 < sj.iterations
+    np.testing.assert_allclose(rm.resistances[0], rj.resistances[0], rtol=1e-6)
+
+
+def test_multigrid_cluster_and_grid_kernels_agree(medium):
+    """The 16-CTA cluster kernel and the grid-wide kernel run the same iteration."""
+    cfg, net = medium
+    cfg.tolerance = 1e-8
+    out = []
+    for cluster in (True, False):
+        ctx = Context(0)
+        ctx.set_solver(preconditioner=3, cluster=cluster)
+        ctx.upload(net)
+        out.append(ctx.network_to_conductance(cfg.params()))
+    a, b = out
+    for sa, sb in zip(a.solves[: a.n_solves], b.solves[: b.n_solves]):
+        assert sa.kernel == sb.kernel == 2
+        assert abs(sa.iterations - sb.iterations) <= 2
+        assert sa.rel_residual <= 1.01e-8 and sb.rel_residual <= 1.01e-8
+    np.testing.assert_allclose(a.resistances[0], b.resistances[0], rtol=1e-7)
