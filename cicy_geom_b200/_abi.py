@@ -95,7 +95,7 @@ class SolveInfo(C.Structure):
         ("kernel", C.c_int32),
         ("restarts", C.c_int32),
         ("levels", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("fallback", C.c_int32),
     ]
 
 
@@ -111,6 +111,19 @@ class Result(C.Structure):
         ("n_solves", C.c_int32),
         ("solves", SolveInfo * 32),
         ("stage_seconds", C.c_double * 6),
+    ]
+
+
+class GnnSystem(C.Structure):
+    _fields_ = [
+        ("n", C.c_int32),
+        ("nnz", C.c_int32),
+        ("row_ptr", C.c_void_p),
+        ("col_ind", C.c_void_p),
+        ("values", C.c_void_p),
+        ("n_chains", C.c_int32),
+        ("chain_start", C.c_void_p),
+        ("chain_len", C.c_void_p),
     ]
 
 
@@ -178,6 +191,16 @@ def lib() -> C.CDLL:
         "cicy_host_network_view": (C.c_int, [C.c_void_p, P(Network)]),
         "cicy_host_network_free": (None, [C.c_void_p]),
         "cicy_host_last_error": (C.c_char_p, []),
+        "cicy_get_chains": (C.c_int, [C.c_void_p, C.c_int32, i32p, i32p, i32p]),
+        "cicy_gnn_param_count": (C.c_int32, []),
+        "cicy_ctx_set_learned_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int32]),
+        "cicy_gnn_create": (C.c_int, [P(C.c_void_p), C.c_int]),
+        "cicy_gnn_destroy": (C.c_int, [C.c_void_p]),
+        "cicy_gnn_set_system": (C.c_int, [C.c_void_p, P(GnnSystem), C.c_void_p]),
+        "cicy_gnn_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "cicy_gnn_loss_grad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, f64p, C.c_void_p, C.c_void_p]),
+        "cicy_gnn_smooth_probes": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p]),
+        "cicy_gnn_adam": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_float, C.c_void_p]),
         "cicy_jacobi_pcg_static": (C.c_int, [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                              C.c_double, C.c_int64, C.c_void_p, i64p, f64p]),
     }

@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <cstring>
 #include <new>
+#include <string>
 
 #include "ctx.cuh"
 
@@ -337,6 +338,27 @@ cicy_status cicy_get_system(cicy_ctx* ctx, int32_t solve, int64_t* nodes, int64_
         d2h(c, x0, s.x0.get(), n);
         d2h(c, voltages, s.volt.get(), s.nodes);
         sync(c);
+    });
+}
+
+cicy_status cicy_get_chains(cicy_ctx* ctx, int32_t solve, int32_t* n_chains, int32_t* start, int32_t* len) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (solve < 0 || solve >= (int)c.systems.size()) throw cicy::Fail{CICY_E_INPUT, "no such solve"};
+        const cicy::DeaSystem& s = *c.systems[solve];
+        const int m = (int)s.h_chain_start.size();
+        if (n_chains) *n_chains = m;
+        if (start) std::memcpy(start, s.h_chain_start.data(), sizeof(int32_t) * m);
+        if (len) std::memcpy(len, s.h_chain_len.data(), sizeof(int32_t) * m);
+    });
+}
+
+cicy_status cicy_ctx_set_learned_params(cicy_ctx* ctx, const float* params, int32_t n) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (!params || n != cicy::gnn_param_count())
+            throw cicy::Fail{CICY_E_INPUT, "cicy_ctx_set_learned_params: expected " + std::to_string(cicy::gnn_param_count()) + " parameters"};
+        c.gnn_params.ensure(n);
+        CICY_CUDA(cudaMemcpyAsync(c.gnn_params.get(), params, sizeof(float) * n, cudaMemcpyHostToDevice, c.stream));
+        CICY_CUDA(cudaStreamSynchronize(c.stream));
     });
 }
 

@@ -25,6 +25,8 @@ struct DeaSystem {
     int restarts = 0;
     bool cluster_solver = false;
     int mg_levels = 0;
+    int fallback = 0;  // 1: the learned preconditioner failed and Jacobi-PCG solved the system
+    std::vector<int32_t> h_chain_start, h_chain_len;
     double rel_residual = 0, seconds = 0;
     // device: strict-lower CSR of the free block (SSS), diagonal, rhs, x0, voltages (all nodes)
     DBuf<int32_t> row_ptr, col;
@@ -114,6 +116,8 @@ struct Ctx {
     std::vector<int32_t> bb_clu_len, bb_cj_len;
     DBuf<int32_t> chain_start, chain_len;
     SolverWork sw;
+    GnnState gnn;
+    DBuf<float> gnn_params;  // learned preconditioner parameters (cicy_ctx_set_learned_params)
 
     ~Ctx();
 };
@@ -124,9 +128,8 @@ void run_contact_grid(Ctx& c, const cicy_params& p);
 void run_clusters(Ctx& c, const cicy_params& p);
 void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out);
 
-// Learned preconditioner scalings for the system being solved (learned.cu).
-void learned_scalings(Ctx& c, const cicy_params& p, const SolverSystem& ss, int n_chains, int r_flag, const float** node_scale,
-                      const float** edge_scale);
+// Learned preconditioner: edge weights for the system being solved (learned.cu).
+const float* learned_edge_weights(Ctx& c, const SolverSystem& ss, int n_chains, cudaStream_t s);
 
 // Helpers shared across translation units.
 int32_t read_i32(Ctx& c, const int32_t* dptr);

@@ -224,6 +224,49 @@ __device__ __forceinline__ double apply_precond(const PcgArgs& a, int i) {
     }
 }
 
+// z = M^-1 r on this CTA's rows, accumulating r.r and r.z.  The SPAI form needs
+// y = T^-1 r of neighbouring rows in other CTAs: one extra grid barrier.
+template <int PRE, bool MIXED>
+__device__ __forceinline__ bool precond_all(const PcgArgs& a, int r_lo, int r_hi, double& rr_l, double& rz_l) {
+    if constexpr (PRE == PRECOND_KIND_SPAI) {
+        for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
+            const int off = a.row_off[i], base = a.row_base[i], m = a.row_m[i];
+            double s = 0;
+            for (int j = 0; j < m; j++) s += a.tinv[off + j] * a.r[base + j];
+            a.y[i] = s;
+        }
+        if (!grid_sync(a.bar, gridDim.x, a.err)) return false;
+        for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
+            double s = 0;
+            for (int k = a.rp[i]; k < a.rp[i + 1]; k++) {
+                const float w = a.ew[k];
+                if (w != 0.0f) s += (double)w * (-a.val[k]) * __ldcg(&a.y[a.ci[k]]);
+            }
+            a.u[i] = s;
+        }
+        __syncthreads();
+        for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
+            const int off = a.row_off[i], base = a.row_base[i], m = a.row_m[i];
+            double s = a.y[i];
+            for (int j = 0; j < m; j++) s += a.tinv[off + j] * a.u[base + j];
+            a.z[i] = s;
+            const double ri = a.r[i];
+            rr_l += ri * ri;
+            rz_l += ri * s;
+        }
+        return true;
+    } else {
+        for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
+            double zi = apply_precond<PRE, MIXED>(a, i);
+            if (MIXED) a.z32[i] = (float)zi; else a.z[i] = zi;
+            double ri = a.r[i];
+            rr_l += ri * ri;
+            rz_l += ri * zi;
+        }
+        return true;
+    }
+}
+
 template <bool MIXED>
 __device__ __forceinline__ double spmv_row_z(const PcgArgs& a, int i) {
     if (MIXED) {
@@ -243,13 +286,7 @@ __global__ void __launch_bounds__(kCgThreads) k_pcg(PcgArgs a) {
     const int r_lo = a.cta_row[blockIdx.x], r_hi = a.cta_row[blockIdx.x + 1];
     // ---- start: r = b - A x0 given; z = M r; partials r.r, r.z
     double rr_l = 0, rz_l = 0;
-    for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
-        double zi = apply_precond<PRE, MIXED>(a, i);
-        if (MIXED) a.z32[i] = (float)zi; else a.z[i] = zi;
-        double ri = a.r[i];
-        rr_l += ri * ri;
-        rz_l += ri * zi;
-    }
+    if (!precond_all<PRE, MIXED>(a, r_lo, r_hi, rr_l, rz_l)) return;
     double s0, s1;
     block_reduce2(rr_l, rz_l, sm, s0, s1);
     if (threadIdx.x == 0) { a.partA[2 * blockIdx.x] = s0; a.partA[2 * blockIdx.x + 1] = s1; }
@@ -301,13 +338,7 @@ __global__ void __launch_bounds__(kCgThreads) k_pcg(PcgArgs a) {
         __syncthreads();  // the block preconditioner reads r of this CTA's other rows
         rr_l = 0;
         rz_l = 0;
-        for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
-            double zi = apply_precond<PRE, MIXED>(a, i);
-            if (MIXED) a.z32[i] = (float)zi; else a.z[i] = zi;
-            double ri = a.r[i];
-            rr_l += ri * ri;
-            rz_l += ri * zi;
-        }
+        if (!precond_all<PRE, MIXED>(a, r_lo, r_hi, rr_l, rz_l)) return;
         block_reduce2(rr_l, rz_l, sm, s0, s1);
         if (threadIdx.x == 0) { a.partA[2 * blockIdx.x] = s0; a.partA[2 * blockIdx.x + 1] = s1; }
         if (!grid_sync(a.bar, nb, a.err)) return;
@@ -327,13 +358,7 @@ __global__ void __launch_bounds__(kCgThreads) k_pcg(PcgArgs a) {
             }
             __syncthreads();
             rz_l = 0;
-            for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
-                double zi = apply_precond<PRE, MIXED>(a, i);
-                if (MIXED) a.z32[i] = (float)zi; else a.z[i] = zi;
-                double ri = a.r[i];
-                rr_l += ri * ri;
-                rz_l += ri * zi;
-            }
+            if (!precond_all<PRE, MIXED>(a, r_lo, r_hi, rr_l, rz_l)) return;
             block_reduce2(rr_l, rz_l, sm, s0, s1);
             if (threadIdx.x == 0) { a.partA[2 * blockIdx.x] = s0; a.partA[2 * blockIdx.x + 1] = s1; }
             if (!grid_sync(a.bar, nb, a.err)) return;
@@ -410,7 +435,8 @@ void build_block_preconditioner(SolverWork& w, const SolverSystem& sys, int ncha
 }
 
 void pcg_solve(SolverWork& w, const SolverSystem& sys, int precond, bool mixed, double tol, long long max_iter, int num_sms,
-               int* status, cudaStream_t s, int64_t& launches, PcgStats& st) {
+               int* status, cudaStream_t s, int64_t& launches, PcgStats& st, const float* ew) {
+    if (precond == PRECOND_KIND_SPAI && (mixed || !ew)) throw Fail{CICY_E_INTERNAL, "SPAI preconditioner: FP64 only, weights required"};
     const int n = sys.n;
     st = PcgStats{};
     if (n <= 0) return;
@@ -437,6 +463,7 @@ void pcg_solve(SolverWork& w, const SolverSystem& sys, int precond, bool mixed, 
     // CTA row ranges
     int cap = 0;
     if (precond == PRECOND_KIND_JACOBI) cap = mixed ? max_coop_blocks<PRECOND_KIND_JACOBI, true>(num_sms) : max_coop_blocks<PRECOND_KIND_JACOBI, false>(num_sms);
+    else if (precond == PRECOND_KIND_SPAI) cap = max_coop_blocks<PRECOND_KIND_SPAI, false>(num_sms);
     else cap = mixed ? max_coop_blocks<PRECOND_KIND_BLOCK, true>(num_sms) : max_coop_blocks<PRECOND_KIND_BLOCK, false>(num_sms);
     const int nb = std::max(1, std::min({cap, num_sms, ceil_div(n, kCgThreads)}));
     w.cta_row.ensure(nb + 1);
@@ -457,6 +484,13 @@ void pcg_solve(SolverWork& w, const SolverSystem& sys, int precond, bool mixed, 
     a.tinv = w.tinv.get(); a.tinv32 = w.tinv32.get();
     a.row_off = w.row_off.get(); a.row_base = w.row_base.get(); a.row_m = w.row_m.get();
     a.cta_row = w.cta_row.get();
+    if (precond == PRECOND_KIND_SPAI) {
+        w.y.ensure(n);
+        w.u.ensure(n);
+        a.y = w.y.get();
+        a.u = w.u.get();
+        a.ew = ew;
+    }
     a.partA = w.part.get(); a.partB = w.part.get() + 2 * nb;
     a.stats = w.stats.get();
     a.bar = GridBarrier{w.barrier.get(), w.barrier.get() + 1};
@@ -471,6 +505,8 @@ void pcg_solve(SolverWork& w, const SolverSystem& sys, int precond, bool mixed, 
     CICY_CUDA(cudaEventRecord(e0, s));
     if (precond == PRECOND_KIND_JACOBI) {
         if (mixed) launch_pcg<PRECOND_KIND_JACOBI, true>(a, nb, s); else launch_pcg<PRECOND_KIND_JACOBI, false>(a, nb, s);
+    } else if (precond == PRECOND_KIND_SPAI) {
+        launch_pcg<PRECOND_KIND_SPAI, false>(a, nb, s);
     } else {
         if (mixed) launch_pcg<PRECOND_KIND_BLOCK, true>(a, nb, s); else launch_pcg<PRECOND_KIND_BLOCK, false>(a, nb, s);
     }

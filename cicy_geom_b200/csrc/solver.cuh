@@ -1,6 +1,8 @@
 // Preconditioned CG for DEA systems (see solver.cu).
 #pragma once
 
+#include <cuda_bf16.h>
+
 #include <vector>
 
 #include "dev_common.cuh"
@@ -10,7 +12,7 @@ namespace cicy {
 constexpr int kBlockMax = 32;  // largest block of the chain block-Jacobi preconditioner
 constexpr int kClusterCtas = 16;                // CTAs of the cluster-resident solver (non-portable cluster size)
 constexpr int kClusterSmemMax = 232448 - 1024;  // dynamic shared memory per CTA it may use
-enum PrecondKind : int { PRECOND_KIND_JACOBI = 0, PRECOND_KIND_BLOCK = 1 };
+enum PrecondKind : int { PRECOND_KIND_JACOBI = 0, PRECOND_KIND_BLOCK = 1, PRECOND_KIND_SPAI = 2 };
 
 // A free-node system in full symmetric CSR (diagonal included).
 struct SolverSystem {
@@ -40,6 +42,9 @@ struct PcgArgs {
     const float* tinv32;
     const int32_t *row_off, *row_base, *row_m;
     const int32_t* cta_row;
+    const float* ew;  // learned weights of the couplings outside the blocks (SPAI), 0 elsewhere
+    double* y;        // SPAI: T^-1 r
+    double* u;        // SPAI: E_w T^-1 r
     double* partA;
     double* partB;
     double* stats;
@@ -117,7 +122,35 @@ struct SolverWork {
     DBuf<unsigned int> barrier;
     int n_blocks = 0, block_entries = 0;
     MgWork mg;
+    DBuf<double> y, u;
 };
+
+// ---- learned preconditioner (learned.cu) ----
+struct GnnState {
+    int n = 0, nnz = 0;
+    const int32_t* rp = nullptr;
+    const int32_t* ci = nullptr;
+    const double* val = nullptr;
+    SolverWork sw;  // chain blocks of the system
+    DBuf<int> status;
+    DBuf<double> diag, logd, ms, vr, vy, vu, vz, vq, vd, vl, dw, part, coef;
+    DBuf<float> deg, f, invdeg, lc, jf, A0, HW, w, dout, dH0, dH1, dA, dM, dG;
+    DBuf<float> A[3];
+    DBuf<__nv_bfloat16> H[4], G[3];
+    DBuf<int32_t> chain, blk, tr;
+    DBuf<uint8_t> offb;
+};
+
+int gnn_param_count();
+// Features, chain blocks and buffers for one system (full symmetric CSR, columns ascending).
+void gnn_set_system(GnnState& g, int n, int nnz, const int32_t* rp, const int32_t* ci, const double* val, int nchains,
+                    const int32_t* cs, const int32_t* cl, cudaStream_t s, int64_t& launches);
+// Network forward: g.w holds the weight of every coupling outside the blocks (0 elsewhere).
+void gnn_forward(GnnState& g, const float* params, cudaStream_t s, int64_t& launches);
+// Mean loss over K probe vectors (K x n, FP64) and its gradient (overwrites grad).
+double gnn_loss_grad(GnnState& g, const float* params, int K, const double* probes, float* grad, cudaStream_t s, int64_t& launches);
+void gnn_smooth_probes(GnnState& g, int K, double* u, int sweeps, cudaStream_t s, int64_t& launches);
+void gnn_adam(float* p, const float* grad, float* m, float* v, int n, int step, float lr, cudaStream_t s);
 
 __global__ void k_residual(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const double* __restrict__ v,
                            const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ r);
@@ -149,7 +182,8 @@ void build_mg_hierarchy(SolverWork& w, const SolverSystem& sys, cudaStream_t s, 
 void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long max_iter, bool allow_cluster, int num_sms, int* status,
                   cudaStream_t s, int64_t& launches, PcgStats& st);
 
+// precond PRECOND_KIND_SPAI needs the block preconditioner and `ew` (learned weights per entry).
 void pcg_solve(SolverWork& w, const SolverSystem& sys, int precond, bool mixed, double tol, long long max_iter, int num_sms,
-               int* status, cudaStream_t s, int64_t& launches, PcgStats& st);
+               int* status, cudaStream_t s, int64_t& launches, PcgStats& st, const float* ew = nullptr);
 
 }  // namespace cicy

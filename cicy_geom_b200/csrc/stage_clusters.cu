@@ -567,6 +567,7 @@ void upload_network(Ctx& c, const cicy_network& n) {
 void run_contact_grid(Ctx& c, const cicy_params& p) {
     if (c.stage < 1) throw Fail{CICY_E_STATE, "cicy_contact_grid: no network uploaded"};
     cudaStream_t s = c.stream;
+    CICY_TRACE("contact_grid", s);
     const cicy_cuboid& w = c.window;
     // Generate_contact_grid + Adjust_regions_if_needed (Contact_grid.cpp:18-102)
     GridGeom& g = c.grid;
@@ -621,6 +622,7 @@ void run_contact_grid(Ctx& c, const cicy_params& p) {
 void run_clusters(Ctx& c, const cicy_params& p) {
     if (c.stage < 2) throw Fail{CICY_E_STATE, "cicy_clusters: run cicy_contact_grid first"};
     cudaStream_t s = c.stream;
+    CICY_TRACE("clusters", s);
     const int S = c.n_slots, NC = std::max(c.n_cnts, 1), NP = std::max(c.n_points, 1);
     // ---- pair tests ----
     int cap = std::max(1 << 16, S / 4);

@@ -702,11 +702,20 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
         ss.x = c.cg_x.get();
         const bool mixed = c.solver.precision == CICY_PRECISION_MIXED;
         int kind = PRECOND_KIND_JACOBI;
-        const float* ns = nullptr;
-        const float* es = nullptr;
-        if (c.solver.preconditioner != CICY_PRECOND_JACOBI && n > 0) {
+        const float* ew = nullptr;
+        if (c.solver.preconditioner == CICY_PRECOND_LEARNED && n > 0) {
+            kind = PRECOND_KIND_SPAI;
+            ew = learned_edge_weights(c, ss, NM, s);
+            tr.mark(r_flag ? "dea.real.gnn" : "dea.unit.gnn");
+        } else if (c.solver.preconditioner != CICY_PRECOND_JACOBI && n > 0) {
             kind = PRECOND_KIND_BLOCK;
-            if (c.solver.preconditioner == CICY_PRECOND_LEARNED) learned_scalings(c, p, ss, NM, r_flag, &ns, &es);
+        }
+        // host copy of the chains, for cicy_get_chains
+        sys->h_chain_start.resize(NM);
+        sys->h_chain_len.resize(NM);
+        if (NM > 0) {
+            CICY_CUDA(cudaMemcpyAsync(sys->h_chain_start.data(), c.chain_start.get(), sizeof(int32_t) * NM, cudaMemcpyDeviceToHost, s));
+            CICY_CUDA(cudaMemcpyAsync(sys->h_chain_len.data(), c.chain_len.get(), sizeof(int32_t) * NM, cudaMemcpyDeviceToHost, s));
         }
         PcgStats st;
         const double tol = (r_flag == 0 && p.tolerance_unit > 0) ? p.tolerance_unit : p.tolerance;
@@ -716,39 +725,57 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
         bool solved = false;
         if (c.solver.preconditioner == CICY_PRECOND_MG && n > 0) {
             build_block_preconditioner(c.sw, ss, NM, c.chain_start.get(), c.chain_len.get(), nullptr, nullptr, false, s, c.launches);
+            tr.mark(r_flag ? "dea.real.blocks" : "dea.unit.blocks");
             build_mg_hierarchy(c.sw, ss, s, c.launches);
+            tr.mark(r_flag ? "dea.real.mg_setup" : "dea.unit.mg_setup");
             pcg_solve_mg(c.sw, ss, tol, max_iter, !(c.solver.flags & CICY_SOLVER_NO_CLUSTER), c.num_sms, c.status.get(), s, c.launches,
                          st);
             solved = true;
         }
-        if (!solved && !mixed && !(c.solver.flags & CICY_SOLVER_NO_CLUSTER))
-            solved = pcg_solve_cluster(c.sw, ss, kind == PRECOND_KIND_BLOCK, ns, es, NM, c.chain_start.get(), c.chain_len.get(), tol,
-                                       max_iter, s, c.launches, st);
+        if (!solved && kind != PRECOND_KIND_SPAI && !mixed && !(c.solver.flags & CICY_SOLVER_NO_CLUSTER))
+            solved = pcg_solve_cluster(c.sw, ss, kind == PRECOND_KIND_BLOCK, nullptr, nullptr, NM, c.chain_start.get(), c.chain_len.get(),
+                                       tol, max_iter, s, c.launches, st);
         if (!solved) {
-            if (kind == PRECOND_KIND_BLOCK)
-                build_block_preconditioner(c.sw, ss, NM, c.chain_start.get(), c.chain_len.get(), ns, es, mixed, s, c.launches);
-            pcg_solve(c.sw, ss, kind, mixed, tol, max_iter, c.num_sms, c.status.get(), s, c.launches, st);
+            if (kind != PRECOND_KIND_JACOBI)
+                build_block_preconditioner(c.sw, ss, NM, c.chain_start.get(), c.chain_len.get(), nullptr, nullptr, mixed, s, c.launches);
+            pcg_solve(c.sw, ss, kind, mixed, tol, max_iter, c.num_sms, c.status.get(), s, c.launches, st, ew);
         }
         check_status(c, "Solve_DEA_equations_CG_SSS");
+        tr.mark(r_flag ? "dea.real.cg" : "dea.unit.cg");
+        // true FP64 residual |b - A x| / |b|
+        auto true_residual = [&]() {
+            double rb[2] = {0, 0};
+            if (n > 0) {
+                c.cg_scal.ensure(4);
+                CICY_CUDA(cudaMemsetAsync(c.cg_scal.get(), 0, sizeof(double) * 2, s));
+                k_true_residual<<<grid_for(n), 256, 0, s>>>(n, c.cg_rp.get(), c.cg_ci.get(), c.cg_val.get(), c.cg_x.get(), sys->b.get(),
+                                                          c.cg_scal.get());
+                c.launches++;
+                CICY_CUDA(cudaMemcpyAsync(rb, c.cg_scal.get(), sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+                CICY_CUDA(cudaStreamSynchronize(s));
+            }
+            return rb[1] > 0 ? std::sqrt(rb[0] / rb[1]) : 0.0;
+        };
+        double rel = true_residual();
+        if (kind == PRECOND_KIND_SPAI && !(rel <= 10 * tol && st.iterations < max_iter)) {
+            // the learned preconditioner did not reduce the residual: Jacobi-PCG from the initial guess
+            const double seconds = st.seconds;
+            CICY_CUDA(cudaMemcpyAsync(c.cg_x.get(), sys->x0.get(), sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+            pcg_solve(c.sw, ss, PRECOND_KIND_JACOBI, false, tol, max_iter, c.num_sms, c.status.get(), s, c.launches, st);
+            check_status(c, "Solve_DEA_equations_CG_SSS (Jacobi fallback)");
+            st.seconds += seconds;
+            sys->fallback = 1;
+            rel = true_residual();
+        }
         sys->cluster_solver = st.cluster;
         sys->mg_levels = st.levels;
         sys->seconds = st.seconds;
         sys->iterations = st.iterations;
         sys->restarts = st.restarts;
-        tr.mark(r_flag ? "dea.real.cg" : "dea.unit.cg");
-        // true FP64 residual |b - A x| / |b|
-        double rb[2] = {0, 0};
-        if (n > 0) {
-            c.cg_scal.ensure(4);
-            CICY_CUDA(cudaMemsetAsync(c.cg_scal.get(), 0, sizeof(double) * 2, s));
-            k_true_residual<<<grid_for(n), 256, 0, s>>>(n, c.cg_rp.get(), c.cg_ci.get(), c.cg_val.get(), c.cg_x.get(), sys->b.get(), c.cg_scal.get());
-            c.launches++;
-            CICY_CUDA(cudaMemcpyAsync(rb, c.cg_scal.get(), sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
-        }
         k_voltages<<<grid_for(nodes), 256, 0, s>>>(nodes, reserved, c.vef.get(), c.cg_x.get(), sys->volt.get());
         c.launches++;
         CICY_CUDA(cudaStreamSynchronize(s));
-        sys->rel_residual = rb[1] > 0 ? std::sqrt(rb[0] / rb[1]) : 0.0;
+        sys->rel_residual = rel;
     } catch (...) {
         delete sys;
         throw;
@@ -802,6 +829,7 @@ void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out) {
         DeaSystem* su = solve_dea(c, p, u, eb, ee);
         c.systems.push_back(su);
         t_unit += su->seconds;
+        TraceSeq trb(s);
         // ---- backbone ----
         cudaEvent_t e0, e1;
         CICY_CUDA(cudaEventCreate(&e0));
@@ -838,6 +866,7 @@ void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out) {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         if (scope != 0) continue;
+        trb.mark("backbone");
         // ---- real-resistor passes per percolated direction (Electrical_analysis.cpp:229-289) ----
         std::vector<int> dirs;
         const int fam = c.h_family[k];
@@ -867,6 +896,7 @@ void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out) {
             CICY_CUDA(cudaMemcpyAsync(&I, c.cur_out.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
             CICY_CUDA(cudaStreamSynchronize(s));
             parallel[d].push_back(p.applied_voltage / I);
+            trb.mark("boundary_current");
         }
     }
     c.h_bbclu_ptr.assign(c.n_perc + 1, 0);
@@ -915,6 +945,7 @@ void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out) {
             si.seconds = sy->seconds;
             si.kernel = sy->mg_levels > 0 ? 2 : sy->cluster_solver ? 1 : 0;
             si.levels = sy->mg_levels;
+            si.fallback = sy->fallback;
             si.restarts = sy->restarts;
         }
         out->stage_seconds[2] = t_unit;

@@ -33,6 +33,7 @@ class Context:
         h = C.c_void_p()
         check(lib().cicy_ctx_create(C.byref(h), device), "cicy_ctx_create")
         self._h = h
+        self._learned = False
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
@@ -70,6 +71,17 @@ class Context:
         cluster: allow the cluster-resident solver for systems that fit in shared memory."""
         o = _abi.SolverOpts(precision, preconditioner, max_iter_factor, 0 if cluster else 1)
         self._check(lib().cicy_ctx_set_solver(self._h, C.byref(o)), "cicy_ctx_set_solver")
+        if preconditioner == 1 and not self._learned:
+            from .learned import default_params
+
+            self.set_learned_params(default_params())
+
+    def set_learned_params(self, params: np.ndarray):
+        """Parameters of the learned preconditioner (flat float32 vector, cicy_gnn_param_count entries)."""
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        self._check(lib().cicy_ctx_set_learned_params(self._h, p.ctypes.data_as(C.POINTER(C.c_float)), len(p)),
+                    "cicy_ctx_set_learned_params")
+        self._learned = True
 
     def kernel_launches(self) -> int:
         return int(lib().cicy_ctx_kernel_launches(self._h))
@@ -156,6 +168,14 @@ class Context:
                     "get_clusters")
         return {"ptr": ptr, "idx": idx[: ni.value], "family": fam[:K], "junc_ptr": jptr, "junc_idx": jidx[: nj.value]}
 
+    def chains(self, solve: int):
+        """(start, len) of the CNT chains of a solve's system."""
+        m = C.c_int32()
+        self._check(lib().cicy_get_chains(self._h, solve, C.byref(m), None, None), "get_chains")
+        st, ln = np.zeros(max(m.value, 1), np.int32), np.zeros(max(m.value, 1), np.int32)
+        self._check(lib().cicy_get_chains(self._h, solve, C.byref(m), _p(st, C.c_int32), _p(ln, C.c_int32)), "get_chains")
+        return st[: m.value], ln[: m.value]
+
     def system(self, solve: int) -> dict:
         nodes, res, m = C.c_int64(), C.c_int64(), C.c_int64()
         self._check(lib().cicy_get_system(self._h, solve, C.byref(nodes), C.byref(res), C.byref(m), None, None, None, None, None,
@@ -185,7 +205,7 @@ def result_dict(r: _abi.Result) -> dict:
         "solves": [
             {"cluster": s.cluster, "pass": s.pass_, "nodes": s.nodes, "reserved": s.reserved, "nnz_lower": s.nnz_lower,
              "iterations": s.iterations, "rel_residual": s.rel_residual, "seconds": s.seconds, "kernel": s.kernel,
-             "restarts": s.restarts, "levels": s.levels}
+             "restarts": s.restarts, "levels": s.levels, "fallback": s.fallback}
             for s in r.solves[: r.n_solves]
         ],
         "stage_seconds": list(r.stage_seconds),

@@ -110,7 +110,8 @@ typedef enum {
 
 typedef enum {
     CICY_PRECOND_JACOBI = 0,  /* M^-1 = 1/diag (Direct_Electrifying.cpp:1662-1668) */
-    CICY_PRECOND_LEARNED = 1, /* learned scalings of the chain blocks, chain blocks when they fail to reduce the residual */
+    CICY_PRECOND_LEARNED = 1, /* chain blocks plus a learned sparse approximate inverse T^-1 + T^-1 E_w T^-1 (graph network
+                                 weights w on the couplings outside the blocks); Jacobi-PCG when it fails to converge */
     CICY_PRECOND_CHAIN = 2,   /* block-Jacobi over CNT element chains (tridiagonal blocks, explicit inverses) */
     CICY_PRECOND_MG = 3       /* chain-aggregation multigrid V-cycle: chain blocks as the fine smoother, one coarse
                                  unknown per chain block, pairwise aggregation below, dense coarsest inverse */
@@ -138,7 +139,7 @@ typedef struct {
     int32_t kernel;           /* 0: grid-wide persistent PCG, 1: cluster-resident PCG, 2: multigrid PCG */
     int32_t restarts;         /* FP64 true-residual restarts taken */
     int32_t levels;           /* multigrid levels (0 for one-level preconditioners) */
-    int32_t reserved0;
+    int32_t fallback;         /* 1: the learned preconditioner did not reach the tolerance; Jacobi-PCG solved it */
 } cicy_solve_info;
 
 typedef struct {
@@ -207,6 +208,46 @@ cicy_status cicy_get_clusters(cicy_ctx* ctx, int32_t which, int32_t* n_clusters,
 cicy_status cicy_get_system(cicy_ctx* ctx, int32_t solve, int64_t* nodes, int64_t* reserved, int64_t* nnz_lower,
                             int64_t* row_ptr, int64_t* col_ind, double* values, double* diag, double* b, double* x0,
                             double* voltages);
+
+/* Chains (consecutive free nodes of one CNT) of a solve's system: start node and
+ * length of each, in the order of the system's CNTs. */
+cicy_status cicy_get_chains(cicy_ctx* ctx, int32_t solve, int32_t* n_chains, int32_t* start, int32_t* len);
+
+/* ---------------- learned preconditioner (no upstream counterpart) ----------------
+ * A graph network (3 message-passing layers, width 32, BF16 weights and
+ * activations, FP32 accumulation) that weights the couplings left out by the
+ * chain block-Jacobi T, giving M^-1 = T^-1 + T^-1 E_w T^-1.  Parameters are one
+ * flat FP32 vector of cicy_gnn_param_count() entries.  The training entry points
+ * take device pointers and a cudaStream_t (as void*); systems are full symmetric
+ * CSR with ascending columns, diagonal included. */
+int32_t cicy_gnn_param_count(void);
+/* Parameters the solver uses for CICY_PRECOND_LEARNED (host array, copied). */
+cicy_status cicy_ctx_set_learned_params(cicy_ctx* ctx, const float* params, int32_t n);
+
+typedef struct cicy_gnn cicy_gnn;
+typedef struct {
+    int32_t n, nnz;
+    const int32_t* row_ptr;   /* device, n + 1 */
+    const int32_t* col_ind;   /* device, nnz */
+    const double* values;     /* device, nnz */
+    int32_t n_chains;
+    const int32_t* chain_start; /* device */
+    const int32_t* chain_len;   /* device */
+} cicy_gnn_system;
+cicy_status cicy_gnn_create(cicy_gnn** out, int device);
+cicy_status cicy_gnn_destroy(cicy_gnn* g);
+/* Features and chain blocks of one system (kept until the next call). */
+cicy_status cicy_gnn_set_system(cicy_gnn* g, const cicy_gnn_system* sys, void* stream);
+/* Forward pass: weight of every matrix entry (0 on the blocks and the diagonal) into w[nnz] (device). */
+cicy_status cicy_gnn_forward(cicy_gnn* g, const float* params, float* w, void* stream);
+/* Mean loss 1 - (r.Az)^2/(|r|^2 |Az|^2), r = A u, z = M^-1 r, over n_probes probe
+ * vectors u (device, n_probes x n, FP64), and its gradient grad[param_count] (device, overwritten). */
+cicy_status cicy_gnn_loss_grad(cicy_gnn* g, const float* params, int32_t n_probes, const double* probes, double* loss, float* grad,
+                               void* stream);
+/* u <- u - 0.9 T^-1 A u, `sweeps` times, on each probe vector (leaves the modes the blocks handle worst). */
+cicy_status cicy_gnn_smooth_probes(cicy_gnn* g, int32_t n_probes, double* probes, int32_t sweeps, void* stream);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) on device arrays of n floats; step counts from 1. */
+cicy_status cicy_gnn_adam(float* params, const float* grad, float* m, float* v, int32_t n, int32_t step, float lr, void* stream);
 
 /* ---------------- host-side network sources (CPU, upstream of the hot path) ---------------- */
 /* Seeded synthetic CNT network (no upstream counterpart; emits the same layout
