@@ -120,3 +120,48 @@ def test_training_on_the_gpu_reduces_the_loss(sys1):
     after = LO.loss_and_grad(theta.astype(np.float64), S, probes)[0]
     assert np.all(np.isfinite(theta)) and len(hist) == 80
     assert after < before, (before, after)
+
+
+@pytest.fixture(scope="module")
+def held_out(cuda_ok):
+    # seeds outside the training set of the shipped parameters (5,000,000 + k)
+    return LG.training_networks(2, seed0=6_000_000)
+
+
+def solve_real(cfg, net, preconditioner, params=None, cluster=False, max_iter_factor=300):
+    ctx = Context(0)
+    ctx.upload(net)
+    ctx.set_solver(preconditioner=preconditioner, cluster=cluster, max_iter_factor=max_iter_factor)
+    if params is not None:
+        ctx.set_learned_params(params)
+    r = ctx.network_to_conductance(cfg.params())
+    return r, [s for s in r.solves[: r.n_solves] if s.pass_ >= 0]
+
+
+def test_trained_network_gains_over_the_blocks_without_it(held_out):
+    """Same grid-wide PCG kernel, same chain blocks: with the trained network's
+    sparse-approximate-inverse term the real-resistor solves take clearly fewer
+    iterations, and far fewer than upstream Jacobi-PCG; same resistance."""
+    for cfg, net in held_out:
+        rj, sj = solve_real(cfg, net, 0)
+        rc, sc = solve_real(cfg, net, 2)
+        rl, sl = solve_real(cfg, net, 1)
+        for j, c, l in zip(sj, sc, sl):
+            assert l.kernel == 0 and c.kernel == 0 and l.fallback == 0
+            assert l.rel_residual <= 1.01 * cfg.tolerance
+            assert l.iterations * 1.4 < c.iterations, (l.iterations, c.iterations)
+            assert l.iterations * 10 < j.iterations, (l.iterations, j.iterations)
+        np.testing.assert_allclose(rl.resistances[0], rj.resistances[0], rtol=1e-6)
+
+
+def test_jacobi_fallback_when_the_learned_preconditioner_fails():
+    """Parameters that make the network output NaN: the solve falls back to
+    Jacobi-PCG from the initial guess and still meets the tolerance."""
+    cfg, net, z = golden_network("c1p_800_s2")
+    bad = LG.init_params(0)
+    bad[:] = np.nan
+    r, s = solve_real(cfg, net, 1, params=bad, max_iter_factor=20)
+    assert all(x.fallback == 1 for x in s)
+    assert all(x.rel_residual <= 1.01 * cfg.tolerance for x in s)
+    ref = O.network_to_conductance(net.arrays(), O.params_from_config(cfg), solver="direct")
+    np.testing.assert_allclose(np.array(r.resistances), ref["resistances"], rtol=1e-6)

@@ -59,3 +59,13 @@ def test_preconditioner_is_symmetric_positive_definite(small_system):
     for _ in range(4):
         r = rng.normal(size=S.n)
         assert LO.precond(S, w, r)[0] @ r > 0
+
+
+def test_shipped_parameters_match_the_library_layout():
+    from cicy_geom_b200 import learned as LG
+
+    p = LG.default_params()
+    assert len(p) == LG.param_count() == LO.n_params()
+    assert np.all(np.isfinite(p))
+    assert len(LG.init_params(0)) == LO.n_params()
+    np.testing.assert_allclose(LG.init_params(0)[-2:], [0.0, np.log(4.0)], rtol=1e-6)
