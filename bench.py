@@ -49,7 +49,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--precond", default="chain", choices=["jacobi", "chain", "learned", "mg"])
+    ap.add_argument("--precond", default="mg", choices=["jacobi", "chain", "learned", "mg"])
+    ap.add_argument("--no-comparison", action="store_true", help="skip the per-preconditioner comparison and the SpMV measurement")
     # a smaller network of the same generator, for profiler captures (the bench line names the size it ran)
     ap.add_argument("--side", type=float, default=SIDE)
     ap.add_argument("--cnts", type=int, default=N_CNTS)
@@ -88,6 +89,11 @@ class ClockSampler:
                                           "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # nvidia-smi's start-up takes the driver for a while: let it finish before the timed region
+            t0 = time.time()
+            while not self.rows and time.time() - t0 < 5.0 and self.proc.poll() is None:
+                time.sleep(0.05)
+            self.rows.clear()
         except FileNotFoundError:
             self.proc = None
         return self
@@ -232,6 +238,83 @@ def cg_bytes(nodes, reserved, nnz_lower, iters, s_val=8, s_v=8):
     return iters * (b_spmv + 12 * s_v * n)
 
 
+def solver_comparison(cfg, net, device, steps=2):
+    """The same network step with each preconditioner (device-resident, CUDA events):
+    upstream Jacobi-PCG ("plain CG"), chain block-Jacobi, learned, multigrid."""
+    import ctypes as C
+
+    import torch
+
+    from cicy_geom_b200._abi import Result, check, lib
+    from cicy_geom_b200.device import Context
+
+    out = {}
+    for name in ("jacobi", "chain", "learned", "mg"):
+        ctx = Context(device)
+        ctx.set_solver(preconditioner=PRECONDS[name])
+        ctx.upload(net)
+        params = cfg.params()
+        res = Result()
+        stream = torch.cuda.ExternalStream(ctx.stream(), device=device)
+        check(lib().cicy_network_to_conductance(ctx.handle, C.byref(params), C.byref(res)), "warm-up", ctx.handle)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            check(lib().cicy_network_to_conductance(ctx.handle, C.byref(params), C.byref(res)), name, ctx.handle)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) * 1e-3 / steps
+        sv = res.solves[: res.n_solves]
+        out[name] = {"networks_per_s": 1.0 / t, "ms_per_step": t * 1e3, "cg_iterations": [int(x.iterations) for x in sv],
+                     "cg_ms": [round(x.seconds * 1e3, 3) for x in sv], "fallback": [int(x.fallback) for x in sv],
+                     "max_rel_residual": max(x.rel_residual for x in sv), "R_x": res.resistances[0]}
+        ctx.close()
+    out["speedup_vs_jacobi"] = {k: out[k]["networks_per_s"] / out["jacobi"]["networks_per_s"] for k in ("chain", "learned", "mg")}
+    return out
+
+
+def spmv_roofline(ctx, device, hbm, target_bytes=320e6, reps=20):
+    """cicy_spmv_csr on copies of the unit-pass system laid out block-diagonally
+    until the matrix is larger than L2 (126 MB); algorithmic bytes
+    12 nnz + 4 (n+1) + 16 n per call over the CUDA-event time."""
+    import ctypes as C
+
+    import scipy.sparse as sp
+    import torch
+
+    from cicy_geom_b200._abi import lib
+    from cicy_geom_b200.learned import full_csr
+
+    A1 = full_csr(ctx.system(0))
+    one = 12 * A1.nnz + 4 * A1.shape[0] + 16 * A1.shape[0]
+    copies = max(1, int(np.ceil(target_bytes / one)))
+    A = sp.block_diag([A1] * copies, format="csr")
+    n, nnz = A.shape[0], A.nnz
+    dev = torch.device(f"cuda:{device}")
+    rp = torch.tensor(A.indptr.astype(np.int32), device=dev)
+    ci = torch.tensor(A.indices.astype(np.int32), device=dev)
+    va = torch.tensor(A.data, device=dev)
+    x = torch.randn(n, dtype=torch.float64, device=dev)
+    y = torch.empty(n, dtype=torch.float64, device=dev)
+    st = torch.cuda.current_stream(dev)
+    args = [C.c_void_p(t.data_ptr()) for t in (rp, ci, va, x, y)]
+    for _ in range(3):
+        lib().cicy_spmv_csr(n, *args, C.c_void_p(st.cuda_stream))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(reps):
+        lib().cicy_spmv_csr(n, *args, C.c_void_p(st.cuda_stream))
+    e1.record(st)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) * 1e-3 / reps
+    bytes_ = 12 * nnz + 4 * (n + 1) + 16 * n
+    return {"kernel": "k_spmv_csr (cicy_spmv_csr, FP64 CSR)", "bound": "hbm", "rows": n, "nnz": nnz,
+            "workload": f"{copies} block-diagonal copies of the 25k-CNT unit-pass system (> L2)",
+            "achieved": bytes_ / t / 1e9, "peak": hbm, "unit": "GB/s", "frac": bytes_ / t / 1e9 / hbm, "us_per_call": t * 1e6,
+            "traffic": None}
+
+
 def run_ours(args):
     import ctypes as C
 
@@ -351,6 +434,9 @@ def run_ours(args):
                                    for k, v in per_kernel.items()}},
             "R_x": R[0],
         }
+        if not args.no_comparison and world == 1:
+            line["solver_comparison"] = solver_comparison(cfg, net, local)
+            line["spmv"] = spmv_roofline(ctx, local, hbm)
         if not args.no_cpu_baseline and world == 1:
             cb = cpu_baseline_reference(cfg, raw)
             if cb:

@@ -191,6 +191,7 @@ def lib() -> C.CDLL:
         "cicy_host_network_view": (C.c_int, [C.c_void_p, P(Network)]),
         "cicy_host_network_free": (None, [C.c_void_p]),
         "cicy_host_last_error": (C.c_char_p, []),
+        "cicy_spmv_csr": (C.c_int, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
         "cicy_get_chains": (C.c_int, [C.c_void_p, C.c_int32, i32p, i32p, i32p]),
         "cicy_gnn_param_count": (C.c_int32, []),
         "cicy_ctx_set_learned_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int32]),

@@ -249,6 +249,13 @@ cicy_status cicy_gnn_smooth_probes(cicy_gnn* g, int32_t n_probes, double* probes
 /* One Adam step (beta 0.9 / 0.999, eps 1e-8) on device arrays of n floats; step counts from 1. */
 cicy_status cicy_gnn_adam(float* params, const float* grad, float* m, float* v, int32_t n, int32_t step, float lr, void* stream);
 
+/* FP64 CSR sparse matrix-vector product y = A x on device arrays: the CG's SpMV
+ * (spM_V_SSS, Direct_Electrifying.cpp:1680-1735, which uses the symmetric
+ * SSS storage; here full CSR).  Enqueued on `stream` (a cudaStream_t, or NULL);
+ * returns without waiting. */
+cicy_status cicy_spmv_csr(int32_t n, const int32_t* row_ptr, const int32_t* col_ind, const double* values, const double* x, double* y,
+                          void* stream);
+
 /* ---------------- host-side network sources (CPU, upstream of the hot path) ---------------- */
 /* Seeded synthetic CNT network (no upstream counterpart; emits the same layout
  * Read_Network::Read_cnt_data_from_dat builds, Read_Network.cpp:348-467):

@@ -83,3 +83,29 @@ def test_multigrid_cluster_and_grid_kernels_agree(medium):
         assert abs(sa.iterations - sb.iterations) <= 2
         assert sa.rel_residual <= 1.01e-8 and sb.rel_residual <= 1.01e-8
     np.testing.assert_allclose(a.resistances[0], b.resistances[0], rtol=1e-7)
+
+
+def test_spmv_matches_scipy(medium):
+    """cicy_spmv_csr on a DEA system against scipy (FP64, summation order aside)."""
+    import ctypes as C
+
+    import torch
+
+    from cicy_geom_b200 import _abi
+    from cicy_geom_b200.learned import full_csr
+
+    cfg, net = medium
+    ctx = Context(0)
+    ctx.set_solver(preconditioner=3)
+    ctx.upload(net)
+    r = ctx.network_to_conductance(cfg.params())
+    A = full_csr(ctx.system(0))
+    x = np.random.default_rng(0).normal(size=A.shape[0])
+    dev = torch.device("cuda:0")
+    t = [torch.tensor(a, device=dev) for a in (A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data, x)]
+    y = torch.zeros(A.shape[0], dtype=torch.float64, device=dev)
+    st = _abi.lib().cicy_spmv_csr(A.shape[0], *[C.c_void_p(v.data_ptr()) for v in t], C.c_void_p(y.data_ptr()), None)
+    assert st == 0
+    torch.cuda.synchronize()
+    ref = A @ x
+    np.testing.assert_allclose(y.cpu().numpy(), ref, rtol=1e-12, atol=1e-12 * np.abs(A.data).max() * np.abs(x).max())
