@@ -127,6 +127,22 @@ class GnnSystem(C.Structure):
     ]
 
 
+class BatchSystem(C.Structure):
+    _fields_ = [
+        ("n", C.c_int32),
+        ("nnz", C.c_int32),
+        ("row_ptr", C.c_void_p),
+        ("col_ind", C.c_void_p),
+        ("values", C.c_void_p),
+        ("b", C.c_void_p),
+        ("x0", C.c_void_p),
+        ("x", C.c_void_p),
+        ("n_chains", C.c_int32),
+        ("chain_start", C.c_void_p),
+        ("chain_len", C.c_void_p),
+    ]
+
+
 class GenParams(C.Structure):
     _fields_ = [
         ("sample", Cuboid),
@@ -192,6 +208,14 @@ def lib() -> C.CDLL:
         "cicy_host_network_free": (None, [C.c_void_p]),
         "cicy_host_last_error": (C.c_char_p, []),
         "cicy_spmv_csr": (C.c_int, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "cicy_batch_create": (C.c_int, [P(C.c_void_p), C.c_int, P(BatchSystem), C.c_int32, C.c_double, C.c_int32, C.c_int32]),
+        "cicy_batch_destroy": (C.c_int, [C.c_void_p]),
+        "cicy_batch_set_shape": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
+        "cicy_batch_enable_multigrid": (C.c_int, [C.c_void_p, f64p]),
+        "cicy_batch_set_method": (C.c_int, [C.c_void_p, C.c_int32]),
+        "cicy_batch_autotune": (C.c_int, [C.c_void_p, i32p, i32p, i32p, f64p]),
+        "cicy_batch_solve": (C.c_int, [C.c_void_p, f64p]),
+        "cicy_batch_results": (C.c_int, [C.c_void_p, i64p, f64p, i32p]),
         "cicy_get_chains": (C.c_int, [C.c_void_p, C.c_int32, i32p, i32p, i32p]),
         "cicy_gnn_param_count": (C.c_int32, []),
         "cicy_ctx_set_learned_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int32]),

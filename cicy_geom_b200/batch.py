@@ -1,0 +1,147 @@
+"""Batched Monte-Carlo solves through the C ABI (cicy_batch_*).
+
+Realisations are drawn like the Monte-Carlo sweep (per-sample seed, cube side
+and CNT volume fraction; N_c = round(phi L^3 / (pi r^2 * 1 um)) for the 1 um
+mean CNT length), each run through the device path to its real-resistor
+system, and all systems are then solved together by one persistent,
+graph-captured launch.  PyTorch only holds the device arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _abi
+
+
+def monte_carlo_configs(count: int, seed0: int = 3_000_000, side=(2.0, 5.0), fraction=(0.005, 0.03), radius=0.005):
+    from .network import NetworkConfig
+
+    rng = np.random.default_rng(seed0)
+    out = []
+    for k in range(count):
+        L = float(rng.uniform(*side))
+        phi = float(rng.uniform(*fraction))
+        n = int(round(phi * L ** 3 / (math.pi * radius ** 2 * 1.0)))
+        out.append(NetworkConfig(side=L, n_cnts=max(n, 1), seed=seed0 + k, tolerance=1e-8, tolerance_unit=1e-10))
+    return out
+
+
+def realisation_systems(configs, device: int = 0, preconditioner: int = 3):
+    """Run each realisation through the device path; keep its real-resistor systems.
+
+    Returns (systems, info): systems are dicts with the full CSR (host), chains,
+    right-hand side, initial guess and the per-network solver's solution and
+    time; info counts the realisations that do not percolate (their resistance
+    is the matrix resistance, no system to solve)."""
+    from .device import Context
+    from .learned import full_csr
+    from .network import generate_cnt_network
+
+    systems, info = [], {"realisations": len(configs), "percolating": 0, "not_percolating": 0, "rejected": 0}
+    for cfg in configs:
+        net = generate_cnt_network(cfg).extract_window(cfg)
+        ctx = Context(device)
+        ctx.set_solver(preconditioner=preconditioner)
+        ctx.upload(net)
+        try:
+            r = ctx.network_to_conductance(cfg.params())
+        except _abi.CicyError:
+            info["rejected"] += 1
+            ctx.close()
+            continue
+        real = [i for i in range(r.n_solves) if r.solves[i].pass_ >= 0]
+        if not real:
+            info["not_percolating"] += 1
+        else:
+            info["percolating"] += 1
+        for i in real:
+            S = ctx.system(i)
+            if len(S["diag"]) == 0:
+                continue
+            st, ln = ctx.chains(i)
+            systems.append({"A": full_csr(S), "b": S["b"], "x0": S["x0"], "chain_start": st, "chain_len": ln,
+                            "x_ref": S["voltages"][S["reserved"]:], "seconds_ref": r.solves[i].seconds,
+                            "iterations_ref": r.solves[i].iterations, "seed": cfg.seed})
+        ctx.close()
+    return systems, info
+
+
+class BatchSolver:
+    """The systems in device memory and one cicy_batch over them."""
+
+    def __init__(self, systems, tol: float = 1e-8, precision: int = 0, max_iter_factor: int = 300, device: int = 0):
+        import torch
+
+        self.dev = torch.device(f"cuda:{device}")
+        self._keep = []
+        descs = (_abi.BatchSystem * len(systems))()
+        self.x = []
+        for k, s in enumerate(systems):
+            A = s["A"]
+            t = {
+                "rp": torch.tensor(A.indptr.astype(np.int32), device=self.dev),
+                "ci": torch.tensor(A.indices.astype(np.int32), device=self.dev),
+                "v": torch.tensor(A.data, dtype=torch.float64, device=self.dev),
+                "b": torch.tensor(s["b"], dtype=torch.float64, device=self.dev),
+                "x0": torch.tensor(s["x0"], dtype=torch.float64, device=self.dev),
+                "x": torch.zeros(A.shape[0], dtype=torch.float64, device=self.dev),
+                "cs": torch.tensor(np.asarray(s["chain_start"], np.int32), device=self.dev),
+                "cl": torch.tensor(np.asarray(s["chain_len"], np.int32), device=self.dev),
+            }
+            self._keep.append(t)
+            self.x.append(t["x"])
+            descs[k] = _abi.BatchSystem(A.shape[0], A.nnz, t["rp"].data_ptr(), t["ci"].data_ptr(), t["v"].data_ptr(), t["b"].data_ptr(),
+                                        t["x0"].data_ptr(), t["x"].data_ptr(), len(s["chain_start"]), t["cs"].data_ptr(), t["cl"].data_ptr())
+        torch.cuda.synchronize(self.dev)
+        self.count = len(systems)
+        self.h = C.c_void_p()
+        _abi.check(_abi.lib().cicy_batch_create(C.byref(self.h), device, descs, self.count, tol, max_iter_factor, precision),
+                   "cicy_batch_create")
+
+    def enable_multigrid(self) -> float:
+        """Build the per-system multigrid hierarchies; returns the setup time (s)."""
+        t = C.c_double()
+        _abi.check(_abi.lib().cicy_batch_enable_multigrid(self.h, C.byref(t)), "cicy_batch_enable_multigrid")
+        return t.value
+
+    def set_method(self, method: int):
+        _abi.check(_abi.lib().cicy_batch_set_method(self.h, method), "cicy_batch_set_method")
+
+    def autotune(self):
+        m, t, c, s = C.c_int32(), C.c_int32(), C.c_int32(), C.c_double()
+        _abi.check(_abi.lib().cicy_batch_autotune(self.h, C.byref(m), C.byref(t), C.byref(c), C.byref(s)), "cicy_batch_autotune")
+        return {"method": ["cta_chain_pcg", "cluster_multigrid"][m.value], "threads": t.value, "ctas_per_sm": c.value,
+                "seconds": s.value}
+
+    def set_shape(self, threads: int, ctas_per_sm: int):
+        _abi.check(_abi.lib().cicy_batch_set_shape(self.h, threads, ctas_per_sm), "cicy_batch_set_shape")
+
+    def solve(self) -> float:
+        s = C.c_double()
+        _abi.check(_abi.lib().cicy_batch_solve(self.h, C.byref(s)), "cicy_batch_solve")
+        return s.value
+
+    def results(self):
+        it = np.zeros(self.count, np.int64)
+        rel = np.zeros(self.count)
+        fl = np.zeros(self.count, np.int32)
+        _abi.check(_abi.lib().cicy_batch_results(self.h, it.ctypes.data_as(_abi.i64p), rel.ctypes.data_as(_abi.f64p),
+                                                 fl.ctypes.data_as(_abi.i32p)), "cicy_batch_results")
+        return it, rel, fl
+
+    def solutions(self):
+        return [x.cpu().numpy() for x in self.x]
+
+    def close(self):
+        if self.h:
+            _abi.lib().cicy_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,570 @@
+// Batched Monte-Carlo solves: many independent DEA systems of uneven size
+// solved by one persistent kernel launch (captured in a CUDA graph and
+// replayed).  Each CTA takes the next system from a largest-first queue (an
+// atomic counter) and solves it alone with preconditioned CG:
+//
+//   - preconditioner: whole-chain block-Jacobi (each CNT's free nodes form one
+//     tridiagonal block; LDL^T factored at the start of the system's solve by
+//     one thread per chain, forward/backward sweeps per chain each iteration;
+//     a singular chain falls back to its diagonal), in FP64 or FP32;
+//   - SpMV, dots and vector updates in FP64; reductions are CTA-local
+//     (__syncthreads only), so an iteration costs a few hundred nanoseconds of
+//     synchronisation instead of the microseconds of a grid barrier;
+//   - stop when |r| <= tol |r0| (Direct_Electrifying.cpp:1571, 1619), then the
+//     FP64 true residual b - A x replaces r and the test is repeated (at most
+//     kBatchRestarts times).
+//
+// Per-CTA scratch (r, p, q, z and the chain factors) lives in one device
+// buffer with a fixed offset per system.  The autotuner times the candidate
+// launch shapes (threads per CTA, CTAs per SM) on the batch itself and keeps
+// the fastest.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <numeric>
+#include <vector>
+
+#include "cicy_internal.h"
+#include "dev_common.cuh"
+#include "solver.cuh"
+
+namespace cicy {
+namespace {
+
+constexpr int kBatchRestarts = 24;
+
+struct BatchSys {
+    int n, nnz, nchains;
+    const int32_t* rp;
+    const int32_t* ci;
+    const double* val;
+    const double* b;
+    const double* x0;
+    double* x;
+    const int32_t* cs;
+    const int32_t* cl;
+    long long off;  // scratch offset (doubles)
+};
+
+struct BatchArgs {
+    const BatchSys* sys;
+    const int* order;  // largest first
+    int count;
+    int* queue;
+    double* scratch;
+    double tol;
+    long long iter_factor;
+    long long* iterations;
+    double* rel;
+    int* flags;  // per system: 1 reached the tolerance, 2 hit the iteration cap
+};
+
+template <int T>
+__device__ __forceinline__ double cta_sum(double v, double* sm) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sm[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        double x = lane < T / 32 ? sm[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) sm[32] = x;
+    }
+    __syncthreads();
+    const double r = sm[32];
+    __syncthreads();
+    return r;
+}
+
+template <int T>
+__device__ __forceinline__ void cta_sum2(double a, double b, double* sm, double& ra, double& rb) {
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) { sm[w] = a; sm[40 + w] = b; }
+    __syncthreads();
+    if (w == 0) {
+        double x = lane < T / 32 ? sm[lane] : 0.0, y = lane < T / 32 ? sm[40 + lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            x += __shfl_xor_sync(0xffffffffu, x, o);
+            y += __shfl_xor_sync(0xffffffffu, y, o);
+        }
+        if (lane == 0) { sm[32] = x; sm[33] = y; }
+    }
+    __syncthreads();
+    ra = sm[32];
+    rb = sm[33];
+    __syncthreads();
+}
+
+__device__ __forceinline__ double upper(const BatchSys& S, int i) {
+    for (int k = S.rp[i]; k < S.rp[i + 1]; k++)
+        if (S.ci[k] == i + 1) return S.val[k];
+    return 0.0;
+}
+
+// LDL^T of every chain: lf[i] = l_i (multiplier), ip[i] = 1 / pivot_i; a singular
+// chain stores l = 0 and 1 / diag (its diagonal).
+template <typename PT>
+__device__ void factor_chains(const BatchSys& S, PT* lf, PT* ip) {
+    for (int c = threadIdx.x; c < S.nchains; c += blockDim.x) {
+        const int s0 = S.cs[c], m = S.cl[c];
+        if (m <= 0) continue;
+        bool singular = false;
+        double piv_prev = 0, e_prev = 0;
+        for (int k = 0; k < m; k++) {
+            const int i = s0 + k;
+            double d = 0;
+            for (int kk = S.rp[i]; kk < S.rp[i + 1]; kk++)
+                if (S.ci[kk] == i) d = S.val[kk];
+            double l = 0, piv = d;
+            if (k > 0) {
+                l = e_prev / piv_prev;
+                piv = d - l * e_prev;
+            }
+            singular |= !(piv > 1e-13 * fabs(d));
+            lf[i] = (PT)l;
+            ip[i] = (PT)(1.0 / piv);
+            piv_prev = piv;
+            e_prev = (k + 1 < m) ? upper(S, i) : 0.0;
+        }
+        if (singular)
+            for (int k = 0; k < m; k++) {
+                const int i = s0 + k;
+                double d = 0;
+                for (int kk = S.rp[i]; kk < S.rp[i + 1]; kk++)
+                    if (S.ci[kk] == i) d = S.val[kk];
+                lf[i] = (PT)0;
+                ip[i] = (PT)(1.0 / d);
+            }
+    }
+}
+
+// z = M^-1 r chain by chain: forward (y_k = r_k - l_k y_{k-1}), backward
+// (z_k = y_k / p_k - l_{k+1} z_{k+1}).  A singular chain has l = 0: z = r / d.
+template <typename PT>
+__device__ void apply_chains(const BatchSys& S, const PT* lf, const PT* ip, const double* r, double* z) {
+    for (int c = threadIdx.x; c < S.nchains; c += blockDim.x) {
+        const int s0 = S.cs[c], m = S.cl[c];
+        if (m <= 0) continue;
+        PT y = (PT)r[s0];
+        z[s0] = (double)y;
+        for (int k = 1; k < m; k++) {
+            y = (PT)r[s0 + k] - lf[s0 + k] * y;
+            z[s0 + k] = (double)y;
+        }
+        PT zn = (PT)z[s0 + m - 1] * ip[s0 + m - 1];
+        z[s0 + m - 1] = (double)zn;
+        for (int k = m - 2; k >= 0; k--) {
+            zn = (PT)z[s0 + k] * ip[s0 + k] - lf[s0 + k + 1] * zn;
+            z[s0 + k] = (double)zn;
+        }
+    }
+}
+
+template <int T, typename PT>
+__global__ void __launch_bounds__(T) k_batch_pcg(BatchArgs a) {
+    __shared__ double sm[80];
+    __shared__ int s_q;
+    while (true) {
+        if (threadIdx.x == 0) s_q = atomicAdd(a.queue, 1);
+        __syncthreads();
+        const int q = s_q;
+        __syncthreads();
+        if (q >= a.count) return;
+        const int id = a.order[q];
+        const BatchSys S = a.sys[id];
+        const int n = S.n;
+        double* r = a.scratch + S.off;
+        double* p = r + n;
+        double* qv = p + n;
+        double* z = qv + n;
+        PT* lf = reinterpret_cast<PT*>(z + n);
+        PT* ip = lf + n;
+        factor_chains<PT>(S, lf, ip);
+        // r = b - A x0, x = x0
+        double rr_l = 0;
+        for (int i = threadIdx.x; i < n; i += T) {
+            double s = 0;
+            for (int k = S.rp[i]; k < S.rp[i + 1]; k++) s += S.val[k] * S.x0[S.ci[k]];
+            const double ri = S.b[i] - s;
+            r[i] = ri;
+            S.x[i] = S.x0[i];
+            rr_l += ri * ri;
+        }
+        double rr = cta_sum<T>(rr_l, sm);
+        const double R0 = a.tol * sqrt(rr);
+        const long long max_iter = a.iter_factor * (long long)n;
+        long long k = 0;
+        int restarts = 0, flag = 0;
+        bool fresh = true;
+        double rz = 0;
+        while (true) {
+            apply_chains<PT>(S, lf, ip, r, z);
+            __syncthreads();
+            double rz_l = 0;
+            for (int i = threadIdx.x; i < n; i += T) rz_l += r[i] * z[i];
+            const double rz_new = cta_sum<T>(rz_l, sm);
+            const double beta = fresh ? 0.0 : rz_new / rz;
+            rz = rz_new;
+            double pq_l = 0;
+            for (int i = threadIdx.x; i < n; i += T) p[i] = z[i] + beta * (fresh ? 0.0 : p[i]);
+            __syncthreads();
+            for (int i = threadIdx.x; i < n; i += T) {
+                double s = 0;
+                for (int kk = S.rp[i]; kk < S.rp[i + 1]; kk++) s += S.val[kk] * p[S.ci[kk]];
+                qv[i] = s;
+                pq_l += p[i] * s;
+            }
+            const double pq = cta_sum<T>(pq_l, sm);
+            fresh = false;
+            k++;
+            const double alpha = rz / pq;
+            rr_l = 0;
+            for (int i = threadIdx.x; i < n; i += T) {
+                S.x[i] += alpha * p[i];
+                const double ri = r[i] - alpha * qv[i];
+                r[i] = ri;
+                rr_l += ri * ri;
+            }
+            rr = cta_sum<T>(rr_l, sm);
+            if (sqrt(rr) <= R0 || !(rr == rr)) {
+                if (!(rr == rr) || restarts >= kBatchRestarts) break;
+                // FP64 true residual
+                double tl = 0;
+                for (int i = threadIdx.x; i < n; i += T) {
+                    double s = 0;
+                    for (int kk = S.rp[i]; kk < S.rp[i + 1]; kk++) s += S.val[kk] * S.x[S.ci[kk]];
+                    const double ri = S.b[i] - s;
+                    r[i] = ri;
+                    tl += ri * ri;
+                }
+                rr = cta_sum<T>(tl, sm);
+                restarts++;
+                if (sqrt(rr) <= R0) { flag = 1; break; }
+                fresh = true;
+            }
+            if (k >= max_iter) { flag = 2; break; }
+        }
+        // FP64 relative residual |b - A x| / |b|
+        double bb_l = 0, tr_l = 0;
+        for (int i = threadIdx.x; i < n; i += T) {
+            double s = 0;
+            for (int kk = S.rp[i]; kk < S.rp[i + 1]; kk++) s += S.val[kk] * S.x[S.ci[kk]];
+            const double ri = S.b[i] - s;
+            tr_l += ri * ri;
+            bb_l += S.b[i] * S.b[i];
+        }
+        double trr, bbb;
+        cta_sum2<T>(tr_l, bb_l, sm, trr, bbb);
+        if (threadIdx.x == 0) {
+            a.iterations[id] = k;
+            a.rel[id] = bbb > 0 ? sqrt(trr / bbb) : 0.0;
+            a.flags[id] = flag;
+        }
+        __syncthreads();
+    }
+}
+
+// FP64 |b - A x| / |b| of every system (one CTA per system).
+__global__ void __launch_bounds__(256) k_batch_residual(const BatchSys* __restrict__ sys, int count, double* __restrict__ rel) {
+    __shared__ double sm[80];
+    for (int id = blockIdx.x; id < count; id += gridDim.x) {
+        const BatchSys S = sys[id];
+        double a = 0, b = 0;
+        for (int i = threadIdx.x; i < S.n; i += 256) {
+            double s = 0;
+            for (int k = S.rp[i]; k < S.rp[i + 1]; k++) s += S.val[k] * S.x[S.ci[k]];
+            const double ri = S.b[i] - s;
+            a += ri * ri;
+            b += S.b[i] * S.b[i];
+        }
+        double ta, tb;
+        cta_sum2<256>(a, b, sm, ta, tb);
+        if (threadIdx.x == 0) rel[id] = tb > 0 ? sqrt(ta / tb) : 0.0;
+    }
+}
+
+template <int T, typename PT>
+void launch(const BatchArgs& a, int grid, cudaStream_t s) {
+    k_batch_pcg<T, PT><<<grid, T, 0, s>>>(a);
+}
+
+}  // namespace
+}  // namespace cicy
+
+// ---------------------------------------------------------------------------
+struct cicy_batch {
+    int device = 0;
+    int count = 0;
+    int precision = 0;
+    double tol = 1e-8;
+    long long iter_factor = 300;
+    int threads = 512, ctas_per_sm = 2, sms = 148;
+    int method = 0;                 // 0: one CTA per system (chain block-Jacobi PCG), 1: one 16-CTA cluster per system (multigrid PCG)
+    cicy::MgBatch* mg = nullptr;
+    int64_t launches = 0;
+    std::vector<cicy_batch_system> inputs;
+    cicy::DBuf<cicy::BatchSys> sys;
+    cicy::DBuf<int> order, queue, flags;
+    cicy::DBuf<double> scratch, rel;
+    cicy::DBuf<long long> iterations;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int graph_threads = 0, graph_ctas = 0, graph_method = -1;
+    cudaStream_t stream = nullptr;
+    ~cicy_batch() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (stream) cudaStreamDestroy(stream);
+        if (mg) cicy::mg_batch_free(mg);
+        sys.release(); order.release(); queue.release(); flags.release(); scratch.release(); rel.release(); iterations.release();
+    }
+};
+
+namespace {
+
+template <class F>
+cicy_status batch_guard(int device, F&& f) {
+    try {
+        CICY_CUDA(cudaSetDevice(device));
+        f();
+        return CICY_OK;
+    } catch (const cicy::Fail& e) {
+        cicy::set_host_error(e.msg);
+        return e.status;
+    }
+}
+
+void enqueue(cicy_batch* B, cudaStream_t s) {
+    if (B->method == 1) {
+        cicy::mg_batch_enqueue(B->mg, s);
+        cicy::k_batch_residual<<<std::min(B->count, B->sms * 4), 256, 0, s>>>(B->sys.get(), B->count, B->rel.get());
+        CICY_LAUNCH_CHECK();
+        return;
+    }
+    cicy::BatchArgs a{};
+    a.sys = B->sys.get();
+    a.order = B->order.get();
+    a.count = B->count;
+    a.queue = B->queue.get();
+    a.scratch = B->scratch.get();
+    a.tol = B->tol;
+    a.iter_factor = B->iter_factor;
+    a.iterations = B->iterations.get();
+    a.rel = B->rel.get();
+    a.flags = B->flags.get();
+    CICY_CUDA(cudaMemsetAsync(B->queue.get(), 0, sizeof(int), s));
+    const int grid = std::max(1, std::min(B->count, B->sms * B->ctas_per_sm));
+    const bool f32 = B->precision == CICY_PRECISION_MIXED;
+    switch (B->threads) {
+        case 256: f32 ? cicy::launch<256, float>(a, grid, s) : cicy::launch<256, double>(a, grid, s); break;
+        case 512: f32 ? cicy::launch<512, float>(a, grid, s) : cicy::launch<512, double>(a, grid, s); break;
+        default: f32 ? cicy::launch<1024, float>(a, grid, s) : cicy::launch<1024, double>(a, grid, s); break;
+    }
+    CICY_LAUNCH_CHECK();
+}
+
+// (Re)build the graph of one batch solve for the current launch shape.
+void ensure_graph(cicy_batch* B) {
+    if (B->exec && B->graph_threads == B->threads && B->graph_ctas == B->ctas_per_sm && B->graph_method == B->method) return;
+    if (B->exec) cudaGraphExecDestroy(B->exec);
+    if (B->graph) cudaGraphDestroy(B->graph);
+    B->exec = nullptr;
+    B->graph = nullptr;
+    CICY_CUDA(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+        enqueue(B, B->stream);
+    } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(B->stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    CICY_CUDA(cudaStreamEndCapture(B->stream, &B->graph));
+    CICY_CUDA(cudaGraphInstantiate(&B->exec, B->graph, 0));
+    B->graph_threads = B->threads;
+    B->graph_ctas = B->ctas_per_sm;
+    B->graph_method = B->method;
+}
+
+double timed_solve(cicy_batch* B) {
+    ensure_graph(B);
+    cudaEvent_t e0, e1;
+    CICY_CUDA(cudaEventCreate(&e0));
+    CICY_CUDA(cudaEventCreate(&e1));
+    CICY_CUDA(cudaEventRecord(e0, B->stream));
+    CICY_CUDA(cudaGraphLaunch(B->exec, B->stream));
+    CICY_CUDA(cudaEventRecord(e1, B->stream));
+    CICY_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return ms * 1e-3;
+}
+
+}  // namespace
+
+extern "C" {
+
+cicy_status cicy_batch_create(cicy_batch** out, int device, const cicy_batch_system* systems, int32_t count, double tol,
+                              int32_t max_iter_factor, int32_t precision) {
+    if (!out || !systems || count <= 0 || !(tol > 0) || max_iter_factor <= 0 || precision < 0 || precision > 1) {
+        cicy::set_host_error("cicy_batch_create: invalid arguments");
+        return CICY_E_INPUT;
+    }
+    *out = nullptr;
+    for (int i = 0; i < count; i++) {
+        const cicy_batch_system& s = systems[i];
+        if (s.n <= 0 || s.nnz <= 0 || !s.row_ptr || !s.col_ind || !s.values || !s.b || !s.x0 || !s.x || s.n_chains <= 0 ||
+            !s.chain_start || !s.chain_len) {
+            cicy::set_host_error("cicy_batch_create: system " + std::to_string(i) + " is incomplete");
+            return CICY_E_INPUT;
+        }
+    }
+    cicy_batch* B = new cicy_batch;
+    cicy_status st = batch_guard(device, [&] {
+        B->device = device;
+        B->count = count;
+        B->inputs.assign(systems, systems + count);
+        B->precision = precision;
+        B->tol = tol;
+        B->iter_factor = max_iter_factor;
+        CICY_CUDA(cudaDeviceGetAttribute(&B->sms, cudaDevAttrMultiProcessorCount, device));
+        CICY_CUDA(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
+        std::vector<cicy::BatchSys> h(count);
+        long long off = 0;
+        const int pt = precision == CICY_PRECISION_MIXED ? 1 : 2;  // factor storage in doubles per node
+        for (int i = 0; i < count; i++) {
+            const cicy_batch_system& s = systems[i];
+            h[i] = cicy::BatchSys{s.n, s.nnz, s.n_chains, s.row_ptr, s.col_ind, s.values, s.b, s.x0, s.x, s.chain_start, s.chain_len, off};
+            off += 4LL * s.n + pt * (long long)s.n + 2;
+        }
+        std::vector<int> ord(count);
+        std::iota(ord.begin(), ord.end(), 0);
+        std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return systems[a].n > systems[b].n; });
+        B->sys.ensure(count);
+        B->order.ensure(count);
+        B->queue.ensure(1);
+        B->flags.ensure(count);
+        B->rel.ensure(count);
+        B->iterations.ensure(count);
+        B->scratch.ensure((size_t)off + 2);
+        CICY_CUDA(cudaMemcpyAsync(B->sys.get(), h.data(), sizeof(cicy::BatchSys) * count, cudaMemcpyHostToDevice, B->stream));
+        CICY_CUDA(cudaMemcpyAsync(B->order.get(), ord.data(), sizeof(int) * count, cudaMemcpyHostToDevice, B->stream));
+        CICY_CUDA(cudaStreamSynchronize(B->stream));
+    });
+    if (st != CICY_OK) {
+        delete B;
+        return st;
+    }
+    *out = B;
+    return CICY_OK;
+}
+
+cicy_status cicy_batch_destroy(cicy_batch* b) {
+    if (b) {
+        cudaSetDevice(b->device);
+        delete b;
+    }
+    return CICY_OK;
+}
+
+cicy_status cicy_batch_set_shape(cicy_batch* b, int32_t threads, int32_t ctas_per_sm) {
+    if (!b || (threads != 256 && threads != 512 && threads != 1024) || ctas_per_sm < 1 || ctas_per_sm > 8 ||
+        threads * ctas_per_sm > 2048) {
+        cicy::set_host_error("cicy_batch_set_shape: threads must be 256, 512 or 1024 and threads x CTAs per SM at most 2048");
+        return CICY_E_INPUT;
+    }
+    b->threads = threads;
+    b->ctas_per_sm = ctas_per_sm;
+    return CICY_OK;
+}
+
+cicy_status cicy_batch_enable_multigrid(cicy_batch* b, double* setup_seconds) {
+    if (!b) return CICY_E_INPUT;
+    return batch_guard(b->device, [&] {
+        if (b->mg) return;
+        const auto t0 = std::chrono::steady_clock::now();
+        std::vector<cicy::MgBatchInput> in(b->count);
+        for (int i = 0; i < b->count; i++) {
+            const cicy_batch_system& s = b->inputs[i];
+            in[i] = cicy::MgBatchInput{s.n, s.nnz, s.n_chains, s.row_ptr, s.col_ind, s.values, s.b, s.x0, s.x, s.chain_start, s.chain_len};
+        }
+        b->mg = cicy::mg_batch_build(in, b->tol, b->iter_factor, b->stream, b->launches);
+        if (setup_seconds) *setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    });
+}
+
+cicy_status cicy_batch_set_method(cicy_batch* b, int32_t method) {
+    if (!b || method < 0 || method > 1 || (method == 1 && !b->mg)) {
+        cicy::set_host_error("cicy_batch_set_method: 0 (one CTA per system) or 1 (multigrid, after cicy_batch_enable_multigrid)");
+        return CICY_E_INPUT;
+    }
+    b->method = method;
+    return CICY_OK;
+}
+
+cicy_status cicy_batch_autotune(cicy_batch* b, int32_t* method, int32_t* threads, int32_t* ctas_per_sm, double* seconds) {
+    if (!b) return CICY_E_INPUT;
+    return batch_guard(b->device, [&] {
+        static const int cand[][3] = {{0, 256, 4}, {0, 256, 8}, {0, 512, 2}, {0, 512, 4}, {0, 1024, 1}, {0, 1024, 2}, {1, 1024, 1}};
+        double best = 1e300;
+        int bm = b->method, bt = b->threads, bc = b->ctas_per_sm;
+        for (const auto& c : cand) {
+            if (c[0] == 1 && !b->mg) continue;
+            b->method = c[0];
+            b->threads = c[1];
+            b->ctas_per_sm = c[2];
+            timed_solve(b);  // warm (also builds the graph)
+            const double t = std::min(timed_solve(b), timed_solve(b));
+            if (t < best) {
+                best = t;
+                bm = c[0];
+                bt = c[1];
+                bc = c[2];
+            }
+        }
+        b->method = bm;
+        b->threads = bt;
+        b->ctas_per_sm = bc;
+        if (method) *method = bm;
+        if (threads) *threads = bt;
+        if (ctas_per_sm) *ctas_per_sm = bm == 1 ? cicy::mg_batch_clusters(b->mg) : bc;
+        if (seconds) *seconds = best;
+    });
+}
+
+cicy_status cicy_batch_solve(cicy_batch* b, double* seconds) {
+    if (!b) return CICY_E_INPUT;
+    return batch_guard(b->device, [&] {
+        const double t = timed_solve(b);
+        if (seconds) *seconds = t;
+    });
+}
+
+cicy_status cicy_batch_results(cicy_batch* b, int64_t* iterations, double* rel_residual, int32_t* flags) {
+    if (!b) return CICY_E_INPUT;
+    return batch_guard(b->device, [&] {
+        std::vector<long long> it(b->count);
+        CICY_CUDA(cudaMemcpyAsync(it.data(), b->iterations.get(), sizeof(long long) * b->count, cudaMemcpyDeviceToHost, b->stream));
+        if (rel_residual) CICY_CUDA(cudaMemcpyAsync(rel_residual, b->rel.get(), sizeof(double) * b->count, cudaMemcpyDeviceToHost, b->stream));
+        if (flags) CICY_CUDA(cudaMemcpyAsync(flags, b->flags.get(), sizeof(int) * b->count, cudaMemcpyDeviceToHost, b->stream));
+        CICY_CUDA(cudaStreamSynchronize(b->stream));
+        if (b->method == 1) {
+            std::vector<double> st;
+            cicy::mg_batch_stats(b->mg, st, b->stream);
+            for (int i = 0; i < b->count; i++) {
+                it[i] = (long long)st[4 * i];
+                if (flags) flags[i] = std::sqrt(st[4 * i + 1]) <= st[4 * i + 2] ? 1 : (it[i] >= b->iter_factor * b->inputs[i].n ? 2 : 0);
+            }
+        }
+        if (iterations)
+            for (int i = 0; i < b->count; i++) iterations[i] = it[i];
+    });
+}
+
+}  // extern "C"

@@ -183,6 +183,22 @@ void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long 
                   cudaStream_t s, int64_t& launches, PcgStats& st);
 
 // precond PRECOND_KIND_SPAI needs the block preconditioner and `ew` (learned weights per entry).
+// Batched MG solves (solver_mg.cu): device arrays of each system; chains partition the rows.
+struct MgBatchInput {
+    int n, nnz, nchains;
+    const int32_t *rp, *ci;
+    const double *val, *b, *x0;
+    double* x;
+    const int32_t *cs, *cl;
+};
+struct MgBatch;
+MgBatch* mg_batch_build(const std::vector<MgBatchInput>& in, double tol, long long iter_factor, cudaStream_t s, int64_t& launches);
+void mg_batch_enqueue(MgBatch* b, cudaStream_t s);
+// per system: iterations, |r|^2 of the last test, tol |r0|, restarts
+void mg_batch_stats(MgBatch* b, std::vector<double>& stats, cudaStream_t s);
+int mg_batch_clusters(const MgBatch* b);
+void mg_batch_free(MgBatch* b);
+
 void pcg_solve(SolverWork& w, const SolverSystem& sys, int precond, bool mixed, double tol, long long max_iter, int num_sms,
                int* status, cudaStream_t s, int64_t& launches, PcgStats& st, const float* ew = nullptr);
 

@@ -336,6 +336,7 @@ struct MgArgs {
     const double* val;
     const double* b;
     double* x;
+    const double* x0;  // when set, the solve starts from x0 (batched solves); else r = b - A x is given
     double *r, *z0, *z, *w, *p, *q;
     const double* tinv;
     const int32_t *row_off, *row_base, *row_m;
@@ -435,8 +436,9 @@ __device__ __forceinline__ double block_apply(const MgArgs& a, const double* __r
     return s;
 }
 
+// One MG-PCG solve by `nctas` CTAs (this is CTA `cta` of them).
 template <bool CL>
-__global__ void __launch_bounds__(CL ? kMgClusterThreads : kMgThreads) k_mg_pcg(MgArgs a) {
+__device__ void mg_pcg_body(const MgArgs& a, int cta, int nctas) {
     __shared__ double sm[72];
     __shared__ MgLevel lv[kMgMaxLevels];
     __shared__ double rc[kMgDenseMax];
@@ -444,11 +446,19 @@ __global__ void __launch_bounds__(CL ? kMgClusterThreads : kMgThreads) k_mg_pcg(
     if (threadIdx.x < a.levels) lv[threadIdx.x] = a.lv[threadIdx.x];
     __syncthreads();
     const int C = a.levels - 1;
-    const int nb = gridDim.x;
-    const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+    const int nb = nctas;
+    const int gt = cta * blockDim.x + threadIdx.x, gs = nctas * blockDim.x;
     const int grp = gt / kGroup, glane = gt % kGroup, ngrp = gs / kGroup;
     const unsigned gmask = ((1u << kGroup) - 1) << ((threadIdx.x & 31) & ~(kGroup - 1));
-    const int r_lo = a.cta_row[blockIdx.x], r_hi = a.cta_row[blockIdx.x + 1];
+    const int r_lo = a.cta_row[cta], r_hi = a.cta_row[cta + 1];
+    if (a.x0) {  // start from x0: x = x0, r = b - A x0 (own rows; x0 is read-only, no barrier needed)
+        for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
+            double s = 0;
+            for (int kk = a.rp[i]; kk < a.rp[i + 1]; kk++) s += a.val[kk] * a.x0[a.ci[kk]];
+            a.x[i] = a.x0[i];
+            a.r[i] = a.b[i] - s;
+        }
+    }
     unsigned long long target = 0;
     double R0 = 0, rr = 0, rz = 0, beta = 0;
     long long k = 0;
@@ -466,7 +476,7 @@ __global__ void __launch_bounds__(CL ? kMgClusterThreads : kMgThreads) k_mg_pcg(
         }
         double s0;
         mg_reduce1(rr_l, sm, s0);
-        if (threadIdx.x == 0) a.partA[blockIdx.x] = s0;
+        if (threadIdx.x == 0) a.partA[cta] = s0;
         if (!sync_all<CL>(a.bar, target, a.err, &s_ok)) return;
         rr = mg_sum_partials(a.partA, nb, sm);
         if (k == 0 && !recursive && restarts == 0) R0 = a.tol * sqrt(rr);
@@ -528,10 +538,10 @@ __global__ void __launch_bounds__(CL ? kMgClusterThreads : kMgThreads) k_mg_pcg(
             const MgLevel& Cl = lv[C];
             const int nC = Cl.n;
             const int wpb = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-            if (blockIdx.x * wpb < nC) {
+            if (cta * wpb < nC) {
                 for (int j = threadIdx.x; j < nC; j += blockDim.x) rc[j] = __ldcg(&Cl.r[j]);
                 __syncthreads();
-                for (int i = blockIdx.x * wpb + warp; i < nC; i += gridDim.x * wpb) {
+                for (int i = cta * wpb + warp; i < nC; i += nctas * wpb) {
                     const double* row = a.cinv + (size_t)i * nC;
                     double s = 0;
                     for (int j = lane; j < nC; j += 32) s += row[j] * rc[j];
@@ -578,7 +588,7 @@ __global__ void __launch_bounds__(CL ? kMgClusterThreads : kMgThreads) k_mg_pcg(
                 rz_l += a.r[i] * zi;
             }
             mg_reduce1(rz_l, sm, s0);
-            if (threadIdx.x == 0) a.partB[blockIdx.x] = s0;
+            if (threadIdx.x == 0) a.partB[cta] = s0;
             if (!sync_all<CL>(a.bar, target, a.err, &s_ok)) return;
             const double rz_new = mg_sum_partials(a.partB, nb, sm);
             beta = fresh ? 0.0 : rz_new / rz;
@@ -597,7 +607,7 @@ __global__ void __launch_bounds__(CL ? kMgClusterThreads : kMgThreads) k_mg_pcg(
             pq_l += pi * qi;
         }
         mg_reduce1(pq_l, sm, s0);
-        if (threadIdx.x == 0) a.partA[nb + blockIdx.x] = s0;
+        if (threadIdx.x == 0) a.partA[nb + cta] = s0;
         if (!sync_all<CL>(a.bar, target, a.err, &s_ok)) return;
         const double pq = mg_sum_partials(a.partA + nb, nb, sm);
         fresh = false;
@@ -610,11 +620,33 @@ __global__ void __launch_bounds__(CL ? kMgClusterThreads : kMgThreads) k_mg_pcg(
         }
         recursive = true;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (cta == 0 && threadIdx.x == 0) {
         a.stats[0] = (double)k;
         a.stats[1] = rr;
         a.stats[2] = R0;
         a.stats[3] = (double)restarts;
+    }
+}
+
+template <bool CL>
+__global__ void __launch_bounds__(CL ? kMgClusterThreads : kMgThreads) k_mg_pcg(MgArgs a) {
+    mg_pcg_body<CL>(a, blockIdx.x, gridDim.x);
+}
+
+// Batched solves: every 16-CTA cluster takes the next system of the queue and
+// runs the MG-PCG on it; `slots` passes the index from cluster rank 0 to the others.
+__global__ void __launch_bounds__(kMgClusterThreads) k_mg_batch(const MgArgs* __restrict__ all, int count, int* queue, int* slots) {
+    const int cl = blockIdx.x / kMgClusterCtas, rank = blockIdx.x % kMgClusterCtas;
+    while (true) {
+        if (rank == 0 && threadIdx.x == 0) slots[cl] = atomicAdd(queue, 1);
+        asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+        asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+        const int s = __ldcg(&slots[cl]);
+        asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+        asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+        if (s >= count) return;
+        const MgArgs a = all[s];
+        mg_pcg_body<true>(a, rank, kMgClusterCtas);
     }
 }
 
@@ -912,5 +944,159 @@ void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long 
     st.levels = g.levels;
     st.cluster = cluster;
 }
+
+}  // namespace cicy
+
+namespace cicy {
+
+// ---------------------------------------------------------------------------
+// Batched MG solves (used by batch.cu): per-system hierarchies built once, all
+// systems solved by k_mg_batch, one 16-CTA cluster per system at a time.
+namespace {
+__global__ void k_diag_of(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const double* __restrict__ v,
+                          double* __restrict__ d) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double x = 0;
+        for (int k = rp[i]; k < rp[i + 1]; k++)
+            if (ci[k] == i) x = v[k];
+        d[i] = x;
+    }
+}
+}  // namespace
+
+struct MgBatch {
+    std::vector<SolverWork*> works;
+    std::vector<DBuf<double>*> diags;
+    DBuf<MgArgs> args;
+    DBuf<int> queue, slots;
+    DBuf<double> stats;
+    int count = 0, nclusters = 0;
+    double tol = 0;
+    ~MgBatch() {
+        for (auto* w : works) delete w;
+        for (auto* d : diags) {
+            d->release();
+            delete d;
+        }
+        args.release();
+        queue.release();
+        slots.release();
+        stats.release();
+    }
+};
+
+MgBatch* mg_batch_build(const std::vector<MgBatchInput>& in, double tol, long long iter_factor, cudaStream_t s, int64_t& launches) {
+    static int cl_attr = 0;
+    if (cl_attr == 0) {
+        cl_attr = cudaFuncSetAttribute(k_mg_batch, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess ? 1 : -1;
+        cudaGetLastError();
+    }
+    if (cl_attr < 0) throw Fail{CICY_E_DEVICE, "batched multigrid: 16-CTA clusters are not available"};
+    MgBatch* B = new MgBatch;
+    try {
+        B->count = (int)in.size();
+        B->tol = tol;
+        B->stats.ensure(4 * in.size() + 4);
+        std::vector<MgArgs> host(in.size());
+        for (size_t k = 0; k < in.size(); k++) {
+            const MgBatchInput& x = in[k];
+            auto* w = new SolverWork;
+            B->works.push_back(w);
+            auto* d = new DBuf<double>;
+            B->diags.push_back(d);
+            d->ensure(x.n + 1);
+            k_diag_of<<<grid_for(x.n), 256, 0, s>>>(x.n, x.rp, x.ci, x.val, d->get());
+            launches++;
+            SolverSystem ss;
+            ss.n = x.n;
+            ss.nnz = x.nnz;
+            ss.rp = x.rp;
+            ss.ci = x.ci;
+            ss.val = x.val;
+            ss.diag = d->get();
+            ss.b = x.b;
+            ss.x = x.x;
+            build_block_preconditioner(*w, ss, x.nchains, x.cs, x.cl, nullptr, nullptr, false, s, launches);
+            build_mg_hierarchy(*w, ss, s, launches);
+            MgWork& g = w->mg;
+            w->r.ensure(x.n); w->z.ensure(x.n); w->p.ensure(x.n); w->q.ensure(x.n);
+            g.z0.ensure(x.n);
+            g.wtmp.ensure(x.n);
+            w->cta_row.ensure(kMgClusterCtas + 1);
+            launch_cta_rows(kMgClusterCtas, x.n, w->is_start.get(), w->cta_row.get(), s);
+            w->part.ensure(4 * kMgClusterCtas + 8);
+            MgArgs a{};
+            a.n = x.n;
+            a.rp = x.rp; a.ci = x.ci; a.val = x.val; a.b = x.b; a.x = x.x; a.x0 = x.x0;
+            a.r = w->r.get(); a.z0 = g.z0.get(); a.z = w->z.get(); a.w = g.wtmp.get(); a.p = w->p.get(); a.q = w->q.get();
+            a.tinv = w->tinv.get(); a.row_off = w->row_off.get(); a.row_base = w->row_base.get(); a.row_m = w->row_m.get();
+            a.cta_row = w->cta_row.get();
+            a.levels = g.levels;
+            a.lv = g.dev_lv.get();
+            a.cinv = g.dense ? g.cinv.get() : nullptr;
+            a.omega0 = kOmega0;
+            a.partA = w->part.get();
+            a.partB = w->part.get() + 2 * kMgClusterCtas;
+            a.stats = B->stats.get() + 4 * k;
+            a.bar = nullptr;
+            a.err = nullptr;
+            a.tol = tol;
+            a.max_iter = iter_factor * (long long)x.n;
+            a.max_restarts = kMgMaxRestarts;
+            host[k] = a;
+        }
+        B->args.ensure(in.size());
+        CICY_CUDA(cudaMemcpyAsync(B->args.get(), host.data(), sizeof(MgArgs) * in.size(), cudaMemcpyHostToDevice, s));
+        B->queue.ensure(1);
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        cfg.gridDim = dim3(kMgClusterCtas);
+        cfg.blockDim = dim3(kMgClusterThreads);
+        cfg.stream = s;
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = kMgClusterCtas;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int nclusters = 0;
+        CICY_CUDA(cudaOccupancyMaxActiveClusters(&nclusters, (void*)k_mg_batch, &cfg));
+        if (nclusters < 1) throw Fail{CICY_E_DEVICE, "batched multigrid: no 16-CTA cluster fits"};
+        B->nclusters = std::min(nclusters, B->count);
+        B->slots.ensure(B->nclusters + 1);
+        CICY_CUDA(cudaStreamSynchronize(s));
+        CICY_LAUNCH_CHECK();
+    } catch (...) {
+        delete B;
+        throw;
+    }
+    return B;
+}
+
+void mg_batch_enqueue(MgBatch* B, cudaStream_t s) {
+    CICY_CUDA(cudaMemsetAsync(B->queue.get(), 0, sizeof(int), s));
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    cfg.gridDim = dim3(kMgClusterCtas * B->nclusters);
+    cfg.blockDim = dim3(kMgClusterThreads);
+    cfg.stream = s;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kMgClusterCtas;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CICY_CUDA(cudaLaunchKernelEx(&cfg, k_mg_batch, (const MgArgs*)B->args.get(), B->count, B->queue.get(), B->slots.get()));
+}
+
+void mg_batch_stats(MgBatch* B, std::vector<double>& stats, cudaStream_t s) {
+    stats.resize(4 * (size_t)B->count);
+    CICY_CUDA(cudaMemcpyAsync(stats.data(), B->stats.get(), sizeof(double) * 4 * B->count, cudaMemcpyDeviceToHost, s));
+    CICY_CUDA(cudaStreamSynchronize(s));
+}
+
+int mg_batch_clusters(const MgBatch* B) { return B->nclusters; }
+
+void mg_batch_free(MgBatch* B) { delete B; }
 
 }  // namespace cicy

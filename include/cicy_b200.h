@@ -256,6 +256,46 @@ cicy_status cicy_gnn_adam(float* params, const float* grad, float* m, float* v, 
 cicy_status cicy_spmv_csr(int32_t n, const int32_t* row_ptr, const int32_t* col_ind, const double* values, const double* x, double* y,
                           void* stream);
 
+/* ---------------- batched Monte-Carlo solves (no upstream counterpart) ----------------
+ * Many independent DEA systems (e.g. the real-resistor systems of hundreds of
+ * seeded realisations) solved by one persistent kernel launch, replayed from a
+ * CUDA graph: each CTA takes the next system of a largest-first queue and runs
+ * preconditioned CG on it alone (whole-chain block-Jacobi; FP64, or FP32
+ * preconditioner apply with CICY_PRECISION_MIXED; FP64 SpMV, dots and true
+ * residual), stopping at |r| <= tol |r0| confirmed on the FP64 true residual
+ * (the test of Direct_Electrifying.cpp:1571, 1619).  All pointers are device
+ * memory the caller keeps alive; the chains must partition the rows. */
+typedef struct {
+    int32_t n, nnz;
+    const int32_t* row_ptr;    /* full symmetric CSR, diagonal included */
+    const int32_t* col_ind;
+    const double* values;
+    const double* b;
+    const double* x0;          /* initial guess */
+    double* x;                 /* solution (written by every solve) */
+    int32_t n_chains;
+    const int32_t* chain_start;
+    const int32_t* chain_len;
+} cicy_batch_system;
+typedef struct cicy_batch cicy_batch;
+cicy_status cicy_batch_create(cicy_batch** out, int device, const cicy_batch_system* systems, int32_t count, double tol,
+                              int32_t max_iter_factor, int32_t precision);
+cicy_status cicy_batch_destroy(cicy_batch* b);
+/* Launch shape: threads per CTA (256, 512, 1024) and CTAs per SM. */
+cicy_status cicy_batch_set_shape(cicy_batch* b, int32_t threads, int32_t ctas_per_sm);
+/* Builds a multigrid hierarchy per system (setup time returned) so the batch can
+ * also run as one 16-CTA cluster per system with the chain-aggregation multigrid PCG. */
+cicy_status cicy_batch_enable_multigrid(cicy_batch* b, double* setup_seconds);
+/* 0: one CTA per system (chain block-Jacobi PCG); 1: one 16-CTA cluster per system (multigrid PCG). */
+cicy_status cicy_batch_set_method(cicy_batch* b, int32_t method);
+/* Times the candidate methods and launch shapes on this batch and keeps the fastest
+ * (for the multigrid method ctas_per_sm returns the number of concurrent clusters). */
+cicy_status cicy_batch_autotune(cicy_batch* b, int32_t* method, int32_t* threads, int32_t* ctas_per_sm, double* seconds);
+/* One batched solve (graph launch); seconds = its device time (CUDA events). */
+cicy_status cicy_batch_solve(cicy_batch* b, double* seconds);
+/* Per system: iterations, FP64 |b - A x| / |b|, flag (1 converged, 2 iteration cap, 0 breakdown). */
+cicy_status cicy_batch_results(cicy_batch* b, int64_t* iterations, double* rel_residual, int32_t* flags);
+
 /* ---------------- host-side network sources (CPU, upstream of the hot path) ---------------- */
 /* Seeded synthetic CNT network (no upstream counterpart; emits the same layout
  * Read_Network::Read_cnt_data_from_dat builds, Read_Network.cpp:348-467):
