@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--precond", default="mg", choices=["jacobi", "chain", "learned", "mg"])
     ap.add_argument("--no-comparison", action="store_true", help="skip the per-preconditioner comparison and the SpMV measurement")
+    ap.add_argument("--mc", type=int, default=256, help="Monte-Carlo realisations for the batched-solve measurement (0: skip)")
     # a smaller network of the same generator, for profiler captures (the bench line names the size it ran)
     ap.add_argument("--side", type=float, default=SIDE)
     ap.add_argument("--cnts", type=int, default=N_CNTS)
@@ -315,6 +316,40 @@ def spmv_roofline(ctx, device, hbm, target_bytes=320e6, reps=20):
             "traffic": None}
 
 
+def batched_monte_carlo(count, device, reps=3):
+    """Monte-Carlo sweep: `count` seeded realisations (cube side U[2,5] um, CNT
+    volume fraction U[0.5%,3%]), each run through the device path to its
+    real-resistor system; then all systems solved at 1e-8 by one graph-captured
+    launch (method and launch shape from the autotuner).  Compared with the sum
+    of the per-network multigrid solve times of the same systems."""
+    import time as _t
+
+    from cicy_geom_b200 import batch as BT
+
+    t0 = _t.time()
+    cfgs = BT.monte_carlo_configs(count)
+    systems, info = BT.realisation_systems(cfgs, device=device)
+    prep = _t.time() - t0
+    if not systems:
+        return {"realisations": count, **info, "systems": 0}
+    bs = BT.BatchSolver(systems, tol=TOL, device=device)
+    setup = bs.enable_multigrid()
+    tuned = bs.autotune()
+    times = [bs.solve() for _ in range(reps)]
+    it, rel, fl = bs.results()
+    bs.close()
+    t = min(times)
+    seq = sum(s["seconds_ref"] for s in systems)
+    n = [s["A"].shape[0] for s in systems]
+    return {"realisations": count, **info, "systems": len(systems), "unknowns_total": int(sum(n)), "unknowns_max": int(max(n)),
+            "autotuned": tuned, "solve_seconds": t, "systems_per_s": len(systems) / t,
+            "sequential_solve_seconds": seq, "speedup_vs_sequential": seq / t, "multigrid_setup_seconds": setup,
+            "generation_and_assembly_seconds": prep, "converged": int((fl == 1).sum()), "max_rel_residual": float(rel.max()),
+            "max_iterations": int(it.max()),
+            "sample": "cube side U[2,5] um, CNT volume fraction U[0.5%,3%], seeds 3,000,000+k; solve stage only "
+                      "(generation, contacts, clusters, assembly and the unit-resistor pass run per network before it)"}
+
+
 def run_ours(args):
     import ctypes as C
 
@@ -437,6 +472,8 @@ def run_ours(args):
         if not args.no_comparison and world == 1:
             line["solver_comparison"] = solver_comparison(cfg, net, local)
             line["spmv"] = spmv_roofline(ctx, local, hbm)
+        if args.mc > 0 and world == 1:
+            line["batched_monte_carlo"] = batched_monte_carlo(args.mc, local)
         if not args.no_cpu_baseline and world == 1:
             cb = cpu_baseline_reference(cfg, raw)
             if cb:
