@@ -91,7 +91,7 @@ struct Ctx {
     // ---- DEA ----
     std::vector<DeaSystem*> systems;
     DBuf<int32_t> lmm;         // node of each point in the current solve (-1 none)
-    DBuf<int32_t> cnt_nodes, cnt_node_base;
+    DBuf<int32_t> cnt_nodes, cnt_node_base, cnt_fresh, claim;
     DBuf<int32_t> e_n1, e_n2, e_op;
     DBuf<double> e_g;
     DBuf<int32_t> work_i32a, work_i32b, work_i32c;

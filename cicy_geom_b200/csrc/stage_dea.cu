@@ -3,6 +3,9 @@
 // voltage solve, backbone extraction and boundary currents
 // (Direct_Electrifying.cpp, Backbone_Network.cpp, Electrical_analysis.cpp).
 #include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
 #include <cmath>
 #include <cooperative_groups.h>
 
@@ -53,24 +56,53 @@ __global__ void k_lmm_face(int b, int e, const int32_t* __restrict__ bpts, int n
 }
 
 // LM_matrix_for_cnts (Direct_Electrifying.cpp:139-215): new nodes per CNT.
+// Upstream walks the cluster's CNTs in order and gives the first and last
+// element point a node only if the point has none yet.  Two CNTs can share an
+// end point (window trimming splits a CNT at a boundary point and both segments
+// keep it); the CNT earlier in the cluster then numbers it and the later one
+// reuses it.  Here the CNTs run in parallel, so each shared end point is first
+// claimed by the smallest cluster position (claim[P] = min i), and only the
+// claimant counts and numbers it.
+__global__ void k_claim_init(int n, const int32_t* __restrict__ eb, const int32_t* __restrict__ ee, const int32_t* __restrict__ elem,
+                             int32_t* __restrict__ claim) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        claim[elem[eb[i]]] = 0x7fffffff;
+        claim[elem[ee[i] - 1]] = 0x7fffffff;
+    }
+}
+
+__global__ void k_claim(int n, const int32_t* __restrict__ eb, const int32_t* __restrict__ ee, const int32_t* __restrict__ elem,
+                        int32_t* __restrict__ claim) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        atomicMin(&claim[elem[eb[i]]], i);
+        atomicMin(&claim[elem[ee[i] - 1]], i);
+    }
+}
+
+// new[i]: bit 0 first point numbered by CNT i, bit 1 last point numbered by CNT i
 __global__ void k_node_counts(int n, const int32_t* __restrict__ eb, const int32_t* __restrict__ ee,
-                              const int32_t* __restrict__ elem, const int32_t* __restrict__ lmm, int32_t* __restrict__ cnt) {
+                              const int32_t* __restrict__ elem, const int32_t* __restrict__ lmm, const int32_t* __restrict__ claim,
+                              int32_t* __restrict__ cnt, int32_t* __restrict__ fresh) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int b = eb[i], e = ee[i];
         int m = e - b;
-        cnt[i] = (lmm[elem[b]] < 0 ? 1 : 0) + (m - 2) + (lmm[elem[e - 1]] < 0 ? 1 : 0);
+        const int P0 = elem[b], P1 = elem[e - 1];
+        const bool f0 = lmm[P0] < 0 && claim[P0] == i;
+        const bool f1 = lmm[P1] < 0 && claim[P1] == i && P1 != P0;
+        cnt[i] = (f0 ? 1 : 0) + (m - 2) + (f1 ? 1 : 0);
+        fresh[i] = (f0 ? 1 : 0) | (f1 ? 2 : 0);
     }
 }
 
 __global__ void k_node_assign(int n, int reserved, const int32_t* __restrict__ eb, const int32_t* __restrict__ ee,
-                              const int32_t* __restrict__ elem, const int32_t* __restrict__ base, int32_t* lmm) {
+                              const int32_t* __restrict__ elem, const int32_t* __restrict__ base, const int32_t* __restrict__ fresh,
+                              int32_t* lmm) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int b = eb[i], e = ee[i];
         int node = reserved + base[i];
-        bool first_free = lmm[elem[b]] < 0, last_free = lmm[elem[e - 1]] < 0;
-        if (first_free) lmm[elem[b]] = node++;
+        if (fresh[i] & 1) lmm[elem[b]] = node++;
         for (int k = b + 1; k < e - 1; k++) lmm[elem[k]] = node++;
-        if (last_free) lmm[elem[e - 1]] = node++;
+        if (fresh[i] & 2) lmm[elem[e - 1]] = node++;
     }
 }
 
@@ -579,10 +611,16 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
         }
         c.cnt_nodes.ensure(NM + 1);
         c.cnt_node_base.ensure(NM + 1);
-        k_node_counts<<<grid_for(NM), 256, 0, s>>>(NM, eb.get(), ee.get(), c.elem_idx.get(), c.lmm.get(), c.cnt_nodes.get());
+        c.claim.ensure(std::max(c.n_points, 1));
+        c.cnt_fresh.ensure(NM + 1);
+        k_claim_init<<<grid_for(NM), 256, 0, s>>>(NM, eb.get(), ee.get(), c.elem_idx.get(), c.claim.get());
+        k_claim<<<grid_for(NM), 256, 0, s>>>(NM, eb.get(), ee.get(), c.elem_idx.get(), c.claim.get());
+        k_node_counts<<<grid_for(NM), 256, 0, s>>>(NM, eb.get(), ee.get(), c.elem_idx.get(), c.lmm.get(), c.claim.get(), c.cnt_nodes.get(),
+                                                   c.cnt_fresh.get());
         exclusive_scan_i32(c.cnt_nodes.get(), c.cnt_node_base.get(), NM, c.i32_scalar.get(), c.scan_tmp32, s, c.launches);
-        k_node_assign<<<grid_for(NM), 256, 0, s>>>(NM, reserved, eb.get(), ee.get(), c.elem_idx.get(), c.cnt_node_base.get(), c.lmm.get());
-        c.launches += 2;
+        k_node_assign<<<grid_for(NM), 256, 0, s>>>(NM, reserved, eb.get(), ee.get(), c.elem_idx.get(), c.cnt_node_base.get(),
+                                                   c.cnt_fresh.get(), c.lmm.get());
+        c.launches += 4;
         const int nodes = reserved + read_i32(c, c.i32_scalar.get());
         // free nodes of each CNT are one consecutive range: the chains of the block preconditioner
         c.chain_start.ensure(NM + 1);
@@ -657,7 +695,27 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
         k_rhs<<<grid_for(NE), 256, 0, s>>>(NE, bn, reserved, c.sort_k.get(), c.work_i32a.get(), c.runval.get(), c.vef.get(), sys->b.get());
         k_diag_free<<<grid_for(n), 256, 0, s>>>(n, reserved, c.work_f64a.get(), sys->diag.get(), c.status.get());
         c.launches += 3;
-        check_status(c, "Fill_sparse_stiffness_matrix");
+        try {
+            check_status(c, "Fill_sparse_stiffness_matrix");
+        } catch (Fail& f) {
+            if (f.status == CICY_E_ZERO_DIAGONAL) {
+                // name the nodes and values, as upstream prints them (Direct_Electrifying.cpp:458-484)
+                std::vector<double> d(n);
+                CICY_CUDA(cudaMemcpy(d.data(), sys->diag.get(), sizeof(double) * n, cudaMemcpyDeviceToHost));
+                std::string nodes, vals;
+                int shown = 0;
+                for (int i = 0; i < n && shown < 8; i++)
+                    if (std::fabs(d[i]) < 1.0e-10) {
+                        nodes += " " + std::to_string(i + reserved);
+                        char buf[32];
+                        std::snprintf(buf, sizeof(buf), " %.3e", d[i]);
+                        vals += buf;
+                        shown++;
+                    }
+                f.msg += std::string(r_flag ? " (real-resistor pass" : " (unit-resistor pass") + "; nodes:" + nodes + "; values:" + vals + ")";
+            }
+            throw;
+        }
         tr.mark(r_flag ? "dea.real.assembly" : "dea.unit.assembly");
         // ---- full CSR for the CG ----
         const int NF = n + 2 * m;
@@ -865,6 +923,14 @@ void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out) {
         t_bb += seconds_between(e0, e1);
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
+        if (trace_enabled()) {
+            unsigned long long bits = 0;
+            CICY_CUDA(cudaMemcpy(&bits, c.imax.get(), sizeof(bits), cudaMemcpyDeviceToHost));
+            double im;
+            std::memcpy(&im, &bits, sizeof(im));
+            std::fprintf(stderr, "[cicy] backbone cluster %d: I_max %.17g, zero current %.17g, CNTs %d, junctions %d\n", k, im,
+                         std::max(im, kZero) * 1e-9, NM, NJ);
+        }
         if (scope != 0) continue;
         trb.mark("backbone");
         // ---- real-resistor passes per percolated direction (Electrical_analysis.cpp:229-289) ----
