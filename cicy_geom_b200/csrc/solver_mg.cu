@@ -51,7 +51,7 @@ namespace {
 constexpr int kMgThreads = 256;
 constexpr int kMgClusterThreads = 1024;
 constexpr int kMgClusterCtas = 16;            // non-portable cluster size
-constexpr int kMgClusterMaxRows = 1 << 18;    // above this the grid-wide variant has more threads per row
+constexpr int kMgClusterMaxRows = 20000;  // above this the grid-wide variant (more threads per row) is faster on B200
 constexpr int kMgMaxRestarts = 24;
 constexpr double kOmega0 = 0.95;
 constexpr int kGjThreads = 1024;
@@ -429,6 +429,76 @@ __device__ __forceinline__ double group_sum(double v, unsigned mask) {
     return v;
 }
 
+// Gathered dot products of the solve phases.  The entries of a chunk (U per
+// thread) have their column indices and values loaded first and their vector
+// entries second, so a chunk costs two dependent L2 round trips instead of two
+// per entry; the sum still runs in entry order.  Vectors other CTAs write are
+// read with __ldcg (L2).
+template <int U>
+__device__ __forceinline__ double gather_dot(const int32_t* __restrict__ ci, const double* __restrict__ v, const double* x, int b, int e,
+                                             int first = 0, int step = 1) {
+    double s = 0;
+    for (int k0 = b + first; k0 < e; k0 += U * step) {
+        int c[U];
+        double w[U], xv[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int k = k0 + u * step;
+            c[u] = k < e ? ci[k] : 0;
+            w[u] = k < e ? v[k] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) xv[u] = (k0 + u * step < e) ? __ldcg(&x[c[u]]) : 0.0;
+#pragma unroll
+        for (int u = 0; u < U; u++) s += w[u] * xv[u];
+    }
+    return s;
+}
+
+// sum_k v[k] (x[ci[k]] + y[cg[k]])
+template <int U>
+__device__ __forceinline__ double gather_dot2(const int32_t* __restrict__ ci, const int32_t* __restrict__ cg, const double* __restrict__ v,
+                                              const double* x, const double* y, int b, int e, int first = 0, int step = 1) {
+    double s = 0;
+    for (int k0 = b + first; k0 < e; k0 += U * step) {
+        int c[U], g[U];
+        double w[U], xv[U], yv[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int k = k0 + u * step;
+            c[u] = k < e ? ci[k] : 0;
+            g[u] = k < e ? cg[k] : 0;
+            w[u] = k < e ? v[k] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const bool ok = k0 + u * step < e;
+            xv[u] = ok ? __ldcg(&x[c[u]]) : 0.0;
+            yv[u] = ok ? __ldcg(&y[g[u]]) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) s += w[u] * (xv[u] + yv[u]);
+    }
+    return s;
+}
+
+// sum_m x[idx[m]]
+template <int U>
+__device__ __forceinline__ double gather_sum(const int32_t* __restrict__ idx, const double* x, int b, int e, int first, int step) {
+    double s = 0;
+    for (int k0 = b + first; k0 < e; k0 += U * step) {
+        int c[U];
+        double xv[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) c[u] = (k0 + u * step < e) ? idx[k0 + u * step] : 0;
+#pragma unroll
+        for (int u = 0; u < U; u++) xv[u] = (k0 + u * step < e) ? __ldcg(&x[c[u]]) : 0.0;
+#pragma unroll
+        for (int u = 0; u < U; u++) s += xv[u];
+    }
+    return s;
+}
+
 __device__ __forceinline__ double block_apply(const MgArgs& a, const double* __restrict__ v, int i) {
     const int off = a.row_off[i], base = a.row_base[i], m = a.row_m[i];
     double s = 0;
@@ -484,9 +554,7 @@ __device__ void mg_pcg_body(const MgArgs& a, int cta, int nctas) {
             if (!recursive || restarts >= a.max_restarts) break;
             // the recursive residual met the test: replace it by the FP64 true residual
             for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
-                double s = 0;
-                for (int kk = a.rp[i]; kk < a.rp[i + 1]; kk++) s += a.val[kk] * __ldcg(&a.x[a.ci[kk]]);
-                a.r[i] = a.b[i] - s;
+                a.r[i] = a.b[i] - gather_dot<4>(a.ci, a.val, a.x, a.rp[i], a.rp[i + 1]);
             }
             restarts++;
             recursive = false;
@@ -499,9 +567,7 @@ __device__ void mg_pcg_body(const MgArgs& a, int cta, int nctas) {
             const MgLevel& F = lv[0];
             const MgLevel& G = lv[1];
             for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
-                double res = a.r[i];
-                for (int kk = a.rp[i]; kk < a.rp[i + 1]; kk++) res -= a.val[kk] * __ldcg(&a.z0[a.ci[kk]]);
-                a.w[i] = res;
+                a.w[i] = a.r[i] - gather_dot<4>(a.ci, a.val, a.z0, a.rp[i], a.rp[i + 1]);
             }
             __syncthreads();
             const bool smooth = (C > 1) || a.cinv == nullptr;
@@ -522,9 +588,8 @@ __device__ void mg_pcg_body(const MgArgs& a, int cta, int nctas) {
             const MgLevel& G = lv[l + 1];
             const bool smooth = (l + 1 < C) || a.cinv == nullptr;
             for (int J = grp; J < G.n; J += ngrp) {
-                double s = 0;
-                for (int m = F.mptr[J] + glane; m < F.mptr[J + 1]; m += kGroup) s += __ldcg(&F.r[F.midx[m]]);
-                for (int e = F.ra_ptr[J] + glane; e < F.ra_ptr[J + 1]; e += kGroup) s -= F.ra_val[e] * __ldcg(&F.z[F.ra_col[e]]);
+                double s = gather_sum<2>(F.midx, F.r, F.mptr[J], F.mptr[J + 1], glane, kGroup) -
+                           gather_dot<4>(F.ra_col, F.ra_val, F.z, F.ra_ptr[J], F.ra_ptr[J + 1], glane, kGroup);
                 s = group_sum(s, gmask);
                 if (glane == 0) {
                     G.r[J] = s;
@@ -556,9 +621,7 @@ __device__ void mg_pcg_body(const MgArgs& a, int cta, int nctas) {
             const MgLevel& F = lv[l];
             const double* zc = lv[l + 1].zf;
             for (int I = grp; I < F.n; I += ngrp) {
-                double w = 0;
-                for (int kk = F.rp[I] + glane; kk < F.rp[I + 1]; kk += kGroup)
-                    w -= F.val[kk] * (__ldcg(&F.z[F.ci[kk]]) + __ldcg(&zc[F.cagg[kk]]));
+                double w = -gather_dot2<4>(F.ci, F.cagg, F.val, F.z, zc, F.rp[I], F.rp[I + 1], glane, kGroup);
                 w = group_sum(w, gmask);
                 if (glane == 0) {
                     const double zp = __ldcg(&F.z[I]) + __ldcg(&zc[F.agg[I]]);
@@ -574,10 +637,7 @@ __device__ void mg_pcg_body(const MgArgs& a, int cta, int nctas) {
             const int32_t* agg = lv[0].agg;
             const int32_t* cagg = lv[0].cagg;
             for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
-                double w = a.r[i];
-                for (int kk = a.rp[i]; kk < a.rp[i + 1]; kk++)
-                    w -= a.val[kk] * (__ldcg(&a.z0[a.ci[kk]]) + __ldcg(&zc[cagg[kk]]));
-                a.w[i] = w;
+                a.w[i] = a.r[i] - gather_dot2<4>(a.ci, cagg, a.val, a.z0, zc, a.rp[i], a.rp[i + 1]);
                 a.z[i] = a.z0[i] + __ldcg(&zc[agg[i]]);
             }
             __syncthreads();
@@ -597,8 +657,7 @@ __device__ void mg_pcg_body(const MgArgs& a, int cta, int nctas) {
         // ---- q = A z + beta q, p = z + beta p; p.q ----
         double pq_l = 0;
         for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
-            double w = 0;
-            for (int kk = a.rp[i]; kk < a.rp[i + 1]; kk++) w += a.val[kk] * __ldcg(&a.z[a.ci[kk]]);
+            const double w = gather_dot<4>(a.ci, a.val, a.z, a.rp[i], a.rp[i + 1]);
             const double zi = a.z[i];
             const double qi = fresh ? w : w + beta * a.q[i];
             const double pi = fresh ? zi : zi + beta * a.p[i];
