@@ -74,7 +74,7 @@ cicy_status cicy_ctx_destroy(cicy_ctx* ctx) {
     cudaSetDevice(ctx->c.device);
     if (ctx->c.stream) cudaStreamSynchronize(ctx->c.stream);
     if (ctx->c.own_stream && ctx->c.stream) cudaStreamDestroy(ctx->c.stream);
-    delete ctx;  // DBuf members hold raw device pointers; the process-wide context frees them at exit
+    delete ctx;  // frees every device buffer of the context
     return CICY_OK;
 }
 

@@ -27,6 +27,19 @@ struct DeaSystem {
     int mg_levels = 0;
     int fallback = 0;  // 1: the learned preconditioner failed and Jacobi-PCG solved the system
     std::vector<int32_t> h_chain_start, h_chain_len;
+    // scalar fields back to their defaults (device buffers are kept)
+    void reset() {
+        cluster = -1;
+        pass = -2;
+        nodes = reserved = nnz_lower = iterations = 0;
+        restarts = 0;
+        cluster_solver = false;
+        mg_levels = 0;
+        fallback = 0;
+        rel_residual = seconds = 0;
+        h_chain_start.clear();
+        h_chain_len.clear();
+    }
     double rel_residual = 0, seconds = 0;
     // device: strict-lower CSR of the free block (SSS), diagonal, rhs, x0, voltages (all nodes)
     DBuf<int32_t> row_ptr, col;
@@ -34,6 +47,9 @@ struct DeaSystem {
 };
 
 struct Ctx {
+    Ctx() = default;
+    Ctx(const Ctx&) = delete;
+    Ctx& operator=(const Ctx&) = delete;
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -90,6 +106,7 @@ struct Ctx {
 
     // ---- DEA ----
     std::vector<DeaSystem*> systems;
+    std::vector<DeaSystem*> sys_pool;  // systems of earlier runs, reused
     DBuf<int32_t> lmm;         // node of each point in the current solve (-1 none)
     DBuf<int32_t> cnt_nodes, cnt_node_base, cnt_fresh, claim;
     DBuf<int32_t> e_n1, e_n2, e_op;

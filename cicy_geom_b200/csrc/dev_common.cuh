@@ -34,11 +34,32 @@ struct Fail {
 
 #define CICY_LAUNCH_CHECK() CICY_CUDA(cudaGetLastError())
 
+// Grow-only device buffer; owns its allocation (freed on destruction, moves
+// transfer it, copies are not allowed).
 template <class T>
 struct DBuf {
     T* p = nullptr;
     size_t cap = 0;
     size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    DBuf(DBuf&& o) noexcept : p(o.p), cap(o.cap), n(o.n) {
+        o.p = nullptr;
+        o.cap = o.n = 0;
+    }
+    DBuf& operator=(DBuf&& o) noexcept {
+        if (this != &o) {
+            release();
+            p = o.p;
+            cap = o.cap;
+            n = o.n;
+            o.p = nullptr;
+            o.cap = o.n = 0;
+        }
+        return *this;
+    }
+    ~DBuf() { release(); }
     void ensure(size_t need) {
         n = need;
         if (need <= cap) return;

@@ -43,6 +43,7 @@
 #include <vector>
 
 #include "solver.cuh"
+#include "trace.cuh"
 
 namespace cicy {
 
@@ -815,6 +816,7 @@ int pairwise(MgWork& g, int l, cudaStream_t s, int64_t& launches) {
 void build_mg_hierarchy(SolverWork& w, const SolverSystem& sys, cudaStream_t s, int64_t& launches) {
     MgWork& g = w.mg;
     const int n = sys.n;
+    TraceSeq tr(s);
     g.total.ensure(2);
     if (g.L.empty()) g.L.resize(1);
     MgWork::Lvl& L0 = g.L[0];
@@ -832,9 +834,11 @@ void build_mg_hierarchy(SolverWork& w, const SolverSystem& sys, cudaStream_t s, 
     int C = 0;
     for (int l = 0;; l++) {
         coarsen(g, l, nc, s, launches);
+        tr.mark("mg.coarsen");
         C = l + 1;
         if (g.L[C].n <= kMgDenseMax || C + 1 >= kMgMaxLevels) break;
         const int nc2 = pairwise(g, C, s, launches);
+        tr.mark("mg.pairwise");
         if (nc2 > 0.9 * g.L[C].n) break;
         nc = nc2;
     }
@@ -850,6 +854,7 @@ void build_mg_hierarchy(SolverWork& w, const SolverSystem& sys, cudaStream_t s, 
         launches += 2;
         g.dense = true;
     }
+    tr.mark("mg.coarsest");
     // restriction rows P^T A_l (levels 1 .. C-1) and column aggregates (levels 0 .. C-1)
     for (int l = 0; l < C; l++) {
         MgWork::Lvl& L = g.L[l];
@@ -871,6 +876,7 @@ void build_mg_hierarchy(SolverWork& w, const SolverSystem& sys, cudaStream_t s, 
                                                 L.ra_ptr.get(), L.ra_col.get(), L.ra_val.get());
         launches += 2;
     }
+    tr.mark("mg.restriction_rows");
     // work vectors and device descriptors
     g.host_lv.assign(C + 1, MgLevel{});
     for (int l = 0; l <= C; l++) {

@@ -467,6 +467,7 @@ int grid_for(long long n, int threads = 256) {
 
 Ctx::~Ctx() {
     for (auto* s : systems) delete s;
+    for (auto* s : sys_pool) delete s;
 }
 
 int32_t read_i32(Ctx& c, const int32_t* dptr) {

@@ -215,12 +215,14 @@ __global__ void k_edge_keys(int ne, int bn, const int32_t* __restrict__ n1, cons
     }
 }
 
-// diagonal[node] += g in insertion order (Add_new_elements_to_2d_sparse_matrix et al.)
-__global__ void k_diag_reduce(int n2e, uint64_t skip, const uint64_t* __restrict__ dkey, const uint32_t* __restrict__ dval,
+// diagonal[node] += g in insertion order (Add_new_elements_to_2d_sparse_matrix et al.).
+// Only free nodes: the prescribed nodes' diagonal is dropped (From_2d_to_1d_vectors)
+// and their runs, one entry per boundary element, are the longest ones.
+__global__ void k_diag_reduce(int n2e, uint64_t skip, uint64_t reserved, const uint64_t* __restrict__ dkey, const uint32_t* __restrict__ dval,
                               const double* __restrict__ g, double* __restrict__ diag_all) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n2e; i += gridDim.x * blockDim.x) {
         uint64_t k = dkey[i];
-        if (k == skip) continue;
+        if (k == skip || k < reserved) continue;
         if (i > 0 && dkey[i - 1] == k) continue;
         double s = 0;
         for (int j = i; j < n2e && dkey[j] == k; j++) s += g[dval[j]];
@@ -587,7 +589,15 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
     if (nbnd < 0) throw Fail{CICY_E_INPUT, "Compute_voltage_field: invalid family"};
     const int reserved = nbnd;  // Get_global_nodes: 2/4/6
     const int NM = in.n_members;
-    DeaSystem* sys = new DeaSystem;
+    // systems of earlier runs are recycled: their grow-only device buffers stay allocated
+    DeaSystem* sys;
+    if (!c.sys_pool.empty()) {
+        sys = c.sys_pool.back();
+        c.sys_pool.pop_back();
+        sys->reset();
+    } else {
+        sys = new DeaSystem;
+    }
     sys->cluster = in.cluster;
     sys->pass = in.pass;
     sys->reserved = reserved;
@@ -663,15 +673,18 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
         c.launches++;
         radix_sort_pairs(c.sort_k.get(), c.sort_v.get(), NE, 2 * bn + 1, c.rs, s, c.launches);
         radix_sort_pairs(dkey.get(), dval.get(), ND, bn + 1, c.rs, s, c.launches);
+        tr.mark("asm.sorts");
         c.work_f64a.ensure(std::max(nodes, NE) + 1);  // diag over all nodes
         CICY_CUDA(cudaMemsetAsync(c.work_f64a.get(), 0, sizeof(double) * (nodes + 1), s));
-        k_diag_reduce<<<grid_for(ND), 256, 0, s>>>(ND, 1ull << bn, dkey.get(), dval.get(), c.e_g.get(), c.work_f64a.get());
+        k_diag_reduce<<<grid_for(ND), 256, 0, s>>>(ND, 1ull << bn, (uint64_t)reserved, dkey.get(), dval.get(), c.e_g.get(),
+                                                   c.work_f64a.get());
         c.work_i32a.ensure(NE + 1);
         c.work_i32b.ensure(NE + 1);
         c.work_i32c.ensure(NE + 1);
         c.runval.ensure(NE + 1);
         k_offdiag_reduce<<<grid_for(NE), 256, 0, s>>>(NE, 1ull << (2 * bn), c.sort_k.get(), c.sort_v.get(), c.e_op.get(), c.e_g.get(), c.work_i32a.get(),
                                                     c.runval.get());
+        tr.mark("asm.reduce");
         k_sss_flags<<<grid_for(NE), 256, 0, s>>>(NE, bn, reserved, c.sort_k.get(), c.work_i32a.get(), c.work_i32b.get());
         exclusive_scan_i32(c.work_i32b.get(), c.work_i32c.get(), NE, c.i32_scalar.get(), c.scan_tmp32, s, c.launches);
         c.launches += 3;
@@ -685,6 +698,7 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
         k_sss_fill<<<grid_for(NE), 256, 0, s>>>(NE, bn, reserved, c.sort_k.get(), c.work_i32b.get(), c.work_i32c.get(), c.runval.get(),
                                               c.cnt_nodes.get(), sys->col.get(), sys->val.get());
         exclusive_scan_i32(c.cnt_nodes.get(), sys->row_ptr.get(), n + 1, nullptr, c.scan_tmp32, s, c.launches);
+        tr.mark("asm.sss");
         // Get_voltage_vector (Direct_Electrifying.cpp:1472-1500)
         std::vector<double> vef(reserved, 0.0);
         const double V = r_flag ? p.applied_voltage : (double)nodes;
@@ -835,7 +849,7 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
         CICY_CUDA(cudaStreamSynchronize(s));
         sys->rel_residual = rel;
     } catch (...) {
-        delete sys;
+        c.sys_pool.push_back(sys);
         throw;
     }
     return sys;
@@ -848,7 +862,7 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
 void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out) {
     if (c.stage < 3) throw Fail{CICY_E_STATE, "cicy_electrical_analysis: run cicy_clusters first"};
     cudaStream_t s = c.stream;
-    for (auto* sy : c.systems) delete sy;
+    for (auto* sy : c.systems) c.sys_pool.push_back(sy);
     c.systems.clear();
     const int NC = std::max(c.n_cnts, 1);
     // current elements_cnt state of every CNT: [lo, hi] into elem_idx
