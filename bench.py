@@ -69,7 +69,9 @@ def dist_env():
 def workload(rank: int, side: float = SIDE, cnts: int = N_CNTS):
     from cicy_geom_b200.network import NetworkConfig, generate_cnt_network
 
-    cfg = NetworkConfig(side=side, n_cnts=cnts, seed=2_000_000 + rank, tolerance=TOL, tolerance_unit=TOL_UNIT)
+    from cicy_geom_b200.replicas import seed
+
+    cfg = NetworkConfig(side=side, n_cnts=cnts, seed=seed(rank), tolerance=TOL, tolerance_unit=TOL_UNIT)
     raw = generate_cnt_network(cfg)
     return cfg, raw, raw.extract_window(cfg)
 
@@ -358,11 +360,10 @@ def run_ours(args):
     from cicy_geom_b200._abi import Result, check, lib
     from cicy_geom_b200.device import Context
 
-    rank, world, local = dist_env()
-    if world > 1:
-        import torch.distributed as dist
+    from cicy_geom_b200 import replicas
 
-        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo", timeout=__import__("datetime").timedelta(seconds=600))
+    rank, world, local = replicas.env()
+    replicas.init(world, gpu=torch.cuda.is_available())
     torch.cuda.set_device(local)
     cfg, raw, net = workload(rank, args.side, args.cnts)
     params = cfg.params()
@@ -381,8 +382,7 @@ def run_ours(args):
         step()
     # ---- device-resident timing ----
     def barrier():
-        if world > 1:
-            torch.distributed.barrier()
+        replicas.barrier(world)
         torch.cuda.synchronize()
 
     per_kernel = {}  # kernel kind -> [device seconds, launches, algorithmic bytes]
@@ -424,10 +424,7 @@ def run_ours(args):
     e1.record(stream)
     barrier()
     t_e2e = e0.elapsed_time(e1) * 1e-3
-    t = torch.tensor([t_dev, t_e2e], dtype=torch.float64, device=f"cuda:{local}")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    t_dev, t_e2e = float(t[0]), float(t[1])
+    t_dev, t_e2e = replicas.max_over_ranks([t_dev, t_e2e], world, device=f"cuda:{local}")
     if rank == 0:
         peaks = {}
         pk_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -480,8 +477,7 @@ def run_ours(args):
                 line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
                 line["R_x_reference"] = cb["R"][0]
         print(json.dumps(line))
-    if world > 1:
-        torch.distributed.destroy_process_group()
+    replicas.finish(world)
     return 0
 
 
