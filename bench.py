@@ -45,7 +45,7 @@ KERNELS = {0: "k_pcg (grid-wide persistent PCG)", 1: "k_pcg_cluster (16-CTA clus
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
@@ -77,14 +77,54 @@ def workload(rank: int, side: float = SIDE, cnts: int = N_CNTS):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region.
+
+    NVML is read every 10 ms from a thread (read-only queries; the same
+    counters nvidia-smi prints); without NVML, nvidia-smi at its 100 ms
+    floor.  Rows: sm MHz, max sm MHz, power W, hw_slowdown,
+    hw_thermal_slowdown, sw_thermal_slowdown, sw_power_cap (bools).
+    """
+
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index: int):
         self.index = index
         self.rows = []
         self.proc = None
+        self.stop = threading.Event()
+        self.source = None
 
     def __enter__(self):
+        try:
+            import pynvml as N
+
+            N.nvmlInit()
+            h = N.nvmlDeviceGetHandleByIndex(self.index)
+            bits = [N.nvmlClocksEventReasonHwSlowdown, N.nvmlClocksEventReasonHwThermalSlowdown,
+                    N.nvmlClocksEventReasonSwThermalSlowdown, N.nvmlClocksEventReasonSwPowerCap]
+            mx = float(N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM))
+
+            def sample():
+                r = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+                return [float(N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)), mx, N.nvmlDeviceGetPowerUsage(h) / 1000.0] + \
+                       [bool(r & b) for b in bits]
+
+            sample()
+
+            def loop():
+                while not self.stop.is_set():
+                    try:
+                        self.rows.append(sample())
+                    except Exception:
+                        pass
+                    self.stop.wait(0.01)
+
+            self.t = threading.Thread(target=loop, daemon=True)
+            self.t.start()
+            self.source = "nvml 10 ms"
+            return self
+        except Exception:
+            pass
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
@@ -97,6 +137,7 @@ class ClockSampler:
             while not self.rows and time.time() - t0 < 5.0 and self.proc.poll() is None:
                 time.sleep(0.05)
             self.rows.clear()
+            self.source = "nvidia-smi 100 ms"
         except FileNotFoundError:
             self.proc = None
         return self
@@ -104,26 +145,32 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) == 7:
-                self.rows.append(parts)
+            if len(parts) != 7:
+                continue
+            try:
+                self.rows.append([float(parts[0]), float(parts[1]), float(parts[2])] +
+                                 [p.lower().startswith("active") for p in parts[3:]])
+            except ValueError:
+                pass
 
     def __exit__(self, *a):
+        self.stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        elif self.source:
+            self.t.join(timeout=1.0)
 
     def summary(self):
-        if not self.rows:
+        rows = list(self.rows)
+        if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i].lower().startswith("active")})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(self.rows)}
+        reasons = sorted({self.NAMES[i] for r in rows for i in range(4) if r[3 + i]})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
+                "samples": len(rows), "power_w_median": statistics.median(r[2] for r in rows), "source": self.source}
 
 
 def pinned_network(net):

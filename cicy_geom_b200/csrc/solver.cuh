@@ -102,11 +102,11 @@ struct MgWork {
     std::vector<Lvl> L;
     std::vector<MgLevel> host_lv;
     DBuf<MgLevel> dev_lv;
-    DBuf<double> cinv, z0, wtmp;
+    DBuf<double> cinv, z0, wtmp, sval;
     DBuf<unsigned long long> bar;
     DBuf<uint64_t> keys;
     DBuf<uint32_t> vals;
-    DBuf<int32_t> flag, pos, head, uidx, row, mate, best, rep, total, scan_tmp;
+    DBuf<int32_t> flag, pos, head, uidx, mate, best, rep, total, scan_tmp;
     RadixScratch radix;
     int levels = 0;
     bool dense = false;

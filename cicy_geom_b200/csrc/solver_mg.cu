@@ -22,9 +22,10 @@
 //             memory, 1e-8 diagonal regularisation, variables with a vanishing
 //             pivot dropped); otherwise an l1-Jacobi step
 //
-// Coarse operators are Galerkin products P^T A P with piecewise-constant P, built
-// by sort-and-reduce of the cross-aggregate couplings (stable radix sort, runs
-// summed in input order: deterministic).  Their diagonals come from summed row
+// Coarse operators are Galerkin products P^T A P with piecewise-constant P: one
+// thread per aggregate gathers its members' cross-aggregate couplings, sorts
+// them stably by coarse column and sums each run in order (deterministic, no
+// host synchronisation inside a level).  Their diagonals come from summed row
 // sums, diag_J = sum_{I in J} rowsum_I - sum_{J' != J} A_JJ', so the large
 // intra-aggregate conductances never cancel in floating point and an aggregate
 // with no outside coupling gets an exact zero row.  Levels >= 1 are smoothed by
@@ -84,96 +85,6 @@ __global__ void k_rowsum0(int n, const int32_t* __restrict__ rp, const int32_t* 
             if (ci[k] == i) d = v[k];
         }
         rs[i] = (fabs(s) <= 1e-13 * fabs(d)) ? 0.0 : s;
-    }
-}
-
-// Per nonzero: 1 if it couples two different aggregates.
-__global__ void k_cross_flags(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const int32_t* __restrict__ agg,
-                              int32_t* __restrict__ flag) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int ai = agg[i];
-        for (int k = rp[i]; k < rp[i + 1]; k++) flag[k] = agg[ci[k]] != ai ? 1 : 0;
-    }
-}
-
-__global__ void k_cross_keys(int n, int b, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                             const int32_t* __restrict__ agg, const int32_t* __restrict__ flag, const int32_t* __restrict__ pos,
-                             uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint64_t ai = (uint64_t)agg[i] << b;
-        for (int k = rp[i]; k < rp[i + 1]; k++)
-            if (flag[k]) {
-                keys[pos[k]] = ai | (uint64_t)agg[ci[k]];
-                vals[pos[k]] = (uint32_t)k;
-            }
-    }
-}
-
-__global__ void k_run_heads64(int n, const uint64_t* __restrict__ keys, int32_t* __restrict__ head) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        head[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1 : 0;
-}
-
-// One thread per run of equal keys: sum its values in sorted (= input) order.
-__global__ void k_run_reduce(int n, int b, const uint64_t* __restrict__ keys, const uint32_t* __restrict__ vals,
-                             const int32_t* __restrict__ head, const int32_t* __restrict__ uidx, const double* __restrict__ src,
-                             int32_t* __restrict__ row, int32_t* __restrict__ col, double* __restrict__ out) {
-    const uint64_t mask = (b >= 64) ? ~0ull : ((1ull << b) - 1);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        if (!head[i]) continue;
-        const uint64_t key = keys[i];
-        double s = 0;
-        for (int j = i; j < n && keys[j] == key; j++) s += src[vals[j]];
-        const int u = uidx[i];
-        row[u] = (int32_t)(key >> b);
-        col[u] = (int32_t)(key & mask);
-        out[u] = s;
-    }
-}
-
-// CSR row pointers from the (sorted) row index of each entry.
-__global__ void k_row_ptr(int m, int nrows, const int32_t* __restrict__ row, int32_t* __restrict__ rp) {
-    for (int u = blockIdx.x * blockDim.x + threadIdx.x; u <= m; u += gridDim.x * blockDim.x) {
-        const int lo = (u == 0) ? 0 : row[u - 1] + 1;
-        const int hi = (u == m) ? nrows : row[u];
-        for (int r = lo; r <= hi && r <= nrows; r++) rp[r] = u;
-        if (u == m && m == 0)
-            for (int r = 0; r <= nrows; r++) rp[r] = 0;
-    }
-}
-
-__global__ void k_member_keys(int n, const int32_t* __restrict__ agg, uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        keys[i] = (uint64_t)agg[i];
-        vals[i] = (uint32_t)i;
-    }
-}
-
-__global__ void k_member_lists(int n, const uint64_t* __restrict__ keys, const uint32_t* __restrict__ vals, int32_t* __restrict__ row,
-                               int32_t* __restrict__ midx) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        row[i] = (int32_t)keys[i];
-        midx[i] = (int32_t)vals[i];
-    }
-}
-
-// Coarse row sums, diagonal and l1-Jacobi weights.
-__global__ void k_coarse_diag(int nc, const int32_t* __restrict__ mptr, const int32_t* __restrict__ midx, const double* __restrict__ rs_f,
-                              const int32_t* __restrict__ rp, const double* __restrict__ v, double* __restrict__ rs,
-                              double* __restrict__ diag, double* __restrict__ l1inv) {
-    for (int J = blockIdx.x * blockDim.x + threadIdx.x; J < nc; J += gridDim.x * blockDim.x) {
-        double s = 0;
-        for (int m = mptr[J]; m < mptr[J + 1]; m++) s += rs_f[midx[m]];
-        double off = 0, offabs = 0;
-        for (int k = rp[J]; k < rp[J + 1]; k++) {
-            off += v[k];
-            offabs += fabs(v[k]);
-        }
-        const double d = s - off;
-        rs[J] = s;
-        diag[J] = d;
-        const double l1 = fabs(d) + offabs;
-        l1inv[J] = l1 > 0 ? 1.0 / l1 : 0.0;
     }
 }
 
@@ -247,9 +158,9 @@ __global__ void __launch_bounds__(kGjThreads) k_gauss_jordan(int n, double* __re
     extern __shared__ double S[];  // n * n + n
     double* f = S + (size_t)n * n;
     __shared__ double dmax_s;
-    __shared__ int drop_s;
-    const int t = threadIdx.x, T = blockDim.x;
-    for (int e = t; e < n * n; e += T) S[e] = M[e];
+    // thread (tx, ty) of a 32 x 32 layout owns rows ty, ty + 32, ... and columns tx, tx + 32, ...
+    const int t = threadIdx.x, tx = t & 31, ty = t >> 5;
+    for (int e = t; e < n * n; e += kGjThreads) S[e] = M[e];
     __syncthreads();
     if (t == 0) {
         double m = 0;
@@ -258,46 +169,30 @@ __global__ void __launch_bounds__(kGjThreads) k_gauss_jordan(int n, double* __re
     }
     __syncthreads();
     const double thr = 1e-12 * dmax_s;
-    for (int i = t; i < n; i += T) S[i * n + i] *= (1.0 + 1e-8);
+    for (int i = t; i < n; i += kGjThreads) S[i * n + i] *= (1.0 + 1e-8);
     __syncthreads();
     for (int k = 0; k < n; k++) {
-        const double p = S[k * n + k];
-        if (t == 0) drop_s = !(p > thr);
-        __syncthreads();
-        if (drop_s) {
-            for (int j = t; j < n; j += T) {
+        const double p = S[k * n + k];  // every thread reads the same pivot: uniform branch
+        if (!(p > thr)) {               // vanishing pivot: drop variable k
+            for (int j = t; j < n; j += kGjThreads) {
                 S[k * n + j] = 0.0;
                 S[j * n + k] = 0.0;
             }
             __syncthreads();
             continue;
         }
-        for (int j = t; j < n; j += T) f[j] = (j == k) ? 0.0 : S[j * n + k];
+        // column k of the other rows (multipliers) and the scaled pivot row: disjoint entries
+        for (int i = t; i < n; i += kGjThreads) f[i] = (i == k) ? 0.0 : S[i * n + k];
+        for (int j = t; j < n; j += kGjThreads) S[k * n + j] = ((j == k) ? 1.0 : S[k * n + j]) / p;
         __syncthreads();
-        for (int j = t; j < n; j += T) S[k * n + j] = ((j == k) ? 1.0 : S[k * n + j]) / p;
-        __syncthreads();
-        for (int e = t; e < n * n; e += T) {
-            const int i = e / n, j = e - i * n;
+        for (int i = ty; i < n; i += 32) {
             if (i == k) continue;
-            S[e] = ((j == k) ? 0.0 : S[e]) - f[i] * S[k * n + j];
+            const double fi = f[i];
+            for (int j = tx; j < n; j += 32) S[i * n + j] = ((j == k) ? 0.0 : S[i * n + j]) - fi * S[k * n + j];
         }
         __syncthreads();
     }
-    for (int e = t; e < n * n; e += T) M[e] = S[e];
-}
-
-// Restriction operator rows P^T A_l of a level l >= 1: row J lists, for each
-// member I of aggregate J (ascending), (I, diag_I) and then row I's couplings.
-__global__ void k_ra_len(int nc, const int32_t* __restrict__ mptr, const int32_t* __restrict__ midx, const int32_t* __restrict__ rp,
-                         int32_t* __restrict__ len) {
-    for (int J = blockIdx.x * blockDim.x + threadIdx.x; J < nc; J += gridDim.x * blockDim.x) {
-        int s = 0;
-        for (int m = mptr[J]; m < mptr[J + 1]; m++) {
-            const int I = midx[m];
-            s += 1 + rp[I + 1] - rp[I];
-        }
-        len[J] = s;
-    }
+    for (int e = t; e < n * n; e += kGjThreads) M[e] = S[e];
 }
 
 __global__ void k_ra_fill(int nc, const int32_t* __restrict__ mptr, const int32_t* __restrict__ midx, const int32_t* __restrict__ rp,
@@ -317,12 +212,6 @@ __global__ void k_ra_fill(int nc, const int32_t* __restrict__ mptr, const int32_
             }
         }
     }
-}
-
-// Aggregate of each nonzero's column, so prolongated values load without a
-// dependent index load.
-__global__ void k_cagg(int nnz, const int32_t* __restrict__ ci, const int32_t* __restrict__ agg, int32_t* __restrict__ cagg) {
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += gridDim.x * blockDim.x) cagg[k] = agg[ci[k]];
 }
 
 // ---------------------------------------------------------------------------
@@ -710,70 +599,239 @@ __global__ void __launch_bounds__(kMgClusterThreads) k_mg_batch(const MgArgs* __
     }
 }
 
-// Galerkin coarse level l+1 from level l and its aggregates (g.L[l].agg, nc of them).
+// Exclusive scan of n ints in one CTA (the setup's arrays are short enough):
+// each thread scans a contiguous chunk; out may alias in; *total gets the sum.
+__global__ void __launch_bounds__(1024) k_scan_single(const int32_t* in, int32_t* out, int n, int32_t* total) {
+    __shared__ int32_t part[1024];
+    const int t = threadIdx.x, T = blockDim.x;
+    const int ch = (n + T - 1) / T;
+    const int lo = min(n, t * ch), hi = min(n, lo + ch);
+    int32_t s = 0;
+    for (int i = lo; i < hi; i++) s += in[i];
+    part[t] = s;
+    __syncthreads();
+    for (int o = 1; o < T; o <<= 1) {  // Hillis-Steele inclusive scan of the chunk sums
+        const int32_t v = t >= o ? part[t - o] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    int32_t run = part[t] - s;
+    for (int i = lo; i < hi; i++) {
+        const int32_t v = in[i];
+        out[i] = run;
+        run += v;
+    }
+    if (t == T - 1 && total) *total = part[T - 1];
+}
+
+void scan_small(const int32_t* in, int32_t* out, int n, int32_t* total, MgWork& g, cudaStream_t s, int64_t& launches) {
+    if (n <= (1 << 20)) {
+        k_scan_single<<<1, 1024, 0, s>>>(in, out, n, total);
+        launches++;
+    } else {
+        exclusive_scan_i32(in, out, n, total, g.scan_tmp, s, launches);
+    }
+}
+
+// Members of level-0 aggregates (chain blocks: consecutive rows).
+__global__ void k_members_contig(int n, int nc, const int32_t* __restrict__ agg, int32_t* __restrict__ mptr, int32_t* __restrict__ midx) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (i == 0 || agg[i] != agg[i - 1]) mptr[agg[i]] = i;
+        midx[i] = i;
+        if (i == n - 1) mptr[nc] = n;
+    }
+}
+
+__global__ void k_member_count(int n, const int32_t* __restrict__ agg, int32_t* __restrict__ cnt) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) atomicAdd(&cnt[agg[i]], 1);
+}
+
+__global__ void k_member_place(int n, const int32_t* __restrict__ agg, const int32_t* __restrict__ mptr, int32_t* __restrict__ cursor,
+                               int32_t* __restrict__ midx) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int J = agg[i];
+        midx[mptr[J] + atomicAdd(&cursor[J], 1)] = i;
+    }
+}
+
+// Members of every aggregate in ascending row order (insertion sort; aggregates are small).
+__global__ void k_member_sort(int nc, const int32_t* __restrict__ mptr, int32_t* __restrict__ midx) {
+    for (int J = blockIdx.x * blockDim.x + threadIdx.x; J < nc; J += gridDim.x * blockDim.x) {
+        const int b = mptr[J], e = mptr[J + 1];
+        for (int i = b + 1; i < e; i++) {
+            const int v = midx[i];
+            int j = i - 1;
+            while (j >= b && midx[j] > v) {
+                midx[j + 1] = midx[j];
+                j--;
+            }
+            midx[j + 1] = v;
+        }
+    }
+}
+
+// Per aggregate: couplings gathered from its members' rows (seg_len) and the
+// length of its restriction row P^T A_l (members' rows with their diagonals).
+__global__ void k_agg_lengths(int nc, const int32_t* __restrict__ mptr, const int32_t* __restrict__ midx, const int32_t* __restrict__ rp,
+                              int32_t* __restrict__ seg_len, int32_t* __restrict__ ra_len) {
+    for (int J = blockIdx.x * blockDim.x + threadIdx.x; J < nc; J += gridDim.x * blockDim.x) {
+        int s = 0;
+        for (int m = mptr[J]; m < mptr[J + 1]; m++) {
+            const int I = midx[m];
+            s += rp[I + 1] - rp[I];
+        }
+        seg_len[J] = s;
+        if (ra_len) ra_len[J] = s + (mptr[J + 1] - mptr[J]);
+    }
+}
+
+// One coarse row per thread: the cross-aggregate couplings of the members (in
+// member then entry order) are gathered into scratch as keys (coarse column,
+// gather position), sorted (Shell sort: keys are unique, so the order equals a
+// stable sort by column) and summed per column in gather order (deterministic);
+// the row's diagonal comes from the summed row sums (no cancellation of the
+// large intra-aggregate entries), and its l1-Jacobi weight from |d| + sum |a|.
+__global__ void k_coarse_rows(int nc, const int32_t* __restrict__ mptr, const int32_t* __restrict__ midx, const int32_t* __restrict__ rp,
+                              const int32_t* __restrict__ ci, const double* __restrict__ v, const int32_t* __restrict__ agg,
+                              const double* __restrict__ rs_f, const int32_t* __restrict__ seg_off, uint64_t* __restrict__ skey,
+                              double* __restrict__ sval, int32_t* __restrict__ ulen, double* __restrict__ rs_c, double* __restrict__ diag,
+                              double* __restrict__ l1inv) {
+    for (int J = blockIdx.x * blockDim.x + threadIdx.x; J < nc; J += gridDim.x * blockDim.x) {
+        const int o = seg_off[J];
+        int cnt = 0;
+        double rs = 0;
+        for (int m = mptr[J]; m < mptr[J + 1]; m++) {
+            const int I = midx[m];
+            rs += rs_f[I];
+            for (int k = rp[I]; k < rp[I + 1]; k++) {
+                const int c = agg[ci[k]];
+                if (c == J) continue;
+                skey[o + cnt] = ((uint64_t)(uint32_t)c << 32) | (uint32_t)cnt;
+                sval[o + cnt] = v[k];
+                cnt++;
+            }
+        }
+        int gap = 1;
+        while (gap * 9 / 4 + 1 < cnt) gap = gap * 9 / 4 + 1;
+        for (;; gap = max(1, (gap - 1) * 4 / 9)) {  // ..., 2, 1: the last pass is insertion sort
+            for (int i = gap; i < cnt; i++) {
+                const uint64_t key = skey[o + i];
+                const double x = sval[o + i];
+                int j = i;
+                while (j >= gap && skey[o + j - gap] > key) {
+                    skey[o + j] = skey[o + j - gap];
+                    sval[o + j] = sval[o + j - gap];
+                    j -= gap;
+                }
+                skey[o + j] = key;
+                sval[o + j] = x;
+            }
+            if (gap == 1) break;
+        }
+        int u = 0;
+        double off = 0, offabs = 0;
+        for (int i = 0; i < cnt;) {  // sum runs of equal columns, in gather order
+            const uint32_t c = (uint32_t)(skey[o + i] >> 32);
+            double acc = 0;
+            while (i < cnt && (uint32_t)(skey[o + i] >> 32) == c) acc += sval[o + i++];
+            skey[o + u] = c;
+            sval[o + u] = acc;
+            u++;
+            off += acc;
+            offabs += fabs(acc);
+        }
+        ulen[J] = u;
+        const double d = rs - off;
+        rs_c[J] = rs;
+        diag[J] = d;
+        const double l1 = fabs(d) + offabs;
+        l1inv[J] = l1 > 0 ? 1.0 / l1 : 0.0;
+    }
+}
+
+__global__ void k_coarse_copy(int nc, const int32_t* __restrict__ seg_off, const int32_t* __restrict__ ulen, const int32_t* __restrict__ rp_c,
+                              const uint64_t* __restrict__ scol, const double* __restrict__ sval, int32_t* __restrict__ ci_c,
+                              double* __restrict__ v_c) {
+    for (int J = blockIdx.x * blockDim.x + threadIdx.x; J < nc; J += gridDim.x * blockDim.x) {
+        const int o = seg_off[J], d = rp_c[J];
+        for (int i = 0; i < ulen[J]; i++) {
+            ci_c[d + i] = (int32_t)scol[o + i];
+            v_c[d + i] = sval[o + i];
+        }
+    }
+}
+
+__global__ void k_cagg_rows(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const int32_t* __restrict__ agg,
+                            int32_t* __restrict__ cagg) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (int k = rp[i]; k < rp[i + 1]; k++) cagg[k] = agg[ci[k]];
+}
+
+// Galerkin coarse level l+1 from level l and its aggregates (g.L[l].agg, nc of
+// them), plus level l's member lists, restriction rows (l >= 1) and column
+// aggregates.  No host synchronisation: buffers are sized by the fine level's
+// non-zeros, an upper bound of the coarse level's.
 void coarsen(MgWork& g, int l, int nc, cudaStream_t s, int64_t& launches) {
     if ((int)g.L.size() < l + 2) g.L.resize(l + 2);
     MgWork::Lvl& F = g.L[l];
     MgWork::Lvl& G = g.L[l + 1];
     const int nf = F.n, nnz = F.nnz;
-    const int b = bits_for((uint64_t)std::max(nc - 1, 1));
-    // cross-aggregate couplings -> sorted (row, col) keys
-    g.flag.ensure(nnz + 1);
-    g.pos.ensure(nnz + 1);
-    k_cross_flags<<<grid_for(nf), 256, 0, s>>>(nf, F.rp_ptr, F.ci_ptr, F.agg.get(), g.flag.get());
-    launches++;
-    exclusive_scan_i32(g.flag.get(), g.pos.get(), nnz, g.total.get(), g.scan_tmp, s, launches);
-    int m = 0;
-    CICY_CUDA(cudaMemcpyAsync(&m, g.total.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
-    CICY_CUDA(cudaStreamSynchronize(s));
-    const int cap = std::max(std::max(m, nf), 1) + 1;
-    g.keys.ensure(cap);
-    g.vals.ensure(cap);
-    g.head.ensure(cap);
-    g.uidx.ensure(cap);
-    g.row.ensure(cap);
-    G.n = nc;
-    int nu = 0;
-    if (m > 0) {
-        k_cross_keys<<<grid_for(nf), 256, 0, s>>>(nf, b, F.rp_ptr, F.ci_ptr, F.agg.get(), g.flag.get(), g.pos.get(), g.keys.get(),
-                                                  g.vals.get());
-        launches++;
-        radix_sort_pairs(g.keys.get(), g.vals.get(), m, 2 * b, g.radix, s, launches);
-        k_run_heads64<<<grid_for(m), 256, 0, s>>>(m, g.keys.get(), g.head.get());
-        launches++;
-        exclusive_scan_i32(g.head.get(), g.uidx.get(), m, g.total.get(), g.scan_tmp, s, launches);
-        CICY_CUDA(cudaMemcpyAsync(&nu, g.total.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
-        CICY_CUDA(cudaStreamSynchronize(s));
-    }
-    G.nnz = nu;
-    G.rp.ensure(nc + 1);
-    G.ci.ensure(std::max(nu, 1));
-    G.val.ensure(std::max(nu, 1));
-    if (m > 0) {
-        k_run_reduce<<<grid_for(m), 256, 0, s>>>(m, b, g.keys.get(), g.vals.get(), g.head.get(), g.uidx.get(), F.val_ptr, g.row.get(),
-                                                 G.ci.get(), G.val.get());
-        launches++;
-    }
-    k_row_ptr<<<grid_for(nu + 1), 256, 0, s>>>(nu, nc, g.row.get(), G.rp.get());
-    launches++;
-    G.rp_ptr = G.rp.get();
-    G.ci_ptr = G.ci.get();
-    G.val_ptr = G.val.get();
-    // members of each aggregate, ascending row order
     F.mptr.ensure(nc + 1);
     F.midx.ensure(std::max(nf, 1));
-    k_member_keys<<<grid_for(nf), 256, 0, s>>>(nf, F.agg.get(), g.keys.get(), g.vals.get());
+    if (l == 0) {
+        k_members_contig<<<grid_for(nf), 256, 0, s>>>(nf, nc, F.agg.get(), F.mptr.get(), F.midx.get());
+        launches++;
+    } else {
+        g.flag.ensure(nc + 1);
+        CICY_CUDA(cudaMemsetAsync(g.flag.get(), 0, sizeof(int32_t) * (nc + 1), s));
+        k_member_count<<<grid_for(nf), 256, 0, s>>>(nf, F.agg.get(), g.flag.get());
+        scan_small(g.flag.get(), F.mptr.get(), nc + 1, nullptr, g, s, launches);
+        CICY_CUDA(cudaMemsetAsync(g.flag.get(), 0, sizeof(int32_t) * (nc + 1), s));
+        k_member_place<<<grid_for(nf), 256, 0, s>>>(nf, F.agg.get(), F.mptr.get(), g.flag.get(), F.midx.get());
+        k_member_sort<<<grid_for(nc), 256, 0, s>>>(nc, F.mptr.get(), F.midx.get());
+        launches += 3;
+    }
+    // lengths and offsets
+    g.pos.ensure(nc + 1);
+    g.head.ensure(nc + 1);
+    g.uidx.ensure(nc + 1);
+    if (l >= 1) F.ra_ptr.ensure(nc + 1);
+    k_agg_lengths<<<grid_for(nc), 256, 0, s>>>(nc, F.mptr.get(), F.midx.get(), F.rp_ptr, g.pos.get(), l >= 1 ? F.ra_ptr.get() : nullptr);
     launches++;
-    radix_sort_pairs(g.keys.get(), g.vals.get(), nf, b, g.radix, s, launches);
-    k_member_lists<<<grid_for(nf), 256, 0, s>>>(nf, g.keys.get(), g.vals.get(), g.row.get(), F.midx.get());
-    k_row_ptr<<<grid_for(nf + 1), 256, 0, s>>>(nf, nc, g.row.get(), F.mptr.get());
-    launches += 2;
-    // row sums, diagonal, l1 weights
+    scan_small(g.pos.get(), g.pos.get(), nc + 1, nullptr, g, s, launches);  // seg_off
+    // coarse rows
+    g.keys.ensure(std::max(nnz, 1));
+    g.sval.ensure(std::max(nnz, 1));
+    G.n = nc;
+    G.nnz = nnz;  // capacity bound
+    G.rp.ensure(nc + 1);
+    G.ci.ensure(std::max(nnz, 1));
+    G.val.ensure(std::max(nnz, 1));
     G.rs.ensure(nc);
     G.diag.ensure(nc);
     G.l1inv.ensure(nc);
-    k_coarse_diag<<<grid_for(nc), 256, 0, s>>>(nc, F.mptr.get(), F.midx.get(), F.rs.get(), G.rp.get(), G.val.get(), G.rs.get(),
-                                               G.diag.get(), G.l1inv.get());
+    k_coarse_rows<<<grid_for(nc, 128), 128, 0, s>>>(nc, F.mptr.get(), F.midx.get(), F.rp_ptr, F.ci_ptr, F.val_ptr, F.agg.get(), F.rs.get(),
+                                                  g.pos.get(), g.keys.get(), g.sval.get(), g.head.get(), G.rs.get(), G.diag.get(),
+                                                  G.l1inv.get());
+    scan_small(g.head.get(), G.rp.get(), nc + 1, nullptr, g, s, launches);
+    k_coarse_copy<<<grid_for(nc), 256, 0, s>>>(nc, g.pos.get(), g.head.get(), G.rp.get(), g.keys.get(), g.sval.get(), G.ci.get(),
+                                               G.val.get());
+    launches += 2;
+    G.rp_ptr = G.rp.get();
+    G.ci_ptr = G.ci.get();
+    G.val_ptr = G.val.get();
+    // restriction rows of level l (l >= 1) and its column aggregates
+    if (l >= 1) {
+        scan_small(F.ra_ptr.get(), F.ra_ptr.get(), nc + 1, nullptr, g, s, launches);
+        F.ra_col.ensure(std::max(nnz + nf, 1));
+        F.ra_val.ensure(std::max(nnz + nf, 1));
+        k_ra_fill<<<grid_for(nc), 256, 0, s>>>(nc, F.mptr.get(), F.midx.get(), F.rp_ptr, F.ci_ptr, F.val_ptr, F.diag.get(), F.ra_ptr.get(),
+                                                F.ra_col.get(), F.ra_val.get());
+        launches++;
+    }
+    F.cagg.ensure(std::max(nnz, 1));
+    k_cagg_rows<<<grid_for(nf), 256, 0, s>>>(nf, F.rp_ptr, F.ci_ptr, F.agg.get(), F.cagg.get());
     launches++;
     CICY_LAUNCH_CHECK();
 }
@@ -799,7 +857,7 @@ int pairwise(MgWork& g, int l, cudaStream_t s, int64_t& launches) {
     k_join<<<grid_for(n), 256, 0, s>>>(n, g.mate.get(), g.best.get(), g.rep.get());
     k_is_rep<<<grid_for(n), 256, 0, s>>>(n, g.rep.get(), g.flag.get());
     launches += 4;
-    exclusive_scan_i32(g.flag.get(), g.pos.get(), n, g.total.get(), g.scan_tmp, s, launches);
+    scan_small(g.flag.get(), g.pos.get(), n, g.total.get(), g, s, launches);
     F.agg.ensure(n + 1);
     k_agg_ids<<<grid_for(n), 256, 0, s>>>(n, g.rep.get(), g.pos.get(), F.agg.get());
     launches++;
@@ -855,27 +913,6 @@ void build_mg_hierarchy(SolverWork& w, const SolverSystem& sys, cudaStream_t s, 
         g.dense = true;
     }
     tr.mark("mg.coarsest");
-    // restriction rows P^T A_l (levels 1 .. C-1) and column aggregates (levels 0 .. C-1)
-    for (int l = 0; l < C; l++) {
-        MgWork::Lvl& L = g.L[l];
-        const int ncl = g.L[l + 1].n;
-        L.cagg.ensure(std::max(L.nnz, 1));
-        k_cagg<<<grid_for(L.nnz), 256, 0, s>>>(L.nnz, L.ci_ptr, L.agg.get(), L.cagg.get());
-        launches++;
-        if (l == 0) continue;
-        L.ra_ptr.ensure(ncl + 1);
-        k_ra_len<<<grid_for(ncl), 256, 0, s>>>(ncl, L.mptr.get(), L.midx.get(), L.rp_ptr, L.ra_ptr.get());
-        exclusive_scan_i32(L.ra_ptr.get(), L.ra_ptr.get(), ncl, g.total.get(), g.scan_tmp, s, launches);
-        int tot = 0;
-        CICY_CUDA(cudaMemcpyAsync(&tot, g.total.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
-        CICY_CUDA(cudaStreamSynchronize(s));
-        CICY_CUDA(cudaMemcpyAsync(L.ra_ptr.get() + ncl, &tot, sizeof(int), cudaMemcpyHostToDevice, s));
-        L.ra_col.ensure(std::max(tot, 1));
-        L.ra_val.ensure(std::max(tot, 1));
-        k_ra_fill<<<grid_for(ncl), 256, 0, s>>>(ncl, L.mptr.get(), L.midx.get(), L.rp_ptr, L.ci_ptr, L.val_ptr, L.diag.get(),
-                                                L.ra_ptr.get(), L.ra_col.get(), L.ra_val.get());
-        launches += 2;
-    }
     tr.mark("mg.restriction_rows");
     // work vectors and device descriptors
     g.host_lv.assign(C + 1, MgLevel{});
