@@ -288,9 +288,34 @@ def cg_bytes(nodes, reserved, nnz_lower, iters, s_val=8, s_v=8):
     return iters * (b_spmv + 12 * s_v * n)
 
 
+def direct_voltage_error(S, x):
+    """max |x - x_d| / max |x_d| over the rows connected to a prescribed node, x_d
+    the FP64 sparse direct solve (SuperLU) of the same system; rows of floating
+    islands (singular, no prescribed node) are left out."""
+    import scipy.sparse as sp
+    from scipy.sparse.csgraph import connected_components
+    from scipy.sparse.linalg import spsolve
+
+    from cicy_geom_b200.learned import full_csr
+
+    A = full_csr(S).tocsr()
+    n = A.shape[0]
+    C = A.tocoo()
+    off = C.row != C.col
+    nc, comp = connected_components(sp.coo_matrix((np.ones(off.sum()), (C.row[off], C.col[off])), shape=(n, n)), directed=False)
+    rs = np.asarray(A.sum(axis=1)).ravel()
+    g = np.zeros(nc, bool)
+    g[comp[rs > 1e-9 * A.diagonal()]] = True
+    idx = np.nonzero(g[comp])[0]
+    xd = spsolve(A[idx][:, idx].tocsc(), np.asarray(S["b"])[idx])
+    return float(np.max(np.abs(x[idx] - xd)) / np.max(np.abs(xd)))
+
+
 def solver_comparison(cfg, net, device, steps=2):
-    """The same network step with each preconditioner (device-resident, CUDA events):
-    upstream Jacobi-PCG ("plain CG"), chain block-Jacobi, learned, multigrid."""
+    """The same network step with each preconditioner and precision (device-resident,
+    CUDA events): upstream Jacobi-PCG ("plain CG"), chain block-Jacobi, learned,
+    multigrid in FP64, and Jacobi, chain and learned in mixed precision; per run
+    the real-pass voltages' error against an FP64 direct solve of the same system."""
     import ctypes as C
 
     import torch
@@ -299,9 +324,11 @@ def solver_comparison(cfg, net, device, steps=2):
     from cicy_geom_b200.device import Context
 
     out = {}
-    for name in ("jacobi", "chain", "learned", "mg"):
+    runs = [("jacobi", "jacobi", 0), ("chain", "chain", 0), ("learned", "learned", 0), ("mg", "mg", 0),
+            ("jacobi_mixed", "jacobi", 1), ("chain_mixed", "chain", 1), ("learned_mixed", "learned", 1)]
+    for name, pk, prec in runs:
         ctx = Context(device)
-        ctx.set_solver(preconditioner=PRECONDS[name])
+        ctx.set_solver(precision=prec, preconditioner=PRECONDS[pk], max_iter_factor=20)  # bounded: a stalled run stops early
         ctx.upload(net)
         params = cfg.params()
         res = Result()
@@ -316,11 +343,19 @@ def solver_comparison(cfg, net, device, steps=2):
         torch.cuda.synchronize()
         t = e0.elapsed_time(e1) * 1e-3 / steps
         sv = res.solves[: res.n_solves]
-        out[name] = {"networks_per_s": 1.0 / t, "ms_per_step": t * 1e3, "cg_iterations": [int(x.iterations) for x in sv],
-                     "cg_ms": [round(x.seconds * 1e3, 3) for x in sv], "fallback": [int(x.fallback) for x in sv],
-                     "max_rel_residual": max(x.rel_residual for x in sv), "R_x": res.resistances[0]}
+        real = [i for i in range(res.n_solves) if sv[i].pass_ >= 0]
+        verr = None
+        if real:
+            S = ctx.system(real[0])
+            verr = direct_voltage_error(S, np.asarray(S["voltages"])[S["reserved"]:])
+        out[name] = {"precision": "mixed" if prec else "fp64", "networks_per_s": 1.0 / t, "ms_per_step": t * 1e3,
+                     "cg_iterations": [int(x.iterations) for x in sv], "cg_ms": [round(x.seconds * 1e3, 3) for x in sv],
+                     "fallback": [int(x.fallback) for x in sv], "max_rel_residual": max(x.rel_residual for x in sv),
+                     "R_x": res.resistances[0], "real_pass_voltage_error_vs_fp64_direct": verr}
         ctx.close()
-    out["speedup_vs_jacobi"] = {k: out[k]["networks_per_s"] / out["jacobi"]["networks_per_s"] for k in ("chain", "learned", "mg")}
+    for name, _, _ in runs:
+        out[name]["R_x_rel_diff_vs_mg_fp64"] = abs(out[name]["R_x"] - out["mg"]["R_x"]) / abs(out["mg"]["R_x"])
+    out["speedup_vs_jacobi"] = {k: out[k]["networks_per_s"] / out["jacobi"]["networks_per_s"] for k, _, _ in runs if k != "jacobi"}
     return out
 
 
@@ -368,9 +403,13 @@ def spmv_roofline(ctx, device, hbm, target_bytes=320e6, reps=20):
 def batched_monte_carlo(count, device, reps=3):
     """Monte-Carlo sweep: `count` seeded realisations (cube side U[2,5] um, CNT
     volume fraction U[0.5%,3%]), each run through the device path to its
-    real-resistor system; then all systems solved at 1e-8 by one graph-captured
-    launch (method and launch shape from the autotuner).  Compared with the sum
-    of the per-network multigrid solve times of the same systems."""
+    real-resistor system; then all systems solved at 1e-8 (|r| <= 1e-8
+    min(|r0|, |b|), FP64-verified) by one graph-captured launch per solver:
+    learned-preconditioned CG in mixed precision and in FP64 (one CTA per
+    system, launch shape from the autotuner), plain Jacobi-CG the same way
+    (the baseline), and the chain-aggregation multigrid (one cluster per
+    system).  The multigrid is also compared with the sum of the per-network
+    multigrid solve times of the same systems."""
     import time as _t
 
     from cicy_geom_b200 import batch as BT
@@ -381,22 +420,40 @@ def batched_monte_carlo(count, device, reps=3):
     prep = _t.time() - t0
     if not systems:
         return {"realisations": count, **info, "systems": 0}
-    bs = BT.BatchSolver(systems, tol=TOL, device=device)
+    bs = BT.BatchSolver(systems, tol=TOL, device=device, learned=True)
+    ns = len(systems)
+
+    def measure(tune=False, runs=reps):
+        shape = bs.autotune() if tune else None
+        t = min(bs.solve() for _ in range(runs))
+        it, rel, fl = bs.results()
+        return {"seconds": t, "systems_per_s": ns / t, "launch": shape, "iterations_total": int(it.sum()), "iterations_max": int(it.max()),
+                "converged": int((fl == 1).sum()), "max_rel_residual": float(rel.max())}
+
+    out = {}
+    bs.set_solver("learned", 1)
+    out["learned_mixed"] = measure(tune=True)
+    bs.set_solver("learned", 0)
+    out["learned_fp64"] = measure(tune=True)
+    bs.set_solver("jacobi", 0)
+    bs.set_shape(1024, 2)
+    out["jacobi_fp64"] = measure(runs=1)  # the plain GPU Jacobi-CG baseline (~40 s)
     setup = bs.enable_multigrid()
-    tuned = bs.autotune()
-    times = [bs.solve() for _ in range(reps)]
-    it, rel, fl = bs.results()
+    bs.set_method(1)
+    out["multigrid"] = measure()
     bs.close()
-    t = min(times)
+    jac = out["jacobi_fp64"]["seconds"]
+    for k in ("learned_mixed", "learned_fp64", "multigrid"):
+        out[k]["speedup_vs_jacobi"] = jac / out[k]["seconds"]
     seq = sum(s["seconds_ref"] for s in systems)
     n = [s["A"].shape[0] for s in systems]
-    return {"realisations": count, **info, "systems": len(systems), "unknowns_total": int(sum(n)), "unknowns_max": int(max(n)),
-            "autotuned": tuned, "solve_seconds": t, "systems_per_s": len(systems) / t,
-            "sequential_solve_seconds": seq, "speedup_vs_sequential": seq / t, "multigrid_setup_seconds": setup,
-            "generation_and_assembly_seconds": prep, "converged": int((fl == 1).sum()), "max_rel_residual": float(rel.max()),
-            "max_iterations": int(it.max()),
+    return {"realisations": count, **info, "systems": ns, "unknowns_total": int(sum(n)), "unknowns_max": int(max(n)), **out,
+            "gnn_forward_seconds": bs.gnn_seconds, "multigrid_setup_seconds": setup,
+            "multigrid_sequential_solve_seconds": seq, "multigrid_speedup_vs_sequential": seq / out["multigrid"]["seconds"],
+            "generation_and_assembly_seconds": prep,
             "sample": "cube side U[2,5] um, CNT volume fraction U[0.5%,3%], seeds 3,000,000+k; solve stage only "
-                      "(generation, contacts, clusters, assembly and the unit-resistor pass run per network before it)"}
+                      "(generation, contacts, clusters, assembly and the unit-resistor pass run per network before it); "
+                      "learned/Jacobi: one CTA per system in one graph launch; multigrid: one 16-CTA cluster per system"}
 
 
 def run_ours(args):

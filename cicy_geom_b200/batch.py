@@ -69,32 +69,82 @@ def realisation_systems(configs, device: int = 0, preconditioner: int = 3):
     return systems, info
 
 
-class BatchSolver:
-    """The systems in device memory and one cicy_batch over them."""
+METHODS = ["cta_pcg", "cluster_multigrid", "sequential_grid"]
+PRECONDITIONERS = {"jacobi": 0, "learned": 1, "chain": 2}
 
-    def __init__(self, systems, tol: float = 1e-8, precision: int = 0, max_iter_factor: int = 300, device: int = 0):
+
+def edge_weights(tensors, params, device: int, stream) -> list:
+    """Learned coupling weights of each system (cicy_gnn_forward; one FP32 value per CSR entry)."""
+    import torch
+
+    L = _abi.lib()
+    dev = torch.device(f"cuda:{device}")
+    P = torch.tensor(np.asarray(params, np.float32), device=dev)
+    gnn = C.c_void_p()
+    _abi.check(L.cicy_gnn_create(C.byref(gnn), device), "cicy_gnn_create")
+    out = []
+    try:
+        for t in tensors:
+            n, nnz = t["rp"].numel() - 1, t["ci"].numel()
+            d = _abi.GnnSystem(n, nnz, t["rp"].data_ptr(), t["ci"].data_ptr(), t["v"].data_ptr(), t["cs"].numel(), t["cs"].data_ptr(),
+                               t["cl"].data_ptr())
+            w = torch.empty(nnz, dtype=torch.float32, device=dev)
+            _abi.check(L.cicy_gnn_set_system(gnn, C.byref(d), C.c_void_p(stream)), "cicy_gnn_set_system")
+            _abi.check(L.cicy_gnn_forward(gnn, C.c_void_p(P.data_ptr()), C.c_void_p(w.data_ptr()), C.c_void_p(stream)), "cicy_gnn_forward")
+            out.append(w)
+        torch.cuda.synchronize(dev)
+    finally:
+        L.cicy_gnn_destroy(gnn)
+    return out
+
+
+class BatchSolver:
+    """The systems in device memory and one cicy_batch over them.
+
+    learned: None, True (the shipped parameters) or a parameter vector; when
+    given, the graph network's coupling weights of every system are computed
+    once here so the learned preconditioner can be selected."""
+
+    def __init__(self, systems, tol: float = 1e-8, precision: int = 0, max_iter_factor: int = 300, device: int = 0, learned=None):
         import torch
 
         self.dev = torch.device(f"cuda:{device}")
         self._keep = []
         descs = (_abi.BatchSystem * len(systems))()
         self.x = []
-        for k, s in enumerate(systems):
+        tensors = []
+        for s in systems:
             A = s["A"]
-            t = {
+            tensors.append({
                 "rp": torch.tensor(A.indptr.astype(np.int32), device=self.dev),
                 "ci": torch.tensor(A.indices.astype(np.int32), device=self.dev),
                 "v": torch.tensor(A.data, dtype=torch.float64, device=self.dev),
-                "b": torch.tensor(s["b"], dtype=torch.float64, device=self.dev),
-                "x0": torch.tensor(s["x0"], dtype=torch.float64, device=self.dev),
-                "x": torch.zeros(A.shape[0], dtype=torch.float64, device=self.dev),
                 "cs": torch.tensor(np.asarray(s["chain_start"], np.int32), device=self.dev),
                 "cl": torch.tensor(np.asarray(s["chain_len"], np.int32), device=self.dev),
-            }
+            })
+        self.gnn_seconds = 0.0
+        if learned is not None:
+            import time
+
+            from .learned import default_params
+
+            params = default_params() if learned is True else learned
+            t0 = time.perf_counter()
+            ws = edge_weights(tensors, params, device, torch.cuda.current_stream(self.dev).cuda_stream)
+            self.gnn_seconds = time.perf_counter() - t0
+            for t, w in zip(tensors, ws):
+                t["ew"] = w
+        for k, s in enumerate(systems):
+            A = s["A"]
+            t = tensors[k]
+            t["b"] = torch.tensor(s["b"], dtype=torch.float64, device=self.dev)
+            t["x0"] = torch.tensor(s["x0"], dtype=torch.float64, device=self.dev)
+            t["x"] = torch.zeros(A.shape[0], dtype=torch.float64, device=self.dev)
             self._keep.append(t)
             self.x.append(t["x"])
             descs[k] = _abi.BatchSystem(A.shape[0], A.nnz, t["rp"].data_ptr(), t["ci"].data_ptr(), t["v"].data_ptr(), t["b"].data_ptr(),
-                                        t["x0"].data_ptr(), t["x"].data_ptr(), len(s["chain_start"]), t["cs"].data_ptr(), t["cl"].data_ptr())
+                                        t["x0"].data_ptr(), t["x"].data_ptr(), len(s["chain_start"]), t["cs"].data_ptr(), t["cl"].data_ptr(),
+                                        t["ew"].data_ptr() if "ew" in t else None)
         torch.cuda.synchronize(self.dev)
         self.count = len(systems)
         self.h = C.c_void_p()
@@ -107,13 +157,20 @@ class BatchSolver:
         _abi.check(_abi.lib().cicy_batch_enable_multigrid(self.h, C.byref(t)), "cicy_batch_enable_multigrid")
         return t.value
 
-    def set_method(self, method: int):
-        _abi.check(_abi.lib().cicy_batch_set_method(self.h, method), "cicy_batch_set_method")
+    def set_method(self, method):
+        """0 / "cta_pcg", 1 / "cluster_multigrid", 2 / "sequential_grid"."""
+        m = METHODS.index(method) if isinstance(method, str) else int(method)
+        _abi.check(_abi.lib().cicy_batch_set_method(self.h, m), "cicy_batch_set_method")
+
+    def set_solver(self, preconditioner, precision: int = 0):
+        """Preconditioner of methods 0 and 2 ("jacobi", "learned", "chain" or its CICY_PRECOND value); precision 0 FP64, 1 mixed."""
+        pk = PRECONDITIONERS[preconditioner] if isinstance(preconditioner, str) else int(preconditioner)
+        _abi.check(_abi.lib().cicy_batch_set_solver(self.h, pk, precision), "cicy_batch_set_solver")
 
     def autotune(self):
         m, t, c, s = C.c_int32(), C.c_int32(), C.c_int32(), C.c_double()
         _abi.check(_abi.lib().cicy_batch_autotune(self.h, C.byref(m), C.byref(t), C.byref(c), C.byref(s)), "cicy_batch_autotune")
-        return {"method": ["cta_chain_pcg", "cluster_multigrid"][m.value], "threads": t.value, "ctas_per_sm": c.value,
+        return {"method": METHODS[m.value], "threads": t.value, "ctas_per_sm": c.value,
                 "seconds": s.value}
 
     def set_shape(self, threads: int, ctas_per_sm: int):

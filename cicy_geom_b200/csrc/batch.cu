@@ -1,27 +1,39 @@
-// Batched Monte-Carlo solves: many independent DEA systems of uneven size
-// solved by one persistent kernel launch (captured in a CUDA graph and
-// replayed).  Each CTA takes the next system from a largest-first queue (an
-// atomic counter) and solves it alone with preconditioned CG:
+// Batched Monte-Carlo solves: many independent DEA systems of uneven size.
 //
-//   - preconditioner: whole-chain block-Jacobi (each CNT's free nodes form one
+// Method 0: one persistent kernel launch (captured in a CUDA graph and
+// replayed).  Each CTA takes the next system from a largest-first queue (an
+// atomic counter) and solves it alone with preconditioned CG; reductions are
+// CTA-local (__syncthreads only), so an iteration costs a few hundred
+// nanoseconds of synchronisation instead of the microseconds of a grid barrier.
+// Preconditioners:
+//   - Jacobi: z = r / diag (the upstream algorithm, Direct_Electrifying.cpp:1662-1676);
+//   - chain: whole-chain block-Jacobi (each CNT's free nodes form one
 //     tridiagonal block; LDL^T factored at the start of the system's solve by
 //     one thread per chain, forward/backward sweeps per chain each iteration;
-//     a singular chain falls back to its diagonal), in FP64 or FP32;
-//   - SpMV, dots and vector updates in FP64; reductions are CTA-local
-//     (__syncthreads only), so an iteration costs a few hundred nanoseconds of
-//     synchronisation instead of the microseconds of a grid barrier;
-//   - stop when |r| <= tol |r0| (Direct_Electrifying.cpp:1571, 1619), then the
-//     FP64 true residual b - A x replaces r and the test is repeated (at most
-//     kBatchRestarts times).
+//     a singular block falls back to its diagonal);
+//   - learned: T^-1 + T^-1 E_w T^-1 with T the chain blocks split every 32
+//     nodes (the blocks the weights were trained on; the split is an LDL^T
+//     multiplier of 0, so the same sweeps apply) and E_w the off-block
+//     couplings scaled by the graph network's weights.
+// Precision: FP64, or mixed: FP32 conductances in a difference-form SpMV,
+//   q_i = rs_i p_i + sum_j g_ij (p_i - p_j)   (rs_i = row sum of A, g_ij = -a_ij),
+// whose FP32 terms are edge currents (differences taken in FP64), so the
+// 1e4-1e10 spread between CNT and junction conductances does not cancel
+// catastrophically as in an FP32 A p; FP32 preconditioner factors; FP64 x, r,
+// p, dots, and FP64 residual replacement each time |r| has fallen 100x.
+// Stop when |r| <= tol min(|r0|, |b|): the test of Direct_Electrifying.cpp:1571,
+// 1619 and the FP64-verified |b - A x| <= tol |b|, confirmed on the true residual.
 //
-// Per-CTA scratch (r, p, q, z and the chain factors) lives in one device
-// buffer with a fixed offset per system.  The autotuner times the candidate
-// launch shapes (threads per CTA, CTAs per SM) on the batch itself and keeps
-// the fastest.
+// Method 2 solves the systems one after another with the per-network
+// grid-wide persistent PCG; method 1 (multigrid, one cluster per system) lives
+// in solver_mg.cu.  Per-system scratch lives in one device buffer with a fixed
+// offset per system.  The autotuner times the candidate launch shapes
+// (threads per CTA, CTAs per SM) on the batch itself and keeps the fastest.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <numeric>
+#include <type_traits>
 #include <vector>
 
 #include "cicy_internal.h"
@@ -31,7 +43,10 @@
 namespace cicy {
 namespace {
 
-constexpr int kBatchRestarts = 24;
+constexpr int kBatchRestarts = 24;       // FP64: true-residual restarts
+constexpr int kBatchReplacements = 400;  // mixed: FP64 residual replacements
+constexpr double kReplaceDrop = 1e-2;    // mixed: replace r once |r| fell by this factor since the last replacement
+constexpr int kSpaiBlock = kBlockMax;    // block length of the learned preconditioner's T
 
 struct BatchSys {
     int n, nnz, nchains;
@@ -43,8 +58,15 @@ struct BatchSys {
     double* x;
     const int32_t* cs;
     const int32_t* cl;
+    const float* ew;
     long long off;  // scratch offset (doubles)
 };
+
+// Scratch doubles of one system: r p q z y u (6n), factors (2n), FP32 g and row sums.
+inline long long batch_scratch(long long n, long long nnz) {
+    long long d = 8 * n + (nnz + n + 1) / 2 + 2;
+    return (d + 1) & ~1LL;  // 16-byte aligned offsets
+}
 
 struct BatchArgs {
     const BatchSys* sys;
@@ -105,45 +127,50 @@ __device__ __forceinline__ double upper(const BatchSys& S, int i) {
     return 0.0;
 }
 
-// LDL^T of every chain: lf[i] = l_i (multiplier), ip[i] = 1 / pivot_i; a singular
-// chain stores l = 0 and 1 / diag (its diagonal).
-template <typename PT>
+__device__ __forceinline__ double diag_of(const BatchSys& S, int i) {
+    for (int k = S.rp[i]; k < S.rp[i + 1]; k++)
+        if (S.ci[k] == i) return S.val[k];
+    return 0.0;
+}
+
+// LDL^T of every chain block (blocks of BLK nodes, BLK = 0: whole chains):
+// lf[i] = l_i (multiplier, 0 at a block start), ip[i] = 1 / pivot_i; a singular
+// block stores l = 0 and 1 / diag (its diagonal).
+template <typename PT, int BLK>
 __device__ void factor_chains(const BatchSys& S, PT* lf, PT* ip) {
     for (int c = threadIdx.x; c < S.nchains; c += blockDim.x) {
         const int s0 = S.cs[c], m = S.cl[c];
-        if (m <= 0) continue;
-        bool singular = false;
-        double piv_prev = 0, e_prev = 0;
-        for (int k = 0; k < m; k++) {
-            const int i = s0 + k;
-            double d = 0;
-            for (int kk = S.rp[i]; kk < S.rp[i + 1]; kk++)
-                if (S.ci[kk] == i) d = S.val[kk];
-            double l = 0, piv = d;
-            if (k > 0) {
-                l = e_prev / piv_prev;
-                piv = d - l * e_prev;
+        const int bl = BLK > 0 ? BLK : m;
+        for (int b0 = 0; b0 < m; b0 += bl) {
+            const int bm = min(bl, m - b0);
+            bool singular = false;
+            double piv_prev = 0, e_prev = 0;
+            for (int k = 0; k < bm; k++) {
+                const int i = s0 + b0 + k;
+                const double d = diag_of(S, i);
+                double l = 0, piv = d;
+                if (k > 0) {
+                    l = e_prev / piv_prev;
+                    piv = d - l * e_prev;
+                }
+                singular |= !(piv > 1e-13 * fabs(d));
+                lf[i] = (PT)l;
+                ip[i] = (PT)(1.0 / piv);
+                piv_prev = piv;
+                e_prev = (k + 1 < bm) ? upper(S, i) : 0.0;
             }
-            singular |= !(piv > 1e-13 * fabs(d));
-            lf[i] = (PT)l;
-            ip[i] = (PT)(1.0 / piv);
-            piv_prev = piv;
-            e_prev = (k + 1 < m) ? upper(S, i) : 0.0;
+            if (singular)
+                for (int k = 0; k < bm; k++) {
+                    const int i = s0 + b0 + k;
+                    lf[i] = (PT)0;
+                    ip[i] = (PT)(1.0 / diag_of(S, i));
+                }
         }
-        if (singular)
-            for (int k = 0; k < m; k++) {
-                const int i = s0 + k;
-                double d = 0;
-                for (int kk = S.rp[i]; kk < S.rp[i + 1]; kk++)
-                    if (S.ci[kk] == i) d = S.val[kk];
-                lf[i] = (PT)0;
-                ip[i] = (PT)(1.0 / d);
-            }
     }
 }
 
-// z = M^-1 r chain by chain: forward (y_k = r_k - l_k y_{k-1}), backward
-// (z_k = y_k / p_k - l_{k+1} z_{k+1}).  A singular chain has l = 0: z = r / d.
+// z = T^-1 r chain by chain: forward (y_k = r_k - l_k y_{k-1}), backward
+// (z_k = y_k / p_k - l_{k+1} z_{k+1}); l = 0 at block starts ends a block.
 template <typename PT>
 __device__ void apply_chains(const BatchSys& S, const PT* lf, const PT* ip, const double* r, double* z) {
     for (int c = threadIdx.x; c < S.nchains; c += blockDim.x) {
@@ -164,8 +191,24 @@ __device__ void apply_chains(const BatchSys& S, const PT* lf, const PT* ip, cons
     }
 }
 
-template <int T, typename PT>
+// FP64 residual r = b - A x, returns this thread's share of |r|^2.
+template <int T>
+__device__ __forceinline__ double true_residual(const BatchSys& S, double* r) {
+    double tl = 0;
+    for (int i = threadIdx.x; i < S.n; i += T) {
+        double s = 0;
+        for (int kk = S.rp[i]; kk < S.rp[i + 1]; kk++) s += S.val[kk] * S.x[S.ci[kk]];
+        const double ri = S.b[i] - s;
+        r[i] = ri;
+        tl += ri * ri;
+    }
+    return tl;
+}
+
+// PK: CICY_PRECOND_JACOBI (0), CICY_PRECOND_LEARNED (1), CICY_PRECOND_CHAIN (2).
+template <int T, int PK, bool MX>
 __global__ void __launch_bounds__(T) k_batch_pcg(BatchArgs a) {
+    using PT = typename std::conditional<MX, float, double>::type;
     __shared__ double sm[80];
     __shared__ int s_q;
     while (true) {
@@ -181,11 +224,30 @@ __global__ void __launch_bounds__(T) k_batch_pcg(BatchArgs a) {
         double* p = r + n;
         double* qv = p + n;
         double* z = qv + n;
-        PT* lf = reinterpret_cast<PT*>(z + n);
+        double* y = z + n;
+        double* u = y + n;
+        PT* lf = reinterpret_cast<PT*>(u + n);
         PT* ip = lf + n;
-        factor_chains<PT>(S, lf, ip);
+        float* g32 = reinterpret_cast<float*>(u + 3 * (long long)n);
+        float* rs32 = g32 + S.nnz;
+        // ---- setup: preconditioner factors, FP32 conductances and row sums
+        if (PK == 0) {
+            for (int i = threadIdx.x; i < n; i += T) ip[i] = (PT)(1.0 / diag_of(S, i));
+        } else {
+            factor_chains<PT, PK == 1 ? kSpaiBlock : 0>(S, lf, ip);
+        }
+        if (MX) {
+            for (int i = threadIdx.x; i < n; i += T) {
+                double rs = 0;
+                for (int k = S.rp[i]; k < S.rp[i + 1]; k++) {
+                    rs += S.val[k];
+                    g32[k] = S.ci[k] == i ? 0.0f : (float)(-S.val[k]);
+                }
+                rs32[i] = (float)rs;
+            }
+        }
         // r = b - A x0, x = x0
-        double rr_l = 0;
+        double rr_l = 0, bb_l = 0;
         for (int i = threadIdx.x; i < n; i += T) {
             double s = 0;
             for (int k = S.rp[i]; k < S.rp[i + 1]; k++) s += S.val[k] * S.x0[S.ci[k]];
@@ -193,32 +255,74 @@ __global__ void __launch_bounds__(T) k_batch_pcg(BatchArgs a) {
             r[i] = ri;
             S.x[i] = S.x0[i];
             rr_l += ri * ri;
+            bb_l += S.b[i] * S.b[i];
         }
-        double rr = cta_sum<T>(rr_l, sm);
-        const double R0 = a.tol * sqrt(rr);
+        double rr, bb;
+        cta_sum2<T>(rr_l, bb_l, sm, rr, bb);  // (its barriers also end the setup)
+        const double R0 = a.tol * sqrt(fmin(rr, bb));  // |r| <= tol |r0| and |b - A x| <= tol |b|
+        double anchor = sqrt(rr);
         const long long max_iter = a.iter_factor * (long long)n;
         long long k = 0;
         int restarts = 0, flag = 0;
         bool fresh = true;
         double rz = 0;
         while (true) {
-            apply_chains<PT>(S, lf, ip, r, z);
+            // ---- z = M^-1 r
+            if (PK == 0) {
+                for (int i = threadIdx.x; i < n; i += T) z[i] = (double)((PT)r[i] * ip[i]);
+            } else if (PK == 2) {
+                apply_chains<PT>(S, lf, ip, r, z);
+            } else {
+                apply_chains<PT>(S, lf, ip, r, y);
+                __syncthreads();
+                for (int i = threadIdx.x; i < n; i += T) {
+                    if (MX) {
+                        float s = 0;
+                        for (int kk = S.rp[i]; kk < S.rp[i + 1]; kk++) {
+                            const float w = S.ew[kk];
+                            if (w != 0.0f) s += w * g32[kk] * (float)y[S.ci[kk]];
+                        }
+                        u[i] = (double)s;
+                    } else {
+                        double s = 0;
+                        for (int kk = S.rp[i]; kk < S.rp[i + 1]; kk++) {
+                            const float w = S.ew[kk];
+                            if (w != 0.0f) s += (double)w * (-S.val[kk]) * y[S.ci[kk]];
+                        }
+                        u[i] = s;
+                    }
+                }
+                __syncthreads();
+                apply_chains<PT>(S, lf, ip, u, z);
+                __syncthreads();
+                for (int i = threadIdx.x; i < n; i += T) z[i] += y[i];
+            }
             __syncthreads();
             double rz_l = 0;
             for (int i = threadIdx.x; i < n; i += T) rz_l += r[i] * z[i];
             const double rz_new = cta_sum<T>(rz_l, sm);
             const double beta = fresh ? 0.0 : rz_new / rz;
             rz = rz_new;
-            double pq_l = 0;
             for (int i = threadIdx.x; i < n; i += T) p[i] = z[i] + beta * (fresh ? 0.0 : p[i]);
             __syncthreads();
+            // ---- q = A p
+            double pq_l = 0;
             for (int i = threadIdx.x; i < n; i += T) {
-                double s = 0;
-                for (int kk = S.rp[i]; kk < S.rp[i + 1]; kk++) s += S.val[kk] * p[S.ci[kk]];
+                double s;
+                if (MX) {
+                    const double pi = p[i];
+                    float f = rs32[i] * (float)pi;
+                    for (int kk = S.rp[i]; kk < S.rp[i + 1]; kk++) f += g32[kk] * (float)(pi - p[S.ci[kk]]);
+                    s = (double)f;
+                } else {
+                    s = 0;
+                    for (int kk = S.rp[i]; kk < S.rp[i + 1]; kk++) s += S.val[kk] * p[S.ci[kk]];
+                }
                 qv[i] = s;
                 pq_l += p[i] * s;
             }
             const double pq = cta_sum<T>(pq_l, sm);
+            if (!(pq > 0) || !(rz > 0)) break;  // breakdown (p.Ap <= 0 from rounding): stop with x intact, flag 0
             fresh = false;
             k++;
             const double alpha = rz / pq;
@@ -230,26 +334,25 @@ __global__ void __launch_bounds__(T) k_batch_pcg(BatchArgs a) {
                 rr_l += ri * ri;
             }
             rr = cta_sum<T>(rr_l, sm);
-            if (sqrt(rr) <= R0 || !(rr == rr)) {
-                if (!(rr == rr) || restarts >= kBatchRestarts) break;
-                // FP64 true residual
-                double tl = 0;
-                for (int i = threadIdx.x; i < n; i += T) {
-                    double s = 0;
-                    for (int kk = S.rp[i]; kk < S.rp[i + 1]; kk++) s += S.val[kk] * S.x[S.ci[kk]];
-                    const double ri = S.b[i] - s;
-                    r[i] = ri;
-                    tl += ri * ri;
-                }
-                rr = cta_sum<T>(tl, sm);
+            if (!(rr == rr)) break;
+            const double rn = sqrt(rr);
+            if (rn <= R0) {
+                if (restarts >= (MX ? kBatchReplacements : kBatchRestarts)) break;
+                rr = cta_sum<T>(true_residual<T>(S, r), sm);
                 restarts++;
                 if (sqrt(rr) <= R0) { flag = 1; break; }
-                fresh = true;
+                anchor = sqrt(rr);
+                fresh = !MX;  // FP64: restart; mixed: residual replacement, directions kept
+            } else if (MX && rn <= kReplaceDrop * anchor && restarts < kBatchReplacements) {
+                rr = cta_sum<T>(true_residual<T>(S, r), sm);
+                restarts++;
+                anchor = sqrt(rr);
             }
             if (k >= max_iter) { flag = 2; break; }
         }
         // FP64 relative residual |b - A x| / |b|
-        double bb_l = 0, tr_l = 0;
+        bb_l = 0;
+        double tr_l = 0;
         for (int i = threadIdx.x; i < n; i += T) {
             double s = 0;
             for (int kk = S.rp[i]; kk < S.rp[i + 1]; kk++) s += S.val[kk] * S.x[S.ci[kk]];
@@ -287,9 +390,21 @@ __global__ void __launch_bounds__(256) k_batch_residual(const BatchSys* __restri
     }
 }
 
-template <int T, typename PT>
-void launch(const BatchArgs& a, int grid, cudaStream_t s) {
-    k_batch_pcg<T, PT><<<grid, T, 0, s>>>(a);
+template <int T>
+void launch(const BatchArgs& a, int grid, int pk, bool mx, cudaStream_t s) {
+    if (pk == 0) mx ? k_batch_pcg<T, 0, true><<<grid, T, 0, s>>>(a) : k_batch_pcg<T, 0, false><<<grid, T, 0, s>>>(a);
+    else if (pk == 1) mx ? k_batch_pcg<T, 1, true><<<grid, T, 0, s>>>(a) : k_batch_pcg<T, 1, false><<<grid, T, 0, s>>>(a);
+    else mx ? k_batch_pcg<T, 2, true><<<grid, T, 0, s>>>(a) : k_batch_pcg<T, 2, false><<<grid, T, 0, s>>>(a);
+}
+
+__global__ void k_diag_extract(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const double* __restrict__ v,
+                               double* __restrict__ d) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double x = 0;
+        for (int k = rp[i]; k < rp[i + 1]; k++)
+            if (ci[k] == i) x = v[k];
+        d[i] = x;
+    }
 }
 
 }  // namespace
@@ -300,27 +415,33 @@ struct cicy_batch {
     int device = 0;
     int count = 0;
     int precision = 0;
+    int precond = CICY_PRECOND_CHAIN;  // methods 0 and 2
     double tol = 1e-8;
     long long iter_factor = 300;
     int threads = 512, ctas_per_sm = 2, sms = 148;
-    int method = 0;                 // 0: one CTA per system (chain block-Jacobi PCG), 1: one 16-CTA cluster per system (multigrid PCG)
+    int method = 0;  // 0: one CTA per system, 1: one 16-CTA cluster per system (multigrid), 2: one system at a time, grid-wide
+    bool have_weights = false;
     cicy::MgBatch* mg = nullptr;
     int64_t launches = 0;
     std::vector<cicy_batch_system> inputs;
     cicy::DBuf<cicy::BatchSys> sys;
-    cicy::DBuf<int> order, queue, flags;
-    cicy::DBuf<double> scratch, rel;
+    cicy::DBuf<int> order, queue, flags, status;
+    cicy::DBuf<double> scratch, rel, diag;
     cicy::DBuf<long long> iterations;
+    std::vector<long long> diag_off, seq_iterations;
+    cicy::SolverWork* sw = nullptr;  // method 2
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    int graph_threads = 0, graph_ctas = 0, graph_method = -1;
+    int graph_threads = 0, graph_ctas = 0, graph_method = -1, graph_precond = -1, graph_precision = -1;
     cudaStream_t stream = nullptr;
     ~cicy_batch() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         if (stream) cudaStreamDestroy(stream);
         if (mg) cicy::mg_batch_free(mg);
-        sys.release(); order.release(); queue.release(); flags.release(); scratch.release(); rel.release(); iterations.release();
+        delete sw;
+        sys.release(); order.release(); queue.release(); flags.release(); status.release(); scratch.release(); rel.release();
+        diag.release(); iterations.release();
     }
 };
 
@@ -358,18 +479,80 @@ void enqueue(cicy_batch* B, cudaStream_t s) {
     a.flags = B->flags.get();
     CICY_CUDA(cudaMemsetAsync(B->queue.get(), 0, sizeof(int), s));
     const int grid = std::max(1, std::min(B->count, B->sms * B->ctas_per_sm));
-    const bool f32 = B->precision == CICY_PRECISION_MIXED;
+    const bool mx = B->precision == CICY_PRECISION_MIXED;
     switch (B->threads) {
-        case 256: f32 ? cicy::launch<256, float>(a, grid, s) : cicy::launch<256, double>(a, grid, s); break;
-        case 512: f32 ? cicy::launch<512, float>(a, grid, s) : cicy::launch<512, double>(a, grid, s); break;
-        default: f32 ? cicy::launch<1024, float>(a, grid, s) : cicy::launch<1024, double>(a, grid, s); break;
+        case 256: cicy::launch<256>(a, grid, B->precond, mx, s); break;
+        case 512: cicy::launch<512>(a, grid, B->precond, mx, s); break;
+        default: cicy::launch<1024>(a, grid, B->precond, mx, s); break;
     }
     CICY_LAUNCH_CHECK();
 }
 
+// Method 2: every system through the per-network grid-wide persistent PCG, one
+// after another; returns the sum of the solves' kernel times.
+double solve_sequential(cicy_batch* B) {
+    cudaStream_t s = B->stream;
+    if (!B->sw) B->sw = new cicy::SolverWork;
+    if (B->diag_off.empty()) {
+        long long tot = 0;
+        B->diag_off.resize(B->count);
+        for (int i = 0; i < B->count; i++) {
+            B->diag_off[i] = tot;
+            tot += B->inputs[i].n;
+        }
+        B->diag.ensure((size_t)std::max(tot, 1LL));
+        for (int i = 0; i < B->count; i++) {
+            const cicy_batch_system& in = B->inputs[i];
+            cicy::k_diag_extract<<<std::min((in.n + 255) / 256, B->sms * 8), 256, 0, s>>>(in.n, in.row_ptr, in.col_ind, in.values,
+                                                                                     B->diag.get() + B->diag_off[i]);
+            CICY_LAUNCH_CHECK();
+        }
+        B->status.ensure(1);
+    }
+    const bool mx = B->precision == CICY_PRECISION_MIXED;
+    const int kind = B->precond == CICY_PRECOND_JACOBI ? cicy::PRECOND_KIND_JACOBI
+                     : B->precond == CICY_PRECOND_LEARNED ? cicy::PRECOND_KIND_SPAI
+                                                          : cicy::PRECOND_KIND_BLOCK;
+    CICY_CUDA(cudaMemsetAsync(B->status.get(), 0, sizeof(int), s));
+    B->seq_iterations.assign(B->count, 0);
+    std::vector<int> fl(B->count, 0);
+    double total = 0;
+    for (int i = 0; i < B->count; i++) {
+        const cicy_batch_system& in = B->inputs[i];
+        cicy::SolverSystem ss;
+        ss.n = in.n;
+        ss.nnz = in.nnz;
+        ss.rp = in.row_ptr;
+        ss.ci = in.col_ind;
+        ss.val = in.values;
+        ss.diag = B->diag.get() + B->diag_off[i];
+        ss.b = in.b;
+        ss.x = in.x;
+        CICY_CUDA(cudaMemcpyAsync(in.x, in.x0, sizeof(double) * in.n, cudaMemcpyDeviceToDevice, s));
+        if (kind != cicy::PRECOND_KIND_JACOBI)
+            cicy::build_block_preconditioner(*B->sw, ss, in.n_chains, in.chain_start, in.chain_len, nullptr, nullptr, mx, s, B->launches);
+        cicy::PcgStats st;
+        const long long max_iter = B->iter_factor * (long long)in.n;
+        cicy::pcg_solve(*B->sw, ss, kind, mx, B->tol, max_iter, B->sms, B->status.get(), s, B->launches, st, in.edge_weights);
+        total += st.seconds;
+        B->seq_iterations[i] = st.iterations;
+        fl[i] = st.iterations < max_iter ? 1 : 2;
+    }
+    int err = 0;
+    CICY_CUDA(cudaMemcpyAsync(&err, B->status.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    CICY_CUDA(cudaMemcpyAsync(B->flags.get(), fl.data(), sizeof(int) * B->count, cudaMemcpyHostToDevice, s));
+    cicy::k_batch_residual<<<std::min(B->count, B->sms * 4), 256, 0, s>>>(B->sys.get(), B->count, B->rel.get());
+    CICY_LAUNCH_CHECK();
+    CICY_CUDA(cudaStreamSynchronize(s));
+    if (err) throw cicy::Fail{CICY_E_TIMEOUT, "cicy_batch method 2: a grid barrier timed out"};
+    return total;
+}
+
 // (Re)build the graph of one batch solve for the current launch shape.
 void ensure_graph(cicy_batch* B) {
-    if (B->exec && B->graph_threads == B->threads && B->graph_ctas == B->ctas_per_sm && B->graph_method == B->method) return;
+    if (B->exec && B->graph_threads == B->threads && B->graph_ctas == B->ctas_per_sm && B->graph_method == B->method &&
+        B->graph_precond == B->precond && B->graph_precision == B->precision)
+        return;
     if (B->exec) cudaGraphExecDestroy(B->exec);
     if (B->graph) cudaGraphDestroy(B->graph);
     B->exec = nullptr;
@@ -388,9 +571,12 @@ void ensure_graph(cicy_batch* B) {
     B->graph_threads = B->threads;
     B->graph_ctas = B->ctas_per_sm;
     B->graph_method = B->method;
+    B->graph_precond = B->precond;
+    B->graph_precision = B->precision;
 }
 
 double timed_solve(cicy_batch* B) {
+    if (B->method == 2) return solve_sequential(B);
     ensure_graph(B);
     cudaEvent_t e0, e1;
     CICY_CUDA(cudaEventCreate(&e0));
@@ -417,6 +603,7 @@ cicy_status cicy_batch_create(cicy_batch** out, int device, const cicy_batch_sys
         return CICY_E_INPUT;
     }
     *out = nullptr;
+    bool weights = true;
     for (int i = 0; i < count; i++) {
         const cicy_batch_system& s = systems[i];
         if (s.n <= 0 || s.nnz <= 0 || !s.row_ptr || !s.col_ind || !s.values || !s.b || !s.x0 || !s.x || s.n_chains <= 0 ||
@@ -424,6 +611,7 @@ cicy_status cicy_batch_create(cicy_batch** out, int device, const cicy_batch_sys
             cicy::set_host_error("cicy_batch_create: system " + std::to_string(i) + " is incomplete");
             return CICY_E_INPUT;
         }
+        weights &= s.edge_weights != nullptr;
     }
     cicy_batch* B = new cicy_batch;
     cicy_status st = batch_guard(device, [&] {
@@ -435,13 +623,14 @@ cicy_status cicy_batch_create(cicy_batch** out, int device, const cicy_batch_sys
         B->iter_factor = max_iter_factor;
         CICY_CUDA(cudaDeviceGetAttribute(&B->sms, cudaDevAttrMultiProcessorCount, device));
         CICY_CUDA(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
+        B->have_weights = weights;
         std::vector<cicy::BatchSys> h(count);
         long long off = 0;
-        const int pt = precision == CICY_PRECISION_MIXED ? 1 : 2;  // factor storage in doubles per node
         for (int i = 0; i < count; i++) {
             const cicy_batch_system& s = systems[i];
-            h[i] = cicy::BatchSys{s.n, s.nnz, s.n_chains, s.row_ptr, s.col_ind, s.values, s.b, s.x0, s.x, s.chain_start, s.chain_len, off};
-            off += 4LL * s.n + pt * (long long)s.n + 2;
+            h[i] = cicy::BatchSys{s.n, s.nnz, s.n_chains, s.row_ptr, s.col_ind, s.values, s.b, s.x0, s.x, s.chain_start, s.chain_len,
+                                  s.edge_weights, off};
+            off += cicy::batch_scratch(s.n, s.nnz);
         }
         std::vector<int> ord(count);
         std::iota(ord.begin(), ord.end(), 0);
@@ -484,6 +673,21 @@ cicy_status cicy_batch_set_shape(cicy_batch* b, int32_t threads, int32_t ctas_pe
     return CICY_OK;
 }
 
+cicy_status cicy_batch_set_solver(cicy_batch* b, int32_t preconditioner, int32_t precision) {
+    if (!b || (preconditioner != CICY_PRECOND_JACOBI && preconditioner != CICY_PRECOND_LEARNED && preconditioner != CICY_PRECOND_CHAIN) ||
+        (precision != CICY_PRECISION_FP64 && precision != CICY_PRECISION_MIXED)) {
+        cicy::set_host_error("cicy_batch_set_solver: preconditioner Jacobi, learned or chain; precision FP64 or mixed");
+        return CICY_E_INPUT;
+    }
+    if (preconditioner == CICY_PRECOND_LEARNED && !b->have_weights) {
+        cicy::set_host_error("cicy_batch_set_solver: the learned preconditioner needs edge_weights in every system");
+        return CICY_E_INPUT;
+    }
+    b->precond = preconditioner;
+    b->precision = precision;
+    return CICY_OK;
+}
+
 cicy_status cicy_batch_enable_multigrid(cicy_batch* b, double* setup_seconds) {
     if (!b) return CICY_E_INPUT;
     return batch_guard(b->device, [&] {
@@ -500,8 +704,9 @@ cicy_status cicy_batch_enable_multigrid(cicy_batch* b, double* setup_seconds) {
 }
 
 cicy_status cicy_batch_set_method(cicy_batch* b, int32_t method) {
-    if (!b || method < 0 || method > 1 || (method == 1 && !b->mg)) {
-        cicy::set_host_error("cicy_batch_set_method: 0 (one CTA per system) or 1 (multigrid, after cicy_batch_enable_multigrid)");
+    if (!b || method < 0 || method > 2 || (method == 1 && !b->mg)) {
+        cicy::set_host_error("cicy_batch_set_method: 0 (one CTA per system), 1 (multigrid, after cicy_batch_enable_multigrid) or 2 "
+                             "(one system at a time, grid-wide)");
         return CICY_E_INPUT;
     }
     b->method = method;
@@ -519,8 +724,9 @@ cicy_status cicy_batch_autotune(cicy_batch* b, int32_t* method, int32_t* threads
             b->method = c[0];
             b->threads = c[1];
             b->ctas_per_sm = c[2];
-            timed_solve(b);  // warm (also builds the graph)
-            const double t = std::min(timed_solve(b), timed_solve(b));
+            const double t0 = timed_solve(b);  // warm (also builds the graph)
+            if (t0 > 1.5 * best) continue;      // clearly slower: not timed again
+            const double t = std::min(t0, timed_solve(b));
             if (t < best) {
                 best = t;
                 bm = c[0];
@@ -554,7 +760,9 @@ cicy_status cicy_batch_results(cicy_batch* b, int64_t* iterations, double* rel_r
         if (rel_residual) CICY_CUDA(cudaMemcpyAsync(rel_residual, b->rel.get(), sizeof(double) * b->count, cudaMemcpyDeviceToHost, b->stream));
         if (flags) CICY_CUDA(cudaMemcpyAsync(flags, b->flags.get(), sizeof(int) * b->count, cudaMemcpyDeviceToHost, b->stream));
         CICY_CUDA(cudaStreamSynchronize(b->stream));
-        if (b->method == 1) {
+        if (b->method == 2 && (int)b->seq_iterations.size() == b->count) {
+            for (int i = 0; i < b->count; i++) it[i] = b->seq_iterations[i];
+        } else if (b->method == 1) {
             std::vector<double> st;
             cicy::mg_batch_stats(b->mg, st, b->stream);
             for (int i = 0; i < b->count; i++) {

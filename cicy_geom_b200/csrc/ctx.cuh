@@ -119,7 +119,6 @@ struct Ctx {
     // CG scratch
     DBuf<int32_t> cg_rp, cg_ci;
     DBuf<double> cg_val, cg_minv, cg_x, cg_r, cg_p, cg_q, cg_z, cg_w, cg_s, cg_part;
-    DBuf<float> cg_val32, cg_minv32, cg_z32;
     DBuf<unsigned int> barrier;
     DBuf<double> cg_scal;
     DBuf<long long> cg_iters;

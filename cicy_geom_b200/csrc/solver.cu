@@ -24,9 +24,17 @@
 // per row (no sequential sweep on the iteration's critical path).  The learned
 // preconditioner is this block family with per-node and per-edge scalings.
 //
-// Mixed precision: the SpMV and the preconditioner apply read FP32 copies of
-// the matrix and of the block inverses and produce FP32 search vectors; x, r, the
-// dot products and the true-residual replacement stay FP64.
+// Mixed precision: q = A p is computed afresh each iteration (not carried as
+// A z + beta q, whose FP32 rounding would accumulate) in FP32 difference form,
+//   (A p)_i = rs_i p_i + sum_j g_ij (p_i - p_j)   (rs_i = row sum, g_ij = -a_ij),
+// whose terms are edge currents (the differences are taken in FP64, then
+// rounded), so the 1e4-1e10 spread between CNT and junction conductances does
+// not cancel catastrophically as in an FP32 A p.  The new p of a neighbour row
+// is rebuilt from z and the previous p (two p buffers), so this needs no extra
+// grid barrier.  The preconditioner apply uses FP32 copies of the block
+// inverses.  x, r, z, p, q, the dot products and the FP64 residual replacement
+// (every time the recursive residual fell by inner_drop; search directions
+// kept) stay FP64.
 #include <algorithm>
 #include <cmath>
 
@@ -229,26 +237,37 @@ __device__ __forceinline__ double apply_precond(const PcgArgs& a, int i) {
 template <int PRE, bool MIXED>
 __device__ __forceinline__ bool precond_all(const PcgArgs& a, int r_lo, int r_hi, double& rr_l, double& rz_l) {
     if constexpr (PRE == PRECOND_KIND_SPAI) {
-        for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
-            const int off = a.row_off[i], base = a.row_base[i], m = a.row_m[i];
-            double s = 0;
-            for (int j = 0; j < m; j++) s += a.tinv[off + j] * a.r[base + j];
-            a.y[i] = s;
-        }
+        for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) a.y[i] = apply_precond<PRECOND_KIND_BLOCK, MIXED>(a, i);
         if (!grid_sync(a.bar, gridDim.x, a.err)) return false;
         for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
-            double s = 0;
-            for (int k = a.rp[i]; k < a.rp[i + 1]; k++) {
-                const float w = a.ew[k];
-                if (w != 0.0f) s += (double)w * (-a.val[k]) * __ldcg(&a.y[a.ci[k]]);
+            if constexpr (MIXED) {
+                float s = 0;
+                for (int k = a.rp[i]; k < a.rp[i + 1]; k++) {
+                    const float w = a.ew[k];
+                    if (w != 0.0f) s += w * a.val32[k] * (float)__ldcg(&a.y[a.ci[k]]);
+                }
+                a.u[i] = (double)s;
+            } else {
+                double s = 0;
+                for (int k = a.rp[i]; k < a.rp[i + 1]; k++) {
+                    const float w = a.ew[k];
+                    if (w != 0.0f) s += (double)w * (-a.val[k]) * __ldcg(&a.y[a.ci[k]]);
+                }
+                a.u[i] = s;
             }
-            a.u[i] = s;
         }
         __syncthreads();
         for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
             const int off = a.row_off[i], base = a.row_base[i], m = a.row_m[i];
-            double s = a.y[i];
-            for (int j = 0; j < m; j++) s += a.tinv[off + j] * a.u[base + j];
+            double s;
+            if constexpr (MIXED) {
+                float f = 0;
+                for (int j = 0; j < m; j++) f += a.tinv32[off + j] * (float)a.u[base + j];
+                s = a.y[i] + (double)f;
+            } else {
+                s = a.y[i];
+                for (int j = 0; j < m; j++) s += a.tinv[off + j] * a.u[base + j];
+            }
             a.z[i] = s;
             const double ri = a.r[i];
             rr_l += ri * ri;
@@ -257,8 +276,8 @@ __device__ __forceinline__ bool precond_all(const PcgArgs& a, int r_lo, int r_hi
         return true;
     } else {
         for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
-            double zi = apply_precond<PRE, MIXED>(a, i);
-            if (MIXED) a.z32[i] = (float)zi; else a.z[i] = zi;
+            const double zi = apply_precond<PRE, MIXED>(a, i);
+            a.z[i] = zi;
             double ri = a.r[i];
             rr_l += ri * ri;
             rz_l += ri * zi;
@@ -269,11 +288,6 @@ __device__ __forceinline__ bool precond_all(const PcgArgs& a, int r_lo, int r_hi
 
 template <bool MIXED>
 __device__ __forceinline__ double spmv_row_z(const PcgArgs& a, int i) {
-    if (MIXED) {
-        float s = 0;
-        for (int k = a.rp[i]; k < a.rp[i + 1]; k++) s += a.val32[k] * a.z32[a.ci[k]];
-        return (double)s;
-    }
     double s = 0;
     for (int k = a.rp[i]; k < a.rp[i + 1]; k++) s += a.val[k] * a.z[a.ci[k]];
     return s;
@@ -294,32 +308,47 @@ __global__ void __launch_bounds__(kCgThreads) k_pcg(PcgArgs a) {
     double rr, rz;
     sum_partials(a.partA, 2, nb, sm, rr, rz);
     const double R0 = a.tol * sqrt(rr);
-    // mixed precision: FP32 inner iterations are restarted from the FP64 true residual
-    // each time the recursive residual has dropped by inner_drop (iterative refinement)
+    // mixed precision: the FP64 true residual replaces the recursive one each time
+    // the latter has dropped by inner_drop (the search directions are kept)
     double anchor = sqrt(rr);
     double beta = 0.0, rr_new = rr, pq = 0, dummy;
     long long k = 0;
     int restarts = 0;
     bool fresh = true;  // first step or restart: p = z, q = A z (old p, q are not read)
     while (true) {
-        // ---- A: w = A z, q = w + beta q, p = z + beta p, partial p.q
+        // ---- A: FP64: w = A z, q = w + beta q, p = z + beta p, partial p.q
+        //         mixed: p = z + beta p_old into the other p buffer, q = A p directly
+        //         (FP32 difference form; p_j of other rows rebuilt from z_j and
+        //         p_old_j), so FP32 rounding does not accumulate in q over iterations
+        double* pcur = a.p;
         double pq_l = 0;
-        for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
-            double w = spmv_row_z<MIXED>(a, i);
-            double zi = MIXED ? (double)a.z32[i] : a.z[i];
-            double qi, pi;
-            if (MIXED) {
-                qi = fresh ? w : (double)((float)w + (float)beta * a.q32[i]);
-                pi = fresh ? zi : (double)((float)zi + (float)beta * a.p32[i]);
-                a.q32[i] = (float)qi;
-                a.p32[i] = (float)pi;
-            } else {
-                qi = fresh ? w : w + beta * a.q[i];
-                pi = fresh ? zi : zi + beta * a.p[i];
+        if constexpr (MIXED) {
+            const double* po = (k & 1) ? a.p2 : a.p;
+            pcur = (k & 1) ? a.p : a.p2;
+            const double bt = fresh ? 0.0 : beta;
+            for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
+                const double pi = fresh ? a.z[i] : a.z[i] + bt * po[i];
+                float f = a.rs32[i] * (float)pi;
+                for (int kk = a.rp[i]; kk < a.rp[i + 1]; kk++) {
+                    const int j = a.ci[kk];
+                    const double pj = fresh ? a.z[j] : a.z[j] + bt * po[j];
+                    f += a.val32[kk] * (float)(pi - pj);
+                }
+                const double qi = (double)f;
+                pcur[i] = pi;
+                a.q[i] = qi;
+                pq_l += pi * qi;
+            }
+        } else {
+            for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
+                const double w = spmv_row_z<false>(a, i);
+                const double zi = a.z[i];
+                const double qi = fresh ? w : w + beta * a.q[i];
+                const double pi = fresh ? zi : zi + beta * a.p[i];
                 a.q[i] = qi;
                 a.p[i] = pi;
+                pq_l += pi * qi;
             }
-            pq_l += pi * qi;
         }
         block_reduce2(pq_l, 0.0, sm, s0, s1);
         if (threadIdx.x == 0) a.partB[blockIdx.x] = s0;
@@ -328,10 +357,11 @@ __global__ void __launch_bounds__(kCgThreads) k_pcg(PcgArgs a) {
         fresh = false;
         k++;
         // ---- B: x += alpha p, r -= alpha q, z = M r, partials r.r, r.z
+        if (!(pq > 0) || !(rz > 0)) break;  // breakdown (p.Ap <= 0 from rounding): stop with x intact
         const double alpha = rz / pq;
         for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
-            double pi = MIXED ? (double)a.p32[i] : a.p[i];
-            double qi = MIXED ? (double)a.q32[i] : a.q[i];
+            const double pi = pcur[i];
+            const double qi = a.q[i];
             a.x[i] += alpha * pi;
             a.r[i] -= alpha * qi;
         }
@@ -344,6 +374,7 @@ __global__ void __launch_bounds__(kCgThreads) k_pcg(PcgArgs a) {
         if (!grid_sync(a.bar, nb, a.err)) return;
         double rz_new;
         sum_partials(a.partA, 2, nb, sm, rr_new, rz_new);
+        const double rz_prev = rz;
         beta = rz_new / rz;
         rz = rz_new;
         if (sqrt(rr_new) <= R0 || (MIXED && sqrt(rr_new) <= a.inner_drop * anchor)) {
@@ -366,7 +397,8 @@ __global__ void __launch_bounds__(kCgThreads) k_pcg(PcgArgs a) {
             restarts++;
             anchor = sqrt(rr_new);
             if (sqrt(rr_new) <= R0) break;
-            fresh = true;  // restart from the true residual
+            if (MIXED) beta = rz / rz_prev;  // residual replacement: continue the directions
+            else fresh = true;               // restart from the true residual
         }
         if (k >= a.max_iter) break;
     }
@@ -391,8 +423,17 @@ int max_coop_blocks(int sms) {
     return std::max(1, occ) * sms;
 }
 
-__global__ void k_f32(int n, const double* __restrict__ a, float* __restrict__ b) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = (float)a[i];
+// FP32 conductances (g = -a off the diagonal, 0 on it) and FP32 row sums (FP64 sums).
+__global__ void k_mixed_prep(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const double* __restrict__ v,
+                             float* __restrict__ g, float* __restrict__ rs) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double s = 0;
+        for (int k = rp[i]; k < rp[i + 1]; k++) {
+            s += v[k];
+            g[k] = ci[k] == i ? 0.0f : (float)(-v[k]);
+        }
+        rs[i] = (float)s;
+    }
 }
 
 }  // namespace
@@ -436,15 +477,15 @@ void build_block_preconditioner(SolverWork& w, const SolverSystem& sys, int ncha
 
 void pcg_solve(SolverWork& w, const SolverSystem& sys, int precond, bool mixed, double tol, long long max_iter, int num_sms,
                int* status, cudaStream_t s, int64_t& launches, PcgStats& st, const float* ew) {
-    if (precond == PRECOND_KIND_SPAI && (mixed || !ew)) throw Fail{CICY_E_INTERNAL, "SPAI preconditioner: FP64 only, weights required"};
+    if (precond == PRECOND_KIND_SPAI && !ew) throw Fail{CICY_E_INTERNAL, "SPAI preconditioner: weights required"};
     const int n = sys.n;
     st = PcgStats{};
     if (n <= 0) return;
     // vectors
     w.r.ensure(n); w.z.ensure(n); w.p.ensure(n); w.q.ensure(n);
     if (mixed) {
-        w.z32.ensure(n); w.p32.ensure(n); w.q32.ensure(n); w.val32.ensure(std::max(sys.nnz, 1));
-        k_f32<<<grid_for(sys.nnz), 256, 0, s>>>(sys.nnz, sys.val, w.val32.get());
+        w.val32.ensure(std::max(sys.nnz, 1)); w.rs32.ensure(n); w.p2.ensure(n);
+        k_mixed_prep<<<grid_for(n), 256, 0, s>>>(n, sys.rp, sys.ci, sys.val, w.val32.get(), w.rs32.get());
         launches++;
     }
     // r = b - A x0
@@ -463,7 +504,7 @@ void pcg_solve(SolverWork& w, const SolverSystem& sys, int precond, bool mixed, 
     // CTA row ranges
     int cap = 0;
     if (precond == PRECOND_KIND_JACOBI) cap = mixed ? max_coop_blocks<PRECOND_KIND_JACOBI, true>(num_sms) : max_coop_blocks<PRECOND_KIND_JACOBI, false>(num_sms);
-    else if (precond == PRECOND_KIND_SPAI) cap = max_coop_blocks<PRECOND_KIND_SPAI, false>(num_sms);
+    else if (precond == PRECOND_KIND_SPAI) cap = mixed ? max_coop_blocks<PRECOND_KIND_SPAI, true>(num_sms) : max_coop_blocks<PRECOND_KIND_SPAI, false>(num_sms);
     else cap = mixed ? max_coop_blocks<PRECOND_KIND_BLOCK, true>(num_sms) : max_coop_blocks<PRECOND_KIND_BLOCK, false>(num_sms);
     const int nb = std::max(1, std::min({cap, num_sms, ceil_div(n, kCgThreads)}));
     w.cta_row.ensure(nb + 1);
@@ -476,10 +517,9 @@ void pcg_solve(SolverWork& w, const SolverSystem& sys, int precond, bool mixed, 
     launches++;
     PcgArgs a{};
     a.n = n;
-    a.rp = sys.rp; a.ci = sys.ci; a.val = sys.val; a.val32 = mixed ? w.val32.get() : nullptr;
+    a.rp = sys.rp; a.ci = sys.ci; a.val = sys.val; a.val32 = mixed ? w.val32.get() : nullptr; a.rs32 = mixed ? w.rs32.get() : nullptr;
     a.b = sys.b; a.x = sys.x; a.r = w.r.get();
-    a.z = w.z.get(); a.p = w.p.get(); a.q = w.q.get();
-    a.z32 = mixed ? w.z32.get() : nullptr; a.p32 = mixed ? w.p32.get() : nullptr; a.q32 = mixed ? w.q32.get() : nullptr;
+    a.z = w.z.get(); a.p = w.p.get(); a.q = w.q.get(); a.p2 = mixed ? w.p2.get() : nullptr;
     a.minv = w.minv.get(); a.minv32 = w.minv32.get();
     a.tinv = w.tinv.get(); a.tinv32 = w.tinv32.get();
     a.row_off = w.row_off.get(); a.row_base = w.row_base.get(); a.row_m = w.row_m.get();
@@ -498,7 +538,7 @@ void pcg_solve(SolverWork& w, const SolverSystem& sys, int precond, bool mixed, 
     a.tol = tol;
     a.max_iter = max_iter;
     a.max_restarts = mixed ? kMaxRestartsMixed : kMaxRestarts;
-    a.inner_drop = 1e-3;
+    a.inner_drop = 1e-2;
     cudaEvent_t e0, e1;
     CICY_CUDA(cudaEventCreate(&e0));
     CICY_CUDA(cudaEventCreate(&e1));
@@ -506,7 +546,7 @@ void pcg_solve(SolverWork& w, const SolverSystem& sys, int precond, bool mixed, 
     if (precond == PRECOND_KIND_JACOBI) {
         if (mixed) launch_pcg<PRECOND_KIND_JACOBI, true>(a, nb, s); else launch_pcg<PRECOND_KIND_JACOBI, false>(a, nb, s);
     } else if (precond == PRECOND_KIND_SPAI) {
-        launch_pcg<PRECOND_KIND_SPAI, false>(a, nb, s);
+        if (mixed) launch_pcg<PRECOND_KIND_SPAI, true>(a, nb, s); else launch_pcg<PRECOND_KIND_SPAI, false>(a, nb, s);
     } else {
         if (mixed) launch_pcg<PRECOND_KIND_BLOCK, true>(a, nb, s); else launch_pcg<PRECOND_KIND_BLOCK, false>(a, nb, s);
     }

@@ -30,12 +30,13 @@ struct PcgArgs {
     const int32_t* rp;
     const int32_t* ci;
     const double* val;
-    const float* val32;
+    const float* val32;   // mixed: conductances g = -a off the diagonal, 0 on it
+    const float* rs32;    // mixed: row sums of A (the conductance to prescribed nodes)
     const double* b;
     double* x;
     double* r;
     double *z, *p, *q;
-    float *z32, *p32, *q32;
+    double* p2;           // mixed: second buffer of the search direction
     const double* minv;
     const float* minv32;
     const double* tinv;
@@ -113,8 +114,8 @@ struct MgWork {
 };
 
 struct SolverWork {
-    DBuf<double> r, z, p, q, minv, tinv, part, stats, lfac, ipiv;
-    DBuf<float> z32, p32, q32, val32, minv32, tinv32;
+    DBuf<double> r, z, p, p2, q, minv, tinv, part, stats, lfac, ipiv;
+    DBuf<float> val32, rs32, minv32, tinv32;
     DBuf<int32_t> is_start, start_scan, blk_row, blk_msq, blk_off, row_off, row_base, row_m, cta_row, total, scan_tmp, cta_stats;
     DBuf<int32_t> halo_mark, halo_scan, halo_ptr, send_cnt, send_ptr;
     DBuf<unsigned long long> send;

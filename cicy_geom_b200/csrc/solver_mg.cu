@@ -243,6 +243,7 @@ struct MgArgs {
     double tol;
     long long max_iter;
     int max_restarts;
+    int cap_b;  // stop at |r| <= tol min(|r0|, |b|) (batched solves); else |r| <= tol |r0| (Direct_Electrifying.cpp:1571, 1619)
 };
 
 // Grid barrier on a monotonic counter: one release-add per CTA, then an acquire
@@ -420,7 +421,16 @@ __device__ void mg_pcg_body(const MgArgs& a, int cta, int nctas) {
         }
     }
     unsigned long long target = 0;
-    double R0 = 0, rr = 0, rz = 0, beta = 0;
+    double R0 = 0, rr = 0, rz = 0, beta = 0, bnorm = 0;
+    if (a.cap_b) {  // |b| (partB is next written after the first barrier of the loop)
+        double bb_l = 0;
+        for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) bb_l += a.b[i] * a.b[i];
+        double s0;
+        mg_reduce1(bb_l, sm, s0);
+        if (threadIdx.x == 0) a.partB[cta] = s0;
+        if (!sync_all<CL>(a.bar, target, a.err, &s_ok)) return;
+        bnorm = sqrt(mg_sum_partials(a.partB, nb, sm));
+    }
     long long k = 0;
     int restarts = 0;
     bool fresh = true;      // p = z, q = A z on the next direction update
@@ -439,7 +449,7 @@ __device__ void mg_pcg_body(const MgArgs& a, int cta, int nctas) {
         if (threadIdx.x == 0) a.partA[cta] = s0;
         if (!sync_all<CL>(a.bar, target, a.err, &s_ok)) return;
         rr = mg_sum_partials(a.partA, nb, sm);
-        if (k == 0 && !recursive && restarts == 0) R0 = a.tol * sqrt(rr);
+        if (k == 0 && !recursive && restarts == 0) R0 = a.tol * (a.cap_b ? fmin(sqrt(rr), bnorm) : sqrt(rr));
         if (k > 0 && sqrt(rr) <= R0) {
             if (!recursive || restarts >= a.max_restarts) break;
             // the recursive residual met the test: replace it by the FP64 true residual
@@ -1145,6 +1155,7 @@ MgBatch* mg_batch_build(const std::vector<MgBatchInput>& in, double tol, long lo
             a.tol = tol;
             a.max_iter = iter_factor * (long long)x.n;
             a.max_restarts = kMgMaxRestarts;
+            a.cap_b = 1;
             host[k] = a;
         }
         B->args.ensure(in.size());

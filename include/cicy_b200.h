@@ -258,16 +258,24 @@ cicy_status cicy_spmv_csr(int32_t n, const int32_t* row_ptr, const int32_t* col_
 
 /* ---------------- batched Monte-Carlo solves (no upstream counterpart) ----------------
  * Many independent DEA systems (e.g. the real-resistor systems of hundreds of
- * seeded realisations) solved by one persistent kernel launch, replayed from a
- * CUDA graph: each CTA takes the next system of a largest-first queue and runs
- * preconditioned CG on it alone (whole-chain block-Jacobi; FP64, or FP32
- * preconditioner apply with CICY_PRECISION_MIXED; FP64 SpMV, dots and true
- * residual), stopping at |r| <= tol |r0| confirmed on the FP64 true residual
- * (the test of Direct_Electrifying.cpp:1571, 1619).  All pointers are device
- * memory the caller keeps alive; the chains must partition the rows. */
+ * seeded realisations) solved together.  Methods 0 and 1 stop at
+ * |r| <= tol min(|r0|, |b|) confirmed on the FP64 true residual (the test of
+ * Direct_Electrifying.cpp:1571, 1619, and |b - A x| <= tol |b|); method 2 is
+ * the per-network solver and uses the upstream test |r| <= tol |r0|.
+ * Methods:
+ *   0  one persistent kernel launch replayed from a CUDA graph; each CTA takes
+ *      the next system of a largest-first queue and runs preconditioned CG on
+ *      it alone, with the preconditioner and precision of cicy_batch_set_solver;
+ *   1  one 16-CTA cluster per system running the chain-aggregation multigrid
+ *      PCG (after cicy_batch_enable_multigrid; FP64);
+ *   2  one system after another through the per-network grid-wide persistent
+ *      PCG (the path cicy_electrical_analysis uses), same preconditioner and
+ *      precision as method 0; seconds = the sum of its kernels' device times.
+ * All pointers are device memory the caller keeps alive; the chains must
+ * partition the rows. */
 typedef struct {
     int32_t n, nnz;
-    const int32_t* row_ptr;    /* full symmetric CSR, diagonal included */
+    const int32_t* row_ptr;    /* full symmetric CSR, diagonal included, ascending columns */
     const int32_t* col_ind;
     const double* values;
     const double* b;
@@ -276,24 +284,36 @@ typedef struct {
     int32_t n_chains;
     const int32_t* chain_start;
     const int32_t* chain_len;
+    const float* edge_weights; /* CICY_PRECOND_LEARNED: weight of every CSR entry, 0 on the chain blocks
+                                  and the diagonal (cicy_gnn_forward's output); NULL otherwise */
 } cicy_batch_system;
 typedef struct cicy_batch cicy_batch;
 cicy_status cicy_batch_create(cicy_batch** out, int device, const cicy_batch_system* systems, int32_t count, double tol,
                               int32_t max_iter_factor, int32_t precision);
 cicy_status cicy_batch_destroy(cicy_batch* b);
-/* Launch shape: threads per CTA (256, 512, 1024) and CTAs per SM. */
+/* Launch shape of method 0: threads per CTA (256, 512, 1024) and CTAs per SM. */
 cicy_status cicy_batch_set_shape(cicy_batch* b, int32_t threads, int32_t ctas_per_sm);
+/* Preconditioner of methods 0 and 2: CICY_PRECOND_JACOBI (plain Jacobi-PCG, the
+ * upstream algorithm), CICY_PRECOND_CHAIN (whole-chain block-Jacobi; method 2
+ * splits chains into blocks of at most 32 nodes), CICY_PRECOND_LEARNED (chain
+ * blocks of at most 32 nodes plus the learned sparse approximate inverse,
+ * needs every system's edge_weights).  Precision: CICY_PRECISION_FP64, or
+ * CICY_PRECISION_MIXED (FP32 conductances in a difference-form SpMV and FP32
+ * preconditioner factors; FP64 vectors, dots and residual replacement).
+ * Default: CICY_PRECOND_CHAIN and the precision given to create. */
+cicy_status cicy_batch_set_solver(cicy_batch* b, int32_t preconditioner, int32_t precision);
 /* Builds a multigrid hierarchy per system (setup time returned) so the batch can
- * also run as one 16-CTA cluster per system with the chain-aggregation multigrid PCG. */
+ * also run method 1. */
 cicy_status cicy_batch_enable_multigrid(cicy_batch* b, double* setup_seconds);
-/* 0: one CTA per system (chain block-Jacobi PCG); 1: one 16-CTA cluster per system (multigrid PCG). */
+/* 0, 1 or 2 (above). */
 cicy_status cicy_batch_set_method(cicy_batch* b, int32_t method);
-/* Times the candidate methods and launch shapes on this batch and keeps the fastest
- * (for the multigrid method ctas_per_sm returns the number of concurrent clusters). */
+/* Times method 0's launch shapes (with the current preconditioner and
+ * precision) and, when multigrid is enabled, method 1, on this batch, and keeps
+ * the fastest (for method 1 ctas_per_sm returns the number of concurrent clusters). */
 cicy_status cicy_batch_autotune(cicy_batch* b, int32_t* method, int32_t* threads, int32_t* ctas_per_sm, double* seconds);
-/* One batched solve (graph launch); seconds = its device time (CUDA events). */
+/* One solve of every system by the current method; seconds = its device time (CUDA events). */
 cicy_status cicy_batch_solve(cicy_batch* b, double* seconds);
-/* Per system: iterations, FP64 |b - A x| / |b|, flag (1 converged, 2 iteration cap, 0 breakdown). */
+/* Per system: iterations, FP64 |b - A x| / |b|, flag (1 converged, 2 iteration cap, 0 breakdown or restart limit). */
 cicy_status cicy_batch_results(cicy_batch* b, int64_t* iterations, double* rel_residual, int32_t* flags);
 
 /* ---------------- host-side network sources (CPU, upstream of the hot path) ---------------- */

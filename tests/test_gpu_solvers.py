@@ -47,6 +47,46 @@ def test_voltages_match_fp64_direct_solve(cuda_ok, name, pre):
     np.testing.assert_allclose(np.array(r.resistances), ref["resistances"], rtol=1e-9)
 
 
+def direct_errors(ctx, r):
+    out = []
+    for i in range(r.n_solves):
+        S = ctx.system(i)
+        if len(S["diag"]) == 0:
+            continue
+        vd = O.solve_direct({**S, "vef": S["voltages"][: S["reserved"]]})
+        m = np.concatenate([np.ones(S["reserved"], bool), O.grounded_mask(S)])
+        out.append(np.max(np.abs(S["voltages"][m] - vd[m])) / np.max(np.abs(vd[m])))
+    return np.array(out)
+
+
+@pytest.mark.parametrize("pre", [0, 2, 1])  # Jacobi, chain blocks, learned
+@pytest.mark.parametrize("name", ["c1p_1200_s1", "c1p_800_s2"])
+def test_mixed_precision_against_fp64(cuda_ok, name, pre):
+    """FP32 difference-form SpMV and preconditioner apply with FP64 residual
+    replacement, at 1e-10 on the FP64 true residual.  The FP64 solve at that
+    tolerance is within ~1e-8 of the direct solve's voltages; mixed precision's
+    FP32 SpMV noise lands partly in small-eigenvalue directions, so at the same
+    residual its voltages are within ~1e-5 (bound 1e-4) and its effective
+    resistance within 1e-6."""
+    cfg, net, z = golden_network(name)
+    cfg.tolerance = 1e-10
+    cfg.tolerance_unit = 1e-10
+    err = {}
+    for prec in (0, 1):
+        ctx = Context(0)
+        ctx.set_solver(precision=prec, preconditioner=pre)
+        ctx.upload(net)
+        r = ctx.network_to_conductance(cfg.params())
+        for i in range(r.n_solves):
+            assert r.solves[i].fallback == 0
+            if prec:
+                assert r.solves[i].kernel == 0
+        err[prec] = direct_errors(ctx, r)
+        ref = O.network_to_conductance(net.arrays(), O.params_from_config(cfg), solver="direct")
+        np.testing.assert_allclose(np.array(r.resistances), ref["resistances"], rtol=1e-6 if prec else 1e-7)
+    assert np.all(err[0] <= 5e-7) and np.all(err[1] <= 1e-4), err
+
+
 @pytest.fixture(scope="module")
 def medium(cuda_ok):
     from cicy_geom_b200.network import NetworkConfig, generate_cnt_network
