@@ -357,7 +357,9 @@ __global__ void __launch_bounds__(kCgThreads) k_pcg(PcgArgs a) {
         fresh = false;
         k++;
         // ---- B: x += alpha p, r -= alpha q, z = M r, partials r.r, r.z
-        if (!(pq > 0) || !(rz > 0)) break;  // breakdown (p.Ap <= 0 from rounding): stop with x intact
+        // mixed: breakdown (p.Ap <= 0 from FP32 rounding) stops with x intact; FP64
+        // keeps the upstream arithmetic (a zero initial residual gives 0/0 = NaN there)
+        if (MIXED && (!(pq > 0) || !(rz > 0))) break;
         const double alpha = rz / pq;
         for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
             const double pi = pcur[i];
