@@ -202,3 +202,45 @@ class BatchSolver:
             self.close()
         except Exception:
             pass
+
+
+def main(argv=None):
+    """Seeded Monte-Carlo realisations solved by one batched call; prints one JSON line.
+
+    python -m cicy_geom_b200.batch --count 32 --precond learned --precision 1"""
+    import argparse
+    import json
+    import time
+
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--count", type=int, default=32)
+    ap.add_argument("--seed0", type=int, default=3_000_000)
+    ap.add_argument("--precond", default="learned", choices=list(PRECONDITIONERS) + ["multigrid"])
+    ap.add_argument("--precision", type=int, default=1)
+    ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--threads", type=int, default=1024)
+    ap.add_argument("--ctas-per-sm", type=int, default=2)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--device", type=int, default=0)
+    a = ap.parse_args(argv)
+    t0 = time.time()
+    systems, info = realisation_systems(monte_carlo_configs(a.count, seed0=a.seed0), device=a.device)
+    prep = time.time() - t0
+    bs = BatchSolver(systems, tol=a.tol, device=a.device, learned=True if a.precond == "learned" else None)
+    if a.precond == "multigrid":
+        bs.enable_multigrid()
+        bs.set_method(1)
+    else:
+        bs.set_solver(a.precond, a.precision)
+        bs.set_shape(a.threads, a.ctas_per_sm)
+    times = [bs.solve() for _ in range(a.reps)]
+    it, rel, fl = bs.results()
+    bs.close()
+    print(json.dumps({**info, "systems": len(systems), "unknowns_total": int(sum(s["A"].shape[0] for s in systems)),
+                      "precond": a.precond, "precision": a.precision, "seconds": min(times), "iterations_total": int(it.sum()),
+                      "iterations_max": int(it.max()), "converged": int((fl == 1).sum()), "max_rel_residual": float(rel.max()),
+                      "prep_seconds": prep}))
+
+
+if __name__ == "__main__":
+    main()
