@@ -359,6 +359,29 @@ def solver_comparison(cfg, net, device, steps=2):
     return out
 
 
+def contact_search_roofline(ctx, net, res, stage_acc, steps, hbm):
+    """Contact grid + tunnelling contacts + HK labels of the timed steps (device
+    events of the two stages, cicy_result.stage_seconds) against the algorithmic
+    bytes B_contact = N_p (24 xyz + 4 CNT id) + N_s (4 write + 4 read) + 4 (R + 1)
+    + 16 N_k and B_label = 8 N_k + 8 N_c per network."""
+    import ctypes as C
+
+    from cicy_geom_b200._abi import lib
+
+    nr, ns = C.c_int64(), C.c_int64()
+    lib().cicy_get_sectioned_domain(ctx.handle, C.byref(nr), C.byref(ns), None, None)
+    a = net.arrays()
+    n_p, n_c = len(a["x"]), len(a["radii"])
+    n_k = int(res.n_point_contacts)
+    b = n_p * 28 + ns.value * 8 + 4 * (nr.value + 1) + 16 * n_k + 8 * n_k + 8 * n_c
+    t = (stage_acc[0] + stage_acc[1]) / steps
+    return {"stages": "cicy_contact_grid + cicy_clusters", "seconds_per_network": t, "points_per_s": n_p / t,
+            "bound": "hbm", "algorithmic_bytes": b, "achieved": b / t / 1e9, "peak": hbm, "unit": "GB/s", "frac": b / t / 1e9 / hbm,
+            "points": n_p, "slots": ns.value, "regions": nr.value, "point_contacts": n_k,
+            "note": "stage time includes the host reads of the sizes (scan totals) between kernels; the largest kernel is "
+                    "k_pairs (one warp per region), see profiles/"}
+
+
 def spmv_roofline(ctx, device, hbm, target_bytes=320e6, reps=20):
     """cicy_spmv_csr on copies of the unit-pass system laid out block-diagonally
     until the matrix is larger than L2 (126 MB); algorithmic bytes
@@ -490,6 +513,7 @@ def run_ours(args):
         torch.cuda.synchronize()
 
     per_kernel = {}  # kernel kind -> [device seconds, launches, algorithmic bytes]
+    stage_acc = [0.0] * 6  # grid, clusters, unit DEA, backbone, real DEA, total (device events per step)
     cg_time, iters, resid = 0.0, [], []
     launches0 = ctx.kernel_launches()
     with ClockSampler(local) as clk:
@@ -500,6 +524,8 @@ def run_ours(args):
             with torch.cuda.stream(stream):
                 flush.zero_()
             step()
+            for j in range(6):
+                stage_acc[j] += res.stage_seconds[j]
             for s in res.solves[: res.n_solves]:
                 cg_time += s.seconds
                 acc = per_kernel.setdefault(int(s.kernel), [0.0, 0, 0])
@@ -561,6 +587,7 @@ def run_ours(args):
                          "note": "algorithmic bytes = iterations x (SpMV + 12 vector passes) of the solves this kernel ran; "
                                  "the systems live in shared memory / L2, so the kernel is latency-bound (one cluster or "
                                  "grid barrier per reduction); peak is the measured HBM copy bandwidth (of measured)"},
+            "contact_search": contact_search_roofline(ctx, net, res, stage_acc, args.steps, hbm),
             "e2e": {"value": world * args.steps / t_e2e, "unit": "networks/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 24},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
