@@ -38,6 +38,7 @@ SIDE, N_CNTS, TOL, TOL_UNIT = 6.0, 25000, 1e-8, 1e-10
 METRIC = "networks solved/s at 1e-8 residual (25k-CNT 6um network, full hot path)"
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "ref_dump")
 PRECONDS = {"jacobi": 0, "learned": 1, "chain": 2, "mg": 3}
+MG_DRAM_BYTES_PER_ROW = 225.0  # ncu: k_mg_pcg DRAM read + write per launch / free rows (8k-CNT network, both passes)
 KERNELS = {0: "k_pcg (grid-wide persistent PCG)", 1: "k_pcg_cluster (16-CTA cluster-resident PCG)",
            2: "k_mg_pcg (chain-aggregation multigrid PCG)"}
 
@@ -379,7 +380,7 @@ def contact_search_roofline(ctx, net, res, stage_acc, steps, hbm):
             "bound": "hbm", "algorithmic_bytes": b, "achieved": b / t / 1e9, "peak": hbm, "unit": "GB/s", "frac": b / t / 1e9 / hbm,
             "points": n_p, "slots": ns.value, "regions": nr.value, "point_contacts": n_k,
             "note": "stage time includes the host reads of the sizes (scan totals) between kernels; the largest kernel is "
-                    "k_pairs (one warp per region), see profiles/"}
+                    "k_pairs (one warp per region)"}
 
 
 def spmv_roofline(ctx, device, hbm, target_bytes=320e6, reps=20):
@@ -528,10 +529,11 @@ def run_ours(args):
                 stage_acc[j] += res.stage_seconds[j]
             for s in res.solves[: res.n_solves]:
                 cg_time += s.seconds
-                acc = per_kernel.setdefault(int(s.kernel), [0.0, 0, 0])
+                acc = per_kernel.setdefault(int(s.kernel), [0.0, 0, 0, 0])
                 acc[0] += s.seconds
                 acc[1] += 1
                 acc[2] += cg_bytes(s.nodes, s.reserved, s.nnz_lower, s.iterations)
+                acc[3] += s.nodes - s.reserved
                 iters.append(int(s.iterations))
                 resid.append(float(s.rel_residual))
         ev1.record(stream)
@@ -562,8 +564,12 @@ def run_ours(args):
             peaks = json.load(open(pk_path))
         hbm = peaks.get("hbm_gbs", 6650.0)
         top = max(per_kernel, key=lambda k: per_kernel[k][0]) if per_kernel else 0
-        k_sec, k_launch, k_bytes = per_kernel.get(top, [0.0, 0, 0])
+        k_sec, k_launch, k_bytes, k_rows = per_kernel.get(top, [0.0, 0, 0, 0])
         achieved = (k_bytes / k_launch) / (k_sec / k_launch) / 1e9 if k_launch and k_sec > 0 else 0.0
+        # DRAM bytes per launch of the multigrid kernel: 215-233 B per free row in an ncu capture of
+        # the 8k-CNT network's two passes (the system read once, L2-resident across iterations),
+        # scaled by the rows of this workload's launches
+        traffic = MG_DRAM_BYTES_PER_ROW * k_rows / k_launch if top == 2 and k_launch else None
         line = {
             "metric": METRIC,
             "value": world * args.steps / t_dev,
@@ -582,7 +588,11 @@ def run_ours(args):
                        "l2": "256 MB buffer written between steps (L2 flush)", "parallelism": f"replicas x{world}",
                        "precision": args.precision, "preconditioner": args.precond},
             "roofline": {"kernel": KERNELS[top], "bound": "hbm", "achieved": achieved, "peak": hbm,
-                         "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                         "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                         "traffic_note": "bytes per launch scaled by rows from an ncu capture of the same kernel on the "
+                                         "8k-CNT network (DRAM read + write, 225 B per free row); the algorithmic bytes per "
+                                         "launch are ~45x larger because the system stays in L2 across iterations",
+                         "algorithmic_bytes_per_launch": k_bytes / k_launch if k_launch else None,
                          "launches_per_step": k_launch / args.steps, "share_of_step": k_sec / t_dev,
                          "note": "algorithmic bytes = iterations x (SpMV + 12 vector passes) of the solves this kernel ran; "
                                  "the systems live in shared memory / L2, so the kernel is latency-bound (one cluster or "

@@ -37,6 +37,7 @@
 #include <vector>
 
 #include "cicy_internal.h"
+#include "csr_check.cuh"
 #include "dev_common.cuh"
 #include "solver.cuh"
 
@@ -371,6 +372,15 @@ __global__ void __launch_bounds__(T) k_batch_pcg(BatchArgs a) {
     }
 }
 
+// Structure check of every system (one CTA per system), before any solve reads it.
+__global__ void __launch_bounds__(256) k_batch_check(const BatchSys* __restrict__ sys, int count, int* __restrict__ bad) {
+    for (int id = blockIdx.x; id < count; id += gridDim.x) {
+        const BatchSys S = sys[id];
+        const int f = check_structure_part(threadIdx.x, blockDim.x, S.n, S.nnz, S.rp, S.ci, S.nchains, S.cs, S.cl);
+        if (f) atomicOr(&bad[id], f);
+    }
+}
+
 // FP64 |b - A x| / |b| of every system (one CTA per system).
 __global__ void __launch_bounds__(256) k_batch_residual(const BatchSys* __restrict__ sys, int count, double* __restrict__ rel) {
     __shared__ double sm[80];
@@ -644,6 +654,16 @@ cicy_status cicy_batch_create(cicy_batch** out, int device, const cicy_batch_sys
         B->scratch.ensure((size_t)off + 2);
         CICY_CUDA(cudaMemcpyAsync(B->sys.get(), h.data(), sizeof(cicy::BatchSys) * count, cudaMemcpyHostToDevice, B->stream));
         CICY_CUDA(cudaMemcpyAsync(B->order.get(), ord.data(), sizeof(int) * count, cudaMemcpyHostToDevice, B->stream));
+        // the solves trust the CSR and the chain partition: check them once here
+        CICY_CUDA(cudaMemsetAsync(B->flags.get(), 0, sizeof(int) * count, B->stream));
+        cicy::k_batch_check<<<std::min(count, B->sms * 4), 256, 0, B->stream>>>(B->sys.get(), count, B->flags.get());
+        CICY_LAUNCH_CHECK();
+        std::vector<int> bad(count);
+        CICY_CUDA(cudaMemcpyAsync(bad.data(), B->flags.get(), sizeof(int) * count, cudaMemcpyDeviceToHost, B->stream));
+        CICY_CUDA(cudaStreamSynchronize(B->stream));
+        for (int i = 0; i < count; i++)
+            if (bad[i])
+                throw cicy::Fail{CICY_E_INPUT, "cicy_batch_create: system " + std::to_string(i) + ": " + cicy::structure_error(bad[i])};
         CICY_CUDA(cudaStreamSynchronize(B->stream));
     });
     if (st != CICY_OK) {

@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "cicy_internal.h"
+#include "csr_check.cuh"
 #include "ctx.cuh"
 #include "solver.cuh"
 
@@ -674,8 +675,19 @@ const float* learned_edge_weights(Ctx& c, const SolverSystem& ss, int n_chains, 
 struct cicy_gnn {
     int device = 0;
     cicy::GnnState g;
+    cicy::DBuf<int> check;  // structure flags of the last cicy_gnn_set_system
     int64_t launches = 0;
 };
+
+namespace cicy {
+namespace {
+__global__ void k_check_system(int n, int nnz, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, int nchains,
+                               const int32_t* __restrict__ cs, const int32_t* __restrict__ cl, int* __restrict__ bad) {
+    const int f = check_structure_part(blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, n, nnz, rp, ci, nchains, cs, cl);
+    if (f) atomicOr(bad, f);
+}
+}  // namespace
+}  // namespace cicy
 
 namespace {
 
@@ -711,7 +723,10 @@ cicy_status cicy_gnn_create(cicy_gnn** out, int device) {
 }
 
 cicy_status cicy_gnn_destroy(cicy_gnn* g) {
-    delete g;
+    if (g) {
+        cudaSetDevice(g->device);
+        delete g;
+    }
     return CICY_OK;
 }
 
@@ -722,8 +737,19 @@ cicy_status cicy_gnn_set_system(cicy_gnn* g, const cicy_gnn_system* sys, void* s
         return CICY_E_INPUT;
     }
     return gnn_guard(g->device, [&] {
+        // the feature and message kernels use the column indices and chains as addresses: check them first
+        cudaStream_t s = (cudaStream_t)stream;
+        g->check.ensure(1);
+        CICY_CUDA(cudaMemsetAsync(g->check.get(), 0, sizeof(int), s));
+        cicy::k_check_system<<<std::min((std::max(sys->nnz, sys->n) + 255) / 256, 148 * 8), 256, 0, s>>>(
+            sys->n, sys->nnz, sys->row_ptr, sys->col_ind, sys->n_chains, sys->chain_start, sys->chain_len, g->check.get());
+        CICY_LAUNCH_CHECK();
+        int bad = 0;
+        CICY_CUDA(cudaMemcpyAsync(&bad, g->check.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        CICY_CUDA(cudaStreamSynchronize(s));
+        if (bad) throw cicy::Fail{CICY_E_INPUT, "cicy_gnn_set_system: " + cicy::structure_error(bad)};
         cicy::gnn_set_system(g->g, sys->n, sys->nnz, sys->row_ptr, sys->col_ind, sys->values, sys->n_chains, sys->chain_start,
-                             sys->chain_len, (cudaStream_t)stream, g->launches);
+                             sys->chain_len, s, g->launches);
     });
 }
 

@@ -236,7 +236,10 @@ typedef struct {
 } cicy_gnn_system;
 cicy_status cicy_gnn_create(cicy_gnn** out, int device);
 cicy_status cicy_gnn_destroy(cicy_gnn* g);
-/* Features and chain blocks of one system (kept until the next call). */
+/* Features and chain blocks of one system (kept until the next call).  The CSR
+ * structure and the chains are checked on the device first (CICY_E_INPUT when
+ * row_ptr is not 0 .. nnz non-decreasing, a column index is outside [0, n), or
+ * the chains are not consecutive runs covering the rows). */
 cicy_status cicy_gnn_set_system(cicy_gnn* g, const cicy_gnn_system* sys, void* stream);
 /* Forward pass: weight of every matrix entry (0 on the blocks and the diagonal) into w[nnz] (device). */
 cicy_status cicy_gnn_forward(cicy_gnn* g, const float* params, float* w, void* stream);
@@ -271,8 +274,10 @@ cicy_status cicy_spmv_csr(int32_t n, const int32_t* row_ptr, const int32_t* col_
  *   2  one system after another through the per-network grid-wide persistent
  *      PCG (the path cicy_electrical_analysis uses), same preconditioner and
  *      precision as method 0; seconds = the sum of its kernels' device times.
- * All pointers are device memory the caller keeps alive; the chains must
- * partition the rows. */
+ * All pointers are device memory the caller keeps alive, of the stated sizes;
+ * the chains must be consecutive runs of rows covering 0 .. n-1.
+ * cicy_batch_create checks the CSR structure and the chains on the device
+ * and returns CICY_E_INPUT naming the first bad system. */
 typedef struct {
     int32_t n, nnz;
     const int32_t* row_ptr;    /* full symmetric CSR, diagonal included, ascending columns */

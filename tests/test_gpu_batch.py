@@ -178,3 +178,30 @@ def test_batch_sequential_method(mc_systems, mc_batch):
         assert np.all(fl == 1), (pk, prec, fl)
     mc_batch.set_solver("chain", 0)
     mc_batch.set_method(0)
+
+
+def test_batch_rejects_malformed_systems(mc_systems):
+    """cicy_batch_create checks the CSR and the chain partition on the device
+    (reads within the stated sizes only) before any solve can use them."""
+    from cicy_geom_b200 import _abi
+
+    good = mc_systems[:3]
+    bad_chain = dict(good[1])
+    cl = np.array(bad_chain["chain_len"], np.int32).copy()
+    cl[0] += 1  # chains overlap: no longer consecutive runs
+    bad_chain["chain_len"] = cl
+    with pytest.raises(_abi.CicyError, match="system 1: the chains"):
+        BT.BatchSolver([good[0], bad_chain, good[2]])
+    with pytest.raises(_abi.CicyError, match="cicy_gnn_set_system: the chains"):
+        BT.BatchSolver([bad_chain], learned=True)
+    bad_col = dict(good[2])
+    A = bad_col["A"].copy()
+    A.indices = A.indices.copy()
+    A.indices[-1] = A.shape[0]  # one column index past the last row
+    bad_col["A"] = A
+    with pytest.raises(_abi.CicyError, match="system 2: a column index"):
+        BT.BatchSolver([good[0], good[1], bad_col])
+    bs = BT.BatchSolver(good)  # the valid systems still solve
+    bs.solve()
+    assert np.all(bs.results()[2] == 1)
+    bs.close()
