@@ -215,7 +215,8 @@ def lib() -> C.CDLL:
         "cicy_batch_enable_multigrid": (C.c_int, [C.c_void_p, f64p]),
         "cicy_batch_set_method": (C.c_int, [C.c_void_p, C.c_int32]),
         "cicy_batch_set_solver": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
-        "cicy_batch_autotune": (C.c_int, [C.c_void_p, i32p, i32p, i32p, f64p]),
+        "cicy_batch_autotune": (C.c_int, [C.c_void_p, i32p, i32p, i32p, i32p, f64p]),
+        "cicy_batch_set_split": (C.c_int, [C.c_void_p, C.c_int32]),
         "cicy_batch_solve": (C.c_int, [C.c_void_p, f64p]),
         "cicy_batch_results": (C.c_int, [C.c_void_p, i64p, f64p, i32p]),
         "cicy_get_chains": (C.c_int, [C.c_void_p, C.c_int32, i32p, i32p, i32p]),

@@ -168,10 +168,15 @@ class BatchSolver:
         _abi.check(_abi.lib().cicy_batch_set_solver(self.h, pk, precision), "cicy_batch_set_solver")
 
     def autotune(self):
-        m, t, c, s = C.c_int32(), C.c_int32(), C.c_int32(), C.c_double()
-        _abi.check(_abi.lib().cicy_batch_autotune(self.h, C.byref(m), C.byref(t), C.byref(c), C.byref(s)), "cicy_batch_autotune")
-        return {"method": METHODS[m.value], "threads": t.value, "ctas_per_sm": c.value,
+        m, t, c, sp, s = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32(), C.c_double()
+        _abi.check(_abi.lib().cicy_batch_autotune(self.h, C.byref(m), C.byref(t), C.byref(c), C.byref(sp), C.byref(s)),
+                   "cicy_batch_autotune")
+        return {"method": METHODS[m.value], "threads": t.value, "ctas_per_sm": c.value, "cluster_split_rows": sp.value,
                 "seconds": s.value}
+
+    def set_split(self, rows: int):
+        """Method 0: systems of at least `rows` rows run on one 16-CTA cluster each (0: none)."""
+        _abi.check(_abi.lib().cicy_batch_set_split(self.h, rows), "cicy_batch_set_split")
 
     def set_shape(self, threads: int, ctas_per_sm: int):
         _abi.check(_abi.lib().cicy_batch_set_shape(self.h, threads, ctas_per_sm), "cicy_batch_set_shape")
@@ -220,6 +225,7 @@ def main(argv=None):
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--threads", type=int, default=1024)
     ap.add_argument("--ctas-per-sm", type=int, default=2)
+    ap.add_argument("--split", type=int, default=0, help="systems of at least this many rows on 16-CTA clusters (0: none)")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--device", type=int, default=0)
     a = ap.parse_args(argv)
@@ -233,6 +239,7 @@ def main(argv=None):
     else:
         bs.set_solver(a.precond, a.precision)
         bs.set_shape(a.threads, a.ctas_per_sm)
+        bs.set_split(a.split)
     times = [bs.solve() for _ in range(a.reps)]
     it, rel, fl = bs.results()
     bs.close()

@@ -72,8 +72,11 @@ inline long long batch_scratch(long long n, long long nnz) {
 struct BatchArgs {
     const BatchSys* sys;
     const int* order;  // largest first
-    int count;
+    int count;         // this launch takes order[first .. count)
+    int first;
     int* queue;
+    int* slots;        // cluster kernel: the system index of each cluster
+    double* part;      // cluster kernel: partial sums, [cluster][bank][rank][2]
     double* scratch;
     double tol;
     long long iter_factor;
@@ -213,7 +216,7 @@ __global__ void __launch_bounds__(T) k_batch_pcg(BatchArgs a) {
     __shared__ double sm[80];
     __shared__ int s_q;
     while (true) {
-        if (threadIdx.x == 0) s_q = atomicAdd(a.queue, 1);
+        if (threadIdx.x == 0) s_q = a.first + atomicAdd(a.queue, 1);
         __syncthreads();
         const int q = s_q;
         __syncthreads();
@@ -372,6 +375,282 @@ __global__ void __launch_bounds__(T) k_batch_pcg(BatchArgs a) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// One 16-CTA cluster per system (large systems: one SM's L2 latency and
+// bandwidth bound the one-CTA solve).  Each CTA owns the chains whose first row
+// lies in its 1/16 of the rows, so the chain factors and sweeps stay CTA-local;
+// SpMV and the learned coupling term read other CTAs' rows from global memory
+// after a hardware cluster barrier (release/acquire).  Reductions: each CTA
+// writes its partial to a bank of `part`, a cluster barrier, then every CTA sums
+// the 16 partials in rank order (identical results, so every CTA takes the same
+// branches).  One bank per reduction kind, so a bank is rewritten only after a
+// later barrier.  Barriers per iteration: 3 (4 with the learned term).
+constexpr int kClCtas = 16;
+constexpr int kClThreads = 512;
+
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+    asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+
+// First chain whose start row is >= row (chain starts ascend).
+__device__ __forceinline__ int chain_at(const BatchSys& S, long long row) {
+    int lo = 0, hi = S.nchains;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (S.cs[mid] < row) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Cluster-wide sum of (a, b): this CTA's partial into bank `bank`, barrier, sum of the 16.
+__device__ __forceinline__ void cl_sum2(double a, double b, double* sm, double* part, int bank, int rank, double& ra, double& rb) {
+    double pa, pb;
+    cta_sum2<kClThreads>(a, b, sm, pa, pb);
+    double* slot = part + (size_t)bank * kClCtas * 2;
+    if (threadIdx.x == 0) {
+        slot[2 * rank] = pa;
+        slot[2 * rank + 1] = pb;
+    }
+    cluster_sync();
+    ra = 0;
+    rb = 0;
+    for (int r = 0; r < kClCtas; r++) {
+        ra += __ldcg(&slot[2 * r]);
+        rb += __ldcg(&slot[2 * r + 1]);
+    }
+}
+
+// z = T^-1 r over this CTA's chains (see apply_chains).
+template <typename PT>
+__device__ void apply_chains_range(const BatchSys& S, int c_lo, int c_hi, const PT* lf, const PT* ip, const double* r, double* z) {
+    for (int c = c_lo + threadIdx.x; c < c_hi; c += blockDim.x) {
+        const int s0 = S.cs[c], m = S.cl[c];
+        PT y = (PT)r[s0];
+        z[s0] = (double)y;
+        for (int k = 1; k < m; k++) {
+            y = (PT)r[s0 + k] - lf[s0 + k] * y;
+            z[s0 + k] = (double)y;
+        }
+        PT zn = (PT)z[s0 + m - 1] * ip[s0 + m - 1];
+        z[s0 + m - 1] = (double)zn;
+        for (int k = m - 2; k >= 0; k--) {
+            zn = (PT)z[s0 + k] * ip[s0 + k] - lf[s0 + k + 1] * zn;
+            z[s0 + k] = (double)zn;
+        }
+    }
+}
+
+template <typename PT, int BLK>
+__device__ void factor_chains_range(const BatchSys& S, int c_lo, int c_hi, PT* lf, PT* ip) {
+    for (int c = c_lo + threadIdx.x; c < c_hi; c += blockDim.x) {
+        const int s0 = S.cs[c], m = S.cl[c];
+        const int bl = BLK > 0 ? BLK : m;
+        for (int b0 = 0; b0 < m; b0 += bl) {
+            const int bm = min(bl, m - b0);
+            bool singular = false;
+            double piv_prev = 0, e_prev = 0;
+            for (int k = 0; k < bm; k++) {
+                const int i = s0 + b0 + k;
+                const double d = diag_of(S, i);
+                double l = 0, piv = d;
+                if (k > 0) {
+                    l = e_prev / piv_prev;
+                    piv = d - l * e_prev;
+                }
+                singular |= !(piv > 1e-13 * fabs(d));
+                lf[i] = (PT)l;
+                ip[i] = (PT)(1.0 / piv);
+                piv_prev = piv;
+                e_prev = (k + 1 < bm) ? upper(S, i) : 0.0;
+            }
+            if (singular)
+                for (int k = 0; k < bm; k++) {
+                    const int i = s0 + b0 + k;
+                    lf[i] = (PT)0;
+                    ip[i] = (PT)(1.0 / diag_of(S, i));
+                }
+        }
+    }
+}
+
+template <int PK, bool MX>
+__global__ void __launch_bounds__(kClThreads) k_batch_pcg_cl(BatchArgs a) {
+    using PT = typename std::conditional<MX, float, double>::type;
+    constexpr int T = kClThreads;
+    __shared__ double sm[80];
+    const int cl = blockIdx.x / kClCtas, rank = blockIdx.x % kClCtas;
+    double* part = a.part + (size_t)cl * 5 * kClCtas * 2;
+    while (true) {
+        if (rank == 0 && threadIdx.x == 0) a.slots[cl] = a.first + atomicAdd(a.queue, 1);
+        cluster_sync();
+        const int q = __ldcg(&a.slots[cl]);
+        cluster_sync();
+        if (q >= a.count) return;
+        const int id = a.order[q];
+        const BatchSys S = a.sys[id];
+        const int n = S.n;
+        const int c_lo = chain_at(S, (long long)rank * n / kClCtas);
+        const int c_hi = rank == kClCtas - 1 ? S.nchains : chain_at(S, (long long)(rank + 1) * n / kClCtas);
+        const int r_lo = c_lo < S.nchains ? S.cs[c_lo] : n, r_hi = c_hi < S.nchains ? S.cs[c_hi] : n;
+        double* r = a.scratch + S.off;
+        double* p = r + n;
+        double* qv = p + n;
+        double* z = qv + n;
+        double* y = z + n;
+        double* u = y + n;
+        PT* lf = reinterpret_cast<PT*>(u + n);
+        PT* ip = lf + n;
+        float* g32 = reinterpret_cast<float*>(u + 3 * (long long)n);
+        float* rs32 = g32 + S.nnz;
+        if (PK == 0) {
+            for (int i = r_lo + threadIdx.x; i < r_hi; i += T) ip[i] = (PT)(1.0 / diag_of(S, i));
+        } else {
+            factor_chains_range<PT, PK == 1 ? kSpaiBlock : 0>(S, c_lo, c_hi, lf, ip);
+        }
+        if (MX) {
+            for (int i = r_lo + threadIdx.x; i < r_hi; i += T) {
+                double rs = 0;
+                for (int k = S.rp[i]; k < S.rp[i + 1]; k++) {
+                    rs += S.val[k];
+                    g32[k] = S.ci[k] == i ? 0.0f : (float)(-S.val[k]);
+                }
+                rs32[i] = (float)rs;
+            }
+        }
+        double rr_l = 0, bb_l = 0;
+        for (int i = r_lo + threadIdx.x; i < r_hi; i += T) {
+            double sacc = 0;
+            for (int k = S.rp[i]; k < S.rp[i + 1]; k++) sacc += S.val[k] * S.x0[S.ci[k]];
+            const double ri = S.b[i] - sacc;
+            r[i] = ri;
+            S.x[i] = S.x0[i];
+            rr_l += ri * ri;
+            bb_l += S.b[i] * S.b[i];
+        }
+        double rr, bb;
+        cl_sum2(rr_l, bb_l, sm, part, 0, rank, rr, bb);
+        const double R0 = a.tol * sqrt(fmin(rr, bb));
+        double anchor = sqrt(rr);
+        const long long max_iter = a.iter_factor * (long long)n;
+        long long k = 0;
+        int restarts = 0, flag = 0;
+        bool fresh = true;
+        double rz = 0, dummy;
+        while (true) {
+            // ---- z = M^-1 r (own rows)
+            if (PK == 0) {
+                for (int i = r_lo + threadIdx.x; i < r_hi; i += T) z[i] = (double)((PT)r[i] * ip[i]);
+            } else if (PK == 2) {
+                apply_chains_range<PT>(S, c_lo, c_hi, lf, ip, r, z);
+            } else {
+                apply_chains_range<PT>(S, c_lo, c_hi, lf, ip, r, y);
+                cluster_sync();  // the coupling term reads y of other CTAs' rows
+                for (int i = r_lo + threadIdx.x; i < r_hi; i += T) {
+                    if (MX) {
+                        float f = 0;
+                        for (int kk = S.rp[i]; kk < S.rp[i + 1]; kk++) {
+                            const float w = S.ew[kk];
+                            if (w != 0.0f) f += w * g32[kk] * (float)__ldcg(&y[S.ci[kk]]);
+                        }
+                        u[i] = (double)f;
+                    } else {
+                        double sacc = 0;
+                        for (int kk = S.rp[i]; kk < S.rp[i + 1]; kk++) {
+                            const float w = S.ew[kk];
+                            if (w != 0.0f) sacc += (double)w * (-S.val[kk]) * __ldcg(&y[S.ci[kk]]);
+                        }
+                        u[i] = sacc;
+                    }
+                }
+                __syncthreads();
+                apply_chains_range<PT>(S, c_lo, c_hi, lf, ip, u, z);
+                __syncthreads();
+                for (int i = r_lo + threadIdx.x; i < r_hi; i += T) z[i] += y[i];
+            }
+            __syncthreads();
+            double rz_l = 0;
+            for (int i = r_lo + threadIdx.x; i < r_hi; i += T) rz_l += r[i] * z[i];
+            double rz_new;
+            cl_sum2(rz_l, 0.0, sm, part, 1, rank, rz_new, dummy);
+            const double beta = fresh ? 0.0 : rz_new / rz;
+            rz = rz_new;
+            for (int i = r_lo + threadIdx.x; i < r_hi; i += T) p[i] = z[i] + beta * (fresh ? 0.0 : p[i]);
+            cluster_sync();  // q = A p reads p of other CTAs' rows
+            // ---- q = A p (own rows)
+            double pq_l = 0;
+            for (int i = r_lo + threadIdx.x; i < r_hi; i += T) {
+                double sq;
+                if (MX) {
+                    const double pi = p[i];
+                    float f = rs32[i] * (float)pi;
+                    for (int kk = S.rp[i]; kk < S.rp[i + 1]; kk++) f += g32[kk] * (float)(pi - __ldcg(&p[S.ci[kk]]));
+                    sq = (double)f;
+                } else {
+                    sq = 0;
+                    for (int kk = S.rp[i]; kk < S.rp[i + 1]; kk++) sq += S.val[kk] * __ldcg(&p[S.ci[kk]]);
+                }
+                qv[i] = sq;
+                pq_l += p[i] * sq;
+            }
+            double pq;
+            cl_sum2(pq_l, 0.0, sm, part, 2, rank, pq, dummy);
+            if (!(pq > 0) || !(rz > 0)) break;  // breakdown: stop with x intact, flag 0
+            fresh = false;
+            k++;
+            const double alpha = rz / pq;
+            rr_l = 0;
+            for (int i = r_lo + threadIdx.x; i < r_hi; i += T) {
+                S.x[i] += alpha * p[i];
+                const double ri = r[i] - alpha * qv[i];
+                r[i] = ri;
+                rr_l += ri * ri;
+            }
+            cl_sum2(rr_l, 0.0, sm, part, 3, rank, rr, dummy);  // (also makes x complete for a true residual)
+            if (!(rr == rr)) break;
+            const double rn = sqrt(rr);
+            const bool conv = rn <= R0;
+            const bool repl = !conv && MX && rn <= kReplaceDrop * anchor && restarts < kBatchReplacements;
+            if (conv || repl) {
+                if (conv && restarts >= (MX ? kBatchReplacements : kBatchRestarts)) break;
+                double tl = 0;
+                for (int i = r_lo + threadIdx.x; i < r_hi; i += T) {
+                    double sacc = 0;
+                    for (int kk = S.rp[i]; kk < S.rp[i + 1]; kk++) sacc += S.val[kk] * __ldcg(&S.x[S.ci[kk]]);
+                    const double ri = S.b[i] - sacc;
+                    r[i] = ri;
+                    tl += ri * ri;
+                }
+                cl_sum2(tl, 0.0, sm, part, 4, rank, rr, dummy);
+                restarts++;
+                if (conv && sqrt(rr) <= R0) { flag = 1; break; }
+                anchor = sqrt(rr);
+                if (conv) fresh = !MX;  // FP64: restart; mixed: residual replacement, directions kept
+            }
+            if (k >= max_iter) { flag = 2; break; }
+        }
+        // FP64 relative residual |b - A x| / |b| (x of all rows complete after a barrier)
+        cluster_sync();
+        bb_l = 0;
+        double tr_l = 0;
+        for (int i = r_lo + threadIdx.x; i < r_hi; i += T) {
+            double sacc = 0;
+            for (int kk = S.rp[i]; kk < S.rp[i + 1]; kk++) sacc += S.val[kk] * __ldcg(&S.x[S.ci[kk]]);
+            const double ri = S.b[i] - sacc;
+            tr_l += ri * ri;
+            bb_l += S.b[i] * S.b[i];
+        }
+        double trr, bbb;
+        cl_sum2(tr_l, bb_l, sm, part, 0, rank, trr, bbb);
+        if (rank == 0 && threadIdx.x == 0) {
+            a.iterations[id] = k;
+            a.rel[id] = bbb > 0 ? sqrt(trr / bbb) : 0.0;
+            a.flags[id] = flag;
+        }
+    }
+}
+
 // Structure check of every system (one CTA per system), before any solve reads it.
 __global__ void __launch_bounds__(256) k_batch_check(const BatchSys* __restrict__ sys, int count, int* __restrict__ bad) {
     for (int id = blockIdx.x; id < count; id += gridDim.x) {
@@ -407,6 +686,68 @@ void launch(const BatchArgs& a, int grid, int pk, bool mx, cudaStream_t s) {
     else mx ? k_batch_pcg<T, 2, true><<<grid, T, 0, s>>>(a) : k_batch_pcg<T, 2, false><<<grid, T, 0, s>>>(a);
 }
 
+template <int PK, bool MX>
+void* cl_kernel() {
+    return (void*)k_batch_pcg_cl<PK, MX>;
+}
+
+void* cl_kernel_for(int pk, bool mx) {
+    if (pk == 0) return mx ? cl_kernel<0, true>() : cl_kernel<0, false>();
+    if (pk == 1) return mx ? cl_kernel<1, true>() : cl_kernel<1, false>();
+    return mx ? cl_kernel<2, true>() : cl_kernel<2, false>();
+}
+
+// 16-CTA clusters are a non-portable size: opt every instantiation in once.
+// Returns the number of clusters of one instantiation that fit at once (0: none).
+int cl_setup(int sms) {
+    static int clusters = -1;
+    if (clusters >= 0) return clusters;
+    clusters = 0;
+    bool ok = true;
+    for (int pk = 0; pk < 3; pk++)
+        for (int mx = 0; mx < 2; mx++)
+            ok &= cudaFuncSetAttribute(cl_kernel_for(pk, mx != 0), cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess;
+    cudaGetLastError();
+    if (!ok) return clusters;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    cfg.gridDim = dim3(kClCtas);
+    cfg.blockDim = dim3(kClThreads);
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kClCtas;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int mn = 1 << 30;
+    for (int pk = 0; pk < 3; pk++)
+        for (int mx = 0; mx < 2; mx++) {
+            int n = 0;
+            if (cudaOccupancyMaxActiveClusters(&n, cl_kernel_for(pk, mx != 0), &cfg) != cudaSuccess) n = 0;
+            mn = std::min(mn, n);
+        }
+    cudaGetLastError();
+    clusters = std::max(0, std::min(mn, sms / kClCtas));
+    return clusters;
+}
+
+void launch_cl(const BatchArgs& a, int nclusters, int pk, bool mx, cudaStream_t s) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    cfg.gridDim = dim3(kClCtas * nclusters);
+    cfg.blockDim = dim3(kClThreads);
+    cfg.stream = s;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kClCtas;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    BatchArgs args = a;
+    void* params[] = {&args};
+    CICY_CUDA(cudaLaunchKernelExC(&cfg, cl_kernel_for(pk, mx), params));
+}
+
 __global__ void k_diag_extract(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const double* __restrict__ v,
                                double* __restrict__ d) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -430,28 +771,36 @@ struct cicy_batch {
     long long iter_factor = 300;
     int threads = 512, ctas_per_sm = 2, sms = 148;
     int method = 0;  // 0: one CTA per system, 1: one 16-CTA cluster per system (multigrid), 2: one system at a time, grid-wide
+    int split = 0;   // method 0: systems of at least this many rows run on 16-CTA clusters (0: none)
+    int n_split = 0; // how many systems that is (the first ones of the largest-first order)
+    int nclusters = 0;
     bool have_weights = false;
     cicy::MgBatch* mg = nullptr;
     int64_t launches = 0;
     std::vector<cicy_batch_system> inputs;
     cicy::DBuf<cicy::BatchSys> sys;
-    cicy::DBuf<int> order, queue, flags, status;
+    cicy::DBuf<int> order, queue, flags, status, queue2, slots;
+    cicy::DBuf<double> part;
     cicy::DBuf<double> scratch, rel, diag;
     cicy::DBuf<long long> iterations;
     std::vector<long long> diag_off, seq_iterations;
     cicy::SolverWork* sw = nullptr;  // method 2
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    int graph_threads = 0, graph_ctas = 0, graph_method = -1, graph_precond = -1, graph_precision = -1;
-    cudaStream_t stream = nullptr;
+    int graph_threads = 0, graph_ctas = 0, graph_method = -1, graph_precond = -1, graph_precision = -1, graph_split = -1;
+    cudaStream_t stream = nullptr, stream2 = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
     ~cicy_batch() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         if (stream) cudaStreamDestroy(stream);
+        if (stream2) cudaStreamDestroy(stream2);
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
         if (mg) cicy::mg_batch_free(mg);
         delete sw;
         sys.release(); order.release(); queue.release(); flags.release(); status.release(); scratch.release(); rel.release();
-        diag.release(); iterations.release();
+        diag.release(); iterations.release(); queue2.release(); slots.release(); part.release();
     }
 };
 
@@ -480,6 +829,7 @@ void enqueue(cicy_batch* B, cudaStream_t s) {
     a.sys = B->sys.get();
     a.order = B->order.get();
     a.count = B->count;
+    a.first = 0;
     a.queue = B->queue.get();
     a.scratch = B->scratch.get();
     a.tol = B->tol;
@@ -487,15 +837,37 @@ void enqueue(cicy_batch* B, cudaStream_t s) {
     a.iterations = B->iterations.get();
     a.rel = B->rel.get();
     a.flags = B->flags.get();
-    CICY_CUDA(cudaMemsetAsync(B->queue.get(), 0, sizeof(int), s));
-    const int grid = std::max(1, std::min(B->count, B->sms * B->ctas_per_sm));
     const bool mx = B->precision == CICY_PRECISION_MIXED;
-    switch (B->threads) {
-        case 256: cicy::launch<256>(a, grid, B->precond, mx, s); break;
-        case 512: cicy::launch<512>(a, grid, B->precond, mx, s); break;
-        default: cicy::launch<1024>(a, grid, B->precond, mx, s); break;
+    const int K = B->split > 0 ? B->n_split : 0;
+    if (K > 0) {  // the largest systems on 16-CTA clusters, concurrently with the rest (fork/join)
+        CICY_CUDA(cudaEventRecord(B->fork, s));
+        CICY_CUDA(cudaStreamWaitEvent(B->stream2, B->fork, 0));
+        cicy::BatchArgs c = a;
+        c.first = 0;
+        c.count = K;
+        c.queue = B->queue2.get();
+        c.slots = B->slots.get();
+        c.part = B->part.get();
+        CICY_CUDA(cudaMemsetAsync(B->queue2.get(), 0, sizeof(int), B->stream2));
+        // with one-CTA solves running beside them, at most 8 clusters (neither kernel waits on the other:
+        // a cluster not yet resident only starts later)
+        const int ncl = std::min({B->nclusters, K, K < B->count ? 8 : B->nclusters});
+        cicy::launch_cl(c, ncl, B->precond, mx, B->stream2);
+        CICY_LAUNCH_CHECK();
+        CICY_CUDA(cudaEventRecord(B->join, B->stream2));
     }
-    CICY_LAUNCH_CHECK();
+    if (K < B->count) {
+        a.first = K;
+        CICY_CUDA(cudaMemsetAsync(B->queue.get(), 0, sizeof(int), s));
+        const int grid = std::max(1, std::min(B->count - K, B->sms * B->ctas_per_sm));
+        switch (B->threads) {
+            case 256: cicy::launch<256>(a, grid, B->precond, mx, s); break;
+            case 512: cicy::launch<512>(a, grid, B->precond, mx, s); break;
+            default: cicy::launch<1024>(a, grid, B->precond, mx, s); break;
+        }
+        CICY_LAUNCH_CHECK();
+    }
+    if (K > 0) CICY_CUDA(cudaStreamWaitEvent(s, B->join, 0));
 }
 
 // Method 2: every system through the per-network grid-wide persistent PCG, one
@@ -561,7 +933,7 @@ double solve_sequential(cicy_batch* B) {
 // (Re)build the graph of one batch solve for the current launch shape.
 void ensure_graph(cicy_batch* B) {
     if (B->exec && B->graph_threads == B->threads && B->graph_ctas == B->ctas_per_sm && B->graph_method == B->method &&
-        B->graph_precond == B->precond && B->graph_precision == B->precision)
+        B->graph_precond == B->precond && B->graph_precision == B->precision && B->graph_split == B->split)
         return;
     if (B->exec) cudaGraphExecDestroy(B->exec);
     if (B->graph) cudaGraphDestroy(B->graph);
@@ -583,6 +955,7 @@ void ensure_graph(cicy_batch* B) {
     B->graph_method = B->method;
     B->graph_precond = B->precond;
     B->graph_precision = B->precision;
+    B->graph_split = B->split;
 }
 
 double timed_solve(cicy_batch* B) {
@@ -633,6 +1006,9 @@ cicy_status cicy_batch_create(cicy_batch** out, int device, const cicy_batch_sys
         B->iter_factor = max_iter_factor;
         CICY_CUDA(cudaDeviceGetAttribute(&B->sms, cudaDevAttrMultiProcessorCount, device));
         CICY_CUDA(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
+        CICY_CUDA(cudaStreamCreateWithFlags(&B->stream2, cudaStreamNonBlocking));
+        CICY_CUDA(cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming));
+        CICY_CUDA(cudaEventCreateWithFlags(&B->join, cudaEventDisableTiming));
         B->have_weights = weights;
         std::vector<cicy::BatchSys> h(count);
         long long off = 0;
@@ -708,6 +1084,29 @@ cicy_status cicy_batch_set_solver(cicy_batch* b, int32_t preconditioner, int32_t
     return CICY_OK;
 }
 
+namespace {
+void apply_split(cicy_batch* b, int rows) {
+    b->split = rows;
+    b->n_split = 0;
+    if (rows <= 0) return;
+    for (const auto& in : b->inputs) b->n_split += in.n >= rows ? 1 : 0;
+    if (b->n_split == 0) return;
+    b->nclusters = cicy::cl_setup(b->sms);
+    if (b->nclusters < 1) throw cicy::Fail{CICY_E_DEVICE, "cicy_batch_set_split: 16-CTA clusters are not available"};
+    b->queue2.ensure(1);
+    b->slots.ensure(b->nclusters);
+    b->part.ensure((size_t)b->nclusters * 5 * cicy::kClCtas * 2);
+}
+}  // namespace
+
+cicy_status cicy_batch_set_split(cicy_batch* b, int32_t rows) {
+    if (!b || rows < 0) {
+        cicy::set_host_error("cicy_batch_set_split: rows >= 0");
+        return CICY_E_INPUT;
+    }
+    return batch_guard(b->device, [&] { apply_split(b, rows); });
+}
+
 cicy_status cicy_batch_enable_multigrid(cicy_batch* b, double* setup_seconds) {
     if (!b) return CICY_E_INPUT;
     return batch_guard(b->device, [&] {
@@ -733,12 +1132,14 @@ cicy_status cicy_batch_set_method(cicy_batch* b, int32_t method) {
     return CICY_OK;
 }
 
-cicy_status cicy_batch_autotune(cicy_batch* b, int32_t* method, int32_t* threads, int32_t* ctas_per_sm, double* seconds) {
+cicy_status cicy_batch_autotune(cicy_batch* b, int32_t* method, int32_t* threads, int32_t* ctas_per_sm, int32_t* split_rows,
+                                double* seconds) {
     if (!b) return CICY_E_INPUT;
     return batch_guard(b->device, [&] {
         static const int cand[][3] = {{0, 256, 4}, {0, 256, 8}, {0, 512, 2}, {0, 512, 4}, {0, 1024, 1}, {0, 1024, 2}, {1, 1024, 1}};
         double best = 1e300;
         int bm = b->method, bt = b->threads, bc = b->ctas_per_sm;
+        apply_split(b, 0);  // launch shapes first, every system on one CTA
         for (const auto& c : cand) {
             if (c[0] == 1 && !b->mg) continue;
             b->method = c[0];
@@ -757,6 +1158,23 @@ cicy_status cicy_batch_autotune(cicy_batch* b, int32_t* method, int32_t* threads
         b->method = bm;
         b->threads = bt;
         b->ctas_per_sm = bc;
+        // method 0: the largest systems on 16-CTA clusters, at a few size thresholds
+        int bs = 0;
+        if (bm == 0 && cicy::cl_setup(b->sms) > 0) {
+            for (int rows : {131072, 32768, 8192}) {
+                apply_split(b, rows);
+                if (b->n_split == 0) continue;
+                const double t0 = timed_solve(b);
+                if (t0 > 1.5 * best) continue;
+                const double t = std::min(t0, timed_solve(b));
+                if (t < best) {
+                    best = t;
+                    bs = rows;
+                }
+            }
+        }
+        apply_split(b, bs);
+        if (split_rows) *split_rows = b->method == 0 ? b->split : 0;
         if (method) *method = bm;
         if (threads) *threads = bt;
         if (ctas_per_sm) *ctas_per_sm = bm == 1 ? cicy::mg_batch_clusters(b->mg) : bc;

@@ -268,7 +268,8 @@ cicy_status cicy_spmv_csr(int32_t n, const int32_t* row_ptr, const int32_t* col_
  * Methods:
  *   0  one persistent kernel launch replayed from a CUDA graph; each CTA takes
  *      the next system of a largest-first queue and runs preconditioned CG on
- *      it alone, with the preconditioner and precision of cicy_batch_set_solver;
+ *      it alone, with the preconditioner and precision of cicy_batch_set_solver
+ *      (the largest systems optionally on 16-CTA clusters, cicy_batch_set_split);
  *   1  one 16-CTA cluster per system running the chain-aggregation multigrid
  *      PCG (after cicy_batch_enable_multigrid; FP64);
  *   2  one system after another through the per-network grid-wide persistent
@@ -307,15 +308,23 @@ cicy_status cicy_batch_set_shape(cicy_batch* b, int32_t threads, int32_t ctas_pe
  * preconditioner factors; FP64 vectors, dots and residual replacement).
  * Default: CICY_PRECOND_CHAIN and the precision given to create. */
 cicy_status cicy_batch_set_solver(cicy_batch* b, int32_t preconditioner, int32_t precision);
+/* Method 0: systems of at least `rows` rows each run on one 16-CTA cluster
+ * (chain-aligned row ranges per CTA, hardware cluster barriers), concurrently
+ * with the one-CTA solves of the rest, in the same graph launch; 0 (the
+ * default): every system on one CTA. */
+cicy_status cicy_batch_set_split(cicy_batch* b, int32_t rows);
 /* Builds a multigrid hierarchy per system (setup time returned) so the batch can
  * also run method 1. */
 cicy_status cicy_batch_enable_multigrid(cicy_batch* b, double* setup_seconds);
 /* 0, 1 or 2 (above). */
 cicy_status cicy_batch_set_method(cicy_batch* b, int32_t method);
 /* Times method 0's launch shapes (with the current preconditioner and
- * precision) and, when multigrid is enabled, method 1, on this batch, and keeps
- * the fastest (for method 1 ctas_per_sm returns the number of concurrent clusters). */
-cicy_status cicy_batch_autotune(cicy_batch* b, int32_t* method, int32_t* threads, int32_t* ctas_per_sm, double* seconds);
+ * precision) and, when multigrid is enabled, method 1, on this batch, then for
+ * method 0 the cluster split at 131072, 32768 and 8192 rows, and keeps the
+ * fastest (for method 1 ctas_per_sm returns the number of concurrent clusters;
+ * split_rows is 0 when no system runs on a cluster). */
+cicy_status cicy_batch_autotune(cicy_batch* b, int32_t* method, int32_t* threads, int32_t* ctas_per_sm, int32_t* split_rows,
+                                double* seconds);
 /* One solve of every system by the current method; seconds = its device time (CUDA events). */
 cicy_status cicy_batch_solve(cicy_batch* b, double* seconds);
 /* Per system: iterations, FP64 |b - A x| / |b|, flag (1 converged, 2 iteration cap, 0 breakdown or restart limit). */

@@ -205,3 +205,30 @@ def test_batch_rejects_malformed_systems(mc_systems):
     bs.solve()
     assert np.all(bs.results()[2] == 1)
     bs.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batch_cluster_split(mc_systems, mc_batch, precision):
+    """Systems on 16-CTA clusters (all of them, then the larger half) reach the
+    same tolerance as on one CTA each, with similar iteration counts."""
+    sizes = sorted(s["A"].shape[0] for s in mc_systems)
+    mc_batch.set_method(0)
+    for pk in ("jacobi", "chain", "learned"):
+        mc_batch.set_solver(pk, precision)
+        mc_batch.set_split(0)
+        mc_batch.solve()
+        it0, _, _ = mc_batch.results()
+        x0 = mc_batch.solutions()
+        for rows in (1, sizes[len(sizes) // 2]):
+            mc_batch.set_split(rows)
+            mc_batch.solve()
+            it, rel, fl = mc_batch.results()
+            assert np.all(fl == 1) and np.all(rel <= 1.01e-8), (pk, rows, fl, rel)
+            # (reduction order differs: Jacobi-CG's iteration count on these systems is the most rounding-sensitive)
+            spread = 0.5 if pk == "jacobi" else 0.25
+            assert np.all(np.abs(it - it0) <= spread * it0 + 10), (pk, rows, it, it0)
+            for s, a, b in zip(mc_systems, mc_batch.solutions(), x0):
+                m = grounded(s["A"])
+                assert np.max(np.abs(a[m] - b[m])) <= 5e-2 * np.max(np.abs(b[m])), (pk, rows)
+    mc_batch.set_split(0)
+    mc_batch.set_solver("chain", 0)
