@@ -205,6 +205,7 @@ def lib() -> C.CDLL:
         "cicy_generate_cnt_network": (C.c_int, [P(GenParams), P(C.c_void_p)]),
         "cicy_extract_window": (C.c_int, [C.c_void_p, P(WindowParams), P(C.c_void_p)]),
         "cicy_host_network_from_arrays": (C.c_int, [P(Network), P(C.c_void_p)]),
+        "cicy_read_network": (C.c_int, [C.c_char_p, C.c_int32, P(C.c_void_p)]),
         "cicy_host_network_view": (C.c_int, [C.c_void_p, P(Network)]),
         "cicy_host_network_free": (None, [C.c_void_p]),
         "cicy_host_last_error": (C.c_char_p, []),

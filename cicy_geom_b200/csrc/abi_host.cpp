@@ -37,6 +37,18 @@ cicy_status cicy_extract_window(const cicy_host_network* in, const cicy_window_p
     return CICY_OK;
 }
 
+cicy_status cicy_read_network(const char* directory, int32_t file_type, cicy_host_network** out) {
+    if (!directory || !out) return CICY_E_INPUT;
+    cicy::HostNetwork* h = nullptr;
+    cicy_status s = cicy::read_network_files(directory, file_type, &h, g_host_error);
+    if (s != CICY_OK) return s;
+    cicy_host_network* w = new cicy_host_network;
+    w->net = std::move(*h);
+    delete h;
+    *out = w;
+    return CICY_OK;
+}
+
 cicy_status cicy_host_network_from_arrays(const cicy_network* n, cicy_host_network** out) {
     if (!n || !out || n->n_points < 0 || n->n_cnts < 0 || !n->structure_ptr) return CICY_E_INPUT;
     cicy::HostNetwork* h = cicy::host_network_from_view(*n);

@@ -9,6 +9,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <thread>
@@ -386,6 +388,149 @@ cicy_status extract_window(const HostNetwork& in, const cicy_window_params& w, H
         h->boundary_pts_ptr.push_back((int64_t)h->boundary_pts_idx.size());
     }
     h->window = c.win;
+    *out = h;
+    return CICY_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Read_Network::Read_sample_geometry + Read_cnt_data_from_dat / _from_csv
+// (Read_Network.cpp:154-467), CNT branch: the files of `dir` into the layout
+// the generator emits (points in CNT order, flag = CNT index, structure = the
+// consecutive point ids, window = the sample).  Both formats are read whole and
+// parsed in memory (strtod, the conversion the upstream stream extraction
+// performs, so the doubles are the same); the upstream error cases (a file
+// ending before every CNT or point was read, n_cnts mismatch on the CSV's first
+// line, missing files) fail with CICY_E_INPUT and the upstream message.
+namespace {
+
+bool slurp(const std::string& path, std::string& out) {
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) return false;
+    std::fseek(f, 0, SEEK_END);
+    const long n = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    out.resize(n > 0 ? (size_t)n : 0);
+    const size_t got = n > 0 ? std::fread(&out[0], 1, (size_t)n, f) : 0;
+    std::fclose(f);
+    return got == out.size();
+}
+
+// `count` numbers separated by one character each (the stream's ignore()), then the rest of the line.
+bool parse_line(const char*& p, const char* end, int count, double* v) {
+    if (p >= end) return false;
+    for (int i = 0; i < count; i++) {
+        char* q = nullptr;
+        v[i] = std::strtod(p, &q);
+        if (q == p) return false;
+        p = q;
+        if (i + 1 < count && p < end) p++;  // the separator
+    }
+    while (p < end && *p != '\n') p++;
+    if (p < end) p++;
+    return true;
+}
+
+}  // namespace
+
+cicy_status read_network_files(const std::string& dir, int file_type, HostNetwork** out, std::string& err) {
+    HostNetwork* h = new HostNetwork;
+    auto fail = [&](const std::string& m) {
+        delete h;
+        err = m;
+        return CICY_E_INPUT;
+    };
+    std::string text;
+    if (!slurp(dir + "/sample_geom.csv", text))
+        return fail("Error in Read_sample_geometry: Failed to open file with sample geometry data sample_geom.csv.");
+    {
+        const char* p = text.data();
+        const char* e = p + text.size();
+        double a[3], l[3];
+        if (!parse_line(p, e, 3, a) || !parse_line(p, e, 3, l)) return fail("Error in Read_sample_geometry: sample_geom.csv needs two lines");
+        cicy_cuboid& w = h->window;
+        w.min_x = a[0]; w.min_y = a[1]; w.min_z = a[2];
+        w.len_x = l[0]; w.len_y = l[1]; w.len_z = l[2];
+        w.max_x = w.min_x + w.len_x;
+        w.max_y = w.min_y + w.len_y;
+        w.max_z = w.min_z + w.len_z;
+    }
+    std::vector<int32_t> np;
+    if (file_type == 0) {
+        std::string st;
+        if (!slurp(dir + "/cnt_struct.dat", st)) return fail("Failed to open CNT structure file cnt_struct.dat.");
+        if (st.size() < 4) return fail("Error in Read_cnt_data_from_dat. The end-of-file of cnt_struct.dat has been reached before reading all CNT data.");
+        int32_t n = 0;
+        std::memcpy(&n, st.data(), 4);
+        if (n < 0 || st.size() < 4 + 12 * (size_t)n)
+            return fail("Error in Read_cnt_data_from_dat. The end-of-file of cnt_struct.dat has been reached before reading all CNT data.");
+        np.resize(n);
+        h->radii.resize(n);
+        for (int32_t i = 0; i < n; i++) {
+            std::memcpy(&np[i], st.data() + 4 + 12 * (size_t)i, 4);
+            std::memcpy(&h->radii[i], st.data() + 8 + 12 * (size_t)i, 8);
+        }
+    } else if (file_type == 1) {
+        std::string st;
+        if (!slurp(dir + "/cnt_struct.csv", st))
+            return fail("Error in Read_cnt_data_from_csv: Failed to open CNT structure file cnt_struct.csv.");
+        const char* p = st.data();
+        const char* e = p + st.size();
+        double v[2];
+        if (!parse_line(p, e, 2, v)) return fail("Error in Read_cnt_data_from_csv. cnt_struct.csv is empty.");
+        if ((int64_t)v[0] != (int64_t)v[1])
+            return fail("Error in Read_cnt_data_from_csv. The first line of file cnt_struct.csv indicates different number of CNTs: " +
+                        std::to_string((int64_t)v[0]) + " and " + std::to_string((int64_t)v[1]));
+        const int32_t n = (int32_t)v[0];
+        np.resize(std::max(n, 0));
+        h->radii.resize(np.size());
+        for (int32_t i = 0; i < n; i++) {
+            if (!parse_line(p, e, 2, v))
+                return fail("Error in Read_cnt_data_from_csv. The end-of-file of cnt_struct.csv has been reached before reading all CNT data.");
+            np[i] = (int32_t)v[0];
+            h->radii[i] = v[1];
+        }
+    } else {
+        return fail("Error in Generate_nanoparticle_network_from_file. Invalid file type to read CNT network from. Valid options are 'csv' or 'dat' only.");
+    }
+    const int32_t n = (int32_t)np.size();
+    h->structure_ptr.assign(n + 1, 0);
+    for (int32_t i = 0; i < n; i++) {
+        if (np[i] < 0) return fail("Error in Read_cnt_data: CNT " + std::to_string(i) + " has a negative number of points");
+        h->structure_ptr[i + 1] = h->structure_ptr[i] + np[i];
+    }
+    const int64_t N = h->structure_ptr[n];
+    h->x.resize(N); h->y.resize(N); h->z.resize(N); h->flag.resize(N); h->structure_idx.resize(N);
+    for (int32_t i = 0; i < n; i++)
+        for (int64_t q = h->structure_ptr[i]; q < h->structure_ptr[i + 1]; q++) {
+            h->flag[q] = i;
+            h->structure_idx[q] = q;
+        }
+    if (file_type == 0) {
+        std::string co;
+        if (!slurp(dir + "/cnt_coordinates.dat", co)) return fail("Failed to open point cordinates file cnt_coordinates.dat.");
+        if (co.size() < 24 * (size_t)N)
+            return fail("Error in Read_cnt_data_from_dat. The end-of-file of cnt_coordinates.dat has been reached before reading all CNT data.");
+        for (int64_t q = 0; q < N; q++) {
+            std::memcpy(&h->x[q], co.data() + 24 * q, 8);
+            std::memcpy(&h->y[q], co.data() + 24 * q + 8, 8);
+            std::memcpy(&h->z[q], co.data() + 24 * q + 16, 8);
+        }
+    } else {
+        std::string co;
+        if (!slurp(dir + "/cnt_coordinates.csv", co)) return fail("Failed to open point cordinates file cnt_coordinates.csv.");
+        const char* p = co.data();
+        const char* e = p + co.size();
+        for (int64_t q = 0; q < N; q++) {
+            double v[3];
+            if (!parse_line(p, e, 3, v))
+                return fail("Error in Read_cnt_data_from_csv. The end-of-file of cnt_coordinates.csv has been reached before reading all CNT data.");
+            h->x[q] = v[0];
+            h->y[q] = v[1];
+            h->z[q] = v[2];
+        }
+    }
+    h->boundary_cnt_ptr.assign(7, 0);
+    h->boundary_pts_ptr.assign(7, 0);
     *out = h;
     return CICY_OK;
 }

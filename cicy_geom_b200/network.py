@@ -198,6 +198,15 @@ class HostNetwork:
         return HostNetwork(out.value)
 
 
+def read_network_files(directory: str, file_type: str = "dat") -> HostNetwork:
+    """The network Read_Network reads from `directory` (cicy_read_network): sample_geom.csv
+    and cnt_struct/cnt_coordinates in the binary ("dat") or CSV ("csv") format."""
+    ft = {"dat": 0, "csv": 1}[file_type]
+    out = C.c_void_p()
+    check(lib().cicy_read_network(directory.encode(), ft, C.byref(out)), "cicy_read_network")
+    return HostNetwork(out.value)
+
+
 def generate_cnt_network(cfg: NetworkConfig) -> HostNetwork:
     """Seeded synthetic CNT network (cicy_generate_cnt_network)."""
     g = _abi.GenParams()
@@ -215,37 +224,48 @@ def generate_cnt_network(cfg: NetworkConfig) -> HostNetwork:
     return HostNetwork(out.value)
 
 
-def write_read_network_files(directory: str, net: HostNetwork, cfg: NetworkConfig) -> None:
-    """Write input.dat, sample_geom.csv, cnt_struct.dat and cnt_coordinates.dat.
+def write_read_network_files(directory: str, net: HostNetwork, cfg: NetworkConfig, file_type: str = "dat") -> None:
+    """Write input.dat, sample_geom.csv and the CNT files Read_Network reads.
 
-    Binary layout as Read_Network::Read_cnt_data_from_dat reads it
+    file_type "dat": binary layout of Read_Network::Read_cnt_data_from_dat
     (Read_Network.cpp:348-467): cnt_struct.dat = int n_cnts, then per CNT
     {int n_points; double radius}; cnt_coordinates.dat = x, y, z doubles per
-    point in CNT order.
+    point in CNT order.  "csv": Read_cnt_data_from_csv (:203-346):
+    cnt_struct.csv = "n_cnts,n_cnts", then "n_points,radius" per CNT;
+    cnt_coordinates.csv = "x,y,z" per point (shortest round-trip decimals).
     """
     os.makedirs(directory, exist_ok=True)
     a = net.arrays()
     sp = a["structure_ptr"]
     counts = np.diff(sp).astype(np.int32)
-    rec = np.zeros(len(counts), dtype=np.dtype([("np", "<i4"), ("r", "<f8")], align=False))
-    rec["np"] = counts
-    rec["r"] = a["radii"]
-    with open(os.path.join(directory, "cnt_struct.dat"), "wb") as f:
-        f.write(np.int32(len(counts)).tobytes())
-        f.write(rec.tobytes())
     idx = a["structure_idx"]
     xyz = np.stack([a["x"][idx], a["y"][idx], a["z"][idx]], axis=1).astype("<f8")
-    with open(os.path.join(directory, "cnt_coordinates.dat"), "wb") as f:
-        f.write(xyz.tobytes())
+    if file_type == "dat":
+        rec = np.zeros(len(counts), dtype=np.dtype([("np", "<i4"), ("r", "<f8")], align=False))
+        rec["np"] = counts
+        rec["r"] = a["radii"]
+        with open(os.path.join(directory, "cnt_struct.dat"), "wb") as f:
+            f.write(np.int32(len(counts)).tobytes())
+            f.write(rec.tobytes())
+        with open(os.path.join(directory, "cnt_coordinates.dat"), "wb") as f:
+            f.write(xyz.tobytes())
+    elif file_type == "csv":
+        with open(os.path.join(directory, "cnt_struct.csv"), "w") as f:
+            f.write(f"{len(counts)},{len(counts)}\n")
+            f.write("".join(f"{int(c)},{float(r)!r}\n" for c, r in zip(counts, a["radii"])))
+        with open(os.path.join(directory, "cnt_coordinates.csv"), "w") as f:
+            f.write("".join(f"{float(x)!r},{float(y)!r},{float(z)!r}\n" for x, y, z in xyz))
+    else:
+        raise ValueError("file_type: 'dat' or 'csv'")
     s = cfg.side
     with open(os.path.join(directory, "sample_geom.csv"), "w") as f:
         f.write(f"0,0,0\n{s!r},{s!r},{s!r}\n")
     with open(os.path.join(directory, "input.dat"), "w") as f:
-        f.write(input_dat(cfg))
+        f.write(input_dat(cfg, file_type))
 
 
-def input_dat(cfg: NetworkConfig) -> str:
-    """An upstream input.dat for a single-window Read_Network run of `cfg`."""
+def input_dat(cfg: NetworkConfig, file_type: str = "dat") -> str:
+    """An upstream input.dat for a single-window Read_Network run of `cfg` (CNT files in `file_type`)."""
     s = repr(float(cfg.side))
     r = cfg.resistances
     if cfg.junction == "exponential":
@@ -260,7 +280,7 @@ Synthetic
 1
 CNT_wires
 Read_Network
-dat
+{file_type}
 vol 0.01
 1
 {scope}

@@ -364,6 +364,14 @@ typedef struct {
 } cicy_window_params;
 cicy_status cicy_extract_window(const cicy_host_network* in, const cicy_window_params* w, cicy_host_network** out);
 
+/* Read_Network::Generate_nanoparticle_network_from_file, CNT branch
+ * (Read_sample_geometry + Read_cnt_data_from_dat / Read_cnt_data_from_csv,
+ * Read_Network.cpp:154-467): sample_geom.csv and cnt_struct / cnt_coordinates
+ * (.dat when file_type = 0, .csv when 1) of `directory`, read whole and parsed
+ * in memory, into the layout the generator emits (window = the sample).  The
+ * upstream error cases return CICY_E_INPUT with the upstream message
+ * (cicy_host_last_error).  GNP files are not read. */
+cicy_status cicy_read_network(const char* directory, int32_t file_type, cicy_host_network** out);
 /* Wrap caller-owned arrays (copied) as a host network, e.g. a network read from files. */
 cicy_status cicy_host_network_from_arrays(const cicy_network* net, cicy_host_network** out);
 /* Borrowed view of a host network; valid until cicy_host_network_free. */
