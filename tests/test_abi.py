@@ -18,6 +18,10 @@ def test_struct_sizes_match_header_layout():
     assert C.sizeof(_abi.Params) == 8 * 3 + 8 * 4 + 4 * 6 + 8 * 8
     assert C.sizeof(_abi.SolveInfo) == 4 * 2 + 8 * 6 + 4 * 4
     assert C.sizeof(_abi.Result) == 8 * 6 + 8 * 2 + 4 * 4 + 32 * C.sizeof(_abi.SolveInfo) + 8 * 6
+    # cicy_batch_system: n, nnz; 6 pointers; n_chains (+4 padding); 3 pointers (chains, edge weights)
+    assert C.sizeof(_abi.BatchSystem) == 4 * 2 + 8 * 6 + 8 + 8 * 3
+    # cicy_gnn_system: n, nnz; 3 pointers; n_chains (+4 padding); 2 pointers
+    assert C.sizeof(_abi.GnnSystem) == 4 * 2 + 8 * 3 + 8 + 8 * 2
 
 
 def test_context_creation_without_gpu_fails_cleanly():
