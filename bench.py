@@ -424,6 +424,60 @@ def spmv_roofline(ctx, device, hbm, target_bytes=320e6, reps=20):
             "traffic": None}
 
 
+MC_REF_SAMPLE = range(8, 16)  # realisations timed with the upstream program (~45 s of single-core work)
+
+
+def mc_reference_sample(cfgs, device_seconds, cores=None, timeout=900):
+    """Upstream program (oracle/_ref/ref_dump, hot path: grid + HK + electrical)
+    on a fixed sample of the Monte-Carlo realisations, one process per host core,
+    against this library's per-network device time of the same realisations."""
+    from cicy_geom_b200.network import generate_cnt_network, write_read_network_files
+
+    if not os.path.exists(REF_BIN):
+        return None
+    sample = [cfgs[k] for k in MC_REF_SAMPLE if k < len(cfgs)]
+    cores = min(cores or os.cpu_count() or 1, len(sample))
+    os.makedirs(os.path.join(ROOT, "_scratch"), exist_ok=True)
+    with tempfile.TemporaryDirectory(dir=os.path.join(ROOT, "_scratch")) as base:
+        dirs = []
+        for c in sample:
+            d = os.path.join(base, str(c.seed))
+            os.makedirs(d)
+            write_read_network_files(d, generate_cnt_network(c), c)
+            dirs.append(d)
+        hot, pending, running = {}, list(zip(sample, dirs)), []
+        t0 = time.perf_counter()
+        while pending or running:
+            while pending and len(running) < cores:
+                c, d = pending.pop(0)
+                running.append((c, subprocess.Popen([REF_BIN, "time", d], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)))
+            time.sleep(0.05)
+            for item in list(running):
+                c, p = item
+                if p.poll() is not None:
+                    running.remove(item)
+                    try:
+                        hot[c.seed] = json.loads(p.stdout.read().strip().splitlines()[-1])["hot_s"]
+                    except Exception:
+                        hot[c.seed] = float("nan")
+            if time.perf_counter() - t0 > timeout:
+                for _, p in running:
+                    p.kill()
+                return None
+        wall = time.perf_counter() - t0
+    seeds = [c.seed for c in sample]
+    ref_sum = sum(hot[s] for s in seeds)
+    dev = [device_seconds.get(s) for s in seeds]
+    ours = sum(dev) if all(v is not None for v in dev) else None
+    return {"kind": "reference", "cores": cores, "realisations": seeds, "reference_hot_seconds": [hot[s] for s in seeds],
+            "reference_networks_per_s_per_core": len(seeds) / ref_sum, "reference_networks_per_s": len(seeds) / wall,
+            "reference_wall_seconds": wall, "ours_device_seconds": dev,
+            "ours_networks_per_s": len(seeds) / ours if ours else None,
+            "sample": f"realisations {MC_REF_SAMPLE.start}-{MC_REF_SAMPLE.stop - 1} of the sweep (seeds {seeds[0]}-{seeds[-1]}), "
+                      f"whole hot path per network; upstream: one process per host core ({cores}); ours: the per-network device "
+                      f"path, one network after another on one GPU (cicy_result.stage_seconds total)"}
+
+
 def batched_monte_carlo(count, device, reps=3):
     """Monte-Carlo sweep: `count` seeded realisations (cube side U[2,5] um, CNT
     volume fraction U[0.5%,3%]), each run through the device path to its
@@ -480,7 +534,12 @@ def batched_monte_carlo(count, device, reps=3):
         out[k]["speedup_vs_jacobi"] = jac / out[k]["seconds"]
     seq = sum(s["seconds_ref"] for s in systems)
     n = [s["A"].shape[0] for s in systems]
+    dev = info.pop("device_seconds", {})
+    ref = mc_reference_sample(cfgs, dev)
     return {"realisations": count, **info, "systems": ns, "unknowns_total": int(sum(n)), "unknowns_max": int(max(n)), **out,
+            "per_network_pipeline": {"networks_per_s_device": len(dev) / sum(dev.values()) if dev else None,
+                                     "realisations": len(dev), "device_seconds_total": sum(dev.values()) if dev else None},
+            "cpu_baseline_sample": ref,
             "gnn_forward_seconds": bs.gnn_seconds, "multigrid_setup_seconds": setup,
             "multigrid_sequential_solve_seconds": seq, "multigrid_speedup_vs_sequential": seq / out["multigrid"]["seconds"],
             "generation_and_assembly_seconds": prep,

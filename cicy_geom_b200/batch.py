@@ -35,12 +35,14 @@ def realisation_systems(configs, device: int = 0, preconditioner: int = 3):
     Returns (systems, info): systems are dicts with the full CSR (host), chains,
     right-hand side, initial guess and the per-network solver's solution and
     time; info counts the realisations that do not percolate (their resistance
-    is the matrix resistance, no system to solve)."""
+    is the matrix resistance, no system to solve) and holds each realisation's
+    device time of the whole hot path by seed ("device_seconds")."""
     from .device import Context
     from .learned import full_csr
     from .network import generate_cnt_network
 
     systems, info = [], {"realisations": len(configs), "percolating": 0, "not_percolating": 0, "rejected": 0}
+    device_seconds = {}  # seed -> device time of the whole hot path (cicy_result.stage_seconds[5])
     for cfg in configs:
         net = generate_cnt_network(cfg).extract_window(cfg)
         ctx = Context(device)
@@ -52,6 +54,7 @@ def realisation_systems(configs, device: int = 0, preconditioner: int = 3):
             info["rejected"] += 1
             ctx.close()
             continue
+        device_seconds[cfg.seed] = float(r.stage_seconds[5])
         real = [i for i in range(r.n_solves) if r.solves[i].pass_ >= 0]
         if not real:
             info["not_percolating"] += 1
@@ -66,6 +69,7 @@ def realisation_systems(configs, device: int = 0, preconditioner: int = 3):
                             "x_ref": S["voltages"][S["reserved"]:], "seconds_ref": r.solves[i].seconds,
                             "iterations_ref": r.solves[i].iterations, "seed": cfg.seed})
         ctx.close()
+    info["device_seconds"] = device_seconds
     return systems, info
 
 
