@@ -676,13 +676,25 @@ def run_ours(args):
                                    for k, v in per_kernel.items()}},
             "R_x": R[0],
         }
+        # the measured step above is the result; a failing extra section is recorded, not fatal
+        def extra(key, fn):
+            try:
+                line[key] = fn()
+            except Exception as e:  # noqa: BLE001
+                line[key] = {"error": f"{type(e).__name__}: {e}"}
+                print(f"bench: {key} failed: {e}", file=sys.stderr)
+
         if not args.no_comparison and world == 1:
-            line["solver_comparison"] = solver_comparison(cfg, net, local)
-            line["spmv"] = spmv_roofline(ctx, local, hbm)
+            extra("solver_comparison", lambda: solver_comparison(cfg, net, local))
+            extra("spmv", lambda: spmv_roofline(ctx, local, hbm))
         if args.mc > 0 and world == 1:
-            line["batched_monte_carlo"] = batched_monte_carlo(args.mc, local)
+            extra("batched_monte_carlo", lambda: batched_monte_carlo(args.mc, local))
         if not args.no_cpu_baseline and world == 1:
-            cb = cpu_baseline_reference(cfg, raw)
+            cb = None
+            try:
+                cb = cpu_baseline_reference(cfg, raw)
+            except Exception as e:  # noqa: BLE001
+                print(f"bench: cpu_baseline failed: {e}", file=sys.stderr)
             if cb:
                 line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
                 line["R_x_reference"] = cb["R"][0]
