@@ -286,7 +286,8 @@ __global__ void k_ew_apply(int n, const int32_t* __restrict__ rp, const int32_t*
     }
 }
 
-__global__ void k_axpy(int n, double a, const double* __restrict__ x, const double* __restrict__ y, double* __restrict__ out) {
+// out = a x + y; out may be y (in-place updates), so neither is restrict-qualified.
+__global__ void k_axpy(int n, double a, const double* __restrict__ x, const double* y, double* out) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = a * x[i] + y[i];
 }
 

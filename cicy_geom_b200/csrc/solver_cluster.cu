@@ -214,38 +214,7 @@ __host__ __device__ inline size_t smem_layout(int nr, int nnz, int nb, int h, in
     return off;
 }
 
-// Block partial -> every CTA's slot[rank] -> cluster barrier -> sum of slots in rank order.
-__device__ __forceinline__ double2 cluster_sum2(cg::cluster_group& cl, double* slot, int nval, double a, double b, double* red,
-                                                int C, unsigned rank) {
-    a = warp_sum(a);
-    b = warp_sum(b);
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    if (lane == 0) { red[w] = a; red[32 + w] = b; }
-    __syncthreads();
-    if (w == 0) {  // warp 0: block total by shuffles, then one store per destination CTA
-        double s0 = lane < nw ? red[lane] : 0.0, s1 = lane < nw ? red[32 + lane] : 0.0;
-        s0 = warp_sum(s0);
-        s1 = warp_sum(s1);
-        s0 = __shfl_sync(0xffffffffu, s0, 0);
-        s1 = __shfl_sync(0xffffffffu, s1, 0);
-        if (lane < C) {
-            double* dst = cl.map_shared_rank(slot, lane);
-            dst[nval * rank] = s0;
-            if (nval > 1) dst[nval * rank + 1] = s1;
-        }
-    }
-    cl.sync();
-    // every warp sums the C slots in rank order with shuffles (same order everywhere)
-    double s0 = lane < C ? slot[nval * lane] : 0.0;
-    double s1 = (nval > 1 && lane < C) ? slot[nval * lane + 1] : 0.0;
-    s0 = warp_sum(s0);
-    s1 = warp_sum(s1);
-    s0 = __shfl_sync(0xffffffffu, s0, 0);
-    s1 = __shfl_sync(0xffffffffu, s1, 0);
-    return make_double2(s0, s1);
-}
-
-// Split form of cluster_sum2: store the block partials into every CTA's slots ...
+// Cluster-wide sum, split in two: store the block partials into every CTA's slots ...
 __device__ __forceinline__ void cluster_store2(cg::cluster_group& cl, double* slot, double a, double b, double* red, int C,
                                                unsigned rank) {
     a = warp_sum(a);
