@@ -338,7 +338,8 @@ def solve_cg(S, tol):
     for k in range(1, 300 * S["nodes"] + 1):
         ap = A @ pvec
         rr0 = y @ r
-        alpha = rr0 / (pvec @ ap)
+        with np.errstate(invalid="ignore", divide="ignore"):  # upstream's 0/0 on a zero initial residual gives NaN
+            alpha = rr0 / (pvec @ ap)
         x += alpha * pvec
         r -= alpha * ap
         if math.sqrt(r @ r) <= R0:
@@ -475,7 +476,8 @@ def network_to_conductance(net: dict, p: dict, solver: str = "cg") -> dict:
             out["systems"].append((d, k, S2))
             b1 = [2, 3, 0][d]
             I = boundary_current(net, p, [int(c) for c in bidx[bptr[b1]:bptr[b1 + 1]]], elems, S2["lmm"], v2)
-            parallel[d].append(p["V"] / I)
+            with np.errstate(divide="ignore", invalid="ignore"):  # a zero current gives upstream's inf / nan R
+                parallel[d].append(p["V"] / I)
     w = net["window"]
     L = [w[3], w[4], w[5]]
     A = [w[4] * w[5], w[3] * w[5], w[3] * w[4]]
