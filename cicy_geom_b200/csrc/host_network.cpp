@@ -518,16 +518,48 @@ cicy_status read_network_files(const std::string& dir, int file_type, HostNetwor
     } else {
         std::string co;
         if (!slurp(dir + "/cnt_coordinates.csv", co)) return fail("Failed to open point cordinates file cnt_coordinates.csv.");
-        const char* p = co.data();
-        const char* e = p + co.size();
-        for (int64_t q = 0; q < N; q++) {
-            double v[3];
-            if (!parse_line(p, e, 3, v))
-                return fail("Error in Read_cnt_data_from_csv. The end-of-file of cnt_coordinates.csv has been reached before reading all CNT data.");
-            h->x[q] = v[0];
-            h->y[q] = v[1];
-            h->z[q] = v[2];
+        // lines are independent: split the text at line ends, count the lines of each
+        // piece, and parse the pieces on host threads into their point ranges
+        const char* text0 = co.data();
+        const size_t len = co.size();
+        const unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+        std::vector<size_t> cut(nt + 1, len);
+        cut[0] = 0;
+        for (unsigned t = 1; t < nt; t++) {
+            size_t c = std::max(cut[t - 1], len * t / nt);
+            while (c > 0 && c < len && text0[c - 1] != '\n') c++;
+            cut[t] = c;
         }
+        std::vector<int64_t> lines(nt + 1, 0);
+        for (unsigned t = 0; t < nt; t++) {
+            int64_t k = 0;
+            for (size_t c = cut[t]; c < cut[t + 1]; c++) k += text0[c] == '\n';
+            if (cut[t + 1] > cut[t] && text0[cut[t + 1] - 1] != '\n') k++;  // a last line without its newline
+            lines[t + 1] = lines[t] + k;
+        }
+        if (lines[nt] < N)
+            return fail("Error in Read_cnt_data_from_csv. The end-of-file of cnt_coordinates.csv has been reached before reading all CNT data.");
+        std::vector<int> bad(nt, 0);
+        auto work = [&](unsigned t) {
+            const char* p = text0 + cut[t];
+            const char* e = text0 + cut[t + 1];
+            for (int64_t q = lines[t]; q < std::min(lines[t + 1], N); q++) {
+                double v[3];
+                if (!parse_line(p, e, 3, v)) {
+                    bad[t] = 1;
+                    return;
+                }
+                h->x[q] = v[0];
+                h->y[q] = v[1];
+                h->z[q] = v[2];
+            }
+        };
+        std::vector<std::thread> th;
+        for (unsigned t = 1; t < nt; t++) th.emplace_back(work, t);
+        work(0);
+        for (auto& t : th) t.join();
+        for (unsigned t = 0; t < nt; t++)
+            if (bad[t]) return fail("Error in Read_cnt_data_from_csv: a line of cnt_coordinates.csv is not x,y,z");
     }
     h->boundary_cnt_ptr.assign(7, 0);
     h->boundary_pts_ptr.assign(7, 0);

@@ -370,7 +370,9 @@ cicy_status cicy_extract_window(const cicy_host_network* in, const cicy_window_p
  * (.dat when file_type = 0, .csv when 1) of `directory`, read whole and parsed
  * in memory, into the layout the generator emits (window = the sample).  The
  * upstream error cases return CICY_E_INPUT with the upstream message
- * (cicy_host_last_error).  GNP files are not read. */
+ * (cicy_host_last_error); so does a CSV line that does not hold its numbers
+ * (upstream would read it as zeros and shift the points after it).  CSV
+ * coordinates are parsed on host threads.  GNP files are not read. */
 cicy_status cicy_read_network(const char* directory, int32_t file_type, cicy_host_network** out);
 /* Wrap caller-owned arrays (copied) as a host network, e.g. a network read from files. */
 cicy_status cicy_host_network_from_arrays(const cicy_network* net, cicy_host_network** out);
