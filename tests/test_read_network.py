@@ -79,3 +79,25 @@ def test_csv_reader_and_window_match_upstream(tmp_path):
     assert np.array_equal(z["cnts_inside"], w["cnts_inside"])
     assert np.array_equal(z["boundary_cnt_ptr"], w["boundary_cnt_ptr"]) and np.array_equal(z["boundary_cnt_idx"], w["boundary_cnt_idx"])
     assert np.array_equal(z["boundary_pts_ptr"], w["boundary_pts_ptr"]) and np.array_equal(z["boundary_pts_idx"], w["boundary_pts_idx"])
+
+
+@pytest.mark.parametrize("n", [1, 3, 40])
+def test_csv_edge_cases(tmp_path, n):
+    """Tiny files (fewer lines than parsing threads), no final newline, a missing
+    point, and a line without its numbers."""
+    cfg, raw = small(seed=5, n=n)
+    d = str(tmp_path)
+    write_read_network_files(d, raw, cfg, "csv")
+    a = raw.arrays()
+    path = os.path.join(d, "cnt_coordinates.csv")
+    text = open(path).read()
+    open(path, "w").write(text.rstrip("\n"))
+    b = read_network_files(d, "csv").arrays()
+    for k in ("x", "y", "z", "flag", "structure_ptr"):
+        assert np.array_equal(a[k], b[k]), k
+    open(path, "w").write("\n".join(text.splitlines()[:-1]) + "\n")
+    with pytest.raises(_abi.CicyError, match="end-of-file of cnt_coordinates.csv"):
+        read_network_files(d, "csv")
+    open(path, "w").write(text.replace("\n", "\n\n", 1))
+    with pytest.raises(_abi.CicyError, match="not x,y,z"):
+        read_network_files(d, "csv")
