@@ -144,6 +144,18 @@ class BatchSystem(C.Structure):
     ]
 
 
+class Gnps(C.Structure):
+    _fields_ = [
+        ("n", C.c_int32),
+        ("l", C.c_void_p),
+        ("t", C.c_void_p),
+        ("center", C.c_void_p),
+        ("rotation", C.c_void_p),
+        ("vertices", C.c_void_p),
+        ("planes", C.c_void_p),
+    ]
+
+
 class GenParams(C.Structure):
     _fields_ = [
         ("sample", Cuboid),
@@ -206,6 +218,9 @@ def lib() -> C.CDLL:
         "cicy_extract_window": (C.c_int, [C.c_void_p, P(WindowParams), P(C.c_void_p)]),
         "cicy_host_network_from_arrays": (C.c_int, [P(Network), P(C.c_void_p)]),
         "cicy_read_network": (C.c_int, [C.c_char_p, C.c_int32, P(C.c_void_p)]),
+        "cicy_read_gnps": (C.c_int, [C.c_char_p, P(C.c_void_p)]),
+        "cicy_gnp_set_view": (C.c_int, [C.c_void_p, P(Gnps)]),
+        "cicy_gnp_set_free": (None, [C.c_void_p]),
         "cicy_host_network_view": (C.c_int, [C.c_void_p, P(Network)]),
         "cicy_host_network_free": (None, [C.c_void_p]),
         "cicy_host_last_error": (C.c_char_p, []),

@@ -49,6 +49,37 @@ cicy_status cicy_read_network(const char* directory, int32_t file_type, cicy_hos
     return CICY_OK;
 }
 
+struct cicy_gnp_set {
+    cicy::GnpSet g;
+};
+
+cicy_status cicy_read_gnps(const char* directory, cicy_gnp_set** out) {
+    if (!directory || !out) return CICY_E_INPUT;
+    cicy::GnpSet* g = nullptr;
+    cicy_status s = cicy::read_gnp_file(directory, &g, g_host_error);
+    if (s != CICY_OK) return s;
+    cicy_gnp_set* w = new cicy_gnp_set;
+    w->g = std::move(*g);
+    delete g;
+    *out = w;
+    return CICY_OK;
+}
+
+cicy_status cicy_gnp_set_view(const cicy_gnp_set* set, cicy_gnps* view) {
+    if (!set || !view) return CICY_E_INPUT;
+    const cicy::GnpSet& g = set->g;
+    view->n = g.n;
+    view->l = g.l.data();
+    view->t = g.t.data();
+    view->center = g.center.data();
+    view->rotation = g.rotation.data();
+    view->vertices = g.vertices.data();
+    view->planes = g.planes.data();
+    return CICY_OK;
+}
+
+void cicy_gnp_set_free(cicy_gnp_set* set) { delete set; }
+
 cicy_status cicy_host_network_from_arrays(const cicy_network* n, cicy_host_network** out) {
     if (!n || !out || n->n_points < 0 || n->n_cnts < 0 || !n->structure_ptr) return CICY_E_INPUT;
     cicy::HostNetwork* h = cicy::host_network_from_view(*n);

@@ -28,6 +28,13 @@ HostNetwork* generate_cnt_network(const cicy_gen_params& g);
 cicy_status extract_window(const HostNetwork& in, const cicy_window_params& w, HostNetwork** out, std::string& err);
 HostNetwork* host_network_from_view(const cicy_network& n);
 cicy_status read_network_files(const std::string& dir, int file_type, HostNetwork** out, std::string& err);
+
+// GNPs of a gnp_data.dat with their upstream vertices and face planes.
+struct GnpSet {
+    int32_t n = 0;
+    std::vector<double> l, t, center, rotation, vertices, planes;  // per GNP: 1, 1, 3, 9, 24, 24
+};
+cicy_status read_gnp_file(const std::string& dir, GnpSet** out, std::string& err);
 // Message returned by cicy_host_last_error() on this thread.
 void set_host_error(const std::string& msg);
 void host_network_view(const HostNetwork& h, cicy_network& v);

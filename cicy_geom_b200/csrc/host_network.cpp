@@ -567,6 +567,94 @@ cicy_status read_network_files(const std::string& dir, int file_type, HostNetwor
     return CICY_OK;
 }
 
+// ---------------------------------------------------------------------------
+// GNPs as Read_Network::Read_gnp_data_from_dat builds them (Read_Network.cpp:576-679):
+// rotation matrix Generate_Network::Get_transformation_matrix (Generate_Network.cpp:3466-3480),
+// vertices Obtain_gnp_vertex_coordinates (:3848-3867) through Point_3D::rotation
+// (Geometry_3D.cpp:147-165), face planes Update_gnp_plane_equations (:3869-3889) through
+// Plane_3D(P1, P2, P3) (Geometry_3D.cpp: normal (P2-P1) x (P3-P1), made unit, offset
+// -N.P1).  Same operation order as upstream, so the doubles are identical (host code,
+// no FMA contraction).
+namespace {
+
+struct V3 {
+    double x, y, z;
+};
+
+V3 rotate(const double* M, const V3& p, const V3& d) {
+    return V3{M[0] * p.x + M[1] * p.y + M[2] * p.z + d.x, M[3] * p.x + M[4] * p.y + M[5] * p.z + d.y,
+              M[6] * p.x + M[7] * p.y + M[8] * p.z + d.z};
+}
+
+void plane(const V3& P1, const V3& P2, const V3& P3, double* out) {
+    const V3 u{P2.x - P1.x, P2.y - P1.y, P2.z - P1.z}, w{P3.x - P1.x, P3.y - P1.y, P3.z - P1.z};
+    double a = u.y * w.z - w.y * u.z;
+    double b = -(u.x * w.z - w.x * u.z);
+    double c = u.x * w.y - w.x * u.y;
+    const double len = std::sqrt(a * a + b * b + c * c);
+    a = a / len;
+    b = b / len;
+    c = c / len;
+    out[0] = a;
+    out[1] = b;
+    out[2] = c;
+    out[3] = (a * P1.x + b * P1.y + c * P1.z) * (-1);
+}
+
+}  // namespace
+
+cicy_status read_gnp_file(const std::string& dir, GnpSet** out, std::string& err) {
+    std::string st;
+    if (!slurp(dir + "/gnp_data.dat", st)) {
+        err = "Failed to open file with GNP geometric data gnp_data.dat.";
+        return CICY_E_INPUT;
+    }
+    int32_t n = 0;
+    if (st.size() >= 4) std::memcpy(&n, st.data(), 4);
+    if (st.size() < 4 || n < 0 || st.size() < 4 + 56 * (size_t)n) {
+        err = "Error in Read_gnp_data_from_dat. The end-of-file of gnp_data.dat has been reached before reading all GNP data.";
+        return CICY_E_INPUT;
+    }
+    GnpSet* g = new GnpSet;
+    g->n = n;
+    g->l.resize(n); g->t.resize(n); g->center.resize(3 * (size_t)n); g->rotation.resize(9 * (size_t)n);
+    g->vertices.resize(24 * (size_t)n); g->planes.resize(24 * (size_t)n);
+    for (int32_t i = 0; i < n; i++) {
+        double r[7];
+        std::memcpy(r, st.data() + 4 + 56 * (size_t)i, 56);
+        const double l = r[0], t = r[1], theta = r[2], phi = r[3];
+        g->l[i] = l;
+        g->t[i] = t;
+        double* M = &g->rotation[9 * (size_t)i];
+        M[0] = std::cos(phi) * std::cos(theta);
+        M[1] = -std::sin(phi);
+        M[2] = std::cos(phi) * std::sin(theta);
+        M[3] = std::sin(phi) * std::cos(theta);
+        M[4] = std::cos(phi);
+        M[5] = std::sin(phi) * std::sin(theta);
+        M[6] = -std::sin(theta);
+        M[7] = 0.0;
+        M[8] = std::cos(theta);
+        const V3 c{r[4], r[5], r[6]};
+        g->center[3 * (size_t)i] = c.x;
+        g->center[3 * (size_t)i + 1] = c.y;
+        g->center[3 * (size_t)i + 2] = c.z;
+        const V3 loc[8] = {{l / 2, l / 2, t / 2},   {-l / 2, l / 2, t / 2},   {-l / 2, -l / 2, t / 2},   {l / 2, -l / 2, t / 2},
+                           {l / 2, l / 2, -t / 2},  {-l / 2, l / 2, -t / 2},  {-l / 2, -l / 2, -t / 2},  {l / 2, -l / 2, -t / 2}};
+        V3 v[8];
+        for (int k = 0; k < 8; k++) {
+            v[k] = rotate(M, loc[k], c);
+            g->vertices[24 * (size_t)i + 3 * k] = v[k].x;
+            g->vertices[24 * (size_t)i + 3 * k + 1] = v[k].y;
+            g->vertices[24 * (size_t)i + 3 * k + 2] = v[k].z;
+        }
+        static const int F[6][3] = {{0, 1, 3}, {4, 7, 5}, {0, 3, 4}, {0, 4, 1}, {1, 5, 2}, {2, 6, 3}};
+        for (int f = 0; f < 6; f++) plane(v[F[f][0]], v[F[f][1]], v[F[f][2]], &g->planes[24 * (size_t)i + 4 * f]);
+    }
+    *out = g;
+    return CICY_OK;
+}
+
 HostNetwork* host_network_from_view(const cicy_network& n) {
     HostNetwork* h = new HostNetwork;
     h->x.assign(n.x, n.x + n.n_points);

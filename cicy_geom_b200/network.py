@@ -320,3 +320,55 @@ Output_Data_Flags
 0
 0
 """
+
+
+# ---------------------------------------------------------------------------
+# GNPs (graphene nanoplatelets): seeded generation and the Read_Network file
+
+
+def generate_gnps(n: int, side: float, seed: int, l_range=(0.5, 1.0), thickness: float = 0.01) -> dict:
+    """Seeded GNPs for a cube of `side` um (the hybrid configuration's distribution):
+    square side U[l_range], thickness `thickness`, centre uniform in the cube,
+    normal uniform on the sphere, stored as the (theta, phi) of the normal that
+    gnp_data.dat holds (Read_Network.cpp:576-679: the rotation matrix's third
+    column is the normal)."""
+    rng = np.random.default_rng(seed)
+    return {"l": rng.uniform(*l_range, n), "t": np.full(n, float(thickness)),
+            "theta": np.arccos(rng.uniform(-1.0, 1.0, n)), "phi": rng.uniform(0.0, 2 * math.pi, n),
+            "center": rng.uniform(0.0, side, (n, 3))}
+
+
+def write_gnp_file(directory: str, gnps: dict) -> None:
+    """gnp_data.dat as Read_Network::Read_gnp_data_from_dat reads it: int n, then per
+    GNP the doubles l, t, theta, phi, centre x, y, z."""
+    os.makedirs(directory, exist_ok=True)
+    n = len(gnps["l"])
+    rec = np.zeros((n, 7), "<f8")
+    rec[:, 0], rec[:, 1], rec[:, 2], rec[:, 3] = gnps["l"], gnps["t"], gnps["theta"], gnps["phi"]
+    rec[:, 4:7] = gnps["center"]
+    with open(os.path.join(directory, "gnp_data.dat"), "wb") as f:
+        f.write(np.int32(n).tobytes())
+        f.write(rec.tobytes())
+
+
+def read_gnps(directory: str) -> dict:
+    """GNPs of `directory`/gnp_data.dat as upstream's Read_Network builds them
+    (cicy_read_gnps): l, t [n]; center [n, 3]; rotation [n, 3, 3]; vertices
+    [n, 8, 3]; planes [n, 6, 4] (normal, offset)."""
+    h = C.c_void_p()
+    check(lib().cicy_read_gnps(directory.encode(), C.byref(h)), "cicy_read_gnps")
+    try:
+        v = _abi.Gnps()
+        check(lib().cicy_gnp_set_view(h, C.byref(v)), "cicy_gnp_set_view")
+        n = v.n
+
+        def arr(ptr, count, shape):
+            if count == 0:
+                return np.zeros(shape)
+            return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_double)), shape=(count,)).copy().reshape(shape)
+
+        return {"l": arr(v.l, n, (n,)), "t": arr(v.t, n, (n,)), "center": arr(v.center, 3 * n, (n, 3)),
+                "rotation": arr(v.rotation, 9 * n, (n, 3, 3)), "vertices": arr(v.vertices, 24 * n, (n, 8, 3)),
+                "planes": arr(v.planes, 24 * n, (n, 6, 4))}
+    finally:
+        lib().cicy_gnp_set_free(h)

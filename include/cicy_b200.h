@@ -374,6 +374,29 @@ cicy_status cicy_extract_window(const cicy_host_network* in, const cicy_window_p
  * (upstream would read it as zeros and shift the points after it).  CSV
  * coordinates are parsed on host threads.  GNP files are not read. */
 cicy_status cicy_read_network(const char* directory, int32_t file_type, cicy_host_network** out);
+/* GNPs (graphene nanoplatelets) of a directory's gnp_data.dat as
+ * Read_Network::Read_gnp_data_from_dat builds them (Read_Network.cpp:576-679):
+ * rotation matrix from the stored (theta, phi) of the normal
+ * (Generate_Network::Get_transformation_matrix), the 8 vertices
+ * (Obtain_gnp_vertex_coordinates) and the 6 face planes
+ * (Update_gnp_plane_equations), in upstream's operation order on the host, so
+ * the doubles equal upstream's.  Input of the GNP contact search (the hybrid
+ * CNT/GNP configuration). */
+typedef struct cicy_gnp_set cicy_gnp_set;
+typedef struct {
+    int32_t n;
+    const double* l;         /* side [n] */
+    const double* t;         /* thickness [n] */
+    const double* center;    /* [3n] */
+    const double* rotation;  /* row-major 3x3 per GNP [9n] */
+    const double* vertices;  /* 8 vertices x (x, y, z) per GNP [24n] */
+    const double* planes;    /* 6 faces x (nx, ny, nz, d) per GNP [24n], n.p + d = 0 on the face */
+} cicy_gnps;
+cicy_status cicy_read_gnps(const char* directory, cicy_gnp_set** out);
+/* Borrowed view; valid until cicy_gnp_set_free. */
+cicy_status cicy_gnp_set_view(const cicy_gnp_set* set, cicy_gnps* view);
+void cicy_gnp_set_free(cicy_gnp_set* set);
+
 /* Wrap caller-owned arrays (copied) as a host network, e.g. a network read from files. */
 cicy_status cicy_host_network_from_arrays(const cicy_network* net, cicy_host_network** out);
 /* Borrowed view of a host network; valid until cicy_host_network_free. */

@@ -1,0 +1,121 @@
+/*
+ * gnp_dump — TEST ORACLE DRIVER (never shipped, never on the product path).
+ *
+ * Links the upstream CICY_geom objects compiled in place by oracle/Makefile
+ * and dumps, for the GNPs of a directory's gnp_data.dat + sample_geom.csv:
+ *   - every GNP as upstream builds it when reading the file
+ *     (Read_Network::Read_gnp_data_from_dat, Read_Network.cpp:576-679):
+ *     side, thickness, centre, rotation matrix, the 8 vertices and the 6 face
+ *     planes (normal and offset);
+ *   - for every candidate pair (a < b whose bounding spheres come within the
+ *     tunnelling cutoff), the upstream GNP-GNP distance step of
+ *     Label_gnps_in_window (Hoshen_Kopelman::Get_distance_between_GNPs,
+ *     Hoshen_Kopelman.cpp:770-823: GJK distance, EPA when the GNPs
+ *     interpenetrate, then the move of GNP b): distance, direction, the
+ *     interpenetration flag and the displacement of b.
+ *
+ *   gnp_dump <dir> <out.bin> <van_der_Waals_dist> <tunneling_dist>
+ *
+ * Output records: u32 name length, name, u8 type ('i' int32, 'd' float64),
+ * u64 count, payload (the layout oracle/dumpio.py reads).
+ */
+#include <cmath>
+#include <cstdio>
+#include <string>
+#include <unistd.h>
+#include <vector>
+
+#include "Hns.h"
+#include "Hoshen_Kopelman.h"
+#include "Input_Reader.h"
+#include "Read_Network.h"
+
+namespace {
+
+struct Out {
+    FILE* f = nullptr;
+    void rec(const std::string& name, char type, const void* data, unsigned long long count, size_t elem) {
+        unsigned n = (unsigned)name.size();
+        fwrite(&n, 4, 1, f);
+        fwrite(name.data(), 1, n, f);
+        fwrite(&type, 1, 1, f);
+        fwrite(&count, 8, 1, f);
+        if (count) fwrite(data, elem, count, f);
+    }
+    void f64(const std::string& name, const std::vector<double>& v) { rec(name, 'd', v.data(), v.size(), 8); }
+    void i32(const std::string& name, const std::vector<int>& v) { rec(name, 'i', v.data(), v.size(), 4); }
+};
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    if (argc < 5) {
+        fprintf(stderr, "usage: gnp_dump <dir> <out.bin> <van_der_Waals_dist> <tunneling_dist>\n");
+        return 1;
+    }
+    const std::string out_path = argv[2];
+    const double vdw = atof(argv[3]), dt = atof(argv[4]);
+    if (chdir(argv[1]) != 0) { fprintf(stderr, "cannot chdir to %s\n", argv[1]); return 2; }
+    open_deffo_stream((char*)"gnp_log.txt");
+    Read_Network RN;
+    Geom_sample geom;
+    if (!RN.Read_sample_geometry(geom)) return 3;
+    std::vector<GNP> gnps;
+    if (!RN.Read_gnp_data_from_dat(geom.sample, gnps)) return 4;
+
+    Out o;
+    o.f = fopen(out_path.c_str(), "wb");
+    if (!o.f) return 5;
+    std::vector<double> lt, center, rot, vert, planes;
+    for (const GNP& g : gnps) {
+        lt.push_back(g.l);
+        lt.push_back(g.t);
+        center.insert(center.end(), {g.center.x, g.center.y, g.center.z});
+        for (int r = 0; r < 3; r++)
+            for (int c = 0; c < 3; c++) rot.push_back(g.rotation.element[r][c]);
+        for (int v = 0; v < 8; v++) vert.insert(vert.end(), {g.vertices[v].x, g.vertices[v].y, g.vertices[v].z});
+        for (int f = 0; f < 6; f++) planes.insert(planes.end(), {g.faces[f].coef[0], g.faces[f].coef[1], g.faces[f].coef[2], g.faces[f].coef[3]});
+    }
+    o.f64("gnp_lt", lt);
+    o.f64("gnp_center", center);
+    o.f64("gnp_rotation", rot);
+    o.f64("gnp_vertices", vert);
+    o.f64("gnp_planes", planes);
+
+    Cutoff_dist cut;
+    cut.van_der_Waals_dist = vdw;
+    cut.tunneling_dist = dt;
+    Hoshen_Kopelman HK;
+    std::vector<int> pa, pb, pflag;
+    std::vector<double> dist, dir, disp;
+    const int n = (int)gnps.size();
+    for (int a = 0; a < n; a++)
+        for (int b = a + 1; b < n; b++) {
+            // bounding spheres (half diagonal of the l x l x t cuboid) within the cutoff
+            const double ra = 0.5 * std::sqrt(2 * gnps[a].l * gnps[a].l + gnps[a].t * gnps[a].t);
+            const double rb = 0.5 * std::sqrt(2 * gnps[b].l * gnps[b].l + gnps[b].t * gnps[b].t);
+            const double dc = std::sqrt((gnps[a].center.x - gnps[b].center.x) * (gnps[a].center.x - gnps[b].center.x) +
+                                        (gnps[a].center.y - gnps[b].center.y) * (gnps[a].center.y - gnps[b].center.y) +
+                                        (gnps[a].center.z - gnps[b].center.z) * (gnps[a].center.z - gnps[b].center.z));
+            if (dc > ra + rb + dt) continue;
+            GNP gnp_B = gnps[b];
+            Point_3D disp_tot(0, 0, 0), N(0, 0, 0);
+            bool p_flag = false;
+            double d = 0;
+            if (!HK.Get_distance_between_GNPs(cut, gnps, a, b, p_flag, disp_tot, N, d, gnp_B)) return 6;
+            pa.push_back(a);
+            pb.push_back(b);
+            pflag.push_back(p_flag ? 1 : 0);
+            dist.push_back(d);
+            dir.insert(dir.end(), {N.x, N.y, N.z});
+            disp.insert(disp.end(), {disp_tot.x, disp_tot.y, disp_tot.z});
+        }
+    o.i32("pair_a", pa);
+    o.i32("pair_b", pb);
+    o.i32("pair_penetrating", pflag);
+    o.f64("pair_dist", dist);
+    o.f64("pair_direction", dir);
+    o.f64("pair_displacement", disp);
+    fclose(o.f);
+    return 0;
+}

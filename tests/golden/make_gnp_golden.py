@@ -1,0 +1,55 @@
+"""Generate tests/golden/gnp_120_s4000000.npz from the upstream program.
+
+Runs oracle/_ref/gnp_dump (upstream CICY_geom objects compiled in place by
+oracle/Makefile) on 120 seeded GNPs in a 2 um cube (side U[0.5, 1.0] um,
+thickness 10 nm, normal uniform on the sphere) and stores, next to the inputs,
+upstream's GNPs as it reads them (rotation, vertices, face planes) and, for
+every candidate pair, upstream's GNP-GNP distance step (GJK distance, EPA when
+the GNPs interpenetrate, the move of the second GNP): the oracle of the GNP
+contact search.  The fixture itself is self-contained.
+
+    python tests/golden/make_gnp_golden.py
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from cicy_geom_b200.network import generate_gnps, write_gnp_file  # noqa: E402
+from oracle.dumpio import read_dump  # noqa: E402
+
+REF = os.path.join(ROOT, "oracle", "_ref", "gnp_dump")
+N, SIDE, SEED = 120, 2.0, 4_000_000
+VDW, TUNNEL = 0.00034, 0.0018  # um, as the CNT configurations
+
+
+def dump(gnps: dict, side: float, directory: str) -> dict:
+    write_gnp_file(directory, gnps)
+    with open(os.path.join(directory, "sample_geom.csv"), "w") as f:
+        f.write(f"0,0,0\n{side!r},{side!r},{side!r}\n")
+    out = os.path.join(directory, "gnp.bin")
+    subprocess.run([REF, directory, out, repr(VDW), repr(TUNNEL)], check=True, capture_output=True, timeout=600)
+    return read_dump(out)
+
+
+def main():
+    g = generate_gnps(N, SIDE, SEED)
+    with tempfile.TemporaryDirectory() as d:
+        z = dump(g, SIDE, d)
+    np.savez_compressed(os.path.join(HERE, f"gnp_{N}_s{SEED}.npz"),
+                        in_l=g["l"], in_t=g["t"], in_theta=g["theta"], in_phi=g["phi"], in_center=g["center"],
+                        meta=np.array([N, SIDE, SEED, VDW, TUNNEL]), **{"ref_" + k: v for k, v in z.items()})
+    print(f"{N} GNPs, {len(z['pair_a'])} candidate pairs, {int(z['pair_penetrating'].sum())} interpenetrating, "
+          f"{int((z['pair_dist'] <= TUNNEL).sum())} within the tunnelling cutoff")
+
+
+if __name__ == "__main__":
+    main()
