@@ -14,17 +14,26 @@
  *     interpenetrate, then the move of GNP b): distance, direction, the
  *     interpenetration flag and the displacement of b.
  *
- *   gnp_dump <dir> <out.bin> <van_der_Waals_dist> <tunneling_dist>
+ *   gnp_dump <dir> <out.bin> <van_der_Waals_dist> <tunneling_dist> [<gs_min> <overlap_cnt> <overlap_gnp>]
+ *
+ * With the last three arguments it also dumps upstream's GNP part of the
+ * contact grid over the whole sample with every GNP inside
+ * (Contact_grid::Fill_sectioned_domain_gnps, Contact_grid.cpp:297-512, on the
+ * region grid of Generate_contact_grid + Adjust_regions_if_needed, :18-102):
+ * the region counts and sizes and each region's GNP list.
  *
  * Output records: u32 name length, name, u8 type ('i' int32, 'd' float64),
  * u64 count, payload (the layout oracle/dumpio.py reads).
  */
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <string>
 #include <unistd.h>
 #include <vector>
 
+#include "Contact_grid.h"
 #include "Hns.h"
 #include "Hoshen_Kopelman.h"
 #include "Input_Reader.h"
@@ -110,6 +119,31 @@ int main(int argc, char** argv) {
             dir.insert(dir.end(), {N.x, N.y, N.z});
             disp.insert(disp.end(), {disp_tot.x, disp_tot.y, disp_tot.z});
         }
+    if (argc >= 8) {
+        const double gs = atof(argv[5]), ov_cnt = atof(argv[6]), ov_gnp = atof(argv[7]);
+        geom.gs_minx = geom.gs_miny = geom.gs_minz = gs;
+        geom.gs_overlap_cnt = ov_cnt;
+        geom.gs_overlap_gnp = ov_gnp;
+        const cuboid& w = geom.sample;
+        int nreg[3] = {std::max(1, (int)(w.len_x / gs)), std::max(1, (int)(w.wid_y / gs)), std::max(1, (int)(w.hei_z / gs))};
+        double lreg[3] = {gs, gs, gs};
+        Contact_grid CG;
+        if (!CG.Adjust_regions_if_needed(std::max(ov_cnt, ov_gnp), geom, w, nreg, lreg)) return 7;
+        const int tot = nreg[0] * nreg[1] * nreg[2];
+        std::vector<int> inside(n);
+        for (int i = 0; i < n; i++) inside[i] = i;
+        CG.sectioned_domain_gnps.assign(tot, std::vector<int>());
+        if (!CG.Fill_sectioned_domain_gnps(w, gnps, inside, ov_gnp, nreg, lreg, tot)) return 8;
+        std::vector<int> sptr(1, 0), sidx;
+        for (const auto& r : CG.sectioned_domain_gnps) {
+            sidx.insert(sidx.end(), r.begin(), r.end());
+            sptr.push_back((int)sidx.size());
+        }
+        o.i32("sd_n_regions", {nreg[0], nreg[1], nreg[2]});
+        o.f64("sd_l_regions", {lreg[0], lreg[1], lreg[2]});
+        o.i32("sd_ptr", sptr);
+        o.i32("sd_idx", sidx);
+    }
     o.i32("pair_a", pa);
     o.i32("pair_b", pb);
     o.i32("pair_penetrating", pflag);

@@ -3,10 +3,11 @@
 Runs oracle/_ref/gnp_dump (upstream CICY_geom objects compiled in place by
 oracle/Makefile) on 120 seeded GNPs in a 2 um cube (side U[0.5, 1.0] um,
 thickness 10 nm, normal uniform on the sphere) and stores, next to the inputs,
-upstream's GNPs as it reads them (rotation, vertices, face planes) and, for
-every candidate pair, upstream's GNP-GNP distance step (GJK distance, EPA when
-the GNPs interpenetrate, the move of the second GNP): the oracle of the GNP
-contact search.  The fixture itself is self-contained.
+upstream's GNPs as it reads them (rotation, vertices, face planes), upstream's
+GNP part of the contact grid (0.05 um regions, overlaps as Input_Reader sets
+them) and, for every candidate pair, upstream's GNP-GNP distance step (GJK
+distance, EPA when the GNPs interpenetrate, the move of the second GNP): the
+oracle of the GNP contact search.  The fixture itself is self-contained.
 
     python tests/golden/make_gnp_golden.py
 """
@@ -29,6 +30,9 @@ from oracle.dumpio import read_dump  # noqa: E402
 REF = os.path.join(ROOT, "oracle", "_ref", "gnp_dump")
 N, SIDE, SEED = 120, 2.0, 4_000_000
 VDW, TUNNEL = 0.00034, 0.0018  # um, as the CNT configurations
+GS_MIN = 0.05
+OVERLAP_CNT = 2 * 0.005 + TUNNEL          # Input_Reader.cpp:1035 (2 r_max + tunnelling cutoff)
+OVERLAP_GNP = GS_MIN / np.sqrt(8.0)       # Input_Reader.cpp:1368
 
 
 def dump(gnps: dict, side: float, directory: str) -> dict:
@@ -36,7 +40,8 @@ def dump(gnps: dict, side: float, directory: str) -> dict:
     with open(os.path.join(directory, "sample_geom.csv"), "w") as f:
         f.write(f"0,0,0\n{side!r},{side!r},{side!r}\n")
     out = os.path.join(directory, "gnp.bin")
-    subprocess.run([REF, directory, out, repr(VDW), repr(TUNNEL)], check=True, capture_output=True, timeout=600)
+    subprocess.run([REF, directory, out, repr(VDW), repr(TUNNEL), repr(GS_MIN), repr(OVERLAP_CNT), repr(float(OVERLAP_GNP))],
+                   check=True, capture_output=True, timeout=600)
     return read_dump(out)
 
 
@@ -46,7 +51,8 @@ def main():
         z = dump(g, SIDE, d)
     np.savez_compressed(os.path.join(HERE, f"gnp_{N}_s{SEED}.npz"),
                         in_l=g["l"], in_t=g["t"], in_theta=g["theta"], in_phi=g["phi"], in_center=g["center"],
-                        meta=np.array([N, SIDE, SEED, VDW, TUNNEL]), **{"ref_" + k: v for k, v in z.items()})
+                        meta=np.array([N, SIDE, SEED, VDW, TUNNEL, GS_MIN, OVERLAP_CNT, OVERLAP_GNP]),
+                        **{"ref_" + k: v for k, v in z.items()})
     print(f"{N} GNPs, {len(z['pair_a'])} candidate pairs, {int(z['pair_penetrating'].sum())} interpenetrating, "
           f"{int((z['pair_dist'] <= TUNNEL).sum())} within the tunnelling cutoff")
 

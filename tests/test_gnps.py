@@ -2,8 +2,9 @@
 (rotation, vertices, face planes) bit for bit as upstream's Read_Network does,
 checked against the golden fixture made by the upstream program
 (tests/golden/make_gnp_golden.py) and, when oracle/_ref/gnp_dump is built, live
-on another seed.  The fixture's GNP-GNP distances (upstream GJK / EPA) are the
-oracle of the GNP contact search; their upstream invariants are checked here."""
+on another seed.  The fixture's GNP-GNP distances (upstream GJK / EPA) and GNP
+region lists are the oracle of the GNP contact search; the distances' upstream
+invariants and the CPU restatement of the region filling are checked here."""
 import os
 import subprocess
 
@@ -81,3 +82,21 @@ def test_gnp_file_errors(tmp_path):
     open(path, "wb").write(data[:-8])
     with pytest.raises(_abi.CicyError, match="end-of-file of gnp_data.dat"):
         read_gnps(d)
+
+
+def test_gnp_contact_grid_oracle_matches_upstream_golden():
+    """The CPU restatement of upstream's GNP region filling (oracle/gnp_oracle.py)
+    gives upstream's region lists on the fixture."""
+    from oracle import gnp_oracle as G
+
+    z = golden()
+    side, gs, ov_cnt, ov_gnp = float(z["meta"][1]), float(z["meta"][5]), float(z["meta"][6]), float(z["meta"][7])
+    win = [0.0, 0.0, 0.0, side, side, side, side, side, side]
+    n, l = G.region_grid(win, [gs] * 3, ov_cnt, ov_gnp)
+    assert list(n) == list(z["ref_sd_n_regions"]) and np.array_equal(l, z["ref_sd_l_regions"])
+    N = len(z["in_l"])
+    regs = G.fill_sectioned_domain_gnps(win, z["ref_gnp_vertices"].reshape(N, 8, 3), z["in_l"], z["in_t"], range(N), n, l, ov_gnp)
+    ptr, idx = z["ref_sd_ptr"], z["ref_sd_idx"]
+    assert len(regs) == len(ptr) - 1
+    assert all(list(idx[ptr[k]:ptr[k + 1]]) == regs[k] for k in range(len(regs)))
+    assert len(idx) > 10000
