@@ -221,6 +221,10 @@ def lib() -> C.CDLL:
         "cicy_read_gnps": (C.c_int, [C.c_char_p, P(C.c_void_p)]),
         "cicy_gnp_set_view": (C.c_int, [C.c_void_p, P(Gnps)]),
         "cicy_gnp_set_free": (None, [C.c_void_p]),
+        "cicy_gnp_sectioned_domain": (C.c_int, [C.c_int, C.c_void_p, i32p, C.c_int32, P(Cuboid), f64p, C.c_double, C.c_double,
+                                                P(C.c_void_p)]),
+        "cicy_gnp_grid_view": (C.c_int, [C.c_void_p, i32p, f64p, P(C.c_void_p), P(C.c_void_p), i64p]),
+        "cicy_gnp_grid_free": (None, [C.c_void_p]),
         "cicy_host_network_view": (C.c_int, [C.c_void_p, P(Network)]),
         "cicy_host_network_free": (None, [C.c_void_p]),
         "cicy_host_last_error": (C.c_char_p, []),

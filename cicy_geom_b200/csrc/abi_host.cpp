@@ -49,10 +49,6 @@ cicy_status cicy_read_network(const char* directory, int32_t file_type, cicy_hos
     return CICY_OK;
 }
 
-struct cicy_gnp_set {
-    cicy::GnpSet g;
-};
-
 cicy_status cicy_read_gnps(const char* directory, cicy_gnp_set** out) {
     if (!directory || !out) return CICY_E_INPUT;
     cicy::GnpSet* g = nullptr;

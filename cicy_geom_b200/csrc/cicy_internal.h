@@ -35,6 +35,16 @@ struct GnpSet {
     std::vector<double> l, t, center, rotation, vertices, planes;  // per GNP: 1, 1, 3, 9, 24, 24
 };
 cicy_status read_gnp_file(const std::string& dir, GnpSet** out, std::string& err);
+
+// GNP part of the contact grid (gnp_grid.cu): region grid and region lists (CSR, GNP indices).
+struct GnpGrid {
+    int n_regions[3] = {0, 0, 0};
+    double l_regions[3] = {0, 0, 0};
+    std::vector<int32_t> ptr, idx;
+    int64_t launches = 0;
+};
+void gnp_sectioned_domain(const GnpSet& g, const std::vector<int32_t>& inside, const cicy_cuboid& w, const double gs_min[3],
+                          double overlap_cnt, double overlap_gnp, GnpGrid& out);
 // Message returned by cicy_host_last_error() on this thread.
 void set_host_error(const std::string& msg);
 void host_network_view(const HostNetwork& h, cicy_network& v);
@@ -43,4 +53,12 @@ void host_network_view(const HostNetwork& h, cicy_network& v);
 
 struct cicy_host_network {
     cicy::HostNetwork net;
+};
+
+struct cicy_gnp_set {
+    cicy::GnpSet g;
+};
+
+struct cicy_gnp_grid {
+    cicy::GnpGrid grid;
 };

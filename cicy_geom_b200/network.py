@@ -372,3 +372,32 @@ def read_gnps(directory: str) -> dict:
                 "planes": arr(v.planes, 24 * n, (n, 6, 4))}
     finally:
         lib().cicy_gnp_set_free(h)
+
+
+def gnp_sectioned_domain(directory: str, inside, window, gs_min, overlap_cnt: float, overlap_gnp: float, device: int = 0):
+    """Upstream's GNP part of the contact grid on the device (cicy_gnp_sectioned_domain) for
+    the GNPs of `directory`/gnp_data.dat: returns (n_regions[3], l_regions[3], ptr, idx),
+    region t's GNPs being idx[ptr[t]:ptr[t + 1]].  window = (min xyz, len xyz, max xyz)."""
+    h = C.c_void_p()
+    check(lib().cicy_read_gnps(directory.encode(), C.byref(h)), "cicy_read_gnps")
+    grid = C.c_void_p()
+    try:
+        ins = np.ascontiguousarray(inside, dtype=np.int32)
+        gs = np.ascontiguousarray(gs_min, dtype=np.float64)
+        w = _abi.Cuboid(*[float(x) for x in window])
+        check(lib().cicy_gnp_sectioned_domain(device, h, ins.ctypes.data_as(_abi.i32p), len(ins), C.byref(w), gs.ctypes.data_as(_abi.f64p),
+                                              float(overlap_cnt), float(overlap_gnp), C.byref(grid)), "cicy_gnp_sectioned_domain")
+        n = np.zeros(3, np.int32)
+        l = np.zeros(3)
+        pp, ip = C.c_void_p(), C.c_void_p()
+        ne = C.c_int64()
+        check(lib().cicy_gnp_grid_view(grid, n.ctypes.data_as(_abi.i32p), l.ctypes.data_as(_abi.f64p), C.byref(pp), C.byref(ip),
+                                       C.byref(ne)), "cicy_gnp_grid_view")
+        tot = int(n[0]) * int(n[1]) * int(n[2])
+        ptr = np.ctypeslib.as_array(C.cast(pp, C.POINTER(C.c_int32)), shape=(tot + 1,)).copy()
+        idx = (np.ctypeslib.as_array(C.cast(ip, C.POINTER(C.c_int32)), shape=(ne.value,)).copy() if ne.value else np.zeros(0, np.int32))
+        return n, l, ptr, idx
+    finally:
+        if grid:
+            lib().cicy_gnp_grid_free(grid)
+        lib().cicy_gnp_set_free(h)

@@ -397,6 +397,24 @@ cicy_status cicy_read_gnps(const char* directory, cicy_gnp_set** out);
 cicy_status cicy_gnp_set_view(const cicy_gnp_set* set, cicy_gnps* view);
 void cicy_gnp_set_free(cicy_gnp_set* set);
 
+/* GNP part of the contact grid on the device: Contact_grid::Fill_sectioned_domain_gnps
+ * (Contact_grid.cpp:297-512) on the region grid of Generate_contact_grid +
+ * Adjust_regions_if_needed (:18-102).  The GNPs of `inside` (indices into the
+ * set, in order) are sampled on upstream's grid of their volume; each sample
+ * point strictly inside `window` adds its GNP to its region and the overlap
+ * neighbours.  Region t = a + b sx + c sx sy lists each GNP once, in `inside`
+ * order (the upstream sectioned_domain_gnps), as CSR of GNP indices.  FP64
+ * without contraction, so the lists equal upstream's.  Limits: regions x
+ * GNPs < 2^32, at most 2^29 sample points (CICY_E_CAPACITY). */
+typedef struct cicy_gnp_grid cicy_gnp_grid;
+cicy_status cicy_gnp_sectioned_domain(int device, const cicy_gnp_set* gnps, const int32_t* inside, int32_t n_inside,
+                                      const cicy_cuboid* window, const double* gs_min, double overlap_cnt, double overlap_gnp,
+                                      cicy_gnp_grid** out);
+/* Region counts, sizes and the CSR (ptr[sx sy sz + 1], idx[n_entries]); valid until cicy_gnp_grid_free. */
+cicy_status cicy_gnp_grid_view(const cicy_gnp_grid* g, int32_t* n_regions, double* l_regions, const int32_t** ptr, const int32_t** idx,
+                               int64_t* n_entries);
+void cicy_gnp_grid_free(cicy_gnp_grid* g);
+
 /* Wrap caller-owned arrays (copied) as a host network, e.g. a network read from files. */
 cicy_status cicy_host_network_from_arrays(const cicy_network* net, cicy_host_network** out);
 /* Borrowed view of a host network; valid until cicy_host_network_free. */
