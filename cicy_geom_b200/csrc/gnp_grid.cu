@@ -17,6 +17,7 @@
 
 #include "cicy_internal.h"
 #include "dev_common.cuh"
+#include "gnp_geom.cuh"
 
 namespace cicy {
 namespace {
@@ -125,6 +126,21 @@ __global__ void k_region_idx(int n_unique, uint32_t n_inside, const int32_t* __r
 }
 
 int blocks_for(long long n) { return (int)std::max(1LL, std::min((n + 255) / 256, 148LL * 16)); }
+
+// Closest GNP point to each query point (gnp_geom.cuh), one thread per query.
+__global__ void k_gnp_closest(int n, const double* __restrict__ xyz, const int32_t* __restrict__ gnp, const double* __restrict__ V,
+                              const double* __restrict__ F, double* __restrict__ dist, double* __restrict__ q, int32_t* __restrict__ flag) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int g = gnp[i];
+        gnp::P3 c;
+        double d;
+        flag[i] = gnp::closest_point(V + 24 * (size_t)g, F + 24 * (size_t)g, gnp::P3{xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]}, c, d);
+        dist[i] = d;
+        q[3 * i] = c.x;
+        q[3 * i + 1] = c.y;
+        q[3 * i + 2] = c.z;
+    }
+}
 
 }  // namespace
 
@@ -266,5 +282,40 @@ cicy_status cicy_gnp_grid_view(const cicy_gnp_grid* g, int32_t* n_regions, doubl
 }
 
 void cicy_gnp_grid_free(cicy_gnp_grid* g) { delete g; }
+
+cicy_status cicy_gnp_point_distance(int device, const cicy_gnp_set* gnps, int32_t n, const double* xyz, const int32_t* gnp, double* dist,
+                                    double* closest, int32_t* flag) {
+    if (!gnps || n < 0 || (n > 0 && (!xyz || !gnp || !dist || !closest || !flag))) {
+        cicy::set_host_error("cicy_gnp_point_distance: invalid arguments");
+        return CICY_E_INPUT;
+    }
+    for (int i = 0; i < n; i++)
+        if (gnp[i] < 0 || gnp[i] >= gnps->g.n) {
+            cicy::set_host_error("cicy_gnp_point_distance: GNP index " + std::to_string(gnp[i]) + " out of range");
+            return CICY_E_INPUT;
+        }
+    if (n == 0) return CICY_OK;
+    try {
+        CICY_CUDA(cudaSetDevice(device));
+        const cicy::GnpSet& g = gnps->g;
+        cicy::DBuf<double> d_xyz, d_v, d_f, d_dist, d_q;
+        cicy::DBuf<int32_t> d_g, d_flag;
+        d_xyz.ensure(3 * (size_t)n); d_g.ensure(n); d_v.ensure(24 * (size_t)g.n); d_f.ensure(24 * (size_t)g.n);
+        d_dist.ensure(n); d_q.ensure(3 * (size_t)n); d_flag.ensure(n);
+        CICY_CUDA(cudaMemcpy(d_xyz.get(), xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
+        CICY_CUDA(cudaMemcpy(d_g.get(), gnp, sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+        CICY_CUDA(cudaMemcpy(d_v.get(), g.vertices.data(), sizeof(double) * 24 * g.n, cudaMemcpyHostToDevice));
+        CICY_CUDA(cudaMemcpy(d_f.get(), g.planes.data(), sizeof(double) * 24 * g.n, cudaMemcpyHostToDevice));
+        cicy::k_gnp_closest<<<cicy::blocks_for(n), 256>>>(n, d_xyz.get(), d_g.get(), d_v.get(), d_f.get(), d_dist.get(), d_q.get(), d_flag.get());
+        CICY_LAUNCH_CHECK();
+        CICY_CUDA(cudaMemcpy(dist, d_dist.get(), sizeof(double) * n, cudaMemcpyDeviceToHost));
+        CICY_CUDA(cudaMemcpy(closest, d_q.get(), sizeof(double) * 3 * n, cudaMemcpyDeviceToHost));
+        CICY_CUDA(cudaMemcpy(flag, d_flag.get(), sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+    } catch (const cicy::Fail& e) {
+        cicy::set_host_error(e.msg);
+        return e.status;
+    }
+    return CICY_OK;
+}
 
 }  // extern "C"

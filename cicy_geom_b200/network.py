@@ -401,3 +401,21 @@ def gnp_sectioned_domain(directory: str, inside, window, gs_min, overlap_cnt: fl
         if grid:
             lib().cicy_gnp_grid_free(grid)
         lib().cicy_gnp_set_free(h)
+
+
+def gnp_closest_points(directory: str, xyz, gnp, device: int = 0):
+    """Closest point of GNP gnp[i] (of `directory`/gnp_data.dat) to xyz[i] on the device
+    (cicy_gnp_point_distance): returns (distance[n], closest[n, 3], flag[n]; -1 inside)."""
+    h = C.c_void_p()
+    check(lib().cicy_read_gnps(directory.encode(), C.byref(h)), "cicy_read_gnps")
+    try:
+        p = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        g = np.ascontiguousarray(gnp, dtype=np.int32)
+        n = len(g)
+        dist, q, fl = np.zeros(n), np.zeros((n, 3)), np.zeros(n, np.int32)
+        check(lib().cicy_gnp_point_distance(device, h, n, p.ctypes.data_as(_abi.f64p), g.ctypes.data_as(_abi.i32p),
+                                            dist.ctypes.data_as(_abi.f64p), q.ctypes.data_as(_abi.f64p), fl.ctypes.data_as(_abi.i32p)),
+              "cicy_gnp_point_distance")
+        return dist, q, fl
+    finally:
+        lib().cicy_gnp_set_free(h)

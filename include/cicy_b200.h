@@ -415,6 +415,16 @@ cicy_status cicy_gnp_grid_view(const cicy_gnp_grid* g, int32_t* n_regions, doubl
                                int64_t* n_entries);
 void cicy_gnp_grid_free(cicy_gnp_grid* g);
 
+/* Closest GNP point to each query point on the device, the CNT-GNP distance of
+ * the mixed contact search (Generate_Network::Get_gnp_point_closest_to_point,
+ * Generate_Network.cpp:5577-5856, called by Hoshen_Kopelman::Find_adjacent_labels):
+ * host arrays xyz[3n] and GNP indices gnp[n] in, distance dist[n], closest
+ * point closest[3n] and flag[n] (0, or -1 with distance 0 and the origin when
+ * the point is inside the GNP) out.  Upstream's decision tree and arithmetic
+ * order without contraction, so the results equal upstream's. */
+cicy_status cicy_gnp_point_distance(int device, const cicy_gnp_set* gnps, int32_t n, const double* xyz, const int32_t* gnp, double* dist,
+                                    double* closest, int32_t* flag);
+
 /* Wrap caller-owned arrays (copied) as a host network, e.g. a network read from files. */
 cicy_status cicy_host_network_from_arrays(const cicy_network* net, cicy_host_network** out);
 /* Borrowed view of a host network; valid until cicy_host_network_free. */

@@ -22,6 +22,12 @@
  * region grid of Generate_contact_grid + Adjust_regions_if_needed, :18-102):
  * the region counts and sizes and each region's GNP list.
  *
+ * If the directory holds gnp_queries.dat (int n, then n x {x, y, z, GNP index}
+ * as doubles), it also dumps upstream's closest GNP point to each query point
+ * (Generate_Network::Get_gnp_point_closest_to_point, Generate_Network.cpp:5577-
+ * 5856, the CNT-GNP distance of Find_adjacent_labels): distance, closest point
+ * and flag (-1: the point is inside the GNP).
+ *
  * Output records: u32 name length, name, u8 type ('i' int32, 'd' float64),
  * u64 count, payload (the layout oracle/dumpio.py reads).
  */
@@ -34,6 +40,7 @@
 #include <vector>
 
 #include "Contact_grid.h"
+#include "Generate_Network.h"
 #include "Hns.h"
 #include "Hoshen_Kopelman.h"
 #include "Input_Reader.h"
@@ -143,6 +150,27 @@ int main(int argc, char** argv) {
         o.f64("sd_l_regions", {lreg[0], lreg[1], lreg[2]});
         o.i32("sd_ptr", sptr);
         o.i32("sd_idx", sidx);
+    }
+    if (FILE* qf = fopen("gnp_queries.dat", "rb")) {
+        int nq = 0;
+        if (fread(&nq, 4, 1, qf) != 1) nq = 0;
+        std::vector<double> q(4 * (size_t)std::max(nq, 0));
+        if (nq > 0 && fread(q.data(), 8, q.size(), qf) != q.size()) nq = 0;
+        fclose(qf);
+        Generate_Network GN;
+        std::vector<double> qd, qp;
+        std::vector<int> qflag;
+        for (int i = 0; i < nq; i++) {
+            Point_3D P(q[4 * i], q[4 * i + 1], q[4 * i + 2]);
+            double dist = 0;
+            Point_3D C = GN.Get_gnp_point_closest_to_point(gnps[(int)q[4 * i + 3]], P, dist);
+            qd.push_back(dist);
+            qp.insert(qp.end(), {C.x, C.y, C.z});
+            qflag.push_back(C.flag);
+        }
+        o.f64("query_dist", qd);
+        o.f64("query_point", qp);
+        o.i32("query_flag", qflag);
     }
     o.i32("pair_a", pa);
     o.i32("pair_b", pb);

@@ -4,6 +4,8 @@ Runs oracle/_ref/gnp_dump (upstream CICY_geom objects compiled in place by
 oracle/Makefile) on 120 seeded GNPs in a 2 um cube (side U[0.5, 1.0] um,
 thickness 10 nm, normal uniform on the sphere) and stores, next to the inputs,
 upstream's GNPs as it reads them (rotation, vertices, face planes), upstream's
+closest GNP point to 20 query points around each GNP (the CNT-GNP distance),
+upstream's
 GNP part of the contact grid (0.05 um regions, overlaps as Input_Reader sets
 them) and, for every candidate pair, upstream's GNP-GNP distance step (GJK
 distance, EPA when the GNPs interpenetrate, the move of the second GNP): the
@@ -35,8 +37,22 @@ OVERLAP_CNT = 2 * 0.005 + TUNNEL          # Input_Reader.cpp:1035 (2 r_max + tun
 OVERLAP_GNP = GS_MIN / np.sqrt(8.0)       # Input_Reader.cpp:1368
 
 
-def dump(gnps: dict, side: float, directory: str) -> dict:
+def queries(gnps: dict, per: int, seed: int) -> np.ndarray:
+    """Points around each GNP at three scales (far, near the faces, inside): x, y, z, GNP index."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(len(gnps["l"])):
+        c, l = gnps["center"][i], gnps["l"][i]
+        for _ in range(per):
+            out.append([*(c + rng.uniform(-0.7 * l, 0.7 * l, 3) * rng.choice([1.0, 0.02, 0.005])), float(i)])
+    return np.array(out)
+
+
+def dump(gnps: dict, side: float, directory: str, q: np.ndarray) -> dict:
     write_gnp_file(directory, gnps)
+    with open(os.path.join(directory, "gnp_queries.dat"), "wb") as f:
+        f.write(np.int32(len(q)).tobytes())
+        f.write(q.astype("<f8").tobytes())
     with open(os.path.join(directory, "sample_geom.csv"), "w") as f:
         f.write(f"0,0,0\n{side!r},{side!r},{side!r}\n")
     out = os.path.join(directory, "gnp.bin")
@@ -47,10 +63,11 @@ def dump(gnps: dict, side: float, directory: str) -> dict:
 
 def main():
     g = generate_gnps(N, SIDE, SEED)
+    q = queries(g, 20, SEED + 1)
     with tempfile.TemporaryDirectory() as d:
-        z = dump(g, SIDE, d)
+        z = dump(g, SIDE, d, q)
     np.savez_compressed(os.path.join(HERE, f"gnp_{N}_s{SEED}.npz"),
-                        in_l=g["l"], in_t=g["t"], in_theta=g["theta"], in_phi=g["phi"], in_center=g["center"],
+                        in_l=g["l"], in_t=g["t"], in_theta=g["theta"], in_phi=g["phi"], in_center=g["center"], in_queries=q,
                         meta=np.array([N, SIDE, SEED, VDW, TUNNEL, GS_MIN, OVERLAP_CNT, OVERLAP_GNP]),
                         **{"ref_" + k: v for k, v in z.items()})
     print(f"{N} GNPs, {len(z['pair_a'])} candidate pairs, {int(z['pair_penetrating'].sum())} interpenetrating, "

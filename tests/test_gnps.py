@@ -100,3 +100,16 @@ def test_gnp_contact_grid_oracle_matches_upstream_golden():
     assert len(regs) == len(ptr) - 1
     assert all(list(idx[ptr[k]:ptr[k + 1]]) == regs[k] for k in range(len(regs)))
     assert len(idx) > 10000
+
+
+def test_golden_gnp_closest_points_keep_upstream_invariants():
+    """Upstream's closest GNP points: inside points flagged -1 at distance 0, the
+    others at the returned distance from the query, every branch represented."""
+    z = golden()
+    q = z["in_queries"]
+    fl, d, c = z["ref_query_flag"], z["ref_query_dist"], z["ref_query_point"].reshape(-1, 3)
+    assert set(np.unique(fl)) == {-1, 0}
+    assert np.all(d[fl == -1] == 0)
+    out = fl == 0
+    assert out.sum() > 500 and (~out).sum() > 500
+    np.testing.assert_allclose(np.linalg.norm(q[out, :3] - c[out], axis=1), d[out], rtol=1e-9, atol=1e-12)

@@ -42,3 +42,17 @@ def test_gnp_grid_matches_oracle_on_a_window(cuda_ok, tmp_path):
     assert len(ptr) == len(regs) + 1
     assert all(list(idx[ptr[k]:ptr[k + 1]]) == regs[k] for k in range(len(regs)))
     assert len(idx) > 1000
+
+
+def test_gnp_closest_point_matches_upstream_golden(cuda_ok, tmp_path):
+    """CNT-GNP distance: closest GNP point to the fixture's query points, bit for bit as upstream."""
+    from cicy_geom_b200.network import gnp_closest_points
+
+    z = dict(np.load(GOLDEN))
+    g = {"l": z["in_l"], "t": z["in_t"], "theta": z["in_theta"], "phi": z["in_phi"], "center": z["in_center"]}
+    write_gnp_file(str(tmp_path), g)
+    q = z["in_queries"]
+    dist, closest, flag = gnp_closest_points(str(tmp_path), q[:, :3], q[:, 3].astype(np.int32))
+    assert np.array_equal(flag, z["ref_query_flag"])
+    assert np.array_equal(dist, z["ref_query_dist"])
+    assert np.array_equal(closest.ravel(), z["ref_query_point"])
