@@ -28,11 +28,21 @@
  * 5856, the CNT-GNP distance of Find_adjacent_labels): distance, closest point
  * and flag (-1: the point is inside the GNP).
  *
+ * If the directory also holds cnt_struct.dat / cnt_coordinates.dat and the grid
+ * arguments are given, it runs upstream's mixed contact pass on the whole
+ * sample (Contact_grid::Generate_contact_grid for GNP_CNT_mix, then
+ * Hoshen_Kopelman::Find_adjacent_labels, Hoshen_Kopelman.cpp:1989-2142, with a
+ * CNT point inside a GNP counted as no contact, ignore_eror_cnt_inside_gnp = 1)
+ * and dumps the CNT sectioned domain and the CNT-GNP contacts: point, GNP,
+ * contact-point number, junction distance, and the contact points in order.
+ *
  * Output records: u32 name length, name, u8 type ('i' int32, 'd' float64),
  * u64 count, payload (the layout oracle/dumpio.py reads).
  */
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <set>
 #include <cstdio>
 #include <cstdlib>
 #include <string>
@@ -145,6 +155,50 @@ int main(int argc, char** argv) {
         for (const auto& r : CG.sectioned_domain_gnps) {
             sidx.insert(sidx.end(), r.begin(), r.end());
             sptr.push_back((int)sidx.size());
+        }
+        std::vector<Point_3D> pts;
+        std::vector<double> radii;
+        std::vector<std::vector<long int> > structure;
+        if (FILE* cf = fopen("cnt_struct.dat", "rb")) {
+            fclose(cf);
+            if (!RN.Read_cnt_data_from_dat(pts, radii, structure)) return 9;
+            std::vector<int> cin(structure.size());
+            for (size_t i = 0; i < cin.size(); i++) cin[i] = (int)i;
+            Contact_grid CG2;
+            if (!CG2.Generate_contact_grid(0, "GNP_CNT_mix", geom, w, cin, pts, structure, inside, gnps)) return 10;
+            Hoshen_Kopelman HK2;
+            HK2.ignore_eror_cnt_inside_gnp = 1;
+            std::vector<int> labels_cnt(structure.size(), -1), labels_gnp(gnps.size(), -1);
+            std::vector<int> labels_mixed(structure.size() + gnps.size(), -1), labels_labels_mixed;
+            std::vector<Point_3D> contact_points_gnp;
+            std::map<long int, std::map<int, long int> > point_contacts;
+            std::map<long int, std::map<int, double> > point_contacts_dist;
+            std::vector<std::map<int, std::set<long int> > > gnp_cnt_point_contacts(gnps.size());
+            if (!HK2.Find_adjacent_labels(0, labels_cnt, labels_gnp, cut, pts, radii, CG2.sectioned_domain_cnts, gnps, CG2.sectioned_domain_gnps,
+                                          contact_points_gnp, point_contacts, point_contacts_dist, gnp_cnt_point_contacts, labels_mixed,
+                                          labels_labels_mixed))
+                return 11;
+            std::vector<int> sdc_ptr(1, 0), sdc_idx, mp, mg, mi;
+            std::vector<double> md, mpts;
+            for (const auto& r : CG2.sectioned_domain_cnts) {
+                for (long int v : r) sdc_idx.push_back((int)v);
+                sdc_ptr.push_back((int)sdc_idx.size());
+            }
+            for (const auto& pc : point_contacts)
+                for (const auto& gc : pc.second) {
+                    mp.push_back((int)pc.first);
+                    mg.push_back(gc.first);
+                    mi.push_back((int)gc.second);
+                    md.push_back(point_contacts_dist[pc.first][gc.first]);
+                }
+            for (const auto& c : contact_points_gnp) mpts.insert(mpts.end(), {c.x, c.y, c.z});
+            o.i32("mix_sd_cnt_ptr", sdc_ptr);
+            o.i32("mix_sd_cnt_idx", sdc_idx);
+            o.i32("mix_point", mp);
+            o.i32("mix_gnp", mg);
+            o.i32("mix_index", mi);
+            o.f64("mix_dist", md);
+            o.f64("mix_contact_points", mpts);
         }
         o.i32("sd_n_regions", {nreg[0], nreg[1], nreg[2]});
         o.f64("sd_l_regions", {lreg[0], lreg[1], lreg[2]});

@@ -9,12 +9,18 @@ upstream's
 GNP part of the contact grid (0.05 um regions, overlaps as Input_Reader sets
 them) and, for every candidate pair, upstream's GNP-GNP distance step (GJK
 distance, EPA when the GNPs interpenetrate, the move of the second GNP): the
-oracle of the GNP contact search.  The fixture itself is self-contained.
+oracle of the GNP contact search.  With a seeded 400-CNT network in the same
+cube (regenerated by the tests from its seed and checked against the stored
+SHA-256), it also stores upstream's CNT-GNP contacts of the mixed contact pass
+(Find_adjacent_labels: point, GNP, contact-point number, junction distance,
+closest GNP point) and the SHA-256 of upstream's CNT region lists.  The fixture
+itself is self-contained apart from the seeded CNT network.
 
     python tests/golden/make_gnp_golden.py
 """
 from __future__ import annotations
 
+import hashlib
 import os
 import subprocess
 import sys
@@ -26,7 +32,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-from cicy_geom_b200.network import generate_gnps, write_gnp_file  # noqa: E402
+from cicy_geom_b200.network import (NetworkConfig, generate_cnt_network, generate_gnps, read_network_files,  # noqa: E402
+                                    write_gnp_file, write_read_network_files)
 from oracle.dumpio import read_dump  # noqa: E402
 
 REF = os.path.join(ROOT, "oracle", "_ref", "gnp_dump")
@@ -35,6 +42,33 @@ VDW, TUNNEL = 0.00034, 0.0018  # um, as the CNT configurations
 GS_MIN = 0.05
 OVERLAP_CNT = 2 * 0.005 + TUNNEL          # Input_Reader.cpp:1035 (2 r_max + tunnelling cutoff)
 OVERLAP_GNP = GS_MIN / np.sqrt(8.0)       # Input_Reader.cpp:1368
+CNT_N, CNT_SEED = 400, SEED + 2
+
+
+def cnt_config() -> NetworkConfig:
+    return NetworkConfig(side=SIDE, n_cnts=CNT_N, seed=CNT_SEED, vdw=VDW, tunnel=TUNNEL)
+
+
+def hybrid_network(directory: str) -> dict:
+    """Write the seeded CNT network's Read_Network files into `directory` and
+    return it as upstream reads them (point numbers in CNT order)."""
+    cfg = cnt_config()
+    write_read_network_files(directory, generate_cnt_network(cfg), cfg)
+    return read_network_files(directory).arrays()
+
+
+def net_hash(a: dict) -> str:
+    h = hashlib.sha256()
+    for k in ("x", "y", "z", "flag", "structure_ptr", "structure_idx", "radii"):
+        h.update(np.ascontiguousarray(a[k]).tobytes())
+    return h.hexdigest()
+
+
+def arr_hash(*arrs) -> str:
+    h = hashlib.sha256()
+    for a in arrs:
+        h.update(np.ascontiguousarray(np.asarray(a, dtype=np.int64)).tobytes())
+    return h.hexdigest()
 
 
 def queries(gnps: dict, per: int, seed: int) -> np.ndarray:
@@ -65,13 +99,17 @@ def main():
     g = generate_gnps(N, SIDE, SEED)
     q = queries(g, 20, SEED + 1)
     with tempfile.TemporaryDirectory() as d:
+        net = hybrid_network(d)
         z = dump(g, SIDE, d, q)
+    sd_sha = arr_hash(z.pop("mix_sd_cnt_ptr"), z.pop("mix_sd_cnt_idx"))
     np.savez_compressed(os.path.join(HERE, f"gnp_{N}_s{SEED}.npz"),
                         in_l=g["l"], in_t=g["t"], in_theta=g["theta"], in_phi=g["phi"], in_center=g["center"], in_queries=q,
                         meta=np.array([N, SIDE, SEED, VDW, TUNNEL, GS_MIN, OVERLAP_CNT, OVERLAP_GNP]),
+                        cnt_meta=np.array([CNT_N, CNT_SEED]), cnt_sha256=np.array(net_hash(net)), mix_sd_sha256=np.array(sd_sha),
                         **{"ref_" + k: v for k, v in z.items()})
     print(f"{N} GNPs, {len(z['pair_a'])} candidate pairs, {int(z['pair_penetrating'].sum())} interpenetrating, "
-          f"{int((z['pair_dist'] <= TUNNEL).sum())} within the tunnelling cutoff")
+          f"{int((z['pair_dist'] <= TUNNEL).sum())} within the tunnelling cutoff; {len(net['x'])} CNT points, "
+          f"{len(z['mix_point'])} CNT-GNP contacts")
 
 
 if __name__ == "__main__":

@@ -4,7 +4,9 @@ checked against the golden fixture made by the upstream program
 (tests/golden/make_gnp_golden.py) and, when oracle/_ref/gnp_dump is built, live
 on another seed.  The fixture's GNP-GNP distances (upstream GJK / EPA) and GNP
 region lists are the oracle of the GNP contact search; the distances' upstream
-invariants and the CPU restatement of the region filling are checked here."""
+invariants and the CPU restatement of the region filling are checked here, and
+so is the CPU restatement of the CNT-GNP contact pass (Find_adjacent_labels)
+against upstream's contacts on the fixture's hybrid sample and live."""
 import os
 import subprocess
 
@@ -113,3 +115,89 @@ def test_golden_gnp_closest_points_keep_upstream_invariants():
     out = fl == 0
     assert out.sum() > 500 and (~out).sum() > 500
     np.testing.assert_allclose(np.linalg.norm(q[out, :3] - c[out], axis=1), d[out], rtol=1e-9, atol=1e-12)
+
+
+def hybrid_inputs(z, directory):
+    """The fixture's CNT network as upstream reads it (regenerated from its seed,
+    checked against the stored hash), its CNT region lists from the CPU
+    restatement, and the fixture's GNP region lists, vertices and planes."""
+    import sys
+
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_gnp_golden as M
+    from oracle import cicy_oracle as O
+
+    net = dict(M.hybrid_network(directory))
+    assert M.net_hash(net) == str(z["cnt_sha256"])
+    side, gs, ov_cnt, ov_gnp = float(z["meta"][1]), float(z["meta"][5]), float(z["meta"][6]), float(z["meta"][7])
+    net["cnts_inside"] = np.arange(len(net["radii"]))
+    net["window"] = np.array([0.0, 0.0, 0.0, side, side, side, side, side, side])
+    _, _, regs = O.contact_grid(net, {"gs_min": (gs,) * 3, "gs_overlap_cnt": ov_cnt, "gs_overlap_gnp": ov_gnp})
+    ptr = np.cumsum([0] + [len(r) for r in regs])
+    idx = np.concatenate([np.asarray(r, dtype=np.int64) for r in regs])
+    assert M.arr_hash(ptr, idx) == str(z["mix_sd_sha256"])  # upstream's CNT region lists of the hybrid grid
+    sp, si = z["ref_sd_ptr"], z["ref_sd_idx"]
+    sd_gnp = [si[sp[k]:sp[k + 1]].tolist() for k in range(len(sp) - 1)]
+    n = len(z["in_l"])
+    return net, regs, sd_gnp, z["ref_gnp_vertices"].reshape(n, 8, 3), z["ref_gnp_planes"].reshape(n, 6, 4)
+
+
+def test_mixed_contacts_oracle_matches_upstream_golden(tmp_path):
+    """The CPU restatement of upstream's CNT-GNP contact pass
+    (oracle/gnp_oracle.py find_adjacent_labels) gives upstream's contacts on the
+    fixture: the same (point, GNP) pairs, contact-point numbers, junction
+    distances and closest GNP points, bit for bit."""
+    from oracle import gnp_oracle as G
+
+    z = golden()
+    net, regs, sd_gnp, V, F = hybrid_inputs(z, str(tmp_path))
+    xyz = np.stack([net["x"], net["y"], net["z"]], 1)
+    out = G.find_adjacent_labels(xyz.tolist(), net["flag"], net["radii"], regs, sd_gnp, V.tolist(), F.tolist(),
+                                 float(z["meta"][3]), float(z["meta"][4]))
+    P, g, i, d = z["ref_mix_point"], z["ref_mix_gnp"], z["ref_mix_index"], z["ref_mix_dist"]
+    cp = z["ref_mix_contact_points"].reshape(-1, 3)
+    assert len(out) == len(P) > 1000
+    for k in range(len(P)):
+        num, dj, q = out[(int(P[k]), int(g[k]))]
+        assert num == i[k] and dj == d[k] and tuple(q) == tuple(cp[num])
+
+
+def test_golden_mixed_contacts_keep_upstream_invariants():
+    z = golden()
+    vdw, tunnel = float(z["meta"][3]), float(z["meta"][4])
+    P, g, i, d = z["ref_mix_point"], z["ref_mix_gnp"], z["ref_mix_index"], z["ref_mix_dist"]
+    assert np.array_equal(np.sort(i), np.arange(len(i)))  # one contact point per (point, GNP) pair
+    assert len(set(zip(P.tolist(), g.tolist()))) == len(P)
+    assert np.all(d >= vdw) and np.all(d <= tunnel)
+    assert (d == vdw).sum() > 100 and (d > vdw).sum() > 100  # clamped and tunnelling junctions
+
+
+@pytest.mark.skipif(not os.path.exists(REF), reason="oracle/_ref/gnp_dump not built")
+def test_mixed_contacts_oracle_matches_upstream_live(tmp_path):
+    """Another seed and sample: the restatement against the upstream program run here."""
+    from cicy_geom_b200.network import NetworkConfig, generate_cnt_network, read_network_files, write_read_network_files
+    from oracle import cicy_oracle as O, gnp_oracle as G
+    from oracle.dumpio import read_dump
+
+    d, side, vdw, tunnel, gs = str(tmp_path), 1.5, 0.00034, 0.0018, 0.05
+    cfg = NetworkConfig(side=side, n_cnts=250, seed=4_000_321)
+    write_read_network_files(d, generate_cnt_network(cfg), cfg)
+    write_gnp_file(d, generate_gnps(50, side, 4_000_322))
+    ov_cnt, ov_gnp = 2 * cfg.radius + tunnel, gs / np.sqrt(8.0)
+    subprocess.run([REF, d, os.path.join(d, "g.bin"), repr(vdw), repr(tunnel), repr(gs), repr(ov_cnt), repr(float(ov_gnp))],
+                   check=True, capture_output=True, timeout=600)
+    z = read_dump(os.path.join(d, "g.bin"))
+    net = dict(read_network_files(d).arrays())
+    net["cnts_inside"] = np.arange(len(net["radii"]))
+    net["window"] = np.array([0.0, 0.0, 0.0, side, side, side, side, side, side])
+    _, _, regs = O.contact_grid(net, {"gs_min": (gs,) * 3, "gs_overlap_cnt": ov_cnt, "gs_overlap_gnp": float(ov_gnp)})
+    assert np.array_equal(np.cumsum([0] + [len(r) for r in regs]), z["mix_sd_cnt_ptr"])
+    sp, si = z["sd_ptr"], z["sd_idx"]
+    n = len(z["gnp_lt"]) // 2
+    out = G.find_adjacent_labels(np.stack([net["x"], net["y"], net["z"]], 1).tolist(), net["flag"], net["radii"], regs,
+                                 [si[sp[k]:sp[k + 1]].tolist() for k in range(len(sp) - 1)],
+                                 z["gnp_vertices"].reshape(n, 8, 3).tolist(), z["gnp_planes"].reshape(n, 6, 4).tolist(), vdw, tunnel)
+    ref = {(int(a), int(b)): (int(c), float(e)) for a, b, c, e in zip(z["mix_point"], z["mix_gnp"], z["mix_index"], z["mix_dist"])}
+    assert len(ref) > 200 and {k: v[:2] for k, v in out.items()} == ref
+    cp = z["mix_contact_points"].reshape(-1, 3)
+    assert all(tuple(v[2]) == tuple(cp[v[0]]) for v in out.values())
