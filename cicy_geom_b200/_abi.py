@@ -226,6 +226,8 @@ def lib() -> C.CDLL:
         "cicy_gnp_grid_view": (C.c_int, [C.c_void_p, i32p, f64p, P(C.c_void_p), P(C.c_void_p), i64p]),
         "cicy_gnp_grid_free": (None, [C.c_void_p]),
         "cicy_gnp_point_distance": (C.c_int, [C.c_int, C.c_void_p, C.c_int32, f64p, i32p, f64p, f64p, i32p]),
+        "cicy_gnp_cnt_contacts": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, P(Params), C.c_int32, i64p]),
+        "cicy_get_gnp_cnt_contacts": (C.c_int, [C.c_void_p, i64p, i64p, i32p, f64p, f64p]),
         "cicy_host_network_view": (C.c_int, [C.c_void_p, P(Network)]),
         "cicy_host_network_free": (None, [C.c_void_p]),
         "cicy_host_last_error": (C.c_char_p, []),

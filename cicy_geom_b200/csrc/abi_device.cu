@@ -4,6 +4,7 @@
 #include <new>
 #include <string>
 
+#include "cicy_internal.h"
 #include "ctx.cuh"
 
 struct cicy_ctx {
@@ -164,6 +165,32 @@ cicy_status cicy_network_to_conductance(cicy_ctx* ctx, const cicy_params* p, cic
             out->stage_seconds[1] = ms[1] * 1e-3;
             out->stage_seconds[5] = ms[2] * 1e-3;
         }
+    });
+}
+
+cicy_status cicy_gnp_cnt_contacts(cicy_ctx* ctx, const cicy_gnp_set* gnps, const cicy_gnp_grid* grid, const cicy_params* p,
+                                  int32_t inside_is_error, int64_t* n_contacts) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (!gnps || !grid || !p) throw cicy::Fail{CICY_E_INPUT, "cicy_gnp_cnt_contacts: null argument"};
+        const int n = cicy::run_gnp_cnt_contacts(c, gnps->g, grid->grid, *p, inside_is_error);
+        if (n_contacts) *n_contacts = n;
+    });
+}
+
+cicy_status cicy_get_gnp_cnt_contacts(cicy_ctx* ctx, int64_t* n, int64_t* point, int32_t* gnp, double* dist, double* closest) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        const int U = c.n_mix;
+        if (n) *n = U;
+        if (point && U) {
+            std::vector<int32_t> h(U);
+            d2h(c, h.data(), c.mix_point.get(), U);
+            sync(c);
+            for (int i = 0; i < U; i++) point[i] = h[i];
+        }
+        d2h(c, gnp, c.mix_gnp.get(), U);
+        d2h(c, dist, c.mix_dist.get(), U);
+        d2h(c, closest, c.mix_closest.get(), 3 * (size_t)U);
+        sync(c);
     });
 }
 

@@ -135,6 +135,11 @@ struct Ctx {
     GnnState gnn;
     DBuf<float> gnn_params;  // learned preconditioner parameters (cicy_ctx_set_learned_params)
 
+    // ---- CNT-GNP contacts (cicy_gnp_cnt_contacts), indexed by contact-point number ----
+    int n_mix = 0;
+    DBuf<int32_t> mix_point, mix_gnp;
+    DBuf<double> mix_dist, mix_closest;
+
     ~Ctx();
 };
 
@@ -143,6 +148,10 @@ void upload_network(Ctx& c, const cicy_network& net);
 void run_contact_grid(Ctx& c, const cicy_params& p);
 void run_clusters(Ctx& c, const cicy_params& p);
 void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out);
+struct GnpSet;
+struct GnpGrid;
+// CNT-GNP contacts of the hybrid grid (gnp_grid.cu); returns the number of contacts.
+int run_gnp_cnt_contacts(Ctx& c, const GnpSet& g, const GnpGrid& grid, const cicy_params& p, int inside_is_error);
 
 // Learned preconditioner: edge weights for the system being solved (learned.cu).
 const float* learned_edge_weights(Ctx& c, const SolverSystem& ss, int n_chains, cudaStream_t s);

@@ -11,11 +11,22 @@
 // (32 bits); a radix sort, a unique pass and a binary search per region give
 // the CSR of region lists.  FP64 without contraction (this file is built with
 // --fmad=false), so points, regions and flags equal upstream's.
+//
+// CNT-GNP contacts of the hybrid grid (Hoshen_Kopelman::Find_adjacent_labels,
+// Hoshen_Kopelman.cpp:1989-2142): upstream visits, region by region, every GNP
+// of the region against every CNT point of the region, and numbers a (point,
+// GNP) pair's contact point when the pair first tests as a contact.  The test
+// depends on the pair only, so the number is the rank of the pair's first
+// visit among the contact pairs.  On the device every visit is one thread
+// (ordinal = region offset + GNP slot x points + point slot); contact visits
+// append (pair key, ordinal), a sort by pair key and a min per run give each
+// pair's first ordinal, and a sort by that ordinal gives upstream's numbers.
 #include <algorithm>
 #include <cmath>
 #include <vector>
 
 #include "cicy_internal.h"
+#include "ctx.cuh"
 #include "dev_common.cuh"
 #include "gnp_geom.cuh"
 
@@ -142,7 +153,222 @@ __global__ void k_gnp_closest(int n, const double* __restrict__ xyz, const int32
     }
 }
 
+// ---------------------------------------------------------------------------
+// CNT-GNP contacts
+
+struct MixArgs {
+    int n_regions;
+    const int64_t* visit_off;   // first visit ordinal of each region [n_regions + 1]
+    const int32_t* gptr;        // GNP region lists (CSR)
+    const int32_t* gidx;
+    const int32_t* cptr;        // CNT region lists: slots of region t are cptr[t] .. cptr[t+1]
+    const uint32_t* slot;       // traversal index of each slot
+    const int32_t* trav_pt;     // point of each traversal index
+    const double *x, *y, *z, *radii;
+    const int32_t* flag;        // CNT of each point
+    const double *V, *F;        // GNP vertices and face planes
+    double vdw, tunnel;
+    uint32_t n_gnps;
+    long long n_visits;
+    uint64_t* keys;             // pair key P * n_gnps + GNP of each contact visit
+    uint32_t* ords;             // visit ordinal of each contact visit
+    int32_t cap;
+    int32_t* counters;          // [0] contact visits, [1] visits of a point inside a GNP
+};
+
+// Junction distance of Find_adjacent_labels; false when the point is no contact.
+__device__ __forceinline__ bool mixed_junction(const MixArgs& a, int P, int G, gnp::P3& q, double& dj, bool& inside) {
+    const int cnt = a.flag[P];
+    double d;
+    inside = gnp::closest_point(a.V + 24 * (size_t)G, a.F + 24 * (size_t)G, gnp::P3{a.x[P], a.y[P], a.z[P]}, q, d) == -1;
+    if (inside) d = a.radii[cnt] + 3.0 * a.tunnel;  // ignored: no contact
+    dj = d - a.radii[cnt];
+    if (dj < a.vdw) dj = a.vdw;
+    return dj - a.tunnel <= gnp::kZero;
+}
+
+__global__ void k_mix_visits(int R, const int32_t* __restrict__ gptr, const int32_t* __restrict__ cptr, int64_t* __restrict__ n) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t <= R; t += gridDim.x * blockDim.x)
+        n[t] = t < R ? (int64_t)(gptr[t + 1] - gptr[t]) * (cptr[t + 1] - cptr[t]) : 0;
+}
+
+__global__ void k_mix_eval(MixArgs a) {
+    for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < a.n_visits; o += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = a.n_regions - 1;  // last region whose first ordinal is <= o (a region with visits)
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (a.visit_off[mid] <= o) lo = mid;
+            else hi = mid - 1;
+        }
+        const int t = lo;
+        const long long loc = o - a.visit_off[t];
+        const int np = a.cptr[t + 1] - a.cptr[t];
+        const int G = a.gidx[a.gptr[t] + (int)(loc / np)];
+        const int P = a.trav_pt[a.slot[a.cptr[t] + (int)(loc % np)]];
+        gnp::P3 q;
+        double dj;
+        bool inside;
+        const bool hit = mixed_junction(a, P, G, q, dj, inside);
+        if (inside) atomicAdd(&a.counters[1], 1);
+        if (hit) {
+            const int pos = atomicAdd(&a.counters[0], 1);
+            if (pos < a.cap) {
+                a.keys[pos] = (uint64_t)P * a.n_gnps + (uint32_t)G;
+                a.ords[pos] = (uint32_t)o;
+            }
+        }
+    }
+}
+
+__global__ void k_mix_heads(int n, const uint64_t* __restrict__ keys, int32_t* __restrict__ head) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        head[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1 : 0;
+}
+
+// One entry per pair: its first visit ordinal (sort key) and its pair key.
+__global__ void k_mix_first(int n, const uint64_t* __restrict__ keys, const uint32_t* __restrict__ ords, const int32_t* __restrict__ head,
+                            const int32_t* __restrict__ pos, uint64_t* __restrict__ first, uint32_t* __restrict__ uidx,
+                            uint64_t* __restrict__ upair) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (!head[i]) continue;
+        uint32_t m = ords[i];
+        for (int k = i + 1; k < n && keys[k] == keys[i]; k++) m = min(m, ords[k]);
+        first[pos[i]] = m;
+        uidx[pos[i]] = (uint32_t)pos[i];
+        upair[pos[i]] = keys[i];
+    }
+}
+
+// Contact number i (pairs in first-visit order): point, GNP, junction distance, closest GNP point.
+__global__ void k_mix_out(MixArgs a, int n, const uint32_t* __restrict__ uidx, const uint64_t* __restrict__ upair,
+                          int32_t* __restrict__ point, int32_t* __restrict__ gnp_out, double* __restrict__ dist, double* __restrict__ closest) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint64_t k = upair[uidx[i]];
+        const int P = (int)(k / a.n_gnps), G = (int)(k % a.n_gnps);
+        gnp::P3 q;
+        double dj;
+        bool inside;
+        mixed_junction(a, P, G, q, dj, inside);
+        point[i] = P;
+        gnp_out[i] = G;
+        dist[i] = dj;
+        closest[3 * i] = q.x;
+        closest[3 * i + 1] = q.y;
+        closest[3 * i + 2] = q.z;
+    }
+}
+
 }  // namespace
+
+int run_gnp_cnt_contacts(Ctx& c, const GnpSet& g, const GnpGrid& grid, const cicy_params& p, int inside_is_error) {
+    if (c.stage < 2) throw Fail{CICY_E_STATE, "cicy_gnp_cnt_contacts: no contact grid"};
+    for (int d = 0; d < 3; d++)
+        if (grid.n_regions[d] != c.grid.n[d] || grid.l_regions[d] != c.grid.l[d])
+            throw Fail{CICY_E_INPUT, "cicy_gnp_cnt_contacts: the GNP grid and the contact grid have different regions"};
+    const int R = (int)c.grid.total;
+    if ((int)grid.ptr.size() != R + 1 || grid.ptr[R] != (int32_t)grid.idx.size())
+        throw Fail{CICY_E_INPUT, "cicy_gnp_cnt_contacts: GNP grid has no region lists"};
+    for (int32_t gi : grid.idx)
+        if (gi < 0 || gi >= g.n) throw Fail{CICY_E_INPUT, "cicy_gnp_cnt_contacts: GNP grid names a GNP outside the set"};
+    if ((unsigned long long)std::max(c.n_points, 1) * (unsigned long long)std::max(g.n, 1) >= (1ULL << 63))
+        throw Fail{CICY_E_CAPACITY, "cicy_gnp_cnt_contacts: points x GNPs too large"};
+    cudaStream_t s = c.stream;
+    c.n_mix = 0;
+    if (grid.idx.empty() || c.n_slots == 0) return 0;
+    DBuf<int32_t> gptr, gidx, counters, head, pos, total;
+    DBuf<int64_t> nvis, off, tot64;
+    DBuf<double> V, F;
+    gptr.ensure(R + 1);
+    gidx.ensure(grid.idx.size());
+    V.ensure(24 * (size_t)g.n);
+    F.ensure(24 * (size_t)g.n);
+    CICY_CUDA(cudaMemcpyAsync(gptr.get(), grid.ptr.data(), sizeof(int32_t) * (R + 1), cudaMemcpyHostToDevice, s));
+    CICY_CUDA(cudaMemcpyAsync(gidx.get(), grid.idx.data(), sizeof(int32_t) * grid.idx.size(), cudaMemcpyHostToDevice, s));
+    CICY_CUDA(cudaMemcpyAsync(V.get(), g.vertices.data(), sizeof(double) * 24 * g.n, cudaMemcpyHostToDevice, s));
+    CICY_CUDA(cudaMemcpyAsync(F.get(), g.planes.data(), sizeof(double) * 24 * g.n, cudaMemcpyHostToDevice, s));
+    nvis.ensure(R + 1);
+    off.ensure(R + 1);
+    tot64.ensure(1);
+    k_mix_visits<<<blocks_for(R + 1), 256, 0, s>>>(R, gptr.get(), c.region_ptr.get(), nvis.get());
+    DBuf<int64_t> scan64;
+    exclusive_scan_i64(nvis.get(), off.get(), R + 1, tot64.get(), scan64, s, c.launches);
+    int64_t T = 0;
+    CICY_CUDA(cudaMemcpyAsync(&T, tot64.get(), sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    CICY_CUDA(cudaStreamSynchronize(s));
+    if (T >= (1LL << 31)) throw Fail{CICY_E_CAPACITY, "cicy_gnp_cnt_contacts: 2^31 or more point-GNP visits"};
+    if (T == 0) return 0;
+    MixArgs a{};
+    a.n_regions = R;
+    a.visit_off = off.get();
+    a.gptr = gptr.get();
+    a.gidx = gidx.get();
+    a.cptr = c.region_ptr.get();
+    a.slot = c.slot_sorted.get();
+    a.trav_pt = c.trav_pt.get();
+    a.x = c.x.get(); a.y = c.y.get(); a.z = c.z.get();
+    a.radii = c.radii.get();
+    a.flag = c.flag.get();
+    a.V = V.get();
+    a.F = F.get();
+    a.vdw = p.van_der_waals_dist;
+    a.tunnel = p.tunneling_dist;
+    a.n_gnps = (uint32_t)g.n;
+    a.n_visits = T;
+    counters.ensure(2);
+    DBuf<uint64_t> keys;
+    DBuf<uint32_t> ords;
+    int32_t h[2] = {0, 0};
+    // contact visits are a small share of all visits: start with a bounded buffer, rerun once at the exact size
+    long long cap = std::min<long long>(T, 1LL << 22);
+    for (int attempt = 0; attempt < 2; attempt++) {
+        keys.ensure(cap);
+        ords.ensure(cap);
+        a.keys = keys.get();
+        a.ords = ords.get();
+        a.cap = (int32_t)cap;
+        a.counters = counters.get();
+        CICY_CUDA(cudaMemsetAsync(counters.get(), 0, sizeof(int32_t) * 2, s));
+        k_mix_eval<<<blocks_for(T), 256, 0, s>>>(a);
+        CICY_LAUNCH_CHECK();
+        c.launches += 1;
+        CICY_CUDA(cudaMemcpyAsync(h, counters.get(), sizeof(int32_t) * 2, cudaMemcpyDeviceToHost, s));
+        CICY_CUDA(cudaStreamSynchronize(s));
+        if (h[0] <= cap) break;
+        cap = h[0];
+    }
+    if (inside_is_error && h[1] > 0)
+        throw Fail{CICY_E_INPUT, "Find_adjacent_labels: a CNT point in a mixed junction is inside a GNP"};
+    const int n = h[0];
+    if (n == 0) return 0;
+    radix_sort_pairs(keys.get(), ords.get(), n, bits_for((uint64_t)c.n_points * (uint64_t)g.n), c.rs, s, c.launches);
+    head.ensure(n);
+    pos.ensure(n);
+    total.ensure(1);
+    k_mix_heads<<<blocks_for(n), 256, 0, s>>>(n, keys.get(), head.get());
+    DBuf<int32_t> scan32;
+    exclusive_scan_i32(head.get(), pos.get(), n, total.get(), scan32, s, c.launches);
+    int U = 0;
+    CICY_CUDA(cudaMemcpyAsync(&U, total.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CICY_CUDA(cudaStreamSynchronize(s));
+    DBuf<uint64_t> first, upair;
+    DBuf<uint32_t> uidx;
+    first.ensure(U);
+    upair.ensure(U);
+    uidx.ensure(U);
+    k_mix_first<<<blocks_for(n), 256, 0, s>>>(n, keys.get(), ords.get(), head.get(), pos.get(), first.get(), uidx.get(), upair.get());
+    radix_sort_pairs(first.get(), uidx.get(), U, bits_for((uint64_t)T), c.rs, s, c.launches);
+    c.mix_point.ensure(U);
+    c.mix_gnp.ensure(U);
+    c.mix_dist.ensure(U);
+    c.mix_closest.ensure(3 * (size_t)U);
+    k_mix_out<<<blocks_for(U), 256, 0, s>>>(a, U, uidx.get(), upair.get(), c.mix_point.get(), c.mix_gnp.get(), c.mix_dist.get(),
+                                           c.mix_closest.get());
+    CICY_LAUNCH_CHECK();
+    c.launches += 4;
+    CICY_CUDA(cudaStreamSynchronize(s));
+    c.n_mix = U;
+    return U;
+}
 
 void gnp_sectioned_domain(const GnpSet& g, const std::vector<int32_t>& inside, const cicy_cuboid& w, const double gs_min[3],
                           double overlap_cnt, double overlap_gnp, GnpGrid& out) {

@@ -33,6 +33,7 @@ class Context:
         h = C.c_void_p()
         check(lib().cicy_ctx_create(C.byref(h), device), "cicy_ctx_create")
         self._h = h
+        self._device = device
         self._learned = False
 
     def close(self):
@@ -90,9 +91,41 @@ class Context:
     def upload(self, net: HostNetwork):
         v = net.view()
         self._check(lib().cicy_upload_network(self._h, C.byref(v)), "cicy_upload_network")
+        self._window = _abi.Cuboid(*[getattr(v.window, f) for f, _ in _abi.Cuboid._fields_])
 
     def contact_grid(self, p: _abi.Params):
         self._check(lib().cicy_contact_grid(self._h, C.byref(p)), "cicy_contact_grid")
+
+    def gnp_cnt_contacts(self, gnp_directory: str, p: _abi.Params, inside_is_error: bool = False):
+        """CNT-GNP contacts of the hybrid sample (cicy_gnp_cnt_contacts), after
+        contact_grid(p) on the uploaded CNT network: the GNPs of
+        gnp_directory/gnp_data.dat, all of them inside the network's window, on the
+        same region grid (Generate_contact_grid for GNP_CNT_mix, then
+        Find_adjacent_labels).  Returns (point, gnp, junction distance, closest GNP
+        point [n, 3]) by contact-point number."""
+        h = C.c_void_p()
+        check(lib().cicy_read_gnps(gnp_directory.encode(), C.byref(h)), "cicy_read_gnps")
+        grid = C.c_void_p()
+        try:
+            v = _abi.Gnps()
+            check(lib().cicy_gnp_set_view(h, C.byref(v)), "cicy_gnp_set_view")
+            ins = np.arange(v.n, dtype=np.int32)
+            gs = np.array(list(p.gs_min), dtype=np.float64)
+            check(lib().cicy_gnp_sectioned_domain(self._device, h, ins.ctypes.data_as(_abi.i32p), len(ins), C.byref(self._window),
+                                                  gs.ctypes.data_as(_abi.f64p), p.gs_overlap_cnt, p.gs_overlap_gnp, C.byref(grid)),
+                  "cicy_gnp_sectioned_domain")
+            n = C.c_int64()
+            self._check(lib().cicy_gnp_cnt_contacts(self._h, h, grid, C.byref(p), int(inside_is_error), C.byref(n)), "cicy_gnp_cnt_contacts")
+        finally:
+            if grid:
+                lib().cicy_gnp_grid_free(grid)
+            lib().cicy_gnp_set_free(h)
+        N = n.value
+        pt, g = np.zeros(max(N, 1), np.int64), np.zeros(max(N, 1), np.int32)
+        d, q = np.zeros(max(N, 1)), np.zeros((max(N, 1), 3))
+        self._check(lib().cicy_get_gnp_cnt_contacts(self._h, C.byref(n), _p(pt, C.c_int64), _p(g, C.c_int32), _p(d, C.c_double),
+                                                    _p(q, C.c_double)), "cicy_get_gnp_cnt_contacts")
+        return pt[:N], g[:N], d[:N], q[:N]
 
     def clusters(self, p: _abi.Params):
         self._check(lib().cicy_clusters(self._h, C.byref(p)), "cicy_clusters")

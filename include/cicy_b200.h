@@ -425,6 +425,26 @@ void cicy_gnp_grid_free(cicy_gnp_grid* g);
 cicy_status cicy_gnp_point_distance(int device, const cicy_gnp_set* gnps, int32_t n, const double* xyz, const int32_t* gnp, double* dist,
                                     double* closest, int32_t* flag);
 
+/* CNT-GNP contacts of the hybrid CNT/GNP sample on the device:
+ * Hoshen_Kopelman::Find_adjacent_labels (Hoshen_Kopelman.cpp:1989-2142) over
+ * Contact_grid::Generate_contact_grid with particle type GNP_CNT_mix.  The
+ * context holds the CNT network and its contact grid (cicy_upload_network,
+ * cicy_contact_grid with the hybrid overlaps); `grid` is the GNP part of the
+ * same grid (cicy_gnp_sectioned_domain with the same window, region sizes and
+ * overlaps; other regions: CICY_E_INPUT).  A (point, GNP) pair of a region is a
+ * contact when max(closest distance - CNT radius, van der Waals) is within the
+ * tunnelling cutoff (+1e-10); contacts are numbered in upstream's visiting
+ * order (regions, the region's GNPs, the region's points).  A point inside a
+ * GNP is no contact (upstream's ignore_eror_cnt_inside_gnp = 1), or, with
+ * inside_is_error = 1, fails with CICY_E_INPUT as upstream's default does.
+ * At most 2^31 point-GNP visits (CICY_E_CAPACITY). */
+cicy_status cicy_gnp_cnt_contacts(cicy_ctx* ctx, const cicy_gnp_set* gnps, const cicy_gnp_grid* grid, const cicy_params* p,
+                                  int32_t inside_is_error, int64_t* n_contacts);
+/* The contacts by contact-point number i: CNT point point[i], GNP gnp[i], junction
+ * distance dist[i] (point_contacts / point_contacts_dist) and the closest GNP point
+ * closest[3i..3i+2] (contact_points_gnp).  Size query: NULL buffers. */
+cicy_status cicy_get_gnp_cnt_contacts(cicy_ctx* ctx, int64_t* n, int64_t* point, int32_t* gnp, double* dist, double* closest);
+
 /* Wrap caller-owned arrays (copied) as a host network, e.g. a network read from files. */
 cicy_status cicy_host_network_from_arrays(const cicy_network* net, cicy_host_network** out);
 /* Borrowed view of a host network; valid until cicy_host_network_free. */

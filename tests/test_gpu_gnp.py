@@ -1,6 +1,7 @@
-"""GNP part of the contact grid on the device (cicy_gnp_sectioned_domain) against
-upstream's region lists (golden fixture made by the upstream program) and the
-CPU restatement (oracle/gnp_oracle.py) on another seed and a smaller window."""
+"""GNP part of the contact grid (cicy_gnp_sectioned_domain) and the CNT-GNP
+contact pass (cicy_gnp_cnt_contacts) on the device against upstream's region
+lists and contacts (golden fixture made by the upstream program) and the CPU
+restatement (oracle/gnp_oracle.py) on other seeds and smaller windows."""
 import os
 
 import numpy as np
@@ -56,3 +57,79 @@ def test_gnp_closest_point_matches_upstream_golden(cuda_ok, tmp_path):
     assert np.array_equal(flag, z["ref_query_flag"])
     assert np.array_equal(dist, z["ref_query_dist"])
     assert np.array_equal(closest.ravel(), z["ref_query_point"])
+
+
+def _hybrid_context_inputs(z, d):
+    import sys
+
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_gnp_golden as M
+
+    net = {k: v for k, v in M.hybrid_network(d).items() if not k.startswith("boundary")}
+    assert M.net_hash(net) == str(z["cnt_sha256"])
+    side, gs, ov_cnt, ov_gnp = float(z["meta"][1]), float(z["meta"][5]), float(z["meta"][6]), float(z["meta"][7])
+    net["cnts_inside"] = np.arange(len(net["radii"]), dtype=np.int32)
+    net["window"] = np.array([0.0, 0.0, 0.0, side, side, side, side, side, side])
+    write_gnp_file(d, {"l": z["in_l"], "t": z["in_t"], "theta": z["in_theta"], "phi": z["in_phi"], "center": z["in_center"]})
+    p = M.cnt_config().params()
+    for a in range(3):
+        p.gs_min[a] = gs
+    p.gs_overlap_cnt, p.gs_overlap_gnp = ov_cnt, ov_gnp
+    return net, p
+
+
+def test_gnp_cnt_contacts_match_upstream_golden(cuda_ok, tmp_path):
+    """The device CNT-GNP contact pass (cicy_gnp_cnt_contacts) gives upstream's
+    Find_adjacent_labels contacts on the hybrid fixture: the same (point, GNP)
+    pairs with the same contact-point numbers, junction distances and closest
+    GNP points, bit for bit; with inside points as errors it fails as upstream's
+    default does (the fixture has CNT points inside GNPs)."""
+    from cicy_geom_b200 import _abi
+    from cicy_geom_b200.device import Context
+    from cicy_geom_b200.network import HostNetwork
+
+    z = dict(np.load(GOLDEN))
+    d = str(tmp_path)
+    net, p = _hybrid_context_inputs(z, d)
+    with Context(0) as ctx:
+        ctx.upload(HostNetwork.from_arrays(net))
+        ctx.contact_grid(p)
+        pt, g, dist, q = ctx.gnp_cnt_contacts(d, p)
+        order = np.argsort(z["ref_mix_index"])
+        assert len(pt) == len(order) > 1000
+        assert np.array_equal(pt, z["ref_mix_point"][order]) and np.array_equal(g, z["ref_mix_gnp"][order])
+        assert np.array_equal(dist, z["ref_mix_dist"][order])
+        assert np.array_equal(q, z["ref_mix_contact_points"].reshape(-1, 3))
+        with pytest.raises(_abi.CicyError, match="inside a GNP"):
+            ctx.gnp_cnt_contacts(d, p, inside_is_error=True)
+
+
+def test_gnp_cnt_contacts_match_oracle_on_a_window(cuda_ok, tmp_path):
+    """A window of another hybrid sample (a subset of CNTs, region size 0.07 um):
+    the device pass against the CPU restatement (oracle/gnp_oracle.py)."""
+    from cicy_geom_b200.device import Context
+    from cicy_geom_b200.network import HostNetwork, NetworkConfig, generate_cnt_network
+    from oracle import cicy_oracle as O
+
+    d = str(tmp_path)
+    cfg = NetworkConfig(side=2.5, n_cnts=500, seed=4_000_555, gs_min=0.07)
+    net = {k: v for k, v in generate_cnt_network(cfg).arrays().items() if not k.startswith("boundary")}
+    net["cnts_inside"] = np.array([i for i in range(cfg.n_cnts) if i % 4 != 3], np.int32)
+    net["window"] = np.array([0.3, 0.4, 0.2, 1.9, 1.8, 2.1, 2.2, 2.2, 2.3])
+    gn = generate_gnps(70, cfg.side, 4_000_556)
+    write_gnp_file(d, gn)
+    p = cfg.params()
+    p.gs_overlap_gnp = 0.07 / np.sqrt(8.0)
+    with Context(0) as ctx:
+        ctx.upload(HostNetwork.from_arrays(net))
+        ctx.contact_grid(p)
+        pt, g, dist, q = ctx.gnp_cnt_contacts(d, p)
+    n, l, regs = O.contact_grid(net, {"gs_min": (0.07,) * 3, "gs_overlap_cnt": p.gs_overlap_cnt, "gs_overlap_gnp": p.gs_overlap_gnp})
+    V = read_gnps(d)
+    sd_gnp = G.fill_sectioned_domain_gnps(net["window"], V["vertices"], V["l"], V["t"], range(70), n, l, p.gs_overlap_gnp)
+    out = G.find_adjacent_labels(np.stack([net["x"], net["y"], net["z"]], 1).tolist(), net["flag"], net["radii"], regs, sd_gnp,
+                                 V["vertices"].tolist(), V["planes"].tolist(), p.van_der_waals_dist, p.tunneling_dist)
+    assert len(out) == len(pt) > 100
+    for i in range(len(pt)):
+        num, dj, c = out[(int(pt[i]), int(g[i]))]
+        assert num == i and dj == dist[i] and tuple(c) == tuple(q[i])
