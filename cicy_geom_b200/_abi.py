@@ -156,6 +156,20 @@ class Gnps(C.Structure):
     ]
 
 
+class GnpPairList(C.Structure):
+    _fields_ = [
+        ("n", C.c_int64),
+        ("n_visits", C.c_int64),
+        ("n_pairs", C.c_int64),
+        ("a", C.c_void_p),
+        ("b", C.c_void_p),
+        ("penetrating", C.c_void_p),
+        ("dist", C.c_void_p),
+        ("direction", C.c_void_p),
+        ("displacement", C.c_void_p),
+    ]
+
+
 class GenParams(C.Structure):
     _fields_ = [
         ("sample", Cuboid),
@@ -226,6 +240,10 @@ def lib() -> C.CDLL:
         "cicy_gnp_grid_view": (C.c_int, [C.c_void_p, i32p, f64p, P(C.c_void_p), P(C.c_void_p), i64p]),
         "cicy_gnp_grid_free": (None, [C.c_void_p]),
         "cicy_gnp_point_distance": (C.c_int, [C.c_int, C.c_void_p, C.c_int32, f64p, i32p, f64p, f64p, i32p]),
+        "cicy_gnp_pair_distance": (C.c_int, [C.c_int, C.c_void_p, C.c_int32, i32p, i32p, C.c_double, f64p, f64p, f64p, i32p]),
+        "cicy_gnp_contact_pairs": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_double, P(C.c_void_p)]),
+        "cicy_gnp_pairs_view": (C.c_int, [C.c_void_p, P(GnpPairList)]),
+        "cicy_gnp_pairs_free": (None, [C.c_void_p]),
         "cicy_gnp_cnt_contacts": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, P(Params), C.c_int32, i64p]),
         "cicy_get_gnp_cnt_contacts": (C.c_int, [C.c_void_p, i64p, i64p, i32p, f64p, f64p]),
         "cicy_host_network_view": (C.c_int, [C.c_void_p, P(Network)]),

@@ -45,6 +45,14 @@ struct GnpGrid {
 };
 void gnp_sectioned_domain(const GnpSet& g, const std::vector<int32_t>& inside, const cicy_cuboid& w, const double gs_min[3],
                           double overlap_cnt, double overlap_gnp, GnpGrid& out);
+// GNP-GNP contact pass (gnp_pairs.cu): pairs within the tunnelling cutoff in
+// upstream's visiting order, with distance, direction and the move of b.
+struct GnpPairs {
+    std::vector<int32_t> a, b, penetrating;
+    std::vector<double> dist, direction, displacement;  // 1, 3, 3 per pair
+    int64_t n_visits = 0, n_pairs = 0, launches = 0;
+};
+void gnp_contact_pairs(const GnpSet& g, const GnpGrid& grid, double vdw, double tunnel, GnpPairs& out);
 // Message returned by cicy_host_last_error() on this thread.
 void set_host_error(const std::string& msg);
 void host_network_view(const HostNetwork& h, cicy_network& v);
@@ -61,4 +69,8 @@ struct cicy_gnp_set {
 
 struct cicy_gnp_grid {
     cicy::GnpGrid grid;
+};
+
+struct cicy_gnp_pairs {
+    cicy::GnpPairs pairs;
 };

@@ -419,3 +419,64 @@ def gnp_closest_points(directory: str, xyz, gnp, device: int = 0):
         return dist, q, fl
     finally:
         lib().cicy_gnp_set_free(h)
+
+
+def gnp_pair_distance(directory: str, a, b, vdw: float, device: int = 0):
+    """Upstream's GNP-GNP distance step (Get_distance_between_GNPs: GJK, EPA when
+    the GNPs interpenetrate) on the device for pairs (a[i], b[i]) of the GNPs of
+    `directory`/gnp_data.dat (cicy_gnp_pair_distance): returns (dist[n],
+    direction[n, 3], displacement of b [n, 3], penetrating[n])."""
+    h = C.c_void_p()
+    check(lib().cicy_read_gnps(directory.encode(), C.byref(h)), "cicy_read_gnps")
+    try:
+        a = np.ascontiguousarray(a, dtype=np.int32)
+        b = np.ascontiguousarray(b, dtype=np.int32)
+        n = len(a)
+        if len(b) != n:
+            raise ValueError("a and b differ in length")
+        d, N, m, p = np.zeros(n), np.zeros((n, 3)), np.zeros((n, 3)), np.zeros(n, np.int32)
+        check(lib().cicy_gnp_pair_distance(device, h, n, a.ctypes.data_as(_abi.i32p), b.ctypes.data_as(_abi.i32p), float(vdw),
+                                           d.ctypes.data_as(_abi.f64p), N.ctypes.data_as(_abi.f64p), m.ctypes.data_as(_abi.f64p),
+                                           p.ctypes.data_as(_abi.i32p)), "cicy_gnp_pair_distance")
+        return d, N, m, p
+    finally:
+        lib().cicy_gnp_set_free(h)
+
+
+def gnp_contact_pairs(directory: str, inside, window, gs_min, overlap_cnt: float, overlap_gnp: float, vdw: float, tunnel: float,
+                      device: int = 0) -> dict:
+    """GNP-GNP contact pass of Label_gnps_in_window on the device: the GNP region
+    lists (cicy_gnp_sectioned_domain of `inside`) and every pair sharing a region,
+    measured once (cicy_gnp_contact_pairs).  Returns the pairs within the
+    tunnelling cutoff in upstream's visiting order: a, b, penetrating, dist,
+    direction [n, 3], displacement [n, 3], and the visit and pair counts."""
+    h = C.c_void_p()
+    check(lib().cicy_read_gnps(directory.encode(), C.byref(h)), "cicy_read_gnps")
+    grid, pairs = C.c_void_p(), C.c_void_p()
+    try:
+        ins = np.ascontiguousarray(inside, dtype=np.int32)
+        gs = np.ascontiguousarray(gs_min, dtype=np.float64)
+        w = _abi.Cuboid(*[float(x) for x in window])
+        check(lib().cicy_gnp_sectioned_domain(device, h, ins.ctypes.data_as(_abi.i32p), len(ins), C.byref(w), gs.ctypes.data_as(_abi.f64p),
+                                              float(overlap_cnt), float(overlap_gnp), C.byref(grid)), "cicy_gnp_sectioned_domain")
+        check(lib().cicy_gnp_contact_pairs(device, h, grid, float(vdw), float(tunnel), C.byref(pairs)), "cicy_gnp_contact_pairs")
+        v = _abi.GnpPairList()
+        check(lib().cicy_gnp_pairs_view(pairs, C.byref(v)), "cicy_gnp_pairs_view")
+        n = int(v.n)
+
+        def arr(ptr, ct, count, dt):
+            if count == 0:
+                return np.zeros(0, dt)
+            return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ct)), shape=(count,)).copy()
+
+        return {"a": arr(v.a, C.c_int32, n, np.int32), "b": arr(v.b, C.c_int32, n, np.int32),
+                "penetrating": arr(v.penetrating, C.c_int32, n, np.int32), "dist": arr(v.dist, C.c_double, n, np.float64),
+                "direction": arr(v.direction, C.c_double, 3 * n, np.float64).reshape(n, 3),
+                "displacement": arr(v.displacement, C.c_double, 3 * n, np.float64).reshape(n, 3),
+                "n_visits": int(v.n_visits), "n_pairs": int(v.n_pairs)}
+    finally:
+        if pairs:
+            lib().cicy_gnp_pairs_free(pairs)
+        if grid:
+            lib().cicy_gnp_grid_free(grid)
+        lib().cicy_gnp_set_free(h)

@@ -425,6 +425,47 @@ void cicy_gnp_grid_free(cicy_gnp_grid* g);
 cicy_status cicy_gnp_point_distance(int device, const cicy_gnp_set* gnps, int32_t n, const double* xyz, const int32_t* gnp, double* dist,
                                     double* closest, int32_t* flag);
 
+/* GNP-GNP distance on the device, Hoshen_Kopelman::Get_distance_between_GNPs
+ * (Hoshen_Kopelman.cpp:770-823): GJK distance (Collision_detection::GJK_distance,
+ * Collision_detection.cpp:751-1703) and, for interpenetrating GNPs, the EPA
+ * penetration depth and direction (:1704-1946), upstream's steps and FP64
+ * operation order, so the doubles equal upstream's.  Pair i is GNPs a[i], b[i]:
+ * dist[i] (the van der Waals distance when they interpenetrate), the direction
+ * direction[3i..] (GJK's last search direction, or EPA's face normal), the move
+ * of b displacement[3i..] (direction x (depth + vdw); 0 when separate) and
+ * penetrating[i].  A pair upstream fails on (GJK beyond 50 iterations) returns
+ * CICY_E_INPUT naming it; an EPA polytope beyond 72 vertices / 160 faces,
+ * CICY_E_CAPACITY. */
+cicy_status cicy_gnp_pair_distance(int device, const cicy_gnp_set* gnps, int32_t n, const int32_t* a, const int32_t* b, double vdw, double* dist,
+                                   double* direction, double* displacement, int32_t* penetrating);
+
+/* GNP-GNP contact pass of Hoshen_Kopelman::Label_gnps_in_window
+ * (Hoshen_Kopelman.cpp:626-767) on the device: every pair of GNPs sharing a
+ * region of `grid` (cicy_gnp_sectioned_domain), measured once; the pairs within
+ * the tunnelling cutoff (dist <= tunnel) in upstream's visiting order (regions,
+ * then j < k within the region, first visit), each as (a < b) with the results
+ * of cicy_gnp_pair_distance.  These are the pairs upstream passes on to
+ * Find_junction_points_for_gnps; the junction points and HK76 are not part of
+ * this call.  Upstream orders a pair as (min(GNP1, GNP2), GNP2); with region
+ * lists in ascending GNP order (an ascending `inside`) that is (a < b) too. */
+typedef struct cicy_gnp_pairs cicy_gnp_pairs;
+typedef struct {
+    int64_t n;                    /* contact pairs */
+    int64_t n_visits;             /* region pair visits */
+    int64_t n_pairs;              /* distinct pairs measured */
+    const int32_t* a;             /* [n] */
+    const int32_t* b;             /* [n] */
+    const int32_t* penetrating;   /* [n] */
+    const double* dist;           /* [n] */
+    const double* direction;      /* [3n] */
+    const double* displacement;   /* [3n] */
+} cicy_gnp_pair_list;
+cicy_status cicy_gnp_contact_pairs(int device, const cicy_gnp_set* gnps, const cicy_gnp_grid* grid, double vdw, double tunnel,
+                                   cicy_gnp_pairs** out);
+/* Borrowed view; valid until cicy_gnp_pairs_free. */
+cicy_status cicy_gnp_pairs_view(const cicy_gnp_pairs* p, cicy_gnp_pair_list* view);
+void cicy_gnp_pairs_free(cicy_gnp_pairs* p);
+
 /* CNT-GNP contacts of the hybrid CNT/GNP sample on the device:
  * Hoshen_Kopelman::Find_adjacent_labels (Hoshen_Kopelman.cpp:1989-2142) over
  * Contact_grid::Generate_contact_grid with particle type GNP_CNT_mix.  The

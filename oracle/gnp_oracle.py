@@ -226,3 +226,276 @@ def find_adjacent_labels(xyz, flag, radii, sd_cnt, sd_gnp, vertices, planes, vdw
                 if hit:
                     out[key] = (len(out), dj, q)
     return out
+
+
+# ---------------------------------------------------------------------------
+# GNP-GNP distance: GJK, EPA (Collision_detection.cpp:751-1946) as
+# Hoshen_Kopelman::Get_distance_between_GNPs combines them (Hoshen_Kopelman.cpp:770-823)
+
+
+def _scale(a, s):
+    return (a[0] * s, a[1] * s, a[2] * s)
+
+
+def _len2(a):
+    return a[0] * a[0] + a[1] * a[1] + a[2] * a[2]
+
+
+def _unit(a):
+    ln = math.sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2])
+    return (a[0] / ln, a[1] / ln, a[2] / ln)
+
+
+def _support_map(D, V):
+    """Support_map: the first vertex of largest D.v (strictly larger replaces)."""
+    best, k = _dot(D, V[0]), 0
+    for i in range(1, 8):
+        d = _dot(D, V[i])
+        if d - best > 0.0:
+            best, k = d, i
+    return V[k]
+
+
+def _support(D, VA, VB):
+    return _sub(_support_map(D, VA), _support_map(_scale(D, -1.0), VB))
+
+
+def _direction(S):
+    """Direction_from_simplex_to_origin (:872-914)."""
+    if len(S) == 1:
+        return _unit(_scale(S[0], -1.0))
+    if len(S) == 2:
+        AO, AB = _scale(S[0], -1.0), _sub(S[1], S[0])
+        return _unit(_cross(_cross(AB, AO), AB))
+    if len(S) == 3:
+        N = _unit(_cross(_sub(S[1], S[0]), _sub(S[2], S[0])))
+        return _scale(N, -1.0) if _dot(N, S[0]) > 0.0 else N
+    raise ValueError("Direction_from_simplex_to_origin: invalid simplex size")
+
+
+def _contained(S, A):
+    """Is_point_contained_in_simplex (:916-967)."""
+    if len(S) == 1:
+        return _dist(S[0], A) < ZERO
+    if len(S) == 2:
+        S0A, S0S1 = _sub(A, S[0]), _sub(S[1], S[0])
+        return _dot(_cross(_cross(S0S1, S0A), S0S1), S0A) < ZERO
+    if len(S) == 3:
+        N = _cross(_sub(S[1], S[0]), _sub(S[2], S[0]))
+        return abs(_dot(N, _sub(A, S[0]))) < ZERO
+    raise ValueError("Is_point_contained_in_simplex: invalid simplex size")
+
+
+def _distance(S):
+    """Distance_from_simplex_to_origin (:969-1010)."""
+    if len(S) == 1:
+        return math.sqrt(_len2(S[0]))
+    if len(S) == 2:
+        AO, AB = _scale(S[0], -1.0), _sub(S[1], S[0])
+        t = _dot(AO, AB)
+        return math.sqrt(_len2(AO) - t * t / _len2(AB))
+    if len(S) == 3:
+        return abs(_dot(_unit(_cross(_sub(S[1], S[0]), _sub(S[2], S[0]))), S[0]))
+    raise ValueError("Distance_from_simplex_to_origin: invalid simplex size")
+
+
+def _outer_normal(A, B, C, D):
+    """Normal_to_face_ouside_tetrahedron (:484-503)."""
+    n = _cross(_sub(B, A), _sub(C, A))
+    return _scale(n, -1.0) if _dot(n, _sub(D, A)) > 0.0 else n
+
+
+def _edge_normal(edge, face_n, ref, flip_if_positive):
+    n = _cross(edge, face_n)
+    t = _dot(n, ref)
+    return _scale(n, -1.0) if (t > 0.0 if flip_if_positive else t < 0.0) else n
+
+
+def _triangle(S):
+    """Voroni_region_case3 (:1068-1206): the triangle's feature closest to the origin."""
+    s0, s1, s2 = S
+    S0S1, S0S2 = _sub(s1, s0), _sub(s2, s0)
+    a01, a02 = -_dot(s0, S0S1), -_dot(s0, S0S2)
+    if a02 < 0.0 and a01 < 0.0:
+        return [s0]
+    S1S2 = _sub(s2, s1)
+    b10, b12 = _dot(s1, S0S1), -_dot(s1, S1S2)
+    if b10 < 0.0 and b12 < 0.0:
+        return [s1]
+    c20, c21 = _dot(s2, S0S2), _dot(s2, S1S2)
+    if c20 < 0.0 and c21 < 0.0:
+        return [s2]
+    NT = _cross(S0S1, S0S2)
+    if -_dot(s0, _edge_normal(S0S1, NT, S1S2, True)) > 0.0 and a01 > 0.0 and b10 > 0.0:
+        return [s0, s1]
+    if -_dot(s0, _edge_normal(S0S2, NT, S0S1, True)) > 0.0 and a02 > 0.0 and c20 > 0.0:
+        return [s0, s2]
+    if -_dot(s1, _edge_normal(S1S2, NT, S0S1, False)) > 0.0 and b12 > 0.0 and c21 > 0.0:
+        return [s1, s2]
+    return S
+
+
+def _tetrahedron(S):
+    """Voroni_region_case4 (:1211-1654): the tetrahedron's feature closest to the
+    origin, or None when the origin is inside it."""
+    s0, s1, s2, s3 = S
+    S0S1, S0S2, S0S3 = _sub(s1, s0), _sub(s2, s0), _sub(s3, s0)
+    a01, a02, a03 = -_dot(s0, S0S1), -_dot(s0, S0S2), -_dot(s0, S0S3)
+    if a02 < 0.0 and a01 < 0.0 and a03 < 0.0:
+        return [s0]
+    S1S2, S1S3 = _sub(s2, s1), _sub(s3, s1)
+    b10, b12, b13 = _dot(s1, S0S1), -_dot(s1, S1S2), -_dot(s1, S1S3)
+    if b10 < 0.0 and b12 < 0.0 and b13 < 0.0:
+        return [s1]
+    S2S3 = _sub(s3, s2)
+    c20, c21, c23 = _dot(s2, S0S2), _dot(s2, S1S2), -_dot(s2, S2S3)
+    if c20 < 0.0 and c21 < 0.0 and c23 < 0.0:
+        return [s2]
+    d30, d31, d32 = _dot(s3, S0S3), _dot(s3, S1S3), _dot(s3, S2S3)
+    if d30 < 0.0 and d31 < 0.0 and d32 < 0.0:
+        return [s3]
+    N013, N012 = _outer_normal(s0, s1, s3, s2), _outer_normal(s0, s1, s2, s3)
+    e01a = -_dot(s0, _edge_normal(S0S1, N012, S0S2, True))
+    e01b = -_dot(s0, _edge_normal(S0S1, N013, S0S3, True))
+    if a01 > 0.0 and b10 > 0.0 and e01a > 0.0 and e01b > 0.0:
+        return [s0, s1]
+    N023 = _outer_normal(s0, s2, s3, s1)
+    e02a = -_dot(s0, _edge_normal(S0S2, N012, S0S1, True))
+    e02b = -_dot(s0, _edge_normal(S0S2, N023, S0S3, True))
+    if a02 > 0.0 and c20 > 0.0 and e02a > 0.0 and e02b > 0.0:
+        return [s0, s2]
+    e03a = -_dot(s0, _edge_normal(S0S3, N013, S0S1, True))
+    e03b = -_dot(s0, _edge_normal(S0S3, N023, S0S2, True))
+    if a03 > 0.0 and d30 > 0.0 and e03a > 0.0 and e03b > 0.0:
+        return [s0, s3]
+    N123 = _outer_normal(s1, s2, s3, s0)
+    e12a = -_dot(s1, _edge_normal(S1S2, N012, S0S1, False))
+    e12b = -_dot(s1, _edge_normal(S1S2, N123, S1S3, True))
+    if b12 > 0.0 and c21 > 0.0 and e12a > 0.0 and e12b > 0.0:
+        return [s1, s2]
+    e13a = -_dot(s1, _edge_normal(S1S3, N013, S0S1, False))
+    e13b = -_dot(s1, _edge_normal(S1S3, N123, S1S2, True))
+    if b13 > 0.0 and d31 > 0.0 and e13a > 0.0 and e13b > 0.0:
+        return [s1, s3]
+    e23a = -_dot(s2, _edge_normal(S2S3, N023, S0S2, False))
+    e23b = -_dot(s2, _edge_normal(S2S3, N123, S1S2, False))
+    if c23 > 0.0 and d32 > 0.0 and e23a > 0.0 and e23b > 0.0:
+        return [s2, s3]
+    if -_dot(s0, N012) > 0.0 and e01a < 0.0 and e02a < 0.0 and e12a < 0.0:
+        return [s0, s1, s2]
+    if -_dot(s0, N023) > 0.0 and e02b < 0.0 and e03b < 0.0 and e23a < 0.0:
+        return [s0, s3, s2]
+    if -_dot(s0, N013) > 0.0 and e01b < 0.0 and e13a < 0.0 and e03a < 0.0:
+        return [s0, s1, s3]
+    if -_dot(s1, N123) > 0.0 and e12b < 0.0 and e13b < 0.0 and e23b < 0.0:
+        return [s3, s1, s2]
+    return None
+
+
+def _reduce(S):
+    """Find_voroni_region (:1012-1063); None when the origin is inside."""
+    if len(S) == 2:
+        S0S1 = _sub(S[1], S[0])
+        d0, d1 = -_dot(S[0], S0S1), _dot(S[1], S0S1)
+        if d0 > 0.0 and d1 > 0.0:
+            return S
+        return [S[1]] if d1 < 0.0 else [S[0]]
+    if len(S) == 3:
+        return _triangle(S)
+    if len(S) == 4:
+        return _tetrahedron(S)
+    return S
+
+
+def gjk_distance(VA, VB):
+    """GJK_distance (:751-870) from an empty simplex: (distance, direction,
+    penetrating, simplex); on interpenetration the simplex is the tetrahedron
+    that encloses the origin."""
+    S = [_sub(VA[0], VB[0])]
+    d = _distance(S)
+    for _ in range(50):
+        D = _direction(S)
+        A = _support(D, VA, VB)
+        if _contained(S, A):
+            return d, D, False, S
+        T = S + [A]
+        S = _reduce(T)
+        if S is None:
+            return None, None, True, T
+        d = _distance(S)
+        if abs(d - abs(_dot(A, D))) < ZERO:
+            return d, D, False, S
+    raise RuntimeError("GJK_distance: maximum number of iterations reached")
+
+
+def _face_plane(P, f):
+    """Normal_and_distance_to_origin (:1785-1812)."""
+    N = _unit(_cross(_sub(P[f[1]], P[f[0]]), _sub(P[f[2]], P[f[0]])))
+    sd = _dot(N, _scale(P[f[0]], -1.0))
+    return (_scale(N, -1.0) if sd > 0.0 else N), abs(sd)
+
+
+def epa(VA, VB, tetra):
+    """EPA (:1704-1780) with Reconstruct_simplex (:1849-1945): (depth, direction)."""
+    P = list(tetra)
+    faces = [(0, 1, 2), (0, 1, 3), (0, 2, 3), (1, 2, 3)]
+    planes = [_face_plane(P, f) for f in faces]
+    while True:
+        k = 0
+        for i in range(1, len(faces)):
+            if planes[i][1] < planes[k][1]:
+                k = i
+        N, pd = planes[k]
+        s = _support(N, VA, VB)
+        if _dot(s, N) - pd < ZERO:
+            return pd, N
+        P.append(s)
+        S = len(P) - 1
+        seen = [i for i in range(len(faces)) if _dot(planes[i][0], _sub(P[S], P[faces[i][0]])) > 0.0]
+        f0 = faces[seen[0]]
+        edges = [(f0[0], f0[1]), (f0[1], f0[2]), (f0[2], f0[0])]
+        for i in seen[1:]:
+            f = faces[i]
+            for e in ((f[0], f[1]), (f[1], f[2]), (f[2], f[0])):
+                hit = next((m for m, g in enumerate(edges) if g == e or g == (e[1], e[0])), -1)
+                if hit < 0:
+                    edges.append(e)
+                else:
+                    del edges[hit]
+        keep = [i for i in range(len(faces)) if i not in set(seen)]
+        faces = [faces[i] for i in keep]
+        planes = [planes[i] for i in keep]
+        for e in edges:
+            faces.append((S, e[0], e[1]))
+            planes.append(_face_plane(P, faces[-1]))
+
+
+def pair_distance(VA, VB, vdw: float):
+    """Get_distance_between_GNPs: (dist, direction, displacement of B, penetrating)."""
+    VA = [tuple(float(c) for c in v) for v in VA]
+    VB = [tuple(float(c) for c in v) for v in VB]
+    d, N, pen, S = gjk_distance(VA, VB)
+    if not pen:
+        return d, N, (0.0, 0.0, 0.0), False
+    depth, N = epa(VA, VB, S)
+    return vdw, N, _scale(N, depth + vdw), True
+
+
+def contact_pairs(sd_gnp, vertices, vdw: float, tunnel: float):
+    """GNP-GNP pairs of Label_gnps_in_window (Hoshen_Kopelman.cpp:626-767) within the
+    tunnelling cutoff, in upstream's visiting order (regions, then j < k in the
+    region; a pair measured at its first visit): list of (a, b, dist, direction,
+    displacement, penetrating), a pair ordered (min, max)."""
+    visited = set()
+    out = []
+    for gs in sd_gnp:
+        for j in range(len(gs) - 1):
+            for k in range(j + 1, len(gs)):
+                a, b = min(gs[j], gs[k]), max(gs[j], gs[k])
+                if (a, b) in visited:
+                    continue
+                visited.add((a, b))
+                d, N, m, pen = pair_distance(vertices[a], vertices[b], vdw)
+                if d <= tunnel:
+                    out.append((a, b, d, N, m, pen))
+    return out

@@ -201,3 +201,41 @@ def test_mixed_contacts_oracle_matches_upstream_live(tmp_path):
     assert len(ref) > 200 and {k: v[:2] for k, v in out.items()} == ref
     cp = z["mix_contact_points"].reshape(-1, 3)
     assert all(tuple(v[2]) == tuple(cp[v[0]]) for v in out.values())
+
+
+def test_gnp_distance_oracle_matches_upstream_golden():
+    """The CPU restatement of upstream's GNP-GNP distance step (GJK, EPA for the
+    interpenetrating pairs, the move apart) gives upstream's doubles on every
+    candidate pair of the fixture."""
+    from oracle import gnp_oracle as G
+
+    z = golden()
+    V = z["ref_gnp_vertices"].reshape(-1, 8, 3).tolist()
+    vdw = float(z["meta"][3])
+    for i, (a, b) in enumerate(zip(z["ref_pair_a"], z["ref_pair_b"])):
+        d, N, m, p = G.pair_distance(V[a], V[b], vdw)
+        assert int(p) == z["ref_pair_penetrating"][i] and d == z["ref_pair_dist"][i]
+        assert tuple(N) == tuple(z["ref_pair_direction"][3 * i:3 * i + 3])
+        assert tuple(m) == tuple(z["ref_pair_displacement"][3 * i:3 * i + 3])
+
+
+def test_gnp_contact_pairs_oracle_agrees_with_upstream_golden():
+    """The restated GNP-GNP contact pass of Label_gnps_in_window over upstream's
+    region lists: exactly the fixture's pairs within the tunnelling cutoff that
+    share a region, each once, with upstream's distances."""
+    from oracle import gnp_oracle as G
+
+    z = golden()
+    V = z["ref_gnp_vertices"].reshape(-1, 8, 3).tolist()
+    sp, si = z["ref_sd_ptr"], z["ref_sd_idx"]
+    sd = [si[sp[k]:sp[k + 1]].tolist() for k in range(len(sp) - 1)]
+    vdw, tunnel = float(z["meta"][3]), float(z["meta"][4])
+    out = G.contact_pairs(sd, V, vdw, tunnel)
+    ref = {(int(a), int(b)): i for i, (a, b) in enumerate(zip(z["ref_pair_a"], z["ref_pair_b"]))}
+    shared = {(min(g[j], g[k]), max(g[j], g[k])) for g in sd for j in range(len(g)) for k in range(j + 1, len(g))}
+    within = {k for k, i in ref.items() if z["ref_pair_dist"][i] <= tunnel}
+    assert {(a, b) for a, b, *_ in out} == within & shared and len(out) == len(within & shared) > 500
+    for a, b, d, N, m, p in out:
+        i = ref[(a, b)]
+        assert d == z["ref_pair_dist"][i] and int(p) == z["ref_pair_penetrating"][i]
+        assert tuple(N) == tuple(z["ref_pair_direction"][3 * i:3 * i + 3])

@@ -133,3 +133,46 @@ def test_gnp_cnt_contacts_match_oracle_on_a_window(cuda_ok, tmp_path):
     for i in range(len(pt)):
         num, dj, c = out[(int(pt[i]), int(g[i]))]
         assert num == i and dj == dist[i] and tuple(c) == tuple(q[i])
+
+
+def test_gnp_pair_distance_matches_upstream_golden(cuda_ok, tmp_path):
+    """Device GJK / EPA (cicy_gnp_pair_distance) against upstream's distance step on
+    the fixture's 2,358 candidate pairs (550 interpenetrating), bit for bit."""
+    from cicy_geom_b200.network import gnp_pair_distance
+
+    z = dict(np.load(GOLDEN))
+    write_gnp_file(str(tmp_path), {"l": z["in_l"], "t": z["in_t"], "theta": z["in_theta"], "phi": z["in_phi"], "center": z["in_center"]})
+    d, N, m, p = gnp_pair_distance(str(tmp_path), z["ref_pair_a"], z["ref_pair_b"], float(z["meta"][3]))
+    assert np.array_equal(p, z["ref_pair_penetrating"]) and np.array_equal(d, z["ref_pair_dist"])
+    assert np.array_equal(N.ravel(), z["ref_pair_direction"]) and np.array_equal(m.ravel(), z["ref_pair_displacement"])
+
+
+def test_gnp_contact_pairs_match_oracle(cuda_ok, tmp_path):
+    """Device GNP-GNP contact pass (cicy_gnp_contact_pairs) against the CPU
+    restatement: the fixture (upstream's region lists) and a window of another
+    seed with a subset of the GNPs; same pairs, order and doubles."""
+    from cicy_geom_b200.network import gnp_contact_pairs
+
+    z = dict(np.load(GOLDEN))
+    side, gs, ov_cnt, ov_gnp = float(z["meta"][1]), float(z["meta"][5]), float(z["meta"][6]), float(z["meta"][7])
+    vdw, tunnel = float(z["meta"][3]), float(z["meta"][4])
+    cases = []
+    d1 = os.path.join(str(tmp_path), "a")
+    os.makedirs(d1)
+    write_gnp_file(d1, {"l": z["in_l"], "t": z["in_t"], "theta": z["in_theta"], "phi": z["in_phi"], "center": z["in_center"]})
+    cases.append((d1, np.arange(len(z["in_l"])), [0.0, 0.0, 0.0, side, side, side, side, side, side], gs))
+    d2 = os.path.join(str(tmp_path), "b")
+    os.makedirs(d2)
+    write_gnp_file(d2, generate_gnps(150, 2.5, 4_000_777))
+    cases.append((d2, np.array([i for i in range(150) if i % 5 != 2]), [0.2, 0.3, 0.1, 2.0, 1.9, 2.2, 2.2, 2.2, 2.3], 0.07))
+    for d, inside, win, g in cases:
+        ov = g / np.sqrt(8.0)
+        out = gnp_contact_pairs(d, inside, win, [g] * 3, ov_cnt, ov, vdw, tunnel)
+        n, l = G.region_grid(win, [g] * 3, ov_cnt, ov)
+        V = read_gnps(d)
+        sd = G.fill_sectioned_domain_gnps(win, V["vertices"], V["l"], V["t"], inside, n, l, ov)
+        ref = G.contact_pairs(sd, V["vertices"].tolist(), vdw, tunnel)
+        assert len(out["a"]) == len(ref) > 50
+        for i, (a, b, dd, N, m, p) in enumerate(ref):
+            assert (out["a"][i], out["b"][i], out["penetrating"][i]) == (a, b, int(p)) and out["dist"][i] == dd
+            assert tuple(out["direction"][i]) == tuple(N) and tuple(out["displacement"][i]) == tuple(m)
