@@ -167,6 +167,9 @@ class GnpPairList(C.Structure):
         ("dist", C.c_void_p),
         ("direction", C.c_void_p),
         ("displacement", C.c_void_p),
+        ("point_a", C.c_void_p),
+        ("point_b", C.c_void_p),
+        ("outside", C.c_void_p),
     ]
 
 
@@ -241,7 +244,10 @@ def lib() -> C.CDLL:
         "cicy_gnp_grid_free": (None, [C.c_void_p]),
         "cicy_gnp_point_distance": (C.c_int, [C.c_int, C.c_void_p, C.c_int32, f64p, i32p, f64p, f64p, i32p]),
         "cicy_gnp_pair_distance": (C.c_int, [C.c_int, C.c_void_p, C.c_int32, i32p, i32p, C.c_double, f64p, f64p, f64p, i32p]),
-        "cicy_gnp_contact_pairs": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_double, P(C.c_void_p)]),
+        "cicy_gnp_junction_points": (C.c_int, [C.c_int, C.c_void_p, C.c_int32, i32p, i32p, C.c_double, P(Cuboid), C.c_int32, f64p, f64p,
+                                               i32p, i32p]),
+        "cicy_gnp_contact_pairs": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_double, P(Cuboid), C.c_int32,
+                                             P(C.c_void_p)]),
         "cicy_gnp_pairs_view": (C.c_int, [C.c_void_p, P(GnpPairList)]),
         "cicy_gnp_pairs_free": (None, [C.c_void_p]),
         "cicy_gnp_cnt_contacts": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, P(Params), C.c_int32, i64p]),

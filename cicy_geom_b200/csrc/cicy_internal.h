@@ -50,9 +50,12 @@ void gnp_sectioned_domain(const GnpSet& g, const std::vector<int32_t>& inside, c
 struct GnpPairs {
     std::vector<int32_t> a, b, penetrating;
     std::vector<double> dist, direction, displacement;  // 1, 3, 3 per pair
+    std::vector<double> point_a, point_b;               // junction points, 3 per pair
+    std::vector<int32_t> outside;                       // 1: point_a outside the sample, 2: point_b
     int64_t n_visits = 0, n_pairs = 0, launches = 0;
 };
-void gnp_contact_pairs(const GnpSet& g, const GnpGrid& grid, double vdw, double tunnel, GnpPairs& out);
+void gnp_contact_pairs(const GnpSet& g, const GnpGrid& grid, double vdw, double tunnel, const cicy_cuboid& sample, bool allow_simplex3,
+                       GnpPairs& out);
 // Message returned by cicy_host_last_error() on this thread.
 void set_host_error(const std::string& msg);
 void host_network_view(const HostNetwork& h, cicy_network& v);

@@ -1,7 +1,8 @@
 // GNP-GNP distances on the device (gnp_gjk.cuh: GJK, EPA for interpenetrating
 // GNPs, Hoshen_Kopelman::Get_distance_between_GNPs) for explicit pairs, and the
 // GNP-GNP contact pass of Hoshen_Kopelman::Label_gnps_in_window
-// (Hoshen_Kopelman.cpp:626-767) over the GNP region lists.
+// (Hoshen_Kopelman.cpp:626-767) over the GNP region lists, with the junction
+// points of each contact (gnp_junction.cuh).
 //
 // Upstream visits, region by region, every pair j < k of the region's GNPs and
 // measures a pair the first time it meets it (a visited set); a pair within
@@ -21,6 +22,7 @@
 #include "cicy_internal.h"
 #include "dev_common.cuh"
 #include "gnp_gjk.cuh"
+#include "gnp_junction.cuh"
 
 namespace cicy {
 namespace {
@@ -48,6 +50,39 @@ __global__ void __launch_bounds__(kPairThreads) k_pair_distance(int n, const int
         disp[3 * i + 1] = m.y;
         disp[3 * i + 2] = m.z;
         pen[i] = p ? 1 : 0;
+    }
+}
+
+struct Box {
+    double lo[3], hi[3];
+};
+Box box_of(const cicy_cuboid& c) { return Box{{c.min_x, c.min_y, c.min_z}, {c.max_x, c.max_y, c.max_z}}; }
+
+// Junction step of Label_gnps_in_window for pair i (Hoshen_Kopelman.cpp:712-746):
+// the second GNP moved apart when the pair interpenetrates, the two junction
+// points, the point on the second GNP moved back, and which points lie outside
+// the sample (1: a's, 2: b's).  Pairs with skip[i] set are left alone.
+__global__ void __launch_bounds__(kPairThreads) k_pair_junction(int n, const int32_t* __restrict__ a, const int32_t* __restrict__ b,
+                                                                const double* __restrict__ V, const double* __restrict__ F,
+                                                                const double* __restrict__ dist, const double* __restrict__ dir,
+                                                                const double* __restrict__ disp, const int32_t* __restrict__ pen,
+                                                                const int32_t* __restrict__ take, Box box, int allow3,
+                                                                double* __restrict__ pa, double* __restrict__ pb,
+                                                                int32_t* __restrict__ outside, int32_t* __restrict__ status) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (take && !take[i]) continue;
+        gnp::Cuboid8 A, B;
+        gnp::load_cuboid(V + 24 * (size_t)a[i], F + 24 * (size_t)a[i], A);
+        const gnp::P3 m{disp[3 * i], disp[3 * i + 1], disp[3 * i + 2]};
+        if (pen[i]) gnp::moved_cuboid(V + 24 * (size_t)b[i], m, B);
+        else gnp::load_cuboid(V + 24 * (size_t)b[i], F + 24 * (size_t)b[i], B);
+        gnp::P3 PA{0.0, 0.0, 0.0}, PB{0.0, 0.0, 0.0};
+        const int st = gnp::junction_points(A, B, gnp::P3{dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]}, dist[i], allow3 != 0, PA, PB);
+        if (st == gnp::kJuncOk && pen[i]) PB = gnp::sub(PB, m);
+        pa[3 * i] = PA.x; pa[3 * i + 1] = PA.y; pa[3 * i + 2] = PA.z;
+        pb[3 * i] = PB.x; pb[3 * i + 1] = PB.y; pb[3 * i + 2] = PB.z;
+        outside[i] = st == gnp::kJuncOk ? (gnp::outside_box(PA, box.lo, box.hi) ? 1 : 0) + (gnp::outside_box(PB, box.lo, box.hi) ? 2 : 0) : -1;
+        status[i] = st;
     }
 }
 
@@ -127,13 +162,24 @@ const char* status_text(int s) {
 
 // Distances of explicit pairs on the device; throws on the first failing pair.
 struct PairBufs {
-    DBuf<int32_t> a, b, pen, status;
-    DBuf<double> dist, dir, disp;
+    DBuf<int32_t> a, b, pen, status, outside, jstatus;
+    DBuf<double> dist, dir, disp, pa, pb;
     void ensure(size_t n) {
-        a.ensure(n); b.ensure(n); pen.ensure(n); status.ensure(n);
-        dist.ensure(n); dir.ensure(3 * n); disp.ensure(3 * n);
+        a.ensure(n); b.ensure(n); pen.ensure(n); status.ensure(n); outside.ensure(n); jstatus.ensure(n);
+        dist.ensure(n); dir.ensure(3 * n); disp.ensure(3 * n); pa.ensure(3 * n); pb.ensure(3 * n);
     }
 };
+
+const char* junction_text(int s) {
+    switch (s) {
+        case gnp::kJuncBadSimplex: return "the closest features have a vertex count upstream rejects";
+        case gnp::kJuncNoIntersection: return "an edge meets a face edge outside [0, 1]";
+        case gnp::kJuncNoInsideVertex: return "no vertex of one face lies inside the other";
+        case gnp::kJuncNoEdge: return "no face edge for the two-intersection average";
+        case gnp::kJuncBadFace: return "a vertex sum names no face";
+        default: return "unknown";
+    }
+}
 
 void check_pair_status(int n, const int32_t* d_status, const int32_t* d_a, const int32_t* d_b) {
     std::vector<int32_t> st(n), a(n), b(n);
@@ -150,7 +196,8 @@ void check_pair_status(int n, const int32_t* d_status, const int32_t* d_a, const
 
 }  // namespace
 
-void gnp_contact_pairs(const GnpSet& g, const GnpGrid& grid, double vdw, double tunnel, GnpPairs& out) {
+void gnp_contact_pairs(const GnpSet& g, const GnpGrid& grid, double vdw, double tunnel, const cicy_cuboid& sample, bool allow_simplex3,
+                       GnpPairs& out) {
     out = GnpPairs{};
     const int R = (int)grid.ptr.size() - 1;
     if (R < 0 || grid.ptr[R] != (int32_t)grid.idx.size()) throw Fail{CICY_E_INPUT, "cicy_gnp_contact_pairs: the GNP grid has no region lists"};
@@ -165,10 +212,12 @@ void gnp_contact_pairs(const GnpSet& g, const GnpGrid& grid, double vdw, double 
     DBuf<int32_t> gptr, gidx, head, pos, total, flag;
     DBuf<int64_t> npairs, off, tot64, scan64;
     DBuf<int32_t> scan32;
-    DBuf<double> V;
+    DBuf<double> V, F;
     gptr.ensure(R + 1);
     gidx.ensure(grid.idx.size());
     V.ensure(24 * (size_t)g.n);
+    F.ensure(24 * (size_t)g.n);
+    CICY_CUDA(cudaMemcpy(F.get(), g.planes.data(), sizeof(double) * 24 * g.n, cudaMemcpyHostToDevice));
     CICY_CUDA(cudaMemcpy(gptr.get(), grid.ptr.data(), sizeof(int32_t) * (R + 1), cudaMemcpyHostToDevice));
     CICY_CUDA(cudaMemcpy(gidx.get(), grid.idx.data(), sizeof(int32_t) * grid.idx.size(), cudaMemcpyHostToDevice));
     CICY_CUDA(cudaMemcpy(V.get(), g.vertices.data(), sizeof(double) * 24 * g.n, cudaMemcpyHostToDevice));
@@ -211,6 +260,11 @@ void gnp_contact_pairs(const GnpSet& g, const GnpGrid& grid, double vdw, double 
     DBuf<int32_t> fpos;
     fpos.ensure(U);
     k_within<<<pair_blocks(U, 256), 256, 0, s>>>(U, pb.dist.get(), tunnel, flag.get());
+    k_pair_junction<<<pair_blocks(U, kPairThreads), kPairThreads, 0, s>>>(U, pb.a.get(), pb.b.get(), V.get(), F.get(), pb.dist.get(), pb.dir.get(),
+                                                                          pb.disp.get(), pb.pen.get(), flag.get(), box_of(sample),
+                                                                          allow_simplex3 ? 1 : 0, pb.pa.get(), pb.pb.get(), pb.outside.get(),
+                                                                          pb.jstatus.get());
+    CICY_LAUNCH_CHECK();
     exclusive_scan_i32(flag.get(), fpos.get(), U, total.get(), scan32, s, launches);
     int C = 0;
     CICY_CUDA(cudaMemcpy(&C, total.get(), sizeof(int32_t), cudaMemcpyDeviceToHost));
@@ -226,7 +280,12 @@ void gnp_contact_pairs(const GnpSet& g, const GnpGrid& grid, double vdw, double 
     radix_sort_pairs(ckeys.get(), cvals.get(), C, bits_for((uint64_t)T), rs, s, launches);
     std::vector<uint32_t> order(C);
     std::vector<int32_t> a(U), b(U), pen(U);
-    std::vector<double> dist(U), dir(3 * (size_t)U), disp(3 * (size_t)U);
+    std::vector<double> dist(U), dir(3 * (size_t)U), disp(3 * (size_t)U), pa(3 * (size_t)U), pbv(3 * (size_t)U);
+    std::vector<int32_t> outside(U), jst(U);
+    CICY_CUDA(cudaMemcpy(pa.data(), pb.pa.get(), sizeof(double) * 3 * U, cudaMemcpyDeviceToHost));
+    CICY_CUDA(cudaMemcpy(pbv.data(), pb.pb.get(), sizeof(double) * 3 * U, cudaMemcpyDeviceToHost));
+    CICY_CUDA(cudaMemcpy(outside.data(), pb.outside.get(), sizeof(int32_t) * U, cudaMemcpyDeviceToHost));
+    CICY_CUDA(cudaMemcpy(jst.data(), pb.jstatus.get(), sizeof(int32_t) * U, cudaMemcpyDeviceToHost));
     CICY_CUDA(cudaMemcpy(order.data(), cvals.get(), sizeof(uint32_t) * C, cudaMemcpyDeviceToHost));
     CICY_CUDA(cudaMemcpy(a.data(), pb.a.get(), sizeof(int32_t) * U, cudaMemcpyDeviceToHost));
     CICY_CUDA(cudaMemcpy(b.data(), pb.b.get(), sizeof(int32_t) * U, cudaMemcpyDeviceToHost));
@@ -235,7 +294,14 @@ void gnp_contact_pairs(const GnpSet& g, const GnpGrid& grid, double vdw, double 
     CICY_CUDA(cudaMemcpy(dir.data(), pb.dir.get(), sizeof(double) * 3 * U, cudaMemcpyDeviceToHost));
     CICY_CUDA(cudaMemcpy(disp.data(), pb.disp.get(), sizeof(double) * 3 * U, cudaMemcpyDeviceToHost));
     out.launches = launches + 9;
+    for (uint32_t i : order)  // upstream stops at the first pair whose junction step fails
+        if (jst[i] != gnp::kJuncOk)
+            throw Fail{CICY_E_INPUT, "Find_junction_points_for_gnps: GNPs " + std::to_string(a[i]) + " and " + std::to_string(b[i]) + ": " +
+                                         junction_text(jst[i])};
     for (uint32_t i : order) {
+        out.point_a.insert(out.point_a.end(), {pa[3 * i], pa[3 * i + 1], pa[3 * i + 2]});
+        out.point_b.insert(out.point_b.end(), {pbv[3 * i], pbv[3 * i + 1], pbv[3 * i + 2]});
+        out.outside.push_back(outside[i]);
         out.a.push_back(a[i]);
         out.b.push_back(b[i]);
         out.penetrating.push_back(pen[i]);
@@ -287,9 +353,54 @@ cicy_status cicy_gnp_pair_distance(int device, const cicy_gnp_set* gnps, int32_t
     return CICY_OK;
 }
 
+cicy_status cicy_gnp_junction_points(int device, const cicy_gnp_set* gnps, int32_t n, const int32_t* a, const int32_t* b, double vdw,
+                                     const cicy_cuboid* sample, int32_t allow_simplex3, double* point_a, double* point_b, int32_t* outside,
+                                     int32_t* status) {
+    if (!gnps || !sample || n < 0 || (n > 0 && (!a || !b || !point_a || !point_b || !outside || !status)) || !(vdw >= 0)) {
+        cicy::set_host_error("cicy_gnp_junction_points: invalid arguments");
+        return CICY_E_INPUT;
+    }
+    for (int i = 0; i < n; i++)
+        if (a[i] < 0 || a[i] >= gnps->g.n || b[i] < 0 || b[i] >= gnps->g.n) {
+            cicy::set_host_error("cicy_gnp_junction_points: GNP index out of range in pair " + std::to_string(i));
+            return CICY_E_INPUT;
+        }
+    if (n == 0) return CICY_OK;
+    try {
+        CICY_CUDA(cudaSetDevice(device));
+        const cicy::GnpSet& g = gnps->g;
+        cicy::PairBufs pb;
+        cicy::DBuf<double> V, F;
+        pb.ensure(n);
+        V.ensure(24 * (size_t)g.n);
+        F.ensure(24 * (size_t)g.n);
+        CICY_CUDA(cudaMemcpy(pb.a.get(), a, sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+        CICY_CUDA(cudaMemcpy(pb.b.get(), b, sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+        CICY_CUDA(cudaMemcpy(V.get(), g.vertices.data(), sizeof(double) * 24 * g.n, cudaMemcpyHostToDevice));
+        CICY_CUDA(cudaMemcpy(F.get(), g.planes.data(), sizeof(double) * 24 * g.n, cudaMemcpyHostToDevice));
+        const int blocks = cicy::pair_blocks(n, cicy::kPairThreads);
+        cicy::k_pair_distance<<<blocks, cicy::kPairThreads>>>(n, pb.a.get(), pb.b.get(), V.get(), vdw, pb.dist.get(), pb.dir.get(), pb.disp.get(),
+                                                             pb.pen.get(), pb.status.get());
+        CICY_LAUNCH_CHECK();
+        cicy::check_pair_status(n, pb.status.get(), pb.a.get(), pb.b.get());
+        cicy::k_pair_junction<<<blocks, cicy::kPairThreads>>>(n, pb.a.get(), pb.b.get(), V.get(), F.get(), pb.dist.get(), pb.dir.get(), pb.disp.get(),
+                                                             pb.pen.get(), nullptr, cicy::box_of(*sample), allow_simplex3 ? 1 : 0, pb.pa.get(),
+                                                             pb.pb.get(), pb.outside.get(), pb.jstatus.get());
+        CICY_LAUNCH_CHECK();
+        CICY_CUDA(cudaMemcpy(point_a, pb.pa.get(), sizeof(double) * 3 * n, cudaMemcpyDeviceToHost));
+        CICY_CUDA(cudaMemcpy(point_b, pb.pb.get(), sizeof(double) * 3 * n, cudaMemcpyDeviceToHost));
+        CICY_CUDA(cudaMemcpy(outside, pb.outside.get(), sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+        CICY_CUDA(cudaMemcpy(status, pb.jstatus.get(), sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+    } catch (const cicy::Fail& e) {
+        cicy::set_host_error(e.msg);
+        return e.status;
+    }
+    return CICY_OK;
+}
+
 cicy_status cicy_gnp_contact_pairs(int device, const cicy_gnp_set* gnps, const cicy_gnp_grid* grid, double vdw, double tunnel,
-                                   cicy_gnp_pairs** out) {
-    if (!gnps || !grid || !out || !(vdw >= 0) || !(tunnel >= 0)) {
+                                   const cicy_cuboid* sample, int32_t allow_simplex3, cicy_gnp_pairs** out) {
+    if (!gnps || !grid || !out || !sample || !(vdw >= 0) || !(tunnel >= 0)) {
         cicy::set_host_error("cicy_gnp_contact_pairs: invalid arguments");
         return CICY_E_INPUT;
     }
@@ -297,7 +408,7 @@ cicy_status cicy_gnp_contact_pairs(int device, const cicy_gnp_set* gnps, const c
     cicy_gnp_pairs* p = new cicy_gnp_pairs;
     try {
         CICY_CUDA(cudaSetDevice(device));
-        cicy::gnp_contact_pairs(gnps->g, grid->grid, vdw, tunnel, p->pairs);
+        cicy::gnp_contact_pairs(gnps->g, grid->grid, vdw, tunnel, *sample, allow_simplex3 != 0, p->pairs);
     } catch (const cicy::Fail& e) {
         cicy::set_host_error(e.msg);
         delete p;
@@ -319,6 +430,9 @@ cicy_status cicy_gnp_pairs_view(const cicy_gnp_pairs* p, cicy_gnp_pair_list* vie
     view->dist = q.dist.data();
     view->direction = q.direction.data();
     view->displacement = q.displacement.data();
+    view->point_a = q.point_a.data();
+    view->point_b = q.point_b.data();
+    view->outside = q.outside.data();
     return CICY_OK;
 }
 

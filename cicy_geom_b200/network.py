@@ -443,13 +443,38 @@ def gnp_pair_distance(directory: str, a, b, vdw: float, device: int = 0):
         lib().cicy_gnp_set_free(h)
 
 
+def gnp_junction_points(directory: str, a, b, vdw: float, sample, allow_simplex3: bool = False, device: int = 0):
+    """Upstream's junction step of Label_gnps_in_window on the device for pairs
+    (a[i], b[i]) (cicy_gnp_junction_points): returns (point_a [n, 3], point_b
+    [n, 3], outside[n] (1: point_a outside `sample`, 2: point_b), status[n]
+    (0, or the step upstream fails in))."""
+    h = C.c_void_p()
+    check(lib().cicy_read_gnps(directory.encode(), C.byref(h)), "cicy_read_gnps")
+    try:
+        a = np.ascontiguousarray(a, dtype=np.int32)
+        b = np.ascontiguousarray(b, dtype=np.int32)
+        n = len(a)
+        if len(b) != n:
+            raise ValueError("a and b differ in length")
+        w = _abi.Cuboid(*[float(x) for x in sample])
+        pa, pb, out, st = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros(n, np.int32), np.zeros(n, np.int32)
+        check(lib().cicy_gnp_junction_points(device, h, n, a.ctypes.data_as(_abi.i32p), b.ctypes.data_as(_abi.i32p), float(vdw), C.byref(w),
+                                             int(allow_simplex3), pa.ctypes.data_as(_abi.f64p), pb.ctypes.data_as(_abi.f64p),
+                                             out.ctypes.data_as(_abi.i32p), st.ctypes.data_as(_abi.i32p)), "cicy_gnp_junction_points")
+        return pa, pb, out, st
+    finally:
+        lib().cicy_gnp_set_free(h)
+
+
 def gnp_contact_pairs(directory: str, inside, window, gs_min, overlap_cnt: float, overlap_gnp: float, vdw: float, tunnel: float,
-                      device: int = 0) -> dict:
+                      sample=None, allow_simplex3: bool = False, device: int = 0) -> dict:
     """GNP-GNP contact pass of Label_gnps_in_window on the device: the GNP region
     lists (cicy_gnp_sectioned_domain of `inside`) and every pair sharing a region,
-    measured once (cicy_gnp_contact_pairs).  Returns the pairs within the
-    tunnelling cutoff in upstream's visiting order: a, b, penetrating, dist,
-    direction [n, 3], displacement [n, 3], and the visit and pair counts."""
+    measured once, with the junction points of each contact
+    (cicy_gnp_contact_pairs).  Returns the pairs within the tunnelling cutoff in
+    upstream's visiting order: a, b, penetrating, dist, direction [n, 3],
+    displacement [n, 3], point_a, point_b [n, 3], outside [n] (against `sample`,
+    default the window), and the visit and pair counts."""
     h = C.c_void_p()
     check(lib().cicy_read_gnps(directory.encode(), C.byref(h)), "cicy_read_gnps")
     grid, pairs = C.c_void_p(), C.c_void_p()
@@ -459,7 +484,9 @@ def gnp_contact_pairs(directory: str, inside, window, gs_min, overlap_cnt: float
         w = _abi.Cuboid(*[float(x) for x in window])
         check(lib().cicy_gnp_sectioned_domain(device, h, ins.ctypes.data_as(_abi.i32p), len(ins), C.byref(w), gs.ctypes.data_as(_abi.f64p),
                                               float(overlap_cnt), float(overlap_gnp), C.byref(grid)), "cicy_gnp_sectioned_domain")
-        check(lib().cicy_gnp_contact_pairs(device, h, grid, float(vdw), float(tunnel), C.byref(pairs)), "cicy_gnp_contact_pairs")
+        smp = _abi.Cuboid(*[float(x) for x in (window if sample is None else sample)])
+        check(lib().cicy_gnp_contact_pairs(device, h, grid, float(vdw), float(tunnel), C.byref(smp), int(allow_simplex3), C.byref(pairs)),
+              "cicy_gnp_contact_pairs")
         v = _abi.GnpPairList()
         check(lib().cicy_gnp_pairs_view(pairs, C.byref(v)), "cicy_gnp_pairs_view")
         n = int(v.n)
@@ -473,6 +500,9 @@ def gnp_contact_pairs(directory: str, inside, window, gs_min, overlap_cnt: float
                 "penetrating": arr(v.penetrating, C.c_int32, n, np.int32), "dist": arr(v.dist, C.c_double, n, np.float64),
                 "direction": arr(v.direction, C.c_double, 3 * n, np.float64).reshape(n, 3),
                 "displacement": arr(v.displacement, C.c_double, 3 * n, np.float64).reshape(n, 3),
+                "point_a": arr(v.point_a, C.c_double, 3 * n, np.float64).reshape(n, 3),
+                "point_b": arr(v.point_b, C.c_double, 3 * n, np.float64).reshape(n, 3),
+                "outside": arr(v.outside, C.c_int32, n, np.int32),
                 "n_visits": int(v.n_visits), "n_pairs": int(v.n_pairs)}
     finally:
         if pairs:

@@ -439,15 +439,31 @@ cicy_status cicy_gnp_point_distance(int device, const cicy_gnp_set* gnps, int32_
 cicy_status cicy_gnp_pair_distance(int device, const cicy_gnp_set* gnps, int32_t n, const int32_t* a, const int32_t* b, double vdw, double* dist,
                                    double* direction, double* displacement, int32_t* penetrating);
 
+/* Junction points of GNP pairs on the device: the distance step above, then
+ * Hoshen_Kopelman::Find_junction_points_for_gnps (Hoshen_Kopelman.cpp:826-1825)
+ * on GNP a and GNP b moved apart when they interpenetrate (Move_gnp), the point
+ * on b moved back, as Label_gnps_in_window does (:712-746).  Per pair: the
+ * points point_a[3i..], point_b[3i..], outside[i] (1: point_a outside `sample`,
+ * 2: point_b, Point_3D::is_outside_cuboid; -1 when the step failed) and
+ * status[i] (0, or the step upstream fails in: 1 simplex size, 2 intersection
+ * outside [0, 1], 3 no vertex inside the other face, 4 no edge for the
+ * two-intersection average, 5 no face for the vertex sum).  allow_simplex3 is
+ * Simu_para::allow_simplex3 (false for App_Network_3D). */
+cicy_status cicy_gnp_junction_points(int device, const cicy_gnp_set* gnps, int32_t n, const int32_t* a, const int32_t* b, double vdw,
+                                     const cicy_cuboid* sample, int32_t allow_simplex3, double* point_a, double* point_b, int32_t* outside,
+                                     int32_t* status);
+
 /* GNP-GNP contact pass of Hoshen_Kopelman::Label_gnps_in_window
  * (Hoshen_Kopelman.cpp:626-767) on the device: every pair of GNPs sharing a
  * region of `grid` (cicy_gnp_sectioned_domain), measured once; the pairs within
  * the tunnelling cutoff (dist <= tunnel) in upstream's visiting order (regions,
  * then j < k within the region, first visit), each as (a < b) with the results
- * of cicy_gnp_pair_distance.  These are the pairs upstream passes on to
- * Find_junction_points_for_gnps; the junction points and HK76 are not part of
- * this call.  Upstream orders a pair as (min(GNP1, GNP2), GNP2); with region
- * lists in ascending GNP order (an ascending `inside`) that is (a < b) too. */
+ * of cicy_gnp_pair_distance and the junction points of
+ * cicy_gnp_junction_points.  Upstream links a pair (HK76) when neither point
+ * is outside the sample; a junction step that fails returns CICY_E_INPUT naming
+ * the pair, where upstream stops.  Upstream orders a pair as (min(GNP1, GNP2),
+ * GNP2); with region lists in ascending GNP order (an ascending `inside`) that
+ * is (a < b) too. */
 typedef struct cicy_gnp_pairs cicy_gnp_pairs;
 typedef struct {
     int64_t n;                    /* contact pairs */
@@ -459,9 +475,12 @@ typedef struct {
     const double* dist;           /* [n] */
     const double* direction;      /* [3n] */
     const double* displacement;   /* [3n] */
+    const double* point_a;        /* [3n] junction point on a */
+    const double* point_b;        /* [3n] junction point on b */
+    const int32_t* outside;       /* [n] 1: point_a outside the sample, 2: point_b, 3: both */
 } cicy_gnp_pair_list;
 cicy_status cicy_gnp_contact_pairs(int device, const cicy_gnp_set* gnps, const cicy_gnp_grid* grid, double vdw, double tunnel,
-                                   cicy_gnp_pairs** out);
+                                   const cicy_cuboid* sample, int32_t allow_simplex3, cicy_gnp_pairs** out);
 /* Borrowed view; valid until cicy_gnp_pairs_free. */
 cicy_status cicy_gnp_pairs_view(const cicy_gnp_pairs* p, cicy_gnp_pair_list* view);
 void cicy_gnp_pairs_free(cicy_gnp_pairs* p);

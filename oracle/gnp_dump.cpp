@@ -36,6 +36,12 @@
  * and dumps the CNT sectioned domain and the CNT-GNP contacts: point, GNP,
  * contact-point number, junction distance, and the contact points in order.
  *
+ * For every candidate pair within the tunnelling cutoff it also runs the
+ * junction step of Label_gnps_in_window (Find_junction_points_for_gnps with
+ * the moved second GNP, allow_simplex3 = false as App_Network_3D sets it, then
+ * the point on the second GNP moved back) and dumps its success flag, both
+ * points and whether each lies outside the sample.
+ *
  * Output records: u32 name length, name, u8 type ('i' int32, 'd' float64),
  * u64 count, payload (the layout oracle/dumpio.py reads).
  */
@@ -114,6 +120,8 @@ int main(int argc, char** argv) {
     Hoshen_Kopelman HK;
     std::vector<int> pa, pb, pflag;
     std::vector<double> dist, dir, disp;
+    std::vector<int> jn_pair, jn_ok, jn_out;
+    std::vector<double> jn_pts;
     const int n = (int)gnps.size();
     for (int a = 0; a < n; a++)
         for (int b = a + 1; b < n; b++) {
@@ -129,6 +137,17 @@ int main(int argc, char** argv) {
             bool p_flag = false;
             double d = 0;
             if (!HK.Get_distance_between_GNPs(cut, gnps, a, b, p_flag, disp_tot, N, d, gnp_B)) return 6;
+            if (d <= dt) {
+                // the junction step of Label_gnps_in_window for a pair within the cutoff
+                Point_3D PA, PB;
+                std::vector<Point_3D> scratch;
+                const int ok = HK.Find_junction_points_for_gnps(false, geom.sample, gnps[a], gnp_B, N, d, scratch, PA, PB);
+                if (ok && p_flag) PB = PB - disp_tot;
+                jn_pair.push_back((int)pa.size());
+                jn_ok.push_back(ok);
+                jn_out.push_back(ok ? (PA.is_outside_cuboid(geom.sample) ? 1 : 0) + (PB.is_outside_cuboid(geom.sample) ? 2 : 0) : -1);
+                jn_pts.insert(jn_pts.end(), {PA.x, PA.y, PA.z, PB.x, PB.y, PB.z});
+            }
             pa.push_back(a);
             pb.push_back(b);
             pflag.push_back(p_flag ? 1 : 0);
@@ -226,6 +245,10 @@ int main(int argc, char** argv) {
         o.f64("query_point", qp);
         o.i32("query_flag", qflag);
     }
+    o.i32("junc_pair", jn_pair);
+    o.i32("junc_ok", jn_ok);
+    o.i32("junc_outside", jn_out);
+    o.f64("junc_points", jn_pts);
     o.i32("pair_a", pa);
     o.i32("pair_b", pb);
     o.i32("pair_penetrating", pflag);

@@ -499,3 +499,233 @@ def contact_pairs(sd_gnp, vertices, vdw: float, tunnel: float):
                 if d <= tunnel:
                     out.append((a, b, d, N, m, pen))
     return out
+
+
+# ---------------------------------------------------------------------------
+# Junction points of two GNPs in contact (Hoshen_Kopelman.cpp:826-1825)
+
+_FACE_EDGES = {  # Get_edges_of_face (:1330-1426): vertex sum -> 4 edges, the face normal bounding each
+    7: (((0, 3), (0, 1), (1, 2), (2, 3)), (2, 3, 4, 5)),
+    22: (((4, 7), (4, 5), (5, 6), (6, 7)), (2, 3, 4, 5)),
+    15: (((0, 3), (3, 7), (7, 4), (0, 4)), (0, 5, 1, 3)),
+    11: (((1, 0), (0, 4), (4, 5), (5, 1)), (0, 2, 1, 4)),
+    14: (((1, 2), (2, 6), (6, 5), (5, 1)), (0, 5, 1, 3)),
+    18: (((2, 3), (3, 7), (7, 6), (6, 2)), (0, 2, 1, 4)),
+}
+_FOURTH = {(0, 1, 2): 3, (0, 1, 3): 2, (0, 2, 3): 1, (1, 2, 3): 0, (4, 5, 6): 7, (4, 5, 7): 6, (4, 6, 7): 5, (5, 6, 7): 4,
+           (0, 1, 4): 5, (0, 1, 5): 4, (0, 4, 5): 1, (1, 4, 5): 0, (1, 2, 5): 6, (1, 2, 6): 5, (1, 5, 6): 2, (2, 5, 6): 1,
+           (2, 3, 6): 7, (2, 3, 7): 6, (2, 6, 7): 3, (3, 6, 7): 2, (0, 3, 4): 7, (0, 3, 7): 4, (0, 4, 7): 3, (3, 4, 7): 0}
+_PLANE_VERTS = ((0, 1, 3), (4, 7, 5), (0, 3, 4), (0, 4, 1), (1, 5, 2), (2, 6, 3))  # Update_gnp_plane_equations
+
+
+class JunctionError(Exception):
+    """A step upstream's junction search fails in (it returns 0 there)."""
+
+
+def _add(a, b):
+    return (a[0] + b[0], a[1] + b[1], a[2] + b[2])
+
+
+def _div(a, s):
+    return (a[0] / s, a[1] / s, a[2] / s)
+
+
+def moved_gnp(V, d):
+    """Generate_Network::Move_gnp: vertices + d and the face normals rebuilt from them."""
+    v = [_add(tuple(float(c) for c in p), d) for p in V]
+    return v, [_unit(_cross(_sub(v[b], v[a]), _sub(v[c], v[a]))) for a, b, c in _PLANE_VERTS]
+
+
+def _lambda(Pin, Pout, e1, e2):
+    """Lambda_of_two_lines (:1529-1540)."""
+    detA = (e2[0] - e1[0]) * (Pin[1] - Pout[1]) - (Pin[0] - Pout[0]) * (e2[1] - e1[1])
+    detAP = (e2[0] - e1[0]) * (e1[1] - Pout[1]) - (e1[0] - Pout[0]) * (e2[1] - e1[1])
+    return detAP / detA
+
+
+def _face(face_sum):
+    if face_sum not in _FACE_EDGES:
+        raise JunctionError("Get_edges_of_face: invalid face")
+    return _FACE_EDGES[face_sum]
+
+
+def _edge_cut(count, arr, A0, A1, edges, BV):
+    """Get_intersection_with_face_edge (:1428-1527)."""
+    if count == 4:
+        return A0
+    if count == 3:
+        e = edges[arr[0]]
+        lam = _lambda(A0, A1, BV[e[0]], BV[e[1]])
+        if (lam < ZERO and abs(lam) > ZERO) or lam > 1.0:
+            raise JunctionError("Get_intersection_with_face_edge (1)")
+    elif count == 2:
+        e = edges[arr[0]]
+        lam = _lambda(A0, A1, BV[e[0]], BV[e[1]])
+        if lam < ZERO and abs(lam) > ZERO:
+            e = edges[arr[1]]
+            lam = _lambda(A0, A1, BV[e[0]], BV[e[1]])
+            if (lam < ZERO and abs(lam) > ZERO) or lam > 1.0:
+                raise JunctionError("Get_intersection_with_face_edge (2)")
+    else:
+        raise JunctionError("Get_intersection_with_face_edge: invalid count")
+    return _add(A1, _scale(_sub(A0, A1), lam))
+
+
+def _inside_face(sA, edges, normals, AV, BV, BN):
+    """Get_vertices_inside_face (:1687-1720)."""
+    out = [v for v in sA if sum(_dot(_sub(AV[v], BV[e[0]]), BN[n]) < ZERO for e, n in zip(edges, normals)) == 4]
+    if not out:
+        raise JunctionError("Get_vertices_inside_face: no vertices inside face")
+    return out
+
+
+def _average_two_cuts(edgesA, normalsA, AV, AN, edgesB, BV, disp, vB, PB):
+    """Average_point_with_two_interserctions (:1722-1778)."""
+    w = []
+    for e in edgesB:
+        if e[0] == vB:
+            w.append(e[1])
+        elif e[1] == vB:
+            w.append(e[0])
+    w = (w + [0, 0])[:2]
+    v1, v2 = 0, -1
+    for e, n in zip(edgesA, normalsA):
+        v1 = e[0]
+        if _dot(_sub(BV[w[0]], AV[v1]), AN[n]) > ZERO and _dot(_sub(BV[w[1]], AV[v1]), AN[n]) > ZERO:
+            v2 = e[1]
+            break
+    if v2 == -1:
+        raise JunctionError("Average_point_with_two_interserctions: no edge")
+    a1, a2 = _sub(AV[v1], disp), _sub(AV[v2], disp)
+    l0 = _lambda(PB, BV[w[0]], a1, a2)
+    l1 = _lambda(PB, BV[w[1]], a1, a2)
+    PB = _add(PB, _add(BV[w[0]], _scale(_sub(PB, BV[w[0]]), l0)))
+    PB = _add(PB, _add(BV[w[1]], _scale(_sub(PB, BV[w[1]]), l1)))
+    return _div(PB, 3.0)
+
+
+def _junction_in(sA, sB, A, B, N, distance, sumA, sumB):
+    """Find_junction_points_in_gnps (:1049-1111) and the point-B cases it calls."""
+    (AV, AN), (BV, BN) = A, B
+    if len(sA) == 1:
+        PA = AV[sA[0]]
+        if len(sB) == 1:
+            return PA, BV[sB[0]]
+        if len(sB) in (2, 4):
+            return PA, _add(PA, _scale(N, distance))
+        raise JunctionError("Find_point_b_for_vertex_in_simplex_a: simplex size")
+    if len(sA) == 2:
+        disp = _scale(N, distance)
+        eA = (_add(AV[sA[0]], disp), _add(AV[sA[1]], disp))
+        if len(sB) == 2:  # Find_point_for_edge_edge_contact (:1187-1262)
+            dA, dB = _sub(eA[1], eA[0]), _sub(BV[sB[1]], BV[sB[0]])
+            cr = _cross(dA, dB)
+            if abs(cr[0]) < ZERO and abs(cr[1]) < ZERO and abs(cr[2]) < ZERO:
+                with np.errstate(divide="ignore", invalid="ignore"):
+                    x1, x2 = np.float64(eA[0][0]), np.float64(eA[1][0])
+                    l0 = float((np.float64(BV[sB[0]][0]) - x1) / (x2 - x1))
+                    l1 = float((np.float64(BV[sB[1]][0]) - x1) / (x2 - x1))
+                PB = None
+                if (abs(l0) < ZERO and abs(l1 - 1) < ZERO) or (abs(l1) < ZERO and abs(l0 - 1) < ZERO):
+                    PB = _div(_add(BV[sB[0]], BV[sB[1]]), 2.0)
+                if l0 >= ZERO and l0 - 1 <= ZERO:
+                    S0 = _add(eA[0], _scale(dA, l0))
+                    PB = _div(_add(eA[0], S0), 2.0) if l1 < ZERO else _div(_add(eA[1], S0), 2.0)
+                else:
+                    S1 = _add(eA[0], _scale(dA, l1))
+                    PB = _div(_add(eA[0], S1), 2.0) if l0 < ZERO else _div(_add(eA[1], S1), 2.0)
+            else:
+                lam = _lambda(BV[sB[1]], BV[sB[0]], eA[0], eA[1])
+                PB = _add(BV[sB[0]], _scale(dB, lam))
+            return _sub(PB, disp), PB
+        if len(sB) == 4:  # Find_point_for_edge_face_contact (:1264-1328)
+            edges, normals = _face(sumB)
+            c, arr = [0, 0], [[-1, -1], [-1, -1]]
+            for i, (e, n) in enumerate(zip(edges, normals)):
+                for k in range(2):
+                    if _dot(_sub(eA[k], BV[e[0]]), BN[n]) < ZERO:
+                        c[k] += 1
+                    elif arr[k][0] == -1:
+                        arr[k][0] = i
+                    else:
+                        arr[k][1] = i
+            A0 = _edge_cut(c[0], arr[0], eA[0], eA[1], edges, BV)
+            A1 = _edge_cut(c[1], arr[1], eA[1], eA[0], edges, BV)
+            PB = _scale(_add(A0, A1), 0.5)
+            return _sub(PB, disp), PB
+        raise JunctionError("Find_point_b_for_edge_in_simplex_a: simplex size")
+    if len(sA) == 4:  # Find_point_b_for_face_in_simplex_a (:1542-1685)
+        if len(sB) != 4:
+            raise JunctionError("Find_point_b_for_face_in_simplex_a: simplex size")
+        edgesB, normalsB = _face(sumB)
+        inA = _inside_face(sA, edgesB, normalsB, AV, BV, BN)
+        if len(inA) == 4:
+            PA, PB = (0.0, 0.0, 0.0), (0.0, 0.0, 0.0)
+            for k in range(4):
+                PA, PB = _add(PA, AV[sA[k]]), _add(PB, BV[sB[k]])
+            return _div(PA, 4.0), _div(PB, 4.0)
+        edgesA, normalsA = _face(sumA)
+        inB = _inside_face(sB, edgesA, normalsA, BV, AV, AN)
+        disp = _scale(N, distance)
+        if len(inA) == 0 and len(inB) == 1:
+            PB = _average_two_cuts(edgesA, normalsA, AV, AN, edgesB, BV, disp, inB[0], BV[inB[0]])
+            return _sub(PB, disp), PB
+        if len(inA) == 1 and len(inB) == 0:  # upstream passes face B's edges for both faces here
+            PA = _average_two_cuts(edgesB, normalsB, BV, BN, edgesB, BV, _scale(disp, -1.0), inA[0], AV[inA[0]])
+            return PA, _add(PA, disp)
+        PB = (0.0, 0.0, 0.0)
+        for v in inA:
+            PB = _add(_add(PB, AV[v]), disp)
+        for v in inB:
+            PB = _add(PB, BV[v])
+        PB = _div(PB, float(len(inA) + len(inB)))
+        return _sub(PB, disp), PB
+    raise JunctionError("Find_junction_points_in_gnps: simplex size")
+
+
+def junction_points(A, B, N, distance: float, allow_simplex3: bool = False):
+    """Find_junction_points_for_gnps (:826-857) with
+    Find_closest_simplices_of_gnps_in_contact (:860-966).  A and B are (vertices,
+    face normals), B already moved apart when the pair interpenetrates.
+    Returns (point on A, point on B); raises JunctionError where upstream fails."""
+    AV, BV = A[0], B[0]
+    setA, setB = set(), set()
+    for i in range(8):
+        for j in range(8):
+            if abs(abs(_dot(_sub(AV[i], BV[j]), N)) - distance) <= ZERO:
+                setA.add(i)
+                setB.add(j)
+    if allow_simplex3:
+        for s in (setA, setB):
+            if len(s) == 3:
+                key = tuple(sorted(s))
+                if key not in _FOURTH:
+                    raise JunctionError("Complete_simplex_of_size_three: no face")
+                s.add(_FOURTH[key])
+    sA, sB = sorted(setA), sorted(setB)
+    sumA, sumB = sum(max(1, v) for v in sA), sum(max(1, v) for v in sB)
+    if len(sA) <= len(sB):
+        return _junction_in(sA, sB, A, B, N, distance, sumA, sumB)
+    PB, PA = _junction_in(sB, sA, B, A, _scale(N, -1.0), distance, sumB, sumA)
+    return PA, PB
+
+
+def outside_box(p, lo, hi) -> bool:
+    """Point_3D::is_outside_cuboid (Geometry_3D.cpp:227-235)."""
+    return any(p[k] - lo[k] < ZERO or p[k] - hi[k] > ZERO for k in range(3))
+
+
+def pair_junction(VA, FA, VB, FB, vdw: float, lo, hi, allow_simplex3: bool = False):
+    """The junction step of Label_gnps_in_window for a pair within the cutoff
+    (Hoshen_Kopelman.cpp:712-746): (point on a, point on b moved back, outside
+    code 1 a / 2 b), or None where upstream fails."""
+    d, N, m, pen = pair_distance(VA, VB, vdw)
+    A = ([tuple(float(c) for c in v) for v in VA], [tuple(float(c) for c in f[:3]) for f in FA])
+    B = moved_gnp(VB, m) if pen else ([tuple(float(c) for c in v) for v in VB], [tuple(float(c) for c in f[:3]) for f in FB])
+    try:
+        PA, PB = junction_points(A, B, N, d, allow_simplex3)
+    except JunctionError:
+        return None
+    if pen:
+        PB = _sub(PB, m)
+    return PA, PB, (1 if outside_box(PA, lo, hi) else 0) + (2 if outside_box(PB, lo, hi) else 0)

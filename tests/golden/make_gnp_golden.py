@@ -8,7 +8,8 @@ closest GNP point to 20 query points around each GNP (the CNT-GNP distance),
 upstream's
 GNP part of the contact grid (0.05 um regions, overlaps as Input_Reader sets
 them) and, for every candidate pair, upstream's GNP-GNP distance step (GJK
-distance, EPA when the GNPs interpenetrate, the move of the second GNP): the
+distance, EPA when the GNPs interpenetrate, the move of the second GNP) and,
+for the pairs within the tunnelling cutoff, upstream's junction points: the
 oracle of the GNP contact search.  With a seeded 400-CNT network in the same
 cube (regenerated by the tests from its seed and checked against the stored
 SHA-256), it also stores upstream's CNT-GNP contacts of the mixed contact pass

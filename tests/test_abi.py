@@ -22,9 +22,9 @@ def test_struct_sizes_match_header_layout():
     assert C.sizeof(_abi.BatchSystem) == 4 * 2 + 8 * 6 + 8 + 8 * 3
     # cicy_gnn_system: n, nnz; 3 pointers; n_chains (+4 padding); 2 pointers
     assert C.sizeof(_abi.GnnSystem) == 4 * 2 + 8 * 3 + 8 + 8 * 2
-    # cicy_gnps: n (+4 padding); 6 pointers.  cicy_gnp_pair_list: 3 counts; 6 pointers
+    # cicy_gnps: n (+4 padding); 6 pointers.  cicy_gnp_pair_list: 3 counts; 9 pointers
     assert C.sizeof(_abi.Gnps) == 8 + 8 * 6
-    assert C.sizeof(_abi.GnpPairList) == 8 * 3 + 8 * 6
+    assert C.sizeof(_abi.GnpPairList) == 8 * 3 + 8 * 9
 
 
 def test_context_creation_without_gpu_fails_cleanly():

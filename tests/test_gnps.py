@@ -239,3 +239,29 @@ def test_gnp_contact_pairs_oracle_agrees_with_upstream_golden():
         i = ref[(a, b)]
         assert d == z["ref_pair_dist"][i] and int(p) == z["ref_pair_penetrating"][i]
         assert tuple(N) == tuple(z["ref_pair_direction"][3 * i:3 * i + 3])
+
+
+KAT = os.path.join(ROOT, "tests", "golden", "gnp_junction_cases.npz")
+
+
+@pytest.mark.parametrize("path,side", [(GOLDEN, 2.0), (KAT, 12.0)])
+def test_junction_oracle_matches_upstream_golden(path, side):
+    """The CPU restatement of upstream's junction step (Find_junction_points_for_gnps
+    on the moved GNP, the point moved back, the outside test) against upstream on
+    the random fixture's 555 contacts (vertex-face, crossing edges) and the 10
+    hand-placed cases (face-face, edge-face, parallel edges with upstream's NaN,
+    vertex-vertex, vertex-edge, and a face-face case upstream fails on); points
+    compared as bit patterns."""
+    from oracle import gnp_oracle as G
+
+    z = dict(np.load(path))
+    V, F = z["ref_gnp_vertices"].reshape(-1, 8, 3).tolist(), z["ref_gnp_planes"].reshape(-1, 6, 4).tolist()
+    vdw = 0.00034
+    for i, p in enumerate(z["ref_junc_pair"]):
+        a, b = z["ref_pair_a"][p], z["ref_pair_b"][p]
+        r = G.pair_junction(V[a], F[a], V[b], F[b], vdw, (0.0, 0.0, 0.0), (side, side, side))
+        assert (r is not None) == bool(z["ref_junc_ok"][i])
+        if r is not None:
+            mine = np.array(list(r[0]) + list(r[1]))
+            assert np.array_equal(mine.view(np.int64), z["ref_junc_points"][6 * i:6 * i + 6].view(np.int64))
+            assert r[2] == z["ref_junc_outside"][i]

@@ -150,7 +150,8 @@ def test_gnp_pair_distance_matches_upstream_golden(cuda_ok, tmp_path):
 def test_gnp_contact_pairs_match_oracle(cuda_ok, tmp_path):
     """Device GNP-GNP contact pass (cicy_gnp_contact_pairs) against the CPU
     restatement: the fixture (upstream's region lists) and a window of another
-    seed with a subset of the GNPs; same pairs, order and doubles."""
+    seed with a subset of the GNPs; same pairs, order, distances and junction
+    points, bit for bit."""
     from cicy_geom_b200.network import gnp_contact_pairs
 
     z = dict(np.load(GOLDEN))
@@ -173,6 +174,32 @@ def test_gnp_contact_pairs_match_oracle(cuda_ok, tmp_path):
         sd = G.fill_sectioned_domain_gnps(win, V["vertices"], V["l"], V["t"], inside, n, l, ov)
         ref = G.contact_pairs(sd, V["vertices"].tolist(), vdw, tunnel)
         assert len(out["a"]) == len(ref) > 50
+        F = V["planes"].tolist()
         for i, (a, b, dd, N, m, p) in enumerate(ref):
             assert (out["a"][i], out["b"][i], out["penetrating"][i]) == (a, b, int(p)) and out["dist"][i] == dd
             assert tuple(out["direction"][i]) == tuple(N) and tuple(out["displacement"][i]) == tuple(m)
+            PA, PB, o = G.pair_junction(V["vertices"][a], F[a], V["vertices"][b], F[b], vdw, win[0:3], win[6:9])
+            pts = np.concatenate([out["point_a"][i], out["point_b"][i]])
+            assert np.array_equal(pts.view(np.int64), np.array(list(PA) + list(PB)).view(np.int64)) and out["outside"][i] == o
+
+
+KAT = os.path.join(ROOT, "tests", "golden", "gnp_junction_cases.npz")
+
+
+@pytest.mark.parametrize("path,side", [(GOLDEN, 2.0), (KAT, 12.0)])
+def test_gnp_junction_points_match_upstream_golden(cuda_ok, tmp_path, path, side):
+    """Device junction step (cicy_gnp_junction_points) against upstream: points as
+    bit patterns (upstream's NaN for parallel edges included), outside codes, and
+    a failure where upstream fails."""
+    from cicy_geom_b200.network import gnp_junction_points
+
+    z = dict(np.load(path))
+    write_gnp_file(str(tmp_path), {"l": z["in_l"], "t": z["in_t"], "theta": z["in_theta"], "phi": z["in_phi"], "center": z["in_center"]})
+    jp = z["ref_junc_pair"]
+    pa, pb, out, st = gnp_junction_points(str(tmp_path), z["ref_pair_a"][jp], z["ref_pair_b"][jp], 0.00034,
+                                          [0.0, 0.0, 0.0, side, side, side, side, side, side])
+    ok = z["ref_junc_ok"].astype(bool)
+    assert np.array_equal(st == 0, ok)
+    pts = np.concatenate([pa, pb], 1)[ok]
+    assert np.array_equal(pts.view(np.int64), z["ref_junc_points"].reshape(-1, 6)[ok].view(np.int64))
+    assert np.array_equal(out[ok], z["ref_junc_outside"][ok])
