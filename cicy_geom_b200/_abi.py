@@ -250,6 +250,8 @@ def lib() -> C.CDLL:
                                              P(C.c_void_p)]),
         "cicy_gnp_pairs_view": (C.c_int, [C.c_void_p, P(GnpPairList)]),
         "cicy_gnp_pairs_free": (None, [C.c_void_p]),
+        "cicy_gnp_labels": (C.c_int, [C.c_int, C.c_void_p, C.c_int32, C.c_int32, i32p, i32p]),
+        "cicy_mixed_labels": (C.c_int, [C.c_void_p, i32p, C.c_int32, C.c_int32, i32p, i32p, i32p]),
         "cicy_gnp_cnt_contacts": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, P(Params), C.c_int32, i64p]),
         "cicy_get_gnp_cnt_contacts": (C.c_int, [C.c_void_p, i64p, i64p, i32p, f64p, f64p]),
         "cicy_host_network_view": (C.c_int, [C.c_void_p, P(Network)]),

@@ -177,6 +177,15 @@ cicy_status cicy_gnp_cnt_contacts(cicy_ctx* ctx, const cicy_gnp_set* gnps, const
     });
 }
 
+cicy_status cicy_mixed_labels(cicy_ctx* ctx, const int32_t* labels_gnp, int32_t n_gnps, int32_t n_total_labels, int32_t* labels_cnt,
+                              int32_t* labels_gnp_out, int32_t* n_clusters) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (n_gnps < 0 || (n_gnps > 0 && !labels_gnp)) throw cicy::Fail{CICY_E_INPUT, "cicy_mixed_labels: null GNP labels"};
+        const int n = cicy::run_mixed_labels(c, labels_gnp, n_gnps, n_total_labels, labels_cnt, labels_gnp_out);
+        if (n_clusters) *n_clusters = n;
+    });
+}
+
 cicy_status cicy_get_gnp_cnt_contacts(cicy_ctx* ctx, int64_t* n, int64_t* point, int32_t* gnp, double* dist, double* closest) {
     return guarded(ctx, [&](cicy::Ctx& c) {
         const int U = c.n_mix;

@@ -152,6 +152,8 @@ struct GnpSet;
 struct GnpGrid;
 // CNT-GNP contacts of the hybrid grid (gnp_grid.cu); returns the number of contacts.
 int run_gnp_cnt_contacts(Ctx& c, const GnpSet& g, const GnpGrid& grid, const cicy_params& p, int inside_is_error);
+// Make_mixed_clusters' labels (gnp_labels.cu); returns the number of clusters.
+int run_mixed_labels(Ctx& c, const int32_t* labels_gnp, int n_gnps, int n_total_labels, int32_t* labels_cnt_out, int32_t* labels_gnp_out);
 
 // Learned preconditioner: edge weights for the system being solved (learned.cu).
 const float* learned_edge_weights(Ctx& c, const SolverSystem& ss, int n_chains, cudaStream_t s);

@@ -5,6 +5,7 @@
 
 #include "ctx.cuh"
 #include "trace.cuh"
+#include "uf.cuh"
 
 namespace cicy {
 
@@ -213,29 +214,7 @@ __global__ void k_contact_unique(int n, const uint64_t* __restrict__ keys, const
 }
 
 // ---------------------------------------------------------------------------
-// Lock-free union-find over CNTs: hook the larger root under the smaller one
-// (so parent[x] <= x always), path halving while uniting.  Loads of parent[]
-// bypass L1 (__ldcg): another SM's CAS must be visible to the retry loop.
-__device__ __forceinline__ int uf_find(int32_t* parent, int x) {
-    while (true) {
-        int p = __ldcg(&parent[x]);
-        if (p == x) return x;
-        int gp = __ldcg(&parent[p]);
-        if (gp != p) parent[x] = gp;
-        x = p;
-    }
-}
-
-// Read-only find for the flattening pass: a writing find there could store a
-// stale, non-root ancestor over a parent[] entry another thread already finalised.
-__device__ __forceinline__ int uf_root(const int32_t* parent, int x) {
-    while (true) {
-        int p = __ldcg(&parent[x]);
-        if (p == x) return x;
-        x = p;
-    }
-}
-
+// Union-find over CNTs (uf.cuh)
 __global__ void k_uf_init(int n, int32_t* parent, unsigned long long* minkey) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         parent[i] = i;
@@ -245,13 +224,7 @@ __global__ void k_uf_init(int n, int32_t* parent, unsigned long long* minkey) {
 
 __global__ void k_uf_union(int n, const int32_t* __restrict__ ua, const int32_t* __restrict__ ub, int32_t* parent) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        int a = ua[i], b = ub[i];
-        while (true) {
-            int ra = uf_find(parent, a), rb = uf_find(parent, b);
-            if (ra == rb) break;
-            if (ra > rb) { int t = ra; ra = rb; rb = t; }
-            if (atomicCAS(&parent[rb], rb, ra) == rb) break;
-        }
+        uf_unite(parent, ua[i], ub[i]);
     }
 }
 

@@ -127,6 +127,18 @@ class Context:
                                                     _p(q, C.c_double)), "cicy_get_gnp_cnt_contacts")
         return pt[:N], g[:N], d[:N], q[:N]
 
+    def mixed_labels(self, labels_gnp, n_total_labels: int):
+        """Make_mixed_clusters' labels (cicy_mixed_labels) after clusters(p) and
+        gnp_cnt_contacts: the GNP labels of the contact pass (numbered after the
+        CNT labels, n_total_labels in all) joined to the CNT labels by the CNT-GNP
+        contacts.  Returns (labels_cnt, labels_gnp, n_clusters)."""
+        g = np.ascontiguousarray(labels_gnp, dtype=np.int32)
+        nc = self.labels()[0].shape[0]
+        lc, lg, n = np.zeros(max(nc, 1), np.int32), np.zeros(max(len(g), 1), np.int32), C.c_int32()
+        self._check(lib().cicy_mixed_labels(self._h, g.ctypes.data_as(_abi.i32p), len(g), int(n_total_labels), _p(lc, C.c_int32),
+                                            _p(lg, C.c_int32), C.byref(n)), "cicy_mixed_labels")
+        return lc[:nc], lg[:len(g)], int(n.value)
+
     def clusters(self, p: _abi.Params):
         self._check(lib().cicy_clusters(self._h, C.byref(p)), "cicy_clusters")
 

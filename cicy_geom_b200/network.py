@@ -467,14 +467,16 @@ def gnp_junction_points(directory: str, a, b, vdw: float, sample, allow_simplex3
 
 
 def gnp_contact_pairs(directory: str, inside, window, gs_min, overlap_cnt: float, overlap_gnp: float, vdw: float, tunnel: float,
-                      sample=None, allow_simplex3: bool = False, device: int = 0) -> dict:
+                      sample=None, allow_simplex3: bool = False, n_labels_cnt=None, device: int = 0) -> dict:
     """GNP-GNP contact pass of Label_gnps_in_window on the device: the GNP region
     lists (cicy_gnp_sectioned_domain of `inside`) and every pair sharing a region,
     measured once, with the junction points of each contact
     (cicy_gnp_contact_pairs).  Returns the pairs within the tunnelling cutoff in
     upstream's visiting order: a, b, penetrating, dist, direction [n, 3],
     displacement [n, 3], point_a, point_b [n, 3], outside [n] (against `sample`,
-    default the window), and the visit and pair counts."""
+    default the window), and the visit and pair counts; with `n_labels_cnt`, also
+    the GNP labels of Make_gnp_clusters (cicy_gnp_labels): labels_gnp and
+    n_total_labels."""
     h = C.c_void_p()
     check(lib().cicy_read_gnps(directory.encode(), C.byref(h)), "cicy_read_gnps")
     grid, pairs = C.c_void_p(), C.c_void_p()
@@ -496,7 +498,15 @@ def gnp_contact_pairs(directory: str, inside, window, gs_min, overlap_cnt: float
                 return np.zeros(0, dt)
             return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ct)), shape=(count,)).copy()
 
-        return {"a": arr(v.a, C.c_int32, n, np.int32), "b": arr(v.b, C.c_int32, n, np.int32),
+        res = {}
+        if n_labels_cnt is not None:
+            gv = _abi.Gnps()
+            check(lib().cicy_gnp_set_view(h, C.byref(gv)), "cicy_gnp_set_view")
+            lab = np.zeros(max(gv.n, 1), np.int32)
+            tot = C.c_int32()
+            check(lib().cicy_gnp_labels(device, pairs, gv.n, int(n_labels_cnt), lab.ctypes.data_as(_abi.i32p), C.byref(tot)), "cicy_gnp_labels")
+            res = {"labels_gnp": lab[:gv.n], "n_total_labels": int(tot.value)}
+        return {**res, "a": arr(v.a, C.c_int32, n, np.int32), "b": arr(v.b, C.c_int32, n, np.int32),
                 "penetrating": arr(v.penetrating, C.c_int32, n, np.int32), "dist": arr(v.dist, C.c_double, n, np.float64),
                 "direction": arr(v.direction, C.c_double, 3 * n, np.float64).reshape(n, 3),
                 "displacement": arr(v.displacement, C.c_double, 3 * n, np.float64).reshape(n, 3),

@@ -485,6 +485,24 @@ cicy_status cicy_gnp_contact_pairs(int device, const cicy_gnp_set* gnps, const c
 cicy_status cicy_gnp_pairs_view(const cicy_gnp_pairs* p, cicy_gnp_pair_list* view);
 void cicy_gnp_pairs_free(cicy_gnp_pairs* p);
 
+/* GNP labels on the device: the HK76 pass of Label_gnps_in_window over the
+ * contact pairs whose junction points are both inside the sample (outside ==
+ * 0), in list order, then Cleanup_labels and Renumber_gnp_labels
+ * (Hoshen_Kopelman.cpp:594-616): labels_gnp[n_gnps] (-1: no cluster) numbered
+ * from n_labels_cnt, and n_total_labels = n_labels_cnt + the GNP clusters. */
+cicy_status cicy_gnp_labels(int device, const cicy_gnp_pairs* pairs, int32_t n_gnps, int32_t n_labels_cnt, int32_t* labels_gnp,
+                            int32_t* n_total_labels);
+
+/* Labels of mixed CNT/GNP clusters on the device, Make_mixed_clusters
+ * (Hoshen_Kopelman.cpp:1925-1987): the context's CNT labels (cicy_clusters on
+ * the hybrid grid) and GNP labels `labels_gnp` (cicy_gnp_labels, n_total_labels
+ * labels in all) joined by the context's CNT-GNP contacts
+ * (cicy_gnp_cnt_contacts) in contact-number order (HK76), then Cleanup_labels:
+ * labels_cnt[n_cnts] and labels_gnp_out[n_gnps] (either may be NULL),
+ * n_clusters.  The context's CNT labels become the mixed ones. */
+cicy_status cicy_mixed_labels(cicy_ctx* ctx, const int32_t* labels_gnp, int32_t n_gnps, int32_t n_total_labels, int32_t* labels_cnt,
+                              int32_t* labels_gnp_out, int32_t* n_clusters);
+
 /* CNT-GNP contacts of the hybrid CNT/GNP sample on the device:
  * Hoshen_Kopelman::Find_adjacent_labels (Hoshen_Kopelman.cpp:1989-2142) over
  * Contact_grid::Generate_contact_grid with particle type GNP_CNT_mix.  The

@@ -34,7 +34,10 @@
  * Hoshen_Kopelman::Find_adjacent_labels, Hoshen_Kopelman.cpp:1989-2142, with a
  * CNT point inside a GNP counted as no contact, ignore_eror_cnt_inside_gnp = 1)
  * and dumps the CNT sectioned domain and the CNT-GNP contacts: point, GNP,
- * contact-point number, junction distance, and the contact points in order.
+ * contact-point number, junction distance, and the contact points in order,
+ * then the labels of the hybrid sample: Make_cnt_clusters, Make_gnp_clusters
+ * (GNP-GNP contacts with junction points) and Make_mixed_clusters, in
+ * Determine_clusters_and_percolation's order.
  *
  * For every candidate pair within the tunnelling cutoff it also runs the
  * junction step of Label_gnps_in_window (Find_junction_points_for_gnps with
@@ -211,6 +214,36 @@ int main(int argc, char** argv) {
                     md.push_back(point_contacts_dist[pc.first][gc.first]);
                 }
             for (const auto& c : contact_points_gnp) mpts.insert(mpts.end(), {c.x, c.y, c.z});
+            // labels of the hybrid sample: Make_cnt_clusters, Make_gnp_clusters, Make_mixed_clusters
+            // (Hoshen_Kopelman.cpp:40-80 order), tol_gnp = 1.5 t_max as Input_Reader.cpp:1161 sets it
+            Hoshen_Kopelman HK3;
+            HK3.ignore_eror_cnt_inside_gnp = 1;
+            Cutoff_dist cut3 = cut;
+            cut3.min_points = 5;
+            double t_max = 0.0;
+            for (const GNP& g : gnps) t_max = std::max(t_max, g.t);
+            cut3.tol_gnp = 1.5 * t_max;
+            cut3.tol_gnp2 = cut3.tol_gnp * cut3.tol_gnp;
+            std::vector<int> lab_cnt(structure.size(), -1), lab_gnp(gnps.size(), -1);
+            int n_labels_cnt = 0;
+            if (!HK3.Make_cnt_clusters("GNP_CNT_mix", pts, radii, cut3, CG2.sectioned_domain_cnts, structure, lab_cnt, n_labels_cnt)) return 12;
+            int n_total = n_labels_cnt;
+            std::vector<std::vector<long int> > structure_gnp(gnps.size());
+            std::vector<Point_3D> points_gnp;
+            std::vector<bool> bp_flags;
+            if (!HK3.Make_gnp_clusters(false, geom.sample, inside, CG2.sectioned_domain_gnps, gnps, cut3, 0, n_labels_cnt, n_total, structure_gnp,
+                                       points_gnp, lab_gnp, bp_flags))
+                return 13;
+            o.i32("lab_cnt", lab_cnt);
+            o.i32("lab_gnp", lab_gnp);
+            o.i32("lab_counts", {n_labels_cnt, n_total});
+            int n_clusters = n_total;
+            if (!HK3.Make_mixed_clusters(n_total, cut3, pts, radii, CG2.sectioned_domain_cnts, gnps, CG2.sectioned_domain_gnps, lab_cnt, lab_gnp,
+                                         structure_gnp, points_gnp, n_clusters))
+                return 14;
+            o.i32("mixlab_cnt", lab_cnt);
+            o.i32("mixlab_gnp", lab_gnp);
+            o.i32("mixlab_count", {n_clusters});
             o.i32("mix_sd_cnt_ptr", sdc_ptr);
             o.i32("mix_sd_cnt_idx", sdc_idx);
             o.i32("mix_point", mp);

@@ -729,3 +729,71 @@ def pair_junction(VA, FA, VB, FB, vdw: float, lo, hi, allow_simplex3: bool = Fal
     if pen:
         PB = _sub(PB, m)
     return PA, PB, (1 if outside_box(PA, lo, hi) else 0) + (2 if outside_box(PB, lo, hi) else 0)
+
+
+# ---------------------------------------------------------------------------
+# Labels: HK76, Find_root, Merge_labels, Cleanup_labels (Hoshen_Kopelman.cpp:2908-2989, 374-425)
+
+
+def hk_labels(labels, labels_labels, contacts):
+    """Upstream's HK76 over `contacts` (pairs of particle indices, in order) on the
+    label state (labels per particle, labels_labels per raw label), then
+    Cleanup_labels: returns (proper labels, number of labels)."""
+    labels, LL = list(labels), list(labels_labels)
+
+    def root(L):
+        while LL[L] <= 0:
+            L = -LL[L]
+            if LL[L] == 0:
+                return 0
+        return L
+
+    new_label = len(LL)
+    for p1, p2 in contacts:
+        if labels[p1] == -1 and labels[p2] == -1:
+            labels[p1] = labels[p2] = new_label
+            new_label += 1
+            LL.append(2)
+        elif labels[p1] == -1 or labels[p2] == -1:
+            q, other = (p1, p2) if labels[p1] == -1 else (p2, p1)
+            L = labels[other]
+            if LL[L] <= 0:
+                L = root(L)
+            labels[q] = L
+            LL[L] += 1
+        elif labels[p1] != labels[p2]:
+            r1, r2 = root(labels[p1]), root(labels[p2])
+            if LL[r1] <= 0 or LL[r2] <= 0:
+                raise RuntimeError("Merge_labels: a root is not a root")
+            if r1 < r2:
+                LL[r1] += LL[r2]
+                LL[r2] = -r1
+            elif r2 < r1:
+                LL[r2] += LL[r1]
+                LL[r1] = -r2
+    proper = {}
+    for i, c in enumerate(LL):
+        if c > 0:
+            proper[i] = len(proper)
+    return [proper[root(L)] if L != -1 else -1 for L in labels], len(proper)
+
+
+def gnp_labels(n_gnps: int, pairs, outside, n_labels_cnt: int):
+    """Make_gnp_clusters' labels (:575-616): HK76 over the GNP-GNP contacts whose
+    junction points are inside the sample, Cleanup_labels, Renumber_gnp_labels."""
+    lab, n = hk_labels([-1] * n_gnps, [], [(a, b) for (a, b), o in zip(pairs, outside) if o == 0])
+    return [l + n_labels_cnt if l >= 0 else -1 for l in lab], n_labels_cnt + n
+
+
+def mixed_labels(labels_cnt, labels_gnp, n_total: int, cnt_gnp_contacts):
+    """Make_mixed_clusters' labels (:1925-1987): labels_labels starts at -1 for the
+    n_total earlier labels plus one per labelled particle (Initialize_mixed_labels),
+    HK76 over (CNT, n_cnts + GNP) in contact-number order, Cleanup_labels."""
+    n_cnts = len(labels_cnt)
+    labels = list(labels_cnt) + list(labels_gnp)
+    LL = [-1] * n_total
+    for L in labels:
+        if L != -1:
+            LL[L] += 1
+    lab, n = hk_labels(labels, LL, [(c, n_cnts + g) for c, g in cnt_gnp_contacts])
+    return lab[:n_cnts], lab[n_cnts:], n

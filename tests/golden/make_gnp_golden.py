@@ -17,6 +17,10 @@ SHA-256), it also stores upstream's CNT-GNP contacts of the mixed contact pass
 closest GNP point) and the SHA-256 of upstream's CNT region lists.  The fixture
 itself is self-contained apart from the seeded CNT network.
 
+Also writes tests/golden/gnp_hybrid_labels.npz: upstream's CNT, GNP and mixed
+labels of a sparser hybrid sample (30 GNPs, 250 CNTs), whose clusters stay
+apart.
+
     python tests/golden/make_gnp_golden.py
 """
 from __future__ import annotations
@@ -113,5 +117,43 @@ def main():
           f"{len(z['mix_point'])} CNT-GNP contacts")
 
 
+# A sparser hybrid sample whose labels stay apart: 30 GNPs (side 0.3-0.5 um) and 250 CNTs in 2 um
+SPARSE_N, SPARSE_SEED, SPARSE_CNTS, SPARSE_CNT_SEED = 30, 4_100_002, 250, 4_100_001
+
+
+def sparse_config() -> NetworkConfig:
+    return NetworkConfig(side=SIDE, n_cnts=SPARSE_CNTS, seed=SPARSE_CNT_SEED, vdw=VDW, tunnel=TUNNEL)
+
+
+def sparse_network(directory: str) -> dict:
+    cfg = sparse_config()
+    write_read_network_files(directory, generate_cnt_network(cfg), cfg)
+    return read_network_files(directory).arrays()
+
+
+def main_labels():
+    """tests/golden/gnp_hybrid_labels.npz: upstream's CNT, GNP and mixed labels of
+    the sparse hybrid sample (Make_cnt_clusters, Make_gnp_clusters,
+    Make_mixed_clusters) with its CNT-GNP contacts."""
+    g = generate_gnps(SPARSE_N, SIDE, SPARSE_SEED, l_range=(0.3, 0.5))
+    with tempfile.TemporaryDirectory() as d:
+        net = sparse_network(d)
+        write_gnp_file(d, g)
+        with open(os.path.join(d, "sample_geom.csv"), "w") as f:
+            f.write(f"0,0,0\n{SIDE!r},{SIDE!r},{SIDE!r}\n")
+        out = os.path.join(d, "gnp.bin")
+        subprocess.run([REF, d, out, repr(VDW), repr(TUNNEL), repr(GS_MIN), repr(OVERLAP_CNT), repr(float(OVERLAP_GNP))],
+                       check=True, capture_output=True, timeout=600)
+        z = read_dump(out)
+    keep = ("gnp_vertices", "gnp_planes", "lab_cnt", "lab_gnp", "lab_counts", "mixlab_cnt", "mixlab_gnp", "mixlab_count", "mix_point", "mix_gnp", "mix_index")
+    np.savez_compressed(os.path.join(HERE, "gnp_hybrid_labels.npz"), in_l=g["l"], in_t=g["t"], in_theta=g["theta"], in_phi=g["phi"],
+                        in_center=g["center"], meta=np.array([SPARSE_N, SIDE, SPARSE_SEED, VDW, TUNNEL, GS_MIN, OVERLAP_CNT, OVERLAP_GNP]),
+                        cnt_meta=np.array([SPARSE_CNTS, SPARSE_CNT_SEED]), cnt_sha256=np.array(net_hash(net)),
+                        **{"ref_" + k: z[k] for k in keep})
+    print(f"sparse hybrid: {int(z['lab_counts'][0])} CNT labels, {int(z['lab_counts'][1])} with the GNPs, "
+          f"{int(z['mixlab_count'][0])} mixed clusters, {len(z['mix_point'])} CNT-GNP contacts")
+
+
 if __name__ == "__main__":
     main()
+    main_labels()

@@ -265,3 +265,55 @@ def test_junction_oracle_matches_upstream_golden(path, side):
             mine = np.array(list(r[0]) + list(r[1]))
             assert np.array_equal(mine.view(np.int64), z["ref_junc_points"][6 * i:6 * i + 6].view(np.int64))
             assert r[2] == z["ref_junc_outside"][i]
+
+
+LABELS = os.path.join(ROOT, "tests", "golden", "gnp_hybrid_labels.npz")
+
+
+def hybrid_oracle_labels(z, directory, network):
+    """The labels of a hybrid sample from the CPU restatements alone: CNT region
+    lists and CNT labels (oracle/cicy_oracle.py), GNP region lists, GNP-GNP
+    contacts and junction points, CNT-GNP contacts, then the GNP and mixed HK76
+    passes (oracle/gnp_oracle.py), on upstream's GNPs."""
+    from oracle import cicy_oracle as O, gnp_oracle as G
+
+    side, gs, ov_cnt, ov_gnp = float(z["meta"][1]), float(z["meta"][5]), float(z["meta"][6]), float(z["meta"][7])
+    vdw, tunnel = float(z["meta"][3]), float(z["meta"][4])
+    net = dict(network(directory))
+    net["cnts_inside"] = np.arange(len(net["radii"]))
+    win = [0.0, 0.0, 0.0, side, side, side, side, side, side]
+    net["window"] = np.array(win)
+    p = {"gs_min": (gs,) * 3, "gs_overlap_cnt": ov_cnt, "gs_overlap_gnp": ov_gnp, "vdw": vdw, "tunnel": tunnel}
+    n, l, regs = O.contact_grid(net, p)
+    lab_cnt, n_cnt, _, _ = O.label_cnts(net, p, regs)
+    N = len(z["in_l"])
+    V, F = z["ref_gnp_vertices"].reshape(N, 8, 3), z["ref_gnp_planes"].reshape(N, 6, 4).tolist()
+    sd_gnp = G.fill_sectioned_domain_gnps(win, V, z["in_l"], z["in_t"], range(N), n, l, ov_gnp)
+    V = V.tolist()
+    pairs = G.contact_pairs(sd_gnp, V, vdw, tunnel)
+    outside = [G.pair_junction(V[a], F[a], V[b], F[b], vdw, win[0:3], win[6:9])[2] for a, b, *_ in pairs]
+    lab_gnp, n_total = G.gnp_labels(N, [(a, b) for a, b, *_ in pairs], outside, n_cnt)
+    mix = G.find_adjacent_labels(np.stack([net["x"], net["y"], net["z"]], 1).tolist(), net["flag"], net["radii"], regs, sd_gnp, V, F, vdw,
+                                 tunnel)
+    contacts = [(int(net["flag"][P]), g) for (P, g), _ in sorted(mix.items(), key=lambda kv: kv[1][0])]
+    return (lab_cnt, n_cnt), (lab_gnp, n_total), G.mixed_labels(lab_cnt, lab_gnp, n_total, contacts)
+
+
+@pytest.mark.parametrize("path", [GOLDEN, LABELS])
+def test_hybrid_labels_oracle_matches_upstream_golden(tmp_path, path):
+    """CNT, GNP and mixed labels of a hybrid sample restated on the CPU against
+    upstream's Make_cnt_clusters, Make_gnp_clusters and Make_mixed_clusters: the
+    120-GNP fixture (one mixed cluster) and the sparse one (28 CNT and 4 GNP
+    labels into 25 mixed clusters)."""
+    import sys
+
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_gnp_golden as M
+
+    z = dict(np.load(path))
+    network = M.hybrid_network if path == GOLDEN else M.sparse_network
+    assert M.net_hash(network(str(tmp_path))) == str(z["cnt_sha256"])
+    (lc, nc), (lg, nt), (mc, mg, nm) = hybrid_oracle_labels(z, str(tmp_path), network)
+    assert list(lc) == list(z["ref_lab_cnt"]) and nc == z["ref_lab_counts"][0]
+    assert list(lg) == list(z["ref_lab_gnp"]) and nt == z["ref_lab_counts"][1]
+    assert list(mc) == list(z["ref_mixlab_cnt"]) and list(mg) == list(z["ref_mixlab_gnp"]) and nm == z["ref_mixlab_count"][0]

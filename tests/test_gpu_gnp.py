@@ -203,3 +203,50 @@ def test_gnp_junction_points_match_upstream_golden(cuda_ok, tmp_path, path, side
     pts = np.concatenate([pa, pb], 1)[ok]
     assert np.array_equal(pts.view(np.int64), z["ref_junc_points"].reshape(-1, 6)[ok].view(np.int64))
     assert np.array_equal(out[ok], z["ref_junc_outside"][ok])
+
+
+LABELS = os.path.join(ROOT, "tests", "golden", "gnp_hybrid_labels.npz")
+
+
+@pytest.mark.parametrize("path", [GOLDEN, LABELS])
+def test_hybrid_labels_match_upstream_golden(cuda_ok, tmp_path, path):
+    """The hybrid labelling chain on the device against upstream: CNT labels of
+    the hybrid grid (cicy_clusters), GNP labels from the GNP-GNP contact pass with
+    junction points (cicy_gnp_contact_pairs, cicy_gnp_labels), CNT-GNP contacts
+    (cicy_gnp_cnt_contacts) and the mixed labels (cicy_mixed_labels)."""
+    import sys
+
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_gnp_golden as M
+    from cicy_geom_b200.device import Context
+    from cicy_geom_b200.network import HostNetwork, gnp_contact_pairs
+
+    z = dict(np.load(path))
+    d = str(tmp_path)
+    network, cfg = (M.hybrid_network, M.cnt_config()) if path == GOLDEN else (M.sparse_network, M.sparse_config())
+    net = {k: v for k, v in network(d).items() if not k.startswith("boundary")}
+    assert M.net_hash(net) == str(z["cnt_sha256"])
+    side, gs, ov_cnt, ov_gnp = float(z["meta"][1]), float(z["meta"][5]), float(z["meta"][6]), float(z["meta"][7])
+    win = [0.0, 0.0, 0.0, side, side, side, side, side, side]
+    net["cnts_inside"] = np.arange(len(net["radii"]), dtype=np.int32)
+    net["window"] = np.array(win)
+    write_gnp_file(d, {"l": z["in_l"], "t": z["in_t"], "theta": z["in_theta"], "phi": z["in_phi"], "center": z["in_center"]})
+    p = cfg.params()
+    for a in range(3):
+        p.gs_min[a] = gs
+    p.gs_overlap_cnt, p.gs_overlap_gnp = ov_cnt, ov_gnp
+    with Context(0) as ctx:
+        ctx.upload(HostNetwork.from_arrays(net))
+        ctx.contact_grid(p)
+        ctx.clusters(p)
+        lab_cnt, n_cnt = ctx.labels()
+        assert np.array_equal(lab_cnt, z["ref_lab_cnt"]) and n_cnt == z["ref_lab_counts"][0]
+        gp = gnp_contact_pairs(d, np.arange(len(z["in_l"])), win, [gs] * 3, ov_cnt, ov_gnp, p.van_der_waals_dist, p.tunneling_dist,
+                               n_labels_cnt=n_cnt)
+        assert np.array_equal(gp["labels_gnp"], z["ref_lab_gnp"]) and gp["n_total_labels"] == z["ref_lab_counts"][1]
+        pt, g, _, _ = ctx.gnp_cnt_contacts(d, p)
+        order = np.argsort(z["ref_mix_index"])
+        assert np.array_equal(pt, z["ref_mix_point"][order]) and np.array_equal(g, z["ref_mix_gnp"][order])
+        mc, mg, nm = ctx.mixed_labels(gp["labels_gnp"], gp["n_total_labels"])
+        assert np.array_equal(mc, z["ref_mixlab_cnt"]) and np.array_equal(mg, z["ref_mixlab_gnp"]) and nm == z["ref_mixlab_count"][0]
+        assert np.array_equal(ctx.labels()[0], mc)
