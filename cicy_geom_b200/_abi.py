@@ -173,6 +173,21 @@ class GnpPairList(C.Structure):
     ]
 
 
+class GnpPointList(C.Structure):
+    _fields_ = [
+        ("n_points", C.c_int64),
+        ("points", C.c_void_p),
+        ("n_gnps", C.c_int32),
+        ("structure_ptr", C.c_void_p),
+        ("structure_idx", C.c_void_p),
+        ("n_junctions", C.c_int64),
+        ("junctions", C.c_void_p),
+        ("junction_dist", C.c_void_p),
+        ("n_boundary", C.c_int32),
+        ("boundary_used", C.c_void_p),
+    ]
+
+
 class GenParams(C.Structure):
     _fields_ = [
         ("sample", Cuboid),
@@ -251,6 +266,11 @@ def lib() -> C.CDLL:
         "cicy_gnp_pairs_view": (C.c_int, [C.c_void_p, P(GnpPairList)]),
         "cicy_gnp_pairs_free": (None, [C.c_void_p]),
         "cicy_gnp_labels": (C.c_int, [C.c_int, C.c_void_p, C.c_int32, C.c_int32, i32p, i32p]),
+        "cicy_gnp_junction_structures": (C.c_int, [C.c_int, C.c_void_p, C.c_int32, C.c_double, C.c_int32, f64p, i32p, i32p, P(C.c_void_p)]),
+        "cicy_gnp_points_view": (C.c_int, [C.c_void_p, P(GnpPointList)]),
+        "cicy_gnp_points_free": (None, [C.c_void_p]),
+        "cicy_mixed_junctions": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, i64p]),
+        "cicy_get_mixed_junctions": (C.c_int, [C.c_void_p, i64p, i64p, i32p, i64p, i32p, f64p, f64p]),
         "cicy_mixed_labels": (C.c_int, [C.c_void_p, i32p, C.c_int32, C.c_int32, i32p, i32p, i32p]),
         "cicy_gnp_cnt_contacts": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, P(Params), C.c_int32, i64p]),
         "cicy_get_gnp_cnt_contacts": (C.c_int, [C.c_void_p, i64p, i64p, i32p, f64p, f64p]),

@@ -186,6 +186,31 @@ cicy_status cicy_mixed_labels(cicy_ctx* ctx, const int32_t* labels_gnp, int32_t 
     });
 }
 
+cicy_status cicy_mixed_junctions(cicy_ctx* ctx, int64_t n_points_gnp, int32_t min_points, int64_t* n_junctions) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (n_points_gnp < 0 || n_points_gnp >= (1LL << 31)) throw cicy::Fail{CICY_E_INPUT, "cicy_mixed_junctions: invalid point count"};
+        const int n = cicy::run_mixed_junctions(c, (int)n_points_gnp, min_points, c.h_mixj, c.h_mixj_dist, c.h_mixj_points);
+        if (n_junctions) *n_junctions = n;
+    });
+}
+
+cicy_status cicy_get_mixed_junctions(cicy_ctx* ctx, int64_t* n, int64_t* cnt_point, int32_t* cnt, int64_t* gnp_point, int32_t* gnp, double* dist,
+                                     double* points) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        const size_t J = c.h_mixj_dist.size();
+        if (n) *n = (int64_t)J;
+        for (size_t j = 0; j < J; j++) {
+            if (cnt_point) cnt_point[j] = c.h_mixj[4 * j];
+            if (cnt) cnt[j] = c.h_mixj[4 * j + 1];
+            if (gnp_point) gnp_point[j] = c.h_mixj[4 * j + 2];
+            if (gnp) gnp[j] = c.h_mixj[4 * j + 3];
+            if (dist) dist[j] = c.h_mixj_dist[j];
+            if (points)
+                for (int d = 0; d < 3; d++) points[3 * j + d] = c.h_mixj_points[3 * j + d];
+        }
+    });
+}
+
 cicy_status cicy_get_gnp_cnt_contacts(cicy_ctx* ctx, int64_t* n, int64_t* point, int32_t* gnp, double* dist, double* closest) {
     return guarded(ctx, [&](cicy::Ctx& c) {
         const int U = c.n_mix;

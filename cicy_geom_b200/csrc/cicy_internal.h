@@ -56,6 +56,18 @@ struct GnpPairs {
 };
 void gnp_contact_pairs(const GnpSet& g, const GnpGrid& grid, double vdw, double tunnel, const cicy_cuboid& sample, bool allow_simplex3,
                        GnpPairs& out);
+// GNP point structures after Add_gnp_junction (gnp_labels.cu).
+struct GnpStructures {
+    std::vector<double> points;                   // 3 per point: the initial ones, then the junction points
+    std::vector<int32_t> structure_ptr, structure_idx;
+    std::vector<int32_t> junctions;               // Pa, GNPa, Pb, GNPb per junction
+    std::vector<double> junction_dist;
+    int32_t n_boundary = 0;                       // initial points (gnp_pts_bdds)
+    std::vector<int32_t> boundary_used;           // bp_flags
+    int64_t launches = 0;
+};
+void gnp_junction_structures(const GnpPairs& pairs, int n_gnps, double tol_gnp2, const std::vector<double>& init_points,
+                             const std::vector<int32_t>& init_ptr, const std::vector<int32_t>& init_idx, GnpStructures& out);
 // Message returned by cicy_host_last_error() on this thread.
 void set_host_error(const std::string& msg);
 void host_network_view(const HostNetwork& h, cicy_network& v);
@@ -76,4 +88,8 @@ struct cicy_gnp_grid {
 
 struct cicy_gnp_pairs {
     cicy::GnpPairs pairs;
+};
+
+struct cicy_gnp_points {
+    cicy::GnpStructures s;
 };

@@ -139,6 +139,8 @@ struct Ctx {
     int n_mix = 0;
     DBuf<int32_t> mix_point, mix_gnp;
     DBuf<double> mix_dist, mix_closest;
+    std::vector<int32_t> h_mixj;        // cicy_mixed_junctions results
+    std::vector<double> h_mixj_dist, h_mixj_points;
 
     ~Ctx();
 };
@@ -154,6 +156,10 @@ struct GnpGrid;
 int run_gnp_cnt_contacts(Ctx& c, const GnpSet& g, const GnpGrid& grid, const cicy_params& p, int inside_is_error);
 // Make_mixed_clusters' labels (gnp_labels.cu); returns the number of clusters.
 int run_mixed_labels(Ctx& c, const int32_t* labels_gnp, int n_gnps, int n_total_labels, int32_t* labels_cnt_out, int32_t* labels_gnp_out);
+// Compress_mixed_contacts on the context's CNT-GNP contacts (gnp_labels.cu):
+// junctions (P_cnt, CNT, P_gnp, GNP) x4, distances and the new GNP points.
+int run_mixed_junctions(Ctx& c, int n_points_before, int min_points, std::vector<int32_t>& junctions, std::vector<double>& dist,
+                        std::vector<double>& points);
 
 // Learned preconditioner: edge weights for the system being solved (learned.cu).
 const float* learned_edge_weights(Ctx& c, const SolverSystem& ss, int n_chains, cudaStream_t s);

@@ -139,6 +139,20 @@ class Context:
                                             _p(lg, C.c_int32), C.byref(n)), "cicy_mixed_labels")
         return lc[:nc], lg[:len(g)], int(n.value)
 
+    def mixed_junctions(self, n_points_gnp: int, min_points: int) -> dict:
+        """Compress_mixed_contacts on the CNT-GNP contacts (cicy_mixed_junctions):
+        junctions (cnt_point, cnt, gnp_point, gnp, dist) and the new GNP points,
+        numbered from n_points_gnp."""
+        n = C.c_int64()
+        self._check(lib().cicy_mixed_junctions(self._h, int(n_points_gnp), int(min_points), C.byref(n)), "cicy_mixed_junctions")
+        J = n.value
+        cp, gp = np.zeros(max(J, 1), np.int64), np.zeros(max(J, 1), np.int64)
+        c, g = np.zeros(max(J, 1), np.int32), np.zeros(max(J, 1), np.int32)
+        d, q = np.zeros(max(J, 1)), np.zeros((max(J, 1), 3))
+        self._check(lib().cicy_get_mixed_junctions(self._h, C.byref(n), _p(cp, C.c_int64), _p(c, C.c_int32), _p(gp, C.c_int64), _p(g, C.c_int32),
+                                                   _p(d, C.c_double), _p(q, C.c_double)), "cicy_get_mixed_junctions")
+        return {"cnt_point": cp[:J], "cnt": c[:J], "gnp_point": gp[:J], "gnp": g[:J], "dist": d[:J], "points": q[:J]}
+
     def clusters(self, p: _abi.Params):
         self._check(lib().cicy_clusters(self._h, C.byref(p)), "cicy_clusters")
 

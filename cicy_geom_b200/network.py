@@ -467,7 +467,7 @@ def gnp_junction_points(directory: str, a, b, vdw: float, sample, allow_simplex3
 
 
 def gnp_contact_pairs(directory: str, inside, window, gs_min, overlap_cnt: float, overlap_gnp: float, vdw: float, tunnel: float,
-                      sample=None, allow_simplex3: bool = False, n_labels_cnt=None, device: int = 0) -> dict:
+                      sample=None, allow_simplex3: bool = False, n_labels_cnt=None, tol_gnp2=None, device: int = 0) -> dict:
     """GNP-GNP contact pass of Label_gnps_in_window on the device: the GNP region
     lists (cicy_gnp_sectioned_domain of `inside`) and every pair sharing a region,
     measured once, with the junction points of each contact
@@ -476,7 +476,10 @@ def gnp_contact_pairs(directory: str, inside, window, gs_min, overlap_cnt: float
     displacement [n, 3], point_a, point_b [n, 3], outside [n] (against `sample`,
     default the window), and the visit and pair counts; with `n_labels_cnt`, also
     the GNP labels of Make_gnp_clusters (cicy_gnp_labels): labels_gnp and
-    n_total_labels."""
+    n_total_labels; with `tol_gnp2`, also the GNP point structures of
+    Add_gnp_junction (cicy_gnp_junction_structures, no initial points):
+    gnp_points [m, 3], structure_ptr, structure_idx, junctions [k, 4] (Pa, GNPa,
+    Pb, GNPb), junction_dist."""
     h = C.c_void_p()
     check(lib().cicy_read_gnps(directory.encode(), C.byref(h)), "cicy_read_gnps")
     grid, pairs = C.c_void_p(), C.c_void_p()
@@ -506,6 +509,23 @@ def gnp_contact_pairs(directory: str, inside, window, gs_min, overlap_cnt: float
             tot = C.c_int32()
             check(lib().cicy_gnp_labels(device, pairs, gv.n, int(n_labels_cnt), lab.ctypes.data_as(_abi.i32p), C.byref(tot)), "cicy_gnp_labels")
             res = {"labels_gnp": lab[:gv.n], "n_total_labels": int(tot.value)}
+        if tol_gnp2 is not None:
+            gv = _abi.Gnps()
+            check(lib().cicy_gnp_set_view(h, C.byref(gv)), "cicy_gnp_set_view")
+            pts = C.c_void_p()
+            check(lib().cicy_gnp_junction_structures(device, pairs, gv.n, float(tol_gnp2), 0, None, None, None, C.byref(pts)),
+                  "cicy_gnp_junction_structures")
+            try:
+                pv = _abi.GnpPointList()
+                check(lib().cicy_gnp_points_view(pts, C.byref(pv)), "cicy_gnp_points_view")
+                npt, nj = int(pv.n_points), int(pv.n_junctions)
+                res.update({"gnp_points": arr(pv.points, C.c_double, 3 * npt, np.float64).reshape(npt, 3),
+                            "structure_ptr": arr(pv.structure_ptr, C.c_int32, pv.n_gnps + 1, np.int32),
+                            "junctions": arr(pv.junctions, C.c_int32, 4 * nj, np.int32).reshape(nj, 4),
+                            "junction_dist": arr(pv.junction_dist, C.c_double, nj, np.float64)})
+                res["structure_idx"] = arr(pv.structure_idx, C.c_int32, int(res["structure_ptr"][-1]), np.int32)
+            finally:
+                lib().cicy_gnp_points_free(pts)
         return {**res, "a": arr(v.a, C.c_int32, n, np.int32), "b": arr(v.b, C.c_int32, n, np.int32),
                 "penetrating": arr(v.penetrating, C.c_int32, n, np.int32), "dist": arr(v.dist, C.c_double, n, np.float64),
                 "direction": arr(v.direction, C.c_double, 3 * n, np.float64).reshape(n, 3),

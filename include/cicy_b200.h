@@ -503,6 +503,48 @@ cicy_status cicy_gnp_labels(int device, const cicy_gnp_pairs* pairs, int32_t n_g
 cicy_status cicy_mixed_labels(cicy_ctx* ctx, const int32_t* labels_gnp, int32_t n_gnps, int32_t n_total_labels, int32_t* labels_cnt,
                               int32_t* labels_gnp_out, int32_t* n_clusters);
 
+/* GNP point structures on the device, Add_gnp_junction and
+ * Add_gnp_point_to_vectors_if_not_repeated (Hoshen_Kopelman.cpp:1837-1923)
+ * over the contact pairs whose junction points are both inside the sample, in
+ * list order: the point on a, then on b, joins its GNP's point list; a point of
+ * an interpenetrating pair reuses the first point of that list within squared
+ * distance tol_gnp2 (Cutoff_dist::tol_gnp2), else it is appended with the next
+ * global number.  Initial points (upstream's points_gnp before the pass, e.g.
+ * window boundary points; gnp_pts_bdds = n_init_points) and per-GNP lists
+ * (CSR; NULL for none) may be given. */
+typedef struct cicy_gnp_points cicy_gnp_points;
+typedef struct {
+    int64_t n_points;
+    const double* points;          /* [3 n_points]: initial points, then the junction points */
+    int32_t n_gnps;
+    const int32_t* structure_ptr;  /* [n_gnps + 1] structure_gnp as CSR */
+    const int32_t* structure_idx;
+    int64_t n_junctions;
+    const int32_t* junctions;      /* [4 n_junctions]: Pa, GNPa, Pb, GNPb (junctions_gnp) */
+    const double* junction_dist;   /* [n_junctions] */
+    int32_t n_boundary;            /* gnp_pts_bdds */
+    const int32_t* boundary_used;  /* [n_boundary] bp_flags */
+} cicy_gnp_point_list;
+cicy_status cicy_gnp_junction_structures(int device, const cicy_gnp_pairs* pairs, int32_t n_gnps, double tol_gnp2, int32_t n_init_points,
+                                         const double* init_points, const int32_t* init_ptr, const int32_t* init_idx, cicy_gnp_points** out);
+/* Borrowed view; valid until cicy_gnp_points_free. */
+cicy_status cicy_gnp_points_view(const cicy_gnp_points* p, cicy_gnp_point_list* view);
+void cicy_gnp_points_free(cicy_gnp_points* p);
+
+/* Compress_mixed_contacts / Add_mixed_junction (Hoshen_Kopelman.cpp:2181-2306)
+ * on the device, over the context's CNT-GNP contacts (cicy_gnp_cnt_contacts):
+ * GNPs ascending, the CNTs in contact with each ascending, their contact
+ * points ascending, cut into runs at min_points past a run's first point, each
+ * run kept at its first point of least junction distance.  Junction j joins CNT
+ * point cnt_point[j] of CNT cnt[j] to the new GNP point gnp_point[j] =
+ * n_points_gnp + j of GNP gnp[j] (its closest point points[3j..]); upstream
+ * appends these points to points_gnp and structure_gnp[gnp[j]] in this order
+ * and adds cnt_point[j] to elements_cnt[cnt[j]].  Results via
+ * cicy_get_mixed_junctions (size query: NULL buffers). */
+cicy_status cicy_mixed_junctions(cicy_ctx* ctx, int64_t n_points_gnp, int32_t min_points, int64_t* n_junctions);
+cicy_status cicy_get_mixed_junctions(cicy_ctx* ctx, int64_t* n, int64_t* cnt_point, int32_t* cnt, int64_t* gnp_point, int32_t* gnp, double* dist,
+                                     double* points);
+
 /* CNT-GNP contacts of the hybrid CNT/GNP sample on the device:
  * Hoshen_Kopelman::Find_adjacent_labels (Hoshen_Kopelman.cpp:1989-2142) over
  * Contact_grid::Generate_contact_grid with particle type GNP_CNT_mix.  The

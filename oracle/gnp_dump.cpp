@@ -49,6 +49,7 @@
  * u64 count, payload (the layout oracle/dumpio.py reads).
  */
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <map>
 #include <set>
@@ -186,8 +187,13 @@ int main(int argc, char** argv) {
             if (!RN.Read_cnt_data_from_dat(pts, radii, structure)) return 9;
             std::vector<int> cin(structure.size());
             for (size_t i = 0; i < cin.size(); i++) cin[i] = (int)i;
+            using clk = std::chrono::steady_clock;
+            auto secs = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); };
+            std::vector<double> ref_seconds;  // contact grid, CNT clusters, GNP clusters, mixed clusters (the upstream calls only)
+            const auto t0 = clk::now();
             Contact_grid CG2;
             if (!CG2.Generate_contact_grid(0, "GNP_CNT_mix", geom, w, cin, pts, structure, inside, gnps)) return 10;
+            ref_seconds.push_back(secs(t0, clk::now()));
             Hoshen_Kopelman HK2;
             HK2.ignore_eror_cnt_inside_gnp = 1;
             std::vector<int> labels_cnt(structure.size(), -1), labels_gnp(gnps.size(), -1);
@@ -226,21 +232,63 @@ int main(int argc, char** argv) {
             cut3.tol_gnp2 = cut3.tol_gnp * cut3.tol_gnp;
             std::vector<int> lab_cnt(structure.size(), -1), lab_gnp(gnps.size(), -1);
             int n_labels_cnt = 0;
+            auto t1 = clk::now();
             if (!HK3.Make_cnt_clusters("GNP_CNT_mix", pts, radii, cut3, CG2.sectioned_domain_cnts, structure, lab_cnt, n_labels_cnt)) return 12;
+            ref_seconds.push_back(secs(t1, clk::now()));
             int n_total = n_labels_cnt;
             std::vector<std::vector<long int> > structure_gnp(gnps.size());
             std::vector<Point_3D> points_gnp;
             std::vector<bool> bp_flags;
+            t1 = clk::now();
             if (!HK3.Make_gnp_clusters(false, geom.sample, inside, CG2.sectioned_domain_gnps, gnps, cut3, 0, n_labels_cnt, n_total, structure_gnp,
                                        points_gnp, lab_gnp, bp_flags))
                 return 13;
+            ref_seconds.push_back(secs(t1, clk::now()));
             o.i32("lab_cnt", lab_cnt);
             o.i32("lab_gnp", lab_gnp);
             o.i32("lab_counts", {n_labels_cnt, n_total});
+            auto dump_points = [&](const std::string& pre) {
+                std::vector<double> xyz;
+                std::vector<int> sp(1, 0), si;
+                for (const Point_3D& q : points_gnp) xyz.insert(xyz.end(), {q.x, q.y, q.z});
+                for (const auto& st : structure_gnp) {
+                    for (long int v : st) si.push_back((int)v);
+                    sp.push_back((int)si.size());
+                }
+                o.f64(pre + "points", xyz);
+                o.i32(pre + "structure_ptr", sp);
+                o.i32(pre + "structure_idx", si);
+            };
+            auto dump_junctions = [&](const std::string& name, const std::vector<Junction>& js) {
+                std::vector<int> v;
+                std::vector<double> dd;
+                for (const Junction& j : js) {
+                    v.insert(v.end(), {(int)j.P1, j.N1, (int)j.P2, j.N2});
+                    dd.push_back(j.junction_dist);
+                }
+                o.i32(name, v);
+                o.f64(name + "_dist", dd);
+            };
+            dump_points("gnpjn_");
+            dump_junctions("junctions_gnp", HK3.junctions_gnp);
             int n_clusters = n_total;
+            t1 = clk::now();
             if (!HK3.Make_mixed_clusters(n_total, cut3, pts, radii, CG2.sectioned_domain_cnts, gnps, CG2.sectioned_domain_gnps, lab_cnt, lab_gnp,
                                          structure_gnp, points_gnp, n_clusters))
                 return 14;
+            ref_seconds.push_back(secs(t1, clk::now()));
+            o.f64("ref_seconds", ref_seconds);
+            dump_points("mixjn_");
+            dump_junctions("junctions_mixed", HK3.junctions_mixed);
+            {
+                std::vector<int> ep(1, 0), ei;
+                for (const auto& e : HK3.elements_cnt) {
+                    for (long int v : e) ei.push_back((int)v);
+                    ep.push_back((int)ei.size());
+                }
+                o.i32("mix_elements_ptr", ep);
+                o.i32("mix_elements_idx", ei);
+            }
             o.i32("mixlab_cnt", lab_cnt);
             o.i32("mixlab_gnp", lab_gnp);
             o.i32("mixlab_count", {n_clusters});

@@ -797,3 +797,81 @@ def mixed_labels(labels_cnt, labels_gnp, n_total: int, cnt_gnp_contacts):
             LL[L] += 1
     lab, n = hk_labels(labels, LL, [(c, n_cnts + g) for c, g in cnt_gnp_contacts])
     return lab[:n_cnts], lab[n_cnts:], n
+
+
+# ---------------------------------------------------------------------------
+# GNP point structures: Add_gnp_junction (Hoshen_Kopelman.cpp:1837-1923) and
+# Compress_mixed_contacts / Add_mixed_junction (:2181-2306)
+
+
+def add_gnp_junctions(contacts, n_gnps: int, tol_gnp2: float, points=None, structure=None):
+    """Add_gnp_junction for every GNP-GNP contact with both junction points inside
+    the sample, in contact order.  `contacts`: (a, b, dist, penetrating, point_a,
+    point_b, outside).  A point of an interpenetrating pair reuses the first point
+    of its GNP's structure within squared distance tol_gnp2
+    (Add_gnp_point_to_vectors_if_not_repeated), else it is appended.  Returns
+    (points, structure, junctions (Pa, a, Pb, b, dist), boundary-point flags)."""
+    points = [tuple(p) for p in (points or [])]
+    structure = [list(s) for s in (structure or [[] for _ in range(n_gnps)])]
+    bp = [False] * len(points)
+    n_bdd = len(points)
+    junctions = []
+
+    def add(P, g, pen):
+        if pen:
+            for q in structure[g]:
+                dx, dy, dz = P[0] - points[q][0], P[1] - points[q][1], P[2] - points[q][2]
+                if dx * dx + dy * dy + dz * dz < tol_gnp2:
+                    return q
+        points.append(tuple(P))
+        structure[g].append(len(points) - 1)
+        return len(points) - 1
+
+    for a, b, d, pen, PA, PB, out in contacts:
+        if out != 0:
+            continue
+        Pa, Pb = add(PA, a, pen), add(PB, b, pen)
+        junctions.append((Pa, a, Pb, b, d))
+        for P in (Pa, Pb):
+            if P < n_bdd:
+                bp[P] = True
+    return points, structure, junctions, bp
+
+
+def compress_mixed_contacts(contacts: dict, cnt_of_point, min_points: int, points, structure):
+    """Compress_mixed_contacts: for each GNP ascending, each CNT in contact with it
+    ascending, the CNT's contact points ascending are cut into runs (a new run
+    when a point is min_points or more past the run's first point); each run
+    keeps its first point of least junction distance, whose closest GNP point is
+    appended to the GNP's structure (Add_mixed_junction).  `contacts`:
+    {(P, GNP): (contact number, junction distance, closest point)}.  Returns
+    (points, structure, junctions (P_cnt, CNT, P_gnp, GNP, dist), CNT element
+    points added)."""
+    points = [tuple(p) for p in points]
+    structure = [list(s) for s in structure]
+    by_gnp = {}
+    for (P, g) in contacts:
+        by_gnp.setdefault(g, {}).setdefault(int(cnt_of_point[P]), []).append(P)
+    closest = {v[0]: v[2] for v in contacts.values()}
+    junctions, elements = [], []
+
+    def emit(Pi, Pj, c, g, d):
+        points.append(tuple(closest[Pi]))
+        structure[g].append(len(points) - 1)
+        junctions.append((Pj, c, len(points) - 1, g, d))
+        elements.append((c, Pj))
+
+    for g in sorted(by_gnp):
+        for c in sorted(by_gnp[g]):
+            Ps = sorted(by_gnp[g][c])
+            Pj0 = Ps[0]
+            Pi_j, Pj_j, dmin = contacts[(Pj0, g)][0], Pj0, contacts[(Pj0, g)][1]
+            for Pj1 in Ps[1:]:
+                Pi1, d = contacts[(Pj1, g)][0], contacts[(Pj1, g)][1]
+                if Pj1 - Pj0 >= min_points:
+                    emit(Pi_j, Pj_j, c, g, dmin)
+                    dmin, Pi_j, Pj_j, Pj0 = d, Pi1, Pj1, Pj1
+                elif d < dmin:
+                    dmin, Pi_j, Pj_j = d, Pi1, Pj1
+            emit(Pi_j, Pj_j, c, g, dmin)
+    return points, structure, junctions, elements

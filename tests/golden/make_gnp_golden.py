@@ -10,7 +10,8 @@ GNP part of the contact grid (0.05 um regions, overlaps as Input_Reader sets
 them) and, for every candidate pair, upstream's GNP-GNP distance step (GJK
 distance, EPA when the GNPs interpenetrate, the move of the second GNP) and,
 for the pairs within the tunnelling cutoff, upstream's junction points: the
-oracle of the GNP contact search.  With a seeded 400-CNT network in the same
+oracle of the GNP contact search.  The hybrid sample also gets upstream's
+labels, GNP point structures and GNP / mixed junction lists.  With a seeded 400-CNT network in the same
 cube (regenerated by the tests from its seed and checked against the stored
 SHA-256), it also stores upstream's CNT-GNP contacts of the mixed contact pass
 (Find_adjacent_labels: point, GNP, contact-point number, junction distance,
@@ -134,7 +135,8 @@ def sparse_network(directory: str) -> dict:
 def main_labels():
     """tests/golden/gnp_hybrid_labels.npz: upstream's CNT, GNP and mixed labels of
     the sparse hybrid sample (Make_cnt_clusters, Make_gnp_clusters,
-    Make_mixed_clusters) with its CNT-GNP contacts."""
+    Make_mixed_clusters) with its CNT-GNP contacts, the GNP point structures and
+    junctions after Add_gnp_junction and after Compress_mixed_contacts."""
     g = generate_gnps(SPARSE_N, SIDE, SPARSE_SEED, l_range=(0.3, 0.5))
     with tempfile.TemporaryDirectory() as d:
         net = sparse_network(d)
@@ -145,7 +147,9 @@ def main_labels():
         subprocess.run([REF, d, out, repr(VDW), repr(TUNNEL), repr(GS_MIN), repr(OVERLAP_CNT), repr(float(OVERLAP_GNP))],
                        check=True, capture_output=True, timeout=600)
         z = read_dump(out)
-    keep = ("gnp_vertices", "gnp_planes", "lab_cnt", "lab_gnp", "lab_counts", "mixlab_cnt", "mixlab_gnp", "mixlab_count", "mix_point", "mix_gnp", "mix_index")
+    keep = ("gnp_vertices", "gnp_planes", "lab_cnt", "lab_gnp", "lab_counts", "mixlab_cnt", "mixlab_gnp", "mixlab_count", "mix_point", "mix_gnp",
+            "mix_index", "gnpjn_points", "gnpjn_structure_ptr", "gnpjn_structure_idx", "junctions_gnp", "junctions_gnp_dist", "mixjn_points",
+            "mixjn_structure_ptr", "mixjn_structure_idx", "junctions_mixed", "junctions_mixed_dist")
     np.savez_compressed(os.path.join(HERE, "gnp_hybrid_labels.npz"), in_l=g["l"], in_t=g["t"], in_theta=g["theta"], in_phi=g["phi"],
                         in_center=g["center"], meta=np.array([SPARSE_N, SIDE, SPARSE_SEED, VDW, TUNNEL, GS_MIN, OVERLAP_CNT, OVERLAP_GNP]),
                         cnt_meta=np.array([SPARSE_CNTS, SPARSE_CNT_SEED]), cnt_sha256=np.array(net_hash(net)),

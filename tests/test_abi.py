@@ -25,6 +25,8 @@ def test_struct_sizes_match_header_layout():
     # cicy_gnps: n (+4 padding); 6 pointers.  cicy_gnp_pair_list: 3 counts; 9 pointers
     assert C.sizeof(_abi.Gnps) == 8 + 8 * 6
     assert C.sizeof(_abi.GnpPairList) == 8 * 3 + 8 * 9
+    # cicy_gnp_point_list: count, pointer, n_gnps (+4), 2 pointers, count, 2 pointers, n_boundary (+4), pointer
+    assert C.sizeof(_abi.GnpPointList) == 8 * 2 + 8 + 8 * 2 + 8 * 3 + 8 + 8
 
 
 def test_context_creation_without_gpu_fails_cleanly():

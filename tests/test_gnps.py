@@ -296,6 +296,7 @@ def hybrid_oracle_labels(z, directory, network):
     mix = G.find_adjacent_labels(np.stack([net["x"], net["y"], net["z"]], 1).tolist(), net["flag"], net["radii"], regs, sd_gnp, V, F, vdw,
                                  tunnel)
     contacts = [(int(net["flag"][P]), g) for (P, g), _ in sorted(mix.items(), key=lambda kv: kv[1][0])]
+    hybrid_oracle_labels.last = {"pairs": pairs, "outside": outside, "mix": mix, "flag": net["flag"], "V": V, "F": F, "win": win}
     return (lab_cnt, n_cnt), (lab_gnp, n_total), G.mixed_labels(lab_cnt, lab_gnp, n_total, contacts)
 
 
@@ -317,3 +318,38 @@ def test_hybrid_labels_oracle_matches_upstream_golden(tmp_path, path):
     assert list(lc) == list(z["ref_lab_cnt"]) and nc == z["ref_lab_counts"][0]
     assert list(lg) == list(z["ref_lab_gnp"]) and nt == z["ref_lab_counts"][1]
     assert list(mc) == list(z["ref_mixlab_cnt"]) and list(mg) == list(z["ref_mixlab_gnp"]) and nm == z["ref_mixlab_count"][0]
+
+
+@pytest.mark.parametrize("path", [GOLDEN, LABELS])
+def test_gnp_structures_oracle_matches_upstream_golden(tmp_path, path):
+    """Add_gnp_junction (GNP point lists with the interpenetrating pairs' points
+    merged within tol_gnp) and Compress_mixed_contacts (one junction per run of
+    CNT points per GNP) restated on the CPU against upstream's points_gnp,
+    structure_gnp, junctions_gnp and junctions_mixed."""
+    import sys
+
+    from oracle import gnp_oracle as G
+
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_gnp_golden as M
+
+    z = dict(np.load(path))
+    hybrid_oracle_labels(z, str(tmp_path), M.hybrid_network if path == GOLDEN else M.sparse_network)
+    r = hybrid_oracle_labels.last
+    V, F, win, vdw = r["V"], r["F"], r["win"], float(z["meta"][3])
+    contacts = []
+    for (a, b, d, N, m, pen), o in zip(r["pairs"], r["outside"]):
+        PA, PB, _ = G.pair_junction(V[a], F[a], V[b], F[b], vdw, win[0:3], win[6:9])
+        contacts.append((a, b, d, pen, PA, PB, o))
+    tol = 1.5 * float(np.max(z["in_t"]))  # Input_Reader.cpp:1161
+    pts, st, jn, _ = G.add_gnp_junctions(contacts, len(V), tol * tol)
+    assert np.array_equal(np.array(pts), z["ref_gnpjn_points"].reshape(-1, 3))
+    assert np.array_equal(np.cumsum([0] + [len(x) for x in st]), z["ref_gnpjn_structure_ptr"])
+    assert np.array_equal(np.array([x for y in st for x in y]), z["ref_gnpjn_structure_idx"])
+    assert np.array_equal(np.array([j[:4] for j in jn]), z["ref_junctions_gnp"].reshape(-1, 4))
+    assert [j[4] for j in jn] == list(z["ref_junctions_gnp_dist"])
+    pts2, st2, jm, _ = G.compress_mixed_contacts(r["mix"], r["flag"], 5, pts, st)
+    assert np.array_equal(np.array(pts2), z["ref_mixjn_points"].reshape(-1, 3))
+    assert np.array_equal(np.array([x for y in st2 for x in y]), z["ref_mixjn_structure_idx"])
+    assert np.array_equal(np.array([j[:4] for j in jm]), z["ref_junctions_mixed"].reshape(-1, 4)) and len(jm) > 10
+    assert [j[4] for j in jm] == list(z["ref_junctions_mixed_dist"])

@@ -211,9 +211,11 @@ LABELS = os.path.join(ROOT, "tests", "golden", "gnp_hybrid_labels.npz")
 @pytest.mark.parametrize("path", [GOLDEN, LABELS])
 def test_hybrid_labels_match_upstream_golden(cuda_ok, tmp_path, path):
     """The hybrid labelling chain on the device against upstream: CNT labels of
-    the hybrid grid (cicy_clusters), GNP labels from the GNP-GNP contact pass with
-    junction points (cicy_gnp_contact_pairs, cicy_gnp_labels), CNT-GNP contacts
-    (cicy_gnp_cnt_contacts) and the mixed labels (cicy_mixed_labels)."""
+    the hybrid grid (cicy_clusters), GNP labels and point structures from the
+    GNP-GNP contact pass with junction points (cicy_gnp_contact_pairs,
+    cicy_gnp_labels, cicy_gnp_junction_structures), CNT-GNP contacts
+    (cicy_gnp_cnt_contacts), the mixed junctions (cicy_mixed_junctions) and the
+    mixed labels (cicy_mixed_labels)."""
     import sys
 
     sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
@@ -241,12 +243,23 @@ def test_hybrid_labels_match_upstream_golden(cuda_ok, tmp_path, path):
         ctx.clusters(p)
         lab_cnt, n_cnt = ctx.labels()
         assert np.array_equal(lab_cnt, z["ref_lab_cnt"]) and n_cnt == z["ref_lab_counts"][0]
+        tol = 1.5 * float(np.max(z["in_t"]))  # Input_Reader.cpp:1161
         gp = gnp_contact_pairs(d, np.arange(len(z["in_l"])), win, [gs] * 3, ov_cnt, ov_gnp, p.van_der_waals_dist, p.tunneling_dist,
-                               n_labels_cnt=n_cnt)
+                               n_labels_cnt=n_cnt, tol_gnp2=tol * tol)
         assert np.array_equal(gp["labels_gnp"], z["ref_lab_gnp"]) and gp["n_total_labels"] == z["ref_lab_counts"][1]
+        # Add_gnp_junction: point lists and junctions_gnp
+        assert np.array_equal(gp["gnp_points"], z["ref_gnpjn_points"].reshape(-1, 3))
+        assert np.array_equal(gp["structure_ptr"], z["ref_gnpjn_structure_ptr"]) and np.array_equal(gp["structure_idx"], z["ref_gnpjn_structure_idx"])
+        assert np.array_equal(gp["junctions"], z["ref_junctions_gnp"].reshape(-1, 4)) and np.array_equal(gp["junction_dist"], z["ref_junctions_gnp_dist"])
         pt, g, _, _ = ctx.gnp_cnt_contacts(d, p)
         order = np.argsort(z["ref_mix_index"])
         assert np.array_equal(pt, z["ref_mix_point"][order]) and np.array_equal(g, z["ref_mix_gnp"][order])
+        # Compress_mixed_contacts: junctions_mixed and the points appended to points_gnp
+        mj = ctx.mixed_junctions(len(gp["gnp_points"]), 5)
+        ref_j = z["ref_junctions_mixed"].reshape(-1, 4)
+        assert np.array_equal(np.stack([mj["cnt_point"], mj["cnt"], mj["gnp_point"], mj["gnp"]], 1), ref_j)
+        assert np.array_equal(mj["dist"], z["ref_junctions_mixed_dist"])
+        assert np.array_equal(mj["points"], z["ref_mixjn_points"].reshape(-1, 3)[len(gp["gnp_points"]):])
         mc, mg, nm = ctx.mixed_labels(gp["labels_gnp"], gp["n_total_labels"])
         assert np.array_equal(mc, z["ref_mixlab_cnt"]) and np.array_equal(mg, z["ref_mixlab_gnp"]) and nm == z["ref_mixlab_count"][0]
         assert np.array_equal(ctx.labels()[0], mc)
