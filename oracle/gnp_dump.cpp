@@ -82,6 +82,17 @@ struct Out {
     void i32(const std::string& name, const std::vector<int>& v) { rec(name, 'i', v.data(), v.size(), 4); }
 };
 
+// A number argument, parsed whole (a stray text such as "np.float64(...)" would read as 0).
+double number(const char* s) {
+    char* end = nullptr;
+    const double v = strtod(s, &end);
+    if (end == s || *end != '\0') {
+        fprintf(stderr, "gnp_dump: not a number: %s\n", s);
+        exit(1);
+    }
+    return v;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -90,7 +101,7 @@ int main(int argc, char** argv) {
         return 1;
     }
     const std::string out_path = argv[2];
-    const double vdw = atof(argv[3]), dt = atof(argv[4]);
+    const double vdw = number(argv[3]), dt = number(argv[4]);
     if (chdir(argv[1]) != 0) { fprintf(stderr, "cannot chdir to %s\n", argv[1]); return 2; }
     open_deffo_stream((char*)"gnp_log.txt");
     Read_Network RN;
@@ -160,7 +171,7 @@ int main(int argc, char** argv) {
             disp.insert(disp.end(), {disp_tot.x, disp_tot.y, disp_tot.z});
         }
     if (argc >= 8) {
-        const double gs = atof(argv[5]), ov_cnt = atof(argv[6]), ov_gnp = atof(argv[7]);
+        const double gs = number(argv[5]), ov_cnt = number(argv[6]), ov_gnp = number(argv[7]);
         geom.gs_minx = geom.gs_miny = geom.gs_minz = gs;
         geom.gs_overlap_cnt = ov_cnt;
         geom.gs_overlap_gnp = ov_gnp;

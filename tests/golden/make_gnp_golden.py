@@ -108,6 +108,7 @@ def main():
         net = hybrid_network(d)
         z = dump(g, SIDE, d, q)
     sd_sha = arr_hash(z.pop("mix_sd_cnt_ptr"), z.pop("mix_sd_cnt_idx"))
+    z.pop("ref_seconds", None)  # timings, not results
     np.savez_compressed(os.path.join(HERE, f"gnp_{N}_s{SEED}.npz"),
                         in_l=g["l"], in_t=g["t"], in_theta=g["theta"], in_phi=g["phi"], in_center=g["center"], in_queries=q,
                         meta=np.array([N, SIDE, SEED, VDW, TUNNEL, GS_MIN, OVERLAP_CNT, OVERLAP_GNP]),
