@@ -274,7 +274,7 @@ def run_reference(args):
     value = conc / per_net
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "networks/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": per_net * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic (seeded CNT polylines, BASELINE statistics)",
+            "dtype": "f64", "data": "synthetic (seeded CNT polylines of the workload's length, radius and step statistics)",
             "config": {"workload": "single CNT network: 25,000 CNTs, 6 um cube, ~2.5M points, CG to 1e-8", "parallelism": "processes"},
             "cpu_baseline": {"value": value, "unit": "networks/s", "cores": conc, "kind": "reference",
                              "sample": f"{n_total} runs of the upstream hot path (grid+HK+electrical) on the same network files, "
@@ -654,7 +654,7 @@ def run_ours(args):
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f32/f64 mixed",
-            "data": "synthetic (seeded CNT polylines with BASELINE statistics; one independent network per GPU)",
+            "data": "synthetic (seeded CNT polylines of the workload's statistics; one independent network per GPU)",
             "config": {"workload": f"single CNT network: {args.cnts:,} CNTs, {args.side:g} um cube, {len(net.arrays()['x']):,} points "
                                    f"in the window, CG to 1e-8",
                        "l2": "256 MB buffer written between steps (L2 flush)", "parallelism": f"replicas x{world}",
