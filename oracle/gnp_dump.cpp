@@ -37,7 +37,9 @@
  * contact-point number, junction distance, and the contact points in order,
  * then the labels of the hybrid sample: Make_cnt_clusters, Make_gnp_clusters
  * (GNP-GNP contacts with junction points) and Make_mixed_clusters, in
- * Determine_clusters_and_percolation's order.
+ * Determine_clusters_and_percolation's order, the GNP point lists and
+ * junctions, and the triangulation of every GNP's points
+ * (Triangulation::Generate_3d_trangulation).
  *
  * For every candidate pair within the tunnelling cutoff it also runs the
  * junction step of Label_gnps_in_window (Find_junction_points_for_gnps with
@@ -65,6 +67,7 @@
 #include "Hoshen_Kopelman.h"
 #include "Input_Reader.h"
 #include "Read_Network.h"
+#include "Triangulation.h"
 
 namespace {
 
@@ -291,6 +294,20 @@ int main(int argc, char** argv) {
             o.f64("ref_seconds", ref_seconds);
             dump_points("mixjn_");
             dump_junctions("junctions_mixed", HK3.junctions_mixed);
+            {
+                // Triangulation::Generate_3d_trangulation of every GNP's points (Triangulation.cpp:12-56)
+                std::vector<int> tp(1, 0), ti;
+                for (size_t g = 0; g < gnps.size(); g++) {
+                    GNP gc = gnps[g];
+                    gc.triangulation.clear();
+                    Triangulation TR;
+                    if (!TR.Generate_3d_trangulation(points_gnp, structure_gnp[g], gc)) return 15;
+                    for (const EdgeL& e : gc.triangulation) ti.insert(ti.end(), {(int)e.v1, (int)e.v2});
+                    tp.push_back((int)ti.size() / 2);
+                }
+                o.i32("tri_ptr", tp);
+                o.i32("tri_edges", ti);
+            }
             {
                 std::vector<int> ep(1, 0), ei;
                 for (const auto& e : HK3.elements_cnt) {

@@ -875,3 +875,78 @@ def compress_mixed_contacts(contacts: dict, cnt_of_point, min_points: int, point
                     dmin, Pi_j, Pj_j = d, Pi1, Pj1
             emit(Pi_j, Pj_j, c, g, dmin)
     return points, structure, junctions, elements
+
+
+# ---------------------------------------------------------------------------
+# Triangulation of a GNP's points (Triangulation.cpp:12-477): Bowyer-Watson on
+# the points projected onto the GNP's mid-plane, from a supertriangle
+
+
+def _rotate(M, p, d):
+    """Point_3D::rotation (Geometry_3D.cpp:147-164): M p + d, row by row."""
+    return tuple(M[r][0] * p[0] + M[r][1] * p[1] + M[r][2] * p[2] + d[r] for r in range(3))
+
+
+def _circumcenter(P1, P2, P3):
+    """Calculate_circumcenter: C = ((Q Pn - P Qn) x R) / (2 Rn) + P3."""
+    P, Q = _sub(P1, P3), _sub(P2, P3)
+    R = _cross(P, Q)
+    Pn, Qn, Rn = _dot(P, P), _dot(Q, Q), _dot(R, R)
+    C = _div(_cross(_sub(_scale(Q, Pn), _scale(P, Qn)), R), 2 * Rn)
+    return _add(C, P3)
+
+
+def _sqdist(a, b):
+    dx, dy, dz = a[0] - b[0], a[1] - b[1], a[2] - b[2]
+    return dx * dx + dy * dy + dz * dz
+
+
+def triangulate_gnp(points, structure, l_side: float, center, rotation, face0_normal):
+    """Triangulation::Generate_3d_trangulation for one GNP: its point numbers
+    `structure` (into `points`), side l, centre, rotation matrix (3x3) and the
+    unit normal of face 0.  Returns the edges (global point numbers) in
+    upstream's order: all pairs for four points or fewer, else the edges of the
+    Bowyer-Watson triangles not touching the supertriangle, first occurrences."""
+    structure = [int(v) for v in structure]
+    if len(structure) <= 4:  # Generate_trivial_triangulation
+        return [(structure[i], structure[j]) for i in range(len(structure) - 1) for j in range(i + 1, len(structure))]
+    N = tuple(float(c) for c in face0_normal)
+    c0 = tuple(float(c) for c in center)
+    plane = []
+    for P in structure:  # Points_on_midplane
+        p = tuple(float(c) for c in points[P])
+        d = _dot(_sub(p, c0), N)
+        plane.append(_sub(p, _scale(N, d)))
+    s3 = math.sqrt(3.0)  # Generate_supertriangle
+    l = float(l_side)
+    sv = [(0.0, ((0.75 * s3) + 0.5) * l, 0.0), ((0.75 + (0.5 * s3)) * l, -l, 0.0)]
+    sv.append((-sv[1][0], sv[1][1], 0.0))
+    M = [[float(x) for x in row] for row in rotation]
+    sv = [_rotate(M, v, c0) for v in sv]
+
+    def pt(i):
+        return plane[i] if i >= 0 else sv[-1 - i]
+
+    triangles = [(-1, -2, -3)]
+    for v in range(len(plane)):  # Bowyer_watson
+        bad = []
+        for j in range(len(triangles) - 1, -1, -1):  # Find_bad_triangles
+            t = triangles[j]
+            C = _circumcenter(pt(t[0]), pt(t[1]), pt(t[2]))
+            if _sqdist(C, plane[v]) - _sqdist(C, pt(t[0])) <= ZERO:
+                bad += [(t[0], t[1]), (t[1], t[2]), (t[2], t[0])]
+                del triangles[j]
+        rep = [0] * len(bad)  # Add_new_triangles
+        for j in range(len(bad) - 1):
+            for k in range(j + 1, len(bad)):
+                if bad[j] == bad[k] or bad[j] == (bad[k][1], bad[k][0]):
+                    rep[j] += 1
+                    rep[k] += 1
+        triangles += [(e[0], e[1], v) for e, r in zip(bad, rep) if not r]
+    edges = []  # Final_triangulation_edges
+    for t in triangles:
+        for a, b in ((t[0], t[1]), (t[1], t[2]), (t[2], t[0])):
+            if a >= 0 and b >= 0:
+                edges.append((a, b))
+    keep = [not any(edges[i] == edges[j] or edges[i] == (edges[j][1], edges[j][0]) for j in range(i)) for i in range(len(edges))]
+    return [(structure[a], structure[b]) for (a, b), k in zip(edges, keep) if k]  # Update_edge_numbers

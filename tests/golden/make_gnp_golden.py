@@ -11,7 +11,8 @@ them) and, for every candidate pair, upstream's GNP-GNP distance step (GJK
 distance, EPA when the GNPs interpenetrate, the move of the second GNP) and,
 for the pairs within the tunnelling cutoff, upstream's junction points: the
 oracle of the GNP contact search.  The hybrid sample also gets upstream's
-labels, GNP point structures and GNP / mixed junction lists.  With a seeded 400-CNT network in the same
+labels, GNP point structures, GNP / mixed junction lists and the triangulation
+of every GNP's points.  With a seeded 400-CNT network in the same
 cube (regenerated by the tests from its seed and checked against the stored
 SHA-256), it also stores upstream's CNT-GNP contacts of the mixed contact pass
 (Find_adjacent_labels: point, GNP, contact-point number, junction distance,
@@ -150,7 +151,8 @@ def main_labels():
         z = read_dump(out)
     keep = ("gnp_vertices", "gnp_planes", "lab_cnt", "lab_gnp", "lab_counts", "mixlab_cnt", "mixlab_gnp", "mixlab_count", "mix_point", "mix_gnp",
             "mix_index", "gnpjn_points", "gnpjn_structure_ptr", "gnpjn_structure_idx", "junctions_gnp", "junctions_gnp_dist", "mixjn_points",
-            "mixjn_structure_ptr", "mixjn_structure_idx", "junctions_mixed", "junctions_mixed_dist")
+            "mixjn_structure_ptr", "mixjn_structure_idx", "junctions_mixed", "junctions_mixed_dist", "gnp_rotation", "gnp_center", "gnp_lt",
+            "tri_ptr", "tri_edges")
     np.savez_compressed(os.path.join(HERE, "gnp_hybrid_labels.npz"), in_l=g["l"], in_t=g["t"], in_theta=g["theta"], in_phi=g["phi"],
                         in_center=g["center"], meta=np.array([SPARSE_N, SIDE, SPARSE_SEED, VDW, TUNNEL, GS_MIN, OVERLAP_CNT, OVERLAP_GNP]),
                         cnt_meta=np.array([SPARSE_CNTS, SPARSE_CNT_SEED]), cnt_sha256=np.array(net_hash(net)),

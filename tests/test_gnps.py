@@ -353,3 +353,24 @@ def test_gnp_structures_oracle_matches_upstream_golden(tmp_path, path):
     assert np.array_equal(np.array([x for y in st2 for x in y]), z["ref_mixjn_structure_idx"])
     assert np.array_equal(np.array([j[:4] for j in jm]), z["ref_junctions_mixed"].reshape(-1, 4)) and len(jm) > 10
     assert [j[4] for j in jm] == list(z["ref_junctions_mixed_dist"])
+
+
+@pytest.mark.parametrize("path", [GOLDEN, LABELS])
+def test_triangulation_oracle_matches_upstream_golden(path):
+    """Triangulation::Generate_3d_trangulation restated on the CPU (points onto
+    the mid-plane, Bowyer-Watson from the supertriangle, first-occurrence edges;
+    all pairs for four points or fewer) against upstream's edges for every GNP's
+    final point list (after the GNP and mixed junctions)."""
+    from oracle import gnp_oracle as G
+
+    z = dict(np.load(path))
+    N = len(z["in_l"])
+    pts = z["ref_mixjn_points"].reshape(-1, 3)
+    sp, si = z["ref_mixjn_structure_ptr"], z["ref_mixjn_structure_idx"]
+    rot, cen = z["ref_gnp_rotation"].reshape(N, 3, 3), z["ref_gnp_center"].reshape(N, 3)
+    F, lt = z["ref_gnp_planes"].reshape(N, 6, 4), z["ref_gnp_lt"].reshape(N, 2)
+    tp, te = z["ref_tri_ptr"], z["ref_tri_edges"].reshape(-1, 2)
+    assert tp[-1] > 100
+    for g in range(N):
+        e = G.triangulate_gnp(pts, si[sp[g]:sp[g + 1]], lt[g, 0], cen[g], rot[g], F[g, 0, :3])
+        assert e == [tuple(x) for x in te[tp[g]:tp[g + 1]].tolist()]
