@@ -9,6 +9,9 @@
 //   pairs:    double p[2 n_items] (a, b); double vdw   -> double (status, penetrating, dist, N3, disp3)
 //   junction: double p[2 n_items]; double vdw, lo[3], hi[3]
 //                                                      -> double (distance status, junction status, outside, PA3, PB3)
+//   triangulate (own layout): int32 n_gnps, n_points; double points[3 n_points];
+//             int32 ptr[n_gnps + 1], idx[ptr[n_gnps]]; double l[n_gnps], centre[3 n_gnps],
+//             rotation[9 n_gnps], planes[24 n_gnps]  -> int32 edge_ptr[n_gnps + 1], edges[2 E]
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -18,13 +21,47 @@
 #define __device__
 #include "gnp_gjk.cuh"
 #include "gnp_junction.cuh"
+#include "gnp_triangulation.cuh"
 
 using namespace cicy::gnp;
+
+template <class T>
+bool get(FILE* f, std::vector<T>& v, size_t n) {
+    v.resize(n);
+    return fread(v.data(), sizeof(T), n, f) == n;
+}
+
+int triangulate_all(FILE* f, const char* out_path) {
+    int hdr[2];
+    if (fread(hdr, 4, 2, f) != 2) return 3;
+    const int n_gnps = hdr[0], n_points = hdr[1];
+    std::vector<double> pts, l, c, M, F;
+    std::vector<int> ptr, idx;
+    if (!get(f, pts, 3 * (size_t)n_points) || !get(f, ptr, n_gnps + 1) || !get(f, idx, ptr[n_gnps]) || !get(f, l, n_gnps) ||
+        !get(f, c, 3 * (size_t)n_gnps) || !get(f, M, 9 * (size_t)n_gnps) || !get(f, F, 24 * (size_t)n_gnps))
+        return 3;
+    static TriWork<256> w;
+    std::vector<int> eptr(1, 0), edges, buf(2 * 3 * TriWork<256>::kTris);
+    for (int g = 0; g < n_gnps; g++) {
+        const int k = triangulate<256>(pts.data(), idx.data() + ptr[g], ptr[g + 1] - ptr[g], l[g], &c[3 * (size_t)g], &M[9 * (size_t)g],
+                                       normal(&F[24 * (size_t)g], 0), w, buf.data(), (int)buf.size() / 2);
+        if (k < 0) return 5;
+        edges.insert(edges.end(), buf.begin(), buf.begin() + 2 * k);
+        eptr.push_back((int)edges.size() / 2);
+    }
+    FILE* o = fopen(out_path, "wb");
+    if (!o) return 4;
+    fwrite(eptr.data(), 4, eptr.size(), o);
+    fwrite(edges.data(), 4, edges.size(), o);
+    fclose(o);
+    return 0;
+}
 
 int main(int argc, char** argv) {
     if (argc != 4) return 1;
     FILE* f = fopen(argv[2], "rb");
     if (!f) return 2;
+    if (std::string(argv[1]) == "triangulate") return triangulate_all(f, argv[3]);
     int n_gnps = 0, n = 0;
     if (fread(&n_gnps, 4, 1, f) != 1 || fread(&n, 4, 1, f) != 1) return 3;
     std::vector<double> V(24 * (size_t)n_gnps), F(24 * (size_t)n_gnps);

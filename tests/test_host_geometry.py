@@ -1,9 +1,10 @@
 """The device geometry headers built for the host: gnp_geom.cuh (closest GNP
-point), gnp_gjk.cuh (GJK / EPA) and gnp_junction.cuh (junction points) are
-compiled by g++ without FMA contraction from the same source the CUDA kernels
-use (tests/host_geometry.cpp drives them) and compared with upstream's doubles
-in the golden fixtures: 2,400 closest points, 2,358 GNP-GNP distance steps, 565
-junction steps (the random fixture and the hand-placed cases)."""
+point), gnp_gjk.cuh (GJK / EPA), gnp_junction.cuh (junction points) and
+gnp_triangulation.cuh (per-GNP triangulation) are compiled by g++ without FMA
+contraction from the same source the CUDA kernels use (tests/host_geometry.cpp
+drives them) and compared with upstream's results in the golden fixtures: 2,400
+closest points, 2,358 GNP-GNP distance steps, 565 junction steps (the random
+fixture and the hand-placed cases), the triangulation edges of 150 GNPs."""
 import os
 import shutil
 import subprocess
@@ -70,3 +71,23 @@ def test_junction_points_host_build_match_upstream(exe, tmp_path, path, side):
     assert np.all(r[:, 0] == 0) and np.array_equal(r[:, 1] == 0, ok)
     assert np.array_equal(r[ok, 2], z["ref_junc_outside"][ok])
     assert np.array_equal(bits(r[ok, 3:9]), bits(z["ref_junc_points"].reshape(-1, 6)[ok]))
+
+
+LABELS = os.path.join(ROOT, "tests", "golden", "gnp_hybrid_labels.npz")
+
+
+@pytest.mark.parametrize("path", [GOLDEN, LABELS])
+def test_triangulation_host_build_matches_upstream(exe, tmp_path, path):
+    z = dict(np.load(path))
+    N = len(z["in_l"])
+    pts = z["ref_mixjn_points"]
+    sp, si = z["ref_mixjn_structure_ptr"], z["ref_mixjn_structure_idx"]
+    inp, out = str(tmp_path / "in.bin"), str(tmp_path / "out.bin")
+    with open(inp, "wb") as f:
+        f.write(np.array([N, len(pts) // 3], "<i4").tobytes() + pts.astype("<f8").tobytes())
+        f.write(sp.astype("<i4").tobytes() + si.astype("<i4").tobytes())
+        f.write(z["ref_gnp_lt"].reshape(N, 2)[:, 0].astype("<f8").tobytes() + z["ref_gnp_center"].astype("<f8").tobytes())
+        f.write(z["ref_gnp_rotation"].astype("<f8").tobytes() + z["ref_gnp_planes"].astype("<f8").tobytes())
+    subprocess.run([exe, "triangulate", inp, out], check=True, timeout=300)
+    r = np.fromfile(out, "<i4")
+    assert np.array_equal(r[:N + 1], z["ref_tri_ptr"]) and np.array_equal(r[N + 1:], z["ref_tri_edges"])
