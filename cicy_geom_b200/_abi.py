@@ -188,6 +188,24 @@ class GnpPointList(C.Structure):
     ]
 
 
+class GnpWindowList(C.Structure):
+    _fields_ = [
+        ("n_inside", C.c_int32),
+        ("gnps_inside", C.c_void_p),
+        ("boundary_gnp_ptr", C.c_void_p),
+        ("boundary_gnp_idx", C.c_void_p),
+        ("n_points", C.c_int64),
+        ("points", C.c_void_p),
+        ("point_gnp", C.c_void_p),
+        ("point_boundary", C.c_void_p),
+        ("boundary_pts_ptr", C.c_void_p),
+        ("boundary_pts_idx", C.c_void_p),
+        ("n_gnps", C.c_int32),
+        ("structure_ptr", C.c_void_p),
+        ("structure_idx", C.c_void_p),
+    ]
+
+
 class GenParams(C.Structure):
     _fields_ = [
         ("sample", Cuboid),
@@ -253,6 +271,9 @@ def lib() -> C.CDLL:
         "cicy_read_gnps": (C.c_int, [C.c_char_p, P(C.c_void_p)]),
         "cicy_gnp_set_view": (C.c_int, [C.c_void_p, P(Gnps)]),
         "cicy_gnp_set_free": (None, [C.c_void_p]),
+        "cicy_gnp_extract_window": (C.c_int, [C.c_void_p, P(WindowParams), P(C.c_void_p)]),
+        "cicy_gnp_window_view": (C.c_int, [C.c_void_p, P(GnpWindowList)]),
+        "cicy_gnp_window_free": (None, [C.c_void_p]),
         "cicy_gnp_sectioned_domain": (C.c_int, [C.c_int, C.c_void_p, i32p, C.c_int32, P(Cuboid), f64p, C.c_double, C.c_double,
                                                 P(C.c_void_p)]),
         "cicy_gnp_grid_view": (C.c_int, [C.c_void_p, i32p, f64p, P(C.c_void_p), P(C.c_void_p), i64p]),

@@ -96,4 +96,55 @@ void cicy_host_network_free(cicy_host_network* h) { delete h; }
 
 const char* cicy_host_last_error(void) { return g_host_error.c_str(); }
 
+
+cicy_status cicy_gnp_extract_window(const cicy_gnp_set* gnps, const cicy_window_params* w, cicy_gnp_window** out) {
+    if (!gnps || !w || !out) {
+        cicy::set_host_error("cicy_gnp_extract_window: null argument");
+        return CICY_E_INPUT;
+    }
+    *out = nullptr;
+    cicy_gnp_window* h = new cicy_gnp_window;
+    std::string err;
+    const cicy_status st = cicy::gnp_window(gnps->g, *w, h->w, err);
+    if (st != CICY_OK) {
+        cicy::set_host_error(err);
+        delete h;
+        return st;
+    }
+    auto flat = [](const std::vector<std::vector<int32_t>>& v, std::vector<int32_t>& ptr, std::vector<int32_t>& idx) {
+        ptr.assign(1, 0);
+        idx.clear();
+        for (const auto& r : v) {
+            idx.insert(idx.end(), r.begin(), r.end());
+            ptr.push_back((int32_t)idx.size());
+        }
+    };
+    cicy::GnpWindow& g = h->w;
+    flat(g.boundary_gnp, g.flat_bgnp_ptr, g.flat_bgnp_idx);
+    flat(g.boundary_pts, g.flat_bpts_ptr, g.flat_bpts_idx);
+    flat(g.structure, g.flat_st_ptr, g.flat_st_idx);
+    *out = h;
+    return CICY_OK;
+}
+
+cicy_status cicy_gnp_window_view(const cicy_gnp_window* h, cicy_gnp_window_list* v) {
+    if (!h || !v) return CICY_E_INPUT;
+    const cicy::GnpWindow& g = h->w;
+    v->n_inside = (int32_t)g.inside.size();
+    v->gnps_inside = g.inside.data();
+    v->boundary_gnp_ptr = g.flat_bgnp_ptr.data();
+    v->boundary_gnp_idx = g.flat_bgnp_idx.data();
+    v->n_points = (int64_t)g.point_gnp.size();
+    v->points = g.points.data();
+    v->point_gnp = g.point_gnp.data();
+    v->point_boundary = g.point_boundary.data();
+    v->boundary_pts_ptr = g.flat_bpts_ptr.data();
+    v->boundary_pts_idx = g.flat_bpts_idx.data();
+    v->n_gnps = (int32_t)g.structure.size();
+    v->structure_ptr = g.flat_st_ptr.data();
+    v->structure_idx = g.flat_st_idx.data();
+    return CICY_OK;
+}
+
+void cicy_gnp_window_free(cicy_gnp_window* h) { delete h; }
 }  // extern "C"

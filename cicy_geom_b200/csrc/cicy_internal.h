@@ -68,6 +68,16 @@ struct GnpStructures {
 };
 void gnp_junction_structures(const GnpPairs& pairs, int n_gnps, double tol_gnp2, const std::vector<double>& init_points,
                              const std::vector<int32_t>& init_ptr, const std::vector<int32_t>& init_idx, GnpStructures& out);
+// GNP part of the window extraction (host_network.cpp): gnps_inside, boundary_gnp,
+// and the GNP boundary points (points_gnp, structure_gnp, boundary_gnp_pts).
+struct GnpWindow {
+    std::vector<int32_t> inside;
+    std::vector<std::vector<int32_t>> boundary_gnp, boundary_pts, structure;
+    std::vector<double> points;  // 3 per point
+    std::vector<int32_t> point_gnp, point_boundary;
+    std::vector<int32_t> flat_bgnp_ptr, flat_bgnp_idx, flat_bpts_ptr, flat_bpts_idx, flat_st_ptr, flat_st_idx;
+};
+cicy_status gnp_window(const GnpSet& g, const cicy_window_params& w, GnpWindow& out, std::string& err);
 // Message returned by cicy_host_last_error() on this thread.
 void set_host_error(const std::string& msg);
 void host_network_view(const HostNetwork& h, cicy_network& v);
@@ -88,6 +98,10 @@ struct cicy_gnp_grid {
 
 struct cicy_gnp_pairs {
     cicy::GnpPairs pairs;
+};
+
+struct cicy_gnp_window {
+    cicy::GnpWindow w;
 };
 
 struct cicy_gnp_points {

@@ -319,9 +319,10 @@ struct WinCtx {
 
 }  // namespace
 
-cicy_status extract_window(const HostNetwork& in, const cicy_window_params& w, HostNetwork** out, std::string& err) {
-    WinCtx c;
-    // Geom_sample::update_observation_window_geometry(0, ...) (Input_Reader.h:110-135)
+// Window 0 and the shell geometry: Geom_sample::update_observation_window_geometry(0, ...)
+// (Input_Reader.h:110-135) and the midpoints / boundary layer / core / half steps of
+// Shells::Generate_shells (Shells.cpp:21-40); single-window runs only.
+bool window_geometry(const cicy_window_params& w, WinCtx& c, std::string& err) {
     c.win.len_x = w.win_max[0];
     c.win.len_y = w.win_max[1];
     c.win.len_z = w.win_max[2];
@@ -342,9 +343,15 @@ cicy_status extract_window(const HostNetwork& in, const cicy_window_params& w, H
     int num = (int)((w.win_max[0] - w.win_min[0] + kZero) / w.win_delt[0]);
     if (num != 0) {
         err = "extract_window: only single-window runs (win_max == win_min, cut_num = 0) are supported";
-        return CICY_E_INPUT;
+        return false;
     }
     c.n_shells = num + 2;
+    return true;
+}
+
+cicy_status extract_window(const HostNetwork& in, const cicy_window_params& w, HostNetwork** out, std::string& err) {
+    WinCtx c;
+    if (!window_geometry(w, c, err)) return CICY_E_INPUT;
     c.step_cutoff = w.step_length * 0.5;
     c.min_points = w.min_points;
     int64_t np = (int64_t)in.x.size();
@@ -696,6 +703,182 @@ void host_network_view(const HostNetwork& h, cicy_network& v) {
     v.boundary_pts_ptr = h.boundary_pts_ptr.data();
     v.boundary_pts_idx = h.boundary_pts_idx.data();
     v.window = h.window;
+}
+
+// ---------------------------------------------------------------------------
+// GNP part of the window extraction (window 0): Shells::Add_to_gnp_shells
+// (Shells.cpp:150-178) and Cutoff_Wins::Fill_gnps_inside (Cutoff_Wins.cpp:833-869)
+// with Find_gnp_boundary_points (:871-987),
+// Find_intersections_of_gnp_edges_with_window_boundaries (:1016-1091),
+// Find_two_intersections_of_gnp_edges_with_window (:1093-1135),
+// Find_intersections_of_window_edges_with_gnp_faces (:1137-1191),
+// Does_edge_intersect_gnp (:1193-1271), Find_window_vertex_inside_gnp
+// (:1273-1318) and GNP::Is_point_inside_gnp (Geometry_3D.h:352-379), in
+// upstream's operation order.  GNPs whose shells reach window 0 get one
+// boundary point per window face they cross: the average of the points
+// accumulated on that face (GNP vertices on it, GNP edges cut by it, window
+// edges through the GNP, a window corner inside it).  The GNP volume inside the
+// window (Approximate_gnp_volume_inside_sample) is not computed.
+namespace {
+
+struct V3w {
+    double x, y, z;
+};
+V3w operator+(const V3w& a, const V3w& b) { return V3w{a.x + b.x, a.y + b.y, a.z + b.z}; }
+V3w operator-(const V3w& a, const V3w& b) { return V3w{a.x - b.x, a.y - b.y, a.z - b.z}; }
+V3w operator*(const V3w& a, double s) { return V3w{a.x * s, a.y * s, a.z * s}; }
+double dotw(const V3w& a, const V3w& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+struct GnpWin {
+    const WinCtx& c;
+    // Where_is_with_boundary: 0 inside, 1 outside, 2 boundary (face in `b`)
+    int where(const V3w& p, int& b) const {
+        auto bounded = [](double v, double lo, double hi) { return (lo - v <= kZero && v - hi <= kZero); };
+        if (!bounded(p.x, c.win.min_x, c.win.max_x) || !bounded(p.y, c.win.min_y, c.win.max_y) || !bounded(p.z, c.win.min_z, c.win.max_z))
+            return 1;
+        if (std::fabs(p.x - c.win.min_x) < kZero) b = 4;
+        else if (std::fabs(p.x - c.win.max_x) < kZero) b = 2;
+        else if (std::fabs(p.y - c.win.min_y) < kZero) b = 5;
+        else if (std::fabs(p.y - c.win.max_y) < kZero) b = 3;
+        else if (std::fabs(p.z - c.win.min_z) < kZero) b = 1;
+        else if (std::fabs(p.z - c.win.max_z) < kZero) b = 0;
+        else return 0;
+        return 2;
+    }
+    void window_vertices(V3w W[8]) const {
+        const V3w m{c.win.min_x, c.win.min_y, c.win.min_z};
+        W[0] = V3w{c.win.max_x, c.win.max_y, c.win.max_z};
+        W[1] = m + V3w{0, c.win.len_y, c.win.len_z};
+        W[2] = m + V3w{0, 0, c.win.len_z};
+        W[3] = m + V3w{c.win.len_x, 0, c.win.len_z};
+        W[4] = m + V3w{c.win.len_x, c.win.len_y, 0};
+        W[5] = m + V3w{0, c.win.len_y, 0};
+        W[6] = m;
+        W[7] = m + V3w{c.win.len_x, 0, 0};
+    }
+};
+
+}  // namespace
+
+cicy_status gnp_window(const GnpSet& g, const cicy_window_params& w, GnpWindow& out, std::string& err) {
+    WinCtx c;
+    if (!window_geometry(w, c, err)) return CICY_E_INPUT;
+    out = GnpWindow{};
+    out.boundary_gnp.assign(6, std::vector<int32_t>());
+    out.boundary_pts.assign(6, std::vector<int32_t>());
+    out.structure.assign(g.n, std::vector<int32_t>());
+    const GnpWin gw{c};
+    V3w W[8];
+    gw.window_vertices(W);
+    static const int ged[12][2] = {{0, 1}, {0, 3}, {0, 4}, {2, 1}, {2, 3}, {2, 6}, {5, 1}, {5, 4}, {5, 6}, {7, 3}, {7, 4}, {7, 6}};
+    static const int wb[12][2] = {{0, 3}, {0, 2}, {2, 3}, {0, 4}, {0, 5}, {4, 5}, {3, 4}, {1, 3}, {1, 4}, {2, 5}, {1, 2}, {1, 5}};
+    static const int corner_b[8][3] = {{0, 2, 3}, {0, 3, 4}, {0, 4, 5}, {0, 2, 5}, {1, 2, 3}, {1, 3, 4}, {1, 4, 5}, {1, 2, 5}};
+    static const int adj[6][4] = {{2, 3, 4, 5}, {2, 3, 4, 5}, {0, 1, 3, 5}, {0, 1, 2, 4}, {0, 1, 3, 5}, {0, 1, 2, 4}};
+    static const int vref[6] = {0, 4, 0, 0, 1, 2};
+    for (int i = 0; i < g.n; i++) {
+        const double* Vd = &g.vertices[24 * (size_t)i];
+        const double* Fd = &g.planes[24 * (size_t)i];
+        V3w V[8], N[6];
+        for (int k = 0; k < 8; k++) V[k] = V3w{Vd[3 * k], Vd[3 * k + 1], Vd[3 * k + 2]};
+        for (int f = 0; f < 6; f++) N[f] = V3w{Fd[4 * f], Fd[4 * f + 1], Fd[4 * f + 2]};
+        // Add_to_gnp_shells: the least and greatest shell of the vertices
+        int smin = 0, smax = 0;
+        for (int k = 0; k < 8; k++) {
+            int s = std::min(c.find_shell(V[k].x, 0), c.find_shell(V[k].y, 1));
+            s = std::min(s, c.find_shell(V[k].z, 2));
+            if (k == 0 || s < smin) smin = s;
+            if (k == 0 || s > smax) smax = s;
+        }
+        if (0 < smin) {
+            out.inside.push_back(i);
+            continue;
+        }
+        if (!(0 >= smin && 0 <= smax)) continue;
+        // Find_gnp_boundary_points
+        std::vector<V3w> acc[6];
+        int loc[8], n_inside = 0;
+        for (int k = 0; k < 8; k++) {
+            int b = -1;
+            loc[k] = gw.where(V[k], b);
+            if (loc[k] == 0) n_inside++;
+            else if (loc[k] == 2) acc[b].push_back(V[k]);
+        }
+        if (n_inside == 0) continue;
+        out.inside.push_back(i);
+        if (n_inside == 8) continue;
+        for (int e = 0; e < 12; e++) {  // GNP edges cut by the window's faces
+            const int v1 = ged[e][0], v2 = ged[e][1];
+            if ((loc[v1] == 0 && loc[v2] == 1) || (loc[v2] == 0 && loc[v1] == 1)) {
+                const V3w& pin = loc[v1] == 0 ? V[v1] : V[v2];
+                const V3w& po = loc[v1] == 0 ? V[v2] : V[v1];
+                P3 a{pin.x, pin.y, pin.z, i}, b{po.x, po.y, po.z, i};
+                c.substitute(a, b);
+                int bb = -1;
+                if (gw.where(V3w{b.x, b.y, b.z}, bb) != 2) {
+                    err = "Error in Find_intersections_of_gnp_edges_with_window_boundaries: point is not at a boundary (GNP " + std::to_string(i) + ")";
+                    return CICY_E_INPUT;
+                }
+                acc[bb].push_back(V3w{b.x, b.y, b.z});
+            } else if (loc[v1] == 1 && loc[v2] == 1) {
+                const V3w A = V[v1], B = V[v2];
+                auto cut = [&](double a1, double a2, double wc) {
+                    if ((a1 - wc < kZero && a2 - wc > kZero) || (a2 - wc < kZero && a1 - wc > kZero)) {
+                        const double lambda = (wc - a1) / (a2 - a1);
+                        const V3w P = A + (B - A) * lambda;
+                        int pb = -1;
+                        if (gw.where(P, pb) == 2) acc[pb].push_back(P);
+                    }
+                };
+                cut(A.x, B.x, c.win.min_x);
+                cut(A.x, B.x, c.win.max_x);
+                cut(A.y, B.y, c.win.min_y);
+                cut(A.y, B.y, c.win.max_y);
+                cut(A.z, B.z, c.win.min_z);
+                cut(A.z, B.z, c.win.max_z);
+            }
+        }
+        for (int e = 0; e < 12; e++) {  // window edges through the GNP's faces
+            const V3w& P1 = W[ged[e][0]];
+            const V3w V1V2 = W[ged[e][1]] - P1;
+            for (int f = 0; f < 6; f++) {
+                const int l1 = dotw(N[f], P1 - V[vref[f]]) > kZero;
+                const int l2 = dotw(N[f], W[ged[e][1]] - V[vref[f]]) > kZero;
+                if (l1 == l2) continue;
+                const double lambda = (-dotw(N[f], P1) - Fd[4 * f + 3]) / dotw(N[f], V1V2);
+                const V3w P = P1 + V1V2 * lambda;
+                bool ignore = false;
+                for (int j = 0; j < 4 && !ignore; j++) ignore = dotw(N[adj[f][j]], P - V[vref[adj[f][j]]]) > kZero;
+                if (!ignore) {
+                    acc[wb[e][0]].push_back(P);
+                    acc[wb[e][1]].push_back(P);
+                    break;
+                }
+            }
+        }
+        for (int k = 0; k < 8; k++) {  // a window corner inside the GNP
+            const V3w& P = W[k];
+            const V3w V4P = P - V[4];
+            if (dotw(N[0], P - V[0]) < kZero && dotw(N[1], V4P) < kZero && dotw(N[2], V4P) < kZero && dotw(N[4], P - V[1]) < kZero &&
+                dotw(N[3], V4P) < kZero && dotw(N[5], P - V[2]) < kZero) {
+                for (int j = 0; j < 3; j++) acc[corner_b[k][j]].push_back(P);
+                break;
+            }
+        }
+        for (int b = 0; b < 6; b++) {
+            if (acc[b].empty()) continue;
+            V3w avg{0.0, 0.0, 0.0};
+            for (const V3w& q : acc[b]) avg = avg + q;
+            const double n = (double)acc[b].size();
+            const int32_t P = (int32_t)(out.points.size() / 3);
+            out.boundary_gnp[b].push_back(i);
+            out.boundary_pts[b].push_back(P);
+            out.structure[i].push_back(P);
+            out.points.insert(out.points.end(), {avg.x / n, avg.y / n, avg.z / n});
+            out.point_gnp.push_back(i);
+            out.point_boundary.push_back(b);
+        }
+    }
+    return CICY_OK;
 }
 
 }  // namespace cicy

@@ -540,3 +540,44 @@ def gnp_contact_pairs(directory: str, inside, window, gs_min, overlap_cnt: float
         if grid:
             lib().cicy_gnp_grid_free(grid)
         lib().cicy_gnp_set_free(h)
+
+
+def gnp_extract_window(directory: str, side: float, window_side=None) -> dict:
+    """GNP part of the window extraction for window 0 (cicy_gnp_extract_window)
+    for the GNPs of `directory`/gnp_data.dat in a cube of `side` um, the window
+    being the sample or a centred cube of `window_side` um: gnps_inside, the
+    GNPs and boundary points of each face (CSR, 7 offsets), the boundary points
+    [m, 3] with their GNP and face, and each GNP's boundary points (CSR)."""
+    h = C.c_void_p()
+    check(lib().cicy_read_gnps(directory.encode(), C.byref(h)), "cicy_read_gnps")
+    win = C.c_void_p()
+    try:
+        w = _abi.WindowParams()
+        w.sample = _abi.Cuboid(0.0, 0.0, 0.0, side, side, side, side, side, side)
+        ws = float(side if window_side is None else window_side)
+        for a in range(3):
+            w.win_max[a] = w.win_min[a] = ws
+            w.win_delt[a] = 0.25
+        check(lib().cicy_gnp_extract_window(h, C.byref(w), C.byref(win)), "cicy_gnp_extract_window")
+        v = _abi.GnpWindowList()
+        check(lib().cicy_gnp_window_view(win, C.byref(v)), "cicy_gnp_window_view")
+
+        def arr(ptr, ct, count, dt):
+            if count == 0:
+                return np.zeros(0, dt)
+            return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ct)), shape=(count,)).copy()
+
+        n = int(v.n_points)
+        bg_ptr = arr(v.boundary_gnp_ptr, C.c_int32, 7, np.int32)
+        bp_ptr = arr(v.boundary_pts_ptr, C.c_int32, 7, np.int32)
+        st_ptr = arr(v.structure_ptr, C.c_int32, v.n_gnps + 1, np.int32)
+        return {"gnps_inside": arr(v.gnps_inside, C.c_int32, v.n_inside, np.int32),
+                "boundary_gnp_ptr": bg_ptr, "boundary_gnp_idx": arr(v.boundary_gnp_idx, C.c_int32, int(bg_ptr[-1]), np.int32),
+                "boundary_pts_ptr": bp_ptr, "boundary_pts_idx": arr(v.boundary_pts_idx, C.c_int32, int(bp_ptr[-1]), np.int32),
+                "points": arr(v.points, C.c_double, 3 * n, np.float64).reshape(n, 3),
+                "point_gnp": arr(v.point_gnp, C.c_int32, n, np.int32), "point_boundary": arr(v.point_boundary, C.c_int32, n, np.int32),
+                "structure_ptr": st_ptr, "structure_idx": arr(v.structure_idx, C.c_int32, int(st_ptr[-1]), np.int32)}
+    finally:
+        if win:
+            lib().cicy_gnp_window_free(win)
+        lib().cicy_gnp_set_free(h)

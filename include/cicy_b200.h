@@ -397,6 +397,37 @@ cicy_status cicy_read_gnps(const char* directory, cicy_gnp_set** out);
 cicy_status cicy_gnp_set_view(const cicy_gnp_set* set, cicy_gnps* view);
 void cicy_gnp_set_free(cicy_gnp_set* set);
 
+/* GNP part of the window extraction (window 0, single-window runs), on the
+ * host: Shells::Add_to_gnp_shells and Cutoff_Wins::Fill_gnps_inside with
+ * Find_gnp_boundary_points (Shells.cpp:150-178, Cutoff_Wins.cpp:833-1318).
+ * GNPs deeper than the boundary shell are inside; a GNP in it with a vertex
+ * inside the window is inside too and gets, per window face it crosses, one
+ * boundary point: the average of its vertices on the face, its edges' cuts
+ * through the face, the window edges through it and a window corner inside it
+ * (upstream's points_gnp / structure_gnp / boundary_gnp / boundary_gnp_pts
+ * before the contact search; n_points is gnp_pts_bdds).  The GNP volume inside
+ * the window is not computed. */
+typedef struct cicy_gnp_window cicy_gnp_window;
+typedef struct {
+    int32_t n_inside;
+    const int32_t* gnps_inside;        /* [n_inside] */
+    const int32_t* boundary_gnp_ptr;   /* [7]: GNPs at face f are boundary_gnp_idx[ptr[f]..ptr[f+1]) */
+    const int32_t* boundary_gnp_idx;
+    int64_t n_points;
+    const double* points;              /* [3 n_points] boundary points */
+    const int32_t* point_gnp;          /* [n_points] */
+    const int32_t* point_boundary;     /* [n_points] face of the point */
+    const int32_t* boundary_pts_ptr;   /* [7] */
+    const int32_t* boundary_pts_idx;
+    int32_t n_gnps;
+    const int32_t* structure_ptr;      /* [n_gnps + 1] each GNP's boundary points */
+    const int32_t* structure_idx;
+} cicy_gnp_window_list;
+cicy_status cicy_gnp_extract_window(const cicy_gnp_set* gnps, const cicy_window_params* w, cicy_gnp_window** out);
+/* Borrowed view; valid until cicy_gnp_window_free. */
+cicy_status cicy_gnp_window_view(const cicy_gnp_window* h, cicy_gnp_window_list* view);
+void cicy_gnp_window_free(cicy_gnp_window* h);
+
 /* GNP part of the contact grid on the device: Contact_grid::Fill_sectioned_domain_gnps
  * (Contact_grid.cpp:297-512) on the region grid of Generate_contact_grid +
  * Adjust_regions_if_needed (:18-102).  The GNPs of `inside` (indices into the

@@ -47,6 +47,11 @@
  * the point on the second GNP moved back) and dumps its success flag, both
  * points and whether each lies outside the sample.
  *
+ * It also runs the GNP part of the window extraction for window 0
+ * (Shells::Generate_shells, Cutoff_Wins::Fill_gnps_inside) with the sample as
+ * the window, or a centred window of side argv[8] when given, and dumps
+ * gnps_inside, boundary_gnp, boundary_gnp_pts and the boundary points.
+ *
  * Output records: u32 name length, name, u8 type ('i' int32, 'd' float64),
  * u64 count, payload (the layout oracle/dumpio.py reads).
  */
@@ -66,7 +71,9 @@
 #include "Hns.h"
 #include "Hoshen_Kopelman.h"
 #include "Input_Reader.h"
+#include "Cutoff_Wins.h"
 #include "Read_Network.h"
+#include "Shells.h"
 #include "Triangulation.h"
 
 namespace {
@@ -85,6 +92,18 @@ struct Out {
     void i32(const std::string& name, const std::vector<int>& v) { rec(name, 'i', v.data(), v.size(), 4); }
 };
 
+// Lists of indices as CSR records <name>_ptr, <name>_idx.
+template <class List>
+void dump_csr(Out& o, const std::string& name, const std::vector<List>& lists) {
+    std::vector<int> p(1, 0), x;
+    for (size_t r = 0; r < lists.size(); r++) {
+        for (size_t k = 0; k < lists[r].size(); k++) x.push_back((int)lists[r][k]);
+        p.push_back((int)x.size());
+    }
+    o.i32(name + "_ptr", p);
+    o.i32(name + "_idx", x);
+}
+
 // A number argument, parsed whole (a stray text such as "np.float64(...)" would read as 0).
 double number(const char* s) {
     char* end = nullptr;
@@ -100,7 +119,7 @@ double number(const char* s) {
 
 int main(int argc, char** argv) {
     if (argc < 5) {
-        fprintf(stderr, "usage: gnp_dump <dir> <out.bin> <van_der_Waals_dist> <tunneling_dist>\n");
+        fprintf(stderr, "usage: gnp_dump <dir> <out.bin> <van_der_Waals_dist> <tunneling_dist> [<gs_min> <overlap_cnt> <overlap_gnp> [<window side>]]\n");
         return 1;
     }
     const std::string out_path = argv[2];
@@ -116,6 +135,36 @@ int main(int argc, char** argv) {
     Out o;
     o.f = fopen(out_path.c_str(), "wb");
     if (!o.f) return 5;
+    {
+        // GNP part of the window extraction for window 0 (Shells::Generate_shells,
+        // Cutoff_Wins::Fill_gnps_inside); the window's side is argv[8] when given, else the sample's
+        Geom_sample gw = geom;
+        const double side = argc >= 9 ? number(argv[8]) : -1.0;
+        gw.win_max_x = gw.win_min_x = side > 0 ? side : geom.sample.len_x;
+        gw.win_max_y = gw.win_min_y = side > 0 ? side : geom.sample.wid_y;
+        gw.win_max_z = gw.win_min_z = side > 0 ? side : geom.sample.hei_z;
+        gw.win_delt_x = gw.win_delt_y = gw.win_delt_z = 0.25;
+        gw.cut_num = 0;
+        std::vector<std::vector<int> > shells_cnt;
+        std::vector<Shell> shells_gnp(gnps.size());
+        std::vector<Point_3D> no_points;
+        Shells SH;
+        if (!SH.Generate_shells("GNP_cuboids", gw, no_points, gnps, shells_cnt, shells_gnp)) return 16;
+        const cuboid win = gw.update_observation_window_geometry(0, "GNP_cuboids");
+        std::vector<GNP> gcopy = gnps;
+        std::vector<std::vector<long int> > st(gnps.size());
+        std::vector<Point_3D> pg;
+        Cutoff_Wins CW;
+        if (!CW.Fill_gnps_inside(0, win, shells_gnp, gcopy, st, pg)) return 17;
+        o.i32("win_inside", CW.gnps_inside);
+        dump_csr(o, "win_bgnp", CW.boundary_gnp);
+        dump_csr(o, "win_bpts", CW.boundary_gnp_pts);
+        dump_csr(o, "win_structure", st);
+        std::vector<double> xyz;
+        for (const Point_3D& q : pg) xyz.insert(xyz.end(), {q.x, q.y, q.z});
+        o.f64("win_points", xyz);
+        o.f64("win_box", {win.poi_min.x, win.poi_min.y, win.poi_min.z, win.len_x, win.wid_y, win.hei_z, win.max_x, win.max_y, win.max_z});
+    }
     std::vector<double> lt, center, rot, vert, planes;
     for (const GNP& g : gnps) {
         lt.push_back(g.l);

@@ -21,7 +21,9 @@ itself is self-contained apart from the seeded CNT network.
 
 Also writes tests/golden/gnp_hybrid_labels.npz: upstream's CNT, GNP and mixed
 labels of a sparser hybrid sample (30 GNPs, 250 CNTs), whose clusters stay
-apart.
+apart, and tests/golden/gnp_windows.npz: upstream's GNP window extraction
+(Fill_gnps_inside) for two centred windows smaller than the sample (the
+120-GNP fixture itself carries it for the whole sample as the window).
 
     python tests/golden/make_gnp_golden.py
 """
@@ -161,6 +163,34 @@ def main_labels():
           f"{int(z['mixlab_count'][0])} mixed clusters, {len(z['mix_point'])} CNT-GNP contacts")
 
 
+# Window extraction cases: (GNPs, sample side, seed, window side)
+WINDOW_CASES = [(120, 2.0, SEED, 1.5), (300, 3.0, 4_300_001, 2.2)]
+
+
+def main_windows():
+    """tests/golden/gnp_windows.npz: upstream's GNP window extraction
+    (Fill_gnps_inside) for centred windows smaller than the sample."""
+    out = {}
+    for k, (n, side, seed, ws) in enumerate(WINDOW_CASES):
+        g = generate_gnps(n, side, seed)
+        with tempfile.TemporaryDirectory() as d:
+            write_gnp_file(d, g)
+            with open(os.path.join(d, "sample_geom.csv"), "w") as f:
+                f.write(f"0,0,0\n{side!r},{side!r},{side!r}\n")
+            subprocess.run([REF, d, os.path.join(d, "g.bin"), repr(VDW), repr(TUNNEL), repr(GS_MIN), repr(OVERLAP_CNT), repr(float(OVERLAP_GNP)),
+                            repr(float(ws))], check=True, capture_output=True, timeout=600)
+            z = read_dump(os.path.join(d, "g.bin"))
+        for key in ("l", "t", "theta", "phi", "center"):
+            out[f"c{k}_in_{key}"] = g[key]
+        out[f"c{k}_meta"] = np.array([n, side, seed, ws])
+        for key in ("win_inside", "win_bgnp_ptr", "win_bgnp_idx", "win_bpts_ptr", "win_bpts_idx", "win_structure_ptr", "win_structure_idx",
+                    "win_points", "win_box"):
+            out[f"c{k}_ref_{key}"] = z[key]
+        print(f"window case {k}: {n} GNPs in {side} um, window {ws} um: {len(z['win_inside'])} inside, {len(z['win_points']) // 3} boundary points")
+    np.savez_compressed(os.path.join(HERE, "gnp_windows.npz"), **out)
+
+
 if __name__ == "__main__":
     main()
     main_labels()
+    main_windows()

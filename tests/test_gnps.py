@@ -374,3 +374,38 @@ def test_triangulation_oracle_matches_upstream_golden(path):
     for g in range(N):
         e = G.triangulate_gnp(pts, si[sp[g]:sp[g + 1]], lt[g, 0], cen[g], rot[g], F[g, 0, :3])
         assert e == [tuple(x) for x in te[tp[g]:tp[g + 1]].tolist()]
+
+
+WINDOWS = os.path.join(ROOT, "tests", "golden", "gnp_windows.npz")
+
+
+def _window_case(tmp_path, k):
+    """(GNP inputs written to tmp_path, sample side, window side, upstream arrays) of a window case;
+    k = -1: the 120-GNP fixture with the sample as the window."""
+    if k < 0:
+        z = golden()
+        g = {"l": z["in_l"], "t": z["in_t"], "theta": z["in_theta"], "phi": z["in_phi"], "center": z["in_center"]}
+        ref = {key[len("ref_"):]: v for key, v in z.items() if key.startswith("ref_win_")}
+        side, ws = float(z["meta"][1]), None
+    else:
+        z = dict(np.load(WINDOWS))
+        g = {key: z[f"c{k}_in_{key}"] for key in ("l", "t", "theta", "phi", "center")}
+        ref = {key[len(f"c{k}_ref_"):]: v for key, v in z.items() if key.startswith(f"c{k}_ref_")}
+        side, ws = float(z[f"c{k}_meta"][1]), float(z[f"c{k}_meta"][3])
+    write_gnp_file(str(tmp_path), g)
+    return side, ws, ref
+
+
+@pytest.mark.parametrize("k", [-1, 0, 1])
+def test_gnp_window_extraction_matches_upstream_golden(tmp_path, k):
+    """cicy_gnp_extract_window (host) against upstream's Fill_gnps_inside:
+    gnps_inside, boundary_gnp, boundary_gnp_pts, structure_gnp and the boundary
+    points bit for bit, for the whole sample and two centred smaller windows."""
+    from cicy_geom_b200.network import gnp_extract_window
+
+    side, ws, ref = _window_case(tmp_path, k)
+    w = gnp_extract_window(str(tmp_path), side, ws)
+    assert np.array_equal(w["gnps_inside"], ref["win_inside"])
+    for mine, theirs in (("boundary_gnp", "win_bgnp"), ("boundary_pts", "win_bpts"), ("structure", "win_structure")):
+        assert np.array_equal(w[mine + "_ptr"], ref[theirs + "_ptr"]) and np.array_equal(w[mine + "_idx"], ref[theirs + "_idx"])
+    assert np.array_equal(w["points"].ravel().view(np.int64), ref["win_points"].view(np.int64)) and len(w["points"]) > 100
