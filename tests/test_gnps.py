@@ -409,3 +409,50 @@ def test_gnp_window_extraction_matches_upstream_golden(tmp_path, k):
     for mine, theirs in (("boundary_gnp", "win_bgnp"), ("boundary_pts", "win_bpts"), ("structure", "win_structure")):
         assert np.array_equal(w[mine + "_ptr"], ref[theirs + "_ptr"]) and np.array_equal(w[mine + "_idx"], ref[theirs + "_idx"])
     assert np.array_equal(w["points"].ravel().view(np.int64), ref["win_points"].view(np.int64)) and len(w["points"]) > 100
+
+
+def test_gnp_entry_points_reject_bad_input(tmp_path):
+    """Argument checks of the GNP entry points that run before any device work:
+    null handles, out-of-range GNP indices, malformed initial structures and
+    multi-window parameters fail with CICY_E_INPUT and a message."""
+    import ctypes as C
+
+    from cicy_geom_b200.network import gnp_extract_window
+
+    L = _abi.lib()
+    d = str(tmp_path)
+    write_gnp_file(d, generate_gnps(6, 2.0, 11))
+    h = C.c_void_p()
+    assert L.cicy_read_gnps(d.encode(), C.byref(h)) == 0
+    try:
+        out = C.c_void_p()
+        assert L.cicy_gnp_labels(0, None, 6, 0, None, None) == 1
+        assert L.cicy_gnp_junction_structures(0, None, 6, 0.1, 0, None, None, None, C.byref(out)) == 1
+        assert L.cicy_gnp_contact_pairs(0, h, None, 0.00034, 0.0018, None, 0, C.byref(out)) == 1
+        assert L.cicy_gnp_extract_window(None, None, C.byref(out)) == 1
+        a = np.array([0, 7], np.int32)  # GNP 7 of 6
+        b = np.array([1, 2], np.int32)
+        r = np.zeros(8)
+        i = np.zeros(2, np.int32)
+        assert L.cicy_gnp_pair_distance(0, h, 2, a.ctypes.data_as(_abi.i32p), b.ctypes.data_as(_abi.i32p), 0.00034,
+                                        r.ctypes.data_as(_abi.f64p), r.ctypes.data_as(_abi.f64p), r.ctypes.data_as(_abi.f64p),
+                                        i.ctypes.data_as(_abi.i32p)) == 1
+        assert b"out of range" in L.cicy_host_last_error()
+        q = np.zeros(3)
+        g = np.array([9], np.int32)
+        assert L.cicy_gnp_point_distance(0, h, 1, q.ctypes.data_as(_abi.f64p), g.ctypes.data_as(_abi.i32p), r.ctypes.data_as(_abi.f64p),
+                                         r.ctypes.data_as(_abi.f64p), i.ctypes.data_as(_abi.i32p)) == 1
+    finally:
+        L.cicy_gnp_set_free(h)
+    with pytest.raises(_abi.CicyError, match="single-window"):
+        w = _abi.WindowParams()
+        w.sample = _abi.Cuboid(0.0, 0.0, 0.0, 2.0, 2.0, 2.0, 2.0, 2.0, 2.0)
+        for k in range(3):
+            w.win_max[k], w.win_min[k], w.win_delt[k] = 2.0, 1.0, 0.25
+        h2, out2 = C.c_void_p(), C.c_void_p()
+        assert L.cicy_read_gnps(d.encode(), C.byref(h2)) == 0
+        try:
+            _abi.check(L.cicy_gnp_extract_window(h2, C.byref(w), C.byref(out2)), "cicy_gnp_extract_window")
+        finally:
+            L.cicy_gnp_set_free(h2)
+    assert len(gnp_extract_window(d, 2.0)["gnps_inside"]) > 0
