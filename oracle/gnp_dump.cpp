@@ -47,6 +47,12 @@
  * the point on the second GNP moved back) and dumps its success flag, both
  * points and whether each lies outside the sample.
  *
+ * With "flow <step length>" after the window side (-1: the sample), it also
+ * runs upstream's stages for GNP_CNT_mix on window 0 (Shells,
+ * Extract_observation_window, Generate_contact_grid,
+ * Determine_clusters_and_percolation) and dumps the clusters, families and
+ * junction groups (flow_* records).
+ *
  * It also runs the GNP part of the window extraction for window 0
  * (Shells::Generate_shells, Cutoff_Wins::Fill_gnps_inside) with the sample as
  * the window, or a centred window of side argv[8] when given, and dumps
@@ -402,6 +408,72 @@ int main(int argc, char** argv) {
         o.f64("query_dist", qd);
         o.f64("query_point", qp);
         o.i32("query_flag", qflag);
+    }
+    if (argc >= 11 && std::string(argv[9]) == "flow") {
+        // Upstream's stages for GNP_CNT_mix on window 0 = the sample, in App_Network_3D's order
+        // (App_Network_3D.cpp:120-180): Shells, Cutoff_Wins::Extract_observation_window,
+        // Contact_grid::Generate_contact_grid, Hoshen_Kopelman::Determine_clusters_and_percolation
+        // (CNT points inside a GNP ignored), with min_points 5 and tol_gnp = 1.5 t_max.
+        Geom_sample gw = geom;
+        gw.win_max_x = gw.win_min_x = geom.sample.len_x;
+        gw.win_max_y = gw.win_min_y = geom.sample.wid_y;
+        gw.win_max_z = gw.win_min_z = geom.sample.hei_z;
+        gw.win_delt_x = gw.win_delt_y = gw.win_delt_z = 0.25;
+        gw.cut_num = 0;
+        gw.gs_minx = gw.gs_miny = gw.gs_minz = number(argv[5]);
+        gw.gs_overlap_cnt = number(argv[6]);
+        gw.gs_overlap_gnp = number(argv[7]);
+        std::vector<Point_3D> pts;
+        std::vector<double> radii;
+        std::vector<std::vector<long int> > structure;
+        if (!RN.Read_cnt_data_from_dat(pts, radii, structure)) return 20;
+        std::vector<std::vector<int> > shells_cnt;
+        std::vector<Shell> shells_gnp(gnps.size());
+        Shells SH;
+        if (!SH.Generate_shells("GNP_CNT_mix", gw, pts, gnps, shells_cnt, shells_gnp)) return 21;
+        const cuboid win = gw.update_observation_window_geometry(0, "GNP_CNT_mix");
+        Nanotube_Geo cg;
+        cg.min_points = 5;
+        cg.step_length = number(argv[10]);
+        std::vector<GNP> gf = gnps;
+        std::vector<std::vector<long int> > sg(gnps.size());
+        std::vector<Point_3D> pg;
+        Cutoff_Wins CW;
+        if (!CW.Extract_observation_window(0, "GNP_CNT_mix", gw, win, cg, gf, structure, radii, pts, shells_cnt, shells_gnp, sg, pg)) return 22;
+        Contact_grid CGf;
+        if (!CGf.Generate_contact_grid(0, "GNP_CNT_mix", gw, win, CW.cnts_inside, pts, structure, CW.gnps_inside, gf)) return 23;
+        Simu_para sp;
+        sp.particle_type = "GNP_CNT_mix";
+        sp.allow_simplex3 = false;
+        Visualization_flags vf;
+        vf.generated_nanoparticles = vf.clusters = vf.percolated_clusters = vf.backbone = vf.triangulations = 0;
+        Cutoff_dist cf = cut;
+        cf.min_points = 5;
+        double t_max = 0.0;
+        for (const GNP& g : gf) t_max = std::max(t_max, g.t);
+        cf.tol_gnp = 1.5 * t_max;
+        cf.tol_gnp2 = cf.tol_gnp * cf.tol_gnp;
+        Hoshen_Kopelman HF;
+        HF.ignore_eror_cnt_inside_gnp = 1;
+        if (!HF.Determine_clusters_and_percolation(0, geom.sample, sp, cf, vf, CW.cnts_inside, CGf.sectioned_domain_cnts, structure, pts, radii,
+                                                   CW.boundary_cnt, CW.gnps_inside, CGf.sectioned_domain_gnps, gf, CW.boundary_gnp, sg, pg))
+            return 24;
+        o.i32("flow_cnts_inside", CW.cnts_inside);
+        o.i32("flow_gnps_inside", CW.gnps_inside);
+        dump_csr(o, "flow_boundary_cnt", CW.boundary_cnt);
+        dump_csr(o, "flow_boundary_gnp", CW.boundary_gnp);
+        dump_csr(o, "flow_clusters_cnt", HF.clusters_cnt);
+        dump_csr(o, "flow_clusters_gnp", HF.clusters_gnp);
+        dump_csr(o, "flow_isolated_cnt", HF.isolated_cnt);
+        dump_csr(o, "flow_isolated_gnp", HF.isolated_gnp);
+        o.i32("flow_family", HF.family);
+        dump_csr(o, "flow_cluster_cnt_junctions", HF.cluster_cnt_junctions);
+        dump_csr(o, "flow_cluster_gnp_junctions", HF.cluster_gnp_junctions);
+        dump_csr(o, "flow_cluster_mix_junctions", HF.cluster_mix_junctions);
+        dump_csr(o, "flow_structure_gnp", sg);
+        std::vector<double> xyz;
+        for (const Point_3D& q : pg) xyz.insert(xyz.end(), {q.x, q.y, q.z});
+        o.f64("flow_points_gnp", xyz);
     }
     o.i32("junc_pair", jn_pair);
     o.i32("junc_ok", jn_ok);

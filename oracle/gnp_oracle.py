@@ -950,3 +950,70 @@ def triangulate_gnp(points, structure, l_side: float, center, rotation, face0_no
                 edges.append((a, b))
     keep = [not any(edges[i] == edges[j] or edges[i] == (edges[j][1], edges[j][0]) for j in range(i)) for i in range(len(edges))]
     return [(structure[a], structure[b]) for (a, b), k in zip(edges, keep) if k]  # Update_edge_numbers
+
+
+# ---------------------------------------------------------------------------
+# Clusters and percolation of a mixed network (Hoshen_Kopelman.cpp:2331-2738)
+
+FAMILY = {1: 0, 11: 1, 21: 2, 12: 3, 22: 4, 32: 5, 33: 6}  # Family_map
+
+
+def mixed_percolation(n_clusters, cnts_inside, gnps_inside, labels_cnt, labels_gnp, boundary_cnt, boundary_gnp, junctions_cnt, junctions_gnp,
+                      junctions_mixed):
+    """Make_particle_clusters (CNTs, then GNPs), Find_percolated_clusters (a
+    cluster percolates along x, y, z when a particle of face 2/3/0 and one of
+    face 4/5/1 carry its label; direction code 10 d + 1), the families, and
+    Group_junctions (CNT-CNT and GNP-GNP junctions by the label of their
+    particles, mixed ones by the CNT's).  Junctions: lists of (N1, N2) particle
+    pairs.  Returns a dict of the public members upstream fills."""
+    def make(inside, labels):
+        clusters, iso = [[] for _ in range(n_clusters)], []
+        for p in inside:
+            (clusters[labels[p]] if labels[p] != -1 else iso).append(int(p))
+        return clusters, iso
+
+    cc, iso_c = make(cnts_inside, labels_cnt) if len(labels_cnt) else ([], None)
+    cg, iso_g = make(gnps_inside, labels_gnp) if len(labels_gnp) else ([], None)
+    dirs = [set() for _ in range(n_clusters)]
+    for d, (b1, b2) in enumerate(((2, 4), (3, 5), (0, 1))):
+        first = set()
+        for parts, labels in ((boundary_cnt, labels_cnt), (boundary_gnp, labels_gnp)):
+            if len(parts):
+                first |= {labels[p] for p in parts[b1] if labels[p] != -1}
+        if first:
+            for parts, labels in ((boundary_cnt, labels_cnt), (boundary_gnp, labels_gnp)):
+                if len(parts):
+                    for p in parts[b2]:
+                        if labels[p] in first:
+                            dirs[labels[p]].add(10 * d + 1)
+    out = {"clusters_cnt": [], "clusters_gnp": [], "isolated_cnt": [iso_c] if iso_c is not None else [],
+           "isolated_gnp": [iso_g] if iso_g is not None else [], "family": []}
+    perc = {}
+    for i in range(n_clusters):
+        if not dirs[i]:
+            if cc:
+                out["isolated_cnt"].append(cc[i])
+            if cg:
+                out["isolated_gnp"].append(cg[i])
+        else:
+            perc[i] = len(out["family"])
+            out["family"].append(FAMILY[sum(dirs[i])])
+            if cc:
+                out["clusters_cnt"].append(cc[i])
+            if cg:
+                out["clusters_gnp"].append(cg[i])
+
+    def group(junctions, l1, l2, n):
+        groups = [[] for _ in range(n)]
+        for k, (a, b) in enumerate(junctions):
+            if l1[a] != l2[b]:
+                raise RuntimeError("Group_junctions: the particles of a junction have different labels")
+            if l1[a] in perc:
+                groups[perc[l1[a]]].append(k)
+        return groups
+
+    if out["clusters_cnt"] or out["clusters_gnp"]:
+        out["cluster_cnt_junctions"] = group(junctions_cnt, labels_cnt, labels_cnt, len(out["clusters_cnt"])) if junctions_cnt else []
+        out["cluster_gnp_junctions"] = group(junctions_gnp, labels_gnp, labels_gnp, len(out["clusters_gnp"])) if junctions_gnp else []
+        out["cluster_mix_junctions"] = group(junctions_mixed, labels_cnt, labels_gnp, len(out["clusters_cnt"])) if junctions_mixed else []
+    return out

@@ -23,7 +23,9 @@ Also writes tests/golden/gnp_hybrid_labels.npz: upstream's CNT, GNP and mixed
 labels of a sparser hybrid sample (30 GNPs, 250 CNTs), whose clusters stay
 apart, and tests/golden/gnp_windows.npz: upstream's GNP window extraction
 (Fill_gnps_inside) for two centred windows smaller than the sample (the
-120-GNP fixture itself carries it for the whole sample as the window).
+120-GNP fixture itself carries it for the whole sample as the window), and
+tests/golden/gnp_hybrid_flow.npz: upstream's own stage sequence for GNP_CNT_mix
+on both hybrid samples up to the percolated clusters.
 
     python tests/golden/make_gnp_golden.py
 """
@@ -190,7 +192,30 @@ def main_windows():
     np.savez_compressed(os.path.join(HERE, "gnp_windows.npz"), **out)
 
 
+def main_flow():
+    """tests/golden/gnp_hybrid_flow.npz: upstream's own stages for GNP_CNT_mix
+    (window extraction, contact grid, Determine_clusters_and_percolation) on the
+    two hybrid samples: cnts/gnps inside, boundary lists, percolated clusters,
+    isolated particles, families and junction groups (flow_* records)."""
+    out = {}
+    samples = (("m", hybrid_network, generate_gnps(N, SIDE, SEED)),
+               ("s", sparse_network, generate_gnps(SPARSE_N, SIDE, SPARSE_SEED, l_range=(0.3, 0.5))))
+    for tag, network, g in samples:
+        with tempfile.TemporaryDirectory() as d:
+            network(d)
+            write_gnp_file(d, g)
+            subprocess.run([REF, d, os.path.join(d, "g.bin"), repr(VDW), repr(TUNNEL), repr(GS_MIN), repr(OVERLAP_CNT), repr(float(OVERLAP_GNP)),
+                            "-1", "flow", repr(cnt_config().step)], check=True, capture_output=True, timeout=600)
+            z = read_dump(os.path.join(d, "g.bin"))
+        for k, v in z.items():
+            if k.startswith("flow_") and k not in ("flow_points_gnp", "flow_structure_gnp_ptr", "flow_structure_gnp_idx"):
+                out[f"{tag}_{k}"] = v
+        print(f"flow {tag}: family {list(z['flow_family'])}, {len(z['flow_cnts_inside'])} CNTs and {len(z['flow_gnps_inside'])} GNPs inside")
+    np.savez_compressed(os.path.join(HERE, "gnp_hybrid_flow.npz"), **out)
+
+
 if __name__ == "__main__":
     main()
     main_labels()
     main_windows()
+    main_flow()

@@ -456,3 +456,74 @@ def test_gnp_entry_points_reject_bad_input(tmp_path):
         finally:
             L.cicy_gnp_set_free(h2)
     assert len(gnp_extract_window(d, 2.0)["gnps_inside"]) > 0
+
+
+FLOW = os.path.join(ROOT, "tests", "golden", "gnp_hybrid_flow.npz")
+
+
+@pytest.mark.parametrize("tag", ["s", "m"])
+def test_hybrid_chain_matches_upstream_flow(tmp_path, tag):
+    """The whole hybrid chain against upstream's own stage sequence for
+    GNP_CNT_mix (window extraction, contact grid, Determine_clusters_and_
+    percolation): the window extraction of CNTs and GNPs on the host
+    (cicy_extract_window, cicy_gnp_extract_window), then the CPU restatements of
+    the CNT contacts, labels and junctions, the GNP contact pass, junction
+    points and labels, the GNP point lists with the boundary points, the CNT-GNP
+    contacts, mixed labels and junctions, and the percolation with junction
+    groups: equal to upstream's clusters, isolated particles, families and
+    junction groups on both hybrid samples."""
+    import sys
+
+    from cicy_geom_b200.network import gnp_extract_window, read_network_files
+    from oracle import cicy_oracle as O, gnp_oracle as G
+    from oracle.dumpio import csr
+
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_gnp_golden as M
+
+    fz = dict(np.load(FLOW))
+    z = {k[len(tag) + 1:]: v for k, v in fz.items() if k.startswith(tag + "_")}
+    d = str(tmp_path)
+    if tag == "m":
+        M.hybrid_network(d)
+        write_gnp_file(d, generate_gnps(M.N, M.SIDE, M.SEED))
+        cfg = M.cnt_config()
+    else:
+        M.sparse_network(d)
+        write_gnp_file(d, generate_gnps(M.SPARSE_N, M.SIDE, M.SPARSE_SEED, l_range=(0.3, 0.5)))
+        cfg = M.sparse_config()
+    side = M.SIDE
+    a = dict(read_network_files(d).extract_window(cfg).arrays())
+    bc = [a["boundary_cnt_idx"][a["boundary_cnt_ptr"][f]:a["boundary_cnt_ptr"][f + 1]].tolist() for f in range(6)]
+    assert np.array_equal(a["cnts_inside"], z["flow_cnts_inside"]) and [list(x) for x in csr(z, "flow_boundary_cnt")] == bc
+    gw = gnp_extract_window(d, side)
+    bg = [gw["boundary_gnp_idx"][gw["boundary_gnp_ptr"][f]:gw["boundary_gnp_ptr"][f + 1]].tolist() for f in range(6)]
+    assert np.array_equal(gw["gnps_inside"], z["flow_gnps_inside"]) and [list(x) for x in csr(z, "flow_boundary_gnp")] == bg
+    vdw, tun, ovg = M.VDW, M.TUNNEL, float(M.OVERLAP_GNP)
+    p = {"gs_min": (M.GS_MIN,) * 3, "gs_overlap_cnt": M.OVERLAP_CNT, "gs_overlap_gnp": ovg, "vdw": vdw, "tunnel": tun, "min_points": 5}
+    n, l, regs = O.contact_grid(a, p)
+    lab_cnt, n_cnt, pc, ce = O.label_cnts(a, p, regs)
+    jc, _ = O.compress_junctions(a, p, pc, ce)
+    Vg = read_gnps(d)
+    sd_gnp = G.fill_sectioned_domain_gnps(a["window"], Vg["vertices"], Vg["l"], Vg["t"], gw["gnps_inside"], n, l, ovg)
+    V, F = Vg["vertices"].tolist(), Vg["planes"].tolist()
+    cts = []
+    for pa, pb, dd, _, _, pen in G.contact_pairs(sd_gnp, V, vdw, tun):
+        PA, PB, o = G.pair_junction(V[pa], F[pa], V[pb], F[pb], vdw, (0.0, 0.0, 0.0), (side, side, side))
+        cts.append((pa, pb, dd, pen, PA, PB, o))
+    NG = len(V)
+    lab_gnp, n_total = G.gnp_labels(NG, [(x[0], x[1]) for x in cts], [x[6] for x in cts], n_cnt)
+    sp = gw["structure_ptr"]
+    tol = 1.5 * float(np.max(Vg["t"]))
+    pts, st, jg, _ = G.add_gnp_junctions(cts, NG, tol * tol, [tuple(q) for q in gw["points"]],
+                                         [gw["structure_idx"][sp[g]:sp[g + 1]].tolist() for g in range(NG)])
+    mix = G.find_adjacent_labels(np.stack([a["x"], a["y"], a["z"]], 1).tolist(), a["flag"], a["radii"], regs, sd_gnp, V, F, vdw, tun)
+    order = sorted(mix.items(), key=lambda kv: kv[1][0])
+    mc, mg, nm = G.mixed_labels(lab_cnt, lab_gnp, n_total, [(int(a["flag"][P]), g) for (P, g), _ in order])
+    _, _, jm, _ = G.compress_mixed_contacts(mix, a["flag"], 5, pts, st)
+    res = G.mixed_percolation(nm, a["cnts_inside"], gw["gnps_inside"], mc, mg, bc, bg, [(j[1], j[3]) for j in jc], [(j[1], j[3]) for j in jg],
+                              [(j[1], j[3]) for j in jm])
+    assert res["family"] == list(z["flow_family"]) and len(res["family"]) >= 1
+    for key in ("clusters_cnt", "clusters_gnp", "isolated_cnt", "isolated_gnp", "cluster_cnt_junctions", "cluster_gnp_junctions",
+                "cluster_mix_junctions"):
+        assert res[key] == [list(x) for x in csr(z, "flow_" + key)], key
