@@ -51,7 +51,9 @@
  * runs upstream's stages for GNP_CNT_mix on window 0 (Shells,
  * Extract_observation_window, Generate_contact_grid,
  * Determine_clusters_and_percolation) and dumps the clusters, families and
- * junction groups (flow_* records).
+ * junction groups (flow_* records); with "electrical" after the step length,
+ * also Electrical_analysis::Perform_analysis_on_clusters along x and the
+ * resistances it writes.
  *
  * It also runs the GNP part of the window extraction for window 0
  * (Shells::Generate_shells, Cutoff_Wins::Fill_gnps_inside) with the sample as
@@ -78,6 +80,7 @@
 #include "Hoshen_Kopelman.h"
 #include "Input_Reader.h"
 #include "Cutoff_Wins.h"
+#include "Electrical_analysis.h"
 #include "Read_Network.h"
 #include "Shells.h"
 #include "Triangulation.h"
@@ -474,6 +477,43 @@ int main(int argc, char** argv) {
         std::vector<double> xyz;
         for (const Point_3D& q : pg) xyz.insert(xyz.end(), {q.x, q.y, q.z});
         o.f64("flow_points_gnp", xyz);
+        if (argc >= 12 && std::string(argv[11]) == "electrical") {
+            // Electrical_analysis::Perform_analysis_on_clusters along x (unit-resistor pass, backbone,
+            // real pass), the parameters of the hybrid configuration: rho_CNT 1e-3, GNP in-plane 1e-4
+            // and through-plane 1 Ohm um, exponential tunnelling junctions (Input_Reader.cpp:1445-1456),
+            // CG tolerance 1e-10; resistances.txt is read back
+            Electric_para ep;
+            ep.applied_voltage = 1.0;
+            ep.resistivity_CNT = 1e-3;
+            ep.resistivity_GNP_surf = 1e-4;
+            ep.resistivity_GNP_t = 1.0;
+            ep.resistivity_matrix = 1.03e20;
+            ep.junction_type = "exponential";
+            ep.junction_resistance = 1e7;
+            ep.h_plank = 6.62606957;
+            ep.e_charge = 1.60217662;
+            ep.e_mass = 9.10938291;
+            ep.lambda_barrier = 0.5;
+            const double sq = sqrt(2.0 * ep.e_mass * ep.lambda_barrier * ep.e_charge);
+            ep.C1 = 10.0 * ep.h_plank * ep.h_plank / (ep.e_mass * ep.e_mass * sq);
+            ep.C2 = 4000.0 * PI * sq / ep.h_plank;
+            sp.simulation_scope = 0;
+            sp.resistances[0] = 1;
+            sp.resistances[1] = sp.resistances[2] = 0;
+            sp.tolerance = 1e-10;
+            Output_data_flags of;
+            of.cnt_gnp_flag = of.gnp_data = of.prec_gnp = of.cnt_data = 0;
+            remove("resistances.txt");
+            Electrical_analysis EA;
+            if (!EA.Perform_analysis_on_clusters(0, win, sp, ep, cf, vf, of, &HF, &CW, structure, pts, radii, pg, sg, gf)) return 25;
+            std::vector<double> res;
+            if (FILE* rf = fopen("resistances.txt", "r")) {
+                double v;
+                while (fscanf(rf, "%lf", &v) == 1) res.push_back(v);
+                fclose(rf);
+            }
+            o.f64("flow_resistances", res);
+        }
     }
     o.i32("junc_pair", jn_pair);
     o.i32("junc_ok", jn_ok);

@@ -196,7 +196,9 @@ def main_flow():
     """tests/golden/gnp_hybrid_flow.npz: upstream's own stages for GNP_CNT_mix
     (window extraction, contact grid, Determine_clusters_and_percolation) on the
     two hybrid samples: cnts/gnps inside, boundary lists, percolated clusters,
-    isolated particles, families and junction groups (flow_* records)."""
+    isolated particles, families and junction groups (flow_* records), and the
+    resistances of Electrical_analysis along x (flow_resistances), the
+    end-to-end result of the hybrid configuration's path."""
     out = {}
     samples = (("m", hybrid_network, generate_gnps(N, SIDE, SEED)),
                ("s", sparse_network, generate_gnps(SPARSE_N, SIDE, SPARSE_SEED, l_range=(0.3, 0.5))))
@@ -205,12 +207,13 @@ def main_flow():
             network(d)
             write_gnp_file(d, g)
             subprocess.run([REF, d, os.path.join(d, "g.bin"), repr(VDW), repr(TUNNEL), repr(GS_MIN), repr(OVERLAP_CNT), repr(float(OVERLAP_GNP)),
-                            "-1", "flow", repr(cnt_config().step)], check=True, capture_output=True, timeout=600)
+                            "-1", "flow", repr(cnt_config().step), "electrical"], check=True, capture_output=True, timeout=1200)
             z = read_dump(os.path.join(d, "g.bin"))
         for k, v in z.items():
             if k.startswith("flow_") and k not in ("flow_points_gnp", "flow_structure_gnp_ptr", "flow_structure_gnp_idx"):
                 out[f"{tag}_{k}"] = v
-        print(f"flow {tag}: family {list(z['flow_family'])}, {len(z['flow_cnts_inside'])} CNTs and {len(z['flow_gnps_inside'])} GNPs inside")
+        print(f"flow {tag}: family {list(z['flow_family'])}, {len(z['flow_cnts_inside'])} CNTs and {len(z['flow_gnps_inside'])} GNPs inside, "
+              f"R_x {z['flow_resistances'][0]:.6g} Ohm")
     np.savez_compressed(os.path.join(HERE, "gnp_hybrid_flow.npz"), **out)
 
 

@@ -527,3 +527,15 @@ def test_hybrid_chain_matches_upstream_flow(tmp_path, tag):
     for key in ("clusters_cnt", "clusters_gnp", "isolated_cnt", "isolated_gnp", "cluster_cnt_junctions", "cluster_gnp_junctions",
                 "cluster_mix_junctions"):
         assert res[key] == [list(x) for x in csr(z, "flow_" + key)], key
+
+
+def test_hybrid_flow_golden_carries_upstream_resistances():
+    """The end-to-end target of the hybrid path: upstream's Electrical_analysis
+    on both hybrid samples gives a finite resistance along x (the percolating
+    direction of both) and the matrix resistance rho_m L / A along y and z,
+    which were not requested."""
+    z = dict(np.load(FLOW))
+    for tag in ("s", "m"):
+        r = z[f"{tag}_flow_resistances"]
+        assert len(r) == 3 and 0 < r[0] < 1e6
+        assert np.allclose(r[1:], 1.03e20 * 2.0 / 4.0)
