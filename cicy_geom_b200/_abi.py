@@ -203,6 +203,7 @@ class GnpWindowList(C.Structure):
         ("n_gnps", C.c_int32),
         ("structure_ptr", C.c_void_p),
         ("structure_idx", C.c_void_p),
+        ("volume", C.c_void_p),
     ]
 
 

@@ -143,6 +143,7 @@ cicy_status cicy_gnp_window_view(const cicy_gnp_window* h, cicy_gnp_window_list*
     v->n_gnps = (int32_t)g.structure.size();
     v->structure_ptr = g.flat_st_ptr.data();
     v->structure_idx = g.flat_st_idx.data();
+    v->volume = g.volume.data();
     return CICY_OK;
 }
 

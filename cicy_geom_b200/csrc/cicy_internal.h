@@ -75,6 +75,7 @@ struct GnpWindow {
     std::vector<std::vector<int32_t>> boundary_gnp, boundary_pts, structure;
     std::vector<double> points;  // 3 per point
     std::vector<int32_t> point_gnp, point_boundary;
+    std::vector<double> volume;  // per GNP: the volume inside the window where the extraction sets it, else NaN
     std::vector<int32_t> flat_bgnp_ptr, flat_bgnp_idx, flat_bpts_ptr, flat_bpts_idx, flat_st_ptr, flat_st_idx;
 };
 cicy_status gnp_window(const GnpSet& g, const cicy_window_params& w, GnpWindow& out, std::string& err);

@@ -717,8 +717,10 @@ void host_network_view(const HostNetwork& h, cicy_network& v) {
 // upstream's operation order.  GNPs whose shells reach window 0 get one
 // boundary point per window face they cross: the average of the points
 // accumulated on that face (GNP vertices on it, GNP edges cut by it, window
-// edges through the GNP, a window corner inside it).  The GNP volume inside the
-// window (Approximate_gnp_volume_inside_sample) is not computed.
+// edges through the GNP, a window corner inside it), and a volume inside the
+// window: l^2 t times the share of a 20 x 20 grid on its mid-plane that lies in
+// the window (Generate_Network::Approximate_gnp_volume_inside_sample,
+// Generate_Network.cpp:4750-4810).
 namespace {
 
 struct V3w {
@@ -767,6 +769,7 @@ cicy_status gnp_window(const GnpSet& g, const cicy_window_params& w, GnpWindow& 
     out.boundary_gnp.assign(6, std::vector<int32_t>());
     out.boundary_pts.assign(6, std::vector<int32_t>());
     out.structure.assign(g.n, std::vector<int32_t>());
+    out.volume.assign(g.n, std::nan(""));
     const GnpWin gw{c};
     V3w W[8];
     gw.window_vertices(W);
@@ -863,6 +866,28 @@ cicy_status gnp_window(const GnpSet& g, const cicy_window_params& w, GnpWindow& 
                 for (int j = 0; j < 3; j++) acc[corner_b[k][j]].push_back(P);
                 break;
             }
+        }
+        {  // Approximate_gnp_volume_inside_sample on the window
+            const V3w c3{(V[3].x + V[7].x) / 2.0, (V[3].y + V[7].y) / 2.0, (V[3].z + V[7].z) / 2.0};
+            const V3w c0{(V[0].x + V[4].x) / 2.0, (V[0].y + V[4].y) / 2.0, (V[0].z + V[4].z) / 2.0};
+            const V3w c2{(V[2].x + V[6].x) / 2.0, (V[2].y + V[6].y) / 2.0, (V[2].z + V[6].z) / 2.0};
+            const V3w c1{(V[1].x + V[5].x) / 2.0, (V[1].y + V[5].y) / 2.0, (V[1].z + V[5].z) / 2.0};
+            const V3w dir_right = c0 - c3, dir_right_up = c1 - c2;
+            const int np = 20;
+            int in = 0;
+            for (int a = 0; a < np; a++) {
+                const double lr = (double)a / (np - 1);
+                const V3w start = c3 + dir_right * lr, end = c2 + dir_right_up * lr, dir_up = end - start;
+                for (int b = 0; b < np; b++) {
+                    const double lu = (double)b / (np - 1);
+                    const V3w q = start + dir_up * lu;
+                    if (!(q.x < c.win.min_x || q.x > c.win.max_x || q.y < c.win.min_y || q.y > c.win.max_y || q.z < c.win.min_z || q.z > c.win.max_z))
+                        in++;
+                }
+            }
+            double vol = g.l[i] * g.l[i] * g.t[i];
+            if (in != 0) vol = vol * ((double)in / (np * np));
+            out.volume[i] = vol;
         }
         for (int b = 0; b < 6; b++) {
             if (acc[b].empty()) continue;

@@ -576,7 +576,8 @@ def gnp_extract_window(directory: str, side: float, window_side=None) -> dict:
                 "boundary_pts_ptr": bp_ptr, "boundary_pts_idx": arr(v.boundary_pts_idx, C.c_int32, int(bp_ptr[-1]), np.int32),
                 "points": arr(v.points, C.c_double, 3 * n, np.float64).reshape(n, 3),
                 "point_gnp": arr(v.point_gnp, C.c_int32, n, np.int32), "point_boundary": arr(v.point_boundary, C.c_int32, n, np.int32),
-                "structure_ptr": st_ptr, "structure_idx": arr(v.structure_idx, C.c_int32, int(st_ptr[-1]), np.int32)}
+                "structure_ptr": st_ptr, "structure_idx": arr(v.structure_idx, C.c_int32, int(st_ptr[-1]), np.int32),
+                "volume": arr(v.volume, C.c_double, v.n_gnps, np.float64)}
     finally:
         if win:
             lib().cicy_gnp_window_free(win)

@@ -405,8 +405,8 @@ void cicy_gnp_set_free(cicy_gnp_set* set);
  * boundary point: the average of its vertices on the face, its edges' cuts
  * through the face, the window edges through it and a window corner inside it
  * (upstream's points_gnp / structure_gnp / boundary_gnp / boundary_gnp_pts
- * before the contact search; n_points is gnp_pts_bdds).  The GNP volume inside
- * the window is not computed. */
+ * before the contact search; n_points is gnp_pts_bdds), and those GNPs'
+ * volume inside the window. */
 typedef struct cicy_gnp_window cicy_gnp_window;
 typedef struct {
     int32_t n_inside;
@@ -422,6 +422,8 @@ typedef struct {
     int32_t n_gnps;
     const int32_t* structure_ptr;      /* [n_gnps + 1] each GNP's boundary points */
     const int32_t* structure_idx;
+    const double* volume;              /* [n_gnps] volume inside the window (Approximate_gnp_volume_inside_sample)
+                                          of the GNPs crossing a face, NaN for the others */
 } cicy_gnp_window_list;
 cicy_status cicy_gnp_extract_window(const cicy_gnp_set* gnps, const cicy_window_params* w, cicy_gnp_window** out);
 /* Borrowed view; valid until cicy_gnp_window_free. */

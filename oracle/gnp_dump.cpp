@@ -173,6 +173,9 @@ int main(int argc, char** argv) {
         for (const Point_3D& q : pg) xyz.insert(xyz.end(), {q.x, q.y, q.z});
         o.f64("win_points", xyz);
         o.f64("win_box", {win.poi_min.x, win.poi_min.y, win.poi_min.z, win.len_x, win.wid_y, win.hei_z, win.max_x, win.max_y, win.max_z});
+        std::vector<double> vol;
+        for (const GNP& gg : gcopy) vol.push_back(gg.volume);
+        o.f64("win_volume", vol);
     }
     std::vector<double> lt, center, rot, vert, planes;
     for (const GNP& g : gnps) {

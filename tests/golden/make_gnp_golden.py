@@ -186,7 +186,7 @@ def main_windows():
             out[f"c{k}_in_{key}"] = g[key]
         out[f"c{k}_meta"] = np.array([n, side, seed, ws])
         for key in ("win_inside", "win_bgnp_ptr", "win_bgnp_idx", "win_bpts_ptr", "win_bpts_idx", "win_structure_ptr", "win_structure_idx",
-                    "win_points", "win_box"):
+                    "win_points", "win_box", "win_volume"):
             out[f"c{k}_ref_{key}"] = z[key]
         print(f"window case {k}: {n} GNPs in {side} um, window {ws} um: {len(z['win_inside'])} inside, {len(z['win_points']) // 3} boundary points")
     np.savez_compressed(os.path.join(HERE, "gnp_windows.npz"), **out)

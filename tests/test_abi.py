@@ -27,8 +27,8 @@ def test_struct_sizes_match_header_layout():
     assert C.sizeof(_abi.GnpPairList) == 8 * 3 + 8 * 9
     # cicy_gnp_point_list: count, pointer, n_gnps (+4), 2 pointers, count, 2 pointers, n_boundary (+4), pointer
     assert C.sizeof(_abi.GnpPointList) == 8 * 2 + 8 + 8 * 2 + 8 * 3 + 8 + 8
-    # cicy_gnp_window_list: n_inside (+4), 3 pointers, count, 5 pointers, n_gnps (+4), 2 pointers
-    assert C.sizeof(_abi.GnpWindowList) == 8 + 8 * 3 + 8 + 8 * 5 + 8 + 8 * 2
+    # cicy_gnp_window_list: n_inside (+4), 3 pointers, count, 5 pointers, n_gnps (+4), 3 pointers
+    assert C.sizeof(_abi.GnpWindowList) == 8 + 8 * 3 + 8 + 8 * 5 + 8 + 8 * 3
 
 
 def test_context_creation_without_gpu_fails_cleanly():

@@ -399,8 +399,9 @@ def _window_case(tmp_path, k):
 @pytest.mark.parametrize("k", [-1, 0, 1])
 def test_gnp_window_extraction_matches_upstream_golden(tmp_path, k):
     """cicy_gnp_extract_window (host) against upstream's Fill_gnps_inside:
-    gnps_inside, boundary_gnp, boundary_gnp_pts, structure_gnp and the boundary
-    points bit for bit, for the whole sample and two centred smaller windows."""
+    gnps_inside, boundary_gnp, boundary_gnp_pts, structure_gnp, the boundary
+    points and the volumes inside the window bit for bit, for the whole sample
+    and two centred smaller windows."""
     from cicy_geom_b200.network import gnp_extract_window
 
     side, ws, ref = _window_case(tmp_path, k)
@@ -409,6 +410,9 @@ def test_gnp_window_extraction_matches_upstream_golden(tmp_path, k):
     for mine, theirs in (("boundary_gnp", "win_bgnp"), ("boundary_pts", "win_bpts"), ("structure", "win_structure")):
         assert np.array_equal(w[mine + "_ptr"], ref[theirs + "_ptr"]) and np.array_equal(w[mine + "_idx"], ref[theirs + "_idx"])
     assert np.array_equal(w["points"].ravel().view(np.int64), ref["win_points"].view(np.int64)) and len(w["points"]) > 100
+    vol = w["volume"]
+    set_ = ~np.isnan(vol)  # the GNPs whose volume the extraction sets (Approximate_gnp_volume_inside_sample)
+    assert set_.sum() > 50 and np.array_equal(vol[set_].view(np.int64), ref["win_volume"][set_].view(np.int64))
 
 
 def test_gnp_entry_points_reject_bad_input(tmp_path):
