@@ -55,6 +55,9 @@
  * also Electrical_analysis::Perform_analysis_on_clusters along x and the
  * resistances it writes.
  *
+ * With a gnp_resistor_cases.dat in the directory it evaluates upstream's
+ * Direct_Electrifying::Calculate_resistance_gnp on each case (gnp_resistances).
+ *
  * It also runs the GNP part of the window extraction for window 0
  * (Shells::Generate_shells, Cutoff_Wins::Fill_gnps_inside) with the sample as
  * the window, or a centred window of side argv[8] when given, and dumps
@@ -80,6 +83,7 @@
 #include "Hoshen_Kopelman.h"
 #include "Input_Reader.h"
 #include "Cutoff_Wins.h"
+#include "Direct_Electrifying.h"
 #include "Electrical_analysis.h"
 #include "Read_Network.h"
 #include "Shells.h"
@@ -144,6 +148,26 @@ int main(int argc, char** argv) {
     Out o;
     o.f = fopen(out_path.c_str(), "wb");
     if (!o.f) return 5;
+    if (FILE* rf = fopen("gnp_resistor_cases.dat", "rb")) {
+        // Direct_Electrifying::Calculate_resistance_gnp on the cases of the file:
+        // int n, then per case P1 (3), P2 (3), rad1, rad2, rho_surf, rho_t
+        int nc = 0;
+        if (fread(&nc, 4, 1, rf) != 1) return 18;
+        std::vector<double> rr;
+        Direct_Electrifying D;
+        for (int k = 0; k < nc; k++) {
+            double v[10];
+            if (fread(v, 8, 10, rf) != 10) return 18;
+            Electric_para ep;
+            ep.resistivity_GNP_surf = v[8];
+            ep.resistivity_GNP_t = v[9];
+            double Re = -1.0;
+            const int ok = D.Calculate_resistance_gnp(Point_3D(v[0], v[1], v[2]), Point_3D(v[3], v[4], v[5]), v[6], v[7], ep, Re);
+            rr.push_back(ok ? Re : -1.0);
+        }
+        fclose(rf);
+        o.f64("gnp_resistances", rr);
+    }
     {
         // GNP part of the window extraction for window 0 (Shells::Generate_shells,
         // Cutoff_Wins::Fill_gnps_inside); the window's side is argv[8] when given, else the sample's
@@ -161,6 +185,7 @@ int main(int argc, char** argv) {
         if (!SH.Generate_shells("GNP_cuboids", gw, no_points, gnps, shells_cnt, shells_gnp)) return 16;
         const cuboid win = gw.update_observation_window_geometry(0, "GNP_cuboids");
         std::vector<GNP> gcopy = gnps;
+        for (GNP& gg : gcopy) gg.volume = std::nan("");  // upstream leaves the volume of GNPs it does not process unset
         std::vector<std::vector<long int> > st(gnps.size());
         std::vector<Point_3D> pg;
         Cutoff_Wins CW;

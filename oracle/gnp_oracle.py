@@ -1017,3 +1017,18 @@ def mixed_percolation(n_clusters, cnts_inside, gnps_inside, labels_cnt, labels_g
         out["cluster_gnp_junctions"] = group(junctions_gnp, labels_gnp, labels_gnp, len(out["clusters_gnp"])) if junctions_gnp else []
         out["cluster_mix_junctions"] = group(junctions_mixed, labels_cnt, labels_gnp, len(out["clusters_cnt"])) if junctions_mixed else []
     return out
+
+
+def gnp_resistance(P1, P2, rad1: float, rad2: float, rho_surf: float, rho_t: float):
+    """Direct_Electrifying::Calculate_resistance_gnp (Direct_Electrifying.cpp:1198-1232):
+    R = rho L / (pi r1 r2) with rho = u . (u_x rho_surf, u_y rho_surf, u_z rho_t),
+    u the unit vector from P1 to P2 (the global z axis as the through-plane
+    direction, as upstream has it); None when the points coincide (L < 1e-10)."""
+    P1 = tuple(float(c) for c in P1)
+    P2 = tuple(float(c) for c in P2)
+    L = _dist(P1, P2)
+    if L < ZERO:
+        return None
+    u = _div(_sub(P2, P1), L)
+    rho = _dot((u[0] * rho_surf, u[1] * rho_surf, u[2] * rho_t), u)
+    return rho * L / (3.1415926535897932384626433832795 * rad1 * rad2)

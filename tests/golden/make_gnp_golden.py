@@ -217,8 +217,39 @@ def main_flow():
     np.savez_compressed(os.path.join(HERE, "gnp_hybrid_flow.npz"), **out)
 
 
+def main_resistors():
+    """tests/golden/gnp_resistors.npz: upstream's Calculate_resistance_gnp on the
+    triangulation edges of the 120-GNP fixture's GNPs (radii t/2, or the CNT
+    radius at a mixed-junction point, as Fill_2d_matrices_gnp takes them; GNP
+    in-plane 1e-4 and through-plane 1 Ohm um) and one edge of coincident points."""
+    z = dict(np.load(os.path.join(HERE, f"gnp_{N}_s{SEED}.npz")))
+    pts = z["ref_mixjn_points"].reshape(-1, 3)
+    n_before_mixed = len(z["ref_gnpjn_points"]) // 3
+    t = z["ref_gnp_lt"].reshape(-1, 2)[:, 1]
+    tp, te = z["ref_tri_ptr"], z["ref_tri_edges"].reshape(-1, 2)
+    cases = []
+    for g in range(len(tp) - 1):
+        for v1, v2 in te[tp[g]:tp[g + 1]]:
+            r = [0.005 if v >= n_before_mixed else t[g] / 2 for v in (v1, v2)]
+            cases.append([*pts[v1], *pts[v2], r[0], r[1], 1e-4, 1.0])
+    cases.append([*pts[0], *pts[0], 0.005, 0.005, 1e-4, 1.0])  # coincident points: upstream fails
+    cases = np.array(cases)
+    g = generate_gnps(N, SIDE, SEED)
+    with tempfile.TemporaryDirectory() as d:
+        write_gnp_file(d, g)
+        with open(os.path.join(d, "sample_geom.csv"), "w") as f:
+            f.write(f"0,0,0\n{SIDE!r},{SIDE!r},{SIDE!r}\n")
+        with open(os.path.join(d, "gnp_resistor_cases.dat"), "wb") as f:
+            f.write(np.int32(len(cases)).tobytes() + cases.astype("<f8").tobytes())
+        subprocess.run([REF, d, os.path.join(d, "g.bin"), repr(VDW), repr(TUNNEL)], check=True, capture_output=True, timeout=600)
+        r = read_dump(os.path.join(d, "g.bin"))["gnp_resistances"]
+    np.savez_compressed(os.path.join(HERE, "gnp_resistors.npz"), cases=cases, ref_resistance=r)
+    print(f"GNP resistors: {len(cases)} cases")
+
+
 if __name__ == "__main__":
     main()
     main_labels()
     main_windows()
     main_flow()
+    main_resistors()

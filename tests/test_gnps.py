@@ -412,7 +412,8 @@ def test_gnp_window_extraction_matches_upstream_golden(tmp_path, k):
     assert np.array_equal(w["points"].ravel().view(np.int64), ref["win_points"].view(np.int64)) and len(w["points"]) > 100
     vol = w["volume"]
     set_ = ~np.isnan(vol)  # the GNPs whose volume the extraction sets (Approximate_gnp_volume_inside_sample)
-    assert set_.sum() > 50 and np.array_equal(vol[set_].view(np.int64), ref["win_volume"][set_].view(np.int64))
+    assert np.array_equal(set_, ~np.isnan(ref["win_volume"])) and set_.sum() > 50
+    assert np.array_equal(vol[set_].view(np.int64), ref["win_volume"][set_].view(np.int64))
 
 
 def test_gnp_entry_points_reject_bad_input(tmp_path):
@@ -543,3 +544,21 @@ def test_hybrid_flow_golden_carries_upstream_resistances():
         r = z[f"{tag}_flow_resistances"]
         assert len(r) == 3 and 0 < r[0] < 1e6
         assert np.allclose(r[1:], 1.03e20 * 2.0 / 4.0)
+
+
+def test_gnp_resistance_oracle_matches_upstream_golden():
+    """The GNP resistor of a triangulation edge restated on the CPU against
+    upstream's Calculate_resistance_gnp on the 120-GNP fixture's edges (radii as
+    Fill_2d_matrices_gnp takes them), bit for bit, and upstream's failure on
+    coincident points."""
+    from oracle import gnp_oracle as G
+
+    z = dict(np.load(os.path.join(ROOT, "tests", "golden", "gnp_resistors.npz")))
+    cases, ref = z["cases"], z["ref_resistance"]
+    assert len(cases) > 1000
+    for c, r in zip(cases, ref):
+        R = G.gnp_resistance(c[0:3], c[3:6], c[6], c[7], c[8], c[9])
+        if r == -1.0:
+            assert R is None
+        else:
+            assert np.float64(R).view(np.int64) == np.float64(r).view(np.int64)
