@@ -251,6 +251,7 @@ def lib() -> C.CDLL:
         "cicy_ctx_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
         "cicy_ctx_stream": (C.c_void_p, [C.c_void_p]),
         "cicy_ctx_set_solver": (C.c_int, [C.c_void_p, P(SolverOpts)]),
+        "cicy_ctx_set_spin_limit": (C.c_int, [C.c_void_p, C.c_int64]),
         "cicy_last_error": (C.c_char_p, [C.c_void_p]),
         "cicy_ctx_kernel_launches": (C.c_int64, [C.c_void_p]),
         "cicy_upload_network": (C.c_int, [C.c_void_p, P(Network)]),
@@ -262,6 +263,7 @@ def lib() -> C.CDLL:
         "cicy_get_point_contacts": (C.c_int, [C.c_void_p, i64p, i64p, i32p, i64p, f64p]),
         "cicy_get_labels": (C.c_int, [C.c_void_p, i32p, i32p, i32p]),
         "cicy_get_junctions": (C.c_int, [C.c_void_p, i64p, i64p, i32p, i64p, i32p, f64p]),
+        "cicy_get_volumes": (C.c_int, [C.c_void_p, f64p, f64p, f64p, f64p]),
         "cicy_get_elements": (C.c_int, [C.c_void_p, C.c_int32, i64p, i64p, i64p, i64p]),
         "cicy_get_clusters": (C.c_int, [C.c_void_p, C.c_int32, i32p, i64p, i64p, i32p, i32p, i64p, i64p, i32p]),
         "cicy_get_system": (C.c_int, [C.c_void_p, C.c_int32, i64p, i64p, i64p, i64p, i64p, f64p, f64p, f64p, f64p, f64p]),

@@ -25,7 +25,7 @@ def monte_carlo_configs(count: int, seed0: int = 3_000_000, side=(2.0, 5.0), fra
         L = float(rng.uniform(*side))
         phi = float(rng.uniform(*fraction))
         n = int(round(phi * L ** 3 / (math.pi * radius ** 2 * 1.0)))
-        out.append(NetworkConfig(side=L, n_cnts=max(n, 1), seed=seed0 + k, tolerance=1e-8, tolerance_unit=1e-10))
+        out.append(NetworkConfig(side=L, n_cnts=max(n, 1), seed=seed0 + k, tolerance=1e-8, tolerance_unit=1e-12))
     return out
 
 

@@ -98,6 +98,10 @@ cicy_status cicy_ctx_set_solver(cicy_ctx* ctx, const cicy_solver_opts* o) {
     });
 }
 
+cicy_status cicy_ctx_set_spin_limit(cicy_ctx* ctx, int64_t polls) {
+    return guarded(ctx, [&](cicy::Ctx& c) { c.sw.spin_limit = polls > 0 ? (long long)polls : cicy::kSpinLimit; });
+}
+
 const char* cicy_last_error(const cicy_ctx* ctx) { return ctx ? ctx->c.err.c_str() : "null context"; }
 
 int64_t cicy_ctx_kernel_launches(const cicy_ctx* ctx) { return ctx ? ctx->c.launches : 0; }
@@ -299,6 +303,19 @@ cicy_status cicy_get_junctions(cicy_ctx* ctx, int64_t* n, int64_t* p1, int32_t* 
         d2h(c, n2, c.j_n2.get(), N);
         d2h(c, dist, c.j_d.get(), N);
         sync(c);
+    });
+}
+
+cicy_status cicy_get_volumes(cicy_ctx* ctx, double* volumes_cnt, double* dead_branches, double* total_volumes, double* fractions) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (!c.have_volumes) throw cicy::Fail{CICY_E_STATE, "no volumes yet (cicy_electrical_analysis with simulation_scope < 2)"};
+        double acc[31];
+        d2h(c, acc, c.vol_acc.get(), 31);
+        sync(c);
+        if (volumes_cnt) std::copy(acc, acc + 8, volumes_cnt);
+        if (dead_branches) std::copy(acc + 8, acc + 15, dead_branches);
+        if (total_volumes) std::copy(acc + 15, acc + 23, total_volumes);
+        if (fractions) std::copy(acc + 23, acc + 31, fractions);
     });
 }
 

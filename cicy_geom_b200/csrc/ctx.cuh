@@ -130,6 +130,13 @@ struct Ctx {
     DBuf<int32_t> eb, ee, alive, alive_scan, tmp_list;
     DBuf<unsigned long long> imax;
     std::vector<int32_t> bb_clu_len, bb_cj_len;
+    // backbone volumes: per-CNT parts of the cluster being classified, the isolated-list sort,
+    // and the volume members (volumes_cnt[8], dead_branches[7], total_volumes[8], fractions[8])
+    DBuf<double> vol3, vol_acc;
+    DBuf<int32_t> vol_kind;
+    DBuf<uint64_t> vol_key;
+    DBuf<uint32_t> vol_cnt;
+    bool have_volumes = false;
     DBuf<int32_t> chain_start, chain_len;
     SolverWork sw;
     GnnState gnn;

@@ -112,6 +112,7 @@ int bits_for(uint64_t max_value);
 struct GridBarrier {
     unsigned int* count;
     unsigned int* gen;
+    long long limit = kSpinLimit;  // polls before the wait gives up
 };
 
 __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
@@ -133,7 +134,7 @@ __device__ __forceinline__ bool grid_sync(GridBarrier b, unsigned int nblocks, i
         } else {
             long long spins = 0;
             while (ld_acquire_u32(b.gen) == g) {
-                if (++spins > kSpinLimit || *((volatile int*)err) != 0) {
+                if (++spins > b.limit || *((volatile int*)err) != 0) {
                     atomicCAS(err, 0, (int)DEV_TIMEOUT);
                     break;
                 }

@@ -15,8 +15,10 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <utility>
 
 #include "cicy_internal.h"
+#include "csr_check.cuh"
 #include "solver.cuh"
 
 namespace cicy {
@@ -45,7 +47,9 @@ static __device__ __align__(256) unsigned char g_pcg_scratch[kStaticBytes];
 std::mutex g_mu;
 unsigned char* g_scratch_addr[64] = {nullptr};  // device address of g_pcg_scratch, per device
 
-// Device address of the static array on the current device (set up once per device).
+// Device address of the static array on the current device, looked up on the
+// first call on each device and kept for the life of the process (a device
+// reset or a re-created primary context invalidates it).
 cicy_status scratch_address(int dev, unsigned char** out, std::string& err) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (dev < 0 || dev >= 64) {
@@ -63,6 +67,15 @@ cicy_status scratch_address(int dev, unsigned char** out, std::string& err) {
     }
     *out = g_scratch_addr[dev];
     return CICY_OK;
+}
+
+// Structure check of the caller's CSR before any kernel uses its indices as
+// addresses: every read stays within row_ptr[n + 1] and col_ind[nnz].
+__global__ void k_check_structure(int n, int nnz, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                  int* __restrict__ flags) {
+    const int f = check_structure_part(blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, n, nnz, rp, ci, 0, nullptr,
+                                       nullptr);
+    if (f) atomicOr(flags, f);
 }
 
 __global__ void k_diag_inverse(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const double* __restrict__ v,
@@ -111,8 +124,13 @@ extern "C" cicy_status cicy_jacobi_pcg_static(int32_t n, int32_t nnz, const int3
     }
     cudaStream_t s = (cudaStream_t)stream;
     int sms = 0, coop = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    for (auto q : {std::make_pair(&sms, cudaDevAttrMultiProcessorCount), std::make_pair(&coop, cudaDevAttrCooperativeLaunch)}) {
+        const cudaError_t e = cudaDeviceGetAttribute(q.first, q.second, dev);
+        if (e != cudaSuccess) {
+            set_host_error(std::string("cicy_jacobi_pcg_static: cudaDeviceGetAttribute: ") + cudaGetErrorString(e));
+            return CICY_E_DEVICE;
+        }
+    }
     if (!coop || sms <= 0) {
         set_host_error("cicy_jacobi_pcg_static: device lacks cooperative launch");
         return CICY_E_DEVICE;
@@ -126,13 +144,24 @@ extern "C" cicy_status cicy_jacobi_pcg_static(int32_t n, int32_t nnz, const int3
     double* stats = reinterpret_cast<double*>(base + kOffStats);
     unsigned int* bar = reinterpret_cast<unsigned int*>(base + kOffBarrier);
     int* status = reinterpret_cast<int*>(base + kOffBarrier + 64);
+    int* structure = reinterpret_cast<int*>(base + kOffBarrier + 128);
     int32_t* cta_row = reinterpret_cast<int32_t*>(base + kOffCtaRow);
     try {
         int64_t launches = 0;
         const int cap = max_coop_blocks_jacobi_fp64(sms);
         const int nb = std::max(1, std::min({cap, sms, ceil_div(n, 256), kStaticMaxCtas}));
         // the array keeps the previous call's contents: reset what must start at zero
+        // (stats, barrier, status and structure words)
         CICY_CUDA(cudaMemsetAsync(base + kOffStats, 0, 256 + 256, s));
+        k_check_structure<<<std::min(ceil_div(std::max(n, nnz), 256), 148 * 8), 256, 0, s>>>(n, nnz, row_ptr, col_ind, structure);
+        CICY_LAUNCH_CHECK();
+        int hflags = 0;
+        CICY_CUDA(cudaMemcpyAsync(&hflags, structure, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CICY_CUDA(cudaStreamSynchronize(s));
+        if (hflags) {
+            set_host_error("cicy_jacobi_pcg_static: " + structure_error(hflags));
+            return CICY_E_INPUT;
+        }
         k_diag_inverse<<<std::min(ceil_div(n, 256), 148 * 8), 256, 0, s>>>(n, row_ptr, col_ind, values, minv, status);
         k_residual<<<std::min(ceil_div(n, 256), 148 * 8), 256, 0, s>>>(n, row_ptr, col_ind, values, x, b, r);
         k_uniform_rows<<<1, 256, 0, s>>>(nb, n, cta_row);
@@ -162,9 +191,13 @@ extern "C" cicy_status cicy_jacobi_pcg_static(int32_t n, int32_t nnz, const int3
             set_host_error("cicy_jacobi_pcg_static: a bounded device wait gave up");
             return CICY_E_TIMEOUT;
         }
-        if (hstatus != 0) {
+        if (hstatus == DEV_ZERO_DIAG) {
             set_host_error("cicy_jacobi_pcg_static: zero on the diagonal");
             return CICY_E_ZERO_DIAGONAL;
+        }
+        if (hstatus != 0) {
+            set_host_error("cicy_jacobi_pcg_static: device status " + std::to_string(hstatus));
+            return CICY_E_INTERNAL;
         }
         if (iterations) *iterations = (int64_t)hs[0];
         if (rel_residual) *rel_residual = hs[2] > 0 ? std::sqrt(hs[1]) / (hs[2] / tol) : 0.0;

@@ -535,7 +535,7 @@ void pcg_solve(SolverWork& w, const SolverSystem& sys, int precond, bool mixed, 
     }
     a.partA = w.part.get(); a.partB = w.part.get() + 2 * nb;
     a.stats = w.stats.get();
-    a.bar = GridBarrier{w.barrier.get(), w.barrier.get() + 1};
+    a.bar = GridBarrier{w.barrier.get(), w.barrier.get() + 1, w.spin_limit};
     a.err = status;
     a.tol = tol;
     a.max_iter = max_iter;

@@ -239,6 +239,7 @@ struct MgArgs {
     double* partB;
     double* stats;
     unsigned long long* bar;  // monotonic arrival counter (zeroed before the launch)
+    long long spin_limit;     // polls of a barrier wait before it gives up
     int* err;
     double tol;
     long long max_iter;
@@ -246,22 +247,23 @@ struct MgArgs {
     int cap_b;  // stop at |r| <= tol min(|r0|, |b|) (batched solves); else |r| <= tol |r0| (Direct_Electrifying.cpp:1571, 1619)
 };
 
-// Grid barrier on a monotonic counter: one release-add per CTA, then an acquire
-// spin until all CTAs of this round arrived.  Bounded: after kSpinLimit polls the
-// CTA records DEV_TIMEOUT and returns false.
-__device__ __forceinline__ bool mg_sync(unsigned long long* bar, unsigned long long& target, int* err, int* s_ok) {
+// Grid barrier on a monotonic counter: one release-reduction per CTA (no return
+// value to wait for; the release orders the CTA's writes, which __syncthreads
+// gathered under thread 0, before the arrival), then an acquire spin until all
+// CTAs of this round arrived.  Bounded: after `limit` polls the CTA records
+// DEV_TIMEOUT and returns false.
+__device__ __forceinline__ bool mg_sync(unsigned long long* bar, unsigned long long& target, int* err, int* s_ok, long long limit) {
     __syncthreads();
     if (threadIdx.x == 0) {
         target += gridDim.x;
-        __threadfence();
-        atomicAdd(bar, 1ull);
+        asm volatile("red.release.gpu.global.add.u64 [%0], 1;" ::"l"(bar) : "memory");
         long long spins = 0;
         int ok = 1;
         while (true) {
             unsigned long long v;
             asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(bar) : "memory");
             if (v >= target) break;
-            if ((++spins & 1023) == 0 && (spins > kSpinLimit || *((volatile int*)err) != 0)) {
+            if (++spins > limit || ((spins & 1023) == 0 && *((volatile int*)err) != 0)) {
                 atomicCAS(err, 0, (int)DEV_TIMEOUT);
                 ok = 0;
                 break;
@@ -276,13 +278,13 @@ __device__ __forceinline__ bool mg_sync(unsigned long long* bar, unsigned long l
 // Cluster variant: the hardware cluster barrier (release/acquire at cluster
 // scope orders the global-memory writes of all CTAs of the cluster).
 template <bool CL>
-__device__ __forceinline__ bool sync_all(unsigned long long* bar, unsigned long long& target, int* err, int* s_ok) {
+__device__ __forceinline__ bool sync_all(unsigned long long* bar, unsigned long long& target, int* err, int* s_ok, long long limit) {
     if constexpr (CL) {
         asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
         asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
         return true;
     } else {
-        return mg_sync(bar, target, err, s_ok);
+        return mg_sync(bar, target, err, s_ok, limit);
     }
 }
 
@@ -428,7 +430,7 @@ __device__ void mg_pcg_body(const MgArgs& a, int cta, int nctas) {
         double s0;
         mg_reduce1(bb_l, sm, s0);
         if (threadIdx.x == 0) a.partB[cta] = s0;
-        if (!sync_all<CL>(a.bar, target, a.err, &s_ok)) return;
+        if (!sync_all<CL>(a.bar, target, a.err, &s_ok, a.spin_limit)) return;
         bnorm = sqrt(mg_sum_partials(a.partB, nb, sm));
     }
     long long k = 0;
@@ -447,7 +449,7 @@ __device__ void mg_pcg_body(const MgArgs& a, int cta, int nctas) {
         double s0;
         mg_reduce1(rr_l, sm, s0);
         if (threadIdx.x == 0) a.partA[cta] = s0;
-        if (!sync_all<CL>(a.bar, target, a.err, &s_ok)) return;
+        if (!sync_all<CL>(a.bar, target, a.err, &s_ok, a.spin_limit)) return;
         rr = mg_sum_partials(a.partA, nb, sm);
         if (k == 0 && !recursive && restarts == 0) R0 = a.tol * (a.cap_b ? fmin(sqrt(rr), bnorm) : sqrt(rr));
         if (k > 0 && sqrt(rr) <= R0) {
@@ -480,7 +482,7 @@ __device__ void mg_pcg_body(const MgArgs& a, int cta, int nctas) {
                     if (smooth) G.z[J] = G.l1inv[J] * s;
                 }
             }
-            if (!sync_all<CL>(a.bar, target, a.err, &s_ok)) return;
+            if (!sync_all<CL>(a.bar, target, a.err, &s_ok, a.spin_limit)) return;
         }
         // ---- restrictions l -> l+1 (l >= 1): r_{l+1} = P^T r_l - (P^T A_l) z_l ----
         for (int l = 1; l < C; l++) {
@@ -496,7 +498,7 @@ __device__ void mg_pcg_body(const MgArgs& a, int cta, int nctas) {
                     if (smooth) G.z[J] = G.l1inv[J] * s;
                 }
             }
-            if (!sync_all<CL>(a.bar, target, a.err, &s_ok)) return;
+            if (!sync_all<CL>(a.bar, target, a.err, &s_ok, a.spin_limit)) return;
         }
         // ---- coarsest: dense inverse, one warp per row ----
         if (a.cinv) {
@@ -514,7 +516,7 @@ __device__ void mg_pcg_body(const MgArgs& a, int cta, int nctas) {
                     if (lane == 0) Cl.zf[i] = s;
                 }
             }
-            if (!sync_all<CL>(a.bar, target, a.err, &s_ok)) return;
+            if (!sync_all<CL>(a.bar, target, a.err, &s_ok, a.spin_limit)) return;
         }
         // ---- prolongation + l1-Jacobi post-smoother, levels C-1 .. 1 ----
         for (int l = C - 1; l >= 1; l--) {
@@ -529,7 +531,7 @@ __device__ void mg_pcg_body(const MgArgs& a, int cta, int nctas) {
                     F.zf[I] = zp + F.l1inv[I] * w;
                 }
             }
-            if (!sync_all<CL>(a.bar, target, a.err, &s_ok)) return;
+            if (!sync_all<CL>(a.bar, target, a.err, &s_ok, a.spin_limit)) return;
         }
         // ---- level-0 post-smoother: z = z0 + P z1, z += w M0^-1 (r - A z); r.z ----
         {
@@ -549,7 +551,7 @@ __device__ void mg_pcg_body(const MgArgs& a, int cta, int nctas) {
             }
             mg_reduce1(rz_l, sm, s0);
             if (threadIdx.x == 0) a.partB[cta] = s0;
-            if (!sync_all<CL>(a.bar, target, a.err, &s_ok)) return;
+            if (!sync_all<CL>(a.bar, target, a.err, &s_ok, a.spin_limit)) return;
             const double rz_new = mg_sum_partials(a.partB, nb, sm);
             beta = fresh ? 0.0 : rz_new / rz;
             rz = rz_new;
@@ -567,7 +569,7 @@ __device__ void mg_pcg_body(const MgArgs& a, int cta, int nctas) {
         }
         mg_reduce1(pq_l, sm, s0);
         if (threadIdx.x == 0) a.partA[nb + cta] = s0;
-        if (!sync_all<CL>(a.bar, target, a.err, &s_ok)) return;
+        if (!sync_all<CL>(a.bar, target, a.err, &s_ok, a.spin_limit)) return;
         const double pq = mg_sum_partials(a.partA + nb, nb, sm);
         fresh = false;
         k++;
@@ -1026,6 +1028,7 @@ void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long 
     a.partB = w.part.get() + 2 * nb;
     a.stats = w.stats.get();
     a.bar = g.bar.get();
+    a.spin_limit = w.spin_limit;
     a.err = status;
     a.tol = tol;
     a.max_iter = max_iter;
@@ -1151,6 +1154,7 @@ MgBatch* mg_batch_build(const std::vector<MgBatchInput>& in, double tol, long lo
             a.partB = w->part.get() + 2 * kMgClusterCtas;
             a.stats = B->stats.get() + 4 * k;
             a.bar = nullptr;
+            a.spin_limit = kSpinLimit;
             a.err = nullptr;
             a.tol = tol;
             a.max_iter = iter_factor * (long long)x.n;

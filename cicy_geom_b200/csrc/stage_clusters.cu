@@ -535,6 +535,7 @@ void upload_network(Ctx& c, const cicy_network& n) {
     CICY_CUDA(cudaStreamSynchronize(s));
     c.stage = 1;
     c.have_backbone = false;
+    c.have_volumes = false;
 }
 
 // ---------------------------------------------------------------------------
@@ -802,6 +803,7 @@ void run_clusters(Ctx& c, const cicy_params& p) {
     check_status(c, "Determine_clusters_and_percolation");
     c.stage = 3;
     c.have_backbone = false;
+    c.have_volumes = false;
 }
 
 }  // namespace cicy

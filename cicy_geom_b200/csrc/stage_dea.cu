@@ -117,6 +117,18 @@ __device__ __forceinline__ double cnt_resistance(int P1, int P2, double radius, 
     return rho * length / (kPI * radius * radius);
 }
 
+// CNT_volume_between_two_points (Backbone_Network.cpp:558-574): the same point-by-point
+// length, times PI r^2 as (length * PI * r) * r.
+__device__ __forceinline__ double cnt_volume(int P1, int P2, double radius, const double* __restrict__ x, const double* __restrict__ y,
+                                             const double* __restrict__ z) {
+    double length = 0;
+    for (int i = P1; i < P2; i++) {
+        double dx = x[i] - x[i + 1], dy = y[i] - y[i + 1], dz = z[i] - z[i + 1];
+        length = length + sqrt(dx * dx + dy * dy + dz * dz);
+    }
+    return length * kPI * radius * radius;
+}
+
 __global__ void k_cnt_edge_counts(int n, const int32_t* __restrict__ eb, const int32_t* __restrict__ ee,
                                   const int32_t* __restrict__ elem, const int32_t* __restrict__ lmm, int32_t* __restrict__ cnt) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -452,10 +464,16 @@ __global__ void k_current_max(int n, const int32_t* __restrict__ eb, const int32
     }
 }
 
+// Find_backbone_cnts (Backbone_Network.cpp:313-345): the kept element run of every CNT of
+// the cluster, and Calculate_cnt_volumes' (:412-556) volumes of its parts: vol3[3i] the dead
+// part before the run (the whole CNT when nothing is kept), vol3[3i+1] the run, vol3[3i+2]
+// the dead part after it; kind[i] = 0 nothing kept, 1 kept to the end, 2 dead part after.
 __global__ void k_backbone_cnts(int n, const int32_t* __restrict__ members, const int32_t* __restrict__ eb, const int32_t* __restrict__ ee,
                                 const int32_t* __restrict__ elem, const int32_t* __restrict__ lmm, const double* __restrict__ volt,
                                 const unsigned long long* __restrict__ imax_bits, int trim, int32_t* __restrict__ cur_lo,
-                                int32_t* __restrict__ cur_hi, int32_t* __restrict__ alive) {
+                                int32_t* __restrict__ cur_hi, int32_t* __restrict__ alive, const double* __restrict__ radii,
+                                const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
+                                double* __restrict__ vol3, int32_t* __restrict__ kind) {
     const double i_max = fmax(__longlong_as_double((long long)*imax_bits), kZero);
     const double zero_current = i_max * 1e-9;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -471,6 +489,26 @@ __global__ void k_backbone_cnts(int n, const int32_t* __restrict__ members, cons
             }
         }
         int c = members[i];
+        {
+            const double r = radii[c];
+            const int Ps = elem[b], Pe = elem[e - 1];
+            if (idx1 == -1) {
+                vol3[3 * i] = cnt_volume(Ps, Pe, r, x, y, z);
+                kind[i] = 0;
+            } else {
+                const int P1 = elem[b + idx1];
+                vol3[3 * i] = cnt_volume(Ps, P1, r, x, y, z);
+                if (idx2 == -1) {
+                    vol3[3 * i + 1] = cnt_volume(P1, Pe, r, x, y, z);
+                    kind[i] = 1;
+                } else {
+                    const int P2 = elem[b + idx2];
+                    vol3[3 * i + 1] = cnt_volume(P1, P2, r, x, y, z);
+                    vol3[3 * i + 2] = cnt_volume(P2, Pe, r, x, y, z);
+                    kind[i] = 2;
+                }
+            }
+        }
         if (!trim) {
             alive[i] = 1;
             continue;
@@ -485,6 +523,69 @@ __global__ void k_backbone_cnts(int n, const int32_t* __restrict__ members, cons
             alive[i] = 1;
         }
     }
+}
+
+// Volume members of Backbone_Network (acc: volumes_cnt[8], dead_branches[7], then the
+// fractions step's total_volumes[8] and fractions[8]).
+constexpr int kVolCnt = 0, kVolDead = 8, kVolTotal = 15, kVolFrac = 23, kVolWords = 31;
+
+// The cluster's volumes added to its family in upstream's order: CNTs last to first
+// (Backbone_Network.cpp:325), per CNT the dead part(s) and then the kept run (:442-543).
+// One thread: the FP64 sums must be the same sequence of additions.
+__global__ void k_volume_sum(int n, int family, const double* __restrict__ vol3, const int32_t* __restrict__ kind, double* acc) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    double dead = acc[kVolDead + family], bb = acc[kVolCnt + family];
+    for (int i = n - 1; i >= 0; i--) {
+        dead = dead + vol3[3 * i];
+        if (kind[i] == 2) dead = dead + vol3[3 * i + 2];
+        if (kind[i] >= 1) bb = bb + vol3[3 * i + 1];
+    }
+    acc[kVolDead + family] = dead;
+    acc[kVolCnt + family] = bb;
+}
+
+// Sort keys of HoKo->isolated_cnt's order (Hoshen_Kopelman.cpp:2331-2363, 2527-2539): CNTs
+// without a label first, then the non-percolated clusters by label, each in cnts_inside
+// order; CNTs of percolated clusters sort last (group n_labels + 1).
+__global__ void k_isolated_keys(int n_inside, int n_labels, const int32_t* __restrict__ inside, const int32_t* __restrict__ labels,
+                                const int32_t* __restrict__ perc_bits, uint64_t* __restrict__ key, uint32_t* __restrict__ val) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n_inside; p += gridDim.x * blockDim.x) {
+        const int c = inside[p];
+        const int L = labels[c];
+        const long long g = L < 0 ? 0 : (perc_bits[L] != 0 ? n_labels + 1 : L + 1);
+        key[p] = (uint64_t)(g * n_inside + p);
+        val[p] = (uint32_t)c;
+    }
+}
+
+// Calculate_percolated_families_fractions with Calculate_volume_of_non_percolated_cnts
+// (Electrical_analysis.cpp:678-786) for CNTs: the whole-CNT volumes of the isolated list in
+// order, volumes_cnt[7] = dead branches + that, then total volumes and fractions (no GNPs:
+// their volumes are 0).  One thread, upstream's sequence of additions.
+__global__ void k_family_fractions(int n_inside, int n_labels, const uint64_t* __restrict__ key, const uint32_t* __restrict__ cnt,
+                                   const int32_t* __restrict__ cstart, const int32_t* __restrict__ clen, const double* __restrict__ radii,
+                                   const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z, double* acc) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    double total_dead = 0, total_dead_gnps = 0;
+    for (int i = 0; i < 7; i++) {
+        total_dead = total_dead + acc[kVolDead + i];
+        total_dead_gnps = total_dead_gnps + 0.0;
+    }
+    const uint64_t end = (uint64_t)(n_labels + 1) * (uint64_t)n_inside;
+    double np_cnts = 0;
+    for (int p = 0; p < n_inside && key[p] < end; p++) {
+        const int c = (int)cnt[p];
+        const int P1 = cstart[c], P2 = cstart[c] + clen[c] - 1;
+        np_cnts = np_cnts + cnt_volume(P1, P2, radii[c], x, y, z);
+    }
+    acc[kVolCnt + 7] = total_dead + np_cnts;
+    double tv = 0;
+    for (int i = 0; i < 8; i++) {
+        acc[kVolTotal + i] = 0.0 + acc[kVolCnt + i] + 0.0;
+        tv = tv + acc[kVolCnt + i] + 0.0;
+    }
+    for (int i = 0; i < 8; i++) acc[kVolFrac + i] = acc[kVolTotal + i] / tv;
+    (void)total_dead_gnps;
 }
 
 // Remove_junctions_with_dead_particles_cnts (Backbone_Network.cpp:950-992).
@@ -893,6 +994,8 @@ void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out) {
     c.alive_scan.ensure(std::max(std::max(n_clu_idx, n_cj_idx), 1) + 1);
     c.tmp_list.ensure(std::max(std::max(n_clu_idx, n_cj_idx), 1) + 1);
     c.cur_out.ensure(4);
+    c.vol_acc.ensure(kVolWords);
+    CICY_CUDA(cudaMemsetAsync(c.vol_acc.get(), 0, sizeof(double) * kVolWords, s));
     const int scope = p.simulation_scope;
     for (int k = 0; k < c.n_perc && scope < 2; k++) {
         int32_t* members = c.bbclu_idx.get() + c.h_clu_ptr[k];
@@ -911,9 +1014,13 @@ void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out) {
         CICY_CUDA(cudaMemsetAsync(c.imax.get(), 0, sizeof(unsigned long long), s));
         k_current_max<<<grid_for(NM + NJ), 256, 0, s>>>(NM, eb.get(), ee.get(), c.elem_idx.get(), c.lmm.get(), su->volt.get(), NJ, jl,
                                                       c.j_p1.get(), c.j_p2.get(), c.imax.get());
+        c.vol3.ensure(3 * (size_t)std::max(NM, 1));
+        c.vol_kind.ensure(std::max(NM, 1));
         k_backbone_cnts<<<grid_for(NM), 256, 0, s>>>(NM, members, eb.get(), ee.get(), c.elem_idx.get(), c.lmm.get(), su->volt.get(),
-                                                   c.imax.get(), scope == 0 ? 1 : 0, c.bb_lo.get(), c.bb_hi.get(), c.alive.get());
-        c.launches += 2;
+                                                   c.imax.get(), scope == 0 ? 1 : 0, c.bb_lo.get(), c.bb_hi.get(), c.alive.get(),
+                                                   c.radii.get(), c.x.get(), c.y.get(), c.z.get(), c.vol3.get(), c.vol_kind.get());
+        k_volume_sum<<<1, 32, 0, s>>>(NM, c.h_family[k], c.vol3.get(), c.vol_kind.get(), c.vol_acc.get());
+        c.launches += 3;
         if (scope == 0) {
             exclusive_scan_i32(c.alive.get(), c.alive_scan.get(), NM, c.i32_scalar.get(), c.scan_tmp32, s, c.launches);
             k_compact_i32<<<grid_for(NM), 256, 0, s>>>(NM, members, c.alive.get(), c.alive_scan.get(), c.tmp_list.get());
@@ -988,6 +1095,19 @@ void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out) {
     c.bb_clu_len = clu_len;
     c.bb_cj_len = cj_len;
     c.have_backbone = true;
+    // Calculate_percolated_families_fractions (Electrical_analysis.cpp:114-119, 678-756)
+    if (scope < 2 && c.n_inside > 0) {
+        c.vol_key.ensure(c.n_inside);
+        c.vol_cnt.ensure(c.n_inside);
+        k_isolated_keys<<<grid_for(c.n_inside), 256, 0, s>>>(c.n_inside, c.n_labels, c.inside.get(), c.labels.get(), c.perc_bits.get(),
+                                                             c.vol_key.get(), c.vol_cnt.get());
+        radix_sort_pairs(c.vol_key.get(), c.vol_cnt.get(), c.n_inside, bits_for((uint64_t)(c.n_labels + 2) * (uint64_t)c.n_inside), c.rs,
+                         s, c.launches);
+        k_family_fractions<<<1, 32, 0, s>>>(c.n_inside, c.n_labels, c.vol_key.get(), c.vol_cnt.get(), c.cstart.get(), c.clen.get(),
+                                            c.radii.get(), c.x.get(), c.y.get(), c.z.get(), c.vol_acc.get());
+        c.launches += 2;
+        c.have_volumes = true;
+    }
     // Calculate_resistances_and_resistivities (Electrical_analysis.cpp:873-987)
     if (out) {
         const cicy_cuboid& w = c.window;

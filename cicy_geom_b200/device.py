@@ -77,6 +77,10 @@ class Context:
 
             self.set_learned_params(default_params())
 
+    def set_spin_limit(self, polls: int = 0):
+        """Polls a grid-barrier wait makes before the solve gives up with CICY_E_TIMEOUT (0: the default)."""
+        self._check(lib().cicy_ctx_set_spin_limit(self._h, int(polls)), "cicy_ctx_set_spin_limit")
+
     def set_learned_params(self, params: np.ndarray):
         """Parameters of the learned preconditioner (flat float32 vector, cicy_gnn_param_count entries)."""
         p = np.ascontiguousarray(params, dtype=np.float32)
@@ -204,6 +208,13 @@ class Context:
                                              _p(n2, C.c_int32), _p(d, C.c_double)), "get_junctions")
         k = n.value
         return p1[:k], n1[:k], p2[:k], n2[:k], d[:k]
+
+    def volumes(self) -> dict:
+        """Backbone_Network's volume members (cicy_get_volumes): volumes_cnt[8], dead_branches[7],
+        total_volumes[8], fractions[8]."""
+        v, d, t, f = np.zeros(8), np.zeros(7), np.zeros(8), np.zeros(8)
+        self._check(lib().cicy_get_volumes(self._h, *[a.ctypes.data_as(_abi.f64p) for a in (v, d, t, f)]), "cicy_get_volumes")
+        return {"volumes_cnt": v, "dead_branches": d, "total_volumes": t, "fractions": f}
 
     def elements(self, which: int = 0):
         nc, ni = C.c_int64(), C.c_int64()

@@ -162,6 +162,13 @@ cicy_status cicy_ctx_destroy(cicy_ctx* ctx);
 cicy_status cicy_ctx_set_stream(cicy_ctx* ctx, void* cuda_stream);
 void* cicy_ctx_stream(cicy_ctx* ctx);
 cicy_status cicy_ctx_set_solver(cicy_ctx* ctx, const cicy_solver_opts* opts);
+/* Polls a grid-barrier wait of this context's persistent solvers makes before it
+ * gives up: the kernel then records a device status, every CTA leaves at its next
+ * barrier, and the call returns CICY_E_TIMEOUT with the context still usable.
+ * polls <= 0 restores the default (2^28, far above any real wait).  Stands in for
+ * upstream's only bound on a solve, the CG's iteration cap
+ * (Direct_Electrifying.cpp:1559, 1640-1641), for waits upstream does not have. */
+cicy_status cicy_ctx_set_spin_limit(cicy_ctx* ctx, int64_t polls);
 const char* cicy_last_error(const cicy_ctx* ctx);
 /* Number of kernels this context has launched so far. */
 int64_t cicy_ctx_kernel_launches(const cicy_ctx* ctx);
@@ -201,6 +208,14 @@ cicy_status cicy_get_elements(cicy_ctx* ctx, int32_t which, int64_t* n_cnts, int
  * which = 0 after percolation, 1 after backbone extraction. */
 cicy_status cicy_get_clusters(cicy_ctx* ctx, int32_t which, int32_t* n_clusters, int64_t* n_idx, int64_t* ptr, int32_t* idx,
                               int32_t* family, int64_t* n_junc_idx, int64_t* junc_ptr, int32_t* junc_idx);
+/* Backbone_Network's volume members after Perform_analysis_on_clusters
+ * (Backbone_Network.h:26-34, filled by Calculate_cnt_volumes, Backbone_Network.cpp:412-574,
+ * and Calculate_percolated_families_fractions, Electrical_analysis.cpp:678-786):
+ * volumes_cnt[8] (backbone volume per family 0-6; [7] dead branches plus isolated and
+ * non-percolated CNTs), dead_branches[7] (per family), and the fractions step's
+ * total_volumes[8] and fractions[8] (volumes.txt, fractions.txt).  CNT networks: the GNP
+ * members are 0.  Any pointer may be NULL.  After cicy_electrical_analysis. */
+cicy_status cicy_get_volumes(cicy_ctx* ctx, double* volumes_cnt, double* dead_branches, double* total_volumes, double* fractions);
 /* One DEA system and its solution, as upstream builds it in SSS form
  * (strict-lower CSR of the free block, diagonal, right-hand side after the BC
  * elimination, initial guess, prescribed voltages, voltages of all nodes).
@@ -618,11 +633,17 @@ const char* cicy_host_last_error(void);
  * holds until exit; systems above 131072 rows are rejected with
  * CICY_E_CAPACITY.  Runs on the current device and `stream` (a cudaStream_t, or
  * NULL); returns once the solve is complete.  The first call on a device looks
- * up the array's device address (cudaGetSymbolAddress), so make that first call
- * before any stream capture.  Every call shares the one array and the call
- * resets the words that must start at zero, so calls that overlap on the GPU
- * (other streams, other host threads) race: serialize them.  Stops when
- * |r| <= tol |r0|; `rel_residual` gets |r| / |r0|.  Errors: message via
+ * up the array's device address (cudaGetSymbolAddress) and keeps it for the
+ * life of the process, so make that first call before any stream capture; after
+ * a cudaDeviceReset the kept address is stale (do not call it again on that
+ * device).  Every call shares the one array and the call resets the words that
+ * must start at zero, so calls that overlap on the GPU (other streams, other
+ * host threads) race: serialize them.  The CSR is checked on the device first
+ * (row_ptr 0 .. nnz non-decreasing, columns in [0, n)); a malformed system
+ * returns CICY_E_INPUT before any kernel uses its indices.  Stops when
+ * |r| <= tol |r0|; `rel_residual` gets |r| / |r0|.  When `max_iter` runs out
+ * first the call still returns CICY_OK, as upstream's CG does, with
+ * `iterations` = max_iter and `rel_residual` > tol.  Errors: message via
  * cicy_host_last_error(). */
 cicy_status cicy_jacobi_pcg_static(int32_t n, int32_t nnz, const int32_t* row_ptr, const int32_t* col_ind, const double* values,
                                    const double* b, double* x, double tol, int64_t max_iter, void* stream, int64_t* iterations,

@@ -185,9 +185,24 @@ def compress_junctions(net: dict, p: dict, point_contacts: dict, ce: dict):
     return junctions, out
 
 
-def percolation(net: dict, labels, n_labels, junctions):
+def isolated_lists(net: dict, labels, n_labels, clusters_all_labels=None):
+    """HoKo->isolated_cnt (Hoshen_Kopelman.cpp:2331-2363, 2527-2539): the CNTs with label -1 in
+    cnts_inside order, then every non-percolated cluster in label order (its CNTs in cnts_inside order)."""
+    tmp = [[] for _ in range(n_labels)]
+    iso0 = []
+    for c in net["cnts_inside"]:
+        if labels[c] != -1:
+            tmp[labels[c]].append(int(c))
+        else:
+            iso0.append(int(c))
+    perc = set(clusters_all_labels or ())
+    return [iso0] + [tmp[L] for L in range(n_labels) if L not in perc]
+
+
+def percolation(net: dict, labels, n_labels, junctions, with_isolated: bool = False):
     """Make_particle_clusters, Find_percolated_clusters, Family_map, Group_junctions
-    (Hoshen_Kopelman.cpp:2331-2710).  Returns clusters (CNT lists), families, cluster junction lists."""
+    (Hoshen_Kopelman.cpp:2331-2710).  Returns clusters (CNT lists), families, cluster junction lists
+    (and, with_isolated, HoKo->isolated_cnt)."""
     bptr, bidx = net["boundary_cnt_ptr"], net["boundary_cnt_idx"]
     face = lambda f: [int(c) for c in bidx[bptr[f]:bptr[f + 1]]]
     tmp = [[] for _ in range(n_labels)]
@@ -213,6 +228,8 @@ def percolation(net: dict, labels, n_labels, junctions):
         assert labels[N1] == labels[N2]
         if labels[N1] in perc:
             cj[perc[labels[N1]]].append(i)
+    if with_isolated:
+        return clusters, families, cj, isolated_lists(net, labels, n_labels, perc)
     return clusters, families, cj
 
 
@@ -383,9 +400,27 @@ def solve_direct(S):
     return np.concatenate([S["vef"], x])
 
 
-def backbone(cluster, cj, elements, junctions, lmm, volt, trim=True):
-    """Find_zero_current, Find_backbone_cnts, Calculate_cnt_volumes (element part),
-    Remove_junctions_with_dead_particles_cnts (Backbone_Network.cpp:64-409, 412-556, 950-992)."""
+def cnt_volume(net, P1, P2, radius):
+    """CNT_volume_between_two_points (Backbone_Network.cpp:558-574): the polyline length from
+    P1 to P2 times PI r^2, as (length * PI * r) * r."""
+    X, Y, Z = net["x"], net["y"], net["z"]
+    length = 0.0
+    for i in range(P1, P2):
+        dx, dy, dz = X[i] - X[i + 1], Y[i] - Y[i + 1], Z[i] - Z[i + 1]
+        length = length + math.sqrt(dx * dx + dy * dy + dz * dz)
+    return length * PI * radius * radius
+
+
+def new_volumes() -> dict:
+    """Backbone_Network's volume members as its constructor sets them (Backbone_Network.h:37-48)."""
+    return {"volumes_cnt": [0.0] * 8, "volumes_gnp": [0.0] * 8, "dead_branches": [0.0] * 7, "dead_gnps": [0.0] * 7}
+
+
+def backbone(cluster, cj, elements, junctions, lmm, volt, trim=True, net=None, family=None, vols=None):
+    """Find_zero_current, Find_backbone_cnts, Calculate_cnt_volumes,
+    Remove_junctions_with_dead_particles_cnts (Backbone_Network.cpp:64-409, 412-556, 950-992).
+    With `vols` (see new_volumes) the backbone and dead-branch volumes of the cluster's CNTs are
+    added to its `family`, CNTs visited last to first as upstream does (Backbone_Network.cpp:325)."""
     imax = ZERO
     cur = []
     for c in cluster:
@@ -397,8 +432,8 @@ def backbone(cluster, cj, elements, junctions, lmm, volt, trim=True):
         P1, _, P2, _, _ = junctions[j]
         imax = max(imax, abs(volt[lmm[P1]] - volt[lmm[P2]]))
     zero = imax * 1e-9
-    new_cluster = []
-    for c, I in zip(cluster, cur):
+    idx = []
+    for I in cur:
         i1 = i2 = -1
         for j, v in enumerate(I):
             if v - zero > ZERO:
@@ -407,6 +442,23 @@ def backbone(cluster, cj, elements, junctions, lmm, volt, trim=True):
             elif i1 != -1 and i2 == -1:
                 i2 = j
                 break
+        idx.append((i1, i2))
+    if vols is not None:
+        R = net["radii"]
+        for c, (i1, i2) in reversed(list(zip(cluster, idx))):
+            e = elements[c]
+            if i1 == -1:
+                vols["dead_branches"][family] = vols["dead_branches"][family] + cnt_volume(net, e[0], e[-1], R[c])
+                continue
+            vols["dead_branches"][family] = vols["dead_branches"][family] + cnt_volume(net, e[0], e[i1], R[c])
+            if i2 == -1:
+                vb = cnt_volume(net, e[i1], e[-1], R[c])
+            else:
+                vb = cnt_volume(net, e[i1], e[i2], R[c])
+                vols["dead_branches"][family] = vols["dead_branches"][family] + cnt_volume(net, e[i2], e[-1], R[c])
+            vols["volumes_cnt"][family] = vols["volumes_cnt"][family] + vb
+    new_cluster = []
+    for c, (i1, i2) in zip(cluster, idx):
         if not trim:
             new_cluster.append(c)
             continue
@@ -422,6 +474,32 @@ def backbone(cluster, cj, elements, junctions, lmm, volt, trim=True):
         if elements.get(N1) and elements.get(N2) and P1 in elements[N1] and P2 in elements[N2]:
             new_cj.append(j)
     return new_cluster, new_cj, zero
+
+
+def family_fractions(net, isolated, vols):
+    """Calculate_percolated_families_fractions with Calculate_volume_of_non_percolated_cnts
+    (Electrical_analysis.cpp:678-786) for a CNT network: volumes_cnt[7] becomes the dead-branch
+    plus non-percolated volume; returns total_volumes and fractions (8 each)."""
+    total_dead, total_dead_gnps = 0.0, 0.0
+    for i in range(7):
+        total_dead = total_dead + vols["dead_branches"][i]
+        total_dead_gnps = total_dead_gnps + vols["dead_gnps"][i]
+    sp, si = net["structure_ptr"], net["structure_idx"]
+    np_cnts = 0.0
+    for lst in isolated:
+        for c in lst:
+            np_cnts = np_cnts + cnt_volume(net, int(si[sp[c]]), int(si[sp[c + 1] - 1]), net["radii"][c])
+    vols["volumes_cnt"][7] = total_dead + np_cnts
+    vols["volumes_gnp"][7] = total_dead_gnps + 0.0
+    vc, vg = vols["volumes_cnt"], vols["volumes_gnp"]
+    total = [0.0] * 8
+    tv = 0.0
+    for i in range(8):
+        total[i] = total[i] + vc[i] + vg[i]
+        tv = tv + vc[i] + vg[i]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        fr = [float(np.float64(total[i]) / np.float64(tv)) for i in range(8)]
+    return total, fr
 
 
 def boundary_current(net, p, bcnt, elements, lmm, volt):
@@ -447,7 +525,8 @@ def network_to_conductance(net: dict, p: dict, solver: str = "cg") -> dict:
     n, l, regions = contact_grid(net, p)
     labels, n_labels, pc, ce = label_cnts(net, p, regions)
     junctions, elements = compress_junctions(net, p, pc, ce)
-    clusters, families, cj = percolation(net, labels, n_labels, junctions)
+    clusters, families, cj, isolated = percolation(net, labels, n_labels, junctions, with_isolated=True)
+    vols = new_volumes()
     out = {"regions": regions, "labels": labels, "n_labels": n_labels, "point_contacts": pc, "junctions": junctions,
            "elements": {k: list(v) for k, v in elements.items()}, "clusters": [list(c) for c in clusters], "families": families,
            "cluster_junctions": [list(c) for c in cj], "systems": [], "backbone": []}
@@ -461,7 +540,7 @@ def network_to_conductance(net: dict, p: dict, solver: str = "cg") -> dict:
         volt, it = solve_cg(S, p["tolerance"]) if solver == "cg" else (solve_direct(S), 0)
         S["voltages"], S["iterations"] = volt, it
         out["systems"].append(("unit", k, S))
-        cl2, cj2, zero = backbone(cl, cj[k], elems, junctions, S["lmm"], volt, trim=p["scope"] == 0)
+        cl2, cj2, zero = backbone(cl, cj[k], elems, junctions, S["lmm"], volt, trim=p["scope"] == 0, net=net, family=fam, vols=vols)
         clusters[k], cj[k] = cl2, cj2
         out["backbone"].append({"cluster": list(cl2), "junctions": list(cj2), "zero_current": zero})
         if p["scope"] != 0:
@@ -494,4 +573,8 @@ def network_to_conductance(net: dict, p: dict, solver: str = "cg") -> dict:
             res.append(1 / s)
     out["elements_backbone"] = elems
     out["resistances"] = res
+    if p["scope"] < 2:
+        out["volumes_before_fractions"] = {k: list(v) for k, v in vols.items()}
+        out["total_volumes"], out["fractions"] = family_fractions(net, isolated, vols)
+        out["volumes"] = vols
     return out

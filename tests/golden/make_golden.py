@@ -100,9 +100,7 @@ def host_network_from_polylines(lines) -> HostNetwork:
 
 
 def capture(name, cfg: NetworkConfig, raw: HostNetwork, full_sd: bool, store_inputs: bool):
-    work = os.path.join(ROOT, "_scratch")
-    os.makedirs(work, exist_ok=True)
-    with tempfile.TemporaryDirectory(dir=work) as d:
+    with tempfile.TemporaryDirectory(prefix="cicy_golden_") as d:
         write_read_network_files(d, raw, cfg)
         dump = os.path.join(d, "dump.bin")
         subprocess.run([REF, "dump", d, dump], check=True, capture_output=True)
@@ -122,7 +120,8 @@ def capture(name, cfg: NetworkConfig, raw: HostNetwork, full_sd: bool, store_inp
             out["in_" + k] = v
     for k in ("pc_Pa", "pc_CNTb", "pc_Pb", "pc_dist", "labels_cnt", "n_labels", "junc_P1", "junc_N1", "junc_P2", "junc_N2",
               "junc_dist", "elements_ptr", "elements_idx", "clusters_ptr", "clusters_idx", "family", "cluster_junc_ptr",
-              "cluster_junc_idx", "isolated_ptr", "isolated_idx", "bn_volumes"):
+              "cluster_junc_idx", "isolated_ptr", "isolated_idx", "bn_volumes", "bn_volumes_cnt", "bn_volumes_gnp",
+              "bn_dead_branches", "bn_dead_gnps"):
         out[k] = D[k]
     for k in list(D):
         if k.startswith("c") and k[1].isdigit() and not k.endswith("times"):

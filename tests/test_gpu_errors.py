@@ -53,3 +53,28 @@ def test_context_is_reusable_after_an_error(cuda_ok):
     r1 = ctx.network_to_conductance(p)
     r2 = ctx.network_to_conductance(p)
     assert list(r1.resistances) == list(r2.resistances)  # deterministic across runs
+
+
+@pytest.mark.parametrize("precond", [0, 3])
+def test_bounded_wait_gives_up_and_the_context_stays_usable(cuda_ok, precond):
+    """A grid-barrier wait limited to one poll gives up: the solve returns
+    CICY_E_TIMEOUT (every CTA leaves at its next barrier; nothing hangs or faults),
+    and the same context then solves the network normally.  Grid-wide kernels only
+    (cluster=False): Jacobi-PCG (k_pcg) and the multigrid PCG (k_mg_pcg)."""
+    from conftest import golden_network
+
+    cfg, net, z = golden_network("c1p_1200_s1")
+    p = cfg.params()
+    ref = Context(0)
+    ref.set_solver(preconditioner=precond, cluster=False)
+    ref.upload(net)
+    r0 = list(ref.network_to_conductance(p).resistances)
+    ctx = Context(0)
+    ctx.set_solver(preconditioner=precond, cluster=False)
+    ctx.upload(net)
+    ctx.set_spin_limit(1)
+    with pytest.raises(_abi.CicyError) as e:
+        ctx.network_to_conductance(p)
+    assert e.value.status == 4 and "bounded device wait" in str(e.value)  # CICY_E_TIMEOUT
+    ctx.set_spin_limit(0)
+    assert list(ctx.network_to_conductance(p).resistances) == r0

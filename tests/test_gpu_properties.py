@@ -12,7 +12,7 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture(scope="module")
 def big(cuda_ok):
-    cfg = NetworkConfig(side=6.0, n_cnts=25000, seed=2_000_000, tolerance=1e-8, tolerance_unit=1e-10)
+    cfg = NetworkConfig(side=6.0, n_cnts=25000, seed=2_000_000, tolerance=1e-8, tolerance_unit=1e-12)
     net = generate_cnt_network(cfg).extract_window(cfg)
     ctx = Context(0)
     ctx.upload(net)

@@ -125,3 +125,16 @@ def test_direct_solve_agrees_with_cg_within_tolerance(runs):
         m = np.concatenate([np.ones(S["reserved"], bool), O.grounded_mask(S)])
         rel = np.max(np.abs(vd[m] - S["voltages"][m])) / np.max(np.abs(vd[m]))
         assert rel < 1e-5
+
+
+@pytest.mark.parametrize("name", FAST)
+def test_backbone_volumes_and_family_fractions(runs, name):
+    """Calculate_cnt_volumes over every percolated cluster and Calculate_percolated_families_fractions:
+    the oracle's volume members equal upstream's bit for bit."""
+    cfg, a, z, out = runs(name)
+    before = out["volumes_before_fractions"]
+    assert before["volumes_cnt"][:3] + before["dead_branches"][:3] == list(z["bn_volumes"])
+    v = out["volumes"]
+    assert v["volumes_cnt"] == list(z["bn_volumes_cnt"])
+    assert v["dead_branches"] == list(z["bn_dead_branches"])
+    assert v["volumes_gnp"] == list(z["bn_volumes_gnp"]) and v["dead_gnps"] == list(z["bn_dead_gnps"])

@@ -78,3 +78,53 @@ def test_static_solve_rejects_systems_above_its_limit(cuda_ok):
                                            C.c_void_p(1), 1e-10, 10, None, C.byref(it), C.byref(rel))
     assert st == 2  # CICY_E_CAPACITY, rejected before any device work
     assert b"static scratch limit" in _abi.lib().cicy_host_last_error()
+
+
+def _device_csr(A):
+    import torch
+
+    dev = torch.device("cuda:0")
+    return (torch.tensor(A.indptr.astype(np.int32), device=dev), torch.tensor(A.indices.astype(np.int32), device=dev),
+            torch.tensor(A.data, dtype=torch.float64, device=dev))
+
+
+def _laplacian_1d(n):
+    import scipy.sparse as sp
+
+    A = sp.diags([-np.ones(n - 1), 2.0 * np.ones(n), -np.ones(n - 1)], [-1, 0, 1], format="csr")
+    A.sort_indices()
+    return A
+
+
+def test_static_solve_rejects_a_malformed_system_before_using_its_indices(cuda_ok):
+    import torch
+
+    A = _laplacian_1d(1000)
+    rp, ci, va = _device_csr(A)
+    ci[17] = A.shape[0] + 5  # a column outside [0, n)
+    b = torch.ones(A.shape[0], dtype=torch.float64, device="cuda:0")
+    x = torch.zeros_like(b)
+    it, rel = C.c_int64(), C.c_double()
+    st = _abi.lib().cicy_jacobi_pcg_static(A.shape[0], A.nnz, rp.data_ptr(), ci.data_ptr(), va.data_ptr(), b.data_ptr(), x.data_ptr(),
+                                           1e-10, 1000, None, C.byref(it), C.byref(rel))
+    assert st == 1  # CICY_E_INPUT
+    assert b"column index" in _abi.lib().cicy_host_last_error()
+    # the library stays usable: the same call on the well-formed system solves it
+    rp, ci, va = _device_csr(A)
+    st = _abi.lib().cicy_jacobi_pcg_static(A.shape[0], A.nnz, rp.data_ptr(), ci.data_ptr(), va.data_ptr(), b.data_ptr(), x.data_ptr(),
+                                           1e-10, 100000, None, C.byref(it), C.byref(rel))
+    assert st == 0 and rel.value <= 1e-10
+
+
+def test_static_solve_out_of_iterations_returns_ok_with_the_residual_above_tol(cuda_ok):
+    import torch
+
+    A = _laplacian_1d(4000)
+    rp, ci, va = _device_csr(A)
+    b = torch.ones(A.shape[0], dtype=torch.float64, device="cuda:0")
+    x = torch.zeros_like(b)
+    it, rel = C.c_int64(), C.c_double()
+    st = _abi.lib().cicy_jacobi_pcg_static(A.shape[0], A.nnz, rp.data_ptr(), ci.data_ptr(), va.data_ptr(), b.data_ptr(), x.data_ptr(),
+                                           1e-10, 1, None, C.byref(it), C.byref(rel))
+    assert st == 0
+    assert it.value == 1 and rel.value > 1e-10
