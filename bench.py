@@ -534,10 +534,11 @@ def batched_monte_carlo(count, device, reps=3):
     bs = BT.BatchSolver(systems, tol=TOL, device=device, learned=True)
     ns = len(systems)
 
-    def measure(tune=False, runs=reps):
-        shape = bs.autotune() if tune else None
-        t = min(bs.solve() for _ in range(runs))
-        it, rel, fl = bs.results()
+    def measure(tune=False, runs=reps, solver=None):
+        b = solver or bs
+        shape = b.autotune() if tune else None
+        t = min(b.solve() for _ in range(runs))
+        it, rel, fl = b.results()
         return {"seconds": t, "systems_per_s": ns / t, "launch": shape, "iterations_total": int(it.sum()), "iterations_max": int(it.max()),
                 "converged": int((fl == 1).sum()), "max_rel_residual": float(rel.max())}
 
@@ -546,6 +547,17 @@ def batched_monte_carlo(count, device, reps=3):
     out["learned_mixed"] = measure(tune=True)
     bs.set_solver("learned", 0)
     out["learned_fp64"] = measure(tune=True)
+    # the same preconditioner without training (every coupling weight 0.8, the initial
+    # parameters) and without the learned term (chain blocks only)
+    from cicy_geom_b200.learned import init_params
+
+    bu = BT.BatchSolver(systems, tol=TOL, device=device, learned=init_params(0))
+    bu.set_solver("learned", 0)
+    out["untrained_constant_fp64"] = measure(tune=True, solver=bu)
+    untrained_gnn_seconds = bu.gnn_seconds
+    bu.close()
+    bs.set_solver("chain", 0)
+    out["chain_fp64"] = measure(tune=True)
     # the plain GPU Jacobi-CG baseline, one CTA per system and with the largest systems on clusters:
     # the faster is the baseline
     bs.set_solver("jacobi", 0)
@@ -565,13 +577,17 @@ def batched_monte_carlo(count, device, reps=3):
     jac = out["jacobi_fp64"]["seconds"]
     # preconditioner set-up outside the timed launch: the graph network's forward (learned)
     # and the hierarchies (multigrid); the chain factors are built inside the launch
-    setup_outside = {"learned_mixed": bs.gnn_seconds, "learned_fp64": bs.gnn_seconds, "multigrid": setup}
-    for k in ("learned_mixed", "learned_fp64", "multigrid"):
+    setup_outside = {"learned_mixed": bs.gnn_seconds, "learned_fp64": bs.gnn_seconds, "multigrid": setup,
+                     "untrained_constant_fp64": untrained_gnn_seconds, "chain_fp64": 0.0}
+    for k in ("learned_mixed", "learned_fp64", "multigrid", "untrained_constant_fp64", "chain_fp64"):
         out[k]["speedup_vs_jacobi"] = jac / out[k]["seconds"]
         t = out[k]["seconds"] + setup_outside[k]
         out[k]["setup_seconds_outside_launch"] = setup_outside[k]
         out[k]["systems_per_s_with_setup"] = ns / t
         out[k]["speedup_vs_jacobi_with_setup"] = jac / t
+    out["trained_gain_over_untrained"] = {
+        "iterations": out["untrained_constant_fp64"]["iterations_total"] / max(out["learned_fp64"]["iterations_total"], 1),
+        "seconds": out["untrained_constant_fp64"]["seconds"] / out["learned_fp64"]["seconds"]}
     seq = sum(s["seconds_ref"] for s in systems)
     n = [s["A"].shape[0] for s in systems]
     dev = info.pop("device_seconds", {})

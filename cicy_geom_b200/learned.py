@@ -176,18 +176,47 @@ def training_networks(count: int, seed0: int = 5_000_000, side=(2.0, 3.0), fract
     return nets
 
 
+def monte_carlo_training_systems(count: int, seed0: int = 5_000_000, device: int = 0, log=print):
+    """`count` real-resistor Laplacians from the Monte-Carlo sweep's generator (cube side
+    U[2,5] um, CNT volume fraction U[0.5%,3%]) on seeds seed0, seed0 + 1, ... -- disjoint
+    from the sweep's own seeds (3,000,000 + k), so the sweep evaluates on fresh networks.
+    Realisations that do not percolate give no system and are skipped."""
+    from .batch import monte_carlo_configs
+
+    out, k, batch = [], 0, 64
+    while len(out) < count:
+        cfgs = monte_carlo_configs(batch, seed0=seed0 + k)
+        for cfg in cfgs:
+            cfg.seed = seed0 + k
+            k += 1
+            from .network import generate_cnt_network
+
+            got = collect_systems([(cfg, generate_cnt_network(cfg).extract_window(cfg))], device=device)
+            out += got[: count - len(out)]
+            if len(out) >= count:
+                break
+        if log:
+            log(f"{k} realisations, {len(out)} systems")
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--networks", type=int, default=24)
     ap.add_argument("--steps", type=int, default=600)
     ap.add_argument("--lr", type=float, default=3e-3)
+    ap.add_argument("--monte-carlo", type=int, default=0,
+                    help="train on this many real-resistor Laplacians of the Monte-Carlo sweep's generator instead")
     ap.add_argument("--out", default=PARAMS_PATH)
     a = ap.parse_args()
-    systems = collect_systems(training_networks(a.networks))
+    if a.monte_carlo:
+        systems = monte_carlo_training_systems(a.monte_carlo)
+    else:
+        systems = collect_systems(training_networks(a.networks))
     print(f"{len(systems)} training systems, n = {min(s['n'] for s in systems)} .. {max(s['n'] for s in systems)}")
     P, hist = train(systems, steps=a.steps, lr=a.lr)
     P.astype(np.float32).tofile(a.out)
-    print("wrote", a.out)
+    print("wrote", a.out, f"loss first 100 steps {np.mean(hist[:100]):.4e}, last 100 steps {np.mean(hist[-100:]):.4e}")
 
 
 if __name__ == "__main__":

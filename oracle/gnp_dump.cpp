@@ -128,6 +128,90 @@ double number(const char* s) {
     return v;
 }
 
+// One DEA system of the staged electrical replay and what its assembly left behind.
+struct StagedSystem {
+    long int nodes = 0, reserved = 0;
+    std::vector<long int> row_ptr, col_ind;
+    std::vector<double> values, diagonal, b, x0, voltages;
+    std::map<long int, long int> lmm_cnts, lmm_gnps;
+    std::map<long int, double> cnt_rad;
+    std::vector<std::vector<long int> > tri;  // triangulation edges (v1, v2 pairs) of each GNP of the cluster
+};
+
+// Direct_Electrifying::Compute_voltage_field (Direct_Electrifying.cpp:11-113) replayed through its
+// public members, CNTs and GNPs, keeping the assembled system.
+int staged_field(Direct_Electrifying* D, int j, int R_flag, const cuboid& win, const Simu_para& sp, const Electric_para& ep,
+                 const Cutoff_dist& cf, Hoshen_Kopelman* HoKo, Cutoff_Wins* CW, const std::vector<Point_3D>& pts,
+                 const std::vector<double>& radii, const std::vector<std::vector<long int> >& sg, const std::vector<Point_3D>& pg,
+                 std::vector<GNP>& gnps, StagedSystem& S) {
+    const int reserved = D->Get_global_nodes(HoKo->family[j]);
+    if (reserved == -1) return 0;
+    long int global_nodes = reserved;
+    if (HoKo->clusters_cnt.size() && HoKo->clusters_cnt[j].size())
+        if (!D->LM_matrix_for_cnts(j, HoKo, CW, global_nodes)) return 0;
+    if (HoKo->clusters_gnp.size() && HoKo->clusters_gnp[j].size())
+        if (!D->LM_matrix_for_gnps(j, HoKo, CW, sg, global_nodes)) return 0;
+    std::vector<long int> col_ind, row_ptr;
+    std::vector<double> values, diagonal(global_nodes, 0), R(global_nodes - reserved, 0), VEF(reserved, 0.0);
+    if (!D->Fill_sparse_stiffness_matrix(R_flag, global_nodes, reserved, cf.van_der_Waals_dist, j, ep, HoKo, pts, radii, sg, pg, gnps,
+                                         col_ind, row_ptr, values, diagonal, R, VEF))
+        return 0;
+    S.b = R;
+    std::vector<double> V_guess(global_nodes - reserved, 0.0);
+    if (R_flag && reserved == 2) {
+        if (!D->Initial_guess_for_CG(j, reserved, HoKo->family[j], win, ep.applied_voltage, HoKo->clusters_cnt, HoKo->elements_cnt, pts,
+                                     HoKo->clusters_gnp, pg, R, V_guess))
+            return 0;
+        if (!D->Update_residual_vector(col_ind, row_ptr, values, diagonal, V_guess, R)) return 0;
+    }
+    S.x0 = V_guess;
+    if (!D->Solve_DEA_equations_CG_SSS(global_nodes, reserved, sp.tolerance, col_ind, row_ptr, values, diagonal, R, VEF, V_guess)) return 0;
+    S.nodes = global_nodes;
+    S.reserved = reserved;
+    S.row_ptr = row_ptr;
+    S.col_ind = col_ind;
+    S.values = values;
+    S.diagonal = diagonal;
+    S.voltages = D->voltages;
+    S.lmm_cnts = D->LMM_cnts;
+    S.lmm_gnps = D->LMM_gnps;
+    S.cnt_rad = D->points_cnt_rad;
+    S.tri.clear();
+    if (HoKo->clusters_gnp.size())
+        for (int g : HoKo->clusters_gnp[j]) {
+            std::vector<long int> e;
+            for (const auto& t : gnps[g].triangulation) { e.push_back(t.v1); e.push_back(t.v2); }
+            S.tri.push_back(e);
+        }
+    return 1;
+}
+
+void dump_staged(Out& o, const std::string& p, const StagedSystem& S) {
+    auto l2i = [](const std::vector<long int>& v) { return std::vector<int>(v.begin(), v.end()); };
+    o.i32(p + "nodes", {(int)S.nodes, (int)S.reserved});
+    o.i32(p + "row_ptr", l2i(S.row_ptr));
+    o.i32(p + "col_ind", l2i(S.col_ind));
+    o.f64(p + "values", S.values);
+    o.f64(p + "diag", S.diagonal);
+    o.f64(p + "b", S.b);
+    o.f64(p + "x0", S.x0);
+    o.f64(p + "voltages", S.voltages);
+    std::vector<int> a, b;
+    for (const auto& kv : S.lmm_cnts) { a.push_back((int)kv.first); b.push_back((int)kv.second); }
+    o.i32(p + "lmm_cnt_pts", a);
+    o.i32(p + "lmm_cnt_nodes", b);
+    a.clear(); b.clear();
+    for (const auto& kv : S.lmm_gnps) { a.push_back((int)kv.first); b.push_back((int)kv.second); }
+    o.i32(p + "lmm_gnp_pts", a);
+    o.i32(p + "lmm_gnp_nodes", b);
+    a.clear();
+    std::vector<double> r;
+    for (const auto& kv : S.cnt_rad) { a.push_back((int)kv.first); r.push_back(kv.second); }
+    o.i32(p + "cnt_rad_pts", a);
+    o.f64(p + "cnt_rad", r);
+    dump_csr(o, p + "tri", S.tri);
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -532,8 +616,104 @@ int main(int argc, char** argv) {
             Output_data_flags of;
             of.cnt_gnp_flag = of.gnp_data = of.prec_gnp = of.cnt_data = 0;
             remove("resistances.txt");
+            // state after Determine_clusters_and_percolation, for the staged replay below
+            Hoshen_Kopelman HS = HF;
+            std::vector<GNP> gs = gf;
+            std::vector<std::vector<long int> > ss = sg;
             Electrical_analysis EA;
             if (!EA.Perform_analysis_on_clusters(0, win, sp, ep, cf, vf, of, &HF, &CW, structure, pts, radii, pg, sg, gf)) return 25;
+            // ---- staged replay of Perform_analysis_on_clusters (Electrical_analysis.cpp:10-145) and
+            // Electrical_resistance_along_each_percolated_direction (:229-289), dumping each stage (e_*)
+            {
+                std::vector<std::vector<long int> > pb;  // GNP boundary points kept by Remove_gnp_points_in_non_relevant_boundaries
+                for (const GNP& g : gs) {
+                    std::vector<long int> v;
+                    for (const auto& q : g.pts_boundary) { v.push_back(q.first); v.push_back(q.second); }
+                    pb.push_back(v);
+                }
+                dump_csr(o, "e_pts_boundary", pb);
+                dump_csr(o, "e_structure_gnp_start", ss);
+                dump_csr(o, "e_boundary_gnp_pts", CW.boundary_gnp_pts);
+                dump_csr(o, "e_boundary_cnt_pts", CW.boundary_cnt_pts);
+                std::vector<double> gvol, gt;
+                for (const GNP& g : gs) { gvol.push_back(g.volume); gt.push_back(g.t); }
+                o.f64("e_gnp_volume", gvol);
+                o.f64("e_gnp_t", gt);
+                std::vector<int> jm;
+                std::vector<double> jmd;
+                for (const Junction& q : HS.junctions_mixed) { jm.insert(jm.end(), {(int)q.P1, q.N1, (int)q.P2, q.N2}); jmd.push_back(q.junction_dist); }
+                o.i32("e_junctions_mixed", jm);
+                o.f64("e_junctions_mixed_dist", jmd);
+                std::vector<int> jgv;
+                std::vector<double> jgd;
+                for (const Junction& q : HS.junctions_gnp) { jgv.insert(jgv.end(), {(int)q.P1, q.N1, (int)q.P2, q.N2}); jgd.push_back(q.junction_dist); }
+                o.i32("e_junctions_gnp", jgv);
+                o.f64("e_junctions_gnp_dist", jgd);
+                std::vector<int> jcv;
+                std::vector<double> jcd;
+                for (const Junction& q : HS.junctions_cnt) { jcv.insert(jcv.end(), {(int)q.P1, q.N1, (int)q.P2, q.N2}); jcd.push_back(q.junction_dist); }
+                o.i32("e_junctions_cnt", jcv);
+                o.f64("e_junctions_cnt_dist", jcd);
+                std::vector<std::vector<long int> > el0;
+                for (const auto& e : HS.elements_cnt) el0.push_back(std::vector<long int>(e.begin(), e.end()));
+                dump_csr(o, "e_elements_start", el0);
+                std::vector<std::vector<double> > par(3);
+                const int nclu = EA.Get_number_of_clusters(HS.clusters_cnt, HS.clusters_gnp);
+                EA.Clear_triangulations(HS.clusters_gnp, gs);
+                Backbone_Network* BN = new Backbone_Network;
+                for (int j = 0; j < nclu; j++) {
+                    const std::string pj = "e_c" + std::to_string(j) + "_";
+                    Direct_Electrifying* D = new Direct_Electrifying;
+                    StagedSystem su;
+                    if (!staged_field(D, j, 0, win, sp, ep, cf, &HS, &CW, pts, radii, ss, pg, gs, su)) return 26;
+                    dump_staged(o, pj + "u_", su);
+                    {
+                        Backbone_Network bz;
+                        std::vector<std::vector<double> > cur;
+                        double zc = 0;
+                        bz.Find_zero_current(j, 0, D->voltages, D->LMM_cnts, D->LMM_gnps, &HS, cf, pts, radii, pg, gs, cur, zc);
+                        o.f64(pj + "zero_current", {zc});
+                    }
+                    if (!BN->Determine_backbone_network(j, 0, sp.simulation_scope, 0, D->voltages, D->LMM_cnts, D->LMM_gnps, ep, cf, structure,
+                                                        pts, radii, pg, ss, gs, &HS)) return 27;
+                    delete D;
+                    std::vector<std::vector<long int> > el;
+                    for (const auto& e : HS.elements_cnt) el.push_back(std::vector<long int>(e.begin(), e.end()));
+                    dump_csr(o, pj + "bb_elements", el);
+                    dump_csr(o, pj + "bb_structure_gnp", ss);
+                    o.i32(pj + "bb_clusters_cnt", HS.clusters_cnt.size() ? HS.clusters_cnt[j] : std::vector<int>());
+                    o.i32(pj + "bb_clusters_gnp", HS.clusters_gnp.size() ? HS.clusters_gnp[j] : std::vector<int>());
+                    o.i32(pj + "bb_cnt_junctions", HS.cluster_cnt_junctions.size() ? HS.cluster_cnt_junctions[j] : std::vector<int>());
+                    o.i32(pj + "bb_gnp_junctions", HS.cluster_gnp_junctions.size() ? HS.cluster_gnp_junctions[j] : std::vector<int>());
+                    o.i32(pj + "bb_mix_junctions", HS.cluster_mix_junctions.size() ? HS.cluster_mix_junctions[j] : std::vector<int>());
+                    if (sp.simulation_scope) continue;
+                    if (HS.clusters_gnp.size() && j) EA.Clear_triangulations_of_cluster(HS.clusters_gnp[j - 1], gs);
+                    std::vector<int> dirs;
+                    if (!EA.Vector_of_directions(HS.family[j], sp, dirs)) return 28;
+                    const int family = HS.family[j];
+                    for (int d : dirs) {
+                        Direct_Electrifying* DR = new Direct_Electrifying;
+                        HS.family[j] = d;
+                        StagedSystem sr;
+                        if (!staged_field(DR, j, 1, win, sp, ep, cf, &HS, &CW, pts, radii, ss, pg, gs, sr)) return 29;
+                        const size_t before = par[d].size();
+                        if (!EA.Calculate_parallel_resistor(d, j, ep, DR, pts, radii, HS.elements_cnt, HS.clusters_cnt, CW.boundary_cnt, pg, gs,
+                                                            HS.clusters_gnp, CW.boundary_gnp, par)) return 30;
+                        const std::string pd = pj + "d" + std::to_string(d) + "_";
+                        dump_staged(o, pd, sr);
+                        o.f64(pd + "R", {par[d].size() > before ? par[d].back() : 0.0});
+                        delete DR;
+                    }
+                    HS.family[j] = family;
+                }
+                std::vector<double> vols;
+                for (double v : BN->volumes_cnt) vols.push_back(v);
+                for (double v : BN->volumes_gnp) vols.push_back(v);
+                for (double v : BN->dead_branches) vols.push_back(v);
+                for (double v : BN->dead_gnps) vols.push_back(v);
+                o.f64("e_bn_volumes", vols);
+                delete BN;
+            }
             std::vector<double> res;
             if (FILE* rf = fopen("resistances.txt", "r")) {
                 double v;

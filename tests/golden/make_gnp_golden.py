@@ -25,7 +25,8 @@ apart, and tests/golden/gnp_windows.npz: upstream's GNP window extraction
 (Fill_gnps_inside) for two centred windows smaller than the sample (the
 120-GNP fixture itself carries it for the whole sample as the window), and
 tests/golden/gnp_hybrid_flow.npz: upstream's own stage sequence for GNP_CNT_mix
-on both hybrid samples up to the percolated clusters.
+on both hybrid samples up to the percolated clusters, and
+tests/golden/gnp_hybrid_electrical.npz: its electrical stage, stage by stage.
 
     python tests/golden/make_gnp_golden.py
 """
@@ -217,6 +218,34 @@ def main_flow():
     np.savez_compressed(os.path.join(HERE, "gnp_hybrid_flow.npz"), **out)
 
 
+def main_electrical():
+    """tests/golden/gnp_hybrid_electrical.npz: upstream's electrical stage of both
+    hybrid samples, replayed by the harness through the public members of
+    Electrical_analysis, Direct_Electrifying and Backbone_Network in
+    Perform_analysis_on_clusters' order (e_* records): per percolated cluster
+    the unit-resistor system (node maps of CNT and GNP points, the SSS matrix,
+    right-hand side, voltages, the GNP triangulations and the GNP points with a
+    CNT radius), the zero current, the backbone (CNT elements, GNP point lists,
+    clusters and junction groups after it), and per percolated direction the
+    real-resistor system and its resistor; the GNP points, point lists and
+    boundary points the stage starts from, and the volume members at the end."""
+    out = {}
+    samples = (("m", hybrid_network, generate_gnps(N, SIDE, SEED)),
+               ("s", sparse_network, generate_gnps(SPARSE_N, SIDE, SPARSE_SEED, l_range=(0.3, 0.5))))
+    for tag, network, g in samples:
+        with tempfile.TemporaryDirectory() as d:
+            network(d)
+            write_gnp_file(d, g)
+            subprocess.run([REF, d, os.path.join(d, "g.bin"), repr(VDW), repr(TUNNEL), repr(GS_MIN), repr(OVERLAP_CNT), repr(float(OVERLAP_GNP)),
+                            "-1", "flow", repr(cnt_config().step), "electrical"], check=True, capture_output=True, timeout=1200)
+            z = read_dump(os.path.join(d, "g.bin"))
+        for k, v in z.items():
+            if k.startswith("e_") or k in ("flow_points_gnp", "flow_structure_gnp_ptr", "flow_structure_gnp_idx", "flow_resistances"):
+                out[f"{tag}_{k}"] = v
+        print(f"electrical {tag}: {sum(1 for k in z if k.endswith('_u_nodes'))} clusters, R_x {z['flow_resistances'][0]:.6g} Ohm")
+    np.savez_compressed(os.path.join(HERE, "gnp_hybrid_electrical.npz"), **out)
+
+
 def main_resistors():
     """tests/golden/gnp_resistors.npz: upstream's Calculate_resistance_gnp on the
     triangulation edges of the 120-GNP fixture's GNPs (radii t/2, or the CNT
@@ -252,4 +281,5 @@ if __name__ == "__main__":
     main_labels()
     main_windows()
     main_flow()
+    main_electrical()
     main_resistors()
