@@ -114,6 +114,30 @@ class Result(C.Structure):
     ]
 
 
+_I64P, _I32P, _F64P = C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_double)
+
+
+class HybridState(C.Structure):
+    """cicy_hybrid_state: a mixed CNT/GNP network after percolation (host arrays)."""
+    _fields_ = [
+        ("n_clusters", C.c_int32), ("family", _I32P),
+        ("clusters_cnt_ptr", _I64P), ("clusters_cnt_idx", _I32P),
+        ("clusters_gnp_ptr", _I64P), ("clusters_gnp_idx", _I32P),
+        ("cnt_junctions_ptr", _I64P), ("cnt_junctions_idx", _I32P),
+        ("gnp_junctions_ptr", _I64P), ("gnp_junctions_idx", _I32P),
+        ("mix_junctions_ptr", _I64P), ("mix_junctions_idx", _I32P),
+        ("n_junctions_cnt", C.c_int64), ("jc_p1", _I64P), ("jc_n1", _I32P), ("jc_p2", _I64P), ("jc_n2", _I32P), ("jc_dist", _F64P),
+        ("n_junctions_gnp", C.c_int64), ("jg_p1", _I64P), ("jg_n1", _I32P), ("jg_p2", _I64P), ("jg_n2", _I32P), ("jg_dist", _F64P),
+        ("n_junctions_mixed", C.c_int64), ("jm_p1", _I64P), ("jm_n1", _I32P), ("jm_p2", _I64P), ("jm_n2", _I32P), ("jm_dist", _F64P),
+        ("elements_ptr", _I64P), ("elements_idx", _I64P),
+        ("n_gnps", C.c_int32), ("n_points_gnp", C.c_int64), ("points_gnp", _F64P),
+        ("structure_gnp_ptr", _I64P), ("structure_gnp_idx", _I64P), ("pts_boundary_count", _I32P),
+        ("gnp_t", _F64P), ("gnp_volume", _F64P), ("gnp_frame", _F64P),
+        ("boundary_gnp_ptr", _I64P), ("boundary_gnp_idx", _I32P),
+        ("boundary_gnp_pts_ptr", _I64P), ("boundary_gnp_pts_idx", _I64P),
+    ]
+
+
 class GnnSystem(C.Structure):
     _fields_ = [
         ("n", C.c_int32),
@@ -264,6 +288,10 @@ def lib() -> C.CDLL:
         "cicy_get_labels": (C.c_int, [C.c_void_p, i32p, i32p, i32p]),
         "cicy_get_junctions": (C.c_int, [C.c_void_p, i64p, i64p, i32p, i64p, i32p, f64p]),
         "cicy_get_volumes": (C.c_int, [C.c_void_p, f64p, f64p, f64p, f64p]),
+        "cicy_hybrid_electrical": (C.c_int, [C.c_void_p, P(HybridState), P(Params), C.c_double, C.c_double, P(Result)]),
+        "cicy_get_hybrid_structure": (C.c_int, [C.c_void_p, i64p, i64p, i64p]),
+        "cicy_get_hybrid_volumes": (C.c_int, [C.c_void_p, f64p]),
+        "cicy_get_hybrid_junctions": (C.c_int, [C.c_void_p, C.c_int32, i64p, i32p, i64p, i32p]),
         "cicy_get_elements": (C.c_int, [C.c_void_p, C.c_int32, i64p, i64p, i64p, i64p]),
         "cicy_get_clusters": (C.c_int, [C.c_void_p, C.c_int32, i32p, i64p, i64p, i32p, i32p, i64p, i64p, i32p]),
         "cicy_get_system": (C.c_int, [C.c_void_p, C.c_int32, i64p, i64p, i64p, i64p, i64p, f64p, f64p, f64p, f64p, f64p]),

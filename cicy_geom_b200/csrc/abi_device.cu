@@ -306,6 +306,71 @@ cicy_status cicy_get_junctions(cicy_ctx* ctx, int64_t* n, int64_t* p1, int32_t* 
     });
 }
 
+cicy_status cicy_hybrid_electrical(cicy_ctx* ctx, const cicy_hybrid_state* st, const cicy_params* p, double resistivity_gnp_surf,
+                                   double resistivity_gnp_t, cicy_result* out) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (!st || !p) throw cicy::Fail{CICY_E_INPUT, "cicy_hybrid_electrical: null argument"};
+        cicy::run_hybrid_electrical(c, *st, *p, resistivity_gnp_surf, resistivity_gnp_t, out);
+    });
+}
+
+cicy_status cicy_get_hybrid_structure(cicy_ctx* ctx, int64_t* n_idx, int64_t* ptr, int64_t* idx) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (!c.have_hybrid || !c.hy) throw cicy::Fail{CICY_E_STATE, "no hybrid electrical stage yet"};
+        cicy::HybridDev& H = *c.hy;
+        const int NG = H.n_gnps;
+        std::vector<int32_t> sp(NG + 1), sc(std::max(NG, 1));
+        if (NG) {
+            d2h(c, sp.data(), H.sptr.get(), NG + 1);
+            d2h(c, sc.data(), H.scount.get(), NG);
+        }
+        sync(c);
+        int64_t tot = 0;
+        if (ptr) ptr[0] = 0;
+        std::vector<int32_t> buf;
+        for (int g = 0; g < NG; g++) {
+            if (idx && sc[g]) {
+                buf.resize(sc[g]);
+                d2h(c, buf.data(), H.sidx.get() + sp[g], sc[g]);
+                sync(c);
+                for (int k = 0; k < sc[g]; k++) idx[tot + k] = buf[k];
+            }
+            tot += sc[g];
+            if (ptr) ptr[g + 1] = tot;
+        }
+        if (n_idx) *n_idx = tot;
+    });
+}
+
+cicy_status cicy_get_hybrid_volumes(cicy_ctx* ctx, double* volumes30) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (!c.have_hybrid || !c.hy) throw cicy::Fail{CICY_E_STATE, "no hybrid electrical stage yet"};
+        if (!volumes30) throw cicy::Fail{CICY_E_INPUT, "null buffer"};
+        double a[31], g[15];
+        d2h(c, a, c.vol_acc.get(), 31);
+        d2h(c, g, c.hy->vol_acc.get(), 15);
+        sync(c);
+        std::copy(a, a + 8, volumes30);            // volumes_cnt
+        std::copy(g, g + 8, volumes30 + 8);        // volumes_gnp
+        std::copy(a + 8, a + 15, volumes30 + 16);  // dead_branches
+        std::copy(g + 8, g + 15, volumes30 + 23);  // dead_gnps
+    });
+}
+
+cicy_status cicy_get_hybrid_junctions(cicy_ctx* ctx, int32_t cluster, int64_t* n_gnp, int32_t* gnp, int64_t* n_mix, int32_t* mix) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (!c.have_hybrid || !c.hy) throw cicy::Fail{CICY_E_STATE, "no hybrid electrical stage yet"};
+        cicy::HybridDev& H = *c.hy;
+        if (cluster < 0 || cluster >= H.n_clusters) throw cicy::Fail{CICY_E_INPUT, "no such cluster"};
+        const int ng = H.cgj_len[cluster], nm = H.cmj_len[cluster];
+        if (n_gnp) *n_gnp = ng;
+        if (n_mix) *n_mix = nm;
+        if (gnp && ng) d2h(c, gnp, H.cgj_idx.get() + H.h_cgj_ptr[cluster], ng);
+        if (mix && nm) d2h(c, mix, H.cmj_idx.get() + H.h_cmj_ptr[cluster], nm);
+        sync(c);
+    });
+}
+
 cicy_status cicy_get_volumes(cicy_ctx* ctx, double* volumes_cnt, double* dead_branches, double* total_volumes, double* fractions) {
     return guarded(ctx, [&](cicy::Ctx& c) {
         if (!c.have_volumes) throw cicy::Fail{CICY_E_STATE, "no volumes yet (cicy_electrical_analysis with simulation_scope < 2)"};

@@ -46,6 +46,46 @@ struct DeaSystem {
     DBuf<double> val, diag, b, x0, volt;
 };
 
+// The GNP side of a mixed CNT/GNP network for its electrical stage (hybrid_dea.cuh):
+// upstream's GNP members after Determine_clusters_and_percolation, on the device,
+// and the working state of the DEA passes.
+struct HybridDev {
+    int n_gnps = 0, n_pts = 0, n_clusters = 0;
+    double rs = 0, rt = 0;              // GNP in-plane and through-plane resistivity
+    int n_tri_pass = 0;                 // triangulation edges of the system being assembled
+    DBuf<double> pts;                   // GNP points, xyz
+    DBuf<int32_t> sptr, sidx, scount;   // structure_gnp: capacity CSR, current length per GNP (kept points at the front)
+    DBuf<int32_t> nb;                   // boundary points per GNP (GNP::pts_boundary.size())
+    DBuf<double> t, vol, geom;          // thickness, volume, triangulation frame (l, centre[3], rotation[9], face-0 normal[3])
+    DBuf<int32_t> bg_idx, bgp_idx;      // boundary_gnp, boundary_gnp_pts (six faces)
+    std::vector<int32_t> h_bg_ptr, h_bgp_ptr;
+    int n_jg = 0, n_jm = 0;             // junctions_gnp, junctions_mixed (P1, N1, P2, N2, distance)
+    DBuf<int32_t> jg_p1, jg_n1, jg_p2, jg_n2, jm_p1, jm_n1, jm_p2, jm_n2;
+    DBuf<double> jg_d, jm_d;
+    // per cluster: GNP list and junction lists (the junction lists shrink in the backbone)
+    std::vector<int32_t> h_cg_ptr, h_cgj_ptr, h_cmj_ptr, cgj_len, cmj_len;
+    DBuf<int32_t> cg_idx, cgj_idx, cmj_idx;
+    // per pass
+    DBuf<int32_t> lmm_g, rad_from, tri_cnt, tri, gcnt, goff, pt_removed, alive, alive_scan, tmp_list, seg_start;
+    DBuf<double> cnt_rad, bterm;
+    DBuf<int32_t> bvalid, boff, elem_removed, removed_cnt, to_remove, mix_alive, gj_alive, live, elem_tmp;
+    DBuf<uint64_t> key;
+    DBuf<uint32_t> val;
+    DBuf<unsigned char> tri_work;
+    DBuf<double> vol_acc;               // volumes_cnt[8], volumes_gnp[8], dead_branches[7], dead_gnps[7]
+};
+
+// The GNP part of one DEA system of a mixed cluster (lists on the device).
+struct GnpPass {
+    HybridDev* hy;
+    const int32_t* gnps;
+    int n_gnps;
+    const int32_t* mix;
+    int n_mix;
+    const int32_t* gj;
+    int n_gj;
+};
+
 struct Ctx {
     Ctx() = default;
     Ctx(const Ctx&) = delete;
@@ -137,6 +177,8 @@ struct Ctx {
     DBuf<uint64_t> vol_key;
     DBuf<uint32_t> vol_cnt;
     bool have_volumes = false;
+    HybridDev* hy = nullptr;  // mixed CNT/GNP electrical stage (cicy_hybrid_electrical)
+    bool have_hybrid = false;
     DBuf<int32_t> chain_start, chain_len;
     SolverWork sw;
     GnnState gnn;
@@ -157,6 +199,9 @@ void upload_network(Ctx& c, const cicy_network& net);
 void run_contact_grid(Ctx& c, const cicy_params& p);
 void run_clusters(Ctx& c, const cicy_params& p);
 void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out);
+// Electrical_analysis::Perform_analysis_on_clusters for a mixed CNT/GNP network (hybrid_dea.cuh).
+void run_hybrid_electrical(Ctx& c, const cicy_hybrid_state& h, const cicy_params& p, double rho_gnp_surf, double rho_gnp_t,
+                           cicy_result* out);
 struct GnpSet;
 struct GnpGrid;
 // CNT-GNP contacts of the hybrid grid (gnp_grid.cu); returns the number of contacts.

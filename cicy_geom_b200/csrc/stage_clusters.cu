@@ -441,6 +441,7 @@ int grid_for(long long n, int threads = 256) {
 Ctx::~Ctx() {
     for (auto* s : systems) delete s;
     for (auto* s : sys_pool) delete s;
+    delete hy;
 }
 
 int32_t read_i32(Ctx& c, const int32_t* dptr) {
@@ -536,6 +537,7 @@ void upload_network(Ctx& c, const cicy_network& n) {
     c.stage = 1;
     c.have_backbone = false;
     c.have_volumes = false;
+    c.have_hybrid = false;
 }
 
 // ---------------------------------------------------------------------------
@@ -804,6 +806,7 @@ void run_clusters(Ctx& c, const cicy_params& p) {
     c.stage = 3;
     c.have_backbone = false;
     c.have_volumes = false;
+    c.have_hybrid = false;
 }
 
 }  // namespace cicy

@@ -673,7 +673,22 @@ struct SolveInput {
     int n_members;
     const int32_t* jlist;
     int n_jlist;
+    const GnpPass* gnp = nullptr;  // the GNP side of a mixed cluster (hybrid_dea.cuh), or none
 };
+
+// GNP side of a mixed cluster's system (hybrid_dea.cuh): GNP point nodes after the CNT
+// nodes (returns how many), then the CNT-GNP, triangulation and GNP-GNP resistors
+// (count, then fill at `base`), as Compute_voltage_field adds them.
+int gnp_lmm(Ctx& c, const GnpPass& g, const int* bnd, int nbnd, int first_node);
+int gnp_prepare_edges(Ctx& c, const GnpPass& g, int r_flag);
+void gnp_fill_edges(Ctx& c, const GnpPass& g, int base, int r_flag, int reserved, const cicy_params& p);
+
+__global__ void k_singleton_chains(int n, int first_chain, int first_row, int32_t* __restrict__ cs, int32_t* __restrict__ cl) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        cs[first_chain + k] = first_row + k;
+        cl[first_chain + k] = 1;
+    }
+}
 
 double seconds_between(cudaEvent_t a, cudaEvent_t b) {
     float ms = 0;
@@ -732,12 +747,23 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
         k_node_assign<<<grid_for(NM), 256, 0, s>>>(NM, reserved, eb.get(), ee.get(), c.elem_idx.get(), c.cnt_node_base.get(),
                                                    c.cnt_fresh.get(), c.lmm.get());
         c.launches += 4;
-        const int nodes = reserved + read_i32(c, c.i32_scalar.get());
-        // free nodes of each CNT are one consecutive range: the chains of the block preconditioner
-        c.chain_start.ensure(NM + 1);
-        c.chain_len.ensure(NM + 1);
-        CICY_CUDA(cudaMemcpyAsync(c.chain_start.get(), c.cnt_node_base.get(), sizeof(int32_t) * NM, cudaMemcpyDeviceToDevice, s));
-        CICY_CUDA(cudaMemcpyAsync(c.chain_len.get(), c.cnt_nodes.get(), sizeof(int32_t) * NM, cudaMemcpyDeviceToDevice, s));
+        int nodes = reserved + read_i32(c, c.i32_scalar.get());
+        const int n_cnt_free = nodes - reserved;
+        const int n_gnp_nodes = in.gnp ? gnp_lmm(c, *in.gnp, bnd, nbnd, nodes) : 0;
+        nodes += n_gnp_nodes;
+        // free nodes of each CNT are one consecutive range: the chains of the block preconditioner;
+        // each GNP point node is a chain of its own
+        const int NMc = NM + n_gnp_nodes;
+        c.chain_start.ensure(NMc + 1);
+        c.chain_len.ensure(NMc + 1);
+        if (NM > 0) {
+            CICY_CUDA(cudaMemcpyAsync(c.chain_start.get(), c.cnt_node_base.get(), sizeof(int32_t) * NM, cudaMemcpyDeviceToDevice, s));
+            CICY_CUDA(cudaMemcpyAsync(c.chain_len.get(), c.cnt_nodes.get(), sizeof(int32_t) * NM, cudaMemcpyDeviceToDevice, s));
+        }
+        if (n_gnp_nodes > 0) {
+            k_singleton_chains<<<grid_for(n_gnp_nodes), 256, 0, s>>>(n_gnp_nodes, NM, n_cnt_free, c.chain_start.get(), c.chain_len.get());
+            c.launches++;
+        }
         const int n = nodes - reserved;
         sys->nodes = nodes;
         tr.mark(r_flag ? "dea.real.lmm" : "dea.unit.lmm");
@@ -746,7 +772,8 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
         exclusive_scan_i32(c.cnt_nodes.get(), c.cnt_node_base.get(), NM, c.i32_scalar.get(), c.scan_tmp32, s, c.launches);
         c.launches++;
         const int n_cnt_edges = read_i32(c, c.i32_scalar.get());
-        const int NE = n_cnt_edges + in.n_jlist;
+        const int n_gnp_edges = in.gnp ? gnp_prepare_edges(c, *in.gnp, r_flag) : 0;
+        const int NE = n_cnt_edges + in.n_jlist + n_gnp_edges;
         c.e_n1.ensure(NE + 1); c.e_n2.ensure(NE + 1); c.e_op.ensure(NE + 1); c.e_g.ensure(NE + 1);
         k_cnt_edges<<<grid_for(NM), 256, 0, s>>>(NM, r_flag, p.resistivity_cnt, in.members, eb.get(), ee.get(), c.elem_idx.get(), c.lmm.get(),
                                                c.cnt_node_base.get(), c.radii.get(), c.x.get(), c.y.get(), c.z.get(), c.e_n1.get(),
@@ -759,6 +786,7 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
                                                                 c.e_n1.get(), c.e_n2.get(), c.e_op.get(), c.e_g.get());
             c.launches++;
         }
+        if (in.gnp) gnp_fill_edges(c, *in.gnp, n_cnt_edges + in.n_jlist, r_flag, reserved, p);
         tr.mark(r_flag ? "dea.real.edges" : "dea.unit.edges");
         // ---- sort-and-reduce assembly ----
         const int bn = bits_for((uint64_t)std::max(nodes, 1));
@@ -878,17 +906,17 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
         const float* ew = nullptr;
         if (c.solver.preconditioner == CICY_PRECOND_LEARNED && n > 0) {
             kind = PRECOND_KIND_SPAI;
-            ew = learned_edge_weights(c, ss, NM, s);
+            ew = learned_edge_weights(c, ss, NMc, s);
             tr.mark(r_flag ? "dea.real.gnn" : "dea.unit.gnn");
         } else if (c.solver.preconditioner != CICY_PRECOND_JACOBI && n > 0) {
             kind = PRECOND_KIND_BLOCK;
         }
         // host copy of the chains, for cicy_get_chains
-        sys->h_chain_start.resize(NM);
-        sys->h_chain_len.resize(NM);
-        if (NM > 0) {
-            CICY_CUDA(cudaMemcpyAsync(sys->h_chain_start.data(), c.chain_start.get(), sizeof(int32_t) * NM, cudaMemcpyDeviceToHost, s));
-            CICY_CUDA(cudaMemcpyAsync(sys->h_chain_len.data(), c.chain_len.get(), sizeof(int32_t) * NM, cudaMemcpyDeviceToHost, s));
+        sys->h_chain_start.resize(NMc);
+        sys->h_chain_len.resize(NMc);
+        if (NMc > 0) {
+            CICY_CUDA(cudaMemcpyAsync(sys->h_chain_start.data(), c.chain_start.get(), sizeof(int32_t) * NMc, cudaMemcpyDeviceToHost, s));
+            CICY_CUDA(cudaMemcpyAsync(sys->h_chain_len.data(), c.chain_len.get(), sizeof(int32_t) * NMc, cudaMemcpyDeviceToHost, s));
         }
         PcgStats st;
         const double tol = (r_flag == 0 && p.tolerance_unit > 0) ? p.tolerance_unit : p.tolerance;
@@ -897,7 +925,7 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
         // otherwise (or when disabled) the grid-wide persistent kernel
         bool solved = false;
         if (c.solver.preconditioner == CICY_PRECOND_MG && n > 0) {
-            build_block_preconditioner(c.sw, ss, NM, c.chain_start.get(), c.chain_len.get(), nullptr, nullptr, false, s, c.launches);
+            build_block_preconditioner(c.sw, ss, NMc, c.chain_start.get(), c.chain_len.get(), nullptr, nullptr, false, s, c.launches);
             tr.mark(r_flag ? "dea.real.blocks" : "dea.unit.blocks");
             build_mg_hierarchy(c.sw, ss, s, c.launches);
             tr.mark(r_flag ? "dea.real.mg_setup" : "dea.unit.mg_setup");
@@ -906,11 +934,11 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
             solved = true;
         }
         if (!solved && kind != PRECOND_KIND_SPAI && !mixed && !(c.solver.flags & CICY_SOLVER_NO_CLUSTER))
-            solved = pcg_solve_cluster(c.sw, ss, kind == PRECOND_KIND_BLOCK, nullptr, nullptr, NM, c.chain_start.get(), c.chain_len.get(),
+            solved = pcg_solve_cluster(c.sw, ss, kind == PRECOND_KIND_BLOCK, nullptr, nullptr, NMc, c.chain_start.get(), c.chain_len.get(),
                                        tol, max_iter, s, c.launches, st);
         if (!solved) {
             if (kind != PRECOND_KIND_JACOBI)
-                build_block_preconditioner(c.sw, ss, NM, c.chain_start.get(), c.chain_len.get(), nullptr, nullptr, mixed, s, c.launches);
+                build_block_preconditioner(c.sw, ss, NMc, c.chain_start.get(), c.chain_len.get(), nullptr, nullptr, mixed, s, c.launches);
             pcg_solve(c.sw, ss, kind, mixed, tol, max_iter, c.num_sms, c.status.get(), s, c.launches, st, ew);
         }
         check_status(c, "Solve_DEA_equations_CG_SSS");
@@ -961,7 +989,7 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
 // ---------------------------------------------------------------------------
 // Electrical_analysis::Perform_analysis_on_clusters (Electrical_analysis.cpp:10-145).
 void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out) {
-    if (c.stage < 3) throw Fail{CICY_E_STATE, "cicy_electrical_analysis: run cicy_clusters first"};
+    if (c.stage < 3 || c.have_hybrid) throw Fail{CICY_E_STATE, "cicy_electrical_analysis: run cicy_clusters first"};
     cudaStream_t s = c.stream;
     for (auto* sy : c.systems) c.sys_pool.push_back(sy);
     c.systems.clear();
@@ -1156,3 +1184,6 @@ void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out) {
 }
 
 }  // namespace cicy
+
+// The GNP branch of the DEA for mixed CNT/GNP networks (same translation unit).
+#include "hybrid_dea.cuh"

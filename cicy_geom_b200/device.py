@@ -170,6 +170,54 @@ class Context:
         self._check(lib().cicy_network_to_conductance(self._h, C.byref(p), C.byref(r)), "cicy_network_to_conductance")
         return r
 
+    def hybrid_electrical(self, st: dict, p: _abi.Params, rho_gnp_surf: float = 1e-4, rho_gnp_t: float = 1.0) -> _abi.Result:
+        """cicy_hybrid_electrical on a mixed CNT/GNP network after percolation.  `st` holds
+        numpy arrays named as the fields of cicy_hybrid_state (CSR lists as *_ptr / *_idx;
+        gnp_frame 16 values per GNP); the CNT network is the context's uploaded one."""
+        types = {f: t for f, t in _abi.HybridState._fields_}
+        keep = []
+        h = _abi.HybridState()
+        for f, t in types.items():
+            if t in (C.c_int32, C.c_int64):
+                setattr(h, f, int(st[f]))
+                continue
+            ct = t._type_
+            dt = {C.c_int64: np.int64, C.c_int32: np.int32, C.c_double: np.float64}[ct]
+            a = np.ascontiguousarray(st[f], dtype=dt)
+            if a.size == 0:
+                a = np.zeros(1, dt)
+            keep.append(a)
+            setattr(h, f, a.ctypes.data_as(t))
+        self.hybrid_n_gnps = int(st["n_gnps"])
+        r = _abi.Result()
+        self._check(lib().cicy_hybrid_electrical(self._h, C.byref(h), C.byref(p), rho_gnp_surf, rho_gnp_t, C.byref(r)),
+                    "cicy_hybrid_electrical")
+        return r
+
+    def hybrid_structure(self):
+        """structure_gnp after the hybrid backbone, as (ptr, idx)."""
+        n = C.c_int64()
+        self._check(lib().cicy_get_hybrid_structure(self._h, C.byref(n), None, None), "cicy_get_hybrid_structure")
+        ng = self.hybrid_n_gnps
+        ptr, idx = np.zeros(ng + 1, np.int64), np.zeros(max(n.value, 1), np.int64)
+        self._check(lib().cicy_get_hybrid_structure(self._h, C.byref(n), _p(ptr, C.c_int64), _p(idx, C.c_int64)), "cicy_get_hybrid_structure")
+        return ptr, idx[: n.value]
+
+    def hybrid_volumes(self) -> np.ndarray:
+        """volumes_cnt[8], volumes_gnp[8], dead_branches[7], dead_gnps[7] of the hybrid stage."""
+        v = np.zeros(30)
+        self._check(lib().cicy_get_hybrid_volumes(self._h, _p(v, C.c_double)), "cicy_get_hybrid_volumes")
+        return v
+
+    def hybrid_junctions(self, cluster: int):
+        """(cluster_gnp_junctions, cluster_mix_junctions) of a cluster after its backbone."""
+        ng, nm = C.c_int64(), C.c_int64()
+        self._check(lib().cicy_get_hybrid_junctions(self._h, cluster, C.byref(ng), None, C.byref(nm), None), "cicy_get_hybrid_junctions")
+        g, m = np.zeros(max(ng.value, 1), np.int32), np.zeros(max(nm.value, 1), np.int32)
+        self._check(lib().cicy_get_hybrid_junctions(self._h, cluster, C.byref(ng), _p(g, C.c_int32), C.byref(nm), _p(m, C.c_int32)),
+                    "cicy_get_hybrid_junctions")
+        return g[: ng.value], m[: nm.value]
+
     # ---- copy-out ----
     def sectioned_domain(self):
         nr, ns = C.c_int64(), C.c_int64()

@@ -190,6 +190,58 @@ cicy_status cicy_electrical_analysis(cicy_ctx* ctx, const cicy_params* p, cicy_r
 /* All three stages (App_Network_3D.cpp:140-179 for one window). */
 cicy_status cicy_network_to_conductance(cicy_ctx* ctx, const cicy_params* p, cicy_result* out);
 
+/* ---------------- electrical stage of a mixed CNT/GNP network (GNP_CNT_mix) ----------------
+ * Upstream's public members after Hoshen_Kopelman::Determine_clusters_and_percolation
+ * and Cutoff_Wins for a mixed network (Hoshen_Kopelman.h:27-51, Cutoff_Wins.h), the
+ * state Electrical_analysis::Perform_analysis_on_clusters reads.  Host arrays, copied.
+ * CSR lists: *_ptr has one offset more than lists.  Junctions: (P1, N1, P2, N2, distance);
+ * mixed junctions have the CNT point and CNT first.  The CNT points, radii and face
+ * point lists are the context's uploaded network. */
+typedef struct {
+    int32_t n_clusters;
+    const int32_t* family;                                                   /* [n_clusters] */
+    const int64_t* clusters_cnt_ptr; const int32_t* clusters_cnt_idx;        /* clusters_cnt */
+    const int64_t* clusters_gnp_ptr; const int32_t* clusters_gnp_idx;        /* clusters_gnp */
+    const int64_t* cnt_junctions_ptr; const int32_t* cnt_junctions_idx;      /* cluster_cnt_junctions */
+    const int64_t* gnp_junctions_ptr; const int32_t* gnp_junctions_idx;      /* cluster_gnp_junctions */
+    const int64_t* mix_junctions_ptr; const int32_t* mix_junctions_idx;      /* cluster_mix_junctions */
+    int64_t n_junctions_cnt;
+    const int64_t* jc_p1; const int32_t* jc_n1; const int64_t* jc_p2; const int32_t* jc_n2; const double* jc_dist;
+    int64_t n_junctions_gnp;
+    const int64_t* jg_p1; const int32_t* jg_n1; const int64_t* jg_p2; const int32_t* jg_n2; const double* jg_dist;
+    int64_t n_junctions_mixed;
+    const int64_t* jm_p1; const int32_t* jm_n1; const int64_t* jm_p2; const int32_t* jm_n2; const double* jm_dist;
+    const int64_t* elements_ptr; const int64_t* elements_idx;                /* elements_cnt of every CNT (ascending) */
+    int32_t n_gnps;
+    int64_t n_points_gnp;
+    const double* points_gnp;                                                /* xyz per GNP point */
+    const int64_t* structure_gnp_ptr; const int64_t* structure_gnp_idx;      /* structure_gnp */
+    const int32_t* pts_boundary_count;                                       /* GNP::pts_boundary.size() */
+    const double* gnp_t; const double* gnp_volume;                           /* GNP::t, GNP::volume */
+    const double* gnp_frame;  /* 16 per GNP: side l, centre[3], rotation[9] (row-major), face-0 normal[3] */
+    const int64_t* boundary_gnp_ptr; const int32_t* boundary_gnp_idx;        /* Cutoff_Wins::boundary_gnp (6 faces) */
+    const int64_t* boundary_gnp_pts_ptr; const int64_t* boundary_gnp_pts_idx;/* Cutoff_Wins::boundary_gnp_pts (6 faces) */
+} cicy_hybrid_state;
+/* Electrical_analysis::Perform_analysis_on_clusters for GNP_CNT_mix (Electrical_analysis.cpp:10-145,
+ * 229-675) on the device: per percolated cluster the unit-resistor DEA (LM_matrix_for_cnts and
+ * LM_matrix_for_gnps, CNT, CNT-CNT, CNT-GNP and GNP-GNP junction resistors and the resistors of
+ * each GNP's triangulation, Direct_Electrifying.cpp:11-1394), the backbone of CNTs and GNPs
+ * (Backbone_Network.cpp:11-1127) and the real-resistor DEA and parallel resistor per
+ * percolated direction with CNT and GNP boundary currents; GNP in-plane / through-plane
+ * resistivities as Electric_para::resistivity_GNP_surf / resistivity_GNP_t.  Needs the uploaded
+ * CNT network (cicy_upload_network); simulation_scope 0.  A GNP with more points than the
+ * triangulation holds (256) gives CICY_E_CAPACITY; upstream's failures give CICY_E_INPUT. */
+cicy_status cicy_hybrid_electrical(cicy_ctx* ctx, const cicy_hybrid_state* st, const cicy_params* p, double resistivity_gnp_surf,
+                                   double resistivity_gnp_t, cicy_result* out);
+/* After cicy_hybrid_electrical: structure_gnp as the backbone left it (CSR over GNPs; size query
+ * with NULL buffers), and the volume members volumes_cnt[8], volumes_gnp[8], dead_branches[7],
+ * dead_gnps[7] before the fractions step (Backbone_Network.h:26-34). */
+cicy_status cicy_get_hybrid_structure(cicy_ctx* ctx, int64_t* n_idx, int64_t* ptr, int64_t* idx);
+cicy_status cicy_get_hybrid_volumes(cicy_ctx* ctx, double* volumes30);
+/* The GNP and mixed junction lists of a percolated cluster after its backbone (cluster_gnp_junctions,
+ * cluster_mix_junctions); sizes in n_gnp / n_mix (NULL buffers: size query). */
+cicy_status cicy_get_hybrid_junctions(cicy_ctx* ctx, int32_t cluster, int64_t* n_gnp, int32_t* gnp, int64_t* n_mix, int32_t* mix);
+
 /* ---------------- copy-out (size query: pass NULL buffers, read the counts) ----------------
  * These fill the public members the upstream classes expose to later stages. */
 /* Contact_grid::sectioned_domain_cnts as CSR (n_regions + 1 offsets). */

@@ -1,0 +1,54 @@
+"""The electrical stage of a mixed CNT/GNP network on the device (cicy_hybrid_electrical)
+against upstream's own stage-by-stage replay (tests/golden/gnp_hybrid_electrical.npz) on
+both hybrid samples: the unit- and real-resistor systems (structure exact; values,
+diagonal and right-hand side within 2 ulp: FP64 exp of CUDA vs glibc), the backbone
+(CNT clusters and junctions, GNP point lists, GNP and mixed junction lists), the volume
+members, and R along x within what the two CG tolerances leave (1e-6)."""
+import numpy as np
+import pytest
+from test_hybrid_electrical import _csr, hybrid_arrays, hybrid_state
+
+from cicy_geom_b200.device import Context
+from cicy_geom_b200.network import HostNetwork
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("tag", ["s", "m"])
+def test_hybrid_electrical_on_device_matches_upstream(cuda_ok, tmp_path, tag):
+    h, p, z, f = hybrid_state(tag, str(tmp_path))
+    from cicy_geom_b200.network import NetworkConfig
+
+    cfg = NetworkConfig(side=2.0, n_cnts=1, seed=0, tolerance=1e-10, vdw=0.00034, tunnel=0.0018)
+    prm = cfg.params()
+    prm.resistances[0], prm.resistances[1], prm.resistances[2] = 1, 0, 0
+    ctx = Context(0)
+    ctx.upload(HostNetwork.from_arrays(h["net"]))
+    r = ctx.hybrid_electrical(hybrid_arrays(h), prm, 1e-4, 1.0)
+    nclu = len(f["flow_family"])
+    pref = []
+    for j in range(nclu):
+        pref.append(f"e_c{j}_u_")
+        pref += [f"e_c{j}_d{d}_" for d in range(3) if f"e_c{j}_d{d}_nodes" in z]
+    assert r.n_solves == len(pref)
+    for i, pfx in enumerate(pref):
+        S = ctx.system(i)
+        assert (S["nodes"], S["reserved"]) == tuple(z[pfx + "nodes"]), pfx
+        assert np.array_equal(S["row_ptr"], z[pfx + "row_ptr"]) and np.array_equal(S["col_ind"], z[pfx + "col_ind"]), pfx
+        for k in ("values", "diag", "b", "x0"):
+            np.testing.assert_allclose(S[k], z[pfx + k], rtol=5e-16, atol=0, err_msg=pfx + k)
+        vr = z[pfx + "voltages"]
+        np.testing.assert_allclose(S["voltages"], vr, rtol=0, atol=1e-6 * np.max(np.abs(vr)), err_msg=pfx)
+    ptr, idx = ctx.hybrid_structure()
+    st = [list(idx[ptr[g]:ptr[g + 1]]) for g in range(len(ptr) - 1)]
+    assert st == _csr(z, f"e_c{nclu - 1}_bb_structure_gnp")
+    cb = ctx.percolated_clusters(1)
+    for j in range(nclu):
+        assert list(cb["idx"][cb["ptr"][j]:cb["ptr"][j + 1]]) == z[f"e_c{j}_bb_clusters_cnt"].tolist()
+        assert list(cb["junc_idx"][cb["junc_ptr"][j]:cb["junc_ptr"][j + 1]]) == z[f"e_c{j}_bb_cnt_junctions"].tolist()
+        g, m = ctx.hybrid_junctions(j)
+        assert g.tolist() == z[f"e_c{j}_bb_gnp_junctions"].tolist() and m.tolist() == z[f"e_c{j}_bb_mix_junctions"].tolist()
+    bp, bi = ctx.elements(1)
+    assert [list(bi[bp[c]:bp[c + 1]]) for c in range(len(bp) - 1)] == _csr(z, f"e_c{nclu - 1}_bb_elements")
+    assert ctx.hybrid_volumes().tolist() == z["e_bn_volumes"].tolist()
+    np.testing.assert_allclose(np.array(r.resistances), z["flow_resistances"], rtol=1e-6)

@@ -69,6 +69,39 @@ def hybrid_state(tag, tmp):
     return h, p, z, f
 
 
+def hybrid_arrays(h):
+    """The oracle's state `h` as the arrays of cicy_hybrid_state (Context.hybrid_electrical)."""
+    def csr(lists, dt=np.int32):
+        ptr = np.concatenate([[0], np.cumsum([len(x) for x in lists])]).astype(np.int64)
+        idx = np.array([v for x in lists for v in x], dtype=dt)
+        return ptr, idx
+
+    out = {"n_clusters": len(h["family"]), "family": np.array(h["family"], np.int32)}
+    for key, name in (("clusters_cnt", "clusters_cnt"), ("clusters_gnp", "clusters_gnp"), ("cluster_cnt_junctions", "cnt_junctions"),
+                      ("cluster_gnp_junctions", "gnp_junctions"), ("cluster_mix_junctions", "mix_junctions")):
+        out[name + "_ptr"], out[name + "_idx"] = csr(h[key])
+    for key, pre in (("junctions_cnt", "jc"), ("junctions_gnp", "jg"), ("junctions_mixed", "jm")):
+        j = h[key]
+        out[f"n_{key}"] = len(j)
+        out[pre + "_p1"] = np.array([x[0] for x in j], np.int64)
+        out[pre + "_n1"] = np.array([x[1] for x in j], np.int32)
+        out[pre + "_p2"] = np.array([x[2] for x in j], np.int64)
+        out[pre + "_n2"] = np.array([x[3] for x in j], np.int32)
+        out[pre + "_dist"] = np.array([x[4] for x in j], np.float64)
+    out["elements_ptr"], out["elements_idx"] = csr(h["elements"], np.int64)
+    out["n_gnps"] = len(h["gnp_t"])
+    out["n_points_gnp"] = len(h["points_gnp"])
+    out["points_gnp"] = np.array(h["points_gnp"], np.float64).ravel()
+    out["structure_gnp_ptr"], out["structure_gnp_idx"] = csr(h["structure_gnp"], np.int64)
+    out["pts_boundary_count"] = np.array([len(x) for x in h["pts_boundary"]], np.int32)
+    out["gnp_t"] = np.array(h["gnp_t"])
+    out["gnp_volume"] = np.array(h["gnp_volume"])
+    out["gnp_frame"] = np.array([np.concatenate([[l], np.ravel(c), np.ravel(r), np.ravel(n)]) for l, c, r, n in h["gnp_geom"]]).ravel()
+    out["boundary_gnp_ptr"], out["boundary_gnp_idx"] = csr(h["boundary_gnp"])
+    out["boundary_gnp_pts_ptr"], out["boundary_gnp_pts_idx"] = csr(h["boundary_gnp_pts"], np.int64)
+    return out
+
+
 def _check_system(S, z, pfx):
     nodes, res = z[pfx + "nodes"]
     assert (S["nodes"], S["reserved"]) == (nodes, res), pfx
