@@ -138,6 +138,30 @@ class HybridState(C.Structure):
     ]
 
 
+class MixedClustersList(C.Structure):
+    """cicy_mixed_clusters_list (borrowed view of a cicy_mixed_clusters result)."""
+    _fields_ = [("n_percolated", C.c_int32), ("family", _I32P),
+                ("clusters_cnt_ptr", _I64P), ("clusters_cnt_idx", _I32P), ("clusters_gnp_ptr", _I64P), ("clusters_gnp_idx", _I32P),
+                ("n_isolated_cnt", C.c_int32), ("isolated_cnt_ptr", _I64P), ("isolated_cnt_idx", _I32P),
+                ("n_isolated_gnp", C.c_int32), ("isolated_gnp_ptr", _I64P), ("isolated_gnp_idx", _I32P),
+                ("cnt_junctions_ptr", _I64P), ("cnt_junctions_idx", _I32P), ("gnp_junctions_ptr", _I64P), ("gnp_junctions_idx", _I32P),
+                ("mix_junctions_ptr", _I64P), ("mix_junctions_idx", _I32P),
+                ("structure_gnp_ptr", _I64P), ("structure_gnp_idx", _I64P),
+                ("pts_boundary_ptr", _I64P), ("pts_boundary_point", _I64P), ("pts_boundary_face", _I32P)]
+
+
+class MixedState(C.Structure):
+    """cicy_mixed_state: a mixed network after Make_mixed_clusters (host arrays)."""
+    _fields_ = [("n_labels", C.c_int32), ("n_cnts", C.c_int32), ("labels_cnt", _I32P), ("n_cnts_inside", C.c_int32), ("cnts_inside", _I32P),
+                ("n_gnps", C.c_int32), ("labels_gnp", _I32P), ("n_gnps_inside", C.c_int32), ("gnps_inside", _I32P),
+                ("boundary_cnt_ptr", _I64P), ("boundary_cnt_idx", _I32P), ("boundary_gnp_ptr", _I64P), ("boundary_gnp_idx", _I32P),
+                ("n_junctions_cnt", C.c_int64), ("jc_n1", _I32P), ("jc_n2", _I32P),
+                ("n_junctions_gnp", C.c_int64), ("jg_n1", _I32P), ("jg_n2", _I32P),
+                ("n_junctions_mixed", C.c_int64), ("jm_n1", _I32P), ("jm_n2", _I32P),
+                ("n_points_gnp", C.c_int64), ("structure_gnp_ptr", _I64P), ("structure_gnp_idx", _I64P),
+                ("pts_boundary_ptr", _I64P), ("pts_boundary_point", _I64P), ("pts_boundary_face", _I32P), ("bp_flags", _I32P)]
+
+
 class GnnSystem(C.Structure):
     _fields_ = [
         ("n", C.c_int32),
@@ -289,6 +313,9 @@ def lib() -> C.CDLL:
         "cicy_get_junctions": (C.c_int, [C.c_void_p, i64p, i64p, i32p, i64p, i32p, f64p]),
         "cicy_get_volumes": (C.c_int, [C.c_void_p, f64p, f64p, f64p, f64p]),
         "cicy_hybrid_electrical": (C.c_int, [C.c_void_p, P(HybridState), P(Params), C.c_double, C.c_double, P(Result)]),
+        "cicy_mixed_percolation": (C.c_int, [C.c_void_p, P(MixedState), P(C.c_void_p)]),
+        "cicy_mixed_clusters_view": (C.c_int, [C.c_void_p, P(MixedClustersList)]),
+        "cicy_mixed_clusters_free": (None, [C.c_void_p]),
         "cicy_get_hybrid_structure": (C.c_int, [C.c_void_p, i64p, i64p, i64p]),
         "cicy_get_hybrid_volumes": (C.c_int, [C.c_void_p, f64p]),
         "cicy_get_hybrid_junctions": (C.c_int, [C.c_void_p, C.c_int32, i64p, i32p, i64p, i32p]),

@@ -11,6 +11,10 @@ struct cicy_ctx {
     cicy::Ctx c;
 };
 
+struct cicy_mixed_clusters {
+    cicy::MixedClusters m;
+};
+
 namespace {
 
 template <class F>
@@ -305,6 +309,54 @@ cicy_status cicy_get_junctions(cicy_ctx* ctx, int64_t* n, int64_t* p1, int32_t* 
         sync(c);
     });
 }
+
+cicy_status cicy_mixed_percolation(cicy_ctx* ctx, const cicy_mixed_state* in, cicy_mixed_clusters** out) {
+    if (!out) return CICY_E_INPUT;
+    *out = nullptr;
+    cicy_mixed_clusters* h = new (std::nothrow) cicy_mixed_clusters;
+    if (!h) return CICY_E_INTERNAL;
+    const cicy_status st = guarded(ctx, [&](cicy::Ctx& c) {
+        if (!in) throw cicy::Fail{CICY_E_INPUT, "cicy_mixed_percolation: null argument"};
+        cicy::run_mixed_percolation(c, *in, h->m);
+    });
+    if (st != CICY_OK) {
+        delete h;
+        return st;
+    }
+    *out = h;
+    return CICY_OK;
+}
+
+cicy_status cicy_mixed_clusters_view(const cicy_mixed_clusters* h, cicy_mixed_clusters_list* v) {
+    if (!h || !v) return CICY_E_INPUT;
+    const cicy::MixedClusters& m = h->m;
+    v->n_percolated = (int32_t)m.family.size();
+    v->family = m.family.data();
+    v->clusters_cnt_ptr = m.clu_cnt_ptr.data();
+    v->clusters_cnt_idx = m.clu_cnt.data();
+    v->clusters_gnp_ptr = m.clu_gnp_ptr.data();
+    v->clusters_gnp_idx = m.clu_gnp.data();
+    v->n_isolated_cnt = (int32_t)m.iso_cnt_ptr.size() - 1;
+    v->isolated_cnt_ptr = m.iso_cnt_ptr.data();
+    v->isolated_cnt_idx = m.iso_cnt.data();
+    v->n_isolated_gnp = (int32_t)m.iso_gnp_ptr.size() - 1;
+    v->isolated_gnp_ptr = m.iso_gnp_ptr.data();
+    v->isolated_gnp_idx = m.iso_gnp.data();
+    v->cnt_junctions_ptr = m.jc_ptr.data();
+    v->cnt_junctions_idx = m.jc.data();
+    v->gnp_junctions_ptr = m.jg_ptr.data();
+    v->gnp_junctions_idx = m.jg.data();
+    v->mix_junctions_ptr = m.jm_ptr.data();
+    v->mix_junctions_idx = m.jm.data();
+    v->structure_gnp_ptr = m.st_ptr.data();
+    v->structure_gnp_idx = m.st_idx.data();
+    v->pts_boundary_ptr = m.pb_ptr.data();
+    v->pts_boundary_point = m.pb_point.data();
+    v->pts_boundary_face = m.pb_face.data();
+    return CICY_OK;
+}
+
+void cicy_mixed_clusters_free(cicy_mixed_clusters* h) { delete h; }
 
 cicy_status cicy_hybrid_electrical(cicy_ctx* ctx, const cicy_hybrid_state* st, const cicy_params* p, double resistivity_gnp_surf,
                                    double resistivity_gnp_t, cicy_result* out) {

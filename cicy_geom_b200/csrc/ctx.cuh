@@ -194,11 +194,22 @@ struct Ctx {
     ~Ctx();
 };
 
+// Public members of Hoshen_Kopelman after Determine_clusters_and_percolation for a mixed
+// network (host copies, CSR with int64 offsets), as cicy_mixed_percolation returns them.
+struct MixedClusters {
+    std::vector<int32_t> family;
+    std::vector<int64_t> clu_cnt_ptr, clu_gnp_ptr, iso_cnt_ptr, iso_gnp_ptr, jc_ptr, jg_ptr, jm_ptr, st_ptr, pb_ptr;
+    std::vector<int32_t> clu_cnt, clu_gnp, iso_cnt, iso_gnp, jc, jg, jm, pb_face;
+    std::vector<int64_t> st_idx, pb_point;
+};
+
 // Stage entry points (throw Fail on error).
 void upload_network(Ctx& c, const cicy_network& net);
 void run_contact_grid(Ctx& c, const cicy_params& p);
 void run_clusters(Ctx& c, const cicy_params& p);
 void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out);
+// Clusters and percolation of a mixed CNT/GNP network (mixed_percolation.cu).
+void run_mixed_percolation(Ctx& c, const cicy_mixed_state& in, MixedClusters& out);
 // Electrical_analysis::Perform_analysis_on_clusters for a mixed CNT/GNP network (hybrid_dea.cuh).
 void run_hybrid_electrical(Ctx& c, const cicy_hybrid_state& h, const cicy_params& p, double rho_gnp_surf, double rho_gnp_t,
                            cicy_result* out);

@@ -467,7 +467,7 @@ def gnp_junction_points(directory: str, a, b, vdw: float, sample, allow_simplex3
 
 
 def gnp_contact_pairs(directory: str, inside, window, gs_min, overlap_cnt: float, overlap_gnp: float, vdw: float, tunnel: float,
-                      sample=None, allow_simplex3: bool = False, n_labels_cnt=None, tol_gnp2=None, device: int = 0) -> dict:
+                      sample=None, allow_simplex3: bool = False, n_labels_cnt=None, tol_gnp2=None, device: int = 0, init=None) -> dict:
     """GNP-GNP contact pass of Label_gnps_in_window on the device: the GNP region
     lists (cicy_gnp_sectioned_domain of `inside`) and every pair sharing a region,
     measured once, with the junction points of each contact
@@ -479,7 +479,9 @@ def gnp_contact_pairs(directory: str, inside, window, gs_min, overlap_cnt: float
     n_total_labels; with `tol_gnp2`, also the GNP point structures of
     Add_gnp_junction (cicy_gnp_junction_structures, no initial points):
     gnp_points [m, 3], structure_ptr, structure_idx, junctions [k, 4] (Pa, GNPa,
-    Pb, GNPb), junction_dist."""
+    Pb, GNPb), junction_dist; `init` = (points [m, 3], structure_ptr, structure_idx)
+    gives the initial points and lists (the window's boundary points) and adds
+    boundary_used (bp_flags)."""
     h = C.c_void_p()
     check(lib().cicy_read_gnps(directory.encode(), C.byref(h)), "cicy_read_gnps")
     grid, pairs = C.c_void_p(), C.c_void_p()
@@ -513,8 +515,18 @@ def gnp_contact_pairs(directory: str, inside, window, gs_min, overlap_cnt: float
             gv = _abi.Gnps()
             check(lib().cicy_gnp_set_view(h, C.byref(gv)), "cicy_gnp_set_view")
             pts = C.c_void_p()
-            check(lib().cicy_gnp_junction_structures(device, pairs, gv.n, float(tol_gnp2), 0, None, None, None, C.byref(pts)),
-                  "cicy_gnp_junction_structures")
+            if init is None:
+                check(lib().cicy_gnp_junction_structures(device, pairs, gv.n, float(tol_gnp2), 0, None, None, None, C.byref(pts)),
+                      "cicy_gnp_junction_structures")
+            else:
+                ip = np.ascontiguousarray(init[0], dtype=np.float64)
+                iptr = np.ascontiguousarray(init[1], dtype=np.int32)
+                iidx = np.ascontiguousarray(init[2], dtype=np.int32)
+                if iidx.size == 0:
+                    iidx = np.zeros(1, np.int32)
+                check(lib().cicy_gnp_junction_structures(device, pairs, gv.n, float(tol_gnp2), len(ip), ip.ctypes.data_as(_abi.f64p),
+                                                         iptr.ctypes.data_as(_abi.i32p), iidx.ctypes.data_as(_abi.i32p), C.byref(pts)),
+                      "cicy_gnp_junction_structures")
             try:
                 pv = _abi.GnpPointList()
                 check(lib().cicy_gnp_points_view(pts, C.byref(pv)), "cicy_gnp_points_view")
@@ -524,6 +536,7 @@ def gnp_contact_pairs(directory: str, inside, window, gs_min, overlap_cnt: float
                             "junctions": arr(pv.junctions, C.c_int32, 4 * nj, np.int32).reshape(nj, 4),
                             "junction_dist": arr(pv.junction_dist, C.c_double, nj, np.float64)})
                 res["structure_idx"] = arr(pv.structure_idx, C.c_int32, int(res["structure_ptr"][-1]), np.int32)
+                res["boundary_used"] = arr(pv.boundary_used, C.c_int32, int(pv.n_boundary), np.int32)
             finally:
                 lib().cicy_gnp_points_free(pts)
         return {**res, "a": arr(v.a, C.c_int32, n, np.int32), "b": arr(v.b, C.c_int32, n, np.int32),

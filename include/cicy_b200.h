@@ -190,6 +190,54 @@ cicy_status cicy_electrical_analysis(cicy_ctx* ctx, const cicy_params* p, cicy_r
 /* All three stages (App_Network_3D.cpp:140-179 for one window). */
 cicy_status cicy_network_to_conductance(cicy_ctx* ctx, const cicy_params* p, cicy_result* out);
 
+/* ---------------- clusters and percolation of a mixed CNT/GNP network ----------------
+ * The state Determine_clusters_and_percolation has for GNP_CNT_mix after Make_mixed_clusters
+ * (host arrays, copied): mixed labels of CNTs and GNPs (-1: no cluster), the particles
+ * inside the window, the face lists of Cutoff_Wins, the particle pairs of every junction
+ * kind, and the GNP point lists with their boundary points (point, face) and the
+ * junction-point flags of Add_gnp_junction (bp_flags). */
+typedef struct {
+    int32_t n_labels;
+    int32_t n_cnts; const int32_t* labels_cnt;
+    int32_t n_cnts_inside; const int32_t* cnts_inside;
+    int32_t n_gnps; const int32_t* labels_gnp;
+    int32_t n_gnps_inside; const int32_t* gnps_inside;
+    const int64_t* boundary_cnt_ptr; const int32_t* boundary_cnt_idx;   /* 6 faces */
+    const int64_t* boundary_gnp_ptr; const int32_t* boundary_gnp_idx;   /* 6 faces */
+    int64_t n_junctions_cnt; const int32_t* jc_n1; const int32_t* jc_n2;
+    int64_t n_junctions_gnp; const int32_t* jg_n1; const int32_t* jg_n2;
+    int64_t n_junctions_mixed; const int32_t* jm_n1; const int32_t* jm_n2; /* CNT, GNP */
+    int64_t n_points_gnp;
+    const int64_t* structure_gnp_ptr; const int64_t* structure_gnp_idx;
+    const int64_t* pts_boundary_ptr; const int64_t* pts_boundary_point; const int32_t* pts_boundary_face;
+    const int32_t* bp_flags;
+} cicy_mixed_state;
+typedef struct cicy_mixed_clusters cicy_mixed_clusters;
+/* Upstream's public members after Determine_clusters_and_percolation (borrowed, valid until
+ * cicy_mixed_clusters_free).  Lists as CSR; junction groups index the junction arrays;
+ * structure_gnp and pts_boundary as Remove_gnp_points_in_non_relevant_boundaries leaves them. */
+typedef struct {
+    int32_t n_percolated;
+    const int32_t* family;
+    const int64_t* clusters_cnt_ptr; const int32_t* clusters_cnt_idx;
+    const int64_t* clusters_gnp_ptr; const int32_t* clusters_gnp_idx;
+    int32_t n_isolated_cnt; const int64_t* isolated_cnt_ptr; const int32_t* isolated_cnt_idx;
+    int32_t n_isolated_gnp; const int64_t* isolated_gnp_ptr; const int32_t* isolated_gnp_idx;
+    const int64_t* cnt_junctions_ptr; const int32_t* cnt_junctions_idx;
+    const int64_t* gnp_junctions_ptr; const int32_t* gnp_junctions_idx;
+    const int64_t* mix_junctions_ptr; const int32_t* mix_junctions_idx;
+    const int64_t* structure_gnp_ptr; const int64_t* structure_gnp_idx;
+    const int64_t* pts_boundary_ptr; const int64_t* pts_boundary_point; const int32_t* pts_boundary_face;
+} cicy_mixed_clusters_list;
+/* Make_particle_clusters for CNTs and GNPs, Find_percolated_clusters with CNT and GNP faces
+ * (direction codes 10 d + 1, families by their sum), Group_junctions for the three junction
+ * kinds and Remove_gnp_points_in_non_relevant_boundaries (Hoshen_Kopelman.cpp:17-201,
+ * 2331-2903), on the device.  A junction whose particles carry different labels is
+ * CICY_E_INPUT, as upstream's error. */
+cicy_status cicy_mixed_percolation(cicy_ctx* ctx, const cicy_mixed_state* in, cicy_mixed_clusters** out);
+cicy_status cicy_mixed_clusters_view(const cicy_mixed_clusters* h, cicy_mixed_clusters_list* view);
+void cicy_mixed_clusters_free(cicy_mixed_clusters* h);
+
 /* ---------------- electrical stage of a mixed CNT/GNP network (GNP_CNT_mix) ----------------
  * Upstream's public members after Hoshen_Kopelman::Determine_clusters_and_percolation
  * and Cutoff_Wins for a mixed network (Hoshen_Kopelman.h:27-51, Cutoff_Wins.h), the

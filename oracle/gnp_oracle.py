@@ -1019,6 +1019,29 @@ def mixed_percolation(n_clusters, cnts_inside, gnps_inside, labels_cnt, labels_g
     return out
 
 
+RELEVANT = {0: (2, 4), 1: (3, 5), 2: (0, 1), 3: (2, 4, 3, 5), 4: (2, 4, 0, 1), 5: (3, 5, 0, 1)}  # Get_vector_with_relevant_boundaries
+
+
+def remove_nonrelevant_boundary_points(clusters_gnp, family, pts_boundary, structure, bp_flags):
+    """Remove_gnp_points_in_non_relevant_boundaries (Hoshen_Kopelman.cpp:2740-2903): in a
+    cluster of family 0-5, a GNP's boundary point on a face the family does not use, and not
+    a junction point (bp_flags), leaves the GNP's point list and its boundary points.  Lists
+    are changed in place."""
+    for i, cl in enumerate(clusters_gnp):
+        if family[i] == 6:
+            continue
+        rb = RELEVANT[family[i]]
+        for g in cl:
+            relevant = []
+            for P, b in pts_boundary[g]:
+                if b in rb or bp_flags[P]:
+                    relevant.append((P, b))
+                elif P in structure[g]:
+                    structure[g].remove(P)
+            if len(relevant) < len(pts_boundary[g]):
+                pts_boundary[g] = relevant
+
+
 def gnp_resistance(P1, P2, rad1: float, rad2: float, rho_surf: float, rho_t: float):
     """Direct_Electrifying::Calculate_resistance_gnp (Direct_Electrifying.cpp:1198-1232):
     R = rho L / (pi r1 r2) with rho = u . (u_x rho_surf, u_y rho_surf, u_z rho_t),

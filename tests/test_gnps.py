@@ -508,7 +508,7 @@ def test_hybrid_chain_matches_upstream_flow(tmp_path, tag):
     p = {"gs_min": (M.GS_MIN,) * 3, "gs_overlap_cnt": M.OVERLAP_CNT, "gs_overlap_gnp": ovg, "vdw": vdw, "tunnel": tun, "min_points": 5}
     n, l, regs = O.contact_grid(a, p)
     lab_cnt, n_cnt, pc, ce = O.label_cnts(a, p, regs)
-    jc, _ = O.compress_junctions(a, p, pc, ce)
+    jc, el_cnt = O.compress_junctions(a, p, pc, ce)
     Vg = read_gnps(d)
     sd_gnp = G.fill_sectioned_domain_gnps(a["window"], Vg["vertices"], Vg["l"], Vg["t"], gw["gnps_inside"], n, l, ovg)
     V, F = Vg["vertices"].tolist(), Vg["planes"].tolist()
@@ -525,13 +525,38 @@ def test_hybrid_chain_matches_upstream_flow(tmp_path, tag):
     mix = G.find_adjacent_labels(np.stack([a["x"], a["y"], a["z"]], 1).tolist(), a["flag"], a["radii"], regs, sd_gnp, V, F, vdw, tun)
     order = sorted(mix.items(), key=lambda kv: kv[1][0])
     mc, mg, nm = G.mixed_labels(lab_cnt, lab_gnp, n_total, [(int(a["flag"][P]), g) for (P, g), _ in order])
-    _, _, jm, _ = G.compress_mixed_contacts(mix, a["flag"], 5, pts, st)
+    _, st_mix, jm, el_mix = G.compress_mixed_contacts(mix, a["flag"], 5, pts, st)
     res = G.mixed_percolation(nm, a["cnts_inside"], gw["gnps_inside"], mc, mg, bc, bg, [(j[1], j[3]) for j in jc], [(j[1], j[3]) for j in jg],
                               [(j[1], j[3]) for j in jm])
     assert res["family"] == list(z["flow_family"]) and len(res["family"]) >= 1
     for key in ("clusters_cnt", "clusters_gnp", "isolated_cnt", "isolated_gnp", "cluster_cnt_junctions", "cluster_gnp_junctions",
                 "cluster_mix_junctions"):
         assert res[key] == [list(x) for x in csr(z, "flow_" + key)], key
+    # Remove_gnp_points_in_non_relevant_boundaries: the point lists and boundary points the
+    # electrical stage starts from (upstream's, tests/golden/gnp_hybrid_electrical.npz)
+    _, _, _, bp = G.add_gnp_junctions(cts, NG, tol * tol, [tuple(q) for q in gw["points"]],
+                                      [gw["structure_idx"][sp[g]:sp[g + 1]].tolist() for g in range(NG)])
+    bpp, bpi = gw["boundary_pts_ptr"], gw["boundary_pts_idx"]
+    pb = [[] for _ in range(NG)]
+    for P, g, b in zip(range(len(gw["point_gnp"])), gw["point_gnp"], gw["point_boundary"]):
+        if b >= 0:
+            pb[int(g)].append((P, int(b)))
+    st2 = [list(x) for x in st_mix]
+    G.remove_nonrelevant_boundary_points(res["clusters_gnp"], res["family"], pb, st2, bp)
+    ez = {k[2:]: v for k, v in np.load(os.path.join(ROOT, "tests", "golden", "gnp_hybrid_electrical.npz")).items() if k.startswith(tag + "_")}
+    assert st2 == [list(x) for x in csr(ez, "e_structure_gnp_start")]
+    epb = csr(ez, "e_pts_boundary")
+    assert [[v for q in x for v in q] for x in pb] == [list(x) for x in epb]
+    # elements_cnt: the CNT junctions' points, every mixed junction's CNT point, then
+    # Complete_cnt_elements (after Make_mixed_clusters for GNP_CNT_mix) adds the end points
+    elems = [set(el_cnt.get(c, ())) for c in range(len(a["radii"]))]
+    for c, P in el_mix:
+        elems[c].add(P)
+    sp_c, si_c = a["structure_ptr"], a["structure_idx"]
+    for c in range(len(elems)):
+        if elems[c]:
+            elems[c] |= {int(si_c[sp_c[c]]), int(si_c[sp_c[c + 1] - 1])}
+    assert [sorted(e) for e in elems] == [list(x) for x in csr(ez, "e_elements_start")]
 
 
 def test_hybrid_flow_golden_carries_upstream_resistances():

@@ -52,3 +52,45 @@ def test_hybrid_electrical_on_device_matches_upstream(cuda_ok, tmp_path, tag):
     assert [list(bi[bp[c]:bp[c + 1]]) for c in range(len(bp) - 1)] == _csr(z, f"e_c{nclu - 1}_bb_elements")
     assert ctx.hybrid_volumes().tolist() == z["e_bn_volumes"].tolist()
     np.testing.assert_allclose(np.array(r.resistances), z["flow_resistances"], rtol=1e-6)
+
+
+@pytest.mark.parametrize("tag", ["s", "m"])
+def test_hybrid_chain_on_device_matches_upstream_flow(cuda_ok, tmp_path, tag):
+    """The whole GNP_CNT_mix path on the device from the network files
+    (cicy_geom_b200.hybrid): window extraction, contact grid, CNT, GNP and mixed
+    contacts and labels, mixed percolation (clusters, isolated particles, families,
+    junction groups, equal to upstream's) and the electrical stage, whose
+    resistances agree with upstream's end-to-end run (tests/golden/gnp_hybrid_flow.npz)."""
+    import os
+    import sys
+
+    from cicy_geom_b200.hybrid import hybrid_network_to_conductance
+    from cicy_geom_b200.network import generate_gnps, write_gnp_file
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, os.path.join(root, "tests", "golden"))
+    import make_gnp_golden as M
+
+    fz = dict(np.load(os.path.join(root, "tests", "golden", "gnp_hybrid_flow.npz")))
+    f = {k[2:]: v for k, v in fz.items() if k.startswith(tag + "_")}
+    d = str(tmp_path)
+    if tag == "m":
+        M.hybrid_network(d)
+        write_gnp_file(d, generate_gnps(M.N, M.SIDE, M.SEED))
+        cfg = M.cnt_config()
+    else:
+        M.sparse_network(d)
+        write_gnp_file(d, generate_gnps(M.SPARSE_N, M.SIDE, M.SPARSE_SEED, l_range=(0.3, 0.5)))
+        cfg = M.sparse_config()
+    cfg.resistances = (1, 0, 0)
+    r, ctx, st = hybrid_network_to_conductance(d, cfg, float(M.OVERLAP_GNP))
+    mc = st["mixed"]
+    assert mc["family"].tolist() == f["flow_family"].tolist()
+    for key in ("clusters_cnt", "clusters_gnp", "isolated_cnt", "isolated_gnp"):
+        got = [list(mc[key + "_idx"][mc[key + "_ptr"][k]:mc[key + "_ptr"][k + 1]]) for k in range(len(mc[key + "_ptr"]) - 1)]
+        assert got == _csr(f, "flow_" + key), key
+    for key, fk in (("cnt_junctions", "cluster_cnt_junctions"), ("gnp_junctions", "cluster_gnp_junctions"), ("mix_junctions", "cluster_mix_junctions")):
+        got = [list(mc[key + "_idx"][mc[key + "_ptr"][k]:mc[key + "_ptr"][k + 1]]) for k in range(len(mc[key + "_ptr"]) - 1)]
+        want = _csr(f, "flow_" + fk)
+        assert got == want or (want == [] and all(not g for g in got)), key
+    np.testing.assert_allclose(np.array(r.resistances), f["flow_resistances"], rtol=1e-6)
