@@ -768,81 +768,56 @@ GNP_DUMP = os.path.join(ROOT, "oracle", "_ref", "gnp_dump")
 
 def run_hybrid(args):
     """Hybrid CNT/GNP sample (4 um cube, 8,000 CNTs, 1,500 GNPs of side U[0.5, 1]
-    um and thickness 10 nm, seeded): one step is the contact and cluster stages
-    of Determine_clusters_and_percolation for GNP_CNT_mix on the device --
-    contact grid (CNT and GNP region lists), CNT contacts and labels, the GNP-GNP
-    contact pass with GJK/EPA and junction points, GNP labels and point
-    structures, the CNT-GNP contacts, Compress_mixed_contacts and the mixed
-    labels.  Stages are timed on the host around the synchronous C-ABI calls
-    (their host<->device copies included).  The upstream program
-    (oracle/_ref/gnp_dump) times the same upstream calls on one host core; the
-    mixed labels are compared with it."""
-    from cicy_geom_b200 import _abi
-    from cicy_geom_b200.device import Context
-    from cicy_geom_b200.network import (HostNetwork, NetworkConfig, generate_cnt_network, generate_gnps, gnp_contact_pairs,
-                                        write_gnp_file, write_read_network_files)
+    um and thickness 10 nm, seeded): one step is the whole GNP_CNT_mix path of
+    window 0 on the device (cicy_geom_b200.hybrid): window extraction, contact
+    grid, CNT / GNP / CNT-GNP contacts and labels, mixed percolation and the
+    electrical stage (unit-resistor DEA, CNT+GNP backbone, real-resistor DEA
+    along x, R_x).  Stages are timed on the host around the synchronous C-ABI
+    calls (their host<->device copies included).  The upstream program
+    (oracle/_ref/gnp_dump, flow mode) runs the same stages on one host core; its
+    resistance is compared with this one."""
+    from cicy_geom_b200.hybrid import hybrid_network_to_conductance
+    from cicy_geom_b200.network import NetworkConfig, generate_cnt_network, generate_gnps, write_gnp_file, write_read_network_files
     from oracle.dumpio import read_dump
 
     side = HYBRID_SIDE
-    cfg = NetworkConfig(side=side, n_cnts=HYBRID_CNTS, seed=HYBRID_SEED)
-    gs, vdw, tunnel = cfg.gs_min, cfg.vdw, cfg.tunnel
-    ov_cnt, ov_gnp = 2 * cfg.radius + tunnel, gs / np.sqrt(8.0)
-    win = [0.0, 0.0, 0.0, side, side, side, side, side, side]
+    cfg = NetworkConfig(side=side, n_cnts=HYBRID_CNTS, seed=HYBRID_SEED, resistances=(1, 0, 0))
+    ov_gnp = cfg.gs_min / np.sqrt(8.0)  # Input_Reader.cpp:1368
     d = tempfile.mkdtemp(prefix="cicy_hybrid_")
-    host = generate_cnt_network(cfg)
-    write_read_network_files(d, host, cfg)
-    gnps = generate_gnps(HYBRID_GNPS, side, HYBRID_SEED + 1)
-    write_gnp_file(d, gnps)
-    arrs = {k: v for k, v in host.arrays().items() if not k.startswith("boundary")}
-    arrs["cnts_inside"] = np.arange(len(arrs["radii"]), dtype=np.int32)
-    arrs["window"] = np.array(win)
-    net = HostNetwork.from_arrays(arrs)
-    p = cfg.params()
-    p.gs_overlap_gnp = ov_gnp
-    tol = 1.5 * float(np.max(gnps["t"]))
-    names = ["contact_grid_cnt", "cnt_clusters", "gnp_pairs_junctions_labels", "cnt_gnp_contacts", "mixed_junctions", "mixed_labels"]
-    times = {k: [] for k in names}
-    out = {}
-    with Context(0) as ctx:
-        for step in range(args.warmup + args.steps):
-            t = [time.perf_counter()]
-            ctx.upload(net)
-            ctx.contact_grid(p)
-            t.append(time.perf_counter())
-            ctx.clusters(p)
-            lab_cnt, n_cnt = ctx.labels()
-            t.append(time.perf_counter())
-            gp = gnp_contact_pairs(d, np.arange(HYBRID_GNPS), win, [gs] * 3, ov_cnt, ov_gnp, vdw, tunnel, n_labels_cnt=n_cnt, tol_gnp2=tol * tol)
-            t.append(time.perf_counter())
-            pt, _, _, _ = ctx.gnp_cnt_contacts(d, p)
-            t.append(time.perf_counter())
-            mj = ctx.mixed_junctions(len(gp["gnp_points"]), cfg.min_points)
-            t.append(time.perf_counter())
-            mc, mg, nm = ctx.mixed_labels(gp["labels_gnp"], gp["n_total_labels"])
-            t.append(time.perf_counter())
-            if step >= args.warmup:
-                for k, name in enumerate(names):
-                    times[name].append(t[k + 1] - t[k])
-            out = {"cnt_labels": int(n_cnt), "gnp_contact_pairs": int(len(gp["a"])), "gnp_junctions": int(len(gp["junctions"])),
-                   "cnt_gnp_contacts": int(len(pt)), "mixed_junctions": int(len(mj["dist"])), "mixed_clusters": int(nm)}
-    stage_ms = {k: 1e3 * statistics.median(v) for k, v in times.items()}
-    step_s = sum(stage_ms.values()) / 1e3
-    line = {"metric": "hybrid CNT/GNP contact + cluster stages per second (4 um, 8,000 CNTs, 1,500 GNPs)", "value": 1.0 / step_s,
-            "unit": "samples/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * step_s,
+    write_read_network_files(d, generate_cnt_network(cfg), cfg)
+    write_gnp_file(d, generate_gnps(HYBRID_GNPS, side, HYBRID_SEED + 1))
+    times, R = [], None
+    for step in range(args.warmup + args.steps):
+        tm = {}
+        r, ctx, st = hybrid_network_to_conductance(d, cfg, ov_gnp, timings=tm)
+        R = list(r.resistances)
+        if step >= args.warmup:
+            times.append(tm)
+        sv = [(int(x.nodes), int(x.iterations)) for x in r.solves[: r.n_solves]]
+        ctx.close()
+    stage_ms = {k: 1e3 * statistics.median(t[k] for t in times) for k in times[0]}
+    step_s = statistics.median(sum(t.values()) for t in times)
+    line = {"metric": "hybrid CNT/GNP networks solved per second (4 um, 8,000 CNTs, 1,500 GNPs, whole path to R_x)", "value": 1.0 / step_s,
+            "unit": "networks/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * step_s,
             "higher_is_better": True, "dtype": "f64", "data": "synthetic (seeded CNT polylines and GNPs)",
-            "config": {"workload": "hybrid 4um 8000 CNTs + 1500 GNPs", "points": int(host.n_points)}, "stage_ms": stage_ms, "counts": out,
+            "config": {"workload": "hybrid 4um 8000 CNTs + 1500 GNPs, window 0 = the sample, R along x, CG to 1e-10"},
+            "stage_ms": stage_ms, "R_x": R[0], "solves": sv, "percolated": int(st["mixed"]["n_percolated"]),
             "timing": "host wall clock around synchronous C-ABI calls, median over steps"}
     if os.path.exists(GNP_DUMP):
-        r = subprocess.run([GNP_DUMP, d, os.path.join(d, "ref.bin"), repr(vdw), repr(tunnel), repr(gs), repr(ov_cnt), repr(float(ov_gnp))],
-                           capture_output=True, timeout=900)
+        r = subprocess.run([GNP_DUMP, d, os.path.join(d, "ref.bin"), repr(cfg.vdw), repr(cfg.tunnel), repr(cfg.gs_min),
+                            repr(2 * cfg.radius + cfg.tunnel), repr(float(ov_gnp)), "-1", "flow", repr(cfg.step), "electrical_time"],
+                           capture_output=True, timeout=1800)
         if r.returncode == 0:
             z = read_dump(os.path.join(d, "ref.bin"))
-            ref = [float(x) for x in z["ref_seconds"]]
-            line["cpu_baseline"] = {"value": 1.0 / sum(ref), "unit": "samples/s", "cores": 1, "kind": "reference",
-                                    "sample": "the upstream calls Generate_contact_grid (GNP_CNT_mix), Make_cnt_clusters, Make_gnp_clusters, "
-                                              "Make_mixed_clusters on the same sample",
+            ref = [float(x) for x in z["flow_seconds"]]
+            line["cpu_baseline"] = {"value": 1.0 / sum(ref), "unit": "networks/s", "cores": 1, "kind": "reference",
+                                    "sample": "upstream's GNP_CNT_mix stages on the same files (window extraction, Generate_contact_grid, "
+                                              "Determine_clusters_and_percolation, Perform_analysis_on_clusters along x), one thread",
                                     "stage_seconds": ref}
-            line["labels_match_upstream"] = bool(np.array_equal(mc, z["mixlab_cnt"]) and np.array_equal(mg, z["mixlab_gnp"]))
+            line["R_x_reference"] = float(z["flow_resistances"][0])
+            line["R_x_rel_diff"] = abs(R[0] - line["R_x_reference"]) / abs(line["R_x_reference"])
+        else:
+            line["cpu_baseline_error"] = r.stderr.decode(errors="replace")[-300:]
     print(json.dumps(line))
     return 0
 

@@ -53,7 +53,9 @@
  * Determine_clusters_and_percolation) and dumps the clusters, families and
  * junction groups (flow_* records); with "electrical" after the step length,
  * also Electrical_analysis::Perform_analysis_on_clusters along x and the
- * resistances it writes.
+ * resistances it writes, then a stage-by-stage replay of it (e_* records);
+ * "electrical_time" skips the replay.  flow_seconds: steady_clock time of the
+ * window extraction, contact grid, clusters and percolation, electrical stage.
  *
  * With a gnp_resistor_cases.dat in the directory it evaluates upstream's
  * Direct_Electrifying::Calculate_resistance_gnp on each case (gnp_resistances).
@@ -529,6 +531,10 @@ int main(int argc, char** argv) {
         // (App_Network_3D.cpp:120-180): Shells, Cutoff_Wins::Extract_observation_window,
         // Contact_grid::Generate_contact_grid, Hoshen_Kopelman::Determine_clusters_and_percolation
         // (CNT points inside a GNP ignored), with min_points 5 and tol_gnp = 1.5 t_max.
+        using fclk = std::chrono::steady_clock;
+        auto fsecs = [](fclk::time_point a, fclk::time_point b) { return std::chrono::duration<double>(b - a).count(); };
+        std::vector<double> flow_seconds;  // window extraction, contact grid, clusters and percolation, electrical analysis
+        auto ft0 = fclk::now();
         Geom_sample gw = geom;
         gw.win_max_x = gw.win_min_x = geom.sample.len_x;
         gw.win_max_y = gw.win_min_y = geom.sample.wid_y;
@@ -555,8 +561,12 @@ int main(int argc, char** argv) {
         std::vector<Point_3D> pg;
         Cutoff_Wins CW;
         if (!CW.Extract_observation_window(0, "GNP_CNT_mix", gw, win, cg, gf, structure, radii, pts, shells_cnt, shells_gnp, sg, pg)) return 22;
+        auto ft1 = fclk::now();
+        flow_seconds.push_back(fsecs(ft0, ft1));
         Contact_grid CGf;
         if (!CGf.Generate_contact_grid(0, "GNP_CNT_mix", gw, win, CW.cnts_inside, pts, structure, CW.gnps_inside, gf)) return 23;
+        auto ft2 = fclk::now();
+        flow_seconds.push_back(fsecs(ft1, ft2));
         Simu_para sp;
         sp.particle_type = "GNP_CNT_mix";
         sp.allow_simplex3 = false;
@@ -573,6 +583,8 @@ int main(int argc, char** argv) {
         if (!HF.Determine_clusters_and_percolation(0, geom.sample, sp, cf, vf, CW.cnts_inside, CGf.sectioned_domain_cnts, structure, pts, radii,
                                                    CW.boundary_cnt, CW.gnps_inside, CGf.sectioned_domain_gnps, gf, CW.boundary_gnp, sg, pg))
             return 24;
+        auto ft3 = fclk::now();
+        flow_seconds.push_back(fsecs(ft2, ft3));
         o.i32("flow_cnts_inside", CW.cnts_inside);
         o.i32("flow_gnps_inside", CW.gnps_inside);
         dump_csr(o, "flow_boundary_cnt", CW.boundary_cnt);
@@ -589,7 +601,8 @@ int main(int argc, char** argv) {
         std::vector<double> xyz;
         for (const Point_3D& q : pg) xyz.insert(xyz.end(), {q.x, q.y, q.z});
         o.f64("flow_points_gnp", xyz);
-        if (argc >= 12 && std::string(argv[11]) == "electrical") {
+        if (argc >= 12 && (std::string(argv[11]) == "electrical" || std::string(argv[11]) == "electrical_time")) {
+            const bool staged = std::string(argv[11]) == "electrical";  // "electrical_time": the timed calls only
             // Electrical_analysis::Perform_analysis_on_clusters along x (unit-resistor pass, backbone,
             // real pass), the parameters of the hybrid configuration: rho_CNT 1e-3, GNP in-plane 1e-4
             // and through-plane 1 Ohm um, exponential tunnelling junctions (Input_Reader.cpp:1445-1456),
@@ -621,10 +634,13 @@ int main(int argc, char** argv) {
             std::vector<GNP> gs = gf;
             std::vector<std::vector<long int> > ss = sg;
             Electrical_analysis EA;
+            auto ft4 = fclk::now();
             if (!EA.Perform_analysis_on_clusters(0, win, sp, ep, cf, vf, of, &HF, &CW, structure, pts, radii, pg, sg, gf)) return 25;
+            flow_seconds.push_back(fsecs(ft4, fclk::now()));
+            o.f64("flow_seconds", flow_seconds);
             // ---- staged replay of Perform_analysis_on_clusters (Electrical_analysis.cpp:10-145) and
             // Electrical_resistance_along_each_percolated_direction (:229-289), dumping each stage (e_*)
-            {
+            if (staged) {
                 std::vector<std::vector<long int> > pb;  // GNP boundary points kept by Remove_gnp_points_in_non_relevant_boundaries
                 for (const GNP& g : gs) {
                     std::vector<long int> v;
