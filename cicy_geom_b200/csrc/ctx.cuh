@@ -176,6 +176,7 @@ struct Ctx {
     DBuf<int32_t> vol_kind;
     DBuf<uint64_t> vol_key;
     DBuf<uint32_t> vol_cnt;
+    DBuf<double> vol_iso;               // whole-CNT volumes of the isolated list
     bool have_volumes = false;
     HybridDev* hy = nullptr;  // mixed CNT/GNP electrical stage (cicy_hybrid_electrical)
     bool have_hybrid = false;

@@ -838,7 +838,7 @@ void run_hybrid_electrical(Ctx& c, const cicy_hybrid_state& h, const cicy_params
         k_backbone_cnts<<<grid_for(NM), 256, 0, s>>>(NM, members, eb.get(), ee.get(), c.elem_idx.get(), c.lmm.get(), su->volt.get(),
                                                    c.imax.get(), 1, c.bb_lo.get(), c.bb_hi.get(), c.alive.get(), c.radii.get(), c.x.get(),
                                                    c.y.get(), c.z.get(), c.vol3.get(), c.vol_kind.get());
-        k_volume_sum<<<1, 32, 0, s>>>(NM, fam, c.vol3.get(), c.vol_kind.get(), c.vol_acc.get());
+        k_volume_sum<<<1, kSumThreads, 0, s>>>(NM, fam, c.vol3.get(), c.vol_kind.get(), c.vol_acc.get());
         c.launches += 4;
         NM = compact_list(c, members, NM, c.alive, c.alive_scan, c.tmp_list);  // Find_backbone_cnts drops dead CNTs
         if (ng > 0) {  // Find_backbone_gnps (:577-660)
@@ -958,7 +958,7 @@ void run_hybrid_electrical(Ctx& c, const cicy_hybrid_state& h, const cicy_params
                                                                  c.bb_lo.get(), c.bb_hi.get(), c.elem_idx.get(), c.lmm.get(), sr->volt.get(),
                                                                  c.radii.get(), p.resistivity_cnt, c.x.get(), c.y.get(), c.z.get(),
                                                                  c.bterm.get(), c.bvalid.get());
-                k_boundary_sum<<<1, 32, 0, s>>>(2 * nb, c.bterm.get(), c.bvalid.get(), c.cur_out.get());
+                k_boundary_sum<<<1, kSumThreads, 0, s>>>(2 * nb, c.bterm.get(), c.bvalid.get(), c.cur_out.get());
                 c.launches += 2;
                 CICY_CUDA(cudaMemcpyAsync(&I_cnt, c.cur_out.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
                 CICY_CUDA(cudaStreamSynchronize(s));
@@ -976,7 +976,7 @@ void run_hybrid_electrical(Ctx& c, const cicy_hybrid_state& h, const cicy_params
                 k_gnp_boundary_terms<<<grid_for(nbg, 64), 64, 0, s>>>(nbg, H.bg_idx.get() + fb, H.boff.get(), 0, H.tri.get(), H.tri_cnt.get(),
                                                                     H.lmm_g.get(), H.rad_from.get(), H.cnt_rad.get(), H.t.get(), H.pts.get(),
                                                                     sr->volt.get(), H.rs, H.rt, H.bterm.get(), H.bvalid.get(), c.status.get());
-                k_boundary_sum<<<1, 32, 0, s>>>(m, H.bterm.get(), H.bvalid.get(), c.cur_out.get() + 1);
+                k_boundary_sum<<<1, kSumThreads, 0, s>>>(m, H.bterm.get(), H.bvalid.get(), c.cur_out.get() + 1);
                 c.launches += 2;
                 CICY_CUDA(cudaMemcpyAsync(&I_gnp, c.cur_out.get() + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
                 check_status(c, "Currents_through_boundary_gnps");

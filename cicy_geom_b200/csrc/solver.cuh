@@ -99,6 +99,11 @@ struct MgWork {
         const double* val_ptr = nullptr;
         DBuf<int32_t> rp, ci, agg, mptr, midx, cagg, ra_ptr, ra_col;
         DBuf<double> val, diag, l1inv, rs, r, z, zf, ra_val;
+        // fused rows for the clustered solve kernel: restriction into level l+1 (members on
+        // r_l, P^T A_l on z_l) and prolongation-smoother rows of level l (A_l on z_l and on P zc)
+        DBuf<int32_t> rr_ptr, rr_col, pq_ptr, pq_col;
+        DBuf<double> rr_val, pq_val;
+        DBuf<double> r_cl, z_cl, zf_cl;  // per-cluster copies of the levels each cluster solves alone
     };
     std::vector<Lvl> L;
     std::vector<MgLevel> host_lv;
@@ -111,6 +116,9 @@ struct MgWork {
     RadixScratch radix;
     int levels = 0;
     bool dense = false;
+    bool fused = false;  // fused rows built (build_mg_hierarchy with fused = true)
+    DBuf<int32_t> cl_fail;
+    DBuf<unsigned char> sec_lv;  // device descriptors of the clustered kernel
 };
 
 struct SolverWork {
@@ -179,7 +187,9 @@ bool pcg_solve_cluster(SolverWork& w, const SolverSystem& sys, bool block_precon
 
 // Multigrid hierarchy over the chain blocks of build_block_preconditioner (which
 // must have run on the same system), then the MG-preconditioned CG solve.
-void build_mg_hierarchy(SolverWork& w, const SolverSystem& sys, cudaStream_t s, int64_t& launches);
+// fused: also build the fused restriction / prolongation rows the clustered grid kernel
+// reads (systems above the single-cluster size).
+void build_mg_hierarchy(SolverWork& w, const SolverSystem& sys, cudaStream_t s, int64_t& launches, bool fused = false);
 // allow_cluster: one 16-CTA cluster with hardware barriers when it fits, else the grid-wide kernel.
 void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long max_iter, bool allow_cluster, int num_sms, int* status,
                   cudaStream_t s, int64_t& launches, PcgStats& st);

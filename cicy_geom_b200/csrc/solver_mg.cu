@@ -214,6 +214,53 @@ __global__ void k_ra_fill(int nc, const int32_t* __restrict__ mptr, const int32_
     }
 }
 
+// Fused restriction rows of level l >= 1 into level l + 1 (clustered kernel): row J holds
+// the members of aggregate J (column m < n: r_l[m], weight 1), then its row of P^T A_l
+// (column n + c: z_l[c], weight -a), so r_{l+1} = P^T (r_l - A_l z_l) is one gathered dot
+// product.  rr_ptr = mptr + ra_ptr, both prefix sums.
+__global__ void k_rr_fill(int nc, int n, const int32_t* __restrict__ mptr, const int32_t* __restrict__ midx,
+                          const int32_t* __restrict__ ra_ptr, const int32_t* __restrict__ ra_col, const double* __restrict__ ra_val,
+                          int32_t* __restrict__ rr_ptr, int32_t* __restrict__ rr_col, double* __restrict__ rr_val) {
+    for (int J = blockIdx.x * blockDim.x + threadIdx.x; J < nc; J += gridDim.x * blockDim.x) {
+        int e = mptr[J] + ra_ptr[J];
+        rr_ptr[J] = e;
+        if (J == nc - 1) rr_ptr[nc] = mptr[nc] + ra_ptr[nc];
+        for (int m = mptr[J]; m < mptr[J + 1]; m++, e++) {
+            rr_col[e] = midx[m];
+            rr_val[e] = 1.0;
+        }
+        for (int k = ra_ptr[J]; k < ra_ptr[J + 1]; k++, e++) {
+            rr_col[e] = n + ra_col[k];
+            rr_val[e] = -ra_val[k];
+        }
+    }
+}
+
+// Fused prolongation-smoother rows of level l (1 <= l < coarsest): row I holds its diagonal
+// and off-diagonal couplings twice, on z_l (column c < n) and on the coarse correction
+// (column n + aggregate of c), so w = r_l - A_l (z_l + P zc) is one gathered dot product.
+__global__ void k_pq_fill(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const double* __restrict__ v,
+                          const double* __restrict__ diag, const int32_t* __restrict__ agg, int32_t* __restrict__ pq_ptr,
+                          int32_t* __restrict__ pq_col, double* __restrict__ pq_val) {
+    for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < n; I += gridDim.x * blockDim.x) {
+        int e = 2 * (rp[I] + I);
+        pq_ptr[I] = e;
+        if (I == n - 1) pq_ptr[n] = 2 * (rp[n] + n);
+        pq_col[e] = I;
+        pq_val[e] = diag[I];
+        pq_col[e + 1] = n + agg[I];
+        pq_val[e + 1] = diag[I];
+        e += 2;
+        for (int k = rp[I]; k < rp[I + 1]; k++, e += 2) {
+            const int c = ci[k];
+            pq_col[e] = c;
+            pq_val[e] = v[k];
+            pq_col[e + 1] = n + agg[c];
+            pq_val[e + 1] = v[k];
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Solve kernel
 
@@ -611,6 +658,278 @@ __global__ void __launch_bounds__(kMgClusterThreads) k_mg_batch(const MgArgs* __
     }
 }
 
+// ---------------------------------------------------------------------------
+// Clustered grid kernel for systems above one cluster's size.  The grid is K clusters of
+// kSecCtas CTAs (cooperative launch).  Level 0 and the levels above `lc` run grid-wide as in
+// k_mg_pcg, on the fused rows (one gathered dot product per restriction or prolongation row);
+// levels lc .. coarsest (at most kSecRows rows at lc) are solved by every cluster on its own
+// copy of their vectors, between hardware cluster barriers (~0.3 us) instead of grid
+// barriers (~1.3 us).  Per CG iteration that leaves 4 + 2 (lc - 1) grid barriers.
+constexpr int kSecCtas = 16;       // CTAs per cluster (non-portable size)
+constexpr int kSecThreads = 512;
+constexpr int kSecGroup = 4;       // lanes per coarse row
+constexpr int kSecRows = 8192;     // largest level the clusters solve alone
+constexpr int kSecMaxClusters = 9; // 144 CTAs: one per SM
+
+struct MgSecLevel {
+    int n;
+    const int32_t* rr_ptr;  // fused restriction rows into level l + 1 (1 <= l < coarsest)
+    const int32_t* rr_col;
+    const double* rr_val;
+    const int32_t* pq_ptr;  // fused prolongation-smoother rows of level l (1 <= l < coarsest)
+    const int32_t* pq_col;
+    const double* pq_val;
+    const int32_t* agg;
+    const double* l1inv;
+    double* r;
+    double* z;
+    double* zf;
+    int priv;  // bit 0: r and z per cluster (stride n), bit 1: zf per cluster
+};
+
+struct MgSecArgs {
+    int lc;                  // first level the clusters solve alone (>= 1)
+    const MgSecLevel* lv;    // levels 0 .. coarsest (level 0: unused but for the count)
+    int* cl_fail;            // per cluster: a grid-barrier wait of one of its CTAs gave up
+};
+
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+    asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+
+// Grid barrier whose outcome is the same on every CTA of a cluster: a CTA whose bounded wait
+// gave up marks its cluster before the cluster barrier, and every CTA of the cluster reads
+// that mark after it, so a cluster leaves as a whole and no cluster barrier waits on a CTA
+// that has returned.
+__device__ __forceinline__ bool sec_sync(const MgArgs& a, const MgSecArgs& sa, unsigned long long& target, int cid, int* s_ok) {
+    const bool ok = mg_sync(a.bar, target, a.err, s_ok, a.spin_limit);
+    if (!ok && threadIdx.x == 0) atomicExch(&sa.cl_fail[cid], 1);
+    cluster_sync_all();
+    return __ldcg(&sa.cl_fail[cid]) == 0;
+}
+
+// sum_k val[k] v(col[k]) with v(c) = v0[c] for c < n, else v1[c - n]; chunks of U entries
+// per lane (indices and weights first, vector entries second).
+template <int U>
+__device__ __forceinline__ double fused_dot(const int32_t* __restrict__ col, const double* __restrict__ val, int b, int e, int first,
+                                            int step, int n, const double* v0, const double* v1) {
+    double s = 0;
+    for (int k0 = b + first; k0 < e; k0 += U * step) {
+        int c[U];
+        double w[U], xv[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int k = k0 + u * step;
+            c[u] = k < e ? col[k] : 0;
+            w[u] = k < e ? val[k] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) xv[u] = (k0 + u * step < e) ? (c[u] < n ? __ldcg(&v0[c[u]]) : __ldcg(&v1[c[u] - n])) : 0.0;
+#pragma unroll
+        for (int u = 0; u < U; u++) s += w[u] * xv[u];
+    }
+    return s;
+}
+
+__device__ __forceinline__ double sec_group_sum(double v, unsigned mask) {
+    for (int o = kSecGroup / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, kSecGroup);
+    return v;
+}
+
+// Restriction rows [lo, hi) of level l + 1: r_{l+1} = P^T (r_l - A_l z_l), z_{l+1} = l1-Jacobi of it.
+__device__ __forceinline__ void sec_restrict(const MgSecLevel& F, const MgSecLevel& G, bool smooth, int lo, int hi) {
+    const int grp = threadIdx.x / kSecGroup, glane = threadIdx.x % kSecGroup, ngrp = blockDim.x / kSecGroup;
+    const unsigned gmask = ((1u << kSecGroup) - 1) << ((threadIdx.x & 31) & ~(kSecGroup - 1));
+    for (int J = lo + grp; J < hi; J += ngrp) {
+        double v = fused_dot<4>(F.rr_col, F.rr_val, F.rr_ptr[J], F.rr_ptr[J + 1], glane, kSecGroup, F.n, F.r, F.z);
+        v = sec_group_sum(v, gmask);
+        if (glane == 0) {
+            G.r[J] = v;
+            if (smooth) G.z[J] = G.l1inv[J] * v;
+        }
+    }
+}
+
+// Prolongation and l1-Jacobi post-smoother on rows [lo, hi) of level l:
+// zp = z_l + P zc, zf_l = zp + D^-1 (r_l - A_l zp).
+__device__ __forceinline__ void sec_prolong(const MgSecLevel& F, const double* zc, int lo, int hi) {
+    const int grp = threadIdx.x / kSecGroup, glane = threadIdx.x % kSecGroup, ngrp = blockDim.x / kSecGroup;
+    const unsigned gmask = ((1u << kSecGroup) - 1) << ((threadIdx.x & 31) & ~(kSecGroup - 1));
+    for (int I = lo + grp; I < hi; I += ngrp) {
+        double zp = 0, rI = 0;
+        if (glane == 0) {
+            zp = __ldcg(&F.z[I]) + __ldcg(&zc[F.agg[I]]);
+            rI = __ldcg(&F.r[I]);
+        }
+        double v = fused_dot<4>(F.pq_col, F.pq_val, F.pq_ptr[I], F.pq_ptr[I + 1], glane, kSecGroup, F.n, F.z, zc);
+        v = sec_group_sum(v, gmask);
+        if (glane == 0) F.zf[I] = zp + F.l1inv[I] * (rI - v);
+    }
+}
+
+__global__ void __launch_bounds__(kSecThreads) k_mg_pcg_sec(MgArgs a, MgSecArgs sa) {
+    __shared__ double sm[72];
+    __shared__ MgSecLevel lv[kMgMaxLevels];
+    __shared__ MgLevel lv0;
+    __shared__ int s_ok;
+    const int cta = blockIdx.x, nb = gridDim.x;
+    const int cid = cta / kSecCtas, crank = cta % kSecCtas;
+    if (threadIdx.x < a.levels) {
+        MgSecLevel L = sa.lv[threadIdx.x];
+        if (L.priv & 1) {
+            L.r += (size_t)cid * L.n;
+            L.z += (size_t)cid * L.n;
+        }
+        if (L.priv & 2) L.zf += (size_t)cid * L.n;
+        lv[threadIdx.x] = L;
+    }
+    if (threadIdx.x == 0) lv0 = a.lv[0];
+    __syncthreads();
+    const int C = a.levels - 1, Lc = sa.lc;
+    const int r_lo = a.cta_row[cta], r_hi = a.cta_row[cta + 1];
+    auto grid_lo = [&](int n) { return (int)((long long)n * cta / nb); };
+    auto grid_hi = [&](int n) { return (int)((long long)n * (cta + 1) / nb); };
+    auto cl_lo = [&](int n) { return (int)((long long)n * crank / kSecCtas); };
+    auto cl_hi = [&](int n) { return (int)((long long)n * (crank + 1) / kSecCtas); };
+    unsigned long long target = 0;
+    double R0 = 0, rr = 0, rz = 0, beta = 0;
+    long long k = 0;
+    int restarts = 0;
+    bool fresh = true;
+    bool recursive = false;
+    double s0;
+    while (true) {
+        // ---- pre-smoother z0 = w M0^-1 r on own rows; r.r ----
+        __syncthreads();
+        double rr_l = 0;
+        for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
+            a.z0[i] = a.omega0 * block_apply(a, a.r, i);
+            const double ri = a.r[i];
+            rr_l += ri * ri;
+        }
+        mg_reduce1(rr_l, sm, s0);
+        if (threadIdx.x == 0) a.partA[cta] = s0;
+        if (!sec_sync(a, sa, target, cid, &s_ok)) return;
+        rr = mg_sum_partials(a.partA, nb, sm);
+        if (k == 0 && !recursive && restarts == 0) R0 = a.tol * sqrt(rr);
+        if (k > 0 && sqrt(rr) <= R0) {
+            if (!recursive || restarts >= a.max_restarts) break;
+            for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) a.r[i] = a.b[i] - gather_dot<4>(a.ci, a.val, a.x, a.rp[i], a.rp[i + 1]);
+            restarts++;
+            recursive = false;
+            fresh = true;
+            continue;
+        }
+        if (k >= a.max_iter) break;
+        // ---- level 0 -> 1 inside the CTA (its blocks, the level-0 aggregates, are its own rows) ----
+        {
+            for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) a.w[i] = a.r[i] - gather_dot<4>(a.ci, a.val, a.z0, a.rp[i], a.rp[i + 1]);
+            __syncthreads();
+            const MgSecLevel& G = lv[1];
+            const bool smooth = (C > 1) || a.cinv == nullptr;
+            if (r_hi > r_lo) {
+                const int b0 = lv0.agg[r_lo], b1 = lv0.agg[r_hi - 1];
+                for (int J = b0 + threadIdx.x; J <= b1; J += blockDim.x) {
+                    double v = 0;
+                    for (int m = lv0.mptr[J]; m < lv0.mptr[J + 1]; m++) v += a.w[lv0.midx[m]];
+                    G.r[J] = v;
+                    if (smooth) G.z[J] = G.l1inv[J] * v;
+                }
+            }
+            if (!sec_sync(a, sa, target, cid, &s_ok)) return;
+        }
+        // ---- restrictions l -> l + 1 grid-wide (1 <= l < lc) ----
+        for (int l = 1; l < Lc; l++) {
+            const int n1 = lv[l + 1].n;
+            sec_restrict(lv[l], lv[l + 1], (l + 1 < C) || a.cinv == nullptr, grid_lo(n1), grid_hi(n1));
+            if (!sec_sync(a, sa, target, cid, &s_ok)) return;
+        }
+        // ---- levels lc .. coarsest: every cluster on its own copy ----
+        for (int l = Lc; l < C; l++) {
+            const int n1 = lv[l + 1].n;
+            sec_restrict(lv[l], lv[l + 1], (l + 1 < C) || a.cinv == nullptr, cl_lo(n1), cl_hi(n1));
+            cluster_sync_all();
+        }
+        {
+            const MgSecLevel& Cl = lv[C];
+            const int nC = Cl.n;
+            const int wpb = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+            if (a.cinv) {  // dense inverse of the coarsest level, one warp per row
+                for (int i = crank * wpb + warp; i < nC; i += kSecCtas * wpb) {
+                    const double* row = a.cinv + (size_t)i * nC;
+                    double v = 0;
+                    for (int j = lane; j < nC; j += 32) v += row[j] * __ldcg(&Cl.r[j]);
+                    v = warp_sum(v);
+                    if (lane == 0) Cl.zf[i] = v;
+                }
+            } else {  // l1-Jacobi only: the correction is the smoothed z
+                for (int i = cl_lo(nC) + threadIdx.x; i < cl_hi(nC); i += blockDim.x) Cl.zf[i] = __ldcg(&Cl.z[i]);
+            }
+            cluster_sync_all();
+        }
+        for (int l = C - 1; l >= Lc; l--) {
+            sec_prolong(lv[l], lv[l + 1].zf, cl_lo(lv[l].n), cl_hi(lv[l].n));
+            cluster_sync_all();
+        }
+        // ---- prolongations lc - 1 .. 1 grid-wide ----
+        for (int l = Lc - 1; l >= 1; l--) {
+            sec_prolong(lv[l], lv[l + 1].zf, grid_lo(lv[l].n), grid_hi(lv[l].n));
+            if (!sec_sync(a, sa, target, cid, &s_ok)) return;
+        }
+        // ---- level-0 post-smoother: z = z0 + P z1, z += w M0^-1 (r - A z); r.z ----
+        {
+            const double* zc = lv[1].zf;
+            for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
+                a.w[i] = a.r[i] - gather_dot2<4>(a.ci, lv0.cagg, a.val, a.z0, zc, a.rp[i], a.rp[i + 1]);
+                a.z[i] = a.z0[i] + __ldcg(&zc[lv0.agg[i]]);
+            }
+            __syncthreads();
+            double rz_l = 0;
+            for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
+                const double zi = a.z[i] + a.omega0 * block_apply(a, a.w, i);
+                a.z[i] = zi;
+                rz_l += a.r[i] * zi;
+            }
+            mg_reduce1(rz_l, sm, s0);
+            if (threadIdx.x == 0) a.partB[cta] = s0;
+            if (!sec_sync(a, sa, target, cid, &s_ok)) return;
+            const double rz_new = mg_sum_partials(a.partB, nb, sm);
+            beta = fresh ? 0.0 : rz_new / rz;
+            rz = rz_new;
+        }
+        // ---- q = A z + beta q, p = z + beta p; p.q ----
+        double pq_l = 0;
+        for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
+            const double w = gather_dot<4>(a.ci, a.val, a.z, a.rp[i], a.rp[i + 1]);
+            const double zi = a.z[i];
+            const double qi = fresh ? w : w + beta * a.q[i];
+            const double pi = fresh ? zi : zi + beta * a.p[i];
+            a.q[i] = qi;
+            a.p[i] = pi;
+            pq_l += pi * qi;
+        }
+        mg_reduce1(pq_l, sm, s0);
+        if (threadIdx.x == 0) a.partA[nb + cta] = s0;
+        if (!sec_sync(a, sa, target, cid, &s_ok)) return;
+        const double pq = mg_sum_partials(a.partA + nb, nb, sm);
+        fresh = false;
+        k++;
+        const double alpha = rz / pq;
+        for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
+            a.x[i] += alpha * a.p[i];
+            a.r[i] -= alpha * a.q[i];
+        }
+        recursive = true;
+    }
+    if (cta == 0 && threadIdx.x == 0) {
+        a.stats[0] = (double)k;
+        a.stats[1] = rr;
+        a.stats[2] = R0;
+        a.stats[3] = (double)restarts;
+    }
+}
+
 // Exclusive scan of n ints in one CTA (the setup's arrays are short enough):
 // each thread scans a contiguous chunk; out may alias in; *total gets the sum.
 __global__ void __launch_bounds__(1024) k_scan_single(const int32_t* in, int32_t* out, int n, int32_t* total) {
@@ -845,6 +1164,19 @@ void coarsen(MgWork& g, int l, int nc, cudaStream_t s, int64_t& launches) {
     F.cagg.ensure(std::max(nnz, 1));
     k_cagg_rows<<<grid_for(nf), 256, 0, s>>>(nf, F.rp_ptr, F.ci_ptr, F.agg.get(), F.cagg.get());
     launches++;
+    if (g.fused && l >= 1) {
+        F.rr_ptr.ensure(nc + 1);
+        F.rr_col.ensure(std::max(nnz + 2 * nf, 1));
+        F.rr_val.ensure(std::max(nnz + 2 * nf, 1));
+        k_rr_fill<<<grid_for(nc), 256, 0, s>>>(nc, nf, F.mptr.get(), F.midx.get(), F.ra_ptr.get(), F.ra_col.get(), F.ra_val.get(),
+                                                F.rr_ptr.get(), F.rr_col.get(), F.rr_val.get());
+        F.pq_ptr.ensure(nf + 1);
+        F.pq_col.ensure(std::max(2 * (nnz + nf), 1));
+        F.pq_val.ensure(std::max(2 * (nnz + nf), 1));
+        k_pq_fill<<<grid_for(nf), 256, 0, s>>>(nf, F.rp_ptr, F.ci_ptr, F.val_ptr, F.diag.get(), F.agg.get(), F.pq_ptr.get(),
+                                                F.pq_col.get(), F.pq_val.get());
+        launches += 2;
+    }
     CICY_LAUNCH_CHECK();
 }
 
@@ -883,9 +1215,10 @@ int pairwise(MgWork& g, int l, cudaStream_t s, int64_t& launches) {
 }  // namespace
 
 // ---------------------------------------------------------------------------
-void build_mg_hierarchy(SolverWork& w, const SolverSystem& sys, cudaStream_t s, int64_t& launches) {
+void build_mg_hierarchy(SolverWork& w, const SolverSystem& sys, cudaStream_t s, int64_t& launches, bool fused) {
     MgWork& g = w.mg;
     const int n = sys.n;
+    g.fused = fused;
     TraceSeq tr(s);
     g.total.ensure(2);
     if (g.L.empty()) g.L.resize(1);
@@ -1000,12 +1333,102 @@ void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long 
         cluster = cudaOccupancyMaxActiveClusters(&nclusters, (void*)k_mg_pcg<true>, &cfg) == cudaSuccess && nclusters >= 1;
         cudaGetLastError();
     }
+    // above one cluster's size: the clustered grid kernel (levels from lc on solved per
+    // cluster) when the fused rows exist and K clusters of kSecCtas can be co-resident
+    bool sec = false;
+    int K = 0;
+    cudaLaunchConfig_t scfg = {};
+    cudaLaunchAttribute sattr[2];
+    if (!cluster && g.fused && g.levels >= 2) {
+        static int sec_state = 0;  // 0 unknown, 1 ok, -1 unsupported
+        if (sec_state == 0) {
+            sec_state = cudaFuncSetAttribute(k_mg_pcg_sec, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess ? 1 : -1;
+            cudaGetLastError();
+        }
+        if (sec_state > 0) {
+            K = std::max(1, std::min({ceil_div(n, kSecCtas * kSecThreads), kSecMaxClusters, num_sms / kSecCtas}));
+            scfg.gridDim = dim3(K * kSecCtas);
+            scfg.blockDim = dim3(kSecThreads);
+            scfg.dynamicSmemBytes = 0;
+            scfg.stream = s;
+            sattr[0].id = cudaLaunchAttributeClusterDimension;
+            sattr[0].val.clusterDim.x = kSecCtas;
+            sattr[0].val.clusterDim.y = 1;
+            sattr[0].val.clusterDim.z = 1;
+            sattr[1].id = cudaLaunchAttributeCooperative;
+            sattr[1].val.cooperative = 1;
+            scfg.attrs = sattr;
+            scfg.numAttrs = 2;
+            int ncl = 0;
+            if (cudaOccupancyMaxActiveClusters(&ncl, (void*)k_mg_pcg_sec, &scfg) == cudaSuccess && ncl >= 1) {
+                K = std::min(K, ncl);
+                scfg.gridDim = dim3(K * kSecCtas);
+                sec = true;
+            }
+            cudaGetLastError();
+        }
+    }
     int nb = kMgClusterCtas;
-    if (!cluster) {
+    if (sec) {
+        nb = K * kSecCtas;
+    } else if (!cluster) {
         int occ = 0;
         CICY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mg_pcg<false>, kMgThreads, 0));
         const int cap = std::max(1, occ) * num_sms;
         nb = std::max(1, std::min({cap, num_sms, ceil_div(n, 2 * kMgThreads)}));
+    }
+    std::vector<MgSecLevel> hl;  // kept until the stream synchronisation below
+    MgSecArgs sa{};
+    if (sec) {
+        // levels lc .. coarsest per cluster: r and z above lc, zf from lc on, K copies each
+        const int C = g.levels - 1;
+        int lc = C;
+        for (int l = 1; l <= C; l++)
+            if (g.L[l].n <= kSecRows) {
+                lc = l;
+                break;
+            }
+        hl.assign(C + 1, MgSecLevel{});
+        for (int l = 0; l <= C; l++) {
+            MgWork::Lvl& L = g.L[l];
+            MgSecLevel& d = hl[l];
+            d.n = L.n;
+            if (l == 0) continue;
+            if (l < C) {
+                d.rr_ptr = L.rr_ptr.get();
+                d.rr_col = L.rr_col.get();
+                d.rr_val = L.rr_val.get();
+                d.pq_ptr = L.pq_ptr.get();
+                d.pq_col = L.pq_col.get();
+                d.pq_val = L.pq_val.get();
+                d.agg = L.agg.get();
+            }
+            d.l1inv = L.l1inv.get();
+            if (l > lc) {
+                L.r_cl.ensure((size_t)K * L.n + 1);
+                L.z_cl.ensure((size_t)K * L.n + 1);
+                d.r = L.r_cl.get();
+                d.z = L.z_cl.get();
+                d.priv |= 1;
+            } else {
+                d.r = L.r.get();
+                d.z = L.z.get();
+            }
+            if (l >= lc) {
+                L.zf_cl.ensure((size_t)K * L.n + 1);
+                d.zf = L.zf_cl.get();
+                d.priv |= 2;
+            } else {
+                d.zf = L.zf.get();
+            }
+        }
+        g.sec_lv.ensure(sizeof(MgSecLevel) * (C + 1));
+        CICY_CUDA(cudaMemcpyAsync(g.sec_lv.get(), hl.data(), sizeof(MgSecLevel) * (C + 1), cudaMemcpyHostToDevice, s));
+        g.cl_fail.ensure(K);
+        CICY_CUDA(cudaMemsetAsync(g.cl_fail.get(), 0, sizeof(int32_t) * K, s));
+        sa.lc = lc;
+        sa.lv = reinterpret_cast<const MgSecLevel*>(g.sec_lv.get());
+        sa.cl_fail = g.cl_fail.get();
     }
     w.cta_row.ensure(nb + 1);
     launch_cta_rows(nb, n, w.is_start.get(), w.cta_row.get(), s);
@@ -1039,6 +1462,8 @@ void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long 
     CICY_CUDA(cudaEventRecord(e0, s));
     if (cluster) {
         CICY_CUDA(cudaLaunchKernelEx(&cfg, k_mg_pcg<true>, a));
+    } else if (sec) {
+        CICY_CUDA(cudaLaunchKernelEx(&scfg, k_mg_pcg_sec, a, sa));
     } else {
         void* args[] = {&a};
         CICY_CUDA(cudaLaunchCooperativeKernel((void*)k_mg_pcg<false>, dim3(nb), dim3(kMgThreads), args, 0, s));

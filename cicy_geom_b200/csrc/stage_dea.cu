@@ -529,19 +529,63 @@ __global__ void k_backbone_cnts(int n, const int32_t* __restrict__ members, cons
 // fractions step's total_volumes[8] and fractions[8]).
 constexpr int kVolCnt = 0, kVolDead = 8, kVolTotal = 15, kVolFrac = 23, kVolWords = 31;
 
+// Ordered FP64 sums on one CTA of kSumThreads: warps 1.. stage chunk ch + 1 of the
+// inputs in shared memory (double-buffered) while thread 0 adds chunk ch in order, so the
+// result is the sequence of additions of a sequential loop, at shared-memory latency.
+constexpr int kSumThreads = 256;
+constexpr int kSumChunk = 512;
+
+template <class Stage, class Consume>
+__device__ __forceinline__ void staged_in_order(int n, Stage stage, Consume consume) {
+    const int nch = (n + kSumChunk - 1) / kSumChunk;
+    const int t = (int)threadIdx.x - 32, T = (int)blockDim.x - 32;
+    if (t >= 0 && nch > 0) stage(0, 0, t, T);
+    __syncthreads();
+    for (int ch = 0; ch < nch; ch++) {
+        const int m = min(kSumChunk, n - ch * kSumChunk);
+        if (threadIdx.x == 0)
+            consume(ch & 1, m);
+        else if (t >= 0 && ch + 1 < nch)
+            stage(ch + 1, (ch + 1) & 1, t, T);
+        __syncthreads();
+    }
+}
+
 // The cluster's volumes added to its family in upstream's order: CNTs last to first
 // (Backbone_Network.cpp:325), per CNT the dead part(s) and then the kept run (:442-543).
-// One thread: the FP64 sums must be the same sequence of additions.
-__global__ void k_volume_sum(int n, int family, const double* __restrict__ vol3, const int32_t* __restrict__ kind, double* acc) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    double dead = acc[kVolDead + family], bb = acc[kVolCnt + family];
-    for (int i = n - 1; i >= 0; i--) {
-        dead = dead + vol3[3 * i];
-        if (kind[i] == 2) dead = dead + vol3[3 * i + 2];
-        if (kind[i] >= 1) bb = bb + vol3[3 * i + 1];
+__global__ void __launch_bounds__(kSumThreads) k_volume_sum(int n, int family, const double* __restrict__ vol3,
+                                                            const int32_t* __restrict__ kind, double* acc) {
+    __shared__ double sv[2][3 * kSumChunk];
+    __shared__ int32_t sk[2][kSumChunk];
+    double dead = 0, bb = 0;
+    if (threadIdx.x == 0) {
+        dead = acc[kVolDead + family];
+        bb = acc[kVolCnt + family];
     }
-    acc[kVolDead + family] = dead;
-    acc[kVolCnt + family] = bb;
+    staged_in_order(
+        n,
+        [&](int ch, int b, int t, int T) {
+            const int i0 = n - 1 - ch * kSumChunk, m = min(kSumChunk, i0 + 1);
+            for (int j = t; j < m; j += T) {
+                const int i = i0 - j, k = kind[i];
+                sk[b][j] = k;
+                sv[b][3 * j] = vol3[3 * i];
+                if (k >= 1) sv[b][3 * j + 1] = vol3[3 * i + 1];
+                if (k == 2) sv[b][3 * j + 2] = vol3[3 * i + 2];
+            }
+        },
+        [&](int b, int m) {
+            for (int j = 0; j < m; j++) {
+                const int k = sk[b][j];
+                dead = dead + sv[b][3 * j];
+                if (k == 2) dead = dead + sv[b][3 * j + 2];
+                if (k >= 1) bb = bb + sv[b][3 * j + 1];
+            }
+        });
+    if (threadIdx.x == 0) {
+        acc[kVolDead + family] = dead;
+        acc[kVolCnt + family] = bb;
+    }
 }
 
 // Sort keys of HoKo->isolated_cnt's order (Hoshen_Kopelman.cpp:2331-2363, 2527-2539): CNTs
@@ -558,25 +602,42 @@ __global__ void k_isolated_keys(int n_inside, int n_labels, const int32_t* __res
     }
 }
 
-// Calculate_percolated_families_fractions with Calculate_volume_of_non_percolated_cnts
-// (Electrical_analysis.cpp:678-786) for CNTs: the whole-CNT volumes of the isolated list in
-// order, volumes_cnt[7] = dead branches + that, then total volumes and fractions (no GNPs:
-// their volumes are 0).  One thread, upstream's sequence of additions.
-__global__ void k_family_fractions(int n_inside, int n_labels, const uint64_t* __restrict__ key, const uint32_t* __restrict__ cnt,
+// Whole-CNT volumes of HoKo->isolated_cnt's entries (keys below `end`, a prefix of the
+// sorted list) for Calculate_volume_of_non_percolated_cnts; count = their number.
+__global__ void k_isolated_volumes(int n_inside, uint64_t end, const uint64_t* __restrict__ key, const uint32_t* __restrict__ cnt,
                                    const int32_t* __restrict__ cstart, const int32_t* __restrict__ clen, const double* __restrict__ radii,
-                                   const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z, double* acc) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+                                   const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
+                                   double* __restrict__ vol, int32_t* count) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n_inside; p += gridDim.x * blockDim.x) {
+        if (key[p] >= end) continue;
+        const int c = (int)cnt[p];
+        vol[p] = cnt_volume(cstart[c], cstart[c] + clen[c] - 1, radii[c], x, y, z);
+        atomicMax(count, p + 1);
+    }
+}
+
+// Calculate_percolated_families_fractions with Calculate_volume_of_non_percolated_cnts
+// (Electrical_analysis.cpp:678-786) for CNTs: the isolated list's volumes added in order,
+// volumes_cnt[7] = dead branches + that, then total volumes and fractions (no GNPs: their
+// volumes are 0), upstream's sequence of additions.
+__global__ void __launch_bounds__(kSumThreads) k_family_fractions(const int32_t* __restrict__ count, const double* __restrict__ vol,
+                                                                  double* acc) {
+    __shared__ double sv[2][kSumChunk];
+    double np_cnts = 0;
+    staged_in_order(
+        *count,
+        [&](int ch, int b, int t, int T) {
+            const int m = min(kSumChunk, *count - ch * kSumChunk);
+            for (int j = t; j < m; j += T) sv[b][j] = vol[ch * kSumChunk + j];
+        },
+        [&](int b, int m) {
+            for (int j = 0; j < m; j++) np_cnts = np_cnts + sv[b][j];
+        });
+    if (threadIdx.x != 0) return;
     double total_dead = 0, total_dead_gnps = 0;
     for (int i = 0; i < 7; i++) {
         total_dead = total_dead + acc[kVolDead + i];
         total_dead_gnps = total_dead_gnps + 0.0;
-    }
-    const uint64_t end = (uint64_t)(n_labels + 1) * (uint64_t)n_inside;
-    double np_cnts = 0;
-    for (int p = 0; p < n_inside && key[p] < end; p++) {
-        const int c = (int)cnt[p];
-        const int P1 = cstart[c], P2 = cstart[c] + clen[c] - 1;
-        np_cnts = np_cnts + cnt_volume(P1, P2, radii[c], x, y, z);
     }
     acc[kVolCnt + 7] = total_dead + np_cnts;
     double tv = 0;
@@ -646,12 +707,26 @@ __global__ void k_boundary_terms(int b, int e, const int32_t* __restrict__ bcnt,
     }
 }
 
-__global__ void k_boundary_sum(int m, const double* __restrict__ term, const int32_t* __restrict__ valid, double* out) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+__global__ void __launch_bounds__(kSumThreads) k_boundary_sum(int m, const double* __restrict__ term, const int32_t* __restrict__ valid,
+                                                              double* out) {
+    __shared__ double sv[2][kSumChunk];
+    __shared__ int32_t sf[2][kSumChunk];
     double I = 0;
-    for (int t = 0; t < m; t++)
-        if (valid[t]) I = I + term[t];
-    *out = I;
+    staged_in_order(
+        m,
+        [&](int ch, int b, int t, int T) {
+            const int mm = min(kSumChunk, m - ch * kSumChunk);
+            for (int j = t; j < mm; j += T) {
+                const int f = valid[ch * kSumChunk + j];
+                sf[b][j] = f;
+                if (f) sv[b][j] = term[ch * kSumChunk + j];
+            }
+        },
+        [&](int b, int mm) {
+            for (int j = 0; j < mm; j++)
+                if (sf[b][j]) I = I + sv[b][j];
+        });
+    if (threadIdx.x == 0) *out = I;
 }
 
 __global__ void k_init_ranges(int nc, const int32_t* __restrict__ cstart, const int32_t* __restrict__ clen, const int32_t* __restrict__ mscan,
@@ -1047,7 +1122,7 @@ void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out) {
         k_backbone_cnts<<<grid_for(NM), 256, 0, s>>>(NM, members, eb.get(), ee.get(), c.elem_idx.get(), c.lmm.get(), su->volt.get(),
                                                    c.imax.get(), scope == 0 ? 1 : 0, c.bb_lo.get(), c.bb_hi.get(), c.alive.get(),
                                                    c.radii.get(), c.x.get(), c.y.get(), c.z.get(), c.vol3.get(), c.vol_kind.get());
-        k_volume_sum<<<1, 32, 0, s>>>(NM, c.h_family[k], c.vol3.get(), c.vol_kind.get(), c.vol_acc.get());
+        k_volume_sum<<<1, kSumThreads, 0, s>>>(NM, c.h_family[k], c.vol3.get(), c.vol_kind.get(), c.vol_acc.get());
         c.launches += 3;
         if (scope == 0) {
             exclusive_scan_i32(c.alive.get(), c.alive_scan.get(), NM, c.i32_scalar.get(), c.scan_tmp32, s, c.launches);
@@ -1105,7 +1180,7 @@ void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out) {
                                                              c.bb_lo.get(), c.bb_hi.get(), c.elem_idx.get(), c.lmm.get(), sr->volt.get(),
                                                              c.radii.get(), p.resistivity_cnt, c.x.get(), c.y.get(), c.z.get(),
                                                              c.bterm.get(), c.bvalid.get());
-            k_boundary_sum<<<1, 32, 0, s>>>(2 * nb, c.bterm.get(), c.bvalid.get(), c.cur_out.get());
+            k_boundary_sum<<<1, kSumThreads, 0, s>>>(2 * nb, c.bterm.get(), c.bvalid.get(), c.cur_out.get());
             c.launches += 2;
             double I = 0;
             CICY_CUDA(cudaMemcpyAsync(&I, c.cur_out.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -1131,9 +1206,14 @@ void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out) {
                                                              c.vol_key.get(), c.vol_cnt.get());
         radix_sort_pairs(c.vol_key.get(), c.vol_cnt.get(), c.n_inside, bits_for((uint64_t)(c.n_labels + 2) * (uint64_t)c.n_inside), c.rs,
                          s, c.launches);
-        k_family_fractions<<<1, 32, 0, s>>>(c.n_inside, c.n_labels, c.vol_key.get(), c.vol_cnt.get(), c.cstart.get(), c.clen.get(),
-                                            c.radii.get(), c.x.get(), c.y.get(), c.z.get(), c.vol_acc.get());
-        c.launches += 2;
+        c.vol_iso.ensure(c.n_inside);
+        CICY_CUDA(cudaMemsetAsync(c.i32_scalar.get() + 2, 0, sizeof(int32_t), s));
+        k_isolated_volumes<<<grid_for(c.n_inside), 256, 0, s>>>(c.n_inside, (uint64_t)(c.n_labels + 1) * (uint64_t)c.n_inside,
+                                                                c.vol_key.get(), c.vol_cnt.get(), c.cstart.get(), c.clen.get(),
+                                                                c.radii.get(), c.x.get(), c.y.get(), c.z.get(), c.vol_iso.get(),
+                                                                c.i32_scalar.get() + 2);
+        k_family_fractions<<<1, kSumThreads, 0, s>>>(c.i32_scalar.get() + 2, c.vol_iso.get(), c.vol_acc.get());
+        c.launches += 3;
         c.have_volumes = true;
     }
     // Calculate_resistances_and_resistivities (Electrical_analysis.cpp:873-987)

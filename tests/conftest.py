@@ -62,6 +62,20 @@ def csr_list(z, name):
     return [list(i[p[k]:p[k + 1]]) for k in range(len(p) - 1)]
 
 
+def assert_ulp(actual, desired, n_ulp, msg=""):
+    """|actual - desired| <= n_ulp units in the last place of the larger magnitude, per entry.
+
+    DEA values built from exp() (exponential tunnelling junctions) differ between CUDA's and
+    glibc's exp by at most 1 ulp; the products and the reciprocal after it carry that through
+    as a few ulp of the conductance."""
+    a = np.asarray(actual, dtype=np.float64)
+    d = np.asarray(desired, dtype=np.float64)
+    assert a.shape == d.shape, (msg, a.shape, d.shape)
+    tol = n_ulp * np.spacing(np.maximum(np.abs(a), np.abs(d)))
+    bad = np.abs(a - d) > tol
+    assert not bad.any(), f"{msg}: {int(bad.sum())} of {a.size} entries beyond {n_ulp} ulp; first at {int(np.argmax(bad))}"
+
+
 def golden_systems(z):
     """[(prefix, kind, cluster)] of the DEA systems a fixture holds, in solve order."""
     out = []
