@@ -100,20 +100,20 @@ class Context:
     def contact_grid(self, p: _abi.Params):
         self._check(lib().cicy_contact_grid(self._h, C.byref(p)), "cicy_contact_grid")
 
-    def gnp_cnt_contacts(self, gnp_directory: str, p: _abi.Params, inside_is_error: bool = False):
+    def gnp_cnt_contacts(self, gnp_directory: str, p: _abi.Params, inside_is_error: bool = False, gnps_inside=None):
         """CNT-GNP contacts of the hybrid sample (cicy_gnp_cnt_contacts), after
         contact_grid(p) on the uploaded CNT network: the GNPs of
-        gnp_directory/gnp_data.dat, all of them inside the network's window, on the
-        same region grid (Generate_contact_grid for GNP_CNT_mix, then
-        Find_adjacent_labels).  Returns (point, gnp, junction distance, closest GNP
-        point [n, 3]) by contact-point number."""
+        gnp_directory/gnp_data.dat listed in `gnps_inside` (Cutoff_Wins::gnps_inside;
+        None: all of them) on the same region grid (Generate_contact_grid for
+        GNP_CNT_mix, then Find_adjacent_labels).  Returns (point, gnp, junction
+        distance, closest GNP point [n, 3]) by contact-point number."""
         h = C.c_void_p()
         check(lib().cicy_read_gnps(gnp_directory.encode(), C.byref(h)), "cicy_read_gnps")
         grid = C.c_void_p()
         try:
             v = _abi.Gnps()
             check(lib().cicy_gnp_set_view(h, C.byref(v)), "cicy_gnp_set_view")
-            ins = np.arange(v.n, dtype=np.int32)
+            ins = np.arange(v.n, dtype=np.int32) if gnps_inside is None else np.ascontiguousarray(gnps_inside, dtype=np.int32)
             gs = np.array(list(p.gs_min), dtype=np.float64)
             check(lib().cicy_gnp_sectioned_domain(self._device, h, ins.ctypes.data_as(_abi.i32p), len(ins), C.byref(self._window),
                                                   gs.ctypes.data_as(_abi.f64p), p.gs_overlap_cnt, p.gs_overlap_gnp, C.byref(grid)),

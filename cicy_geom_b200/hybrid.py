@@ -112,7 +112,7 @@ def hybrid_network_to_conductance(directory: str, cfg, overlap_gnp: float, devic
                            p.tunneling_dist, n_labels_cnt=n_cnt, tol_gnp2=tol * tol, device=device,
                            init=(gw["points"], gw["structure_ptr"], gw["structure_idx"]))
     t.append(time.perf_counter())
-    ctx.gnp_cnt_contacts(directory, p)
+    ctx.gnp_cnt_contacts(directory, p, gnps_inside=gw["gnps_inside"])
     mj = ctx.mixed_junctions(len(gp["gnp_points"]), min_points)
     lc, lg, nm = ctx.mixed_labels(gp["labels_gnp"], gp["n_total_labels"])
     t.append(time.perf_counter())

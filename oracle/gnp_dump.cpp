@@ -56,6 +56,11 @@
  * resistances it writes, then a stage-by-stage replay of it (e_* records);
  * "electrical_time" skips the replay.  flow_seconds: steady_clock time of the
  * window extraction, contact grid, clusters and percolation, electrical stage.
+ * A unit-pass tolerance after the mode (> 0) solves the unit-resistor systems to that
+ * tolerance and the real-resistor ones to 1e-10: the electrical stage is then the
+ * replay alone (upstream's own calls in Perform_analysis_on_clusters' order, since that
+ * method takes one tolerance for both passes), timed as the electrical stage, with the
+ * resistances from its parallel resistors (Calculate_resistances_and_resistivities).
  *
  * With a gnp_resistor_cases.dat in the directory it evaluates upstream's
  * Direct_Electrifying::Calculate_resistance_gnp on each case (gnp_resistances).
@@ -142,6 +147,9 @@ struct StagedSystem {
 
 // Direct_Electrifying::Compute_voltage_field (Direct_Electrifying.cpp:11-113) replayed through its
 // public members, CNTs and GNPs, keeping the assembled system.
+// Tolerance of the unit-resistor (R_flag = 0) solves of the replay; <= 0: the flow's tolerance.
+double g_tol_unit = 0.0;
+
 int staged_field(Direct_Electrifying* D, int j, int R_flag, const cuboid& win, const Simu_para& sp, const Electric_para& ep,
                  const Cutoff_dist& cf, Hoshen_Kopelman* HoKo, Cutoff_Wins* CW, const std::vector<Point_3D>& pts,
                  const std::vector<double>& radii, const std::vector<std::vector<long int> >& sg, const std::vector<Point_3D>& pg,
@@ -167,7 +175,8 @@ int staged_field(Direct_Electrifying* D, int j, int R_flag, const cuboid& win, c
         if (!D->Update_residual_vector(col_ind, row_ptr, values, diagonal, V_guess, R)) return 0;
     }
     S.x0 = V_guess;
-    if (!D->Solve_DEA_equations_CG_SSS(global_nodes, reserved, sp.tolerance, col_ind, row_ptr, values, diagonal, R, VEF, V_guess)) return 0;
+    const double tol = (!R_flag && g_tol_unit > 0) ? g_tol_unit : sp.tolerance;
+    if (!D->Solve_DEA_equations_CG_SSS(global_nodes, reserved, tol, col_ind, row_ptr, values, diagonal, R, VEF, V_guess)) return 0;
     S.nodes = global_nodes;
     S.reserved = reserved;
     S.row_ptr = row_ptr;
@@ -603,6 +612,8 @@ int main(int argc, char** argv) {
         o.f64("flow_points_gnp", xyz);
         if (argc >= 12 && (std::string(argv[11]) == "electrical" || std::string(argv[11]) == "electrical_time")) {
             const bool staged = std::string(argv[11]) == "electrical";  // "electrical_time": the timed calls only
+            if (argc >= 13) g_tol_unit = number(argv[12]);
+            const bool replay = staged || g_tol_unit > 0;  // replay-only when the unit pass has its own tolerance
             // Electrical_analysis::Perform_analysis_on_clusters along x (unit-resistor pass, backbone,
             // real pass), the parameters of the hybrid configuration: rho_CNT 1e-3, GNP in-plane 1e-4
             // and through-plane 1 Ohm um, exponential tunnelling junctions (Input_Reader.cpp:1445-1456),
@@ -635,12 +646,14 @@ int main(int argc, char** argv) {
             std::vector<std::vector<long int> > ss = sg;
             Electrical_analysis EA;
             auto ft4 = fclk::now();
-            if (!EA.Perform_analysis_on_clusters(0, win, sp, ep, cf, vf, of, &HF, &CW, structure, pts, radii, pg, sg, gf)) return 25;
-            flow_seconds.push_back(fsecs(ft4, fclk::now()));
-            o.f64("flow_seconds", flow_seconds);
+            if (g_tol_unit <= 0) {
+                if (!EA.Perform_analysis_on_clusters(0, win, sp, ep, cf, vf, of, &HF, &CW, structure, pts, radii, pg, sg, gf)) return 25;
+                flow_seconds.push_back(fsecs(ft4, fclk::now()));
+            }
+            std::vector<double> res;
             // ---- staged replay of Perform_analysis_on_clusters (Electrical_analysis.cpp:10-145) and
             // Electrical_resistance_along_each_percolated_direction (:229-289), dumping each stage (e_*)
-            if (staged) {
+            if (replay) {
                 std::vector<std::vector<long int> > pb;  // GNP boundary points kept by Remove_gnp_points_in_non_relevant_boundaries
                 for (const GNP& g : gs) {
                     std::vector<long int> v;
@@ -729,13 +742,34 @@ int main(int argc, char** argv) {
                 for (double v : BN->dead_gnps) vols.push_back(v);
                 o.f64("e_bn_volumes", vols);
                 delete BN;
+                if (g_tol_unit > 0) {
+                    // Calculate_resistances_and_resistivities (Electrical_analysis.cpp:873-987): parallel
+                    // resistors of each direction, the matrix resistance where none percolates
+                    const double len[3] = {win.len_x, win.wid_y, win.hei_z};
+                    const double area[3] = {win.wid_y * win.hei_z, win.len_x * win.hei_z, win.len_x * win.wid_y};
+                    for (int d = 0; d < 3; d++) {
+                        if (par[d].empty()) {
+                            res.push_back(ep.resistivity_matrix * len[d] / area[d]);
+                            continue;
+                        }
+                        if (par[d].size() == 1) {
+                            res.push_back(par[d].front());
+                            continue;
+                        }
+                        double inv = 0;
+                        for (double r : par[d]) inv = inv + 1 / r;
+                        res.push_back(1 / inv);
+                    }
+                    flow_seconds.push_back(fsecs(ft4, fclk::now()));
+                }
             }
-            std::vector<double> res;
-            if (FILE* rf = fopen("resistances.txt", "r")) {
-                double v;
-                while (fscanf(rf, "%lf", &v) == 1) res.push_back(v);
-                fclose(rf);
-            }
+            o.f64("flow_seconds", flow_seconds);
+            if (g_tol_unit <= 0)
+                if (FILE* rf = fopen("resistances.txt", "r")) {
+                    double v;
+                    while (fscanf(rf, "%lf", &v) == 1) res.push_back(v);
+                    fclose(rf);
+                }
             o.f64("flow_resistances", res);
         }
     }

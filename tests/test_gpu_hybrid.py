@@ -95,3 +95,44 @@ def test_hybrid_chain_on_device_matches_upstream_flow(cuda_ok, tmp_path, tag):
         want = _csr(f, "flow_" + fk)
         assert got == want or (want == [] and all(not g for g in got)), key
     np.testing.assert_allclose(np.array(r.resistances), f["flow_resistances"], rtol=1e-6)
+
+
+def test_hybrid_configuration_against_upstream_binary(cuda_ok, tmp_path):
+    """The hybrid configuration at its full size (4 um cube, 8,000 CNTs, 1,500 GNPs,
+    seeded; eight GNPs lie outside Cutoff_Wins::gnps_inside) through the whole device
+    path, against upstream's own stages run at test time (oracle/_ref/gnp_dump, flow
+    mode, unit-resistor pass to 1e-12 on both sides, real pass to 1e-10): equal
+    clusters, isolated particles, families and junction groups, and R_x within what
+    the CG tolerances leave."""
+    import os
+    import subprocess
+
+    from cicy_geom_b200.hybrid import hybrid_network_to_conductance
+    from cicy_geom_b200.network import NetworkConfig, generate_cnt_network, generate_gnps, write_gnp_file, write_read_network_files
+    from oracle.dumpio import read_dump
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = os.path.join(root, "oracle", "_ref", "gnp_dump")
+    if not os.path.exists(exe):
+        pytest.skip("oracle/_ref/gnp_dump not built")
+    cfg = NetworkConfig(side=4.0, n_cnts=8000, seed=4_200_001, resistances=(1, 0, 0), tolerance_unit=1e-12)
+    d = str(tmp_path)
+    write_read_network_files(d, generate_cnt_network(cfg), cfg)
+    write_gnp_file(d, generate_gnps(1500, 4.0, 4_200_002))
+    ov_gnp = float(cfg.gs_min / np.sqrt(8.0))
+    subprocess.run([exe, d, os.path.join(d, "ref.bin"), repr(cfg.vdw), repr(cfg.tunnel), repr(cfg.gs_min), repr(2 * cfg.radius + cfg.tunnel),
+                    repr(ov_gnp), "-1", "flow", repr(cfg.step), "electrical_time", "1e-12"], check=True, capture_output=True, timeout=900)
+    z = read_dump(os.path.join(d, "ref.bin"))
+    assert len(z["flow_gnps_inside"]) < 1500
+    ctx = Context(0)
+    ctx.set_solver(0, 3)
+    r, _, st = hybrid_network_to_conductance(d, cfg, ov_gnp, ctx=ctx)
+    mc = st["mixed"]
+    assert mc["family"].tolist() == z["flow_family"].tolist()
+    for key, fk in (("clusters_cnt", "clusters_cnt"), ("clusters_gnp", "clusters_gnp"), ("isolated_cnt", "isolated_cnt"),
+                    ("isolated_gnp", "isolated_gnp"), ("cnt_junctions", "cluster_cnt_junctions"), ("gnp_junctions", "cluster_gnp_junctions"),
+                    ("mix_junctions", "cluster_mix_junctions")):
+        got = [list(mc[key + "_idx"][mc[key + "_ptr"][k]:mc[key + "_ptr"][k + 1]]) for k in range(len(mc[key + "_ptr"]) - 1)]
+        want = _csr(z, "flow_" + fk)
+        assert got == want or (want == [] and all(not g for g in got)), key
+    np.testing.assert_allclose(np.array(r.resistances), z["flow_resistances"], rtol=1e-6)
