@@ -112,7 +112,7 @@ struct MgWork {
     DBuf<unsigned long long> bar;
     DBuf<uint64_t> keys;
     DBuf<uint32_t> vals;
-    DBuf<int32_t> flag, pos, head, uidx, mate, best, rep, total, scan_tmp;
+    DBuf<int32_t> flag, pos, head, uidx, mate, best, rep, total, scan_tmp, long_rows;
     RadixScratch radix;
     int levels = 0;
     bool dense = false;

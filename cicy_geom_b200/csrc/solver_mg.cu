@@ -659,19 +659,25 @@ __global__ void __launch_bounds__(kMgClusterThreads) k_mg_batch(const MgArgs* __
 }
 
 // ---------------------------------------------------------------------------
-// Clustered grid kernel for systems above one cluster's size.  The grid is K clusters of
-// kSecCtas CTAs (cooperative launch).  Level 0 and the levels above `lc` run grid-wide as in
-// k_mg_pcg, on the fused rows (one gathered dot product per restriction or prolongation row);
-// levels lc .. coarsest (at most kSecRows rows at lc) are solved by every cluster on its own
-// copy of their vectors, between hardware cluster barriers (~0.3 us) instead of grid
-// barriers (~1.3 us).  Per CG iteration that leaves 4 + 2 (lc - 1) grid barriers.
-constexpr int kSecCtas = 16;       // CTAs per cluster (non-portable size)
-constexpr int kSecThreads = 512;
-constexpr int kSecGroup = 4;       // lanes per coarse row
-constexpr int kSecRows = 8192;     // largest level the clusters solve alone
-constexpr int kSecMaxClusters = 9; // 144 CTAs: one per SM
+// Shared-memory-resident clustered grid kernel for systems above one cluster's size.
+//
+// The grid is K clusters of kSmCtas CTAs, one CTA per SM (cooperative launch).  Every
+// operator of the V-cycle is static during the solve, so each CTA copies once, at launch,
+// the rows it owns into shared memory: its level-0 rows (CSR, column aggregates, chain-block
+// inverses, aggregate ranges) with the CG vectors of those rows, and its share of the fused
+// restriction / prolongation rows of every coarse level.  A phase then costs one round trip
+// for the vector entries other CTAs wrote, plus its barrier, instead of three to six
+// dependent L2 round trips for indices, weights and vectors.  Levels lc .. coarsest (at most
+// kSmRows rows at lc) are solved by every cluster on its own copy of their vectors between
+// hardware cluster barriers (~0.3 us) instead of grid barriers (~1.1 us plus skew).  A row
+// set that does not fit the shared-memory budget is read from global memory instead.
+constexpr int kSmCtas = 8;          // CTAs per cluster (portable size)
+constexpr int kSmThreads = 512;
+constexpr int kSmRows = 4096;       // largest level the clusters solve alone
+constexpr int kSmMaxClusters = 18;  // 144 CTAs
+constexpr int kSmBytes = 200 * 1024;
 
-struct MgSecLevel {
+struct MgSmLevel {
     int n;
     const int32_t* rr_ptr;  // fused restriction rows into level l + 1 (1 <= l < coarsest)
     const int32_t* rr_col;
@@ -684,13 +690,55 @@ struct MgSecLevel {
     double* r;
     double* z;
     double* zf;
-    int priv;  // bit 0: r and z per cluster (stride n), bit 1: zf per cluster
+    int priv;      // bit 0: r and z per cluster (stride n), bit 1: zf per cluster
+    int rr_lanes;  // lanes per restriction row into l + 1 / per prolongation row of l (powers of two)
+    int pq_lanes;
 };
 
-struct MgSecArgs {
+struct MgSmArgs {
     int lc;                  // first level the clusters solve alone (>= 1)
-    const MgSecLevel* lv;    // levels 0 .. coarsest (level 0: unused but for the count)
+    const MgSmLevel* lv;     // levels 0 .. coarsest
     int* cl_fail;            // per cluster: a grid-barrier wait of one of its CTAs gave up
+    const int32_t* mptr0;    // level-0 aggregates (the chain blocks): first row of each, then n
+    int smem_bytes;          // dynamic shared memory of the launch
+};
+
+// Rows [lo, hi) of one fused operator.  ptr[i - lo] - sub and ptr[i - lo + 1] - sub bound the
+// entries of row i in col / val; agg and l1inv are indexed by i - lo.  Staged copies have
+// sub = 0; a set read from global memory points into the global arrays with sub = ptr[lo].
+struct SmRows {
+    int lo, hi, sub;
+    const int32_t* ptr;
+    const int32_t* col;
+    const double* val;
+    const int32_t* agg;
+    const double* l1inv;
+};
+
+// The CTA's level-0 rows [lo, hi): CSR (entries ent_sub-based), column aggregates, chain-block
+// inverse rows (tinv, row offsets tofs-based, block bases lo-based), aggregates alo .. ahi with
+// their row ranges (lo-based), and the CG vectors of its rows (lo-based).
+struct SmL0 {
+    int lo, hi, alo, ahi;
+    int rp_sub, roff_sub, rbase_sub, mptr_sub;
+    const int32_t *rp, *ci, *cagg, *roff, *rbase, *rm, *agg, *mptr;
+    const double *val, *tinv, *b;
+    double *r, *x, *p, *q, *z, *z0, *w;
+};
+
+struct SmPlan {
+    SmL0 l0;
+    SmRows R[kMgMaxLevels];  // restriction rows into level l + 1 (index l)
+    SmRows Q[kMgMaxLevels];  // prolongation rows of level l
+    int clo, chi;            // coarsest rows of this CTA (dense inverse rows)
+    const double* cinv;      // its rows, (i - clo) * nC based
+    unsigned int used;
+};
+
+struct SmStage {  // one copy from global into shared memory
+    void* dst;
+    const void* src;
+    int count, elem, rebase;  // elem 4: int32 (minus rebase), 8: double
 };
 
 __device__ __forceinline__ void cluster_sync_all() {
@@ -702,18 +750,18 @@ __device__ __forceinline__ void cluster_sync_all() {
 // gave up marks its cluster before the cluster barrier, and every CTA of the cluster reads
 // that mark after it, so a cluster leaves as a whole and no cluster barrier waits on a CTA
 // that has returned.
-__device__ __forceinline__ bool sec_sync(const MgArgs& a, const MgSecArgs& sa, unsigned long long& target, int cid, int* s_ok) {
+__device__ __forceinline__ bool sm_sync(const MgArgs& a, int* cl_fail, unsigned long long& target, int cid, int* s_ok) {
     const bool ok = mg_sync(a.bar, target, a.err, s_ok, a.spin_limit);
-    if (!ok && threadIdx.x == 0) atomicExch(&sa.cl_fail[cid], 1);
+    if (!ok && threadIdx.x == 0) atomicExch(&cl_fail[cid], 1);
     cluster_sync_all();
-    return __ldcg(&sa.cl_fail[cid]) == 0;
+    return __ldcg(&cl_fail[cid]) == 0;
 }
 
 // sum_k val[k] v(col[k]) with v(c) = v0[c] for c < n, else v1[c - n]; chunks of U entries
 // per lane (indices and weights first, vector entries second).
 template <int U>
-__device__ __forceinline__ double fused_dot(const int32_t* __restrict__ col, const double* __restrict__ val, int b, int e, int first,
-                                            int step, int n, const double* v0, const double* v1) {
+__device__ __forceinline__ double fused_dot(const int32_t* col, const double* val, int b, int e, int first, int step, int n,
+                                            const double* v0, const double* v1) {
     double s = 0;
     for (int k0 = b + first; k0 < e; k0 += U * step) {
         int c[U];
@@ -732,51 +780,112 @@ __device__ __forceinline__ double fused_dot(const int32_t* __restrict__ col, con
     return s;
 }
 
-__device__ __forceinline__ double sec_group_sum(double v, unsigned mask) {
-    for (int o = kSecGroup / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, kSecGroup);
+__device__ __forceinline__ double lanes_sum(double v, int lanes) {
+    const unsigned mask = lanes >= 32 ? 0xffffffffu : (((1u << lanes) - 1) << ((threadIdx.x & 31) & ~(lanes - 1)));
+    for (int o = lanes / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, lanes);
     return v;
 }
 
-// Restriction rows [lo, hi) of level l + 1: r_{l+1} = P^T (r_l - A_l z_l), z_{l+1} = l1-Jacobi of it.
-__device__ __forceinline__ void sec_restrict(const MgSecLevel& F, const MgSecLevel& G, bool smooth, int lo, int hi) {
-    const int grp = threadIdx.x / kSecGroup, glane = threadIdx.x % kSecGroup, ngrp = blockDim.x / kSecGroup;
-    const unsigned gmask = ((1u << kSecGroup) - 1) << ((threadIdx.x & 31) & ~(kSecGroup - 1));
-    for (int J = lo + grp; J < hi; J += ngrp) {
-        double v = fused_dot<4>(F.rr_col, F.rr_val, F.rr_ptr[J], F.rr_ptr[J + 1], glane, kSecGroup, F.n, F.r, F.z);
-        v = sec_group_sum(v, gmask);
-        if (glane == 0) {
-            G.r[J] = v;
-            if (smooth) G.z[J] = G.l1inv[J] * v;
+// r_{l+1} = P^T (r_l - A_l z_l) and its l1-Jacobi smoothing on the rows of R.
+__device__ __forceinline__ void sm_restrict(const SmRows& R, int lanes, int nF, const double* rF, const double* zF, double* rG, double* zG,
+                                            bool smooth) {
+    const int grp = threadIdx.x / lanes, gl = threadIdx.x % lanes, ngrp = blockDim.x / lanes;
+    for (int J = R.lo + grp; J < R.hi; J += ngrp) {
+        const int j = J - R.lo;
+        double v = fused_dot<4>(R.col, R.val, R.ptr[j] - R.sub, R.ptr[j + 1] - R.sub, gl, lanes, nF, rF, zF);
+        v = lanes_sum(v, lanes);
+        if (gl == 0) {
+            rG[J] = v;
+            if (smooth) zG[J] = R.l1inv[j] * v;
         }
     }
 }
 
-// Prolongation and l1-Jacobi post-smoother on rows [lo, hi) of level l:
-// zp = z_l + P zc, zf_l = zp + D^-1 (r_l - A_l zp).
-__device__ __forceinline__ void sec_prolong(const MgSecLevel& F, const double* zc, int lo, int hi) {
-    const int grp = threadIdx.x / kSecGroup, glane = threadIdx.x % kSecGroup, ngrp = blockDim.x / kSecGroup;
-    const unsigned gmask = ((1u << kSecGroup) - 1) << ((threadIdx.x & 31) & ~(kSecGroup - 1));
-    for (int I = lo + grp; I < hi; I += ngrp) {
+// zp = z_l + P zc, zf_l = zp + D^-1 (r_l - A_l zp) on the rows of Q.
+__device__ __forceinline__ void sm_prolong(const SmRows& Q, int lanes, int nF, const double* rF, const double* zF, const double* zc, double* zf) {
+    const int grp = threadIdx.x / lanes, gl = threadIdx.x % lanes, ngrp = blockDim.x / lanes;
+    for (int I = Q.lo + grp; I < Q.hi; I += ngrp) {
+        const int i = I - Q.lo;
         double zp = 0, rI = 0;
-        if (glane == 0) {
-            zp = __ldcg(&F.z[I]) + __ldcg(&zc[F.agg[I]]);
-            rI = __ldcg(&F.r[I]);
+        if (gl == 0) {
+            zp = __ldcg(&zF[I]) + __ldcg(&zc[Q.agg[i]]);
+            rI = __ldcg(&rF[I]);
         }
-        double v = fused_dot<4>(F.pq_col, F.pq_val, F.pq_ptr[I], F.pq_ptr[I + 1], glane, kSecGroup, F.n, F.z, zc);
-        v = sec_group_sum(v, gmask);
-        if (glane == 0) F.zf[I] = zp + F.l1inv[I] * (rI - v);
+        double v = fused_dot<4>(Q.col, Q.val, Q.ptr[i] - Q.sub, Q.ptr[i + 1] - Q.sub, gl, lanes, nF, zF, zc);
+        v = lanes_sum(v, lanes);
+        if (gl == 0) zf[I] = zp + Q.l1inv[i] * (rI - v);
     }
 }
 
-__global__ void __launch_bounds__(kSecThreads) k_mg_pcg_sec(MgArgs a, MgSecArgs sa) {
+// Thread 0: place rows [lo, hi) of (ptr, col, val) plus optional per-row agg / l1inv into the
+// shared budget, or point at global memory; records the copies in st[] (returns their count).
+__device__ int sm_place_rows(SmRows& R, int lo, int hi, const int32_t* ptr, const int32_t* col, const double* val, const int32_t* agg,
+                             const double* l1inv, unsigned char* base, unsigned int cap, unsigned int& used, SmStage* st, int ns, int max_st) {
+    R.lo = lo;
+    R.hi = hi;
+    R.agg = agg ? agg + lo : nullptr;
+    R.l1inv = l1inv ? l1inv + lo : nullptr;
+    if (hi <= lo || !ptr) {
+        R.ptr = ptr ? ptr + lo : nullptr;
+        R.col = col;
+        R.val = val;
+        R.sub = 0;
+        return ns;
+    }
+    const int e0 = ptr[lo], e1 = ptr[hi], E = e1 - e0, nr = hi - lo;
+    auto al = [](unsigned int u) { return (u + 15u) & ~15u; };
+    unsigned int u = al(used);
+    const unsigned int o_ptr = u;
+    u = al(u + 4u * (nr + 1));
+    const unsigned int o_col = u;
+    u = al(u + 4u * E);
+    const unsigned int o_val = u;
+    u = al(u + 8u * E);
+    const unsigned int o_agg = u;
+    if (agg) u = al(u + 4u * nr);
+    const unsigned int o_l1 = u;
+    if (l1inv) u = al(u + 8u * nr);
+    if (u > cap || ns + 5 > max_st) {  // read from global memory
+        R.ptr = ptr + lo;
+        R.col = col + e0;
+        R.val = val + e0;
+        R.sub = e0;
+        return ns;
+    }
+    used = u;
+    R.ptr = reinterpret_cast<const int32_t*>(base + o_ptr);
+    R.col = reinterpret_cast<const int32_t*>(base + o_col);
+    R.val = reinterpret_cast<const double*>(base + o_val);
+    R.sub = 0;
+    st[ns++] = SmStage{base + o_ptr, ptr + lo, nr + 1, 4, e0};
+    st[ns++] = SmStage{base + o_col, col + e0, E, 4, 0};
+    st[ns++] = SmStage{base + o_val, val + e0, E, 8, 0};
+    if (agg) {
+        R.agg = reinterpret_cast<const int32_t*>(base + o_agg);
+        st[ns++] = SmStage{base + o_agg, agg + lo, nr, 4, 0};
+    }
+    if (l1inv) {
+        R.l1inv = reinterpret_cast<const double*>(base + o_l1);
+        st[ns++] = SmStage{base + o_l1, l1inv + lo, nr, 8, 0};
+    }
+    return ns;
+}
+
+constexpr int kSmMaxStages = 160;
+
+__global__ void __launch_bounds__(kSmThreads) k_mg_pcg_sm(MgArgs a, MgSmArgs sa) {
+    extern __shared__ __align__(16) unsigned char sm_dyn[];
     __shared__ double sm[72];
-    __shared__ MgSecLevel lv[kMgMaxLevels];
-    __shared__ MgLevel lv0;
+    __shared__ MgSmLevel lv[kMgMaxLevels];
+    __shared__ SmPlan P;
+    __shared__ SmStage st[kSmMaxStages];
+    __shared__ int n_st;
     __shared__ int s_ok;
     const int cta = blockIdx.x, nb = gridDim.x;
-    const int cid = cta / kSecCtas, crank = cta % kSecCtas;
+    const int cid = cta / kSmCtas, crank = cta % kSmCtas;
+    const int C = a.levels - 1, Lc = sa.lc;
     if (threadIdx.x < a.levels) {
-        MgSecLevel L = sa.lv[threadIdx.x];
+        MgSmLevel L = sa.lv[threadIdx.x];
         if (L.priv & 1) {
             L.r += (size_t)cid * L.n;
             L.z += (size_t)cid * L.n;
@@ -784,14 +893,150 @@ __global__ void __launch_bounds__(kSecThreads) k_mg_pcg_sec(MgArgs a, MgSecArgs 
         if (L.priv & 2) L.zf += (size_t)cid * L.n;
         lv[threadIdx.x] = L;
     }
-    if (threadIdx.x == 0) lv0 = a.lv[0];
     __syncthreads();
-    const int C = a.levels - 1, Lc = sa.lc;
-    const int r_lo = a.cta_row[cta], r_hi = a.cta_row[cta + 1];
-    auto grid_lo = [&](int n) { return (int)((long long)n * cta / nb); };
-    auto grid_hi = [&](int n) { return (int)((long long)n * (cta + 1) / nb); };
-    auto cl_lo = [&](int n) { return (int)((long long)n * crank / kSecCtas); };
-    auto cl_hi = [&](int n) { return (int)((long long)n * (crank + 1) / kSecCtas); };
+    // ---- placement (thread 0), then the copies (all threads) ----
+    if (threadIdx.x == 0) {
+        const unsigned int cap = (unsigned int)sa.smem_bytes;
+        unsigned int used = 0;
+        int ns = 0;
+        auto al = [](unsigned int u) { return (u + 15u) & ~15u; };
+        auto take = [&](unsigned int bytes) -> unsigned char* {
+            const unsigned int u = al(used);
+            if (u + bytes > cap) return nullptr;
+            used = u + bytes;
+            return sm_dyn + u;
+        };
+        SmL0& L = P.l0;
+        const MgLevel& G0 = a.lv[0];
+        L.lo = a.cta_row[cta];
+        L.hi = a.cta_row[cta + 1];
+        const int nr = L.hi - L.lo;
+        // vectors of the own rows (x, r from global; the others are written before read)
+        double* vec = nr > 0 ? reinterpret_cast<double*>(take(8u * 7 * nr)) : nullptr;
+        if (vec) {
+            L.r = vec; L.x = vec + nr; L.p = vec + 2 * nr; L.q = vec + 3 * nr; L.z = vec + 4 * nr; L.z0 = vec + 5 * nr; L.w = vec + 6 * nr;
+            st[ns++] = SmStage{L.r, a.r + L.lo, nr, 8, 0};
+            st[ns++] = SmStage{L.x, a.x + L.lo, nr, 8, 0};
+        } else {
+            L.r = a.r + L.lo; L.x = a.x + L.lo; L.p = a.p + L.lo; L.q = a.q + L.lo; L.z = a.z + L.lo; L.z0 = a.z0 + L.lo; L.w = a.w + L.lo;
+        }
+        L.b = a.b + L.lo;
+        // CSR rows with their column aggregates
+        const int e0 = nr > 0 ? a.rp[L.lo] : 0, E = nr > 0 ? a.rp[L.hi] - e0 : 0;
+        unsigned char* m_rp = nr > 0 ? take(4u * (nr + 1)) : nullptr;
+        unsigned char* m_ci = m_rp ? take(4u * E) : nullptr;
+        unsigned char* m_cg = m_ci ? take(4u * E) : nullptr;
+        unsigned char* m_v = m_cg ? take(8u * E) : nullptr;
+        if (m_v) {
+            L.rp = reinterpret_cast<const int32_t*>(m_rp); L.rp_sub = 0;
+            L.ci = reinterpret_cast<const int32_t*>(m_ci);
+            L.cagg = reinterpret_cast<const int32_t*>(m_cg);
+            L.val = reinterpret_cast<const double*>(m_v);
+            st[ns++] = SmStage{m_rp, a.rp + L.lo, nr + 1, 4, e0};
+            st[ns++] = SmStage{m_ci, a.ci + e0, E, 4, 0};
+            st[ns++] = SmStage{m_cg, G0.cagg + e0, E, 4, 0};
+            st[ns++] = SmStage{m_v, a.val + e0, E, 8, 0};
+        } else {
+            L.rp = a.rp + L.lo; L.rp_sub = e0;
+            L.ci = a.ci + e0; L.cagg = G0.cagg + e0; L.val = a.val + e0;
+        }
+        // chain-block inverse rows
+        const int t0 = nr > 0 ? a.row_off[L.lo] : 0;
+        const int T = nr > 0 ? a.row_off[L.hi - 1] + a.row_m[L.hi - 1] - t0 : 0;
+        unsigned char* m_meta = nr > 0 ? take(12u * nr) : nullptr;
+        unsigned char* m_t = m_meta ? take(8u * T) : nullptr;
+        if (m_t) {
+            L.roff = reinterpret_cast<const int32_t*>(m_meta); L.roff_sub = 0;
+            L.rbase = L.roff + nr; L.rbase_sub = 0;
+            L.rm = L.rbase + nr;
+            L.tinv = reinterpret_cast<const double*>(m_t);
+            st[ns++] = SmStage{m_meta, a.row_off + L.lo, nr, 4, t0};
+            st[ns++] = SmStage{m_meta + 4u * nr, a.row_base + L.lo, nr, 4, L.lo};
+            st[ns++] = SmStage{m_meta + 8u * nr, a.row_m + L.lo, nr, 4, 0};
+            st[ns++] = SmStage{m_t, a.tinv + t0, T, 8, 0};
+        } else {
+            L.roff = a.row_off + L.lo; L.roff_sub = t0;
+            L.rbase = a.row_base + L.lo; L.rbase_sub = L.lo;
+            L.rm = a.row_m + L.lo;
+            L.tinv = a.tinv + t0;
+        }
+        // row -> aggregate, and the own aggregates' row ranges
+        L.alo = nr > 0 ? G0.agg[L.lo] : 0;
+        L.ahi = nr > 0 ? G0.agg[L.hi - 1] + 1 : 0;
+        const int na = L.ahi - L.alo;
+        unsigned char* m_ag = nr > 0 ? take(4u * nr) : nullptr;
+        unsigned char* m_mp = m_ag ? take(4u * (na + 1)) : nullptr;
+        if (m_mp) {
+            L.agg = reinterpret_cast<const int32_t*>(m_ag);
+            L.mptr = reinterpret_cast<const int32_t*>(m_mp); L.mptr_sub = 0;
+            st[ns++] = SmStage{m_ag, G0.agg + L.lo, nr, 4, 0};
+            st[ns++] = SmStage{m_mp, sa.mptr0 + L.alo, na + 1, 4, L.lo};
+        } else {
+            L.agg = G0.agg + L.lo;
+            L.mptr = sa.mptr0 + L.alo; L.mptr_sub = L.lo;
+        }
+        // coarse levels: grid rows below lc, cluster rows from lc on
+        auto lanes_for = [](long long entries, int rows) {
+            int ln = 2;
+            while (ln < 32 && (long long)ln * 4 * rows < entries) ln <<= 1;  // about one chunk of 4 entries per lane
+            return ln;
+        };
+        for (int l = 1; l < C; l++) {
+            MgSmLevel& F = lv[l];
+            const MgSmLevel& G = lv[l + 1];
+            F.rr_lanes = lanes_for(F.rr_ptr[G.n], G.n);
+            F.pq_lanes = lanes_for(F.pq_ptr[F.n], F.n);
+            const bool sec_r = l >= Lc, sec_q = l >= Lc;
+            const int n1 = G.n, n0 = F.n;
+            const int rlo = sec_r ? (int)((long long)n1 * crank / kSmCtas) : (int)((long long)n1 * cta / nb);
+            const int rhi = sec_r ? (int)((long long)n1 * (crank + 1) / kSmCtas) : (int)((long long)n1 * (cta + 1) / nb);
+            ns = sm_place_rows(P.R[l], rlo, rhi, F.rr_ptr, F.rr_col, F.rr_val, nullptr, G.l1inv, sm_dyn, cap, used, st, ns, kSmMaxStages);
+            const int qlo = sec_q ? (int)((long long)n0 * crank / kSmCtas) : (int)((long long)n0 * cta / nb);
+            const int qhi = sec_q ? (int)((long long)n0 * (crank + 1) / kSmCtas) : (int)((long long)n0 * (cta + 1) / nb);
+            ns = sm_place_rows(P.Q[l], qlo, qhi, F.pq_ptr, F.pq_col, F.pq_val, F.agg, F.l1inv, sm_dyn, cap, used, st, ns, kSmMaxStages);
+        }
+        const int nC = lv[C].n;
+        P.clo = (int)((long long)nC * crank / kSmCtas);
+        P.chi = (int)((long long)nC * (crank + 1) / kSmCtas);
+        P.cinv = nullptr;
+        if (a.cinv) {
+            const int cr = P.chi - P.clo;
+            unsigned char* m_c = cr > 0 && ns < kSmMaxStages ? take(8u * cr * nC) : nullptr;
+            if (m_c) {
+                P.cinv = reinterpret_cast<const double*>(m_c);
+                st[ns++] = SmStage{m_c, a.cinv + (size_t)P.clo * nC, cr * nC, 8, 0};
+            } else {
+                P.cinv = a.cinv + (size_t)P.clo * nC;
+            }
+        }
+        P.used = used;
+        n_st = ns;
+    }
+    __syncthreads();
+    for (int q = 0; q < n_st; q++) {
+        const SmStage S = st[q];
+        if (S.elem == 8) {
+            double* d = static_cast<double*>(S.dst);
+            const double* g = static_cast<const double*>(S.src);
+            for (int i = threadIdx.x; i < S.count; i += blockDim.x) d[i] = g[i];
+        } else {
+            int32_t* d = static_cast<int32_t*>(S.dst);
+            const int32_t* g = static_cast<const int32_t*>(S.src);
+            for (int i = threadIdx.x; i < S.count; i += blockDim.x) d[i] = g[i] - S.rebase;
+        }
+    }
+    __syncthreads();
+    const SmL0& L = P.l0;
+    const int lo = L.lo, hi = L.hi;
+    auto own = [&](int c) { return c >= lo && c < hi; };
+    // chain-block inverse row of own row li applied to a vector of own rows
+    auto block_row = [&](int li, const double* v) {
+        const int off = L.roff[li] - L.roff_sub, base = L.rbase[li] - L.rbase_sub, m = L.rm[li];
+        double s = 0;
+        for (int j = 0; j < m; j++) s += L.tinv[off + j] * v[base + j];
+        return s;
+    };
+    auto row_b = [&](int li) { return L.rp[li] - L.rp_sub; };
     unsigned long long target = 0;
     double R0 = 0, rr = 0, rz = 0, beta = 0;
     long long k = 0;
@@ -803,122 +1048,149 @@ __global__ void __launch_bounds__(kSecThreads) k_mg_pcg_sec(MgArgs a, MgSecArgs 
         // ---- pre-smoother z0 = w M0^-1 r on own rows; r.r ----
         __syncthreads();
         double rr_l = 0;
-        for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
-            a.z0[i] = a.omega0 * block_apply(a, a.r, i);
-            const double ri = a.r[i];
+        for (int li = threadIdx.x; li < hi - lo; li += blockDim.x) {
+            const double z0 = a.omega0 * block_row(li, L.r);
+            L.z0[li] = z0;
+            a.z0[lo + li] = z0;
+            const double ri = L.r[li];
             rr_l += ri * ri;
         }
         mg_reduce1(rr_l, sm, s0);
         if (threadIdx.x == 0) a.partA[cta] = s0;
-        if (!sec_sync(a, sa, target, cid, &s_ok)) return;
+        if (!sm_sync(a, sa.cl_fail, target, cid, &s_ok)) return;
         rr = mg_sum_partials(a.partA, nb, sm);
         if (k == 0 && !recursive && restarts == 0) R0 = a.tol * sqrt(rr);
         if (k > 0 && sqrt(rr) <= R0) {
             if (!recursive || restarts >= a.max_restarts) break;
-            for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) a.r[i] = a.b[i] - gather_dot<4>(a.ci, a.val, a.x, a.rp[i], a.rp[i + 1]);
+            // the recursive residual met the test: replace it by the FP64 true residual
+            for (int li = threadIdx.x; li < hi - lo; li += blockDim.x) {
+                double sx = 0;
+                for (int q = row_b(li); q < row_b(li + 1); q++) {
+                    const int c = L.ci[q];
+                    sx += L.val[q] * (own(c) ? L.x[c - lo] : __ldcg(&a.x[c]));
+                }
+                L.r[li] = L.b[li] - sx;
+            }
             restarts++;
             recursive = false;
             fresh = true;
             continue;
         }
         if (k >= a.max_iter) break;
-        // ---- level 0 -> 1 inside the CTA (its blocks, the level-0 aggregates, are its own rows) ----
+        // ---- w = r - A z0; level 0 -> 1 over the own aggregates (the chain blocks) ----
         {
-            for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) a.w[i] = a.r[i] - gather_dot<4>(a.ci, a.val, a.z0, a.rp[i], a.rp[i + 1]);
-            __syncthreads();
-            const MgSecLevel& G = lv[1];
-            const bool smooth = (C > 1) || a.cinv == nullptr;
-            if (r_hi > r_lo) {
-                const int b0 = lv0.agg[r_lo], b1 = lv0.agg[r_hi - 1];
-                for (int J = b0 + threadIdx.x; J <= b1; J += blockDim.x) {
-                    double v = 0;
-                    for (int m = lv0.mptr[J]; m < lv0.mptr[J + 1]; m++) v += a.w[lv0.midx[m]];
-                    G.r[J] = v;
-                    if (smooth) G.z[J] = G.l1inv[J] * v;
+            for (int li = threadIdx.x; li < hi - lo; li += blockDim.x) {
+                double sx = 0;
+                for (int q = row_b(li); q < row_b(li + 1); q++) {
+                    const int c = L.ci[q];
+                    sx += L.val[q] * (own(c) ? L.z0[c - lo] : __ldcg(&a.z0[c]));
                 }
+                L.w[li] = L.r[li] - sx;
             }
-            if (!sec_sync(a, sa, target, cid, &s_ok)) return;
+            __syncthreads();
+            const MgSmLevel& G = lv[1];
+            const bool smooth = (C > 1) || a.cinv == nullptr;
+            for (int J = L.alo + threadIdx.x; J < L.ahi; J += blockDim.x) {
+                const int j = J - L.alo;
+                const int m0 = L.mptr[j] - L.mptr_sub, m1 = L.mptr[j + 1] - L.mptr_sub;
+                double v = 0;
+                for (int m = m0; m < m1; m++) v += L.w[m];
+                G.r[J] = v;
+                if (smooth) G.z[J] = G.l1inv[J] * v;
+            }
+            if (!sm_sync(a, sa.cl_fail, target, cid, &s_ok)) return;
         }
         // ---- restrictions l -> l + 1 grid-wide (1 <= l < lc) ----
         for (int l = 1; l < Lc; l++) {
-            const int n1 = lv[l + 1].n;
-            sec_restrict(lv[l], lv[l + 1], (l + 1 < C) || a.cinv == nullptr, grid_lo(n1), grid_hi(n1));
-            if (!sec_sync(a, sa, target, cid, &s_ok)) return;
+            sm_restrict(P.R[l], lv[l].rr_lanes, lv[l].n, lv[l].r, lv[l].z, lv[l + 1].r, lv[l + 1].z, (l + 1 < C) || a.cinv == nullptr);
+            if (!sm_sync(a, sa.cl_fail, target, cid, &s_ok)) return;
         }
         // ---- levels lc .. coarsest: every cluster on its own copy ----
         for (int l = Lc; l < C; l++) {
-            const int n1 = lv[l + 1].n;
-            sec_restrict(lv[l], lv[l + 1], (l + 1 < C) || a.cinv == nullptr, cl_lo(n1), cl_hi(n1));
+            sm_restrict(P.R[l], lv[l].rr_lanes, lv[l].n, lv[l].r, lv[l].z, lv[l + 1].r, lv[l + 1].z, (l + 1 < C) || a.cinv == nullptr);
             cluster_sync_all();
         }
         {
-            const MgSecLevel& Cl = lv[C];
+            const MgSmLevel& Cl = lv[C];
             const int nC = Cl.n;
             const int wpb = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
             if (a.cinv) {  // dense inverse of the coarsest level, one warp per row
-                for (int i = crank * wpb + warp; i < nC; i += kSecCtas * wpb) {
-                    const double* row = a.cinv + (size_t)i * nC;
+                for (int i = P.clo + warp; i < P.chi; i += wpb) {
+                    const double* row = P.cinv + (size_t)(i - P.clo) * nC;
                     double v = 0;
                     for (int j = lane; j < nC; j += 32) v += row[j] * __ldcg(&Cl.r[j]);
                     v = warp_sum(v);
                     if (lane == 0) Cl.zf[i] = v;
                 }
             } else {  // l1-Jacobi only: the correction is the smoothed z
-                for (int i = cl_lo(nC) + threadIdx.x; i < cl_hi(nC); i += blockDim.x) Cl.zf[i] = __ldcg(&Cl.z[i]);
+                for (int i = P.clo + threadIdx.x; i < P.chi; i += blockDim.x) Cl.zf[i] = __ldcg(&Cl.z[i]);
             }
             cluster_sync_all();
         }
         for (int l = C - 1; l >= Lc; l--) {
-            sec_prolong(lv[l], lv[l + 1].zf, cl_lo(lv[l].n), cl_hi(lv[l].n));
+            sm_prolong(P.Q[l], lv[l].pq_lanes, lv[l].n, lv[l].r, lv[l].z, lv[l + 1].zf, lv[l].zf);
             cluster_sync_all();
         }
         // ---- prolongations lc - 1 .. 1 grid-wide ----
         for (int l = Lc - 1; l >= 1; l--) {
-            sec_prolong(lv[l], lv[l + 1].zf, grid_lo(lv[l].n), grid_hi(lv[l].n));
-            if (!sec_sync(a, sa, target, cid, &s_ok)) return;
+            sm_prolong(P.Q[l], lv[l].pq_lanes, lv[l].n, lv[l].r, lv[l].z, lv[l + 1].zf, lv[l].zf);
+            if (!sm_sync(a, sa.cl_fail, target, cid, &s_ok)) return;
         }
         // ---- level-0 post-smoother: z = z0 + P z1, z += w M0^-1 (r - A z); r.z ----
         {
             const double* zc = lv[1].zf;
-            for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
-                a.w[i] = a.r[i] - gather_dot2<4>(a.ci, lv0.cagg, a.val, a.z0, zc, a.rp[i], a.rp[i + 1]);
-                a.z[i] = a.z0[i] + __ldcg(&zc[lv0.agg[i]]);
+            for (int li = threadIdx.x; li < hi - lo; li += blockDim.x) {
+                double sx = 0;
+                for (int q = row_b(li); q < row_b(li + 1); q++) {
+                    const int c = L.ci[q];
+                    sx += L.val[q] * ((own(c) ? L.z0[c - lo] : __ldcg(&a.z0[c])) + __ldcg(&zc[L.cagg[q]]));
+                }
+                L.w[li] = L.r[li] - sx;
+                L.z[li] = L.z0[li] + __ldcg(&zc[L.agg[li]]);
             }
             __syncthreads();
             double rz_l = 0;
-            for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
-                const double zi = a.z[i] + a.omega0 * block_apply(a, a.w, i);
-                a.z[i] = zi;
-                rz_l += a.r[i] * zi;
+            for (int li = threadIdx.x; li < hi - lo; li += blockDim.x) {
+                const double zi = L.z[li] + a.omega0 * block_row(li, L.w);
+                L.z[li] = zi;
+                a.z[lo + li] = zi;
+                rz_l += L.r[li] * zi;
             }
             mg_reduce1(rz_l, sm, s0);
             if (threadIdx.x == 0) a.partB[cta] = s0;
-            if (!sec_sync(a, sa, target, cid, &s_ok)) return;
+            if (!sm_sync(a, sa.cl_fail, target, cid, &s_ok)) return;
             const double rz_new = mg_sum_partials(a.partB, nb, sm);
             beta = fresh ? 0.0 : rz_new / rz;
             rz = rz_new;
         }
         // ---- q = A z + beta q, p = z + beta p; p.q ----
         double pq_l = 0;
-        for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
-            const double w = gather_dot<4>(a.ci, a.val, a.z, a.rp[i], a.rp[i + 1]);
-            const double zi = a.z[i];
-            const double qi = fresh ? w : w + beta * a.q[i];
-            const double pi = fresh ? zi : zi + beta * a.p[i];
-            a.q[i] = qi;
-            a.p[i] = pi;
+        for (int li = threadIdx.x; li < hi - lo; li += blockDim.x) {
+            double w = 0;
+            for (int q = row_b(li); q < row_b(li + 1); q++) {
+                const int c = L.ci[q];
+                w += L.val[q] * (own(c) ? L.z[c - lo] : __ldcg(&a.z[c]));
+            }
+            const double zi = L.z[li];
+            const double qi = fresh ? w : w + beta * L.q[li];
+            const double pi = fresh ? zi : zi + beta * L.p[li];
+            L.q[li] = qi;
+            L.p[li] = pi;
             pq_l += pi * qi;
         }
         mg_reduce1(pq_l, sm, s0);
         if (threadIdx.x == 0) a.partA[nb + cta] = s0;
-        if (!sec_sync(a, sa, target, cid, &s_ok)) return;
+        if (!sm_sync(a, sa.cl_fail, target, cid, &s_ok)) return;
         const double pq = mg_sum_partials(a.partA + nb, nb, sm);
         fresh = false;
         k++;
+        // ---- x += alpha p, r -= alpha q (x also to global: other CTAs read it for a true residual) ----
         const double alpha = rz / pq;
-        for (int i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
-            a.x[i] += alpha * a.p[i];
-            a.r[i] -= alpha * a.q[i];
+        for (int li = threadIdx.x; li < hi - lo; li += blockDim.x) {
+            const double xi = L.x[li] + alpha * L.p[li];
+            L.x[li] = xi;
+            a.x[lo + li] = xi;
+            L.r[li] -= alpha * L.q[li];
         }
         recursive = true;
     }
@@ -1017,18 +1289,122 @@ __global__ void k_agg_lengths(int nc, const int32_t* __restrict__ mptr, const in
     }
 }
 
-// One coarse row per thread: the cross-aggregate couplings of the members (in
-// member then entry order) are gathered into scratch as keys (coarse column,
-// gather position), sorted (Shell sort: keys are unique, so the order equals a
-// stable sort by column) and summed per column in gather order (deterministic);
-// the row's diagonal comes from the summed row sums (no cancellation of the
-// large intra-aggregate entries), and its l1-Jacobi weight from |d| + sum |a|.
-__global__ void k_coarse_rows(int nc, const int32_t* __restrict__ mptr, const int32_t* __restrict__ midx, const int32_t* __restrict__ rp,
-                              const int32_t* __restrict__ ci, const double* __restrict__ v, const int32_t* __restrict__ agg,
-                              const double* __restrict__ rs_f, const int32_t* __restrict__ seg_off, uint64_t* __restrict__ skey,
-                              double* __restrict__ sval, int32_t* __restrict__ ulen, double* __restrict__ rs_c, double* __restrict__ diag,
-                              double* __restrict__ l1inv) {
-    for (int J = blockIdx.x * blockDim.x + threadIdx.x; J < nc; J += gridDim.x * blockDim.x) {
+// Coarse row J: the cross-aggregate couplings of its members (in member then entry
+// order), gathered as keys (coarse column, gather position) with their values, are sorted
+// (keys are unique, so the order equals a stable sort by column) and summed per column in
+// gather order (deterministic); the row's diagonal comes from the summed row sums (no
+// cancellation of the large intra-aggregate entries), and its l1-Jacobi weight from
+// |d| + sum |a|.  `reduce_row` does the summing and writes the compacted row at seg_off[J].
+__device__ __forceinline__ void reduce_row(int J, int cnt, double rs, const uint64_t* key, const double* val, uint64_t* __restrict__ okey,
+                                           double* __restrict__ oval, int32_t* __restrict__ ulen, double* __restrict__ rs_c,
+                                           double* __restrict__ diag, double* __restrict__ l1inv) {
+    int u = 0;
+    double off = 0, offabs = 0;
+    for (int i = 0; i < cnt;) {  // sum runs of equal columns, in gather order
+        const uint32_t c = (uint32_t)(key[i] >> 32);
+        double acc = 0;
+        while (i < cnt && (uint32_t)(key[i] >> 32) == c) acc += val[i++];
+        okey[u] = c;
+        oval[u] = acc;
+        u++;
+        off += acc;
+        offabs += fabs(acc);
+    }
+    ulen[J] = u;
+    const double d = rs - off;
+    rs_c[J] = rs;
+    diag[J] = d;
+    const double l1 = fabs(d) + offabs;
+    l1inv[J] = l1 > 0 ? 1.0 / l1 : 0.0;
+}
+
+// One warp per coarse row: the lanes gather a member row's couplings 32 at a time (ballot
+// ranks keep the gather order), a bitonic sort orders them in shared memory, lane 0 sums the
+// runs.  Rows with more than kCrCap couplings are listed for k_coarse_rows_long.
+constexpr int kCrWarps = 4;
+constexpr int kCrCap = 512;  // power of two
+__global__ void __launch_bounds__(kCrWarps * 32) k_coarse_rows(int nc, const int32_t* __restrict__ mptr, const int32_t* __restrict__ midx,
+                                                               const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                                               const double* __restrict__ v, const int32_t* __restrict__ agg,
+                                                               const double* __restrict__ rs_f, const int32_t* __restrict__ seg_off,
+                                                               uint64_t* __restrict__ skey, double* __restrict__ sval, int32_t* __restrict__ ulen,
+                                                               double* __restrict__ rs_c, double* __restrict__ diag, double* __restrict__ l1inv,
+                                                               int32_t* __restrict__ long_rows, int32_t* __restrict__ n_long) {
+    __shared__ uint64_t sk[kCrWarps][kCrCap];
+    __shared__ double sv[kCrWarps][kCrCap];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint64_t* K = sk[warp];
+    double* V = sv[warp];
+    for (int J = blockIdx.x * kCrWarps + warp; J < nc; J += gridDim.x * kCrWarps) {
+        int cnt = 0;
+        double rs = 0;
+        for (int m = mptr[J]; m < mptr[J + 1]; m++) {
+            const int I = midx[m];
+            if (lane == 0) rs += rs_f[I];
+            const int b = rp[I], e = rp[I + 1];
+            for (int k0 = b; k0 < e; k0 += 32) {
+                const int k = k0 + lane;
+                int c = -1;
+                double x = 0;
+                if (k < e) {
+                    c = agg[ci[k]];
+                    x = v[k];
+                }
+                const bool keep = k < e && c != J;
+                const unsigned bal = __ballot_sync(0xffffffffu, keep);
+                const int pos = cnt + __popc(bal & ((1u << lane) - 1));
+                if (keep && pos < kCrCap) {
+                    K[pos] = ((uint64_t)(uint32_t)c << 32) | (uint32_t)pos;
+                    V[pos] = x;
+                }
+                cnt += __popc(bal);
+            }
+        }
+        if (cnt > kCrCap) {
+            if (lane == 0) long_rows[atomicAdd(n_long, 1)] = J;
+            __syncwarp();
+            continue;
+        }
+        int P = 1;
+        while (P < cnt) P <<= 1;
+        for (int i = cnt + lane; i < P; i += 32) K[i] = ~0ull;
+        __syncwarp();
+        for (int size = 2; size <= P; size <<= 1)
+            for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                for (int i = lane; i < P; i += 32) {
+                    const int j = i ^ stride;
+                    if (j > i) {
+                        const bool up = (i & size) == 0;
+                        const uint64_t ki = K[i], kj = K[j];
+                        if ((ki > kj) == up) {
+                            K[i] = kj;
+                            K[j] = ki;
+                            const double t = V[i];
+                            V[i] = V[j];
+                            V[j] = t;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        if (lane == 0) {
+            const int o = seg_off[J];
+            reduce_row(J, cnt, rs, K, V, skey + o, sval + o, ulen, rs_c, diag, l1inv);
+        }
+        __syncwarp();
+    }
+}
+
+// The rows k_coarse_rows listed as too long for shared memory: one thread each, gathered and
+// Shell-sorted in the global scratch at seg_off[J].
+__global__ void k_coarse_rows_long(const int32_t* __restrict__ long_rows, const int32_t* __restrict__ n_long, const int32_t* __restrict__ mptr,
+                                   const int32_t* __restrict__ midx, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                   const double* __restrict__ v, const int32_t* __restrict__ agg, const double* __restrict__ rs_f,
+                                   const int32_t* __restrict__ seg_off, uint64_t* __restrict__ skey, double* __restrict__ sval,
+                                   int32_t* __restrict__ ulen, double* __restrict__ rs_c, double* __restrict__ diag, double* __restrict__ l1inv) {
+    const int nl = *n_long;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nl; t += gridDim.x * blockDim.x) {
+        const int J = long_rows[t];
         const int o = seg_off[J];
         int cnt = 0;
         double rs = 0;
@@ -1060,24 +1436,7 @@ __global__ void k_coarse_rows(int nc, const int32_t* __restrict__ mptr, const in
             }
             if (gap == 1) break;
         }
-        int u = 0;
-        double off = 0, offabs = 0;
-        for (int i = 0; i < cnt;) {  // sum runs of equal columns, in gather order
-            const uint32_t c = (uint32_t)(skey[o + i] >> 32);
-            double acc = 0;
-            while (i < cnt && (uint32_t)(skey[o + i] >> 32) == c) acc += sval[o + i++];
-            skey[o + u] = c;
-            sval[o + u] = acc;
-            u++;
-            off += acc;
-            offabs += fabs(acc);
-        }
-        ulen[J] = u;
-        const double d = rs - off;
-        rs_c[J] = rs;
-        diag[J] = d;
-        const double l1 = fabs(d) + offabs;
-        l1inv[J] = l1 > 0 ? 1.0 / l1 : 0.0;
+        reduce_row(J, cnt, rs, skey + o, sval + o, skey + o, sval + o, ulen, rs_c, diag, l1inv);
     }
 }
 
@@ -1142,9 +1501,15 @@ void coarsen(MgWork& g, int l, int nc, cudaStream_t s, int64_t& launches) {
     G.rs.ensure(nc);
     G.diag.ensure(nc);
     G.l1inv.ensure(nc);
-    k_coarse_rows<<<grid_for(nc, 128), 128, 0, s>>>(nc, F.mptr.get(), F.midx.get(), F.rp_ptr, F.ci_ptr, F.val_ptr, F.agg.get(), F.rs.get(),
-                                                  g.pos.get(), g.keys.get(), g.sval.get(), g.head.get(), G.rs.get(), G.diag.get(),
-                                                  G.l1inv.get());
+    g.long_rows.ensure(nc + 1);
+    CICY_CUDA(cudaMemsetAsync(g.total.get() + 1, 0, sizeof(int32_t), s));
+    k_coarse_rows<<<grid_for((long long)nc * 32, kCrWarps * 32), kCrWarps * 32, 0, s>>>(
+        nc, F.mptr.get(), F.midx.get(), F.rp_ptr, F.ci_ptr, F.val_ptr, F.agg.get(), F.rs.get(), g.pos.get(), g.keys.get(), g.sval.get(),
+        g.head.get(), G.rs.get(), G.diag.get(), G.l1inv.get(), g.long_rows.get(), g.total.get() + 1);
+    k_coarse_rows_long<<<grid_for(nc, 128), 128, 0, s>>>(g.long_rows.get(), g.total.get() + 1, F.mptr.get(), F.midx.get(), F.rp_ptr,
+                                                       F.ci_ptr, F.val_ptr, F.agg.get(), F.rs.get(), g.pos.get(), g.keys.get(),
+                                                       g.sval.get(), g.head.get(), G.rs.get(), G.diag.get(), G.l1inv.get());
+    launches++;
     scan_small(g.head.get(), G.rp.get(), nc + 1, nullptr, g, s, launches);
     k_coarse_copy<<<grid_for(nc), 256, 0, s>>>(nc, g.pos.get(), g.head.get(), G.rp.get(), g.keys.get(), g.sval.get(), G.ci.get(),
                                                G.val.get());
@@ -1333,26 +1698,27 @@ void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long 
         cluster = cudaOccupancyMaxActiveClusters(&nclusters, (void*)k_mg_pcg<true>, &cfg) == cudaSuccess && nclusters >= 1;
         cudaGetLastError();
     }
-    // above one cluster's size: the clustered grid kernel (levels from lc on solved per
-    // cluster) when the fused rows exist and K clusters of kSecCtas can be co-resident
+    // above one cluster's size: the shared-memory-resident clustered grid kernel (one CTA per
+    // SM, levels from lc on solved per cluster) when the fused rows exist and K clusters of
+    // kSmCtas can be co-resident
     bool sec = false;
     int K = 0;
     cudaLaunchConfig_t scfg = {};
     cudaLaunchAttribute sattr[2];
     if (!cluster && g.fused && g.levels >= 2) {
-        static int sec_state = 0;  // 0 unknown, 1 ok, -1 unsupported
-        if (sec_state == 0) {
-            sec_state = cudaFuncSetAttribute(k_mg_pcg_sec, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess ? 1 : -1;
+        static int sm_state = 0;  // 0 unknown, 1 ok, -1 unsupported
+        if (sm_state == 0) {
+            sm_state = cudaFuncSetAttribute(k_mg_pcg_sm, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmBytes) == cudaSuccess ? 1 : -1;
             cudaGetLastError();
         }
-        if (sec_state > 0) {
-            K = std::max(1, std::min({ceil_div(n, kSecCtas * kSecThreads), kSecMaxClusters, num_sms / kSecCtas}));
-            scfg.gridDim = dim3(K * kSecCtas);
-            scfg.blockDim = dim3(kSecThreads);
-            scfg.dynamicSmemBytes = 0;
+        if (sm_state > 0) {
+            K = std::max(1, std::min({ceil_div(n, kSmCtas * kSmThreads), kSmMaxClusters, num_sms / kSmCtas}));
+            scfg.gridDim = dim3(K * kSmCtas);
+            scfg.blockDim = dim3(kSmThreads);
+            scfg.dynamicSmemBytes = kSmBytes;
             scfg.stream = s;
             sattr[0].id = cudaLaunchAttributeClusterDimension;
-            sattr[0].val.clusterDim.x = kSecCtas;
+            sattr[0].val.clusterDim.x = kSmCtas;
             sattr[0].val.clusterDim.y = 1;
             sattr[0].val.clusterDim.z = 1;
             sattr[1].id = cudaLaunchAttributeCooperative;
@@ -1360,9 +1726,9 @@ void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long 
             scfg.attrs = sattr;
             scfg.numAttrs = 2;
             int ncl = 0;
-            if (cudaOccupancyMaxActiveClusters(&ncl, (void*)k_mg_pcg_sec, &scfg) == cudaSuccess && ncl >= 1) {
+            if (cudaOccupancyMaxActiveClusters(&ncl, (void*)k_mg_pcg_sm, &scfg) == cudaSuccess && ncl >= 1) {
                 K = std::min(K, ncl);
-                scfg.gridDim = dim3(K * kSecCtas);
+                scfg.gridDim = dim3(K * kSmCtas);
                 sec = true;
             }
             cudaGetLastError();
@@ -1370,28 +1736,28 @@ void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long 
     }
     int nb = kMgClusterCtas;
     if (sec) {
-        nb = K * kSecCtas;
+        nb = K * kSmCtas;
     } else if (!cluster) {
         int occ = 0;
         CICY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mg_pcg<false>, kMgThreads, 0));
         const int cap = std::max(1, occ) * num_sms;
         nb = std::max(1, std::min({cap, num_sms, ceil_div(n, 2 * kMgThreads)}));
     }
-    std::vector<MgSecLevel> hl;  // kept until the stream synchronisation below
-    MgSecArgs sa{};
+    std::vector<MgSmLevel> hl;  // kept until the stream synchronisation below
+    MgSmArgs sa{};
     if (sec) {
         // levels lc .. coarsest per cluster: r and z above lc, zf from lc on, K copies each
         const int C = g.levels - 1;
         int lc = C;
         for (int l = 1; l <= C; l++)
-            if (g.L[l].n <= kSecRows) {
+            if (g.L[l].n <= kSmRows) {
                 lc = l;
                 break;
             }
-        hl.assign(C + 1, MgSecLevel{});
+        hl.assign(C + 1, MgSmLevel{});
         for (int l = 0; l <= C; l++) {
             MgWork::Lvl& L = g.L[l];
-            MgSecLevel& d = hl[l];
+            MgSmLevel& d = hl[l];
             d.n = L.n;
             if (l == 0) continue;
             if (l < C) {
@@ -1422,13 +1788,15 @@ void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long 
                 d.zf = L.zf.get();
             }
         }
-        g.sec_lv.ensure(sizeof(MgSecLevel) * (C + 1));
-        CICY_CUDA(cudaMemcpyAsync(g.sec_lv.get(), hl.data(), sizeof(MgSecLevel) * (C + 1), cudaMemcpyHostToDevice, s));
+        g.sec_lv.ensure(sizeof(MgSmLevel) * (C + 1));
+        CICY_CUDA(cudaMemcpyAsync(g.sec_lv.get(), hl.data(), sizeof(MgSmLevel) * (C + 1), cudaMemcpyHostToDevice, s));
         g.cl_fail.ensure(K);
         CICY_CUDA(cudaMemsetAsync(g.cl_fail.get(), 0, sizeof(int32_t) * K, s));
         sa.lc = lc;
-        sa.lv = reinterpret_cast<const MgSecLevel*>(g.sec_lv.get());
+        sa.lv = reinterpret_cast<const MgSmLevel*>(g.sec_lv.get());
         sa.cl_fail = g.cl_fail.get();
+        sa.mptr0 = g.L[0].mptr.get();
+        sa.smem_bytes = kSmBytes;
     }
     w.cta_row.ensure(nb + 1);
     launch_cta_rows(nb, n, w.is_start.get(), w.cta_row.get(), s);
@@ -1463,7 +1831,7 @@ void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long 
     if (cluster) {
         CICY_CUDA(cudaLaunchKernelEx(&cfg, k_mg_pcg<true>, a));
     } else if (sec) {
-        CICY_CUDA(cudaLaunchKernelEx(&scfg, k_mg_pcg_sec, a, sa));
+        CICY_CUDA(cudaLaunchKernelEx(&scfg, k_mg_pcg_sm, a, sa));
     } else {
         void* args[] = {&a};
         CICY_CUDA(cudaLaunchCooperativeKernel((void*)k_mg_pcg<false>, dim3(nb), dim3(kMgThreads), args, 0, s));

@@ -67,19 +67,23 @@ def full_csr(S: dict):
     return A
 
 
-def collect_systems(networks, device: int = 0, real_only: bool = True):
-    """Solve each (NetworkConfig, window network) with the chain preconditioner and keep its DEA systems."""
+def collect_systems(networks, device: int = 0, real_only: bool = True, ctx=None, preconditioner: int = 2):
+    """Solve each (NetworkConfig, window network) (chain preconditioner by default) and keep its
+    DEA systems; with `ctx`, every network goes through that one context."""
     from .device import Context
 
     out = []
+    own = ctx is None
     for cfg, net in networks:
-        ctx = Context(device)
-        ctx.set_solver(preconditioner=2)
+        if own:
+            ctx = Context(device)
+        ctx.set_solver(preconditioner=preconditioner)
         ctx.upload(net)
         try:
             r = ctx.network_to_conductance(cfg.params())
         except _abi.CicyError:  # networks upstream rejects too (e.g. a zero stiffness diagonal) are skipped
-            ctx.close()
+            if own:
+                ctx.close()
             continue
         for i in range(r.n_solves):
             if real_only and r.solves[i].pass_ < 0:
@@ -91,7 +95,8 @@ def collect_systems(networks, device: int = 0, real_only: bool = True):
             st, ln = ctx.chains(i)
             x = S["voltages"][S["reserved"]:]
             out.append({"A": A, "chain_start": st, "chain_len": ln, "err0": x - S["x0"], "n": A.shape[0]})
-        ctx.close()
+        if own:
+            ctx.close()
     return out
 
 
@@ -182,21 +187,22 @@ def monte_carlo_training_systems(count: int, seed0: int = 5_000_000, device: int
     from the sweep's own seeds (3,000,000 + k), so the sweep evaluates on fresh networks.
     Realisations that do not percolate give no system and are skipped."""
     from .batch import monte_carlo_configs
+    from .device import Context
+    from .network import generate_cnt_network
 
     out, k, batch = [], 0, 64
-    while len(out) < count:
-        cfgs = monte_carlo_configs(batch, seed0=seed0 + k)
-        for cfg in cfgs:
-            cfg.seed = seed0 + k
-            k += 1
-            from .network import generate_cnt_network
-
-            got = collect_systems([(cfg, generate_cnt_network(cfg).extract_window(cfg))], device=device)
-            out += got[: count - len(out)]
-            if len(out) >= count:
-                break
-        if log:
-            log(f"{k} realisations, {len(out)} systems")
+    with Context(device) as ctx:  # one context; the multigrid solve gives the same systems faster
+        while len(out) < count:
+            cfgs = monte_carlo_configs(batch, seed0=seed0 + k)
+            for cfg in cfgs:
+                cfg.seed = seed0 + k
+                k += 1
+                got = collect_systems([(cfg, generate_cnt_network(cfg).extract_window(cfg))], device=device, ctx=ctx, preconditioner=3)
+                out += got[: count - len(out)]
+                if len(out) >= count:
+                    break
+            if log:
+                log(f"{k} realisations, {len(out)} systems")
     return out
 
 
