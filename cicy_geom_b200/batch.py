@@ -65,6 +65,8 @@ def realisation_systems(configs, device: int = 0, preconditioner: int = 3):
             if len(S["diag"]) == 0:
                 continue
             st, ln = ctx.chains(i)
+            keep = ln > 0  # a CNT whose element nodes are all prescribed has an empty chain
+            st, ln = st[keep], ln[keep]
             systems.append({"A": full_csr(S), "b": S["b"], "x0": S["x0"], "chain_start": st, "chain_len": ln,
                             "x_ref": S["voltages"][S["reserved"]:], "seconds_ref": r.solves[i].seconds,
                             "iterations_ref": r.solves[i].iterations, "seed": cfg.seed})

@@ -673,7 +673,7 @@ __global__ void __launch_bounds__(kMgClusterThreads) k_mg_batch(const MgArgs* __
 // set that does not fit the shared-memory budget is read from global memory instead.
 constexpr int kSmCtas = 8;          // CTAs per cluster (portable size)
 constexpr int kSmThreads = 512;
-constexpr int kSmRows = 4096;       // largest level the clusters solve alone
+constexpr int kSmRows = 1000;       // largest level the clusters solve alone
 constexpr int kSmMaxClusters = 18;  // 144 CTAs
 constexpr int kSmBytes = 200 * 1024;
 
@@ -746,13 +746,16 @@ __device__ __forceinline__ void cluster_sync_all() {
     asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
 }
 
-// Grid barrier whose outcome is the same on every CTA of a cluster: a CTA whose bounded wait
-// gave up marks its cluster before the cluster barrier, and every CTA of the cluster reads
-// that mark after it, so a cluster leaves as a whole and no cluster barrier waits on a CTA
-// that has returned.
-__device__ __forceinline__ bool sm_sync(const MgArgs& a, int* cl_fail, unsigned long long& target, int cid, int* s_ok) {
-    const bool ok = mg_sync(a.bar, target, a.err, s_ok, a.spin_limit);
-    if (!ok && threadIdx.x == 0) atomicExch(&cl_fail[cid], 1);
+// Grid barrier (bounded).  A CTA whose wait gave up marks its cluster and carries on through
+// the iteration with the same control flow (its data are then stale, the device status says
+// why); sm_cluster_ok, once per iteration before the first data-dependent branch, lets every
+// CTA of a marked cluster leave together, so no cluster barrier ever waits on a CTA that has
+// returned and no CTA branches on partial sums another CTA of its cluster read differently.
+__device__ __forceinline__ void sm_sync(const MgArgs& a, int* cl_fail, unsigned long long& target, int cid, int* s_ok) {
+    if (!mg_sync(a.bar, target, a.err, s_ok, a.spin_limit) && threadIdx.x == 0) atomicExch(&cl_fail[cid], 1);
+}
+
+__device__ __forceinline__ bool sm_cluster_ok(const int* cl_fail, int cid) {
     cluster_sync_all();
     return __ldcg(&cl_fail[cid]) == 0;
 }
@@ -778,6 +781,43 @@ __device__ __forceinline__ double fused_dot(const int32_t* col, const double* va
         for (int u = 0; u < U; u++) s += w[u] * xv[u];
     }
     return s;
+}
+
+// Level-0 row gather: sum_q val[q] v(ci[q]) over entries [b, e), v(c) = vs[c - lo] for the
+// CTA's own rows [lo, hi) (shared memory), else the global vector vg; with zc, each entry also
+// adds zc[cagg[q]].  Chunks of U entries: indices and weights first, vector entries second.
+template <int U>
+__device__ __forceinline__ double own_dot(const int32_t* ci, const double* val, const int32_t* cagg, int b, int e, int lo, int hi,
+                                          const double* vs, const double* vg, const double* zc) {
+    double s = 0;
+    for (int q0 = b; q0 < e; q0 += U) {
+        int c[U], g[U];
+        double w[U], x[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int q = q0 + u;
+            c[u] = q < e ? ci[q] : lo;
+            w[u] = q < e ? val[q] : 0.0;
+            g[u] = (zc && q < e) ? cagg[q] : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            x[u] = (c[u] >= lo && c[u] < hi) ? vs[c[u] - lo] : __ldcg(&vg[c[u]]);
+            if (zc) x[u] += __ldcg(&zc[g[u]]);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) s += w[u] * x[u];
+    }
+    return s;
+}
+
+// Sum of the nb per-CTA partials: one load per thread, then the CTA reduction.
+__device__ __forceinline__ double sm_sum_partials(const double* part, int nb, double* sm) {
+    double v = 0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) v += __ldcg(&part[i]);
+    double r;
+    mg_reduce1(v, sm, r);
+    return r;
 }
 
 __device__ __forceinline__ double lanes_sum(double v, int lanes) {
@@ -881,6 +921,7 @@ __global__ void __launch_bounds__(kSmThreads) k_mg_pcg_sm(MgArgs a, MgSmArgs sa)
     __shared__ SmStage st[kSmMaxStages];
     __shared__ int n_st;
     __shared__ int s_ok;
+    __shared__ double rc[kMgDenseMax];
     const int cta = blockIdx.x, nb = gridDim.x;
     const int cid = cta / kSmCtas, crank = cta % kSmCtas;
     const int C = a.levels - 1, Lc = sa.lc;
@@ -940,26 +981,6 @@ __global__ void __launch_bounds__(kSmThreads) k_mg_pcg_sm(MgArgs a, MgSmArgs sa)
             L.rp = a.rp + L.lo; L.rp_sub = e0;
             L.ci = a.ci + e0; L.cagg = G0.cagg + e0; L.val = a.val + e0;
         }
-        // chain-block inverse rows
-        const int t0 = nr > 0 ? a.row_off[L.lo] : 0;
-        const int T = nr > 0 ? a.row_off[L.hi - 1] + a.row_m[L.hi - 1] - t0 : 0;
-        unsigned char* m_meta = nr > 0 ? take(12u * nr) : nullptr;
-        unsigned char* m_t = m_meta ? take(8u * T) : nullptr;
-        if (m_t) {
-            L.roff = reinterpret_cast<const int32_t*>(m_meta); L.roff_sub = 0;
-            L.rbase = L.roff + nr; L.rbase_sub = 0;
-            L.rm = L.rbase + nr;
-            L.tinv = reinterpret_cast<const double*>(m_t);
-            st[ns++] = SmStage{m_meta, a.row_off + L.lo, nr, 4, t0};
-            st[ns++] = SmStage{m_meta + 4u * nr, a.row_base + L.lo, nr, 4, L.lo};
-            st[ns++] = SmStage{m_meta + 8u * nr, a.row_m + L.lo, nr, 4, 0};
-            st[ns++] = SmStage{m_t, a.tinv + t0, T, 8, 0};
-        } else {
-            L.roff = a.row_off + L.lo; L.roff_sub = t0;
-            L.rbase = a.row_base + L.lo; L.rbase_sub = L.lo;
-            L.rm = a.row_m + L.lo;
-            L.tinv = a.tinv + t0;
-        }
         // row -> aggregate, and the own aggregates' row ranges
         L.alo = nr > 0 ? G0.agg[L.lo] : 0;
         L.ahi = nr > 0 ? G0.agg[L.hi - 1] + 1 : 0;
@@ -1009,6 +1030,27 @@ __global__ void __launch_bounds__(kSmThreads) k_mg_pcg_sm(MgArgs a, MgSmArgs sa)
                 P.cinv = a.cinv + (size_t)P.clo * nC;
             }
         }
+        // chain-block inverse rows (last: a phase reads them from shared memory with no other
+        // global trip, so they are the cheapest to leave in global memory)
+        const int t0 = nr > 0 ? a.row_off[L.lo] : 0;
+        const int T = nr > 0 ? a.row_off[L.hi - 1] + a.row_m[L.hi - 1] - t0 : 0;
+        unsigned char* m_meta = nr > 0 && ns + 4 <= kSmMaxStages ? take(12u * nr) : nullptr;
+        unsigned char* m_t = m_meta ? take(8u * T) : nullptr;
+        if (m_t) {
+            L.roff = reinterpret_cast<const int32_t*>(m_meta); L.roff_sub = 0;
+            L.rbase = L.roff + nr; L.rbase_sub = 0;
+            L.rm = L.rbase + nr;
+            L.tinv = reinterpret_cast<const double*>(m_t);
+            st[ns++] = SmStage{m_meta, a.row_off + L.lo, nr, 4, t0};
+            st[ns++] = SmStage{m_meta + 4u * nr, a.row_base + L.lo, nr, 4, L.lo};
+            st[ns++] = SmStage{m_meta + 8u * nr, a.row_m + L.lo, nr, 4, 0};
+            st[ns++] = SmStage{m_t, a.tinv + t0, T, 8, 0};
+        } else {
+            L.roff = a.row_off + L.lo; L.roff_sub = t0;
+            L.rbase = a.row_base + L.lo; L.rbase_sub = L.lo;
+            L.rm = a.row_m + L.lo;
+            L.tinv = a.tinv + t0;
+        }
         P.used = used;
         n_st = ns;
     }
@@ -1028,7 +1070,6 @@ __global__ void __launch_bounds__(kSmThreads) k_mg_pcg_sm(MgArgs a, MgSmArgs sa)
     __syncthreads();
     const SmL0& L = P.l0;
     const int lo = L.lo, hi = L.hi;
-    auto own = [&](int c) { return c >= lo && c < hi; };
     // chain-block inverse row of own row li applied to a vector of own rows
     auto block_row = [&](int li, const double* v) {
         const int off = L.roff[li] - L.roff_sub, base = L.rbase[li] - L.rbase_sub, m = L.rm[li];
@@ -1057,20 +1098,15 @@ __global__ void __launch_bounds__(kSmThreads) k_mg_pcg_sm(MgArgs a, MgSmArgs sa)
         }
         mg_reduce1(rr_l, sm, s0);
         if (threadIdx.x == 0) a.partA[cta] = s0;
-        if (!sm_sync(a, sa.cl_fail, target, cid, &s_ok)) return;
-        rr = mg_sum_partials(a.partA, nb, sm);
+        sm_sync(a, sa.cl_fail, target, cid, &s_ok);
+        if (!sm_cluster_ok(sa.cl_fail, cid)) break;
+        rr = sm_sum_partials(a.partA, nb, sm);
         if (k == 0 && !recursive && restarts == 0) R0 = a.tol * sqrt(rr);
         if (k > 0 && sqrt(rr) <= R0) {
             if (!recursive || restarts >= a.max_restarts) break;
             // the recursive residual met the test: replace it by the FP64 true residual
-            for (int li = threadIdx.x; li < hi - lo; li += blockDim.x) {
-                double sx = 0;
-                for (int q = row_b(li); q < row_b(li + 1); q++) {
-                    const int c = L.ci[q];
-                    sx += L.val[q] * (own(c) ? L.x[c - lo] : __ldcg(&a.x[c]));
-                }
-                L.r[li] = L.b[li] - sx;
-            }
+            for (int li = threadIdx.x; li < hi - lo; li += blockDim.x)
+                L.r[li] = L.b[li] - own_dot<4>(L.ci, L.val, nullptr, row_b(li), row_b(li + 1), lo, hi, L.x, a.x, nullptr);
             restarts++;
             recursive = false;
             fresh = true;
@@ -1079,14 +1115,8 @@ __global__ void __launch_bounds__(kSmThreads) k_mg_pcg_sm(MgArgs a, MgSmArgs sa)
         if (k >= a.max_iter) break;
         // ---- w = r - A z0; level 0 -> 1 over the own aggregates (the chain blocks) ----
         {
-            for (int li = threadIdx.x; li < hi - lo; li += blockDim.x) {
-                double sx = 0;
-                for (int q = row_b(li); q < row_b(li + 1); q++) {
-                    const int c = L.ci[q];
-                    sx += L.val[q] * (own(c) ? L.z0[c - lo] : __ldcg(&a.z0[c]));
-                }
-                L.w[li] = L.r[li] - sx;
-            }
+            for (int li = threadIdx.x; li < hi - lo; li += blockDim.x)
+                L.w[li] = L.r[li] - own_dot<4>(L.ci, L.val, nullptr, row_b(li), row_b(li + 1), lo, hi, L.z0, a.z0, nullptr);
             __syncthreads();
             const MgSmLevel& G = lv[1];
             const bool smooth = (C > 1) || a.cinv == nullptr;
@@ -1098,12 +1128,12 @@ __global__ void __launch_bounds__(kSmThreads) k_mg_pcg_sm(MgArgs a, MgSmArgs sa)
                 G.r[J] = v;
                 if (smooth) G.z[J] = G.l1inv[J] * v;
             }
-            if (!sm_sync(a, sa.cl_fail, target, cid, &s_ok)) return;
+            sm_sync(a, sa.cl_fail, target, cid, &s_ok);
         }
         // ---- restrictions l -> l + 1 grid-wide (1 <= l < lc) ----
         for (int l = 1; l < Lc; l++) {
             sm_restrict(P.R[l], lv[l].rr_lanes, lv[l].n, lv[l].r, lv[l].z, lv[l + 1].r, lv[l + 1].z, (l + 1 < C) || a.cinv == nullptr);
-            if (!sm_sync(a, sa.cl_fail, target, cid, &s_ok)) return;
+            sm_sync(a, sa.cl_fail, target, cid, &s_ok);
         }
         // ---- levels lc .. coarsest: every cluster on its own copy ----
         for (int l = Lc; l < C; l++) {
@@ -1114,11 +1144,13 @@ __global__ void __launch_bounds__(kSmThreads) k_mg_pcg_sm(MgArgs a, MgSmArgs sa)
             const MgSmLevel& Cl = lv[C];
             const int nC = Cl.n;
             const int wpb = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-            if (a.cinv) {  // dense inverse of the coarsest level, one warp per row
+            if (a.cinv) {  // dense inverse of the coarsest level (r_C staged once), one warp per row
+                for (int j = threadIdx.x; j < nC; j += blockDim.x) rc[j] = __ldcg(&Cl.r[j]);
+                __syncthreads();
                 for (int i = P.clo + warp; i < P.chi; i += wpb) {
                     const double* row = P.cinv + (size_t)(i - P.clo) * nC;
                     double v = 0;
-                    for (int j = lane; j < nC; j += 32) v += row[j] * __ldcg(&Cl.r[j]);
+                    for (int j = lane; j < nC; j += 32) v += row[j] * rc[j];
                     v = warp_sum(v);
                     if (lane == 0) Cl.zf[i] = v;
                 }
@@ -1134,19 +1166,15 @@ __global__ void __launch_bounds__(kSmThreads) k_mg_pcg_sm(MgArgs a, MgSmArgs sa)
         // ---- prolongations lc - 1 .. 1 grid-wide ----
         for (int l = Lc - 1; l >= 1; l--) {
             sm_prolong(P.Q[l], lv[l].pq_lanes, lv[l].n, lv[l].r, lv[l].z, lv[l + 1].zf, lv[l].zf);
-            if (!sm_sync(a, sa.cl_fail, target, cid, &s_ok)) return;
+            sm_sync(a, sa.cl_fail, target, cid, &s_ok);
         }
         // ---- level-0 post-smoother: z = z0 + P z1, z += w M0^-1 (r - A z); r.z ----
         {
             const double* zc = lv[1].zf;
             for (int li = threadIdx.x; li < hi - lo; li += blockDim.x) {
-                double sx = 0;
-                for (int q = row_b(li); q < row_b(li + 1); q++) {
-                    const int c = L.ci[q];
-                    sx += L.val[q] * ((own(c) ? L.z0[c - lo] : __ldcg(&a.z0[c])) + __ldcg(&zc[L.cagg[q]]));
-                }
-                L.w[li] = L.r[li] - sx;
-                L.z[li] = L.z0[li] + __ldcg(&zc[L.agg[li]]);
+                const double zci = __ldcg(&zc[L.agg[li]]);
+                L.w[li] = L.r[li] - own_dot<4>(L.ci, L.val, L.cagg, row_b(li), row_b(li + 1), lo, hi, L.z0, a.z0, zc);
+                L.z[li] = L.z0[li] + zci;
             }
             __syncthreads();
             double rz_l = 0;
@@ -1158,19 +1186,15 @@ __global__ void __launch_bounds__(kSmThreads) k_mg_pcg_sm(MgArgs a, MgSmArgs sa)
             }
             mg_reduce1(rz_l, sm, s0);
             if (threadIdx.x == 0) a.partB[cta] = s0;
-            if (!sm_sync(a, sa.cl_fail, target, cid, &s_ok)) return;
-            const double rz_new = mg_sum_partials(a.partB, nb, sm);
+            sm_sync(a, sa.cl_fail, target, cid, &s_ok);
+            const double rz_new = sm_sum_partials(a.partB, nb, sm);
             beta = fresh ? 0.0 : rz_new / rz;
             rz = rz_new;
         }
         // ---- q = A z + beta q, p = z + beta p; p.q ----
         double pq_l = 0;
         for (int li = threadIdx.x; li < hi - lo; li += blockDim.x) {
-            double w = 0;
-            for (int q = row_b(li); q < row_b(li + 1); q++) {
-                const int c = L.ci[q];
-                w += L.val[q] * (own(c) ? L.z[c - lo] : __ldcg(&a.z[c]));
-            }
+            const double w = own_dot<4>(L.ci, L.val, nullptr, row_b(li), row_b(li + 1), lo, hi, L.z, a.z, nullptr);
             const double zi = L.z[li];
             const double qi = fresh ? w : w + beta * L.q[li];
             const double pi = fresh ? zi : zi + beta * L.p[li];
@@ -1180,8 +1204,8 @@ __global__ void __launch_bounds__(kSmThreads) k_mg_pcg_sm(MgArgs a, MgSmArgs sa)
         }
         mg_reduce1(pq_l, sm, s0);
         if (threadIdx.x == 0) a.partA[nb + cta] = s0;
-        if (!sm_sync(a, sa.cl_fail, target, cid, &s_ok)) return;
-        const double pq = mg_sum_partials(a.partA + nb, nb, sm);
+        sm_sync(a, sa.cl_fail, target, cid, &s_ok);
+        const double pq = sm_sum_partials(a.partA + nb, nb, sm);
         fresh = false;
         k++;
         // ---- x += alpha p, r -= alpha q (x also to global: other CTAs read it for a true residual) ----

@@ -43,6 +43,15 @@ def _fill(struct_cls, arrays: dict):
     return s, keep
 
 
+def _merge_csr(ptr, idx, row, val, n):
+    """CSR (ptr, idx) over n rows with the pairs (row[k], val[k]) appended to their rows in
+    k order, after the row's own entries."""
+    rows = np.concatenate([np.repeat(np.arange(n, dtype=np.int64), np.diff(ptr)), row])
+    vals = np.concatenate([np.asarray(idx, np.int64), val])
+    order = np.argsort(rows, kind="stable")
+    return np.concatenate([[0], np.cumsum(np.bincount(rows, minlength=n))]).astype(np.int64), vals[order]
+
+
 def _csr(lists, dt=np.int32):
     ptr = np.concatenate([[0], np.cumsum([len(x) for x in lists])]).astype(np.int64)
     return ptr, np.array([v for x in lists for v in x], dtype=dt)
@@ -118,30 +127,35 @@ def hybrid_network_to_conductance(directory: str, cfg, overlap_gnp: float, devic
     t.append(time.perf_counter())
     NG = len(gv["t"])
     # points_gnp and structure_gnp after Compress_mixed_contacts appends the mixed points
+    # (each GNP's list, then its mixed-junction points in junction order)
     pts = np.concatenate([gp["gnp_points"], mj["points"].reshape(-1, 3)]) if len(mj["points"]) else gp["gnp_points"]
     sp, si = gp["structure_ptr"], gp["structure_idx"]
-    lists = [list(si[sp[g]:sp[g + 1]]) for g in range(NG)]
-    for q, g in zip(mj["gnp_point"], mj["gnp"]):
-        lists[int(g)].append(int(q))
-    # elements_cnt: CNT junction points, mixed junction points, end points (Complete_cnt_elements)
-    elems = [set(ei[ep[c]:ep[c + 1]].tolist()) for c in range(len(ep) - 1)]
-    for q, c in zip(mj["cnt_point"], mj["cnt"]):
-        elems[int(c)].add(int(q))
+    st_ptr, st_idx = _merge_csr(sp, si, np.asarray(mj["gnp"], np.int64), np.asarray(mj["gnp_point"], np.int64), NG)
+    # elements_cnt: CNT junction points, mixed junction points, end points (Complete_cnt_elements),
+    # ascending and without repeats per CNT
+    nc = len(ep) - 1
+    e_cnt = np.repeat(np.arange(nc, dtype=np.int64), np.diff(ep))
+    m_cnt = np.asarray(mj["cnt"], np.int64)
+    has = np.zeros(nc, bool)
+    has[e_cnt] = True
+    has[m_cnt] = True
+    ends = np.nonzero(has)[0]
     csp, csi = a["structure_ptr"], a["structure_idx"]
-    for c, e in enumerate(elems):
-        if e:
-            e.add(int(csi[csp[c]]))
-            e.add(int(csi[csp[c + 1] - 1]))
-    # boundary points of each GNP (GNP::pts_boundary) and the junction-point flags
-    pb = [[] for _ in range(NG)]
-    for P, (g, f) in enumerate(zip(gw["point_gnp"], gw["point_boundary"])):
-        if f >= 0:
-            pb[int(g)].append((P, int(f)))
+    ec = np.concatenate([e_cnt, m_cnt, ends, ends])
+    eq = np.concatenate([np.asarray(ei, np.int64), np.asarray(mj["cnt_point"], np.int64), csi[csp[ends]], csi[csp[ends + 1] - 1]])
+    span = int(eq.max(initial=0)) + 1
+    key = np.unique(ec * span + eq)
+    ep2 = np.concatenate([[0], np.cumsum(np.bincount(key // span, minlength=nc))]).astype(np.int64)
+    ei2 = (key % span).astype(np.int64)
+    # boundary points of each GNP (GNP::pts_boundary, point order) and the junction-point flags
+    pg_, pf_ = np.asarray(gw["point_gnp"], np.int64), np.asarray(gw["point_boundary"], np.int64)
+    bsel = np.nonzero(pf_ >= 0)[0]
+    border = bsel[np.argsort(pg_[bsel], kind="stable")]
+    pb_ptr = np.concatenate([[0], np.cumsum(np.bincount(pg_[border], minlength=NG))]).astype(np.int64)
+    pb_pt = border.astype(np.int64)
+    pb_face = pf_[border].astype(np.int32)
     bp = np.zeros(len(pts), np.int32)
     bp[: len(gp["boundary_used"])] = gp["boundary_used"]
-    st_ptr, st_idx = _csr(lists, np.int64)
-    pb_ptr, pb_pt = _csr([[q[0] for q in x] for x in pb], np.int64)
-    _, pb_face = _csr([[q[1] for q in x] for x in pb], np.int32)
     J = gp["junctions"]
     mst = {"n_labels": nm, "n_cnts": len(lc), "labels_cnt": lc, "n_cnts_inside": len(a["cnts_inside"]), "cnts_inside": a["cnts_inside"],
            "n_gnps": NG, "labels_gnp": lg, "n_gnps_inside": len(gw["gnps_inside"]), "gnps_inside": gw["gnps_inside"],
@@ -155,7 +169,6 @@ def hybrid_network_to_conductance(directory: str, cfg, overlap_gnp: float, devic
     t.append(time.perf_counter())
     vol = np.where(np.isnan(gw["volume"]), gv["l"] * gv["l"] * gv["t"], gw["volume"])
     frame = np.concatenate([gv["l"][:, None], gv["center"], gv["rotation"].reshape(NG, 9), gv["planes"][:, 0, :3]], axis=1)
-    ep2, ei2 = _csr([sorted(e) for e in elems], np.int64)
     hst = {"n_clusters": mc["n_percolated"], "family": mc["family"]}
     for k in ("clusters_cnt", "clusters_gnp", "cnt_junctions", "gnp_junctions", "mix_junctions"):
         hst[k + "_ptr"], hst[k + "_idx"] = mc[k + "_ptr"], mc[k + "_idx"]

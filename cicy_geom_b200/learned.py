@@ -25,6 +25,9 @@ from . import _abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 PARAMS_PATH = os.path.join(HERE, "learned_params.f32")
+# the same network trained on 2,000 real-resistor Laplacians of the Monte-Carlo generator
+# (python -m cicy_geom_b200.learned --monte-carlo 2000 --steps 4000 --out <this file>)
+MC_PARAMS_PATH = os.path.join(HERE, "learned_params_mc2000.f32")
 WIDTH, LAYERS = 32, 3
 
 
@@ -53,6 +56,14 @@ def default_params() -> np.ndarray:
     p = np.fromfile(PARAMS_PATH, dtype=np.float32)
     if len(p) != param_count():
         raise RuntimeError(f"{PARAMS_PATH}: {len(p)} parameters, the library expects {param_count()}")
+    return p
+
+
+def monte_carlo_params() -> np.ndarray:
+    """The parameters trained on 2,000 Monte-Carlo Laplacians (MC_PARAMS_PATH)."""
+    p = np.fromfile(MC_PARAMS_PATH, dtype=np.float32)
+    if len(p) != param_count():
+        raise RuntimeError(f"{MC_PARAMS_PATH}: {len(p)} parameters, the library expects {param_count()}")
     return p
 
 
@@ -93,6 +104,8 @@ def collect_systems(networks, device: int = 0, real_only: bool = True, ctx=None,
                 continue
             A = full_csr(S)
             st, ln = ctx.chains(i)
+            keep = ln > 0  # a CNT whose element nodes are all prescribed has an empty chain
+            st, ln = st[keep], ln[keep]
             x = S["voltages"][S["reserved"]:]
             out.append({"A": A, "chain_start": st, "chain_len": ln, "err0": x - S["x0"], "n": A.shape[0]})
         if own:
