@@ -51,7 +51,7 @@ METRIC = "networks solved/s at 1e-8 residual (25k-CNT 6um network, full hot path
 DATA = "synthetic (seeded CNT polylines of the workload's length, radius and step statistics; one independent network per GPU)"
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "ref_dump")
 PRECONDS = {"jacobi": 0, "learned": 1, "chain": 2, "mg": 3}
-MG_DRAM_BYTES_PER_ROW = 225.0  # ncu: k_mg_pcg DRAM read + write per launch / free rows (8k-CNT network, both passes)
+MG_DRAM_BYTES_PER_ROW = 245.0  # ncu: k_mg_pcg_sm DRAM read + write per launch / free rows (8k-CNT network: 233 and 258 B)
 KERNELS = {0: "k_pcg (grid-wide persistent PCG)", 1: "k_pcg_cluster (16-CTA cluster-resident PCG)",
            2: "k_mg_pcg (chain-aggregation multigrid PCG)"}
 
@@ -108,8 +108,8 @@ def config_dict(side: float = SIDE, cnts: int = N_CNTS) -> dict:
 class ClockSampler:
     """SM clocks and throttle reasons sampled during the timed region.
 
-    NVML is read every 10 ms from a thread (read-only queries; the same
-    counters nvidia-smi prints); without NVML, nvidia-smi at its 100 ms
+    NVML is read every 20 ms by a separate process (read-only queries; the
+    same counters nvidia-smi prints); without NVML, nvidia-smi at its 100 ms
     floor.  Rows: sm MHz, max sm MHz, power W, hw_slowdown,
     hw_thermal_slowdown, sw_thermal_slowdown, sw_power_cap (bools).
     """
@@ -123,37 +123,41 @@ class ClockSampler:
         self.stop = threading.Event()
         self.source = None
 
+    # NVML polled from a separate process, so its driver calls never queue behind or in front of
+    # this process's launches and synchronisations
+    NVML_LOOP = (
+        "import sys, time\n"
+        "import pynvml as N\n"
+        "N.nvmlInit()\n"
+        "h = N.nvmlDeviceGetHandleByIndex(int(sys.argv[1]))\n"
+        "bits = [N.nvmlClocksEventReasonHwSlowdown, N.nvmlClocksEventReasonHwThermalSlowdown,\n"
+        "        N.nvmlClocksEventReasonSwThermalSlowdown, N.nvmlClocksEventReasonSwPowerCap]\n"
+        "mx = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)\n"
+        "while True:\n"
+        "    r = N.nvmlDeviceGetCurrentClocksEventReasons(h)\n"
+        "    v = [N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM), mx, N.nvmlDeviceGetPowerUsage(h) / 1000.0]\n"
+        "    print(', '.join([str(x) for x in v] + ['Active' if r & b else 'Not Active' for b in bits]), flush=True)\n"
+        "    time.sleep(0.02)\n")
+
     def __enter__(self):
         try:
-            import pynvml as N
+            import pynvml  # noqa: F401
 
-            N.nvmlInit()
-            h = N.nvmlDeviceGetHandleByIndex(self.index)
-            bits = [N.nvmlClocksEventReasonHwSlowdown, N.nvmlClocksEventReasonHwThermalSlowdown,
-                    N.nvmlClocksEventReasonSwThermalSlowdown, N.nvmlClocksEventReasonSwPowerCap]
-            mx = float(N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM))
-
-            def sample():
-                r = N.nvmlDeviceGetCurrentClocksEventReasons(h)
-                return [float(N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)), mx, N.nvmlDeviceGetPowerUsage(h) / 1000.0] + \
-                       [bool(r & b) for b in bits]
-
-            sample()
-
-            def loop():
-                while not self.stop.is_set():
-                    try:
-                        self.rows.append(sample())
-                    except Exception:
-                        pass
-                    self.stop.wait(0.01)
-
-            self.t = threading.Thread(target=loop, daemon=True)
+            self.proc = subprocess.Popen([sys.executable, "-c", self.NVML_LOOP, str(self.index)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
-            self.source = "nvml 10 ms"
-            return self
+            t0 = time.time()
+            while not self.rows and time.time() - t0 < 30.0 and self.proc.poll() is None:
+                time.sleep(0.02)
+            if self.rows:
+                self.rows.clear()
+                self.source = "nvml 20 ms (separate process)"
+                return self
+            self.proc.terminate()
+            self.proc = None
         except Exception:
-            pass
+            self.proc = None
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
@@ -734,8 +738,9 @@ def run_ours(args):
             "roofline": {"kernel": KERNELS[top], "bound": "hbm", "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                          "traffic_note": "bytes per launch scaled by rows from an ncu capture of the same kernel on the "
-                                         "8k-CNT network (DRAM read + write, 225 B per free row); the algorithmic bytes per "
-                                         "launch are ~45x larger because the system stays in L2 across iterations",
+                                         "8k-CNT network (DRAM read + write, 245 B per free row: the system and hierarchy read "
+                                         "once into shared memory and L2); the algorithmic bytes per launch are ~45x larger "
+                                         "because the system stays on chip across iterations",
                          "algorithmic_bytes_per_launch": k_bytes / k_launch if k_launch else None,
                          "launches_per_step": k_launch / args.steps, "share_of_step": k_sec / t_dev,
                          "note": "algorithmic bytes = iterations x (SpMV + 12 vector passes) of the solves this kernel ran; "

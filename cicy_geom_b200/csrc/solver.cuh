@@ -190,6 +190,9 @@ bool pcg_solve_cluster(SolverWork& w, const SolverSystem& sys, bool block_precon
 // fused: also build the fused restriction / prolongation rows the clustered grid kernel
 // reads (systems above the single-cluster size).
 void build_mg_hierarchy(SolverWork& w, const SolverSystem& sys, cudaStream_t s, int64_t& launches, bool fused = false);
+// Whether pcg_solve_mg takes the clustered grid kernel for a system of n rows (build the
+// hierarchy with fused = this).
+bool mg_fused_path(int n, bool allow_cluster);
 // allow_cluster: one 16-CTA cluster with hardware barriers when it fits, else the grid-wide kernel.
 void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long max_iter, bool allow_cluster, int num_sms, int* status,
                   cudaStream_t s, int64_t& launches, PcgStats& st);

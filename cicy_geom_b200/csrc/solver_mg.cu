@@ -154,12 +154,20 @@ __global__ void k_dense_coarse(int nc, const int32_t* __restrict__ rp, const int
     }
 }
 
+// Blocked in-place Gauss-Jordan (32 pivots per block).  For pivot block b with the others o:
+// one warp inverts the Schur-complemented diagonal block D = S_bb pivot by pivot (dropping a
+// variable whose pivot vanishes: its row and column of D^-1 are zero), then the CTA applies the
+// block step S_bo <- D^-1 S_bo, S_ob <- -S_ob D^-1, S_oo <- S_oo - S_ob D^-1 S_bo, S_bb <- D^-1:
+// the unblocked elimination's result with 4 barriers per block instead of 2 per pivot.
+constexpr int kGjBlock = 32;
 __global__ void __launch_bounds__(kGjThreads) k_gauss_jordan(int n, double* __restrict__ M) {
-    extern __shared__ double S[];  // n * n + n
-    double* f = S + (size_t)n * n;
+    extern __shared__ double S[];  // n * n, then Cb (n x 32), Rb (32 x n), D (32 x 33), f (32)
+    double* Cb = S + (size_t)n * n;
+    double* Rb = Cb + (size_t)n * kGjBlock;
+    double* D = Rb + (size_t)kGjBlock * n;
+    double* f = D + kGjBlock * (kGjBlock + 1);
     __shared__ double dmax_s;
-    // thread (tx, ty) of a 32 x 32 layout owns rows ty, ty + 32, ... and columns tx, tx + 32, ...
-    const int t = threadIdx.x, tx = t & 31, ty = t >> 5;
+    const int t = threadIdx.x;
     for (int e = t; e < n * n; e += kGjThreads) S[e] = M[e];
     __syncthreads();
     if (t == 0) {
@@ -171,24 +179,62 @@ __global__ void __launch_bounds__(kGjThreads) k_gauss_jordan(int n, double* __re
     const double thr = 1e-12 * dmax_s;
     for (int i = t; i < n; i += kGjThreads) S[i * n + i] *= (1.0 + 1e-8);
     __syncthreads();
-    for (int k = 0; k < n; k++) {
-        const double p = S[k * n + k];  // every thread reads the same pivot: uniform branch
-        if (!(p > thr)) {               // vanishing pivot: drop variable k
-            for (int j = t; j < n; j += kGjThreads) {
-                S[k * n + j] = 0.0;
-                S[j * n + k] = 0.0;
-            }
-            __syncthreads();
-            continue;
-        }
-        // column k of the other rows (multipliers) and the scaled pivot row: disjoint entries
-        for (int i = t; i < n; i += kGjThreads) f[i] = (i == k) ? 0.0 : S[i * n + k];
-        for (int j = t; j < n; j += kGjThreads) S[k * n + j] = ((j == k) ? 1.0 : S[k * n + j]) / p;
+    constexpr int DS = kGjBlock + 1;
+    for (int b0 = 0; b0 < n; b0 += kGjBlock) {
+        const int m = min(kGjBlock, n - b0);
+        for (int e = t; e < m * m; e += kGjThreads) D[(e / m) * DS + e % m] = S[(b0 + e / m) * n + b0 + e % m];
+        for (int e = t; e < n * m; e += kGjThreads) Cb[(e / m) * kGjBlock + e % m] = S[(e / m) * n + b0 + e % m];
         __syncthreads();
-        for (int i = ty; i < n; i += 32) {
-            if (i == k) continue;
-            const double fi = f[i];
-            for (int j = tx; j < n; j += 32) S[i * n + j] = ((j == k) ? 0.0 : S[i * n + j]) - fi * S[k * n + j];
+        if (t < 32) {  // one warp: D <- D^-1, lane j owns column j
+            const int j = t;
+            for (int k = 0; k < m; k++) {
+                const double p = D[k * DS + k];
+                if (!(p > thr)) {  // vanishing pivot: drop variable k
+                    if (j < m) {
+                        D[k * DS + j] = 0.0;
+                        D[j * DS + k] = 0.0;
+                    }
+                    __syncwarp();
+                    continue;
+                }
+                if (j < m) f[j] = (j == k) ? 0.0 : D[j * DS + k];
+                __syncwarp();
+                if (j < m) D[k * DS + j] = ((j == k) ? 1.0 : D[k * DS + j]) / p;
+                __syncwarp();
+                if (j < m) {
+                    const double dk = D[k * DS + j];
+                    for (int i = 0; i < m; i++)
+                        if (i != k) D[i * DS + j] = ((j == k) ? 0.0 : D[i * DS + j]) - f[i] * dk;
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        // Rb = D^-1 S_bo (columns outside the block)
+        for (int e = t; e < m * n; e += kGjThreads) {
+            const int ii = e / n, jc = e % n;
+            if (jc >= b0 && jc < b0 + m) continue;
+            double acc = 0;
+            for (int kk = 0; kk < m; kk++) acc += D[ii * DS + kk] * S[(b0 + kk) * n + jc];
+            Rb[ii * n + jc] = acc;
+        }
+        __syncthreads();
+        for (int e = t; e < n * n; e += kGjThreads) {
+            const int i = e / n, jc = e % n;
+            const bool ib = i >= b0 && i < b0 + m, jb = jc >= b0 && jc < b0 + m;
+            double v;
+            if (ib) {
+                v = jb ? D[(i - b0) * DS + (jc - b0)] : Rb[(i - b0) * n + jc];
+            } else if (jb) {
+                double acc = 0;
+                for (int kk = 0; kk < m; kk++) acc += Cb[i * kGjBlock + kk] * D[kk * DS + (jc - b0)];
+                v = -acc;
+            } else {
+                double acc = 0;
+                for (int kk = 0; kk < m; kk++) acc += Cb[i * kGjBlock + kk] * Rb[kk * n + jc];
+                v = S[e] - acc;
+            }
+            S[e] = v;
         }
         __syncthreads();
     }
@@ -215,12 +261,14 @@ __global__ void k_ra_fill(int nc, const int32_t* __restrict__ mptr, const int32_
 }
 
 // Fused restriction rows of level l >= 1 into level l + 1 (clustered kernel): row J holds
-// the members of aggregate J (column m < n: r_l[m], weight 1), then its row of P^T A_l
-// (column n + c: z_l[c], weight -a), so r_{l+1} = P^T (r_l - A_l z_l) is one gathered dot
-// product.  rr_ptr = mptr + ra_ptr, both prefix sums.
+// the members of aggregate J (column m < n: r_l[m], weight 1), then for each member I its
+// diagonal and couplings (column n + c: z_l[c], weight -a), the rows of P^T A_l, so
+// r_{l+1} = P^T (r_l - A_l z_l) is one gathered dot product.  rr_ptr = mptr + ra_ptr, both
+// prefix sums (ra_ptr: the P^T A_l row lengths).
 __global__ void k_rr_fill(int nc, int n, const int32_t* __restrict__ mptr, const int32_t* __restrict__ midx,
-                          const int32_t* __restrict__ ra_ptr, const int32_t* __restrict__ ra_col, const double* __restrict__ ra_val,
-                          int32_t* __restrict__ rr_ptr, int32_t* __restrict__ rr_col, double* __restrict__ rr_val) {
+                          const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const double* __restrict__ v,
+                          const double* __restrict__ diag, const int32_t* __restrict__ ra_ptr, int32_t* __restrict__ rr_ptr,
+                          int32_t* __restrict__ rr_col, double* __restrict__ rr_val) {
     for (int J = blockIdx.x * blockDim.x + threadIdx.x; J < nc; J += gridDim.x * blockDim.x) {
         int e = mptr[J] + ra_ptr[J];
         rr_ptr[J] = e;
@@ -229,9 +277,15 @@ __global__ void k_rr_fill(int nc, int n, const int32_t* __restrict__ mptr, const
             rr_col[e] = midx[m];
             rr_val[e] = 1.0;
         }
-        for (int k = ra_ptr[J]; k < ra_ptr[J + 1]; k++, e++) {
-            rr_col[e] = n + ra_col[k];
-            rr_val[e] = -ra_val[k];
+        for (int m = mptr[J]; m < mptr[J + 1]; m++) {
+            const int I = midx[m];
+            rr_col[e] = n + I;
+            rr_val[e] = -diag[I];
+            e++;
+            for (int k = rp[I]; k < rp[I + 1]; k++, e++) {
+                rr_col[e] = n + ci[k];
+                rr_val[e] = -v[k];
+            }
         }
     }
 }
@@ -1541,23 +1595,28 @@ void coarsen(MgWork& g, int l, int nc, cudaStream_t s, int64_t& launches) {
     G.rp_ptr = G.rp.get();
     G.ci_ptr = G.ci.get();
     G.val_ptr = G.val.get();
-    // restriction rows of level l (l >= 1) and its column aggregates
+    // restriction rows of level l (l >= 1) and its column aggregates; the clustered kernel
+    // (g.fused) reads the fused rows instead of P^T A_l and the coarse column aggregates
     if (l >= 1) {
         scan_small(F.ra_ptr.get(), F.ra_ptr.get(), nc + 1, nullptr, g, s, launches);
-        F.ra_col.ensure(std::max(nnz + nf, 1));
-        F.ra_val.ensure(std::max(nnz + nf, 1));
-        k_ra_fill<<<grid_for(nc), 256, 0, s>>>(nc, F.mptr.get(), F.midx.get(), F.rp_ptr, F.ci_ptr, F.val_ptr, F.diag.get(), F.ra_ptr.get(),
-                                                F.ra_col.get(), F.ra_val.get());
+        if (!g.fused) {
+            F.ra_col.ensure(std::max(nnz + nf, 1));
+            F.ra_val.ensure(std::max(nnz + nf, 1));
+            k_ra_fill<<<grid_for(nc), 256, 0, s>>>(nc, F.mptr.get(), F.midx.get(), F.rp_ptr, F.ci_ptr, F.val_ptr, F.diag.get(),
+                                                    F.ra_ptr.get(), F.ra_col.get(), F.ra_val.get());
+            launches++;
+        }
+    }
+    if (!g.fused || l == 0) {
+        F.cagg.ensure(std::max(nnz, 1));
+        k_cagg_rows<<<grid_for(nf), 256, 0, s>>>(nf, F.rp_ptr, F.ci_ptr, F.agg.get(), F.cagg.get());
         launches++;
     }
-    F.cagg.ensure(std::max(nnz, 1));
-    k_cagg_rows<<<grid_for(nf), 256, 0, s>>>(nf, F.rp_ptr, F.ci_ptr, F.agg.get(), F.cagg.get());
-    launches++;
     if (g.fused && l >= 1) {
         F.rr_ptr.ensure(nc + 1);
         F.rr_col.ensure(std::max(nnz + 2 * nf, 1));
         F.rr_val.ensure(std::max(nnz + 2 * nf, 1));
-        k_rr_fill<<<grid_for(nc), 256, 0, s>>>(nc, nf, F.mptr.get(), F.midx.get(), F.ra_ptr.get(), F.ra_col.get(), F.ra_val.get(),
+        k_rr_fill<<<grid_for(nc), 256, 0, s>>>(nc, nf, F.mptr.get(), F.midx.get(), F.rp_ptr, F.ci_ptr, F.val_ptr, F.diag.get(), F.ra_ptr.get(),
                                                 F.rr_ptr.get(), F.rr_col.get(), F.rr_val.get());
         F.pq_ptr.ensure(nf + 1);
         F.pq_col.ensure(std::max(2 * (nnz + nf), 1));
@@ -1639,7 +1698,7 @@ void build_mg_hierarchy(SolverWork& w, const SolverSystem& sys, cudaStream_t s, 
     if (Lc.n <= kMgDenseMax) {
         g.cinv.ensure((size_t)Lc.n * Lc.n);
         k_dense_coarse<<<grid_for(Lc.n, 128), 128, 0, s>>>(Lc.n, Lc.rp.get(), Lc.ci.get(), Lc.val.get(), Lc.diag.get(), g.cinv.get());
-        const size_t smem = sizeof(double) * ((size_t)Lc.n * Lc.n + Lc.n);
+        const size_t smem = sizeof(double) * ((size_t)Lc.n * Lc.n + 2 * (size_t)Lc.n * kGjBlock + kGjBlock * (kGjBlock + 1) + kGjBlock);
         if (smem > 48 * 1024)
             CICY_CUDA(cudaFuncSetAttribute(k_gauss_jordan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_gauss_jordan<<<1, kGjThreads, smem, s>>>(Lc.n, g.cinv.get());
@@ -1686,6 +1745,8 @@ void build_mg_hierarchy(SolverWork& w, const SolverSystem& sys, cudaStream_t s, 
     CICY_LAUNCH_CHECK();
 }
 
+bool mg_fused_path(int n, bool allow_cluster) { return !(allow_cluster && n <= kMgClusterMaxRows); }
+
 void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long max_iter, bool allow_cluster, int num_sms, int* status,
                   cudaStream_t s, int64_t& launches, PcgStats& st) {
     const int n = sys.n;
@@ -1707,7 +1768,7 @@ void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long 
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
     bool cluster = false;
-    if (allow_cluster && cl_state > 0 && n <= kMgClusterMaxRows) {
+    if (allow_cluster && !g.fused && cl_state > 0 && n <= kMgClusterMaxRows) {
         cfg.gridDim = dim3(kMgClusterCtas);
         cfg.blockDim = dim3(kMgClusterThreads);
         cfg.dynamicSmemBytes = 0;
@@ -1758,6 +1819,7 @@ void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long 
             cudaGetLastError();
         }
     }
+    if (g.fused && !sec) throw Fail{CICY_E_INTERNAL, "multigrid: the clustered kernel cannot be launched for a hierarchy built for it"};
     int nb = kMgClusterCtas;
     if (sec) {
         nb = K * kSmCtas;

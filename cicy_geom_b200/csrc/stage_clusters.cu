@@ -99,8 +99,8 @@ __global__ void k_grid_scatter(int n_trav, const int32_t* __restrict__ trav_pt, 
 // them.  A block stages the points of a contiguous run of slots in shared
 // memory; each thread owns one slot j and walks k = j+1 .. end of its region.
 constexpr int kPairThreads = 256;
-constexpr int kPairTile = 1024;     // slots owned by one block
-constexpr int kPairStage = 2048;    // slots staged in shared memory (tile + region tail)
+constexpr int kPairTile = 512;      // slots owned by one block
+constexpr int kPairStage = 1024;    // slots staged in shared memory (tile + region tail): 40 KB, five blocks per SM
 
 struct StagedPt {
     double x, y, z, r;
@@ -600,6 +600,7 @@ void run_clusters(Ctx& c, const cicy_params& p) {
     if (c.stage < 2) throw Fail{CICY_E_STATE, "cicy_clusters: run cicy_contact_grid first"};
     cudaStream_t s = c.stream;
     CICY_TRACE("clusters", s);
+    TraceSeq tr(s);
     const int S = c.n_slots, NC = std::max(c.n_cnts, 1), NP = std::max(c.n_points, 1);
     // ---- pair tests ----
     int cap = std::max(1 << 16, S / 4);
@@ -630,6 +631,7 @@ void run_clusters(Ctx& c, const cicy_params& p) {
         if (attempt == 1) throw Fail{CICY_E_INTERNAL, "contact buffer overflow"};
     }
     const int NR = c.n_raw;
+    tr.mark("clusters.pairs");
     // ---- point_contacts ----
     const int bp = bits_for((uint64_t)NP), bc = bits_for((uint64_t)NC);
     if (bp + 2 * bc > 64) throw Fail{CICY_E_CAPACITY, "too many points/CNTs for the 64-bit contact key"};
@@ -656,6 +658,7 @@ void run_clusters(Ctx& c, const cicy_params& p) {
         c.n_uc = 0;
     }
     const int NU = c.n_uc;
+    tr.mark("clusters.point_contacts");
     // ---- labels ----
     c.parent.ensure(NC); c.minkey.ensure(NC); c.labels.ensure(NC); c.root_rank.ensure(NC);
     k_uf_init<<<grid_for(NC), 256, 0, s>>>(c.n_cnts, c.parent.get(), c.minkey.get());
@@ -684,6 +687,7 @@ void run_clusters(Ctx& c, const cicy_params& p) {
     }
     k_labels<<<grid_for(NC), 256, 0, s>>>(c.n_cnts, c.parent.get(), c.minkey.get(), c.root_rank.get(), c.labels.get());
     c.launches++;
+    tr.mark("clusters.labels");
     // ---- junction compression ----
     c.grp_start.ensure(std::max(NU, 1)); c.junc_cnt.ensure(std::max(NU, 1) + 1); c.junc_ofs.ensure(std::max(NU, 1) + 1);
     int n_groups = 0;
@@ -711,6 +715,7 @@ void run_clusters(Ctx& c, const cicy_params& p) {
                                                         c.j_p1.get(), c.j_n1.get(), c.j_p2.get(), c.j_n2.get(), c.j_d.get());
         c.launches++;
     }
+    tr.mark("clusters.junctions");
     // ---- elements ----
     c.mark.ensure(NP + 1); c.mark_scan.ensure(NP + 1); c.has_junc.ensure(NC);
     CICY_CUDA(cudaMemsetAsync(c.mark.get(), 0, sizeof(int32_t) * (NP + 1), s));
@@ -725,6 +730,7 @@ void run_clusters(Ctx& c, const cicy_params& p) {
     c.elem_idx.ensure(std::max(n_elem, 1));
     k_fill_elements<<<grid_for(NP), 256, 0, s>>>(c.n_points, c.mark.get(), c.mark_scan.get(), c.elem_idx.get());
     c.launches++;
+    tr.mark("clusters.elements");
     // ---- percolation and families ----
     const int NL = std::max(c.n_labels, 1);
     c.face_bits.ensure(NL); c.perc_bits.ensure(NL); c.perc_index.ensure(NL + 1);
@@ -749,6 +755,7 @@ void run_clusters(Ctx& c, const cicy_params& p) {
         for (int L = 0; L < c.n_labels; L++)
             if (bits[L]) c.h_family.push_back(fam_of_bits[bits[L]]);
     }
+    tr.mark("clusters.percolation");
     // percolated clusters (CNTs in cnts_inside order) and their junctions
     const int NP_ = std::max(c.n_perc, 1);
     c.clu_ptr.ensure(NP_ + 1); c.cj_ptr.ensure(NP_ + 1);
@@ -803,6 +810,7 @@ void run_clusters(Ctx& c, const cicy_params& p) {
     }
     CICY_LAUNCH_CHECK();
     check_status(c, "Determine_clusters_and_percolation");
+    tr.mark("clusters.members");
     c.stage = 3;
     c.have_backbone = false;
     c.have_volumes = false;

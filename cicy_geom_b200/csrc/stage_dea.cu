@@ -553,10 +553,11 @@ __device__ __forceinline__ void staged_in_order(int n, Stage stage, Consume cons
 
 // The cluster's volumes added to its family in upstream's order: CNTs last to first
 // (Backbone_Network.cpp:325), per CNT the dead part(s) and then the kept run (:442-543).
+// The staging threads turn the parts a CNT does not have into +0.0 terms: the sums start at
+// +0.0 and only add volumes >= 0, so x + 0.0 == x and the consumer adds without branches.
 __global__ void __launch_bounds__(kSumThreads) k_volume_sum(int n, int family, const double* __restrict__ vol3,
                                                             const int32_t* __restrict__ kind, double* acc) {
     __shared__ double sv[2][3 * kSumChunk];
-    __shared__ int32_t sk[2][kSumChunk];
     double dead = 0, bb = 0;
     if (threadIdx.x == 0) {
         dead = acc[kVolDead + family];
@@ -568,18 +569,17 @@ __global__ void __launch_bounds__(kSumThreads) k_volume_sum(int n, int family, c
             const int i0 = n - 1 - ch * kSumChunk, m = min(kSumChunk, i0 + 1);
             for (int j = t; j < m; j += T) {
                 const int i = i0 - j, k = kind[i];
-                sk[b][j] = k;
                 sv[b][3 * j] = vol3[3 * i];
-                if (k >= 1) sv[b][3 * j + 1] = vol3[3 * i + 1];
-                if (k == 2) sv[b][3 * j + 2] = vol3[3 * i + 2];
+                sv[b][3 * j + 1] = k == 2 ? vol3[3 * i + 2] : 0.0;
+                sv[b][3 * j + 2] = k >= 1 ? vol3[3 * i + 1] : 0.0;
             }
         },
         [&](int b, int m) {
+            const double* v = sv[b];
+#pragma unroll 4
             for (int j = 0; j < m; j++) {
-                const int k = sk[b][j];
-                dead = dead + sv[b][3 * j];
-                if (k == 2) dead = dead + sv[b][3 * j + 2];
-                if (k >= 1) bb = bb + sv[b][3 * j + 1];
+                dead = (dead + v[3 * j]) + v[3 * j + 1];
+                bb = bb + v[3 * j + 2];
             }
         });
     if (threadIdx.x == 0) {
@@ -710,21 +710,16 @@ __global__ void k_boundary_terms(int b, int e, const int32_t* __restrict__ bcnt,
 __global__ void __launch_bounds__(kSumThreads) k_boundary_sum(int m, const double* __restrict__ term, const int32_t* __restrict__ valid,
                                                               double* out) {
     __shared__ double sv[2][kSumChunk];
-    __shared__ int32_t sf[2][kSumChunk];
-    double I = 0;
+    double I = 0;  // starts at +0.0 and never becomes -0.0, so skipped terms can be added as +0.0
     staged_in_order(
         m,
         [&](int ch, int b, int t, int T) {
             const int mm = min(kSumChunk, m - ch * kSumChunk);
-            for (int j = t; j < mm; j += T) {
-                const int f = valid[ch * kSumChunk + j];
-                sf[b][j] = f;
-                if (f) sv[b][j] = term[ch * kSumChunk + j];
-            }
+            for (int j = t; j < mm; j += T) sv[b][j] = valid[ch * kSumChunk + j] ? term[ch * kSumChunk + j] : 0.0;
         },
         [&](int b, int mm) {
-            for (int j = 0; j < mm; j++)
-                if (sf[b][j]) I = I + sv[b][j];
+#pragma unroll 4
+            for (int j = 0; j < mm; j++) I = I + sv[b][j];
         });
     if (threadIdx.x == 0) *out = I;
 }
@@ -1002,7 +997,7 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
         if (c.solver.preconditioner == CICY_PRECOND_MG && n > 0) {
             build_block_preconditioner(c.sw, ss, NMc, c.chain_start.get(), c.chain_len.get(), nullptr, nullptr, false, s, c.launches);
             tr.mark(r_flag ? "dea.real.blocks" : "dea.unit.blocks");
-            build_mg_hierarchy(c.sw, ss, s, c.launches, true);
+            build_mg_hierarchy(c.sw, ss, s, c.launches, mg_fused_path(n, !(c.solver.flags & CICY_SOLVER_NO_CLUSTER)));
             tr.mark(r_flag ? "dea.real.mg_setup" : "dea.unit.mg_setup");
             pcg_solve_mg(c.sw, ss, tol, max_iter, !(c.solver.flags & CICY_SOLVER_NO_CLUSTER), c.num_sms, c.status.get(), s, c.launches,
                          st);
