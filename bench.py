@@ -417,7 +417,7 @@ def contact_search_roofline(ctx, net, res, stage_acc, steps, hbm):
             "bound": "hbm", "algorithmic_bytes": b, "achieved": b / t / 1e9, "peak": hbm, "unit": "GB/s", "frac": b / t / 1e9 / hbm,
             "points": n_p, "slots": ns.value, "regions": nr.value, "point_contacts": n_k,
             "note": "stage time includes the host reads of the sizes (scan totals) between kernels; the largest kernel is "
-                    "k_pairs (one warp per region)"}
+                    "k_pairs (one thread per region slot)"}
 
 
 def spmv_roofline(ctx, device, hbm, target_bytes=320e6, reps=20):
