@@ -108,9 +108,10 @@ def config_dict(side: float = SIDE, cnts: int = N_CNTS) -> dict:
 class ClockSampler:
     """SM clocks and throttle reasons sampled during the timed region.
 
-    NVML is read every 20 ms by a separate process (read-only queries; the
-    same counters nvidia-smi prints); without NVML, nvidia-smi at its 100 ms
-    floor.  Rows: sm MHz, max sm MHz, power W, hw_slowdown,
+    NVML is read every 100 ms by a separate process (read-only queries; the
+    same counters nvidia-smi prints; faster polling was seen to slow the
+    timed steps' host synchronisations on some boxes); without NVML,
+    nvidia-smi at its 100 ms floor.  Rows: sm MHz, max sm MHz, power W, hw_slowdown,
     hw_thermal_slowdown, sw_thermal_slowdown, sw_power_cap (bools).
     """
 
@@ -137,7 +138,7 @@ class ClockSampler:
         "    r = N.nvmlDeviceGetCurrentClocksEventReasons(h)\n"
         "    v = [N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM), mx, N.nvmlDeviceGetPowerUsage(h) / 1000.0]\n"
         "    print(', '.join([str(x) for x in v] + ['Active' if r & b else 'Not Active' for b in bits]), flush=True)\n"
-        "    time.sleep(0.02)\n")
+        "    time.sleep(0.1)\n")
 
     def __enter__(self):
         try:
@@ -152,7 +153,7 @@ class ClockSampler:
                 time.sleep(0.02)
             if self.rows:
                 self.rows.clear()
-                self.source = "nvml 20 ms (separate process)"
+                self.source = "nvml 100 ms (separate process)"
                 return self
             self.proc.terminate()
             self.proc = None

@@ -93,10 +93,43 @@ __global__ void k_scan_apply(const T* in, T* out, int n, const T* __restrict__ b
     }
 }
 
+// Scans of at most kScanSmallMax items in one launch: each of 1,024 threads holds a contiguous
+// chunk of up to 16 items in registers (so out may alias in), one block-wide exclusive sum.
+constexpr int kScanSmallItems = 16;
+constexpr int kScanSmallMax = 1024 * kScanSmallItems;
+template <class T>
+__global__ void __launch_bounds__(1024) k_scan_small(const T* in, T* out, int n, T* total) {
+    __shared__ T sw[33];
+    const int ch = (n + 1023) / 1024;
+    const int lo = min(n, (int)threadIdx.x * ch), hi = min(n, lo + ch);
+    T v[kScanSmallItems];
+    T s = 0;
+#pragma unroll
+    for (int i = 0; i < kScanSmallItems; i++) {
+        v[i] = lo + i < hi ? in[lo + i] : T(0);
+        s += v[i];
+    }
+    T tot;
+    T ex = block_exclusive_sum<T>(s, sw, tot);
+#pragma unroll
+    for (int i = 0; i < kScanSmallItems; i++)
+        if (lo + i < hi) {
+            out[lo + i] = ex;
+            ex += v[i];
+        }
+    if (threadIdx.x == 0 && total) *total = tot;
+}
+
 template <class T>
 void exclusive_scan_impl(const T* in, T* out, int n, T* total, DBuf<T>& tmp, cudaStream_t s, int64_t& launches) {
     if (n <= 0) {
         if (total) CICY_CUDA(cudaMemsetAsync(total, 0, sizeof(T), s));
+        return;
+    }
+    if (n <= kScanSmallMax) {
+        k_scan_small<T><<<1, 1024, 0, s>>>(in, out, n, total);
+        launches++;
+        CICY_LAUNCH_CHECK();
         return;
     }
     int nb = ceil_div(n, kScanTile);
@@ -237,6 +270,75 @@ void exclusive_scan_i64(const int64_t* in, int64_t* out, int n, int64_t* total, 
     exclusive_scan_impl<int64_t>(in, out, n, total, tmp, s, launches);
 }
 
+// Small sorts in one launch: one CTA of 32 warps runs every 8-bit pass.  Per pass each warp
+// counts the digits of its contiguous segment, one CTA-wide scan turns the (digit, warp)
+// counts into stable offsets, and each warp places its segment 32 keys at a time in order
+// (ranks among equal digits by __match_any_sync), so the sort is a stable LSD radix sort like
+// the multi-CTA one.  Launch-bound sorts (labels, cluster members) take one launch instead of
+// five per pass.
+constexpr int kRadixCtaThreads = 1024;
+constexpr int kRadixCtaMax = 32768;  // largest n sorted this way
+__global__ void __launch_bounds__(kRadixCtaThreads) k_radix_sort_cta(uint64_t* ka, uint32_t* va, uint64_t* kb, uint32_t* vb, int n,
+                                                                     int passes, int* final_in_b) {
+    __shared__ int32_t cnt[32][256];
+    __shared__ int32_t tot[256];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int seg = ((n + 31) / 32 + 31) & ~31;
+    const int b0 = min(n, w * seg), b1 = min(n, b0 + seg);
+    for (int p = 0; p < passes; p++) {
+        const int shift = 8 * p;
+        for (int i = threadIdx.x; i < 32 * 256; i += blockDim.x) (&cnt[0][0])[i] = 0;
+        __syncthreads();
+        for (int j = b0 + lane; j < b1; j += 32) atomicAdd(&cnt[w][(ka[j] >> shift) & 0xff], 1);
+        __syncthreads();
+        if (threadIdx.x < 256) {
+            int acc = 0;
+            for (int ww = 0; ww < 32; ww++) acc += cnt[ww][threadIdx.x];
+            tot[threadIdx.x] = acc;
+        }
+        __syncthreads();
+        for (int o = 1; o < 256; o <<= 1) {  // inclusive scan of the digit totals
+            int v = 0;
+            if (threadIdx.x < 256 && threadIdx.x >= o) v = tot[threadIdx.x - o];
+            __syncthreads();
+            if (threadIdx.x < 256) tot[threadIdx.x] += v;
+            __syncthreads();
+        }
+        if (threadIdx.x < 256) {
+            const int d = threadIdx.x;
+            int acc = d > 0 ? tot[d - 1] : 0;
+            for (int ww = 0; ww < 32; ww++) {
+                const int c = cnt[ww][d];
+                cnt[ww][d] = acc;
+                acc += c;
+            }
+        }
+        __syncthreads();
+        for (int j0 = b0; j0 < b1; j0 += 32) {
+            const int j = j0 + lane;
+            const bool valid = j < b1;
+            const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+            const uint64_t k = valid ? ka[j] : 0;
+            const uint32_t v = valid ? va[j] : 0;
+            const int d = (int)((k >> shift) & 0xff);
+            unsigned peers = __match_any_sync(0xffffffffu, valid ? d : 256 + lane) & vmask;
+            const unsigned lt = (1u << lane) - 1u;
+            const int pos = valid ? cnt[w][d] + __popc(peers & lt) : 0;
+            __syncwarp();
+            if (valid && (peers & lt) == 0) cnt[w][d] += __popc(peers);
+            __syncwarp();
+            if (valid) {
+                kb[pos] = k;
+                vb[pos] = v;
+            }
+        }
+        __syncthreads();
+        uint64_t* tk = ka; ka = kb; kb = tk;
+        uint32_t* tv = va; va = vb; vb = tv;
+    }
+    if (threadIdx.x == 0 && final_in_b) *final_in_b = passes & 1;
+}
+
 int bits_for(uint64_t v) {
     int b = 0;
     while (b < 64 && (v >> b) != 0) b++;
@@ -246,6 +348,18 @@ int bits_for(uint64_t v) {
 void radix_sort_pairs(uint64_t* keys, uint32_t* vals, int n, int bits, RadixScratch& rs, cudaStream_t s, int64_t& launches) {
     if (n <= 1) return;
     int passes = (bits + 7) / 8;
+    if (n <= kRadixCtaMax) {
+        rs.keys_tmp.ensure(n);
+        rs.vals_tmp.ensure(n);
+        k_radix_sort_cta<<<1, kRadixCtaThreads, 0, s>>>(keys, vals, rs.keys_tmp.get(), rs.vals_tmp.get(), n, passes, nullptr);
+        launches++;
+        CICY_LAUNCH_CHECK();
+        if (passes & 1) {  // the result is in the scratch arrays
+            CICY_CUDA(cudaMemcpyAsync(keys, rs.keys_tmp.get(), sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, s));
+            CICY_CUDA(cudaMemcpyAsync(vals, rs.vals_tmp.get(), sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s));
+        }
+        return;
+    }
     int n_tiles = ceil_div(n, kRadixTile);
     rs.keys_tmp.ensure(n);
     rs.vals_tmp.ensure(n);

@@ -162,52 +162,98 @@ __global__ void k_layer0(int n, const float* __restrict__ f, const float* __rest
     }
 }
 
-// Y[n x 32] = X[n x 32] (bf16) * W[32 x 32] (fp32 master weights rounded to bf16),
-// FP32 accumulate, on the tensor cores (mma.sync m16n8k16, one warp per 16 rows).
-__global__ void __launch_bounds__(256) k_gemm32(int n, const __nv_bfloat16* __restrict__ X, const float* __restrict__ W,
-                                                float* __restrict__ Yf, __nv_bfloat16* __restrict__ Yb) {
-    __shared__ __align__(16) __nv_bfloat16 WT[kW * kW];  // WT[j][k] = W[k][j]
-    for (int e = threadIdx.x; e < kW * kW; e += blockDim.x) {
-        const int k = e / kW, j = e - k * kW;
-        WT[j * kW + k] = __float2bfloat16_rn(W[e]);
+// Y[n x 32] = X[n x 32] (bf16) * W[32 x 32] (fp32 master weights rounded to bf16), FP32
+// accumulate, on the 5th-generation tensor cores: one CTA of 4 warps per 128-row tile, the
+// tile and W^T staged in shared memory in the canonical K-major no-swizzle layout (core
+// matrices of 8 rows x 16 bytes: element (row, k) at ((row / 8) * 4 + k / 8) * 128 +
+// (row % 8) * 16 + (k % 8) * 2 bytes, so the K step is 128 bytes (LBO) and an 8-row group 512
+// bytes (SBO)), two tcgen05.mma of M = 128, N = 32, K = 16 issued by one thread into a 32-column
+// TMEM accumulator, completion by tcgen05.commit on an mbarrier (bounded wait), and each warp
+// reading its 32 accumulator lanes back with tcgen05.ld (one row of 32 FP32 per thread).
+constexpr int kGemmRows = 128;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ int umma_off(int row, int k) { return ((row >> 3) * 4 + (k >> 3)) * 128 + (row & 7) * 16 + (k & 7) * 2; }
+
+// shared-memory matrix descriptor: start address, LBO 128 B, SBO 512 B, descriptor version 1,
+// no swizzle
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr) {
+    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(512 >> 4) << 32) | (1ull << 46);
+}
+
+__global__ void __launch_bounds__(kGemmRows) k_gemm32(int n, const __nv_bfloat16* __restrict__ X, const float* __restrict__ W,
+                                                      float* __restrict__ Yf, __nv_bfloat16* __restrict__ Yb, int* status) {
+    __shared__ __align__(1024) unsigned char sA[kGemmRows * kW * 2];
+    __shared__ __align__(1024) unsigned char sB[kW * kW * 2];
+    __shared__ __align__(8) unsigned long long mbar;
+    __shared__ uint32_t tmem_base;
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    for (int e = t; e < kW * kW; e += kGemmRows) {  // B = W^T, K-major
+        const int k = e / kW, j = e % kW;
+        *reinterpret_cast<__nv_bfloat16*>(sB + umma_off(j, k)) = __float2bfloat16_rn(W[e]);
     }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)), "r"(kW));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (t == 0) asm volatile("mbarrier.init.shared.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t* X32 = reinterpret_cast<const uint32_t*>(X);
-    const uint32_t* W32 = reinterpret_cast<const uint32_t*>(WT);
-    for (int tile = warp; tile * 16 < n; tile += nwarps) {
-        const int r0 = tile * 16 + g, r1 = r0 + 8;
-        uint32_t a[2][4];
-        for (int ks = 0; ks < 2; ks++) {
-            const int c = ks * 16 + 2 * t;
-            a[ks][0] = r0 < n ? X32[(r0 * kW + c) >> 1] : 0u;
-            a[ks][1] = r1 < n ? X32[(r1 * kW + c) >> 1] : 0u;
-            a[ks][2] = r0 < n ? X32[(r0 * kW + c + 8) >> 1] : 0u;
-            a[ks][3] = r1 < n ? X32[(r1 * kW + c + 8) >> 1] : 0u;
-        }
-        for (int nt = 0; nt < 4; nt++) {
-            float d0 = 0, d1 = 0, d2 = 0, d3 = 0;
-            for (int ks = 0; ks < 2; ks++) {
-                const int jrow = nt * 8 + g;
-                const uint32_t b0 = W32[(jrow * kW + ks * 16 + 2 * t) >> 1];
-                const uint32_t b1 = W32[(jrow * kW + ks * 16 + 8 + 2 * t) >> 1];
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base;
+    // kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, both K-major, N = 32, M = 128
+    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kW >> 3) << 17) | ((uint32_t)(kGemmRows >> 4) << 24);
+    uint32_t phase = 0;
+    const int ntiles = (n + kGemmRows - 1) / kGemmRows;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int r = tile * kGemmRows + t;
+        const uint4* src = reinterpret_cast<const uint4*>(X + (size_t)r * kW);
+        for (int kc = 0; kc < kW / 8; kc++)
+            *reinterpret_cast<uint4*>(sA + umma_off(t, kc * 8)) = r < n ? src[kc] : make_uint4(0, 0, 0, 0);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic-proxy stores -> the MMA's async proxy
+        __syncthreads();
+        if (t == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+            for (int ks = 0; ks < kW / 16; ks++) {
+                const uint64_t da = umma_desc(a0 + ks * 256), db = umma_desc(b0 + ks * 256);
                 asm volatile(
-                    "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-                    : "+f"(d0), "+f"(d1), "+f"(d2), "+f"(d3)
-                    : "r"(a[ks][0]), "r"(a[ks][1]), "r"(a[ks][2]), "r"(a[ks][3]), "r"(b0), "r"(b1));
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(idesc), "r"((uint32_t)ks));
             }
-            const int col = nt * 8 + 2 * t;
-            if (r0 < n) {
-                if (Yf) { Yf[r0 * kW + col] = d0; Yf[r0 * kW + col + 1] = d1; }
-                if (Yb) { Yb[r0 * kW + col] = __float2bfloat16_rn(d0); Yb[r0 * kW + col + 1] = __float2bfloat16_rn(d1); }
-            }
-            if (r1 < n) {
-                if (Yf) { Yf[r1 * kW + col] = d2; Yf[r1 * kW + col + 1] = d3; }
-                if (Yb) { Yb[r1 * kW + col] = __float2bfloat16_rn(d2); Yb[r1 * kW + col + 1] = __float2bfloat16_rn(d3); }
-            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(&mbar)) : "memory");
         }
+        uint32_t done = 0;
+        for (long long it = 0; it < (1ll << 26) && !done; it++)
+            asm volatile("{\n\t.reg .pred q;\n\tmbarrier.try_wait.parity.shared.b64 q, [%1], %2;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
+                         : "=r"(done) : "r"(smem_u32(&mbar)), "r"(phase) : "memory");
+        if (!done && t == 0) atomicCAS(status, 0, (int)DEV_TIMEOUT);
+        phase ^= 1;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        uint32_t d[32];
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                     "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                     : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
+                       "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15]),
+                       "=r"(d[16]), "=r"(d[17]), "=r"(d[18]), "=r"(d[19]), "=r"(d[20]), "=r"(d[21]), "=r"(d[22]), "=r"(d[23]),
+                       "=r"(d[24]), "=r"(d[25]), "=r"(d[26]), "=r"(d[27]), "=r"(d[28]), "=r"(d[29]), "=r"(d[30]), "=r"(d[31])
+                     : "r"(tmem + ((uint32_t)(warp * 32) << 16)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        const int row = tile * kGemmRows + warp * 32 + lane;
+        if (row < n) {
+            if (Yf)
+                for (int j = 0; j < kW; j++) Yf[(size_t)row * kW + j] = __uint_as_float(d[j]);
+            if (Yb)
+                for (int j = 0; j < kW; j++) Yb[(size_t)row * kW + j] = __float2bfloat16_rn(__uint_as_float(d[j]));
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
     }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kW));
 }
 
 // Message passing + update of one layer: one warp per node, lane = feature.
@@ -556,11 +602,12 @@ void gnn_forward(GnnState& g, const float* P, cudaStream_t s, int64_t& launches)
     const int n = g.n;
     k_layer0<<<grid_for((long long)n * kW), 256, 0, s>>>(n, g.f.get(), P, g.A0.get(), g.H[0].get());
     launches++;
-    const int gemm_grid = std::max(1, std::min(148 * 8, ceil_div(n, 16 * 8)));
+    const int gemm_grid = std::max(1, std::min(148 * 4, ceil_div(n, kGemmRows)));
+    g.status.ensure(1);
     for (int l = 0; l < kLayers; l++) {
         const float* Pl = P + kOffLayer0 + l * kLayerParams;
-        k_gemm32<<<gemm_grid, 256, 0, s>>>(n, g.H[l].get(), Pl + kOffU, nullptr, g.G[l].get());
-        k_gemm32<<<gemm_grid, 256, 0, s>>>(n, g.H[l].get(), Pl + kOffW, g.HW.get(), nullptr);
+        k_gemm32<<<gemm_grid, kGemmRows, 0, s>>>(n, g.H[l].get(), Pl + kOffU, nullptr, g.G[l].get(), g.status.get());
+        k_gemm32<<<gemm_grid, kGemmRows, 0, s>>>(n, g.H[l].get(), Pl + kOffW, g.HW.get(), nullptr, g.status.get());
         k_layer<<<warps_grid(n), 256, 0, s>>>(n, g.rp, g.ci, g.lc.get(), g.jf.get(), g.invdeg.get(), Pl, g.H[l].get(), g.G[l].get(),
                                               g.HW.get(), g.A[l].get(), g.H[l + 1].get());
         launches += 3;
