@@ -64,6 +64,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--precond", default="mg", choices=["jacobi", "chain", "learned", "mg"])
+    ap.add_argument("--unsmoothed", action="store_true", help="multigrid without the smoothed level-1 prolongator")
     ap.add_argument("--no-comparison", action="store_true", help="skip the per-preconditioner comparison and the SpMV measurement")
     ap.add_argument("--mc", type=int, default=256, help="Monte-Carlo realisations for the batched-solve measurement (0: skip)")
     # a smaller network of the same generator, for profiler captures (the bench line names the size it ran)
@@ -364,10 +365,11 @@ def solver_comparison(cfg, net, device, steps=2):
 
     out = {}
     runs = [("jacobi", "jacobi", 0), ("chain", "chain", 0), ("learned", "learned", 0), ("mg", "mg", 0),
-            ("jacobi_mixed", "jacobi", 1), ("chain_mixed", "chain", 1), ("learned_mixed", "learned", 1)]
+            ("mg_unsmoothed", "mg", 0), ("jacobi_mixed", "jacobi", 1), ("chain_mixed", "chain", 1), ("learned_mixed", "learned", 1)]
     for name, pk, prec in runs:
         ctx = Context(device)
-        ctx.set_solver(precision=prec, preconditioner=PRECONDS[pk], max_iter_factor=20)  # bounded: a stalled run stops early
+        # bounded: a stalled run stops early
+        ctx.set_solver(precision=prec, preconditioner=PRECONDS[pk], max_iter_factor=20, smoothed=name != "mg_unsmoothed")
         ctx.upload(net)
         params = cfg.params()
         res = Result()
@@ -645,7 +647,7 @@ def run_ours(args):
     cfg, raw, net = workload(rank, args.side, args.cnts)
     params = cfg.params()
     ctx = Context(local)
-    ctx.set_solver(precision=1 if args.precision == "mixed" else 0, preconditioner=PRECONDS[args.precond])
+    ctx.set_solver(precision=1 if args.precision == "mixed" else 0, preconditioner=PRECONDS[args.precond], smoothed=not args.unsmoothed)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=local)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")  # 256 MB > L2
     ctx.upload(net)
@@ -735,7 +737,7 @@ def run_ours(args):
             "config": config_dict(args.side, args.cnts),
             "points_in_window": len(net.arrays()["x"]),
             "solver_settings": {"precision": args.precision, "preconditioner": args.precond, "tolerance_real": TOL,
-                                "tolerance_unit": TOL_UNIT},
+                                "tolerance_unit": TOL_UNIT, "mg_level1_prolongator": "piecewise constant" if args.unsmoothed else "smoothed"},
             "roofline": {"kernel": KERNELS[top], "bound": "hbm", "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                          "traffic_note": "bytes per launch scaled by rows from an ncu capture of the same kernel on the "

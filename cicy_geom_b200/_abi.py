@@ -78,6 +78,10 @@ class Network(C.Structure):
     ]
 
 
+SOLVER_NO_CLUSTER = 1
+SOLVER_NO_SMOOTHED = 2
+
+
 class SolverOpts(C.Structure):
     _fields_ = [("precision", C.c_int32), ("preconditioner", C.c_int32), ("max_iter_factor", C.c_int32), ("flags", C.c_int32)]
 

@@ -108,15 +108,25 @@ struct MgWork {
     std::vector<Lvl> L;
     std::vector<MgLevel> host_lv;
     DBuf<MgLevel> dev_lv;
-    DBuf<double> cinv, z0, wtmp, sval;
+    DBuf<double> cinv, z0, wtmp, sval, gj_panel;
+    DBuf<unsigned long long> gj_sync;  // grid Gauss-Jordan: barrier counter, largest diagonal (bits)
+    DBuf<int32_t> gj_err;
     DBuf<unsigned long long> bar;
     DBuf<uint64_t> keys;
     DBuf<uint32_t> vals;
     DBuf<int32_t> flag, pos, head, uidx, mate, best, rep, total, scan_tmp, long_rows;
     RadixScratch radix;
+    // smoothed level-1 prolongator (fused hierarchy): Q = P - w D^-1 A_1 P and the sparse
+    // products built from it (T = A_1 P, Q^T, W = A_1 Q, Q^T A_1), plus the gather scratch
+    struct Smoothed {
+        DBuf<int32_t> tp, tc, qtp, qti, wp, wc, ap, ac, seg, ulen, longr;
+        DBuf<double> tv, qv, qpv, qtv, wv, wpv, av, y, v, gv, gv2, ov, ov2;
+        DBuf<uint64_t> gkey, okey;
+    } sa;
     int levels = 0;
     bool dense = false;
     bool fused = false;  // fused rows built (build_mg_hierarchy with fused = true)
+    bool smooth = true;  // with fused: level 1's prolongator smoothed (coarsen_smoothed)
     DBuf<int32_t> cl_fail;
     DBuf<unsigned char> sec_lv;  // device descriptors of the clustered kernel
 };
@@ -189,7 +199,8 @@ bool pcg_solve_cluster(SolverWork& w, const SolverSystem& sys, bool block_precon
 // must have run on the same system), then the MG-preconditioned CG solve.
 // fused: also build the fused restriction / prolongation rows the clustered grid kernel
 // reads (systems above the single-cluster size).
-void build_mg_hierarchy(SolverWork& w, const SolverSystem& sys, cudaStream_t s, int64_t& launches, bool fused = false);
+void build_mg_hierarchy(SolverWork& w, const SolverSystem& sys, cudaStream_t s, int64_t& launches, bool fused = false, bool smooth = true,
+                        int* status = nullptr);
 // Whether pcg_solve_mg takes the clustered grid kernel for a system of n rows (build the
 // hierarchy with fused = this).
 bool mg_fused_path(int n, bool allow_cluster);

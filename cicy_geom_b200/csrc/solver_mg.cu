@@ -56,7 +56,7 @@ constexpr int kMgClusterCtas = 16;            // non-portable cluster size
 constexpr int kMgClusterMaxRows = 20000;  // above this the grid-wide variant (more threads per row) is faster on B200
 constexpr int kMgMaxRestarts = 24;
 constexpr double kOmega0 = 0.95;
-constexpr int kGjThreads = 1024;
+constexpr int kGjThreads = 512;
 
 int grid_for(long long n, int threads = 256) {
     long long b = (n + threads - 1) / threads;
@@ -143,12 +143,11 @@ __global__ void k_fill_neg(int n, int32_t* __restrict__ a) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = -1;
 }
 
-// Dense coarsest matrix, then its inverse in place by Gauss-Jordan without
-// pivoting (SPD up to floating islands) in shared memory.
+// Dense coarsest matrix (M zeroed before), then its inverse in place by Gauss-Jordan
+// without pivoting (SPD up to floating islands).
 __global__ void k_dense_coarse(int nc, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const double* __restrict__ v,
                                const double* __restrict__ diag, double* __restrict__ M) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nc; i += gridDim.x * blockDim.x) {
-        for (int j = 0; j < nc; j++) M[(size_t)i * nc + j] = 0.0;
         for (int k = rp[i]; k < rp[i + 1]; k++) M[(size_t)i * nc + ci[k]] = v[k];
         M[(size_t)i * nc + i] = diag[i];
     }
@@ -160,12 +159,51 @@ __global__ void k_dense_coarse(int nc, const int32_t* __restrict__ rp, const int
 // block step S_bo <- D^-1 S_bo, S_ob <- -S_ob D^-1, S_oo <- S_oo - S_ob D^-1 S_bo, S_bb <- D^-1:
 // the unblocked elimination's result with 4 barriers per block instead of 2 per pivot.
 constexpr int kGjBlock = 32;
+constexpr int kGjDS = kGjBlock + 1;  // row stride of a diagonal block in shared memory
+
+// One warp: D <- D^-1 in place (m x m, row stride kGjDS); a variable whose pivot is not
+// above thr is dropped (its row and column of D^-1 are zero).  Lane j holds column j in
+// registers for the whole elimination and the pivot column is broadcast by shuffles, so a
+// pivot step has no shared-memory round trips.
+__device__ __forceinline__ void gj_warp_invert(double* D, int m, double thr, int j) {
+    double col[kGjBlock];
+#pragma unroll
+    for (int i = 0; i < kGjBlock; i++) col[i] = (i < m && j < m) ? D[i * kGjDS + j] : 0.0;
+#pragma unroll
+    for (int k = 0; k < kGjBlock; k++) {
+        if (k < m) {  // warp-uniform
+            const double p = __shfl_sync(0xffffffffu, col[k], k);
+            if (!(p > thr)) {  // vanishing pivot: drop variable k (row k and column k)
+                col[k] = 0.0;
+                if (j == k) {
+#pragma unroll
+                    for (int i = 0; i < kGjBlock; i++) col[i] = 0.0;
+                }
+            } else {
+                const double dk = ((j == k) ? 1.0 : col[k]) / p;  // the new pivot row
+#pragma unroll
+                for (int i = 0; i < kGjBlock; i++) {
+                    if (i == k) continue;
+                    const double fi = __shfl_sync(0xffffffffu, col[i], k);  // D[i][k] before this step
+                    col[i] = ((j == k) ? 0.0 : col[i]) - fi * dk;
+                }
+                col[k] = dk;
+            }
+        }
+    }
+    if (j < m) {
+#pragma unroll
+        for (int i = 0; i < kGjBlock; i++)
+            if (i < m) D[i * kGjDS + j] = col[i];
+    }
+    __syncwarp();
+}
+
 __global__ void __launch_bounds__(kGjThreads) k_gauss_jordan(int n, double* __restrict__ M) {
     extern __shared__ double S[];  // n * n, then Cb (n x 32), Rb (32 x n), D (32 x 33), f (32)
     double* Cb = S + (size_t)n * n;
     double* Rb = Cb + (size_t)n * kGjBlock;
     double* D = Rb + (size_t)kGjBlock * n;
-    double* f = D + kGjBlock * (kGjBlock + 1);
     __shared__ double dmax_s;
     const int t = threadIdx.x;
     for (int e = t; e < n * n; e += kGjThreads) S[e] = M[e];
@@ -179,36 +217,13 @@ __global__ void __launch_bounds__(kGjThreads) k_gauss_jordan(int n, double* __re
     const double thr = 1e-12 * dmax_s;
     for (int i = t; i < n; i += kGjThreads) S[i * n + i] *= (1.0 + 1e-8);
     __syncthreads();
-    constexpr int DS = kGjBlock + 1;
+    constexpr int DS = kGjDS;
     for (int b0 = 0; b0 < n; b0 += kGjBlock) {
         const int m = min(kGjBlock, n - b0);
         for (int e = t; e < m * m; e += kGjThreads) D[(e / m) * DS + e % m] = S[(b0 + e / m) * n + b0 + e % m];
         for (int e = t; e < n * m; e += kGjThreads) Cb[(e / m) * kGjBlock + e % m] = S[(e / m) * n + b0 + e % m];
         __syncthreads();
-        if (t < 32) {  // one warp: D <- D^-1, lane j owns column j
-            const int j = t;
-            for (int k = 0; k < m; k++) {
-                const double p = D[k * DS + k];
-                if (!(p > thr)) {  // vanishing pivot: drop variable k
-                    if (j < m) {
-                        D[k * DS + j] = 0.0;
-                        D[j * DS + k] = 0.0;
-                    }
-                    __syncwarp();
-                    continue;
-                }
-                if (j < m) f[j] = (j == k) ? 0.0 : D[j * DS + k];
-                __syncwarp();
-                if (j < m) D[k * DS + j] = ((j == k) ? 1.0 : D[k * DS + j]) / p;
-                __syncwarp();
-                if (j < m) {
-                    const double dk = D[k * DS + j];
-                    for (int i = 0; i < m; i++)
-                        if (i != k) D[i * DS + j] = ((j == k) ? 0.0 : D[i * DS + j]) - f[i] * dk;
-                }
-                __syncwarp();
-            }
-        }
+        if (t < 32) gj_warp_invert(D, m, thr, t);
         __syncthreads();
         // Rb = D^-1 S_bo (columns outside the block)
         for (int e = t; e < m * n; e += kGjThreads) {
@@ -374,6 +389,127 @@ __device__ __forceinline__ bool mg_sync(unsigned long long* bar, unsigned long l
     }
     __syncthreads();
     return *s_ok != 0;
+}
+
+// Dense inverse of a coarsest level too large for one CTA: blocked Gauss-Jordan (32 pivots
+// per block, the drop rule and regularisation of k_gauss_jordan) over the whole grid, one
+// cooperative launch with one grid barrier per block.  CTA c keeps the column strip
+// [c0, c1) of the matrix in shared memory.  Block step b: every CTA reads the block's column
+// panel S[:, b] (global, double-buffered; the strips holding the panel's columns wrote it at
+// the end of step b - 1), inverts the diagonal block D = S_bb (one warp), and updates its own
+// columns j: outside the block R_j = D^-1 S_bj, S_ij -= S_ib R_j (rows outside), S_bj = R_j;
+// inside it S_ij = -S_ib (D^-1)_j (rows outside), S_bj = (D^-1)_j.  The products sum over the
+// block's pivots in order, as k_gauss_jordan's do.
+constexpr int kGjgThreads = 512;
+constexpr int kMgDenseGridMax = 1280;  // largest dense coarsest (the grid Gauss-Jordan's strip budget)
+constexpr int kGjgMaxStrip = 12;       // columns per CTA strip (the launch uses at least n / 12 CTAs)
+
+__global__ void __launch_bounds__(kGjgThreads) k_gauss_jordan_grid(int n, double* __restrict__ M, double* __restrict__ panel,
+                                                                   unsigned long long* bar, unsigned long long* dmax_bits, int* err,
+                                                                   long long limit) {
+    extern __shared__ double gsm[];
+    __shared__ double Dm[kGjBlock * kGjDS];
+    __shared__ int s_ok;
+    const int G = gridDim.x, t = threadIdx.x;
+    const int c0 = (int)((long long)n * blockIdx.x / G), c1 = (int)((long long)n * (blockIdx.x + 1) / G), w = c1 - c0;
+    double* S = gsm;                   // the strip, column-major: S[jj * n + i] = M[i][c0 + jj]
+    double* R = S + (size_t)n * w;     // kGjBlock x w: the block rows' new values on the strip
+    unsigned long long target = 0;
+    // the strip, its regularised diagonal, and the largest diagonal (the drop threshold)
+    for (int e = t; e < n * w; e += kGjgThreads) {
+        const int i = e / w, jj = e % w;
+        double v = M[(size_t)i * n + c0 + jj];
+        if (i == c0 + jj) v *= (1.0 + 1e-8);
+        S[(size_t)jj * n + i] = v;
+    }
+    if (t == 0) {
+        double m = 0;
+        for (int jj = 0; jj < w; jj++) m = fmax(m, fabs(M[(size_t)(c0 + jj) * n + c0 + jj]));
+        atomicMax(dmax_bits, (unsigned long long)__double_as_longlong(m));  // non-negative: the bits order as the values
+    }
+    __syncthreads();
+    // panel of block 0 (columns 0 .. 31, column-major) from the strips that hold them
+    for (int e = t; e < n * w; e += kGjgThreads) {
+        const int jj = e / n, i = e % n, j = c0 + jj;
+        if (j < kGjBlock) panel[(size_t)j * n + i] = S[e];
+    }
+    if (!mg_sync(bar, target, err, &s_ok, limit)) return;
+    const double thr = 1e-12 * __longlong_as_double((long long)__ldcg(dmax_bits));
+    const int nblk = (n + kGjBlock - 1) / kGjBlock;
+    for (int bk = 0; bk < nblk; bk++) {
+        const int b0 = bk * kGjBlock, m = min(kGjBlock, n - b0);
+        const double* P = panel + (size_t)(bk & 1) * n * kGjBlock;  // P[kk * n + i] = S[i][b0 + kk]
+        double* Pn = panel + (size_t)((bk + 1) & 1) * n * kGjBlock;
+        for (int e = t; e < m * m; e += kGjgThreads) {
+            const int c = e / m, r = e % m;
+            Dm[r * kGjDS + c] = __ldcg(&P[(size_t)c * n + b0 + r]);
+        }
+        __syncthreads();
+        if (t < 32) gj_warp_invert(Dm, m, thr, t);
+        __syncthreads();
+        // X = the block rows' new values on the strip: D^-1 S_b,j outside the block, (D^-1)_j inside
+        for (int e = t; e < m * w; e += kGjgThreads) {
+            const int ii = e / w, jj = e % w, j = c0 + jj;
+            double v;
+            if (j >= b0 && j < b0 + m) {
+                v = Dm[ii * kGjDS + (j - b0)];
+            } else {
+                v = 0;
+                for (int kk = 0; kk < m; kk++) v += Dm[ii * kGjDS + kk] * S[(size_t)jj * n + b0 + kk];
+            }
+            R[ii * w + jj] = v;
+        }
+        __syncthreads();
+        // rows: thread per row; S_ij <- (j in the block ? 0 : S_ij) - sum_k S_ik X_kj, the panel row
+        // read in two halves, the sums over the block's pivots in order
+        for (int i = t; i < n; i += kGjgThreads) {
+            if (i >= b0 && i < b0 + m) {
+                for (int jj = 0; jj < w; jj++) S[(size_t)jj * n + i] = R[(i - b0) * w + jj];
+                continue;
+            }
+            double acc[kGjgMaxStrip];
+#pragma unroll
+            for (int jj = 0; jj < kGjgMaxStrip; jj++) acc[jj] = 0.0;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                double ph[kGjBlock / 2];
+#pragma unroll
+                for (int u = 0; u < kGjBlock / 2; u++) {
+                    const int kk = h * (kGjBlock / 2) + u;
+                    ph[u] = kk < m ? __ldcg(&P[(size_t)kk * n + i]) : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < kGjBlock / 2; u++) {
+                    const int kk = h * (kGjBlock / 2) + u;
+#pragma unroll
+                    for (int jj = 0; jj < kGjgMaxStrip; jj++)
+                        if (jj < w && kk < m) acc[jj] += ph[u] * R[kk * w + jj];
+                }
+            }
+#pragma unroll
+            for (int jj = 0; jj < kGjgMaxStrip; jj++) {
+                if (jj < w) {
+                    const int j = c0 + jj;
+                    const double old = (j >= b0 && j < b0 + m) ? 0.0 : S[(size_t)jj * n + i];
+                    S[(size_t)jj * n + i] = old - acc[jj];
+                }
+            }
+        }
+        __syncthreads();
+        // the next block's panel from the strips that hold its columns
+        if (bk + 1 < nblk) {
+            const int nb0 = b0 + kGjBlock, nm = min(kGjBlock, n - nb0);
+            for (int e = t; e < n * w; e += kGjgThreads) {
+                const int jj = e / n, i = e % n, j = c0 + jj;
+                if (j >= nb0 && j < nb0 + nm) Pn[(size_t)(j - nb0) * n + i] = S[e];
+            }
+        }
+        if (!mg_sync(bar, target, err, &s_ok, limit)) return;
+    }
+    for (int e = t; e < n * w; e += kGjgThreads) {
+        const int i = e / w, jj = e % w;
+        M[(size_t)i * n + c0 + jj] = S[(size_t)jj * n + i];
+    }
 }
 
 // Cluster variant: the hardware cluster barrier (release/acquire at cluster
@@ -755,6 +891,7 @@ struct MgSmArgs {
     int* cl_fail;            // per cluster: a grid-barrier wait of one of its CTAs gave up
     const int32_t* mptr0;    // level-0 aggregates (the chain blocks): first row of each, then n
     int smem_bytes;          // dynamic shared memory of the launch
+    int grid_coarse;         // dense coarsest solved by all CTAs between grid barriers (lc = coarsest, no clusters)
 };
 
 // Rows [lo, hi) of one fused operator.  ptr[i - lo] - sub and ptr[i - lo + 1] - sub bound the
@@ -975,7 +1112,7 @@ __global__ void __launch_bounds__(kSmThreads) k_mg_pcg_sm(MgArgs a, MgSmArgs sa)
     __shared__ SmStage st[kSmMaxStages];
     __shared__ int n_st;
     __shared__ int s_ok;
-    __shared__ double rc[kMgDenseMax];
+    __shared__ double rc[kMgDenseGridMax];
     const int cta = blockIdx.x, nb = gridDim.x;
     const int cid = cta / kSmCtas, crank = cta % kSmCtas;
     const int C = a.levels - 1, Lc = sa.lc;
@@ -1050,6 +1187,26 @@ __global__ void __launch_bounds__(kSmThreads) k_mg_pcg_sm(MgArgs a, MgSmArgs sa)
             L.agg = G0.agg + L.lo;
             L.mptr = sa.mptr0 + L.alo; L.mptr_sub = L.lo;
         }
+        // chain-block inverse rows (both smoother phases read them: before the coarse rows)
+        const int t0 = nr > 0 ? a.row_off[L.lo] : 0;
+        const int T = nr > 0 ? a.row_off[L.hi - 1] + a.row_m[L.hi - 1] - t0 : 0;
+        unsigned char* m_meta = nr > 0 && ns + 4 <= kSmMaxStages ? take(12u * nr) : nullptr;
+        unsigned char* m_t = m_meta ? take(8u * T) : nullptr;
+        if (m_t) {
+            L.roff = reinterpret_cast<const int32_t*>(m_meta); L.roff_sub = 0;
+            L.rbase = L.roff + nr; L.rbase_sub = 0;
+            L.rm = L.rbase + nr;
+            L.tinv = reinterpret_cast<const double*>(m_t);
+            st[ns++] = SmStage{m_meta, a.row_off + L.lo, nr, 4, t0};
+            st[ns++] = SmStage{m_meta + 4u * nr, a.row_base + L.lo, nr, 4, L.lo};
+            st[ns++] = SmStage{m_meta + 8u * nr, a.row_m + L.lo, nr, 4, 0};
+            st[ns++] = SmStage{m_t, a.tinv + t0, T, 8, 0};
+        } else {
+            L.roff = a.row_off + L.lo; L.roff_sub = t0;
+            L.rbase = a.row_base + L.lo; L.rbase_sub = L.lo;
+            L.rm = a.row_m + L.lo;
+            L.tinv = a.tinv + t0;
+        }
         // coarse levels: grid rows below lc, cluster rows from lc on
         auto lanes_for = [](long long entries, int rows) {
             int ln = 2;
@@ -1071,8 +1228,8 @@ __global__ void __launch_bounds__(kSmThreads) k_mg_pcg_sm(MgArgs a, MgSmArgs sa)
             ns = sm_place_rows(P.Q[l], qlo, qhi, F.pq_ptr, F.pq_col, F.pq_val, F.agg, F.l1inv, sm_dyn, cap, used, st, ns, kSmMaxStages);
         }
         const int nC = lv[C].n;
-        P.clo = (int)((long long)nC * crank / kSmCtas);
-        P.chi = (int)((long long)nC * (crank + 1) / kSmCtas);
+        P.clo = sa.grid_coarse ? (int)((long long)nC * cta / nb) : (int)((long long)nC * crank / kSmCtas);
+        P.chi = sa.grid_coarse ? (int)((long long)nC * (cta + 1) / nb) : (int)((long long)nC * (crank + 1) / kSmCtas);
         P.cinv = nullptr;
         if (a.cinv) {
             const int cr = P.chi - P.clo;
@@ -1083,27 +1240,6 @@ __global__ void __launch_bounds__(kSmThreads) k_mg_pcg_sm(MgArgs a, MgSmArgs sa)
             } else {
                 P.cinv = a.cinv + (size_t)P.clo * nC;
             }
-        }
-        // chain-block inverse rows (last: a phase reads them from shared memory with no other
-        // global trip, so they are the cheapest to leave in global memory)
-        const int t0 = nr > 0 ? a.row_off[L.lo] : 0;
-        const int T = nr > 0 ? a.row_off[L.hi - 1] + a.row_m[L.hi - 1] - t0 : 0;
-        unsigned char* m_meta = nr > 0 && ns + 4 <= kSmMaxStages ? take(12u * nr) : nullptr;
-        unsigned char* m_t = m_meta ? take(8u * T) : nullptr;
-        if (m_t) {
-            L.roff = reinterpret_cast<const int32_t*>(m_meta); L.roff_sub = 0;
-            L.rbase = L.roff + nr; L.rbase_sub = 0;
-            L.rm = L.rbase + nr;
-            L.tinv = reinterpret_cast<const double*>(m_t);
-            st[ns++] = SmStage{m_meta, a.row_off + L.lo, nr, 4, t0};
-            st[ns++] = SmStage{m_meta + 4u * nr, a.row_base + L.lo, nr, 4, L.lo};
-            st[ns++] = SmStage{m_meta + 8u * nr, a.row_m + L.lo, nr, 4, 0};
-            st[ns++] = SmStage{m_t, a.tinv + t0, T, 8, 0};
-        } else {
-            L.roff = a.row_off + L.lo; L.roff_sub = t0;
-            L.rbase = a.row_base + L.lo; L.rbase_sub = L.lo;
-            L.rm = a.row_m + L.lo;
-            L.tinv = a.tinv + t0;
         }
         P.used = used;
         n_st = ns;
@@ -1153,7 +1289,7 @@ __global__ void __launch_bounds__(kSmThreads) k_mg_pcg_sm(MgArgs a, MgSmArgs sa)
         mg_reduce1(rr_l, sm, s0);
         if (threadIdx.x == 0) a.partA[cta] = s0;
         sm_sync(a, sa.cl_fail, target, cid, &s_ok);
-        if (!sm_cluster_ok(sa.cl_fail, cid)) break;
+        if (!sa.grid_coarse && !sm_cluster_ok(sa.cl_fail, cid)) break;
         rr = sm_sum_partials(a.partA, nb, sm);
         if (k == 0 && !recursive && restarts == 0) R0 = a.tol * sqrt(rr);
         if (k > 0 && sqrt(rr) <= R0) {
@@ -1211,7 +1347,10 @@ __global__ void __launch_bounds__(kSmThreads) k_mg_pcg_sm(MgArgs a, MgSmArgs sa)
             } else {  // l1-Jacobi only: the correction is the smoothed z
                 for (int i = P.clo + threadIdx.x; i < P.chi; i += blockDim.x) Cl.zf[i] = __ldcg(&Cl.z[i]);
             }
-            cluster_sync_all();
+            if (sa.grid_coarse)
+                sm_sync(a, sa.cl_fail, target, cid, &s_ok);
+            else
+                cluster_sync_all();
         }
         for (int l = C - 1; l >= Lc; l--) {
             sm_prolong(P.Q[l], lv[l].pq_lanes, lv[l].n, lv[l].r, lv[l].z, lv[l + 1].zf, lv[l].zf);
@@ -1536,12 +1675,507 @@ __global__ void k_cagg_rows(int n, const int32_t* __restrict__ rp, const int32_t
         for (int k = rp[i]; k < rp[i + 1]; k++) cagg[k] = agg[ci[k]];
 }
 
+// ---------------------------------------------------------------------------
+// Smoothed level-1 prolongator (hierarchies of the clustered kernel).
+//
+// Why: with piecewise-constant aggregates below the chain level the V-cycle is weak on
+// the chain graph, whose junction conductances span five orders of magnitude.  Smoothing
+// the first pairwise prolongator once, Q = (I - w D^-1 A_1) P with D the l1-Jacobi
+// diagonal and w = 4/3, takes a real-resistor pass of the 25k-CNT network from ~90 to
+// ~35 PCG iterations and its unit pass from 54 to 39.  Then A_2 = Q^T A_1 Q, the
+// restriction rows are Q^T on r_1 and -Q^T A_1 on z_1, and the prolongation-smoother rows
+// are A_1 on z_1 and A_1 (Q + w P) on zc, so that the solve kernel's unchanged
+//   zf = z + zc[agg] + D^-1 (r - A_1 z - A_1 (Q + w P) zc)
+// equals z + Q zc + D^-1 (r - A_1 (z + Q zc)), since Q zc = zc[agg] - w D^-1 T zc with
+// T = A_1 P.  Every product is a row gather: output row J sums w * (row s of B) over its
+// sources (s, w); the terms are sorted by column (keys (column, gather position) are
+// unique) and summed in gather order, so no result depends on thread timing.
+constexpr double kSaOmega = 4.0 / 3.0;
+constexpr int kGrWarps = 4;
+constexpr int kGrCap = 512;  // power of two
+
+struct RowSrc {  // sources of output row J: (J, 1) when ptr is null, else (J, diag[J]) (with diag) and row J of the CSR
+    const int32_t* ptr;
+    const int32_t* idx;
+    const double* val;
+    const double* diag;
+};
+struct RowMat {  // row s of B: (s, diag[s]) (with diag), then its CSR entries; val2 / diag2: a second value set
+    const int32_t* ptr;
+    const int32_t* col;
+    const double* val;
+    const double* diag;
+    const double* val2;
+    const double* diag2;
+    const int32_t* cmap;  // column map (null: identity)
+};
+struct GatherOut {
+    const int32_t* seg;                 // per output row: offset of its segment (candidate terms)
+    uint64_t* gkey;                     // long rows: gathered terms (segment layout)
+    double* gv;
+    double* gv2;
+    uint64_t* okey;                     // summed runs (segment layout)
+    double* ov;
+    double* ov2;
+    int32_t* ulen;                      // runs per row
+    int32_t* longr;                     // rows with more than kGrCap terms
+    int32_t* nlong;
+    int skip_diag;                      // drop column J of row J
+    const double* rsv;                  // with rs_out: row sum of row J = sum_t w_t rsv[s_t]
+    double* rs_out;
+    double* diag_out;
+    double* l1_out;
+};
+
+__device__ __forceinline__ int src_count(const RowSrc& S, int J) { return S.ptr ? (S.ptr[J + 1] - S.ptr[J]) + (S.diag ? 1 : 0) : 1; }
+
+__device__ __forceinline__ void src_get(const RowSrc& S, int J, int t, int& s, double& w) {
+    if (!S.ptr) {
+        s = J;
+        w = 1.0;
+        return;
+    }
+    if (S.diag) {
+        if (t == 0) {
+            s = J;
+            w = S.diag[J];
+            return;
+        }
+        t--;
+    }
+    const int k = S.ptr[J] + t;
+    s = S.idx[k];
+    w = S.val[k];
+}
+
+__device__ __forceinline__ int mat_len(const RowMat& B, int s) { return (B.ptr[s + 1] - B.ptr[s]) + (B.diag ? 1 : 0); }
+
+__device__ __forceinline__ void mat_get(const RowMat& B, int s, int t, int& c, double& v, double& v2) {
+    if (B.diag && t == 0) {
+        c = s;
+        v = B.diag[s];
+        v2 = B.diag2 ? B.diag2[s] : 0.0;
+    } else {
+        const int k = B.ptr[s] + t - (B.diag ? 1 : 0);
+        c = B.col[k];
+        v = B.val[k];
+        v2 = B.val2 ? B.val2[k] : 0.0;
+    }
+    if (B.cmap) c = B.cmap[c];
+}
+
+__global__ void k_gather_len(int nrows, RowSrc S, RowMat B, int32_t* __restrict__ seg) {
+    for (int J = blockIdx.x * blockDim.x + threadIdx.x; J < nrows; J += gridDim.x * blockDim.x) {
+        int c = 0;
+        const int ns = src_count(S, J);
+        for (int t = 0; t < ns; t++) {
+            int s;
+            double w;
+            src_get(S, J, t, s, w);
+            c += mat_len(B, s);
+        }
+        seg[J] = c;
+        if (J == 0) seg[nrows] = 0;
+    }
+}
+
+// Sorted keys of one row (gather positions in their low half) summed into runs of equal
+// columns in gather order; with rs_out, the row's diagonal from its row sum (skip_diag rows)
+// and its l1-Jacobi weight, as reduce_row does.
+__device__ __forceinline__ void gather_reduce(int J, int cnt, const uint64_t* key, const double* val, const double* val2, double rs,
+                                              const GatherOut& O, int o) {
+    int u = 0;
+    double off = 0, offabs = 0;
+    for (int i = 0; i < cnt;) {
+        const uint32_t c = (uint32_t)(key[i] >> 32);
+        double acc = 0, acc2 = 0;
+        while (i < cnt && (uint32_t)(key[i] >> 32) == c) {
+            const uint32_t p = (uint32_t)key[i];
+            acc += val[p];
+            if (val2) acc2 += val2[p];
+            i++;
+        }
+        O.okey[o + u] = c;
+        O.ov[o + u] = acc;
+        if (val2) O.ov2[o + u] = acc2;
+        u++;
+        off += acc;
+        offabs += fabs(acc);
+    }
+    O.ulen[J] = u;
+    if (O.rs_out) {
+        const double d = rs - off;
+        O.rs_out[J] = rs;
+        O.diag_out[J] = d;
+        const double l1 = fabs(d) + offabs;
+        O.l1_out[J] = l1 > 0 ? 1.0 / l1 : 0.0;
+    }
+}
+
+// One warp per output row: ballot-ranked gather into shared memory, bitonic sort of the
+// keys, lane 0 sums the runs.  Rows with more than kGrCap terms go to k_gather_rows_long.
+__global__ void __launch_bounds__(kGrWarps * 32) k_gather_rows(int nrows, RowSrc S, RowMat B, GatherOut O) {
+    extern __shared__ __align__(16) unsigned char gr_sm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool two = B.val2 != nullptr;
+    uint64_t* K = reinterpret_cast<uint64_t*>(gr_sm) + warp * kGrCap;
+    double* V = reinterpret_cast<double*>(gr_sm) + (kGrWarps + warp) * kGrCap;
+    double* V2 = two ? reinterpret_cast<double*>(gr_sm) + (2 * kGrWarps + warp) * kGrCap : nullptr;
+    for (int J = blockIdx.x * kGrWarps + warp; J < nrows; J += gridDim.x * kGrWarps) {
+        int cnt = 0;
+        double rs = 0;
+        const int ns = src_count(S, J);
+        for (int t = 0; t < ns; t++) {
+            int s;
+            double w;
+            src_get(S, J, t, s, w);
+            if (O.rsv && lane == 0) rs += w * O.rsv[s];
+            const int L = mat_len(B, s);
+            for (int k0 = 0; k0 < L; k0 += 32) {
+                const int k = k0 + lane;
+                int c = 0;
+                double x = 0, x2 = 0;
+                bool keep = false;
+                if (k < L) {
+                    mat_get(B, s, k, c, x, x2);
+                    keep = !(O.skip_diag && c == J);
+                }
+                const unsigned bal = __ballot_sync(0xffffffffu, keep);
+                const int pos = cnt + __popc(bal & ((1u << lane) - 1u));
+                if (keep && pos < kGrCap) {
+                    K[pos] = ((uint64_t)(uint32_t)c << 32) | (uint32_t)pos;
+                    V[pos] = w * x;
+                    if (two) V2[pos] = w * x2;
+                }
+                cnt += __popc(bal);
+            }
+        }
+        if (cnt > kGrCap) {
+            if (lane == 0) O.longr[atomicAdd(O.nlong, 1)] = J;
+            __syncwarp();
+            continue;
+        }
+        int P = 1;
+        while (P < cnt) P <<= 1;
+        for (int i = cnt + lane; i < P; i += 32) K[i] = ~0ull;
+        __syncwarp();
+        for (int size = 2; size <= P; size <<= 1)
+            for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                for (int i = lane; i < P; i += 32) {
+                    const int j = i ^ stride;
+                    if (j > i) {
+                        const bool up = (i & size) == 0;
+                        const uint64_t ki = K[i], kj = K[j];
+                        if ((ki > kj) == up) {
+                            K[i] = kj;
+                            K[j] = ki;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        if (lane == 0) gather_reduce(J, cnt, K, V, V2, rs, O, O.seg[J]);
+        __syncwarp();
+    }
+}
+
+// The rows k_gather_rows listed as too long: one thread each, gathered and Shell-sorted in
+// the global scratch at the row's segment (same keys, so the same sums as the warp path).
+__global__ void k_gather_rows_long(RowSrc S, RowMat B, GatherOut O) {
+    const int nl = *O.nlong;
+    const bool two = B.val2 != nullptr;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nl; q += gridDim.x * blockDim.x) {
+        const int J = O.longr[q];
+        const int o = O.seg[J];
+        uint64_t* K = O.gkey + o;
+        double* V = O.gv + o;
+        double* V2 = two ? O.gv2 + o : nullptr;
+        int cnt = 0;
+        double rs = 0;
+        const int ns = src_count(S, J);
+        for (int t = 0; t < ns; t++) {
+            int s;
+            double w;
+            src_get(S, J, t, s, w);
+            if (O.rsv) rs += w * O.rsv[s];
+            const int L = mat_len(B, s);
+            for (int k = 0; k < L; k++) {
+                int c;
+                double x, x2;
+                mat_get(B, s, k, c, x, x2);
+                if (O.skip_diag && c == J) continue;
+                K[cnt] = ((uint64_t)(uint32_t)c << 32) | (uint32_t)cnt;
+                V[cnt] = w * x;
+                if (two) V2[cnt] = w * x2;
+                cnt++;
+            }
+        }
+        int gap = 1;
+        while (gap * 9 / 4 + 1 < cnt) gap = gap * 9 / 4 + 1;
+        for (;; gap = max(1, (gap - 1) * 4 / 9)) {  // ..., 2, 1: the last pass is insertion sort
+            for (int i = gap; i < cnt; i++) {
+                const uint64_t key = K[i];
+                int j = i;
+                while (j >= gap && K[j - gap] > key) {
+                    K[j] = K[j - gap];
+                    j -= gap;
+                }
+                K[j] = key;
+            }
+            if (gap == 1) break;
+        }
+        gather_reduce(J, cnt, K, V, V2, rs, O, o);
+    }
+}
+
+__global__ void k_gather_copy(int nrows, const int32_t* __restrict__ seg, const int32_t* __restrict__ ulen, const int32_t* __restrict__ rp,
+                              const uint64_t* __restrict__ okey, const double* __restrict__ ov, const double* __restrict__ ov2,
+                              int32_t* __restrict__ col, double* __restrict__ val, double* __restrict__ val2) {
+    for (int J = blockIdx.x * blockDim.x + threadIdx.x; J < nrows; J += gridDim.x * blockDim.x) {
+        const int o = seg[J], d = rp[J];
+        for (int i = 0; i < ulen[J]; i++) {
+            col[d + i] = (int32_t)okey[o + i];
+            val[d + i] = ov[o + i];
+            if (val2) val2[d + i] = ov2[o + i];
+        }
+    }
+}
+
+// Q = P - w D^-1 T and Q + w P on T's pattern (T_i always holds column agg[i]).
+__global__ void k_sa_q(int n, const int32_t* __restrict__ tp, const int32_t* __restrict__ tc, const double* __restrict__ tv,
+                       const int32_t* __restrict__ agg, const double* __restrict__ l1inv, double* __restrict__ qv, double* __restrict__ qpv) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int a = agg[i];
+        const double m = l1inv[i];
+        for (int k = tp[i]; k < tp[i + 1]; k++) {
+            const double base = tc[k] == a ? 1.0 : 0.0;
+            const double q = base - kSaOmega * m * tv[k];
+            qv[k] = q;
+            qpv[k] = q + kSaOmega * base;
+        }
+    }
+}
+
+// Transpose of a CSR with unique columns per row: count, place, then each column's rows in order.
+__global__ void k_col_count(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ col, int32_t* __restrict__ cnt) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (int k = rp[i]; k < rp[i + 1]; k++) atomicAdd(&cnt[col[k]], 1);
+}
+
+__global__ void k_col_place(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ col, const double* __restrict__ val,
+                            const int32_t* __restrict__ cptr, int32_t* __restrict__ cursor, int32_t* __restrict__ ridx, double* __restrict__ rval) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (int k = rp[i]; k < rp[i + 1]; k++) {
+            const int c = col[k];
+            const int p = cptr[c] + atomicAdd(&cursor[c], 1);
+            ridx[p] = i;
+            rval[p] = val[k];
+        }
+}
+
+__global__ void k_seg_sort(int nc, const int32_t* __restrict__ ptr, int32_t* __restrict__ idx, double* __restrict__ val) {
+    for (int J = blockIdx.x * blockDim.x + threadIdx.x; J < nc; J += gridDim.x * blockDim.x) {
+        const int b = ptr[J], e = ptr[J + 1];
+        for (int i = b + 1; i < e; i++) {
+            const int x = idx[i];
+            const double y = val[i];
+            int j = i - 1;
+            while (j >= b && idx[j] > x) {
+                idx[j + 1] = idx[j];
+                val[j + 1] = val[j];
+                j--;
+            }
+            idx[j + 1] = x;
+            val[j + 1] = y;
+        }
+    }
+}
+
+// v = A_1 Q 1 for the coarse row sums: Q 1 = 1 - w D^-1 rs, so v = rs - w A_1 (D^-1 rs); rs
+// is nonzero only next to prescribed nodes, so the chain conductances never cancel here.
+__global__ void k_sa_y(int n, const double* __restrict__ l1inv, const double* __restrict__ rs, double* __restrict__ y) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = l1inv[i] * rs[i];
+}
+
+__global__ void k_sa_v(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const double* __restrict__ val,
+                       const double* __restrict__ diag, const double* __restrict__ rs, const double* __restrict__ y, double* __restrict__ v) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double s = diag[i] * y[i];
+        for (int k = rp[i]; k < rp[i + 1]; k++) s += val[k] * y[ci[k]];
+        v[i] = rs[i] - kSaOmega * s;
+    }
+}
+
+// Fused restriction rows of the smoothed level: row J = Q^T row J on r_1 (columns < n), then
+// -(Q^T A_1) row J on z_1 (columns n + c).
+__global__ void k_rr_fill_sa(int nc, int n, const int32_t* __restrict__ qtp, const int32_t* __restrict__ qti, const double* __restrict__ qtv,
+                             const int32_t* __restrict__ ap, const int32_t* __restrict__ ac, const double* __restrict__ av,
+                             int32_t* __restrict__ rr_ptr, int32_t* __restrict__ rr_col, double* __restrict__ rr_val) {
+    for (int J = blockIdx.x * blockDim.x + threadIdx.x; J < nc; J += gridDim.x * blockDim.x) {
+        int e = qtp[J] + ap[J];
+        rr_ptr[J] = e;
+        if (J == nc - 1) rr_ptr[nc] = qtp[nc] + ap[nc];
+        for (int k = qtp[J]; k < qtp[J + 1]; k++, e++) {
+            rr_col[e] = qti[k];
+            rr_val[e] = qtv[k];
+        }
+        for (int k = ap[J]; k < ap[J + 1]; k++, e++) {
+            rr_col[e] = n + ac[k];
+            rr_val[e] = -av[k];
+        }
+    }
+}
+
+// Fused prolongation-smoother rows of the smoothed level: row I = A_1 row I with its diagonal
+// on z_1, then A_1 (Q + w P) row I on zc (columns n + J).
+__global__ void k_pq_fill_sa(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const double* __restrict__ v,
+                             const double* __restrict__ diag, const int32_t* __restrict__ wp, const int32_t* __restrict__ wc,
+                             const double* __restrict__ wv, int32_t* __restrict__ pq_ptr, int32_t* __restrict__ pq_col,
+                             double* __restrict__ pq_val) {
+    for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < n; I += gridDim.x * blockDim.x) {
+        int e = rp[I] + I + wp[I];
+        pq_ptr[I] = e;
+        if (I == n - 1) pq_ptr[n] = rp[n] + n + wp[n];
+        pq_col[e] = I;
+        pq_val[e] = diag[I];
+        e++;
+        for (int k = rp[I]; k < rp[I + 1]; k++, e++) {
+            pq_col[e] = ci[k];
+            pq_val[e] = v[k];
+        }
+        for (int k = wp[I]; k < wp[I + 1]; k++, e++) {
+            pq_col[e] = n + wc[k];
+            pq_val[e] = wv[k];
+        }
+    }
+}
+
+// One row-gather product: the compacted CSR (optr, ocol, oval[, oval2]) of nrows rows, its
+// arrays sized by the candidate-term count (one host read), which is returned (>= entries).
+long long gather_product(MgWork& g, int nrows, const RowSrc& S, const RowMat& B, bool skip_diag, const double* rsv, double* rs_out,
+                         double* diag_out, double* l1_out, DBuf<int32_t>& optr, DBuf<int32_t>& ocol, DBuf<double>& oval,
+                         DBuf<double>* oval2, cudaStream_t s, int64_t& launches) {
+    MgWork::Smoothed& w = g.sa;
+    w.seg.ensure(nrows + 1);
+    k_gather_len<<<grid_for(nrows), 256, 0, s>>>(nrows, S, B, w.seg.get());
+    launches++;
+    scan_small(w.seg.get(), w.seg.get(), nrows + 1, g.total.get(), g, s, launches);
+    int cand = 0;
+    CICY_CUDA(cudaMemcpyAsync(&cand, g.total.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    CICY_CUDA(cudaStreamSynchronize(s));
+    const size_t cap = (size_t)std::max(cand, 1);
+    const bool two = B.val2 != nullptr;
+    w.gkey.ensure(cap);
+    w.gv.ensure(cap);
+    w.okey.ensure(cap);
+    w.ov.ensure(cap);
+    if (two) {
+        w.gv2.ensure(cap);
+        w.ov2.ensure(cap);
+    }
+    w.ulen.ensure(nrows + 1);
+    w.longr.ensure(nrows + 1);
+    CICY_CUDA(cudaMemsetAsync(g.total.get() + 1, 0, sizeof(int32_t), s));
+    CICY_CUDA(cudaMemsetAsync(w.ulen.get() + nrows, 0, sizeof(int32_t), s));
+    const GatherOut O{w.seg.get(),  w.gkey.get(), w.gv.get(),  two ? w.gv2.get() : nullptr, w.okey.get(), w.ov.get(),
+                      two ? w.ov2.get() : nullptr, w.ulen.get(), w.longr.get(), g.total.get() + 1, skip_diag ? 1 : 0,
+                      rsv, rs_out, diag_out, l1_out};
+    const int smem = (int)(sizeof(double) * kGrWarps * kGrCap * (two ? 3 : 2));
+    static bool attr = false;
+    if (!attr) {
+        CICY_CUDA(cudaFuncSetAttribute(k_gather_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(sizeof(double) * kGrWarps * kGrCap * 3)));
+        attr = true;
+    }
+    k_gather_rows<<<grid_for((long long)nrows * 32, kGrWarps * 32), kGrWarps * 32, smem, s>>>(nrows, S, B, O);
+    k_gather_rows_long<<<grid_for(nrows, 128), 128, 0, s>>>(S, B, O);
+    optr.ensure(nrows + 1);
+    scan_small(w.ulen.get(), optr.get(), nrows + 1, nullptr, g, s, launches);
+    ocol.ensure(cap);
+    oval.ensure(cap);
+    if (two) oval2->ensure(cap);
+    k_gather_copy<<<grid_for(nrows), 256, 0, s>>>(nrows, w.seg.get(), w.ulen.get(), optr.get(), w.okey.get(), w.ov.get(),
+                                                  two ? w.ov2.get() : nullptr, ocol.get(), oval.get(), two ? oval2->get() : nullptr);
+    launches += 3;
+    CICY_LAUNCH_CHECK();
+    return cand;
+}
+
+// Level 2 from level 1 through the smoothed prolongator (nc pairwise aggregates in
+// g.L[1].agg), with level 1's fused restriction and prolongation-smoother rows.
+void coarsen_smoothed(MgWork& g, int nc, cudaStream_t s, int64_t& launches) {
+    MgWork::Lvl& F = g.L[1];
+    MgWork::Lvl& G = g.L[2];
+    MgWork::Smoothed& w = g.sa;
+    const int n = F.n;
+    const RowSrc one{nullptr, nullptr, nullptr, nullptr};
+    const RowSrc a1_src{F.rp_ptr, F.ci_ptr, F.val_ptr, F.diag.get()};
+    const RowMat a1{F.rp_ptr, F.ci_ptr, F.val_ptr, F.diag.get(), nullptr, nullptr, nullptr};
+    const RowMat a1_agg{F.rp_ptr, F.ci_ptr, F.val_ptr, F.diag.get(), nullptr, nullptr, F.agg.get()};
+    // T = A_1 P, then Q and Q + w P on its pattern
+    const long long nt = gather_product(g, n, one, a1_agg, false, nullptr, nullptr, nullptr, nullptr, w.tp, w.tc, w.tv, nullptr, s, launches);
+    w.qv.ensure(nt);
+    w.qpv.ensure(nt);
+    k_sa_q<<<grid_for(n), 256, 0, s>>>(n, w.tp.get(), w.tc.get(), w.tv.get(), F.agg.get(), F.l1inv.get(), w.qv.get(), w.qpv.get());
+    // Q^T: each aggregate's rows in ascending order
+    w.qtp.ensure(nc + 1);
+    w.qti.ensure(nt);
+    w.qtv.ensure(nt);
+    g.flag.ensure(nc + 1);
+    CICY_CUDA(cudaMemsetAsync(g.flag.get(), 0, sizeof(int32_t) * (nc + 1), s));
+    k_col_count<<<grid_for(n), 256, 0, s>>>(n, w.tp.get(), w.tc.get(), g.flag.get());
+    scan_small(g.flag.get(), w.qtp.get(), nc + 1, nullptr, g, s, launches);
+    CICY_CUDA(cudaMemsetAsync(g.flag.get(), 0, sizeof(int32_t) * (nc + 1), s));
+    k_col_place<<<grid_for(n), 256, 0, s>>>(n, w.tp.get(), w.tc.get(), w.qv.get(), w.qtp.get(), g.flag.get(), w.qti.get(), w.qtv.get());
+    k_seg_sort<<<grid_for(nc), 256, 0, s>>>(nc, w.qtp.get(), w.qti.get(), w.qtv.get());
+    launches += 4;
+    const RowSrc qt_src{w.qtp.get(), w.qti.get(), w.qtv.get(), nullptr};
+    // W = A_1 Q and A_1 (Q + w P)
+    const RowMat q{w.tp.get(), w.tc.get(), w.qv.get(), nullptr, w.qpv.get(), nullptr, nullptr};
+    const long long nw = gather_product(g, n, a1_src, q, false, nullptr, nullptr, nullptr, nullptr, w.wp, w.wc, w.wv, &w.wpv, s, launches);
+    // Q^T A_1 (the restriction rows' part on z_1)
+    const long long na = gather_product(g, nc, qt_src, a1, false, nullptr, nullptr, nullptr, nullptr, w.ap, w.ac, w.av, nullptr, s, launches);
+    // A_2 = Q^T W off the diagonal; its diagonal from the row sums Q^T A_1 Q 1
+    w.y.ensure(n);
+    w.v.ensure(n);
+    k_sa_y<<<grid_for(n), 256, 0, s>>>(n, F.l1inv.get(), F.rs.get(), w.y.get());
+    k_sa_v<<<grid_for(n), 256, 0, s>>>(n, F.rp_ptr, F.ci_ptr, F.val_ptr, F.diag.get(), F.rs.get(), w.y.get(), w.v.get());
+    launches += 2;
+    G.n = nc;
+    G.rs.ensure(nc);
+    G.diag.ensure(nc);
+    G.l1inv.ensure(nc);
+    const RowMat wm{w.wp.get(), w.wc.get(), w.wv.get(), nullptr, nullptr, nullptr, nullptr};
+    const long long n2 = gather_product(g, nc, qt_src, wm, true, w.v.get(), G.rs.get(), G.diag.get(), G.l1inv.get(), G.rp, G.ci, G.val,
+                                        nullptr, s, launches);
+    G.nnz = (int)std::max<long long>(n2, 1);
+    G.rp_ptr = G.rp.get();
+    G.ci_ptr = G.ci.get();
+    G.val_ptr = G.val.get();
+    // level 1's fused rows
+    F.rr_ptr.ensure(nc + 1);
+    F.rr_col.ensure(std::max<long long>(nt + na, 1));
+    F.rr_val.ensure(std::max<long long>(nt + na, 1));
+    k_rr_fill_sa<<<grid_for(nc), 256, 0, s>>>(nc, n, w.qtp.get(), w.qti.get(), w.qtv.get(), w.ap.get(), w.ac.get(), w.av.get(), F.rr_ptr.get(),
+                                               F.rr_col.get(), F.rr_val.get());
+    F.pq_ptr.ensure(n + 1);
+    F.pq_col.ensure(std::max<long long>((long long)F.nnz + n + nw, 1));
+    F.pq_val.ensure(std::max<long long>((long long)F.nnz + n + nw, 1));
+    k_pq_fill_sa<<<grid_for(n), 256, 0, s>>>(n, F.rp_ptr, F.ci_ptr, F.val_ptr, F.diag.get(), w.wp.get(), w.wc.get(), w.wpv.get(),
+                                              F.pq_ptr.get(), F.pq_col.get(), F.pq_val.get());
+    launches += 2;
+    CICY_LAUNCH_CHECK();
+}
+
 // Galerkin coarse level l+1 from level l and its aggregates (g.L[l].agg, nc of
 // them), plus level l's member lists, restriction rows (l >= 1) and column
 // aggregates.  No host synchronisation: buffers are sized by the fine level's
 // non-zeros, an upper bound of the coarse level's.
 void coarsen(MgWork& g, int l, int nc, cudaStream_t s, int64_t& launches) {
     if ((int)g.L.size() < l + 2) g.L.resize(l + 2);
+    if (g.fused && g.smooth && l == 1) {
+        coarsen_smoothed(g, nc, s, launches);
+        return;
+    }
     MgWork::Lvl& F = g.L[l];
     MgWork::Lvl& G = g.L[l + 1];
     const int nf = F.n, nnz = F.nnz;
@@ -1663,10 +2297,11 @@ int pairwise(MgWork& g, int l, cudaStream_t s, int64_t& launches) {
 }  // namespace
 
 // ---------------------------------------------------------------------------
-void build_mg_hierarchy(SolverWork& w, const SolverSystem& sys, cudaStream_t s, int64_t& launches, bool fused) {
+void build_mg_hierarchy(SolverWork& w, const SolverSystem& sys, cudaStream_t s, int64_t& launches, bool fused, bool smooth, int* status) {
     MgWork& g = w.mg;
     const int n = sys.n;
     g.fused = fused;
+    g.smooth = smooth;
     TraceSeq tr(s);
     g.total.ensure(2);
     if (g.L.empty()) g.L.resize(1);
@@ -1683,11 +2318,19 @@ void build_mg_hierarchy(SolverWork& w, const SolverSystem& sys, cudaStream_t s, 
     launches += 2;
     int nc = w.n_blocks;
     int C = 0;
+    // the clustered kernel solves a dense coarsest of up to kMgDenseGridMax rows on all CTAs
+    int dense_cap = kMgDenseMax;
+    if (fused) {
+        int dev = 0, sms = 0;
+        CICY_CUDA(cudaGetDevice(&dev));
+        CICY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        dense_cap = std::max(kMgDenseMax, std::min(kMgDenseGridMax, sms * kGjgMaxStrip));
+    }
     for (int l = 0;; l++) {
         coarsen(g, l, nc, s, launches);
         tr.mark("mg.coarsen");
         C = l + 1;
-        if (g.L[C].n <= kMgDenseMax || C + 1 >= kMgMaxLevels) break;
+        if (g.L[C].n <= dense_cap || C + 1 >= kMgMaxLevels) break;
         const int nc2 = pairwise(g, C, s, launches);
         tr.mark("mg.pairwise");
         if (nc2 > 0.9 * g.L[C].n) break;
@@ -1697,11 +2340,43 @@ void build_mg_hierarchy(SolverWork& w, const SolverSystem& sys, cudaStream_t s, 
     MgWork::Lvl& Lc = g.L[C];
     if (Lc.n <= kMgDenseMax) {
         g.cinv.ensure((size_t)Lc.n * Lc.n);
+        CICY_CUDA(cudaMemsetAsync(g.cinv.get(), 0, sizeof(double) * Lc.n * Lc.n, s));
         k_dense_coarse<<<grid_for(Lc.n, 128), 128, 0, s>>>(Lc.n, Lc.rp.get(), Lc.ci.get(), Lc.val.get(), Lc.diag.get(), g.cinv.get());
         const size_t smem = sizeof(double) * ((size_t)Lc.n * Lc.n + 2 * (size_t)Lc.n * kGjBlock + kGjBlock * (kGjBlock + 1) + kGjBlock);
         if (smem > 48 * 1024)
             CICY_CUDA(cudaFuncSetAttribute(k_gauss_jordan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_gauss_jordan<<<1, kGjThreads, smem, s>>>(Lc.n, g.cinv.get());
+        launches += 2;
+        g.dense = true;
+    } else if (Lc.n <= dense_cap) {
+        // larger dense coarsest: the grid Gauss-Jordan (one cooperative launch, column strips)
+        int nC = Lc.n, dev = 0, sms = 0;
+        CICY_CUDA(cudaGetDevice(&dev));
+        CICY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        g.cinv.ensure((size_t)nC * nC);
+        g.gj_panel.ensure((size_t)2 * nC * kGjBlock);
+        g.gj_sync.ensure(2);
+        g.gj_err.ensure(1);
+        CICY_CUDA(cudaMemsetAsync(g.gj_sync.get(), 0, sizeof(unsigned long long) * 2, s));
+        int* err = status;
+        if (!err) {
+            CICY_CUDA(cudaMemsetAsync(g.gj_err.get(), 0, sizeof(int32_t), s));
+            err = g.gj_err.get();
+        }
+        CICY_CUDA(cudaMemsetAsync(g.cinv.get(), 0, sizeof(double) * nC * nC, s));
+        k_dense_coarse<<<grid_for(nC, 128), 128, 0, s>>>(nC, Lc.rp.get(), Lc.ci.get(), Lc.val.get(), Lc.diag.get(), g.cinv.get());
+        const int G = std::max(1, std::min(sms, nC));
+        const int wmax = (nC + G - 1) / G + 1;
+        if ((nC + G - 1) / G > kGjgMaxStrip) throw Fail{CICY_E_INTERNAL, "multigrid: dense coarsest too large for this GPU"};
+        const size_t smem = sizeof(double) * ((size_t)nC * wmax + (size_t)kGjBlock * wmax);
+        CICY_CUDA(cudaFuncSetAttribute(k_gauss_jordan_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        double* M = g.cinv.get();
+        double* panel = g.gj_panel.get();
+        unsigned long long* bar = g.gj_sync.get();
+        unsigned long long* dmax = g.gj_sync.get() + 1;
+        long long limit = w.spin_limit;
+        void* args[] = {&nC, &M, &panel, &bar, &dmax, &err, &limit};
+        CICY_CUDA(cudaLaunchCooperativeKernel((void*)k_gauss_jordan_grid, dim3(G), dim3(kGjgThreads), args, smem, s));
         launches += 2;
         g.dense = true;
     }
@@ -1787,7 +2462,8 @@ void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long 
     // SM, levels from lc on solved per cluster) when the fused rows exist and K clusters of
     // kSmCtas can be co-resident
     bool sec = false;
-    int K = 0;
+    const bool gridc = g.fused && g.dense;  // dense coarsest solved by all CTAs (no cluster levels)
+    int K = 0, nbg = 0;
     cudaLaunchConfig_t scfg = {};
     cudaLaunchAttribute sattr[2];
     if (!cluster && g.fused && g.levels >= 2) {
@@ -1796,7 +2472,23 @@ void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long 
             sm_state = cudaFuncSetAttribute(k_mg_pcg_sm, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmBytes) == cudaSuccess ? 1 : -1;
             cudaGetLastError();
         }
-        if (sm_state > 0) {
+        if (sm_state > 0 && gridc) {
+            // dense coarsest on all CTAs: no clusters, one CTA per SM
+            int occ = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mg_pcg_sm, kSmThreads, kSmBytes) == cudaSuccess && occ >= 1) {
+                nbg = std::max(1, std::min({num_sms * occ, num_sms, ceil_div(n, 128)}));
+                scfg.gridDim = dim3(nbg);
+                scfg.blockDim = dim3(kSmThreads);
+                scfg.dynamicSmemBytes = kSmBytes;
+                scfg.stream = s;
+                sattr[0].id = cudaLaunchAttributeCooperative;
+                sattr[0].val.cooperative = 1;
+                scfg.attrs = sattr;
+                scfg.numAttrs = 1;
+                sec = true;
+            }
+            cudaGetLastError();
+        } else if (sm_state > 0) {
             K = std::max(1, std::min({ceil_div(n, kSmCtas * kSmThreads), kSmMaxClusters, num_sms / kSmCtas}));
             scfg.gridDim = dim3(K * kSmCtas);
             scfg.blockDim = dim3(kSmThreads);
@@ -1822,7 +2514,7 @@ void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long 
     if (g.fused && !sec) throw Fail{CICY_E_INTERNAL, "multigrid: the clustered kernel cannot be launched for a hierarchy built for it"};
     int nb = kMgClusterCtas;
     if (sec) {
-        nb = K * kSmCtas;
+        nb = gridc ? nbg : K * kSmCtas;
     } else if (!cluster) {
         int occ = 0;
         CICY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mg_pcg<false>, kMgThreads, 0));
@@ -1835,7 +2527,7 @@ void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long 
         // levels lc .. coarsest per cluster: r and z above lc, zf from lc on, K copies each
         const int C = g.levels - 1;
         int lc = C;
-        for (int l = 1; l <= C; l++)
+        for (int l = 1; l <= C && !gridc; l++)
             if (g.L[l].n <= kSmRows) {
                 lc = l;
                 break;
@@ -1866,7 +2558,7 @@ void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long 
                 d.r = L.r.get();
                 d.z = L.z.get();
             }
-            if (l >= lc) {
+            if (l >= lc && !gridc) {
                 L.zf_cl.ensure((size_t)K * L.n + 1);
                 d.zf = L.zf_cl.get();
                 d.priv |= 2;
@@ -1876,9 +2568,11 @@ void pcg_solve_mg(SolverWork& w, const SolverSystem& sys, double tol, long long 
         }
         g.sec_lv.ensure(sizeof(MgSmLevel) * (C + 1));
         CICY_CUDA(cudaMemcpyAsync(g.sec_lv.get(), hl.data(), sizeof(MgSmLevel) * (C + 1), cudaMemcpyHostToDevice, s));
-        g.cl_fail.ensure(K);
-        CICY_CUDA(cudaMemsetAsync(g.cl_fail.get(), 0, sizeof(int32_t) * K, s));
+        const int ncl = ceil_div(nb, kSmCtas);
+        g.cl_fail.ensure(ncl);
+        CICY_CUDA(cudaMemsetAsync(g.cl_fail.get(), 0, sizeof(int32_t) * ncl, s));
         sa.lc = lc;
+        sa.grid_coarse = gridc ? 1 : 0;
         sa.lv = reinterpret_cast<const MgSmLevel*>(g.sec_lv.get());
         sa.cl_fail = g.cl_fail.get();
         sa.mptr0 = g.L[0].mptr.get();

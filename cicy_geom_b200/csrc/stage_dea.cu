@@ -997,7 +997,8 @@ DeaSystem* solve_dea(Ctx& c, const cicy_params& p, const SolveInput& in, DBuf<in
         if (c.solver.preconditioner == CICY_PRECOND_MG && n > 0) {
             build_block_preconditioner(c.sw, ss, NMc, c.chain_start.get(), c.chain_len.get(), nullptr, nullptr, false, s, c.launches);
             tr.mark(r_flag ? "dea.real.blocks" : "dea.unit.blocks");
-            build_mg_hierarchy(c.sw, ss, s, c.launches, mg_fused_path(n, !(c.solver.flags & CICY_SOLVER_NO_CLUSTER)));
+            build_mg_hierarchy(c.sw, ss, s, c.launches, mg_fused_path(n, !(c.solver.flags & CICY_SOLVER_NO_CLUSTER)),
+                               !(c.solver.flags & CICY_SOLVER_NO_SMOOTHED), c.status.get());
             tr.mark(r_flag ? "dea.real.mg_setup" : "dea.unit.mg_setup");
             pcg_solve_mg(c.sw, ss, tol, max_iter, !(c.solver.flags & CICY_SOLVER_NO_CLUSTER), c.num_sms, c.status.get(), s, c.launches,
                          st);

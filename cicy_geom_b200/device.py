@@ -67,10 +67,13 @@ class Context:
     def stream(self) -> int:
         return lib().cicy_ctx_stream(self._h) or 0
 
-    def set_solver(self, precision: int = 0, preconditioner: int = 0, max_iter_factor: int = 300, cluster: bool = True):
+    def set_solver(self, precision: int = 0, preconditioner: int = 0, max_iter_factor: int = 300, cluster: bool = True,
+                   smoothed: bool = True):
         """precision: 0 FP64, 1 mixed; preconditioner: 0 Jacobi (upstream), 1 learned, 2 chain blocks, 3 multigrid;
-        cluster: allow the cluster-resident solver for systems that fit in shared memory."""
-        o = _abi.SolverOpts(precision, preconditioner, max_iter_factor, 0 if cluster else 1)
+        cluster: allow the cluster-resident solver for systems that fit in shared memory; smoothed: the multigrid
+        hierarchy above 20,000 rows smooths its first pairwise prolongator (CICY_SOLVER_NO_SMOOTHED when false)."""
+        flags = (0 if cluster else _abi.SOLVER_NO_CLUSTER) | (0 if smoothed else _abi.SOLVER_NO_SMOOTHED)
+        o = _abi.SolverOpts(precision, preconditioner, max_iter_factor, flags)
         self._check(lib().cicy_ctx_set_solver(self._h, C.byref(o)), "cicy_ctx_set_solver")
         if preconditioner == 1 and not self._learned:
             from .learned import default_params

@@ -121,10 +121,13 @@ typedef struct {
     int32_t precision;        /* cicy_precision */
     int32_t preconditioner;   /* cicy_preconditioner */
     int32_t max_iter_factor;  /* max iterations = factor * nodes (upstream 300, Direct_Electrifying.cpp:1559) */
-    int32_t flags;            /* bit 0: never use the cluster-resident solver (grid-wide persistent kernel only) */
+    int32_t flags;            /* bit 0: never use the cluster-resident solver (grid-wide persistent kernel only);
+                                 bit 1: multigrid above 20,000 rows keeps its first pairwise prolongator piecewise
+                                 constant (no smoothing) */
 } cicy_solver_opts;
 
 #define CICY_SOLVER_NO_CLUSTER 1
+#define CICY_SOLVER_NO_SMOOTHED 2
 
 /* One DEA linear solve (unit-resistor or real-resistor pass) of one cluster. */
 typedef struct {

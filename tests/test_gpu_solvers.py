@@ -109,7 +109,9 @@ def test_multigrid_matches_jacobi_on_a_medium_network(medium):
 
 def test_multigrid_cluster_and_grid_kernels_agree(cuda_ok):
     """The 16-CTA cluster kernel (systems up to 20k rows) and the grid-wide
-    kernel run the same iteration."""
+    kernel (smoothed level-1 prolongator, dense coarsest of up to 1,280 rows
+    solved on all CTAs) converge to the same answer; the grid-wide hierarchy
+    is the stronger one."""
     cfg, net, z = golden_network("c1p_1200_s1")
     cfg.tolerance = 1e-10
     out = []
@@ -121,9 +123,11 @@ def test_multigrid_cluster_and_grid_kernels_agree(cuda_ok):
     a, b = out
     for sa, sb in zip(a.solves[: a.n_solves], b.solves[: b.n_solves]):
         assert sa.kernel == sb.kernel == 2
-        assert abs(sa.iterations - sb.iterations) <= 2
+        assert sb.iterations <= sa.iterations + 2
         assert sa.rel_residual <= 1.01e-10 and sb.rel_residual <= 1.01e-10
-    np.testing.assert_allclose(a.resistances[0], b.resistances[0], rtol=1e-9)
+    # two different preconditioners stopped at a 1e-10 relative residual: R agrees to the
+    # solves' accuracy (each is within 1e-9 of an FP64 direct solve in the tests above)
+    np.testing.assert_allclose(a.resistances[0], b.resistances[0], rtol=5e-9)
 
 
 def test_spmv_matches_scipy(medium):
