@@ -56,7 +56,6 @@ constexpr int kMgClusterCtas = 16;            // non-portable cluster size
 constexpr int kMgClusterMaxRows = 20000;  // above this the grid-wide variant (more threads per row) is faster on B200
 constexpr int kMgMaxRestarts = 24;
 constexpr double kOmega0 = 0.95;
-constexpr int kGjThreads = 512;
 
 int grid_for(long long n, int threads = 256) {
     long long b = (n + threads - 1) / threads;
@@ -161,46 +160,44 @@ __global__ void k_dense_coarse(int nc, const int32_t* __restrict__ rp, const int
 constexpr int kGjBlock = 32;
 constexpr int kGjDS = kGjBlock + 1;  // row stride of a diagonal block in shared memory
 
-// One warp: D <- D^-1 in place (m x m, row stride kGjDS); a variable whose pivot is not
-// above thr is dropped (its row and column of D^-1 are zero).  Lane j holds column j in
-// registers for the whole elimination and the pivot column is broadcast by shuffles, so a
-// pivot step has no shared-memory round trips.
-__device__ __forceinline__ void gj_warp_invert(double* D, int m, double thr, int j) {
-    double col[kGjBlock];
-#pragma unroll
-    for (int i = 0; i < kGjBlock; i++) col[i] = (i < m && j < m) ? D[i * kGjDS + j] : 0.0;
-#pragma unroll
+// The CTA's kGjThreads (512) threads: D <- D^-1 in place (32 x 32, row stride kGjDS; a smaller
+// block is padded with the identity, which stays decoupled); a variable whose pivot is not
+// above thr is dropped (its row and column of D^-1 are zero).  Thread t holds column t % 32 of
+// rows t / 32 and t / 32 + 16 in registers; each pivot's row and column go through shared
+// memory (fcol, frow), two barriers per pivot, so the pivot chain is a barrier, a division and
+// one FMA per step rather than a warp's serial sweep over the block.
+constexpr int kGjThreads = 512;
+__device__ __forceinline__ void gj_cta_invert(double* D, double* fcol, double* frow, double thr) {
+    static_assert(kGjThreads == 16 * kGjBlock, "two entries of the 32 x 32 block per thread");
+    const int t = threadIdx.x, j = t & 31, i0 = t >> 5, i1 = i0 + 16;
+    double a0 = D[i0 * kGjDS + j], a1 = D[i1 * kGjDS + j];
     for (int k = 0; k < kGjBlock; k++) {
-        if (k < m) {  // warp-uniform
-            const double p = __shfl_sync(0xffffffffu, col[k], k);
-            if (!(p > thr)) {  // vanishing pivot: drop variable k (row k and column k)
-                col[k] = 0.0;
-                if (j == k) {
-#pragma unroll
-                    for (int i = 0; i < kGjBlock; i++) col[i] = 0.0;
-                }
-            } else {
-                const double dk = ((j == k) ? 1.0 : col[k]) / p;  // the new pivot row
-#pragma unroll
-                for (int i = 0; i < kGjBlock; i++) {
-                    if (i == k) continue;
-                    const double fi = __shfl_sync(0xffffffffu, col[i], k);  // D[i][k] before this step
-                    col[i] = ((j == k) ? 0.0 : col[i]) - fi * dk;
-                }
-                col[k] = dk;
-            }
+        if (j == k) {
+            fcol[i0] = a0;
+            fcol[i1] = a1;
         }
+        if (i0 == k) frow[j] = a0;
+        if (i1 == k) frow[j] = a1;
+        __syncthreads();
+        const double p = frow[k];
+        if (!(p > thr)) {  // vanishing pivot: drop variable k (row k and column k)
+            if (i0 == k || j == k) a0 = 0.0;
+            if (i1 == k || j == k) a1 = 0.0;
+        } else {
+            const double dk = ((j == k) ? 1.0 : frow[j]) / p;  // the new pivot row
+            a0 = (i0 == k) ? dk : ((j == k) ? 0.0 : a0) - fcol[i0] * dk;
+            a1 = (i1 == k) ? dk : ((j == k) ? 0.0 : a1) - fcol[i1] * dk;
+        }
+        __syncthreads();
     }
-    if (j < m) {
-#pragma unroll
-        for (int i = 0; i < kGjBlock; i++)
-            if (i < m) D[i * kGjDS + j] = col[i];
-    }
-    __syncwarp();
+    D[i0 * kGjDS + j] = a0;
+    D[i1 * kGjDS + j] = a1;
+    __syncthreads();
 }
 
 __global__ void __launch_bounds__(kGjThreads) k_gauss_jordan(int n, double* __restrict__ M) {
     extern __shared__ double S[];  // n * n, then Cb (n x 32), Rb (32 x n), D (32 x 33), f (32)
+    __shared__ double gj_fcol[kGjBlock], gj_frow[kGjBlock];
     double* Cb = S + (size_t)n * n;
     double* Rb = Cb + (size_t)n * kGjBlock;
     double* D = Rb + (size_t)kGjBlock * n;
@@ -220,11 +217,13 @@ __global__ void __launch_bounds__(kGjThreads) k_gauss_jordan(int n, double* __re
     constexpr int DS = kGjDS;
     for (int b0 = 0; b0 < n; b0 += kGjBlock) {
         const int m = min(kGjBlock, n - b0);
-        for (int e = t; e < m * m; e += kGjThreads) D[(e / m) * DS + e % m] = S[(b0 + e / m) * n + b0 + e % m];
+        for (int e = t; e < kGjBlock * kGjBlock; e += kGjThreads) {
+            const int r = e / kGjBlock, c = e % kGjBlock;
+            D[r * DS + c] = (r < m && c < m) ? S[(b0 + r) * n + b0 + c] : (r == c ? 1.0 : 0.0);
+        }
         for (int e = t; e < n * m; e += kGjThreads) Cb[(e / m) * kGjBlock + e % m] = S[(e / m) * n + b0 + e % m];
         __syncthreads();
-        if (t < 32) gj_warp_invert(D, m, thr, t);
-        __syncthreads();
+        gj_cta_invert(D, gj_fcol, gj_frow, thr);
         // Rb = D^-1 S_bo (columns outside the block)
         for (int e = t; e < m * n; e += kGjThreads) {
             const int ii = e / n, jc = e % n;
@@ -401,19 +400,23 @@ __device__ __forceinline__ bool mg_sync(unsigned long long* bar, unsigned long l
 // inside it S_ij = -S_ib (D^-1)_j (rows outside), S_bj = (D^-1)_j.  The products sum over the
 // block's pivots in order, as k_gauss_jordan's do.
 constexpr int kGjgThreads = 512;
+static_assert(kGjgThreads == kGjThreads, "gj_cta_invert runs on the whole CTA");
 constexpr int kMgDenseGridMax = 1280;  // largest dense coarsest (the grid Gauss-Jordan's strip budget)
-constexpr int kGjgMaxStrip = 12;       // columns per CTA strip (the launch uses at least n / 12 CTAs)
+constexpr int kGjgMaxStrip = 10;       // columns per CTA strip (the launch uses at least n / 10 CTAs)
+static_assert(kMgDenseGridMax <= 3 * kGjgThreads, "the grid Gauss-Jordan updates three rows per thread");
 
+template <int W>
 __global__ void __launch_bounds__(kGjgThreads) k_gauss_jordan_grid(int n, double* __restrict__ M, double* __restrict__ panel,
                                                                    unsigned long long* bar, unsigned long long* dmax_bits, int* err,
                                                                    long long limit) {
     extern __shared__ double gsm[];
     __shared__ double Dm[kGjBlock * kGjDS];
+    __shared__ double R[kGjBlock * W];  // the block rows' new values on the strip (rows past the block: 0)
+    __shared__ double gj_fcol[kGjBlock], gj_frow[kGjBlock];
     __shared__ int s_ok;
     const int G = gridDim.x, t = threadIdx.x;
     const int c0 = (int)((long long)n * blockIdx.x / G), c1 = (int)((long long)n * (blockIdx.x + 1) / G), w = c1 - c0;
-    double* S = gsm;                   // the strip, column-major: S[jj * n + i] = M[i][c0 + jj]
-    double* R = S + (size_t)n * w;     // kGjBlock x w: the block rows' new values on the strip
+    double* S = gsm;  // the strip, column-major: S[jj * n + i] = M[i][c0 + jj]
     unsigned long long target = 0;
     // the strip, its regularised diagonal, and the largest diagonal (the drop threshold)
     for (int e = t; e < n * w; e += kGjgThreads) {
@@ -428,81 +431,100 @@ __global__ void __launch_bounds__(kGjgThreads) k_gauss_jordan_grid(int n, double
         atomicMax(dmax_bits, (unsigned long long)__double_as_longlong(m));  // non-negative: the bits order as the values
     }
     __syncthreads();
-    // panel of block 0 (columns 0 .. 31, column-major) from the strips that hold them
+    // panel of block 0 (columns 0 .. 31, column-major; columns past n are zero) from the strips holding them
     for (int e = t; e < n * w; e += kGjgThreads) {
         const int jj = e / n, i = e % n, j = c0 + jj;
         if (j < kGjBlock) panel[(size_t)j * n + i] = S[e];
     }
+    if (blockIdx.x == 0)
+        for (int e = n * n < kGjBlock * n ? n * n + t : kGjBlock * n; e < kGjBlock * n; e += kGjgThreads) panel[e] = 0.0;
     if (!mg_sync(bar, target, err, &s_ok, limit)) return;
     const double thr = 1e-12 * __longlong_as_double((long long)__ldcg(dmax_bits));
     const int nblk = (n + kGjBlock - 1) / kGjBlock;
     for (int bk = 0; bk < nblk; bk++) {
         const int b0 = bk * kGjBlock, m = min(kGjBlock, n - b0);
-        const double* P = panel + (size_t)(bk & 1) * n * kGjBlock;  // P[kk * n + i] = S[i][b0 + kk]
+        const double* P = panel + (size_t)(bk & 1) * n * kGjBlock;  // P[kk * n + i] = S[i][b0 + kk] (0 for kk >= m)
         double* Pn = panel + (size_t)((bk + 1) & 1) * n * kGjBlock;
-        for (int e = t; e < m * m; e += kGjgThreads) {
-            const int c = e / m, r = e % m;
-            Dm[r * kGjDS + c] = __ldcg(&P[(size_t)c * n + b0 + r]);
+        for (int e = t; e < kGjBlock * kGjBlock; e += kGjgThreads) {
+            const int c = e / kGjBlock, r = e % kGjBlock;
+            Dm[r * kGjDS + c] = (r < m && c < m) ? __ldcg(&P[(size_t)c * n + b0 + r]) : (r == c ? 1.0 : 0.0);
         }
         __syncthreads();
-        if (t < 32) gj_warp_invert(Dm, m, thr, t);
-        __syncthreads();
+        gj_cta_invert(Dm, gj_fcol, gj_frow, thr);
         // X = the block rows' new values on the strip: D^-1 S_b,j outside the block, (D^-1)_j inside
-        for (int e = t; e < m * w; e += kGjgThreads) {
-            const int ii = e / w, jj = e % w, j = c0 + jj;
-            double v;
-            if (j >= b0 && j < b0 + m) {
-                v = Dm[ii * kGjDS + (j - b0)];
-            } else {
-                v = 0;
-                for (int kk = 0; kk < m; kk++) v += Dm[ii * kGjDS + kk] * S[(size_t)jj * n + b0 + kk];
+        for (int e = t; e < kGjBlock * W; e += kGjgThreads) {
+            const int ii = e / W, jj = e % W, j = c0 + jj;
+            double v = 0;
+            if (ii < m && jj < w) {
+                if (j >= b0 && j < b0 + m) {
+                    v = Dm[ii * kGjDS + (j - b0)];
+                } else {
+                    for (int kk = 0; kk < m; kk++) v += Dm[ii * kGjDS + kk] * S[(size_t)jj * n + b0 + kk];
+                }
             }
-            R[ii * w + jj] = v;
+            R[e] = v;
         }
         __syncthreads();
-        // rows: thread per row; S_ij <- (j in the block ? 0 : S_ij) - sum_k S_ik X_kj, the panel row
-        // read in two halves, the sums over the block's pivots in order
-        for (int i = t; i < n; i += kGjgThreads) {
-            if (i >= b0 && i < b0 + m) {
-                for (int jj = 0; jj < w; jj++) S[(size_t)jj * n + i] = R[(i - b0) * w + jj];
-                continue;
-            }
-            double acc[kGjgMaxStrip];
+        // rows: three per thread (t, t + 512, t + 1024); S_ij <- (j in the block ? 0 : S_ij) - sum_k S_ik X_kj,
+        // the sums over the block's pivots in order; the block's own rows take X
+        constexpr int RPT = 3;
+        int ri[RPT];
+        bool live[RPT], upd[RPT];
 #pragma unroll
-            for (int jj = 0; jj < kGjgMaxStrip; jj++) acc[jj] = 0.0;
+        for (int q = 0; q < RPT; q++) {
+            ri[q] = t + q * kGjgThreads;
+            live[q] = ri[q] < n;
+            upd[q] = live[q] && !(ri[q] >= b0 && ri[q] < b0 + m);
+        }
+        double acc[RPT][W];
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
-                double ph[kGjBlock / 2];
+        for (int q = 0; q < RPT; q++)
 #pragma unroll
-                for (int u = 0; u < kGjBlock / 2; u++) {
-                    const int kk = h * (kGjBlock / 2) + u;
-                    ph[u] = kk < m ? __ldcg(&P[(size_t)kk * n + i]) : 0.0;
+            for (int jj = 0; jj < W; jj++) acc[q][jj] = 0.0;
+#pragma unroll
+        for (int kc = 0; kc < kGjBlock; kc += 4) {
+            double ph[RPT][4];
+#pragma unroll
+            for (int q = 0; q < RPT; q++)
+#pragma unroll
+                for (int u = 0; u < 4; u++) ph[q][u] = upd[q] ? __ldcg(&P[(size_t)(kc + u) * n + ri[q]]) : 0.0;
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+                for (int jj = 0; jj < W; jj++) {
+                    const double x = R[(kc + u) * W + jj];
+#pragma unroll
+                    for (int q = 0; q < RPT; q++) acc[q][jj] += ph[q][u] * x;
                 }
+        }
 #pragma unroll
-                for (int u = 0; u < kGjBlock / 2; u++) {
-                    const int kk = h * (kGjBlock / 2) + u;
+        for (int q = 0; q < RPT; q++) {
+            if (!live[q]) continue;
+            const int i = ri[q];
 #pragma unroll
-                    for (int jj = 0; jj < kGjgMaxStrip; jj++)
-                        if (jj < w && kk < m) acc[jj] += ph[u] * R[kk * w + jj];
-                }
-            }
-#pragma unroll
-            for (int jj = 0; jj < kGjgMaxStrip; jj++) {
-                if (jj < w) {
-                    const int j = c0 + jj;
+            for (int jj = 0; jj < W; jj++) {
+                if (jj >= w) continue;
+                const int j = c0 + jj;
+                double v;
+                if (!upd[q]) {
+                    v = R[(i - b0) * W + jj];
+                } else {
                     const double old = (j >= b0 && j < b0 + m) ? 0.0 : S[(size_t)jj * n + i];
-                    S[(size_t)jj * n + i] = old - acc[jj];
+                    v = old - acc[q][jj];
                 }
+                S[(size_t)jj * n + i] = v;
             }
         }
         __syncthreads();
-        // the next block's panel from the strips that hold its columns
+        // the next block's panel (columns past n zero) from the strips that hold its columns
         if (bk + 1 < nblk) {
             const int nb0 = b0 + kGjBlock, nm = min(kGjBlock, n - nb0);
             for (int e = t; e < n * w; e += kGjgThreads) {
                 const int jj = e / n, i = e % n, j = c0 + jj;
                 if (j >= nb0 && j < nb0 + nm) Pn[(size_t)(j - nb0) * n + i] = S[e];
             }
+            if (blockIdx.x == 0)
+                for (int e = nm * n + t; e < kGjBlock * n; e += kGjgThreads) Pn[e] = 0.0;
         }
         if (!mg_sync(bar, target, err, &s_ok, limit)) return;
     }
@@ -2366,17 +2388,30 @@ void build_mg_hierarchy(SolverWork& w, const SolverSystem& sys, cudaStream_t s, 
         CICY_CUDA(cudaMemsetAsync(g.cinv.get(), 0, sizeof(double) * nC * nC, s));
         k_dense_coarse<<<grid_for(nC, 128), 128, 0, s>>>(nC, Lc.rp.get(), Lc.ci.get(), Lc.val.get(), Lc.diag.get(), g.cinv.get());
         const int G = std::max(1, std::min(sms, nC));
-        const int wmax = (nC + G - 1) / G + 1;
-        if ((nC + G - 1) / G > kGjgMaxStrip) throw Fail{CICY_E_INTERNAL, "multigrid: dense coarsest too large for this GPU"};
-        const size_t smem = sizeof(double) * ((size_t)nC * wmax + (size_t)kGjBlock * wmax);
-        CICY_CUDA(cudaFuncSetAttribute(k_gauss_jordan_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const int wmax = (nC + G - 1) / G;
+        if (wmax > kGjgMaxStrip) throw Fail{CICY_E_INTERNAL, "multigrid: dense coarsest too large for this GPU"};
+        const size_t smem = sizeof(double) * (size_t)nC * wmax;
+        void (*kern)(int, double*, double*, unsigned long long*, unsigned long long*, int*, long long) = nullptr;
+        switch (wmax) {
+            case 1: kern = k_gauss_jordan_grid<1>; break;
+            case 2: kern = k_gauss_jordan_grid<2>; break;
+            case 3: kern = k_gauss_jordan_grid<3>; break;
+            case 4: kern = k_gauss_jordan_grid<4>; break;
+            case 5: kern = k_gauss_jordan_grid<5>; break;
+            case 6: kern = k_gauss_jordan_grid<6>; break;
+            case 7: kern = k_gauss_jordan_grid<7>; break;
+            case 8: kern = k_gauss_jordan_grid<8>; break;
+            case 9: kern = k_gauss_jordan_grid<9>; break;
+            default: kern = k_gauss_jordan_grid<10>; break;
+        }
+        CICY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         double* M = g.cinv.get();
         double* panel = g.gj_panel.get();
         unsigned long long* bar = g.gj_sync.get();
         unsigned long long* dmax = g.gj_sync.get() + 1;
         long long limit = w.spin_limit;
         void* args[] = {&nC, &M, &panel, &bar, &dmax, &err, &limit};
-        CICY_CUDA(cudaLaunchCooperativeKernel((void*)k_gauss_jordan_grid, dim3(G), dim3(kGjgThreads), args, smem, s));
+        CICY_CUDA(cudaLaunchCooperativeKernel((void*)kern, dim3(G), dim3(kGjgThreads), args, smem, s));
         launches += 2;
         g.dense = true;
     }
