@@ -51,7 +51,7 @@ METRIC = "networks solved/s at 1e-8 residual (25k-CNT 6um network, full hot path
 DATA = "synthetic (seeded CNT polylines of the workload's length, radius and step statistics; one independent network per GPU)"
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "ref_dump")
 PRECONDS = {"jacobi": 0, "learned": 1, "chain": 2, "mg": 3}
-MG_DRAM_BYTES_PER_ROW = 245.0  # ncu: k_mg_pcg_sm DRAM read + write per launch / free rows (8k-CNT network: 233 and 258 B)
+MG_DRAM_BYTES_PER_ROW = 660.0  # ncu: k_mg_pcg_sm DRAM read + write per launch / free rows (8k-CNT network: 589 and 747 B)
 KERNELS = {0: "k_pcg (grid-wide persistent PCG)", 1: "k_pcg_cluster (16-CTA cluster-resident PCG)",
            2: "k_mg_pcg (chain-aggregation multigrid PCG)"}
 
@@ -741,9 +741,9 @@ def run_ours(args):
             "roofline": {"kernel": KERNELS[top], "bound": "hbm", "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                          "traffic_note": "bytes per launch scaled by rows from an ncu capture of the same kernel on the "
-                                         "8k-CNT network (DRAM read + write, 245 B per free row: the system and hierarchy read "
-                                         "once into shared memory and L2); the algorithmic bytes per launch are ~45x larger "
-                                         "because the system stays on chip across iterations",
+                                         "8k-CNT network (DRAM read + write, 660 B per free row: the system, the hierarchy and "
+                                         "the dense coarsest inverse read once into shared memory and L2); the algorithmic bytes "
+                                         "per launch are several times larger because the system stays on chip across iterations",
                          "algorithmic_bytes_per_launch": k_bytes / k_launch if k_launch else None,
                          "launches_per_step": k_launch / args.steps, "share_of_step": k_sec / t_dev,
                          "note": "algorithmic bytes = iterations x (SpMV + 12 vector passes) of the solves this kernel ran; "
