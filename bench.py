@@ -16,7 +16,9 @@ Metric: networks solved per second.
 
 `ours`: `value` times the device path with the network already resident in
 HBM; `e2e` times the same step through the C ABI from pinned host buffers
-(upload of the window-trimmed network + solve + read-back of R).  The
+(upload of the window-trimmed network + solve + read-back of R), with two
+contexts in a pipeline (step k + 1's upload overlaps step k's device work;
+`e2e.sequential_value` is the same without the overlap).  The
 `reference` arm runs the upstream program (oracle/_ref/ref_dump, built from
 the upstream sources) on the same network files, written by numpy alone
 (cicy_geom_b200.netgen: the reference process never loads libcicy_b200.so),
@@ -351,7 +353,7 @@ def direct_voltage_error(S, x):
     return float(np.max(np.abs(x[idx] - xd)) / np.max(np.abs(xd)))
 
 
-def solver_comparison(cfg, net, device, steps=2):
+def solver_comparison(cfg, net, device, steps=3, warmup=2):
     """The same network step with each preconditioner and precision (device-resident,
     CUDA events): upstream Jacobi-PCG ("plain CG"), chain block-Jacobi, learned,
     multigrid in FP64, and Jacobi, chain and learned in mixed precision; per run
@@ -374,7 +376,8 @@ def solver_comparison(cfg, net, device, steps=2):
         params = cfg.params()
         res = Result()
         stream = torch.cuda.ExternalStream(ctx.stream(), device=device)
-        check(lib().cicy_network_to_conductance(ctx.handle, C.byref(params), C.byref(res)), "warm-up", ctx.handle)
+        for _ in range(warmup):
+            check(lib().cicy_network_to_conductance(ctx.handle, C.byref(params), C.byref(res)), "warm-up", ctx.handle)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -706,8 +709,62 @@ def run_ours(args):
         out_host.numpy()[:] = np.array(res.resistances)
     e1.record(stream)
     barrier()
+    t_seq = e0.elapsed_time(e1) * 1e-3
+    # ---- end to end, pipelined: two contexts, as a serving loop runs them ----
+    # One host thread uploads step k + 1's network into one context (host checks, pinned H2D
+    # copies on that context's stream) while this thread runs step k on the other context and
+    # reads its resistances back.  All device work of the steps is issued by this thread, one
+    # step after the other, so kernels of the two contexts never run at the same time; every
+    # step's copies and read-back are inside the timed region.
+    ctx2 = Context(local)
+    ctx2.set_solver(precision=1 if args.precision == "mixed" else 0, preconditioner=PRECONDS[args.precond], smoothed=not args.unsmoothed)
+    ctx2.upload(net)
+    res2 = Result()
+    check(L.cicy_network_to_conductance(ctx2.handle, C.byref(params), C.byref(res2)), "cicy_network_to_conductance", ctx2.handle)
+    stream2 = torch.cuda.ExternalStream(ctx2.stream(), device=local)
+    ctxs, streams, results = [ctx, ctx2], [stream, stream2], [res, res2]
+    free = [threading.Semaphore(1), threading.Semaphore(1)]
+    ready = [threading.Semaphore(0), threading.Semaphore(0)]
+    up_err = []
+
+    def uploader():
+        try:
+            for k in range(args.steps):
+                i = k % 2
+                free[i].acquire()
+                check(L.cicy_upload_network(ctxs[i].handle, C.byref(hnet)), "cicy_upload_network", ctxs[i].handle)
+                ready[i].release()
+        except Exception as e:  # noqa: BLE001
+            up_err.append(e)
+            for r_ in ready:
+                r_.release()
+
+    barrier()
+    e0.record(stream)
+    th = threading.Thread(target=uploader)
+    th.start()
+    for k in range(args.steps):
+        i = k % 2
+        ready[i].acquire()
+        if up_err:
+            break
+        with torch.cuda.stream(streams[i]):
+            flush.zero_()
+        check(L.cicy_network_to_conductance(ctxs[i].handle, C.byref(params), C.byref(results[i])), "cicy_network_to_conductance",
+              ctxs[i].handle)
+        out_host.numpy()[:] = np.array(results[i].resistances)
+        free[i].release()
+    th.join()
+    if up_err:
+        raise up_err[0]
+    last = torch.cuda.Event()
+    last.record(streams[(args.steps - 1) % 2])
+    stream.wait_event(last)
+    e1.record(stream)
+    barrier()
     t_e2e = e0.elapsed_time(e1) * 1e-3
-    t_dev, t_e2e = replicas.max_over_ranks([t_dev, t_e2e], world, device=f"cuda:{local}")
+    ctx2.close()
+    t_dev, t_e2e, t_seq = replicas.max_over_ranks([t_dev, t_e2e, t_seq], world, device=f"cuda:{local}")
     if rank == 0:
         peaks = {}
         pk_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -750,7 +807,10 @@ def run_ours(args):
                                  "the systems live in shared memory / L2, so the kernel is latency-bound (one cluster or "
                                  "grid barrier per reduction); peak is the measured HBM copy bandwidth (of measured)"},
             "contact_search": contact_search_roofline(ctx, net, res, stage_acc, args.steps, hbm),
-            "e2e": {"value": world * args.steps / t_e2e, "unit": "networks/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 24},
+            "e2e": {"value": world * args.steps / t_e2e, "unit": "networks/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 24,
+                    "pipeline": "two contexts: step k + 1's upload (host checks, pinned H2D copies) overlaps step k's device work "
+                                "and read-back; one thread issues all device work, so the contexts' kernels never overlap",
+                    "sequential_value": world * args.steps / t_seq},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "solver": {"cg_iterations": iters[: len(iters) // max(args.steps, 1)], "max_rel_residual": max(resid) if resid else None,
