@@ -27,9 +27,11 @@ cicy_status guarded(cicy_ctx* ctx, F&& f) {
         return CICY_OK;
     } catch (const cicy::Fail& e) {
         ctx->c.err = e.msg;
+        if (ctx->c.side) cudaStreamSynchronize(ctx->c.side);  // no side-stream work outlives a failed call
         return e.status;
     } catch (const std::bad_alloc&) {
         ctx->c.err = "host allocation failed";
+        if (ctx->c.side) cudaStreamSynchronize(ctx->c.side);
         return CICY_E_INTERNAL;
     }
 }
@@ -57,6 +59,9 @@ cicy_status cicy_ctx_create(cicy_ctx** out, int device) {
     cicy_status s = guarded(ctx, [](cicy::Ctx& c) {
         CICY_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
         c.own_stream = true;
+        CICY_CUDA(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
+        CICY_CUDA(cudaEventCreateWithFlags(&c.ev_main, cudaEventDisableTiming));
+        CICY_CUDA(cudaEventCreateWithFlags(&c.ev_side, cudaEventDisableTiming));
         cudaDeviceProp prop;
         CICY_CUDA(cudaGetDeviceProperties(&prop, c.device));
         c.num_sms = prop.multiProcessorCount;
@@ -78,7 +83,11 @@ cicy_status cicy_ctx_destroy(cicy_ctx* ctx) {
     if (!ctx) return CICY_OK;
     cudaSetDevice(ctx->c.device);
     if (ctx->c.stream) cudaStreamSynchronize(ctx->c.stream);
+    if (ctx->c.side) cudaStreamSynchronize(ctx->c.side);
     if (ctx->c.own_stream && ctx->c.stream) cudaStreamDestroy(ctx->c.stream);
+    if (ctx->c.side) cudaStreamDestroy(ctx->c.side);
+    if (ctx->c.ev_main) cudaEventDestroy(ctx->c.ev_main);
+    if (ctx->c.ev_side) cudaEventDestroy(ctx->c.ev_side);
     delete ctx;  // frees every device buffer of the context
     return CICY_OK;
 }
@@ -86,6 +95,7 @@ cicy_status cicy_ctx_destroy(cicy_ctx* ctx) {
 cicy_status cicy_ctx_set_stream(cicy_ctx* ctx, void* stream) {
     return guarded(ctx, [&](cicy::Ctx& c) {
         if (c.stream) CICY_CUDA(cudaStreamSynchronize(c.stream));
+        if (c.side) CICY_CUDA(cudaStreamSynchronize(c.side));
         if (c.own_stream && c.stream) CICY_CUDA(cudaStreamDestroy(c.stream));
         c.stream = (cudaStream_t)stream;
         c.own_stream = false;

@@ -93,6 +93,11 @@ struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    // second stream for the backbone and family volumes, which no later stage of the step reads:
+    // they run beside the real-resistor pass (events order them after their inputs and before
+    // the results are read)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_main = nullptr, ev_side = nullptr;
     std::string err;
     int64_t launches = 0;
     int stage = 0;  // 1 uploaded, 2 grid, 3 clusters, 4 electrical
@@ -154,6 +159,7 @@ struct Ctx {
     DBuf<int32_t> work_i32a, work_i32b, work_i32c;
     DBuf<double> work_f64a;
     RadixScratch rs;
+    RadixScratch rs_side;  // sorts issued on `side`
     DBuf<int32_t> scan_tmp32;
     DBuf<int64_t> scan_tmp64;
     // CG scratch
@@ -174,6 +180,7 @@ struct Ctx {
     // and the volume members (volumes_cnt[8], dead_branches[7], total_volumes[8], fractions[8])
     DBuf<double> vol3, vol_acc;
     DBuf<int32_t> vol_kind;
+    DBuf<int32_t> bb_pts;  // per backbone member: CNT, end points and cut points of its current-carrying part
     DBuf<uint64_t> vol_key;
     DBuf<uint32_t> vol_cnt;
     DBuf<double> vol_iso;               // whole-CNT volumes of the isolated list

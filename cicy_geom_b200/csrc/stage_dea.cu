@@ -468,6 +468,60 @@ __global__ void k_current_max(int n, const int32_t* __restrict__ eb, const int32
 // the cluster, and Calculate_cnt_volumes' (:412-556) volumes of its parts: vol3[3i] the dead
 // part before the run (the whole CNT when nothing is kept), vol3[3i+1] the run, vol3[3i+2]
 // the dead part after it; kind[i] = 0 nothing kept, 1 kept to the end, 2 dead part after.
+// The current-carrying run of one backbone member: element offsets idx1 (first element whose
+// current exceeds the zero current) and idx2 (first one after it that does not), -1 when absent.
+__device__ __forceinline__ void backbone_run(int b, int e, const int32_t* __restrict__ elem, const int32_t* __restrict__ lmm,
+                                             const double* __restrict__ volt, double zero_current, int& idx1, int& idx2) {
+    idx1 = -1;
+    idx2 = -1;
+    for (int k = 0; k < e - b - 1; k++) {
+        double I = fabs(volt[lmm[elem[b + k]]] - volt[lmm[elem[b + k + 1]]]);
+        if (I - zero_current > kZero) {
+            if (idx1 == -1) idx1 = k;
+        } else if (idx1 != -1 && idx2 == -1) {
+            idx2 = k;
+            break;
+        }
+    }
+}
+
+// Volumes of member i's parts from its end points Ps, Pe and cut points P1, P2 (-1: absent).
+__device__ __forceinline__ void backbone_volumes(int i, double r, int Ps, int P1, int P2, int Pe, const double* __restrict__ x,
+                                                 const double* __restrict__ y, const double* __restrict__ z, double* __restrict__ vol3,
+                                                 int32_t* __restrict__ kind) {
+    if (P1 < 0) {
+        vol3[3 * i] = cnt_volume(Ps, Pe, r, x, y, z);
+        kind[i] = 0;
+    } else {
+        vol3[3 * i] = cnt_volume(Ps, P1, r, x, y, z);
+        if (P2 < 0) {
+            vol3[3 * i + 1] = cnt_volume(P1, Pe, r, x, y, z);
+            kind[i] = 1;
+        } else {
+            vol3[3 * i + 1] = cnt_volume(P1, P2, r, x, y, z);
+            vol3[3 * i + 2] = cnt_volume(P2, Pe, r, x, y, z);
+            kind[i] = 2;
+        }
+    }
+}
+
+__device__ __forceinline__ void backbone_trim(int i, int c, int b, int e, int idx1, int idx2, int trim, int32_t* __restrict__ cur_lo,
+                                              int32_t* __restrict__ cur_hi, int32_t* __restrict__ alive) {
+    if (!trim) {
+        alive[i] = 1;
+        return;
+    }
+    if (idx1 == -1) {
+        cur_lo[c] = -1;
+        cur_hi[c] = -2;
+        alive[i] = 0;
+    } else {
+        cur_lo[c] = b + idx1;
+        cur_hi[c] = (idx2 == -1) ? e - 1 : b + idx2;
+        alive[i] = 1;
+    }
+}
+
 __global__ void k_backbone_cnts(int n, const int32_t* __restrict__ members, const int32_t* __restrict__ eb, const int32_t* __restrict__ ee,
                                 const int32_t* __restrict__ elem, const int32_t* __restrict__ lmm, const double* __restrict__ volt,
                                 const unsigned long long* __restrict__ imax_bits, int trim, int32_t* __restrict__ cur_lo,
@@ -477,52 +531,43 @@ __global__ void k_backbone_cnts(int n, const int32_t* __restrict__ members, cons
     const double i_max = fmax(__longlong_as_double((long long)*imax_bits), kZero);
     const double zero_current = i_max * 1e-9;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        int b = eb[i], e = ee[i];
-        int idx1 = -1, idx2 = -1;
-        for (int k = 0; k < e - b - 1; k++) {
-            double I = fabs(volt[lmm[elem[b + k]]] - volt[lmm[elem[b + k + 1]]]);
-            if (I - zero_current > kZero) {
-                if (idx1 == -1) idx1 = k;
-            } else if (idx1 != -1 && idx2 == -1) {
-                idx2 = k;
-                break;
-            }
-        }
-        int c = members[i];
-        {
-            const double r = radii[c];
-            const int Ps = elem[b], Pe = elem[e - 1];
-            if (idx1 == -1) {
-                vol3[3 * i] = cnt_volume(Ps, Pe, r, x, y, z);
-                kind[i] = 0;
-            } else {
-                const int P1 = elem[b + idx1];
-                vol3[3 * i] = cnt_volume(Ps, P1, r, x, y, z);
-                if (idx2 == -1) {
-                    vol3[3 * i + 1] = cnt_volume(P1, Pe, r, x, y, z);
-                    kind[i] = 1;
-                } else {
-                    const int P2 = elem[b + idx2];
-                    vol3[3 * i + 1] = cnt_volume(P1, P2, r, x, y, z);
-                    vol3[3 * i + 2] = cnt_volume(P2, Pe, r, x, y, z);
-                    kind[i] = 2;
-                }
-            }
-        }
-        if (!trim) {
-            alive[i] = 1;
-            continue;
-        }
-        if (idx1 == -1) {
-            cur_lo[c] = -1;
-            cur_hi[c] = -2;
-            alive[i] = 0;
-        } else {
-            cur_lo[c] = b + idx1;
-            cur_hi[c] = (idx2 == -1) ? e - 1 : b + idx2;
-            alive[i] = 1;
-        }
+        const int b = eb[i], e = ee[i];
+        int idx1, idx2;
+        backbone_run(b, e, elem, lmm, volt, zero_current, idx1, idx2);
+        const int c = members[i];
+        backbone_volumes(i, radii[c], elem[b], idx1 < 0 ? -1 : elem[b + idx1], idx2 < 0 ? -1 : elem[b + idx2], elem[e - 1], x, y, z, vol3,
+                         kind);
+        backbone_trim(i, c, b, e, idx1, idx2, trim, cur_lo, cur_hi, alive);
     }
+}
+
+// k_backbone_cnts split for the side stream: the run and the trim here, the member's CNT and
+// part end points into pts (5 per member) for k_backbone_volumes.
+__global__ void k_backbone_scan(int n, const int32_t* __restrict__ members, const int32_t* __restrict__ eb, const int32_t* __restrict__ ee,
+                                const int32_t* __restrict__ elem, const int32_t* __restrict__ lmm, const double* __restrict__ volt,
+                                const unsigned long long* __restrict__ imax_bits, int trim, int32_t* __restrict__ cur_lo,
+                                int32_t* __restrict__ cur_hi, int32_t* __restrict__ alive, int32_t* __restrict__ pts) {
+    const double i_max = fmax(__longlong_as_double((long long)*imax_bits), kZero);
+    const double zero_current = i_max * 1e-9;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int b = eb[i], e = ee[i];
+        int idx1, idx2;
+        backbone_run(b, e, elem, lmm, volt, zero_current, idx1, idx2);
+        const int c = members[i];
+        pts[5 * i] = c;
+        pts[5 * i + 1] = elem[b];
+        pts[5 * i + 2] = idx1 < 0 ? -1 : elem[b + idx1];
+        pts[5 * i + 3] = idx2 < 0 ? -1 : elem[b + idx2];
+        pts[5 * i + 4] = elem[e - 1];
+        backbone_trim(i, c, b, e, idx1, idx2, trim, cur_lo, cur_hi, alive);
+    }
+}
+
+__global__ void k_backbone_volumes(int n, const int32_t* __restrict__ pts, const double* __restrict__ radii, const double* __restrict__ x,
+                                   const double* __restrict__ y, const double* __restrict__ z, double* __restrict__ vol3,
+                                   int32_t* __restrict__ kind) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        backbone_volumes(i, radii[pts[5 * i]], pts[5 * i + 1], pts[5 * i + 2], pts[5 * i + 3], pts[5 * i + 4], x, y, z, vol3, kind);
 }
 
 // Volume members of Backbone_Network (acc: volumes_cnt[8], dead_branches[7], then the
@@ -1094,8 +1139,31 @@ void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out) {
     c.tmp_list.ensure(std::max(std::max(n_clu_idx, n_cj_idx), 1) + 1);
     c.cur_out.ensure(4);
     c.vol_acc.ensure(kVolWords);
+    CICY_CUDA(cudaStreamWaitEvent(s, c.ev_side, 0));  // the previous step's side-stream volumes are done
     CICY_CUDA(cudaMemsetAsync(c.vol_acc.get(), 0, sizeof(double) * kVolWords, s));
     const int scope = p.simulation_scope;
+    // Calculate_percolated_families_fractions' isolated-CNT volumes (Electrical_analysis.cpp:678-756) need
+    // only the labels: on the side stream from here, beside the DEA passes
+    CICY_CUDA(cudaEventRecord(c.ev_main, s));
+    CICY_CUDA(cudaStreamWaitEvent(c.side, c.ev_main, 0));
+    const bool fractions = scope < 2 && c.n_inside > 0;
+    if (fractions) {
+        cudaStream_t ss = c.side;
+        c.vol_key.ensure(c.n_inside);
+        c.vol_cnt.ensure(c.n_inside);
+        k_isolated_keys<<<grid_for(c.n_inside), 256, 0, ss>>>(c.n_inside, c.n_labels, c.inside.get(), c.labels.get(), c.perc_bits.get(),
+                                                              c.vol_key.get(), c.vol_cnt.get());
+        radix_sort_pairs(c.vol_key.get(), c.vol_cnt.get(), c.n_inside, bits_for((uint64_t)(c.n_labels + 2) * (uint64_t)c.n_inside),
+                         c.rs_side, ss, c.launches);
+        c.vol_iso.ensure(c.n_inside);
+        CICY_CUDA(cudaMemsetAsync(c.i32_scalar.get() + 2, 0, sizeof(int32_t), ss));
+        k_isolated_volumes<<<grid_for(c.n_inside), 256, 0, ss>>>(c.n_inside, (uint64_t)(c.n_labels + 1) * (uint64_t)c.n_inside,
+                                                                 c.vol_key.get(), c.vol_cnt.get(), c.cstart.get(), c.clen.get(),
+                                                                 c.radii.get(), c.x.get(), c.y.get(), c.z.get(), c.vol_iso.get(),
+                                                                 c.i32_scalar.get() + 2);
+        c.launches += 2;
+    }
+    CICY_CUDA(cudaEventRecord(c.ev_side, c.side));
     for (int k = 0; k < c.n_perc && scope < 2; k++) {
         int32_t* members = c.bbclu_idx.get() + c.h_clu_ptr[k];
         int32_t* jl = c.bbcj_idx.get() + c.h_cj_ptr[k];
@@ -1115,10 +1183,18 @@ void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out) {
                                                       c.j_p1.get(), c.j_p2.get(), c.imax.get());
         c.vol3.ensure(3 * (size_t)std::max(NM, 1));
         c.vol_kind.ensure(std::max(NM, 1));
-        k_backbone_cnts<<<grid_for(NM), 256, 0, s>>>(NM, members, eb.get(), ee.get(), c.elem_idx.get(), c.lmm.get(), su->volt.get(),
+        c.bb_pts.ensure(5 * (size_t)std::max(NM, 1));
+        CICY_CUDA(cudaStreamWaitEvent(s, c.ev_side, 0));  // the side stream's previous volumes have read bb_pts
+        k_backbone_scan<<<grid_for(NM), 256, 0, s>>>(NM, members, eb.get(), ee.get(), c.elem_idx.get(), c.lmm.get(), su->volt.get(),
                                                    c.imax.get(), scope == 0 ? 1 : 0, c.bb_lo.get(), c.bb_hi.get(), c.alive.get(),
-                                                   c.radii.get(), c.x.get(), c.y.get(), c.z.get(), c.vol3.get(), c.vol_kind.get());
-        k_volume_sum<<<1, kSumThreads, 0, s>>>(NM, c.h_family[k], c.vol3.get(), c.vol_kind.get(), c.vol_acc.get());
+                                                   c.bb_pts.get());
+        // the volumes (read by no later stage of the step) beside the real-resistor pass
+        CICY_CUDA(cudaEventRecord(c.ev_main, s));
+        CICY_CUDA(cudaStreamWaitEvent(c.side, c.ev_main, 0));
+        k_backbone_volumes<<<grid_for(NM), 256, 0, c.side>>>(NM, c.bb_pts.get(), c.radii.get(), c.x.get(), c.y.get(), c.z.get(), c.vol3.get(),
+                                                            c.vol_kind.get());
+        k_volume_sum<<<1, kSumThreads, 0, c.side>>>(NM, c.h_family[k], c.vol3.get(), c.vol_kind.get(), c.vol_acc.get());
+        CICY_CUDA(cudaEventRecord(c.ev_side, c.side));
         c.launches += 3;
         if (scope == 0) {
             exclusive_scan_i32(c.alive.get(), c.alive_scan.get(), NM, c.i32_scalar.get(), c.scan_tmp32, s, c.launches);
@@ -1195,23 +1271,14 @@ void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out) {
     c.bb_cj_len = cj_len;
     c.have_backbone = true;
     // Calculate_percolated_families_fractions (Electrical_analysis.cpp:114-119, 678-756)
-    if (scope < 2 && c.n_inside > 0) {
-        c.vol_key.ensure(c.n_inside);
-        c.vol_cnt.ensure(c.n_inside);
-        k_isolated_keys<<<grid_for(c.n_inside), 256, 0, s>>>(c.n_inside, c.n_labels, c.inside.get(), c.labels.get(), c.perc_bits.get(),
-                                                             c.vol_key.get(), c.vol_cnt.get());
-        radix_sort_pairs(c.vol_key.get(), c.vol_cnt.get(), c.n_inside, bits_for((uint64_t)(c.n_labels + 2) * (uint64_t)c.n_inside), c.rs,
-                         s, c.launches);
-        c.vol_iso.ensure(c.n_inside);
-        CICY_CUDA(cudaMemsetAsync(c.i32_scalar.get() + 2, 0, sizeof(int32_t), s));
-        k_isolated_volumes<<<grid_for(c.n_inside), 256, 0, s>>>(c.n_inside, (uint64_t)(c.n_labels + 1) * (uint64_t)c.n_inside,
-                                                                c.vol_key.get(), c.vol_cnt.get(), c.cstart.get(), c.clen.get(),
-                                                                c.radii.get(), c.x.get(), c.y.get(), c.z.get(), c.vol_iso.get(),
-                                                                c.i32_scalar.get() + 2);
-        k_family_fractions<<<1, kSumThreads, 0, s>>>(c.i32_scalar.get() + 2, c.vol_iso.get(), c.vol_acc.get());
-        c.launches += 3;
+    if (fractions) {
+        k_family_fractions<<<1, kSumThreads, 0, c.side>>>(c.i32_scalar.get() + 2, c.vol_iso.get(), c.vol_acc.get());
+        c.launches++;
         c.have_volumes = true;
     }
+    // the main stream (and so every later read of the volumes) waits for the side stream's work
+    CICY_CUDA(cudaEventRecord(c.ev_side, c.side));
+    CICY_CUDA(cudaStreamWaitEvent(s, c.ev_side, 0));
     // Calculate_resistances_and_resistivities (Electrical_analysis.cpp:873-987)
     if (out) {
         const cicy_cuboid& w = c.window;
