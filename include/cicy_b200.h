@@ -163,8 +163,8 @@ cicy_status cicy_ctx_create(cicy_ctx** out, int device);
 cicy_status cicy_ctx_destroy(cicy_ctx* ctx);
 /* Use an external cudaStream_t (passed as void*) instead of the context's own.  The context keeps
    a second stream of its own for work no later stage reads (the backbone and family volumes);
-   every call orders that work before it returns on the main stream, so results read on the
-   main stream (or after the call) are complete. */
+   each call makes the main stream wait for it, so any later work or read on the main stream
+   (the getters included) sees it complete. */
 cicy_status cicy_ctx_set_stream(cicy_ctx* ctx, void* cuda_stream);
 void* cicy_ctx_stream(cicy_ctx* ctx);
 cicy_status cicy_ctx_set_solver(cicy_ctx* ctx, const cicy_solver_opts* opts);
