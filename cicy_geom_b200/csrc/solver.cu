@@ -460,11 +460,10 @@ void build_block_preconditioner(SolverWork& w, const SolverSystem& sys, int ncha
     k_block_fill<<<grid_for(n), 256, 0, s>>>(n, w.is_start.get(), w.start_scan.get(), w.blk_row.get());
     k_block_sizes<<<grid_for(nblk), 256, 0, s>>>(nblk, n, w.blk_row.get(), w.blk_msq.get());
     exclusive_scan_i32(w.blk_msq.get(), w.blk_off.get(), nblk, w.total.get(), w.scan_tmp, s, launches);
-    int tot = 0;
-    CICY_CUDA(cudaMemcpyAsync(&tot, w.total.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
-    CICY_CUDA(cudaStreamSynchronize(s));
-    w.tinv.ensure(std::max(tot, 1));
-    if (mixed) w.tinv32.ensure(std::max(tot, 1));
+    // the blocks' m^2 entries sum to at most kBlockMax per row: sized by that bound, no host read
+    const size_t tot = (size_t)std::max(n, 1) * kBlockMax;
+    w.tinv.ensure(tot);
+    if (mixed) w.tinv32.ensure(tot);
     w.row_off.ensure(n + 1);
     w.row_base.ensure(n + 1);
     w.row_m.ensure(n + 1);
@@ -474,7 +473,6 @@ void build_block_preconditioner(SolverWork& w, const SolverSystem& sys, int ncha
     launches += 4;
     CICY_LAUNCH_CHECK();
     w.n_blocks = nblk;
-    w.block_entries = tot;
 }
 
 void pcg_solve(SolverWork& w, const SolverSystem& sys, int precond, bool mixed, double tol, long long max_iter, int num_sms,

@@ -139,7 +139,7 @@ struct SolverWork {
     DBuf<unsigned long long> send;
     DBuf<uint16_t> code;
     DBuf<unsigned int> barrier;
-    int n_blocks = 0, block_entries = 0;
+    int n_blocks = 0;
     long long spin_limit = kSpinLimit;  // polls of a grid-barrier wait before it gives up (DEV_TIMEOUT)
     MgWork mg;
     DBuf<double> y, u;
