@@ -307,6 +307,10 @@ def lib() -> C.CDLL:
         "cicy_last_error": (C.c_char_p, [C.c_void_p]),
         "cicy_ctx_kernel_launches": (C.c_int64, [C.c_void_p]),
         "cicy_upload_network": (C.c_int, [C.c_void_p, P(Network)]),
+        "cicy_ctx_generate_cnt_network": (C.c_int, [C.c_void_p, P(GenParams)]),
+        "cicy_ctx_extract_window": (C.c_int, [C.c_void_p, P(WindowParams)]),
+        "cicy_get_network": (C.c_int, [C.c_void_p, i64p, i32p, i32p, i64p, i64p, f64p, f64p, f64p, i32p, i32p, i32p, f64p, i32p, i64p,
+                                       i32p, i64p, i32p, P(Cuboid)]),
         "cicy_contact_grid": (C.c_int, [C.c_void_p, P(Params)]),
         "cicy_clusters": (C.c_int, [C.c_void_p, P(Params)]),
         "cicy_electrical_analysis": (C.c_int, [C.c_void_p, P(Params), P(Result)]),

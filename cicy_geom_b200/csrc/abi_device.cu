@@ -127,6 +127,52 @@ cicy_status cicy_upload_network(cicy_ctx* ctx, const cicy_network* net) {
     });
 }
 
+cicy_status cicy_ctx_generate_cnt_network(cicy_ctx* ctx, const cicy_gen_params* g) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (!g) throw cicy::Fail{CICY_E_INPUT, "cicy_ctx_generate_cnt_network: null parameters"};
+        cicy::generate_network_device(c, *g);
+    });
+}
+
+cicy_status cicy_ctx_extract_window(cicy_ctx* ctx, const cicy_window_params* w) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (!w) throw cicy::Fail{CICY_E_INPUT, "cicy_ctx_extract_window: null parameters"};
+        cicy::extract_window_device(c, *w);
+    });
+}
+
+cicy_status cicy_get_network(cicy_ctx* ctx, int64_t* n_points, int32_t* n_cnts, int32_t* n_inside, int64_t* n_bcnt, int64_t* n_bpts,
+                             double* x, double* y, double* z, int32_t* flag, int32_t* cnt_start, int32_t* cnt_len, double* radii,
+                             int32_t* cnts_inside, int64_t* bcnt_ptr, int32_t* bcnt_idx, int64_t* bpts_ptr, int32_t* bpts_idx,
+                             cicy_cuboid* window) {
+    return guarded(ctx, [&](cicy::Ctx& c) {
+        if (c.stage < 1) throw cicy::Fail{CICY_E_STATE, "cicy_get_network: no network on the device"};
+        const bool faces = c.h_bcnt_ptr.size() == 7 && c.h_bpts_ptr.size() == 7;
+        const int64_t nb = faces ? c.h_bcnt_ptr[6] : 0, np = faces ? c.h_bpts_ptr[6] : 0;
+        if (n_points) *n_points = c.n_points;
+        if (n_cnts) *n_cnts = c.n_cnts;
+        if (n_inside) *n_inside = c.n_inside;
+        if (n_bcnt) *n_bcnt = nb;
+        if (n_bpts) *n_bpts = np;
+        if (window) *window = c.window;
+        d2h(c, x, c.x.get(), c.n_points);
+        d2h(c, y, c.y.get(), c.n_points);
+        d2h(c, z, c.z.get(), c.n_points);
+        d2h(c, flag, c.flag.get(), c.n_points);
+        d2h(c, cnt_start, c.cstart.get(), c.n_cnts);
+        d2h(c, cnt_len, c.clen.get(), c.n_cnts);
+        d2h(c, radii, c.radii.get(), c.n_cnts);
+        d2h(c, cnts_inside, c.inside.get(), c.n_inside);
+        d2h(c, bcnt_idx, c.bcnt_idx.get(), nb);
+        d2h(c, bpts_idx, c.bpts_idx.get(), np);
+        for (int f = 0; f < 7; f++) {
+            if (bcnt_ptr) bcnt_ptr[f] = faces ? c.h_bcnt_ptr[f] : 0;
+            if (bpts_ptr) bpts_ptr[f] = faces ? c.h_bpts_ptr[f] : 0;
+        }
+        sync(c);
+    });
+}
+
 cicy_status cicy_contact_grid(cicy_ctx* ctx, const cicy_params* p) {
     return guarded(ctx, [&](cicy::Ctx& c) {
         if (!p) throw cicy::Fail{CICY_E_INPUT, "null params"};

@@ -192,6 +192,12 @@ struct Ctx {
     GnnState gnn;
     DBuf<float> gnn_params;  // learned preconditioner parameters (cicy_ctx_set_learned_params)
 
+    // ---- network construction on the device (stage_window.cu) ----
+    DBuf<int32_t> win_cnt, win_first, win_slot, win_nev, win_face, win_off, win_keep, win_pos;
+    DBuf<int32_t> win_prun, win_pparent, win_pnev, win_cs, win_cl, win_raw_p, win_raw_c;
+    DBuf<int64_t> win_ev, win_pev;
+    DBuf<double> win_rad;
+
     // ---- CNT-GNP contacts (cicy_gnp_cnt_contacts), indexed by contact-point number ----
     int n_mix = 0;
     DBuf<int32_t> mix_point, mix_gnp;
@@ -213,6 +219,9 @@ struct MixedClusters {
 
 // Stage entry points (throw Fail on error).
 void upload_network(Ctx& c, const cicy_network& net);
+// Network construction on the device (stage_window.cu).
+void generate_network_device(Ctx& c, const cicy_gen_params& g);
+void extract_window_device(Ctx& c, const cicy_window_params& w);
 void run_contact_grid(Ctx& c, const cicy_params& p);
 void run_clusters(Ctx& c, const cicy_params& p);
 void run_electrical(Ctx& c, const cicy_params& p, cicy_result* out);

@@ -100,6 +100,52 @@ class Context:
         self._check(lib().cicy_upload_network(self._h, C.byref(v)), "cicy_upload_network")
         self._window = _abi.Cuboid(*[getattr(v.window, f) for f, _ in _abi.Cuboid._fields_])
 
+    def generate_network(self, cfg, trim: bool = True):
+        """The seeded network of generate_cnt_network(cfg) generated on the device
+        (cicy_ctx_generate_cnt_network), then, with `trim`, its window trimmed on the
+        device (cicy_ctx_extract_window): the network the host pipeline
+        generate_cnt_network(cfg).extract_window(cfg) uploads, built without the host."""
+        from .network import gen_params
+
+        g = gen_params(cfg)
+        self._check(lib().cicy_ctx_generate_cnt_network(self._h, C.byref(g)), "cicy_ctx_generate_cnt_network")
+        if trim:
+            self.extract_window(cfg)
+
+    def extract_window(self, cfg):
+        """Window 0 of the context's untrimmed network, trimmed on the device (cicy_ctx_extract_window)."""
+        wp = cfg.window_params()
+        self._check(lib().cicy_ctx_extract_window(self._h, C.byref(wp)), "cicy_ctx_extract_window")
+        w = _abi.Cuboid()
+        self._check(lib().cicy_get_network(self._h, None, None, None, None, None, None, None, None, None, None, None, None, None,
+                                           None, None, None, None, C.byref(w)), "cicy_get_network")
+        self._window = w
+
+    def network(self) -> dict:
+        """The context's network (cicy_get_network) in the layout of HostNetwork.arrays()."""
+        npt, nc, ni, nb, nq = C.c_int64(), C.c_int32(), C.c_int32(), C.c_int64(), C.c_int64()
+        self._check(lib().cicy_get_network(self._h, C.byref(npt), C.byref(nc), C.byref(ni), C.byref(nb), C.byref(nq), None, None, None,
+                                           None, None, None, None, None, None, None, None, None, None), "cicy_get_network")
+        n, c = npt.value, nc.value
+        x, y, z = (np.zeros(max(n, 1)) for _ in range(3))
+        flag = np.zeros(max(n, 1), np.int32)
+        cs, cl, ins = np.zeros(max(c, 1), np.int32), np.zeros(max(c, 1), np.int32), np.zeros(max(ni.value, 1), np.int32)
+        rad = np.zeros(max(c, 1))
+        bcp, bpp = np.zeros(7, np.int64), np.zeros(7, np.int64)
+        bci, bpi = np.zeros(max(nb.value, 1), np.int32), np.zeros(max(nq.value, 1), np.int32)
+        w = _abi.Cuboid()
+        self._check(lib().cicy_get_network(self._h, C.byref(npt), C.byref(nc), C.byref(ni), C.byref(nb), C.byref(nq), _p(x, C.c_double),
+                                           _p(y, C.c_double), _p(z, C.c_double), _p(flag, C.c_int32), _p(cs, C.c_int32),
+                                           _p(cl, C.c_int32), _p(rad, C.c_double), _p(ins, C.c_int32), _p(bcp, C.c_int64),
+                                           _p(bci, C.c_int32), _p(bpp, C.c_int64), _p(bpi, C.c_int32), C.byref(w)), "cicy_get_network")
+        cl = cl[:c].astype(np.int64)
+        sp = np.concatenate([[0], np.cumsum(cl)]).astype(np.int64)
+        sidx = np.concatenate([np.arange(s0, s0 + k, dtype=np.int64) for s0, k in zip(cs[:c], cl)]) if c else np.zeros(0, np.int64)
+        return {"x": x[:n], "y": y[:n], "z": z[:n], "flag": flag[:n], "structure_ptr": sp, "structure_idx": sidx.astype(np.int64),
+                "radii": rad[:c], "cnts_inside": ins[: ni.value], "boundary_cnt_ptr": bcp, "boundary_cnt_idx": bci[: nb.value],
+                "boundary_pts_ptr": bpp, "boundary_pts_idx": bpi[: nq.value].astype(np.int64),
+                "window": np.array([w.min_x, w.min_y, w.min_z, w.len_x, w.len_y, w.len_z, w.max_x, w.max_y, w.max_z])}
+
     def contact_grid(self, p: _abi.Params):
         self._check(lib().cicy_contact_grid(self._h, C.byref(p)), "cicy_contact_grid")
 

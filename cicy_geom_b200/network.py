@@ -207,8 +207,8 @@ def read_network_files(directory: str, file_type: str = "dat") -> HostNetwork:
     return HostNetwork(out.value)
 
 
-def generate_cnt_network(cfg: NetworkConfig) -> HostNetwork:
-    """Seeded synthetic CNT network (cicy_generate_cnt_network)."""
+def gen_params(cfg: NetworkConfig) -> _abi.GenParams:
+    """Generator parameters of a configuration (cicy_gen_params)."""
     g = _abi.GenParams()
     g.sample = cfg.sample()
     g.n_cnts = cfg.n_cnts
@@ -219,6 +219,12 @@ def generate_cnt_network(cfg: NetworkConfig) -> HostNetwork:
     g.len_max = cfg.len_max
     g.radius = cfg.radius
     g.max_turn_rad = math.radians(cfg.max_turn_deg)
+    return g
+
+
+def generate_cnt_network(cfg: NetworkConfig) -> HostNetwork:
+    """Seeded synthetic CNT network (cicy_generate_cnt_network)."""
+    g = gen_params(cfg)
     out = C.c_void_p()
     check(lib().cicy_generate_cnt_network(C.byref(g), C.byref(out)), "cicy_generate_cnt_network")
     return HostNetwork(out.value)

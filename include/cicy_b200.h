@@ -298,6 +298,16 @@ cicy_status cicy_get_hybrid_junctions(cicy_ctx* ctx, int32_t cluster, int64_t* n
 
 /* ---------------- copy-out (size query: pass NULL buffers, read the counts) ----------------
  * These fill the public members the upstream classes expose to later stages. */
+/* The context's network (after an upload, cicy_ctx_generate_cnt_network or
+ * cicy_ctx_extract_window): points (x, y, z, flag; n_points), each CNT's run
+ * (cnt_start, cnt_len; n_cnts), radii, cnts_inside (n_inside), the six faces'
+ * boundary CNT and point lists (Cutoff_Wins::boundary_cnt / boundary_flags_cnt as
+ * CSR: 7 offsets each, n_bcnt / n_bpts entries) and the window cuboid.  Any buffer
+ * may be NULL. */
+cicy_status cicy_get_network(cicy_ctx* ctx, int64_t* n_points, int32_t* n_cnts, int32_t* n_inside, int64_t* n_bcnt, int64_t* n_bpts,
+                             double* x, double* y, double* z, int32_t* flag, int32_t* cnt_start, int32_t* cnt_len, double* radii,
+                             int32_t* cnts_inside, int64_t* bcnt_ptr, int32_t* bcnt_idx, int64_t* bpts_ptr, int32_t* bpts_idx,
+                             cicy_cuboid* window);
 /* Contact_grid::sectioned_domain_cnts as CSR (n_regions + 1 offsets). */
 cicy_status cicy_get_sectioned_domain(cicy_ctx* ctx, int64_t* n_regions, int64_t* n_slots, int64_t* ptr, int64_t* idx);
 /* The point_contacts / point_contacts_dist maps of Hoshen_Kopelman::Label_cnts_in_window
@@ -484,6 +494,27 @@ typedef struct {
     int32_t reserved0;
 } cicy_window_params;
 cicy_status cicy_extract_window(const cicy_host_network* in, const cicy_window_params* w, cicy_host_network** out);
+/* The seeded synthetic network of cicy_generate_cnt_network generated on the device
+ * into the context (replaces its network; only the per-CNT point counts and runs
+ * travel to the host, for the context's bookkeeping).  Same Philox streams: point counts, structure,
+ * flags and start points equal the host generator's; later points follow from the
+ * device's sin/cos, so coordinates agree with the host generator's to rounding
+ * (~1e-13 um), not bit for bit.  The result is the untrimmed network (window =
+ * sample, no CNTs inside yet): call cicy_ctx_extract_window before the stages. */
+cicy_status cicy_ctx_generate_cnt_network(cicy_ctx* ctx, const cicy_gen_params* g);
+/* Window 0 of a single-window run trimmed on the device, in place on the context's
+ * network: Shells::Generate_shells / Find_shell (Shells.cpp:21-149) and
+ * Cutoff_Wins::Trim_boundary_cnts (Cutoff_Wins.cpp:82-276),
+ * Add_cnt_segment_to_structure (:298-467), Substitute_boundary_point (:468-548),
+ * Where_is_with_boundary (:683-743), Add_cnt_point_to_boundary_vectors (:745-769)
+ * and Fill_cnts_inside (:803-831), CNT_wires branch; equal bit for bit to
+ * cicy_extract_window on the same network.  The network must be in the layout the
+ * generator and Read_Network emit (CNT i is the i-th run of consecutive points and
+ * its points carry flag i), as after cicy_ctx_generate_cnt_network or the upload of
+ * an untrimmed network; else CICY_E_INPUT.  Limits: at most 16 segments per CNT
+ * (CICY_E_CAPACITY), min_points >= 2.  Upstream's errors (a cut point off the
+ * window, a CNT left with one point) return CICY_E_INPUT with its message. */
+cicy_status cicy_ctx_extract_window(cicy_ctx* ctx, const cicy_window_params* w);
 
 /* Read_Network::Generate_nanoparticle_network_from_file, CNT branch
  * (Read_sample_geometry + Read_cnt_data_from_dat / Read_cnt_data_from_csv,
