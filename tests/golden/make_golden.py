@@ -3,10 +3,10 @@
 Runs oracle/_ref/ref_dump (the upstream CICY_geom sources compiled in place by
 oracle/Makefile) on seeded synthetic networks and on hand-made known-answer
 networks, and stores the upstream outputs of every hot-path stage as .npz.
-Needs the upstream tree (REF_DIR, default /root/reference) only to build
-ref_dump; the fixtures themselves are self-contained.
+Needs the upstream tree only to build ref_dump (its path in the environment
+variable CICY_REF_DIR); the fixtures themselves are self-contained.
 
-    python tests/golden/make_golden.py
+    CICY_REF_DIR=<upstream CICY_geom source tree> python tests/golden/make_golden.py
 """
 from __future__ import annotations
 
@@ -133,7 +133,10 @@ def capture(name, cfg: NetworkConfig, raw: HostNetwork, full_sd: bool, store_inp
 
 def main():
     if not os.path.exists(REF):
-        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", "-j8"], check=True)
+        ref_dir = os.environ.get("CICY_REF_DIR")
+        if not ref_dir:
+            sys.exit("set CICY_REF_DIR to the upstream CICY_geom source tree to build oracle/_ref/ref_dump")
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF_DIR={ref_dir}", "-j8"], check=True)
     for name, side, n, seed, full in SEEDED:
         cfg = NetworkConfig(side=side, n_cnts=n, seed=seed)
         capture(name, cfg, generate_cnt_network(cfg), full, False)
