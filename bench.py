@@ -426,6 +426,42 @@ def contact_search_roofline(ctx, net, res, stage_acc, steps, hbm):
                     "k_pairs (one thread per region slot)"}
 
 
+def network_construction(cfg, device, args, R_step, reps=5):
+    """The step's window network built on the device (cicy_ctx_generate_cnt_network +
+    cicy_ctx_extract_window: generator and Shells + Cutoff_Wins trim in one context)
+    against the host route the timed step's inputs take (host generator, host trim,
+    upload from host memory).  Both routes' calls return with their device work
+    complete, so host wall clock times them (best of `reps`).  The device-built
+    network then runs the hot path with the step's solver settings; its R_x is
+    compared with the step's."""
+    import time as _t
+
+    from cicy_geom_b200.device import Context
+    from cicy_geom_b200.network import generate_cnt_network
+
+    with Context(device) as ctx:
+        ctx.set_solver(precision=1 if args.precision == "mixed" else 0, preconditioner=PRECONDS[args.precond], smoothed=not args.unsmoothed)
+        ctx.generate_network(cfg)  # warm-up: buffers grow to this network's size
+        dev = []
+        for _ in range(reps):
+            t0 = _t.perf_counter()
+            ctx.generate_network(cfg)
+            dev.append(_t.perf_counter() - t0)
+        host = []
+        for _ in range(2):
+            t0 = _t.perf_counter()
+            net = generate_cnt_network(cfg).extract_window(cfg)
+            ctx.upload(net)
+            host.append(_t.perf_counter() - t0)
+        ctx.generate_network(cfg)
+        r = ctx.network_to_conductance(cfg.params())
+    R = float(r.resistances[0])
+    return {"device_seconds": min(dev), "host_seconds": min(host), "speedup": min(host) / min(dev),
+            "R_x_device_built": R, "R_x_rel_diff_vs_step": abs(R - R_step) / abs(R_step) if R_step else None,
+            "note": "device: generator + window trim on the device; host: generator, Shells + Cutoff_Wins on the host, upload "
+                    "(the route of the timed step's inputs); wall clock around synchronous calls, best of the repeats"}
+
+
 def spmv_roofline(ctx, device, hbm, target_bytes=320e6, reps=20):
     """cicy_spmv_csr on copies of the unit-pass system laid out block-diagonally
     until the matrix is larger than L2 (126 MB); algorithmic bytes
@@ -830,6 +866,8 @@ def run_ours(args):
         if not args.no_comparison and world == 1:
             extra("solver_comparison", lambda: solver_comparison(cfg, net, local))
             extra("spmv", lambda: spmv_roofline(ctx, local, hbm))
+        if world == 1:
+            extra("network_construction", lambda: network_construction(cfg, local, args, R[0]))
         if args.mc > 0 and world == 1:
             extra("batched_monte_carlo", lambda: batched_monte_carlo(args.mc, local))
         if not args.no_cpu_baseline and world == 1:
