@@ -664,6 +664,10 @@ def batched_monte_carlo(count, device, reps=3):
             "gnn_forward_seconds": bs.gnn_seconds, "multigrid_setup_seconds": setup,
             "multigrid_sequential_solve_seconds": seq, "multigrid_speedup_vs_sequential": seq / out["multigrid"]["seconds"],
             "generation_and_assembly_seconds": prep,
+            "construction": info.get("construction"),
+            "generation_and_assembly_note": "per realisation, in one context: the network generated and window-trimmed on the "
+                                            "device, contacts, clusters, both DEA passes, and the real-resistor systems copied "
+                                            "to the host for the batched solves",
             "sample": "cube side U[2,5] um, CNT volume fraction U[0.5%,3%], seeds 3,000,000+k; solve stage only "
                       "(generation, contacts, clusters, assembly and the unit-resistor pass run per network before it); "
                       "learned/Jacobi: one CTA per system, the largest systems on 16-CTA clusters when the autotuner picks it, in one "

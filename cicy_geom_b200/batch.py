@@ -29,8 +29,12 @@ def monte_carlo_configs(count: int, seed0: int = 3_000_000, side=(2.0, 5.0), fra
     return out
 
 
-def realisation_systems(configs, device: int = 0, preconditioner: int = 3):
+def realisation_systems(configs, device: int = 0, preconditioner: int = 3, construction: str = "device"):
     """Run each realisation through the device path; keep its real-resistor systems.
+
+    construction "device": each network is generated and window-trimmed on the
+    device (Context.generate_network); "host": generated and trimmed on the host,
+    then uploaded.  One context serves every realisation.
 
     Returns (systems, info): systems are dicts with the full CSR (host), chains,
     right-hand side, initial guess and the per-network solver's solution and
@@ -43,16 +47,19 @@ def realisation_systems(configs, device: int = 0, preconditioner: int = 3):
 
     systems, info = [], {"realisations": len(configs), "percolating": 0, "not_percolating": 0, "rejected": 0}
     device_seconds = {}  # seed -> device time of the whole hot path (cicy_result.stage_seconds[5])
+    if construction not in ("device", "host"):
+        raise ValueError(f"construction must be 'device' or 'host', not {construction!r}")
+    ctx = Context(device)
+    ctx.set_solver(preconditioner=preconditioner)
     for cfg in configs:
-        net = generate_cnt_network(cfg).extract_window(cfg)
-        ctx = Context(device)
-        ctx.set_solver(preconditioner=preconditioner)
-        ctx.upload(net)
         try:
+            if construction == "device":
+                ctx.generate_network(cfg)
+            else:
+                ctx.upload(generate_cnt_network(cfg).extract_window(cfg))
             r = ctx.network_to_conductance(cfg.params())
         except _abi.CicyError:
             info["rejected"] += 1
-            ctx.close()
             continue
         device_seconds[cfg.seed] = float(r.stage_seconds[5])
         real = [i for i in range(r.n_solves) if r.solves[i].pass_ >= 0]
@@ -70,7 +77,8 @@ def realisation_systems(configs, device: int = 0, preconditioner: int = 3):
             systems.append({"A": full_csr(S), "b": S["b"], "x0": S["x0"], "chain_start": st, "chain_len": ln,
                             "x_ref": S["voltages"][S["reserved"]:], "seconds_ref": r.solves[i].seconds,
                             "iterations_ref": r.solves[i].iterations, "seed": cfg.seed})
-        ctx.close()
+    ctx.close()
+    info["construction"] = construction
     info["device_seconds"] = device_seconds
     return systems, info
 

@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 @pytest.fixture(scope="module")
 def mc_systems(cuda_ok):
     cfgs = BT.monte_carlo_configs(12, seed0=3_100_000, side=(2.0, 2.6), fraction=(0.012, 0.03))
-    systems, info = BT.realisation_systems(cfgs)
+    systems, info = BT.realisation_systems(cfgs, construction="host")
     assert info["percolating"] >= 6 and len(systems) >= 6
     return systems
 
