@@ -499,7 +499,7 @@ cicy_status cicy_extract_window(const cicy_host_network* in, const cicy_window_p
  * travel to the host, for the context's bookkeeping).  Same Philox streams: point counts, structure,
  * flags and start points equal the host generator's; later points follow from the
  * device's sin/cos, so coordinates agree with the host generator's to rounding
- * (~1e-13 um), not bit for bit.  The result is the untrimmed network (window =
+ * (checked within 1e-10 um), not bit for bit.  The result is the untrimmed network (window =
  * sample, no CNTs inside yet): call cicy_ctx_extract_window before the stages. */
 cicy_status cicy_ctx_generate_cnt_network(cicy_ctx* ctx, const cicy_gen_params* g);
 /* Window 0 of a single-window run trimmed on the device, in place on the context's
