@@ -49,3 +49,14 @@ def test_host_calls_reject_bad_input():
     out = C.c_void_p()
     assert L.cicy_generate_cnt_network(C.byref(g), C.byref(out)) == 1  # CICY_E_INPUT
     assert L.cicy_extract_window(None, None, C.byref(out)) == 1
+
+
+def test_device_network_construction_rejects_a_missing_context():
+    # the context-bound construction and copy-out calls check their handle before any CUDA call
+    L = _abi.lib()
+    g, w = _abi.GenParams(), _abi.WindowParams()
+    assert L.cicy_ctx_generate_cnt_network(None, C.byref(g)) == 1  # CICY_E_INPUT
+    assert L.cicy_ctx_extract_window(None, C.byref(w)) == 1
+    n = C.c_int64()
+    assert L.cicy_get_network(None, C.byref(n), None, None, None, None, None, None, None, None, None, None, None, None, None, None, None,
+                              None, None) == 1
