@@ -674,6 +674,53 @@ def batched_monte_carlo(count, device, reps=3):
                       "graph launch; multigrid: one 16-CTA cluster per system"}
 
 
+def sharded_monte_carlo(count, device, rank, world):
+    """Monte-Carlo sweep split over the ranks (replicas.shard: the realisations,
+    largest first, dealt round-robin): each rank builds its realisations' systems
+    on its GPU (device generator and window trim) and solves them in one
+    multigrid batch launch.  The sweep's time is the slowest rank's; its
+    throughput is all ranks' systems over that time.  Every rank takes the same
+    reductions, also when its own shard fails, so no rank waits on another."""
+    import time as _t
+
+    from cicy_geom_b200 import batch as BT
+    from cicy_geom_b200 import replicas
+
+    t_prep = t_solve = 0.0
+    ns, failed, err = 0, False, None
+    try:
+        all_cfgs = BT.monte_carlo_configs(count)
+        cfgs = replicas.shard(all_cfgs, [c.n_cnts for c in all_cfgs], rank, world)
+        t0 = _t.perf_counter()
+        systems, _ = BT.realisation_systems(cfgs, device=device)
+        t_prep = _t.perf_counter() - t0
+        if systems:
+            bs = BT.BatchSolver(systems, tol=TOL, device=device)
+            try:
+                setup = bs.enable_multigrid()
+                bs.set_method(1)
+                t_solve = setup + min(bs.solve() for _ in range(3))
+                _, _, fl = bs.results()
+                failed = bool((fl != 1).any())
+            finally:
+                bs.close()
+        ns = len(systems)
+    except Exception as e:  # noqa: BLE001
+        failed, err = True, f"{type(e).__name__}: {e}"
+    import torch
+
+    dev = f"cuda:{device}" if torch.cuda.is_available() else None  # NCCL reduces device tensors, gloo host tensors
+    t_solve_max, n_total, any_failed = replicas.sweep_totals(t_solve, ns, failed, world, device=dev)
+    t_prep_max, _, _ = replicas.sweep_totals(t_prep, 0, False, world, device=dev)
+    out = {"realisations": count, "ranks": world, "systems": int(n_total), "solver": "multigrid batch (one launch per rank)",
+           "solve_seconds_incl_setup_max_over_ranks": t_solve_max, "systems_per_s": n_total / t_solve_max if t_solve_max else None,
+           "preparation_seconds_max_over_ranks": t_prep_max, "failed_on_some_rank": any_failed,
+           "shard": "realisations sorted by CNT count, dealt round-robin; no data-path collective"}
+    if err:
+        out["error_on_rank_0" if rank == 0 else "error"] = err
+    return out
+
+
 def run_ours(args):
     import ctypes as C
 
@@ -805,6 +852,8 @@ def run_ours(args):
     t_e2e = e0.elapsed_time(e1) * 1e-3
     ctx2.close()
     t_dev, t_e2e, t_seq = replicas.max_over_ranks([t_dev, t_e2e, t_seq], world, device=f"cuda:{local}")
+    # N > 1: the Monte-Carlo sweep split over the ranks (every rank takes part in its reductions)
+    mc_sharded = sharded_monte_carlo(args.mc, local, rank, world) if args.mc > 0 and world > 1 else None
     if rank == 0:
         peaks = {}
         pk_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -874,6 +923,8 @@ def run_ours(args):
             extra("network_construction", lambda: network_construction(cfg, local, args, R[0]))
         if args.mc > 0 and world == 1:
             extra("batched_monte_carlo", lambda: batched_monte_carlo(args.mc, local))
+        if mc_sharded is not None:
+            line["batched_monte_carlo_sharded"] = mc_sharded
         if not args.no_cpu_baseline and world == 1:
             cb = None
             try:

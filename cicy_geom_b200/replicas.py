@@ -2,9 +2,10 @@
 
 One network's systems are too small to split across GPUs (its solve is
 latency-bound on one), so N GPUs solve N independent seeded networks, one
-process per GPU.  The only collectives are the timing barrier and the
-max-over-ranks of the measured times (NCCL on GPUs, gloo on CPU); the data
-path has none.
+process per GPU; a Monte-Carlo sweep splits its realisations over the ranks
+(`shard`).  The only collectives are the timing barrier and the reductions of
+the measured times and counts (NCCL on GPUs, gloo on CPU); the data path has
+none.
 """
 from __future__ import annotations
 
@@ -49,6 +50,35 @@ def max_over_ranks(values, world: int, device=None):
     t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return [float(v) for v in t.cpu()]
+
+
+def sum_over_ranks(values, world: int, device=None):
+    """Element-wise sum of a list of floats over all ranks."""
+    if world <= 1:
+        return [float(v) for v in values]
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return [float(v) for v in t.cpu()]
+
+
+def shard(items, sizes, rank: int, world: int):
+    """The items rank `rank` takes when independent work items (Monte-Carlo
+    realisations) are split over `world` ranks: largest first, dealt round-robin,
+    so the ranks' totals stay close; every item goes to exactly one rank."""
+    order = sorted(range(len(items)), key=lambda k: (-sizes[k], k))
+    return [items[k] for k in order[rank::world]]
+
+
+def sweep_totals(seconds: float, count: float, failed: bool, world: int, device=None):
+    """(slowest rank's seconds, total count, any rank failed) of a sharded sweep.
+    Every rank calls it once, also when its own shard failed, so all ranks take
+    the same collective steps."""
+    t = max_over_ranks([seconds, 1.0 if failed else 0.0], world, device)
+    n = sum_over_ranks([count], world, device)
+    return t[0], n[0], t[1] > 0
 
 
 def finish(world: int):
