@@ -121,6 +121,22 @@ def test_device_window_trim_equals_host_restatement(exe, tmp_path, side, n, seed
     assert len(ref["radii"]) > n
 
 
+def test_device_window_trim_edge_cases(exe, tmp_path):
+    # short CNTs far from the faces (no pieces, possibly no boundary entries), and an empty network
+    for cfg in (replace(NetworkConfig(side=6.0, n_cnts=40, seed=21), len_min=0.06, len_max=0.08),
+                NetworkConfig(side=1.0, n_cnts=0, seed=22)):
+        raw_net = generate_cnt_network(cfg)
+        raw = raw_net.arrays()
+        ref = raw_net.extract_window(cfg).arrays()
+        got = emulate(exe, tmp_path, raw, cfg)
+        assert got["status"] == 0
+        for k in ("x", "y", "z"):
+            assert np.array_equal(bits(got[k]), bits(ref[k]))
+        for k in ("flag", "structure_ptr", "structure_idx", "cnts_inside", "boundary_cnt_ptr", "boundary_cnt_idx", "boundary_pts_ptr",
+                  "boundary_pts_idx"):
+            assert np.array_equal(got[k].astype(np.int64), ref[k].astype(np.int64)), k
+
+
 def test_layout_check_rejects_a_network_out_of_generator_order(exe, tmp_path):
     cfg = NetworkConfig(side=1.0, n_cnts=50, seed=3)
     raw = generate_cnt_network(cfg).arrays()
